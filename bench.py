@@ -1,0 +1,320 @@
+#!/usr/bin/env python
+"""Benchmark: reference DM at 512^2 over a 30x30 raster (900 positions), patterns/s.
+
+One step = one DM iteration over all 900 patterns (forward propagation, modulus projection, back-propagation,
+object/probe update).  `value` is measured with the inputs resident in HBM, CUDA events on the session's
+stream, after `--warmup` untimed steps; `e2e` times the public API call (ptychopy.dmnp) end to end with the
+patterns in pinned host memory.  Multi-GPU runs (torchrun) are independent replicas, one per GPU.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DM/ePIE patterns/s at 512² (HBM roofline %); time to NRMSE≤0.05 warm vs plain"
+UNIT = "patterns/s"
+WORKLOAD = ("reference DM, 512x512 detector, 30x30 raster (900 positions), 50 nm step, lambda 2.48e-10 m, "
+            "z 1 m, dx_d 172 um, 1 probe mode, object 1027x1027, 1e7 photons/pattern")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=30)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--e2e-calls", type=int, default=2)
+    ap.add_argument("--e2e-iters", type=int, default=100, help="iterations per public-API call (the config's 100)")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """SM clock and throttle-reason samples (NVML) taken while the timed region runs."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, index, interval=0.02):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.ok = False
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            return
+        self.interval = interval
+        self.stop_ev = threading.Event()
+        self.th = threading.Thread(target=self._run, daemon=True)
+
+    def _sample(self):
+        try:
+            self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+            r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            for bit, name in self.REASONS.items():
+                if r & bit:
+                    self.reasons.add(name)
+        except Exception:
+            pass
+
+    def _run(self):
+        while not self.stop_ev.is_set():
+            self._sample()
+            time.sleep(self.interval)
+
+    def start(self):
+        if self.ok:
+            self._sample()
+            self.th.start()
+
+    def stop(self):
+        if not self.ok:
+            return None
+        self.stop_ev.set()
+        self.th.join()
+        self._sample()
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per DM iteration from the committed ncu summary (line `traffic_bytes_per_step: <int>`)."""
+    path = os.path.join(ROOT, "profiles", "dm_pipeline_512.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("traffic_bytes_per_step:"):
+            try:
+                return int(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def dataset(device):
+    """Seeded synthetic DM workload; patterns generated on `device` (torch) to keep set-up short."""
+    import numpy as np
+
+    from ptychopy_b200 import synth
+
+    cfg = synth.CONFIGS["dm512"]
+    rng = np.random.default_rng(20261204)
+    N = cfg["N"]
+    dx_s = synth.sample_pixel(cfg["lambd"], cfg["z"], cfg["dx_d"], N)
+    pos, X, Y = synth.raster_positions(cfg["nx"], cfg["ny"], cfg["step"], cfg["step"], dx_s, N)
+    obj = synth.make_object(X, Y, rng)
+    probe = synth.make_probe(N, dx_s, K=1)
+    amp = synth.make_patterns_torch(obj, probe, pos, N, cfg["photons"], seed=20261204, device=device)
+    kwargs = dict(size=N, scanDimsx=cfg["nx"], scanDimsy=cfg["ny"], stepx=cfg["step"], stepy=cfg["step"],
+                  lambd=cfg["lambd"], z=cfg["z"], dx_d=cfg["dx_d"], beamSize=synth.BEAM_FWHM, probeModes=1)
+    return dict(amp=amp, pos=pos, X=X, Y=Y, probe=probe, kwargs=kwargs, N=N, P=pos.shape[0])
+
+
+def cpu_port_rate(amp_np, ds, budget_s=15.0, threads=None):
+    """The oracle's FP32 multithreaded DM on a bounded sample: returns (patterns/s, threads, sample text)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    threads = threads or os.cpu_count() or 1
+    pos, X, Y, probe = ds["pos"], ds["X"], ds["Y"], ds["probe"]
+    n0 = min(ds["P"], 4 * threads)
+    t0, _ = pyoracle.dm_baseline_f32(amp_np[:n0], pos[:n0], probe, X, Y, 1, threads)
+    n = int(min(ds["P"], max(n0, budget_s / max(t0 / n0, 1e-9))))
+    t, _ = pyoracle.dm_baseline_f32(amp_np[:n], pos[:n], probe, X, Y, 1, threads)
+    return n / t, threads, f"1 DM iteration over {n} of the 900 patterns (512^2, FP32, {threads} threads)"
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    import numpy as np
+
+    try:
+        import torch
+
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+    except Exception:
+        dev = None
+    if dev is None:
+        print(json.dumps({"impl": "reference", "unavailable": "torch is required to generate the dataset"}))
+        return
+    ds = dataset(dev)
+    amp_np = ds["amp"].cpu().numpy().astype(np.float32)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    threads = os.cpu_count() or 1
+    # calibrate the per-step sample so the whole run stays within a few minutes
+    n0 = min(ds["P"], 4 * threads)
+    t0, _ = pyoracle.dm_baseline_f32(amp_np[:n0], ds["pos"][:n0], ds["probe"], ds["X"], ds["Y"], 1, threads)
+    per = t0 / n0
+    budget = max(1.0, 150.0 / max(args.steps + args.warmup, 1))
+    n = int(min(ds["P"], max(n0, budget / per)))
+    rates = []
+    for i in range(args.warmup + args.steps):
+        t, _ = pyoracle.dm_baseline_f32(amp_np[:n], ds["pos"][:n], ds["probe"], ds["X"], ds["Y"], 1, threads)
+        if i >= args.warmup:
+            rates.append(n / t)
+    value = statistics.median(rates)
+    sample = f"1 DM iteration over {n} of the 900 patterns per step (512^2, FP32 C++ port, {threads} threads)"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * n / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "N": 512, "positions": 900, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's CUDA sources do not build with CUDA 12.9; its DM is restated as a multithreaded "
+                "FP32 C++ port of the same equations",
+    }))
+
+
+def run_b200(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    from ptychopy_b200 import abi
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    ds = dataset("cuda")
+    N, P = ds["N"], ds["P"]
+    stream = torch.cuda.Stream()
+    s = abi.Session(**dict(ds["kwargs"], algorithm="DM", device=local))
+    s.set_stream(stream.cuda_stream)
+    s.set_patterns_ptr(ds["amp"].data_ptr(), P, N)
+    s.init()
+    for _ in range(args.warmup):
+        s.step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    l0 = s.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.start()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            s.step()
+        e1.record(stream)
+    stream.synchronize()
+    ck = clocks.stop()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = s.launches() - l0
+    obj = s.object()
+    finite = bool(np.isfinite(obj).all())
+    s.close()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = P * args.steps * world / (ms_max / 1000.0)
+    ms_step = ms_max / args.steps
+
+    # end to end through the public API: pinned host patterns -> dmnp(iter=...) -> object/probe on the host
+    import ptychopy_b200
+
+    pt = ptychopy_b200.import_ptychopy()
+    host = torch.empty((P, N, N), dtype=torch.float32, pin_memory=True)
+    host.copy_(ds["amp"])
+    amp_host = host.numpy()
+    del ds["amp"]
+    torch.cuda.empty_cache()
+    kw = dict(ds["kwargs"], iter=args.e2e_iters, returnResults=1, writeResults=0, device=local)
+    pt.dmnp(diffractionNP=amp_host, **dict(kw, iter=2))  # warm-up call
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    res = None
+    for _ in range(args.e2e_calls):
+        res = pt.dmnp(diffractionNP=amp_host, **kw)
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = P * args.e2e_iters * args.e2e_calls * world / float(t.item())
+    d2h = res[0].nbytes + res[1].nbytes
+
+    if rank == 0:
+        peak, kind = peaks()
+        XY = ds["X"] * ds["Y"]
+        bytes_step = 20 * N * N * P + 16 * XY + 16 * N * N  # psi r+w, A r; object/probe pass
+        achieved = bytes_step / (ms_step / 1000.0) / 1e9
+        traffic = profiled_traffic()
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; object GRF phase, 110 nm probe, Poisson)",
+            "config": {"workload": WORKLOAD, "N": N, "positions": P, "object": [ds["X"], ds["Y"]],
+                       "step": "one DM iteration over all 900 patterns",
+                       "l2": "inputs larger than L2 (exit waves 1.89 GB + amplitudes 0.94 GB per step)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": kind,
+                         "kernel": "DM iteration graph (fwd_rows, cols, inv_rows per wave + finalize)",
+                         "algorithmic_bytes_per_step": bytes_step},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(amp_host.nbytes),
+                    "d2h_bytes_per_step": int(d2h),
+                    "step": f"ptychopy.dmnp(iter={args.e2e_iters}) from pinned host patterns, results to host"},
+            "gpu_launches": int(launches), "clocks": ck, "finite": finite,
+        }
+        if world == 1 and not args.no_cpu:
+            rate, cores, sample = cpu_port_rate(amp_host, ds)
+            out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank)
+    else:
+        run_b200(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

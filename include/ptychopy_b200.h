@@ -1,0 +1,153 @@
+/* ptychopy_b200 — C ABI of the B200 ptychographic reconstruction engine.
+ *
+ * This is the drop-in boundary underneath the CPython module `ptychopy` (same 20 method names and keyword
+ * arguments as the reference's extension, src/ptychopy.c:117-140).  The reference has no C ABI of its own: its
+ * CPython functions drive the C++ class IPhaser directly.  Each entry point below names the reference
+ * interface whose behaviour it replaces.  All buffers are host buffers owned by the caller unless a name says
+ * `dev`; complex arrays are interleaved (re, im) float32 ("complex64"), row-major, first index = x (row).
+ *
+ * Every function returns an int status: PTY_OK (0) or a negative PTY_ERR_* code; pty_last_error() gives the
+ * message of the last failure on the calling thread.  No function calls exit(); the reference exits the
+ * process on any CUDA error (src/utilities.h:73-92) and on a negative scan position (src/ePIE.cpp:100-105).
+ */
+#ifndef PTYCHOPY_B200_H_
+#define PTYCHOPY_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PTY_OK 0
+#define PTY_ERR_INVALID (-1)   /* bad argument, shape or dtype */
+#define PTY_ERR_OOM (-2)       /* device or host allocation failed */
+#define PTY_ERR_CUDA (-3)      /* CUDA runtime error (message in pty_last_error) */
+#define PTY_ERR_STATE (-4)     /* call out of order (e.g. pty_step before pty_init) */
+#define PTY_ERR_UNSUPPORTED (-5) /* valid request this build does not implement */
+#define PTY_ERR_TIMEOUT (-6)   /* a bounded device-side wait gave up */
+#define PTY_ERR_IO (-7)        /* file could not be written */
+
+#define PTY_F32 0
+#define PTY_F64 1
+
+/* Reconstruction parameters.  Field names and meanings follow the reference's keyword arguments
+ * (src/ptychopy.c:242-246, mapped to CXParams at src/Parameters.cpp:380-653); defaults (pty_params_init) are
+ * the reference's C defaults (src/ptychopy.c:200-240).  Fields after `PPS` are additions of this engine. */
+typedef struct pty_params {
+  char jobID[128];
+  char algorithm[8];      /* "ePIE", "DM" or "MLs" */
+  char fp[256];           /* data file pattern (file ingest is not part of this engine; must be empty) */
+  int fs;
+  char hdf5path[128];
+  int dpf;
+  double beamSize;        /* m */
+  char probeGuess[256];   /* CSV probe guess file (reference format) or "" */
+  char objectGuess[256];  /* CSV object guess file or "" */
+  int size;               /* detector / probe size N */
+  int qx, qy, nx, ny;     /* file-ingest cropping (unused without file ingest) */
+  int scanDimsx, scanDimsy;
+  int spiralScan, flipScanAxis, mirror1stScanAxis, mirror2ndScanAxis;
+  double stepx, stepy;    /* m */
+  int probeModes;
+  double lambd, dx_d, z;  /* m */
+  int iter;
+  int T;                  /* wall-time limit in s (0 = none) */
+  int jitterRadius;
+  double delta_p;
+  int threshold, rotate90, sqrtData, fftShiftData, binaryOutput, simulate;
+  int phaseConstraint, updateProbe, updateModes, beamstopMask;
+  char lf[256];           /* positions list file or "" */
+  int PPS;
+  /* --- additions --- */
+  uint64_t seed;          /* seed of the ePIE visiting-order stream (reference: time(NULL)) */
+  int calculateRMS;       /* compute the per-iteration error metric (the reference's Python path never does) */
+  int device;             /* CUDA device ordinal */
+  int wave;               /* DM patterns per pipeline wave (0 = automatic) */
+} pty_params;
+
+typedef struct pty_session pty_session;
+
+/* Fill `p` with the reference's Python-call defaults.  Replaces the default block of
+ * ptychopy_algorithmnp (src/ptychopy.c:282-323). */
+int pty_params_init(pty_params* p);
+
+/* Create a reconstruction session on p->device.  Replaces `new IPhaser` + CXParams::parseFromCPython
+ * (src/ptychopy.c:474-482, src/Parameters.cpp:380-653); the parameter struct is per session, not a
+ * process-wide singleton. */
+int pty_session_create(const pty_params* p, pty_session** out);
+
+/* Release all device and host resources.  Replaces `delete phaser` (src/ptychopy.c:489). */
+int pty_session_destroy(pty_session* s);
+
+/* Diffraction data, P patterns of N x N, as float32 (dtype PTY_F32) or float64 (PTY_F64), raster order
+ * i*scanDimsy+j.  float32 data may also be passed as a device pointer (unified addressing).  ePIE/DM take amplitudes, MLs intensities (it square-roots them), as in the reference.
+ * Replaces Diffractions::loadarr (src/Diffractions.cpp:159-186) fed from diffractionNP (src/ptychopy.c:357-362). */
+int pty_set_patterns(pty_session* s, const void* host, int dtype, int P, int N);
+
+/* Scan positions in metres, P x 2 (x, y) float64.  Replaces ListScanMesh::loadarr (src/ListScanMesh.cpp:91-103)
+ * fed from positionNP (src/ptychopy.c:364-376).  Without it a Cartesian raster is generated
+ * (CartesianScanMesh::generateMesh, src/CartesianScanMesh.cpp:57-92). */
+int pty_set_positions(pty_session* s, const double* xy_m, int P);
+
+/* Initial object, complex64 X x Y (must equal the size the scan geometry implies; see pty_get_dims).
+ * Replaces Sample::loadarr (src/Sample.cpp:184-198) fed from objectNP (src/ptychopy.c:378-421). */
+int pty_set_object(pty_session* s, const float* c64, int X, int Y);
+
+/* Initial probe modes, complex64 K x N x N, K <= probeModes.  K = 1 replaces Probe::init's probearr branch
+ * (src/Probe.cpp:354-358, fed from probeNP at src/ptychopy.c:423-471); K > 1 supplies all modes (extension). */
+int pty_set_probe(pty_session* s, const float* c64, int K, int N);
+
+/* Build geometry, probe guess and device state.  Replaces IPhaser::init + prePhase (src/IPhaser.cpp:224-365).
+ * Fails (PTY_ERR_INVALID) when patterns are missing or a position is negative. */
+int pty_init(pty_session* s);
+
+/* One iteration of the session's algorithm (iteration counter i+1 drives the phaseConstraint / updateProbe /
+ * updateModes schedule).  Replaces IPhaser::phasestepvis / phaseStep (src/IPhaser.cpp:391-398,479-494) and the
+ * epiestep / mlsstep calls (src/ptychopy.c:955-962,1036-1043).  err (may be NULL) receives the error metric
+ * (0 unless calculateRMS). */
+int pty_step(pty_session* s, double* err);
+
+/* `iters` iterations (errs may be NULL or hold `iters` values).  Replaces IPhaser::phaseLoop
+ * (src/IPhaser.cpp:367-389). */
+int pty_run(pty_session* s, int iters, double* errs);
+
+/* Sizes: object X, Y; probe modes K, size N; pattern count P; iterations done. */
+int pty_get_dims(const pty_session* s, int* X, int* Y, int* K, int* N, int* P, int* iters_done);
+
+/* Copy the object (X x Y complex64) to the host.  Replaces epieresobj / mlsresobj (src/ptychopy.c:964-976). */
+int pty_get_object(pty_session* s, float* c64_out, int X, int Y);
+
+/* Copy the probe stack (K x N x N complex64).  Replaces epieresprobe / mlsresprobe (src/ptychopy.c:978-990). */
+int pty_get_probe(pty_session* s, float* c64_out, int K, int N);
+
+/* Scan positions in pixels after the -min shift, P x 2 float32 (IPtychoScanMesh::getScanPositions). */
+int pty_get_positions(const pty_session* s, float* xy_px, int P);
+
+/* Write `<dir>/<jobID>_probes_<r>.{csv|bin}` and `<dir>/<jobID>_object_<r>.{csv|bin}`.  Replaces
+ * IPhaser::writeResultsToDisk (src/IPhaser.cpp:417-428) with the CSV format of Cuda2DArray::save
+ * (src/Cuda2DArray.hpp:439-464, src/Cuda2DArray.cpp:46-52). */
+int pty_write_results(pty_session* s, const char* dir, int r, int binary);
+
+/* Run all subsequent device work of the session on this cudaStream_t (NULL = the session's own stream). */
+int pty_set_stream(pty_session* s, void* cuda_stream);
+
+/* Number of this library's kernel launches issued by the session so far (graph nodes counted per launch). */
+int64_t pty_kernel_launches(const pty_session* s);
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char* pty_last_error(void);
+
+/* ---- device-pointer operators (building blocks, used by the parity tests) ---------------------------- */
+
+/* In-place batched 2-D FFT of `batch` N x N complex64 arrays in device memory (unnormalised; forward uses
+ * exp(-2*pi*i*k*n/N), the CUFFT_FORWARD convention).  Replaces the cuFFT plans of FFTPlanner
+ * (src/CudaFFTPlan.cpp:72-101).  `work_dev` is a device buffer of batch*N*N complex64. */
+int pty_fft2_dev(void* data_dev, void* work_dev, int batch, int N, int inverse, void* cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PTYCHOPY_B200_H_ */

@@ -1,0 +1,674 @@
+// ============================================================================================================
+// ORACLE — TEST INFRASTRUCTURE ONLY.  NOT PART OF THE PRODUCT.
+//
+// A plain C++ restatement of the reference's ptychography inner loop (ePIE and its "reference DM"), used by
+// tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker.  The product (libptychopy_b200)
+// never links, loads or calls anything in this directory.
+//
+// Parity status: UNPINNED by the reference.  The reference ships no tests, golden vectors or known-answer
+// fixtures, and its CUDA sources do not build with CUDA 12.9 (removed texture-reference API, missing
+// CUDA-samples headers), so this restatement cannot be checked against reference outputs.  It is pinned instead
+// by (a) numpy.fft for the FFT convention, (b) hand-derived known-answer cases in tests/, and (c) committed
+// golden fixtures generated from this file (tests/golden/make_golden.py).
+//
+// Numerics: templated on the real type.  `double` is the FP64 oracle; `float` + std::thread is the multithreaded
+// FP32 CPU baseline that bench.py times.  Scan geometry is computed in FP32 exactly as the reference does it
+// (its positions are FP32 on the device), so both instantiations share it.
+//
+// Reference files restated (paths inside the ptychopy project):
+//   geometry       src/Parameters.h:175-179, src/Parameters.cpp:650-652, src/ScanMeshKernels.cu:46-93,153-170,
+//                  src/IPtychoScanMesh.cpp:86-109, src/CartesianScanMesh.cpp:57-92, src/ListScanMesh.cpp:55-129
+//   probe guess    src/Probe.cpp:303-318,342-374, src/ProbeKernels.cu:52-63,207-218,388-407,582-590,
+//                  src/utilities.cpp:138-154, src/utilitiesKernels.cu:619-682
+//   ePIE           src/ePIE.cpp:65-129, src/SampleKernels.cu:167-178,209-215,244-294 (texture setup :493-502),
+//                  src/ProbeKernels.cu:425-458, src/Sample.cpp:266-275,333-345, src/Probe.cpp:1750-1774,
+//                  src/utilities.cpp:188-216, src/utilitiesKernels.cu:619-712,1866-1925
+//   probe modes    src/Probe.cpp:229-242,320-330,1768-1781, src/ProbeKernels.cu:82-97,509-515,
+//                  src/utilitiesKernels.cu:853-867,2051-2082
+//   DM             src/DM.cu:46-128, src/SampleKernels.cu:416-490,686-719, src/Sample.cpp:333-345,
+//                  src/Probe.cpp:296-301,1761-1766
+//   error metric   src/utilities.cpp:188-195, src/utilitiesKernels.cu:684-712, src/Diffractions.cpp:234-242
+// ============================================================================================================
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <thread>
+#include <vector>
+
+namespace {
+
+template <typename R> using cx = std::complex<R>;
+
+// ---------------------------------------------------------------- FFT (unnormalised, cuFFT sign convention)
+// Forward: X[k] = sum_n x[n] exp(-2*pi*i*k*n/L); inverse: exp(+...), no 1/L scaling (CUFFT_FORWARD/INVERSE).
+template <typename R> struct Fft1 {
+  int L = 0, logL = 0;
+  std::vector<cx<R>> tw;       // exp(-2*pi*i*m/L), m < L/2, computed in double
+  std::vector<int> rev;
+  explicit Fft1(int n) : L(n) {
+    while ((1 << logL) < L) ++logL;
+    tw.resize(L / 2);
+    for (int m = 0; m < L / 2; ++m) {
+      double a = -2.0 * M_PI * double(m) / double(L);
+      tw[m] = cx<R>(R(std::cos(a)), R(std::sin(a)));
+    }
+    rev.resize(L);
+    for (int i = 0; i < L; ++i) {
+      int r = 0;
+      for (int b = 0; b < logL; ++b) r |= ((i >> b) & 1) << (logL - 1 - b);
+      rev[i] = r;
+    }
+  }
+  // In-place transform of L points with element stride `stride`.
+  void run(cx<R>* x, int stride, bool inverse, cx<R>* scratch) const {
+    for (int i = 0; i < L; ++i) scratch[rev[i]] = x[i * stride];
+    for (int len = 2; len <= L; len <<= 1) {
+      int half = len >> 1, step = L / len;
+      for (int s = 0; s < L; s += len)
+        for (int j = 0; j < half; ++j) {
+          cx<R> w = tw[j * step];
+          if (inverse) w = std::conj(w);
+          cx<R> a = scratch[s + j], b = scratch[s + j + half] * w;
+          scratch[s + j] = a + b;
+          scratch[s + j + half] = a - b;
+        }
+    }
+    for (int i = 0; i < L; ++i) x[i * stride] = scratch[i];
+  }
+};
+
+// 2-D transform of an N x N row-major array (rows = first index x, columns = second index y).
+template <typename R> void fft2(const Fft1<R>& f, cx<R>* a, bool inverse, std::vector<cx<R>>& scratch) {
+  const int N = f.L;
+  scratch.resize(N);
+  for (int r = 0; r < N; ++r) f.run(a + size_t(r) * N, 1, inverse, scratch.data());
+  for (int c = 0; c < N; ++c) f.run(a + c, N, inverse, scratch.data());
+}
+
+// ---------------------------------------------------------------- geometry (FP32 like the reference)
+// src/Parameters.h:175-179 returns real_t (float): dx_s = (float)(lambda*z/(N*dx_d)).
+double sample_pixel(double lambda, double z, double dx_d, int N) {
+  return double(float((lambda * z) / (double(N) * dx_d)));
+}
+
+struct Mesh {
+  std::vector<float> pos;  // 2*P, (x=row, y=column), shifted by -min
+  int X = 0, Y = 0;
+};
+
+// Applies min/max, object size and -min shift: src/IPtychoScanMesh.cpp:86-109.
+void finish_mesh(std::vector<float>& raw, int P, bool padZero, int N, bool flip, Mesh& m) {
+  float mnx = std::numeric_limits<float>::max(), mny = mnx, mxx = -mnx, mxy = -mnx;
+  for (int i = 0; i < P; ++i) {
+    mnx = std::min(mnx, raw[2 * i]); mxx = std::max(mxx, raw[2 * i]);
+    mny = std::min(mny, raw[2 * i + 1]); mxy = std::max(mxy, raw[2 * i + 1]);
+  }
+  if (padZero) {  // list meshes are padded to a multiple of 1024 with (0,0) entries that join the min/max
+    mnx = std::min(mnx, 0.f); mxx = std::max(mxx, 0.f); mny = std::min(mny, 0.f); mxy = std::max(mxy, 0.f);
+  }
+  volatile float ex = (mxx - mnx) + float(N), ey = (mxy - mny) + float(N);
+  m.X = int(std::ceil(ex));
+  m.Y = int(std::ceil(ey));
+  m.pos.resize(2 * size_t(P));
+  for (int i = 0; i < P; ++i) {
+    float tx = raw[2 * i], ty = raw[2 * i + 1];
+    m.pos[2 * i] = flip ? ty - mny : tx - mnx;
+    m.pos[2 * i + 1] = flip ? tx - mnx : ty - mny;
+  }
+}
+
+// ---------------------------------------------------------------- bilinear patch fetch (texture emulation)
+// tex2D(obj, col+qy+0.5f, row+qx+0.5f) with linear filtering, clamp addressing, unnormalised coordinates
+// (src/SampleKernels.cu:167-178, :493-502).  Texture filtering weights are 1.8 fixed point; this restatement
+// rounds the fractional part to the nearest 1/256.
+inline void tex_coord(float base, int idx, int extent, int& i0, int& i1, double& a) {
+  volatile float c = float(idx) + base;  // col + offsetY, rounded to float
+  volatile float t = c + 0.5f;           // + 0.5f, rounded to float
+  double xb = double(t) - 0.5;
+  double fl = std::floor(xb);
+  double fr = xb - fl;
+  a = std::floor(fr * 256.0 + 0.5) / 256.0;
+  long long i = (long long)fl;
+  auto clampi = [&](long long v) { return int(v < 0 ? 0 : (v >= extent ? extent - 1 : v)); };
+  i0 = clampi(i);
+  i1 = clampi(i + 1);
+}
+
+template <typename R>
+void extract_patch(const cx<R>* O, int X, int Y, float qx, float qy, int N, cx<R>* out) {
+  std::vector<int> c0(N), c1(N);
+  std::vector<double> ca(N);
+  for (int c = 0; c < N; ++c) tex_coord(qy, c, Y, c0[c], c1[c], ca[c]);
+  for (int r = 0; r < N; ++r) {
+    int r0, r1;
+    double b;
+    tex_coord(qx, r, X, r0, r1, b);
+    for (int c = 0; c < N; ++c) {
+      double a = ca[c];
+      cx<R> v00 = O[size_t(r0) * Y + c0[c]], v01 = O[size_t(r0) * Y + c1[c]];
+      cx<R> v10 = O[size_t(r1) * Y + c0[c]], v11 = O[size_t(r1) * Y + c1[c]];
+      out[size_t(r) * N + c] = v00 * R((1 - a) * (1 - b)) + v01 * R(a * (1 - b)) + v10 * R((1 - a) * b) +
+                               v11 * R(a * b);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- seeded visiting order (ePIE)
+// The reference draws `rand() % remaining` from the list of not-yet-visited positions and erases the pick
+// (src/ePIE.cpp:93-97) with a time seed.  The seeded generator here is SplitMix64; one stream per session,
+// continued across iterations.  The product's host code implements the same generator.
+inline uint64_t splitmix64(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+void visiting_order(uint64_t& state, int P, int* order) {
+  std::vector<int> rem(P);
+  for (int i = 0; i < P; ++i) rem[i] = i;
+  for (int s = 0; s < P; ++s) {
+    int k = int(splitmix64(state) % uint64_t(rem.size()));
+    order[s] = rem[k];
+    rem.erase(rem.begin() + k);
+  }
+}
+
+template <typename R> inline cx<R> constrain_phase(cx<R> v) {
+  // src/SampleKernels.cu:209-215: arg clamped to <= 0, magnitude kept.
+  R mag = std::abs(v), arg = std::atan2(v.imag(), v.real());
+  arg = arg <= R(0) ? arg : R(0);
+  return cx<R>(mag * std::cos(arg), mag * std::sin(arg));
+}
+
+template <typename R> inline cx<R> modulus_phase(cx<R> psi, R amp) {
+  // src/utilitiesKernels.cu:626-631 / src/SampleKernels.cu:443-447: amp * exp(i*atan2(im, re)).
+  // psi == 0 (either zero sign) is pinned to phase 0: atan2 of signed zeros is implementation-defined there.
+  if (psi.real() == R(0) && psi.imag() == R(0)) return cx<R>(amp, R(0));
+  R ph = std::atan2(psi.imag(), psi.real());
+  return cx<R>(amp * std::cos(ph), amp * std::sin(ph));
+}
+
+// ---------------------------------------------------------------- probe guess (Q10 in the build notes)
+// src/Probe.cpp:360-372 with d_initProbe (src/ProbeKernels.cu:207-218), d_normalizeDiffractionIntensities
+// (:388-407), the modulus projection onto the mean amplitude (src/utilities.cpp:138-154) and normalize()
+// (src/Probe.cpp:303-318).  Mode 0 only; modes >= 1 are zero.
+template <typename R>
+void probe_guess(const R* amp, int P, int N, double beamSize, double dx_s, int K, cx<R>* probe) {
+  const double window = double(N) / (2 * 2.35);
+  const double factor = double(float(dx_s / beamSize));
+  std::fill(probe, probe + size_t(K) * N * N, cx<R>(0, 0));
+  for (int x = 0; x < N; ++x)
+    for (int y = 0; y < N; ++y) {
+      double a = double(x) - N * 0.5, b = double(y) - N * 0.5;
+      double r = std::sqrt(a * a + b * b);
+      double p = r * factor;
+      p = (p != 0) ? std::sin(M_PI * p) / (M_PI * p) : 1.0;
+      double g = std::exp(-std::pow(window, -2.0) * r * r);
+      probe[size_t(x) * N + y] = cx<R>(R(std::fabs(p * g)), 0);
+    }
+  std::vector<R> avg(size_t(N) * N, R(0));
+  for (int p = 0; p < P; ++p)
+    for (size_t i = 0; i < size_t(N) * N; ++i) avg[i] += amp[size_t(p) * N * N + i];
+  for (auto& v : avg) v *= R(1.0 / double(P));
+  Fft1<R> f(N);
+  std::vector<cx<R>> scr;
+  fft2(f, probe, false, scr);
+  const R nrm = R(1.0 / double(N * N));
+  for (size_t i = 0; i < size_t(N) * N; ++i) probe[i] = modulus_phase(probe[i], avg[i]) * nrm;
+  fft2(f, probe, true, scr);
+  R mx = 0;
+  for (size_t i = 0; i < size_t(K) * N * N; ++i) mx = std::max(mx, std::abs(probe[i]));
+  for (size_t i = 0; i < size_t(K) * N * N; ++i) probe[i] *= R(1.0 / double(mx));
+}
+
+// ---------------------------------------------------------------- session state shared by ePIE and DM
+struct Flags {
+  int phaseConstraint = 1, updateProbe = 10, updateModes = 20;
+  int calculateRMS = 0;
+};
+
+template <typename R> struct State {
+  int N = 0, K = 1, P = 0, X = 0, Y = 0;
+  std::vector<cx<R>> O, Pr;     // object X*Y, probe K*N*N
+  std::vector<R> Ocache, Pcache;  // |O|^2 (m_objectIntensities), |P_k|^2 (m_intensities)
+  R objMax = 0;                   // Sample::m_maxObjectIntensity (starts 0, src/Sample.cpp:216-220)
+  R probeMax = 1;                 // Probe::m_maxIntensity (constructor value 1, src/Probe.cpp:54-58)
+  bool useAll = false, modesInitialized = false;
+};
+
+// Probe::getModalDoubleMax (src/utilities.cpp:204-216): with all modes active and K>1, the max over pixels of
+// the per-pixel modal sum; otherwise the max over the whole stacked K*N*N intensity array.
+template <typename R> R probe_modal_max(const State<R>& s) {
+  const size_t NN = size_t(s.N) * s.N;
+  R mx = 0;
+  if (s.useAll && s.K > 1) {
+    for (size_t i = 0; i < NN; ++i) {
+      R t = 0;
+      for (int k = 0; k < s.K; ++k) t += s.Pcache[k * NN + i];
+      mx = std::max(mx, t);
+    }
+  } else {
+    for (size_t i = 0; i < size_t(s.K) * NN; ++i) mx = std::max(mx, s.Pcache[i]);
+  }
+  return mx;
+}
+
+// Probe::orthogonalize (src/Probe.cpp:229-242) with h_projectUtoV (src/ProbeKernels.cu:509-515):
+// classical Gram-Schmidt against the ORIGINAL copy of mode i; factor = <v,u>/<u,u> with <a,b> = sum conj(a)*b.
+template <typename R> void orthogonalize(State<R>& s) {
+  const size_t NN = size_t(s.N) * s.N;
+  std::vector<cx<R>> copy(s.Pr);
+  for (int i = 1; i < s.K; ++i)
+    for (int j = i - 1; j >= 0; --j) {
+      const cx<R>* u = &s.Pr[j * NN];
+      const cx<R>* v = &copy[i * NN];
+      cx<R> vu(0, 0), uu(0, 0);
+      for (size_t p = 0; p < NN; ++p) {
+        vu += std::conj(v[p]) * u[p];
+        uu += std::conj(u[p]) * u[p];
+      }
+      cx<R> fac = vu / uu;
+      for (size_t p = 0; p < NN; ++p) s.Pr[i * NN + p] -= fac * u[p];
+    }
+}
+
+// Probe::beginModalReconstruction / initProbeModes (src/Probe.cpp:320-330,1768-1774).
+template <typename R> void begin_modal(State<R>& s) {
+  const size_t NN = size_t(s.N) * s.N;
+  s.useAll = true;
+  if (!s.modesInitialized) {
+    if (s.K > 1) {
+      for (int k = 1; k < s.K; ++k)
+        for (size_t p = 0; p < NN; ++p) {
+          cx<R> v = s.Pr[p] * R(0.05);
+          s.Pr[k * NN + p] = v;
+          R m = std::abs(v);
+          s.Pcache[k * NN + p] = m * m;
+        }
+      orthogonalize(s);
+      s.modesInitialized = true;
+    }
+    s.probeMax = probe_modal_max(s);
+  }
+}
+
+// ---------------------------------------------------------------- ePIE iteration (src/ePIE.cpp:65-129)
+template <typename R>
+R epie_iteration(State<R>& s, const R* amp, const float* pos, const R* sqsum, const Flags& fl, int iter,
+                 uint64_t& rng, int* status) {
+  const int N = s.N, K = s.K, P = s.P;
+  const size_t NN = size_t(N) * N;
+  const bool pc = iter <= fl.phaseConstraint, up = iter >= fl.updateProbe, um = iter >= fl.updateModes;
+  if (um) begin_modal(s);
+  const int Ka = s.useAll ? K : 1;
+  std::vector<int> order(P);
+  visiting_order(rng, P, order.data());
+  Fft1<R> f(N);
+  std::vector<cx<R>> scr, patch(NN), psiOld(size_t(Ka) * NN), Psi(size_t(Ka) * NN), psi(size_t(Ka) * NN);
+  const R nrm = R(1.0 / double(N * N));
+  double err = 0;
+  for (int step = 0; step < P; ++step) {
+    const int i = order[step];
+    const float qx = pos[2 * i], qy = pos[2 * i + 1];
+    if (qx < 0 || qy < 0) { *status = -2; return R(0); }
+    extract_patch(s.O.data(), s.X, s.Y, qx, qy, N, patch.data());
+    for (int k = Ka - 1; k >= 0; --k)
+      for (size_t p = 0; p < NN; ++p) psiOld[k * NN + p] = patch[p] * s.Pr[k * NN + p];
+    for (int k = 0; k < Ka; ++k) {
+      std::copy(&psiOld[k * NN], &psiOld[k * NN] + NN, &Psi[k * NN]);
+      fft2(f, &Psi[k * NN], false, scr);
+    }
+    const R* A = amp + size_t(i) * NN;
+    if (Ka == 1) {
+      for (size_t p = 0; p < NN; ++p) psi[p] = modulus_phase(Psi[p], A[p]) * nrm;
+    } else {
+      for (size_t p = 0; p < NN; ++p) {
+        R m2 = 0;
+        for (int k = 0; k < Ka; ++k) m2 += std::norm(Psi[k * NN + p]);
+        // rsqrt(0) gives inf and 0*inf = NaN in the reference; a pixel with no modal power is pinned to 0 here.
+        R sc = m2 > R(0) ? R(1) / std::sqrt(m2) : R(0);
+        for (int k = 0; k < Ka; ++k) psi[k * NN + p] = Psi[k * NN + p] * (A[p] * sc * nrm);
+      }
+    }
+    if (fl.calculateRMS) {  // error on FFT(psi_old), src/utilities.cpp:188-195, src/utilitiesKernels.cu:684-712
+      double e = 0;
+      for (size_t p = 0; p < NN; ++p) {
+        cx<R> t(0, 0);
+        for (int k = 0; k < Ka; ++k) t += Psi[k * NN + p];
+        e += std::fabs(double(A[p]) - double(std::abs(t)));
+      }
+      err += (e / Ka) / double(sqsum[i]);
+    }
+    for (int k = 0; k < Ka; ++k) fft2(f, &psi[k * NN], true, scr);
+    const int ox = int(std::round(qx)), oy = int(std::round(qy));
+    // Object update (d_updateObjectArray[M], src/SampleKernels.cu:244-294), c = 1/probeMax.
+    const R cO = R(1.0 / double(s.probeMax));
+    for (int r = 0; r < N; ++r)
+      for (int c = 0; c < N; ++c) {
+        size_t p = size_t(r) * N + c, o = size_t(r + ox) * s.Y + (c + oy);
+        cx<R> inc(0, 0);
+        for (int k = 0; k < Ka; ++k) inc += std::conj(s.Pr[k * NN + p]) * (psi[k * NN + p] - psiOld[k * NN + p]);
+        cx<R> v = s.O[o] + inc * cO;
+        R mag = std::abs(v);
+        if (pc) v = constrain_phase(v);
+        s.O[o] = v;
+        s.Ocache[o] = mag * mag;
+      }
+    s.objMax = *std::max_element(s.Ocache.begin(), s.Ocache.end());
+    if (up) {  // d_updateProbe[M] (src/ProbeKernels.cu:425-458), c = 1/objMax, uses the updated object
+      const R cP = R(1.0 / double(s.objMax));
+      for (int r = 0; r < N; ++r)
+        for (int c = 0; c < N; ++c) {
+          size_t p = size_t(r) * N + c, o = size_t(r + ox) * s.Y + (c + oy);
+          cx<R> oc = std::conj(s.O[o]);
+          for (int k = 0; k < Ka; ++k) {
+            cx<R> v = oc * (psi[k * NN + p] - psiOld[k * NN + p]) * cP + s.Pr[k * NN + p];
+            R m = std::abs(v);
+            s.Pr[k * NN + p] = v;
+            s.Pcache[k * NN + p] = m * m;
+          }
+        }
+      s.probeMax = probe_modal_max(s);
+    }
+  }
+  return R(err / P);
+}
+
+// ---------------------------------------------------------------- reference DM iteration (src/DM.cu:80-128)
+template <typename R> struct DMState {
+  std::vector<cx<R>> psi;        // P*N*N, zero at start (Cuda3DArray zeroed on allocation)
+  double fac[2] = {0, 0};        // {1/objMax, 1/probeMax}, cached with hysteresis EPS
+  bool started = false;
+};
+
+template <typename R> double sum_sq(const cx<R>* a, size_t n) {
+  double t = 0;
+  for (size_t i = 0; i < n; ++i) t += double(std::norm(a[i]));
+  return t;
+}
+
+template <typename R>
+void dm_iteration(State<R>& s, DMState<R>& d, const R* amp, const float* pos, const Flags& fl, int iter,
+                  int nthreads) {
+  const int N = s.N, P = s.P;
+  const size_t NN = size_t(N) * N, XY = size_t(s.X) * s.Y;
+  const bool pc = iter <= fl.phaseConstraint, up = iter >= fl.updateProbe;
+  if (!d.started) {
+    d.started = true;
+    d.psi.assign(size_t(P) * NN, cx<R>(0, 0));
+    d.fac[0] = 1.0 / double(s.objMax);
+    d.fac[1] = 1.0 / double(s.probeMax);
+  }
+  // checkCache (src/DM.cu:54-73): a factor moves only when it changed by more than EPS = 1e-3.
+  const double passed[2] = {1.0 / double(s.objMax), 1.0 / double(s.probeMax)};
+  for (int j = 0; j < 2; ++j)
+    if (std::fabs(d.fac[j] - passed[j]) > 1e-3) d.fac[j] = passed[j];
+  const R f0 = R(d.fac[0]), f1 = R(d.fac[1]);
+  const R nrm = R(1.0 / double(N * N));
+  if (nthreads < 1) nthreads = 1;
+  std::vector<std::vector<cx<R>>> dO(nthreads, std::vector<cx<R>>(XY)), dP(nthreads, std::vector<cx<R>>(NN));
+  auto work = [&](int t) {
+    Fft1<R> f(N);
+    std::vector<cx<R>> scr, u(NN);
+    for (int j = t; j < P; j += nthreads) {
+      const int ox = int(std::round(pos[2 * j])), oy = int(std::round(pos[2 * j + 1]));
+      cx<R>* pj = &d.psi[size_t(j) * NN];
+      const R* A = amp + size_t(j) * NN;
+      // forward: load callback 2*P*O - psi, store callback A*exp(i*arg)/N^2 (src/SampleKernels.cu:418-450)
+      for (int r = 0; r < N; ++r)
+        for (int c = 0; c < N; ++c) {
+          size_t p = size_t(r) * N + c;
+          cx<R> ph = s.Pr[p] * s.O[size_t(r + ox) * s.Y + (c + oy)];
+          u[p] = ph * R(2) - pj[p];
+        }
+      fft2(f, u.data(), false, scr);
+      for (size_t p = 0; p < NN; ++p) u[p] = modulus_phase(u[p], A[p]) * nrm;
+      fft2(f, u.data(), true, scr);
+      // inverse store callback (src/SampleKernels.cu:452-490) with snapshot O and P
+      for (int r = 0; r < N; ++r)
+        for (int c = 0; c < N; ++c) {
+          size_t p = size_t(r) * N + c, o = size_t(r + ox) * s.Y + (c + oy);
+          cx<R> ov = s.O[o], pv = s.Pr[p];
+          cx<R> v = pj[p] + u[p] - (ov * pv) * R(2);
+          cx<R> inc = std::conj(pv) * v * f1;
+          if (pc) inc = constrain_phase(inc);
+          dO[t][o] += inc;
+          if (up) dP[t][p] += std::conj(ov) * v * f0;
+          pj[p] = v;
+        }
+    }
+  };
+  if (nthreads == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; ++t) th.emplace_back(work, t);
+    for (auto& x : th) x.join();
+  }
+  for (int t = 0; t < nthreads; ++t) {
+    for (size_t i = 0; i < XY; ++i) s.O[i] += dO[t][i];
+    if (up)
+      for (size_t i = 0; i < NN; ++i) s.Pr[i] += dP[t][i];
+  }
+  // updateIntensities(true) on object and probe: sums of |.|^2 (all stacked modes for the probe)
+  s.objMax = R(sum_sq(s.O.data(), XY));
+  s.probeMax = R(sum_sq(s.Pr.data(), size_t(s.K) * NN));
+}
+
+template <typename R> void load_state(State<R>& s, int N, int K, int P, int X, int Y, const double* obj,
+                                      const double* probe, int probeCacheValid) {
+  s.N = N; s.K = K; s.P = P; s.X = X; s.Y = Y;
+  const size_t NN = size_t(N) * N, XY = size_t(X) * Y;
+  s.O.resize(XY); s.Ocache.assign(XY, R(0));
+  s.Pr.resize(size_t(K) * NN); s.Pcache.assign(size_t(K) * NN, R(0));
+  for (size_t i = 0; i < XY; ++i) s.O[i] = cx<R>(R(obj[2 * i]), R(obj[2 * i + 1]));
+  for (size_t i = 0; i < size_t(K) * NN; ++i) s.Pr[i] = cx<R>(R(probe[2 * i]), R(probe[2 * i + 1]));
+  if (probeCacheValid) {  // Probe::init's guess path ends in updateIntensities(); a given probe does not
+    for (size_t i = 0; i < size_t(K) * NN; ++i) s.Pcache[i] = std::norm(s.Pr[i]);
+    s.probeMax = probe_modal_max(s);
+  }
+}
+
+template <typename R> void store_state(const State<R>& s, double* obj, double* probe) {
+  for (size_t i = 0; i < s.O.size(); ++i) { obj[2 * i] = double(s.O[i].real()); obj[2 * i + 1] = double(s.O[i].imag()); }
+  for (size_t i = 0; i < s.Pr.size(); ++i) {
+    probe[2 * i] = double(s.Pr[i].real());
+    probe[2 * i + 1] = double(s.Pr[i].imag());
+  }
+}
+
+}  // namespace
+
+// ============================================================================================================
+// C ABI of the oracle (ctypes from tests/ and bench.py).  Complex arrays are interleaved (re, im) doubles.
+// ============================================================================================================
+extern "C" {
+
+int orc_version() { return 1; }
+
+// 2-D FFT of an N x N complex array in place (unnormalised, cuFFT sign convention).
+int orc_fft2(double* data, int N, int inverse) {
+  if (N < 2 || (N & (N - 1))) return -1;
+  Fft1<double> f(N);
+  std::vector<cx<double>> a(size_t(N) * N), scr;
+  for (size_t i = 0; i < a.size(); ++i) a[i] = cx<double>(data[2 * i], data[2 * i + 1]);
+  fft2(f, a.data(), inverse != 0, scr);
+  for (size_t i = 0; i < a.size(); ++i) { data[2 * i] = a[i].real(); data[2 * i + 1] = a[i].imag(); }
+  return 0;
+}
+
+double orc_sample_pixel(double lambda, double z, double dx_d, int N) { return sample_pixel(lambda, z, dx_d, N); }
+
+// Cartesian raster mesh (d_generateMesh<1>, src/ScanMeshKernels.cu:46-93, launched at :153-160).
+// pos receives 2*nx*ny floats (raster order i*ny+j), objXY the object size.
+int orc_cartesian_mesh(int nx, int ny, double stepx, double stepy, double lambda, double z, double dx_d, int N,
+                       int mirrorX, int mirrorY, int flip, float* pos, int* objXY) {
+  if (nx < 1 || ny < 1 || N < 1) return -1;
+  const double dx_s = sample_pixel(lambda, z, dx_d, N);
+  const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
+  std::vector<float> raw(2 * size_t(nx) * ny);
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      volatile float mi = float(i), md = float(nx - 1) * 0.5f;
+      volatile float dxv = mirrorX ? (md - mi) : (mi - md);
+      volatile float vx = dxv * sx;
+      volatile float mj = float(j), mdy = float(ny - 1) * 0.5f;
+      volatile float dyv = mirrorY ? (mdy - mj) : (mj - mdy);
+      volatile float vy = dyv * sy;
+      volatile float px = vx * inv, py = vy * inv;
+      raw[2 * (size_t(i) * ny + j)] = px;
+      raw[2 * (size_t(i) * ny + j) + 1] = py;
+    }
+  Mesh m;
+  finish_mesh(raw, nx * ny, false, N, flip != 0, m);
+  std::memcpy(pos, m.pos.data(), m.pos.size() * sizeof(float));
+  objXY[0] = m.X; objXY[1] = m.Y;
+  return 0;
+}
+
+// List mesh from positions in metres (ListScanMesh::loadarr + d_generateMesh<2>, src/ListScanMesh.cpp:55-129).
+int orc_list_mesh(const double* xy_m, int P, double lambda, double z, double dx_d, int N, int flip, float* pos,
+                  int* objXY) {
+  if (P < 1) return -1;
+  const double dx_s = sample_pixel(lambda, z, dx_d, N);
+  const float inv = float(1.0 / dx_s);
+  std::vector<float> raw(2 * size_t(P));
+  for (int i = 0; i < P; ++i) {
+    volatile float x = float(xy_m[2 * i]), y = float(xy_m[2 * i + 1]);
+    volatile float px = x * inv, py = y * inv;
+    raw[2 * i] = px; raw[2 * i + 1] = py;
+  }
+  Mesh m;
+  finish_mesh(raw, P, (P % 1024) != 0, N, flip != 0, m);
+  std::memcpy(pos, m.pos.data(), m.pos.size() * sizeof(float));
+  objXY[0] = m.X; objXY[1] = m.Y;
+  return 0;
+}
+
+// Probe guess from the mean diffraction amplitude; probe_out has K*N*N complex (modes >= 1 zero).
+int orc_probe_guess(const double* amp, int P, int N, double beamSize, double dx_s, int K, double* probe_out) {
+  if (P < 1 || N < 2 || (N & (N - 1)) || K < 1) return -1;
+  std::vector<cx<double>> pr(size_t(K) * N * N);
+  probe_guess<double>(amp, P, N, beamSize, dx_s, K, pr.data());
+  for (size_t i = 0; i < pr.size(); ++i) { probe_out[2 * i] = pr[i].real(); probe_out[2 * i + 1] = pr[i].imag(); }
+  return 0;
+}
+
+// The seeded visiting order: `state` is advanced in place (one stream per session).
+void orc_visiting_order(uint64_t* state, int P, int* order) { visiting_order(*state, P, order); }
+
+// Bilinear patch fetch at fractional (qx, qy) (texture emulation); obj X*Y complex, out N*N complex.
+int orc_extract_patch(const double* obj, int X, int Y, float qx, float qy, int N, double* out) {
+  std::vector<cx<double>> O(size_t(X) * Y), o(size_t(N) * N);
+  for (size_t i = 0; i < O.size(); ++i) O[i] = cx<double>(obj[2 * i], obj[2 * i + 1]);
+  extract_patch(O.data(), X, Y, qx, qy, N, o.data());
+  for (size_t i = 0; i < o.size(); ++i) { out[2 * i] = o[i].real(); out[2 * i + 1] = o[i].imag(); }
+  return 0;
+}
+
+// Oracle session: one reconstruction (algo 0 = ePIE, 1 = reference DM) driven one iteration at a time, so the
+// flag schedule (i <= phaseConstraint, i >= updateProbe, i >= updateModes) and all cached state (|O|^2 cache,
+// probe intensity cache, running maxima, DM factors, visiting-order stream) persist exactly as in a session.
+struct OrcSession {
+  int algo = 0, iter = 0, nthreads = 1;
+  State<double> s;
+  DMState<double> d;
+  Flags fl;
+  uint64_t rng = 0;
+  std::vector<double> amp, sq;
+  std::vector<float> pos;
+};
+
+// probeGuessPath != 0: the probe came from the guess (its intensity cache and max are valid, as after
+// Probe::init's normalize()); otherwise it was supplied and the cache is zero with max 1 (src/Probe.cpp:354-358).
+// modesGiven != 0: modes >= 1 were supplied, so the modal switch does not re-initialise them.
+void* orc_create(int algo, int N, int K, int P, int X, int Y, const double* amp, const float* pos,
+                 const double* obj, const double* probe, int probeGuessPath, int modesGiven, uint64_t seed,
+                 int phaseConstraint, int updateProbe, int updateModes, int calculateRMS, int nthreads) {
+  if (N < 2 || (N & (N - 1)) || K < 1 || P < 1 || X < N || Y < N) return nullptr;
+  auto* h = new OrcSession;
+  h->algo = algo;
+  h->nthreads = nthreads < 1 ? 1 : nthreads;
+  load_state(h->s, N, K, P, X, Y, obj, probe, probeGuessPath);
+  h->s.modesInitialized = modesGiven != 0;
+  h->fl.phaseConstraint = phaseConstraint; h->fl.updateProbe = updateProbe; h->fl.updateModes = updateModes;
+  h->fl.calculateRMS = calculateRMS;
+  h->rng = seed;
+  const size_t NN = size_t(N) * N;
+  h->amp.assign(amp, amp + size_t(P) * NN);
+  h->pos.assign(pos, pos + 2 * size_t(P));
+  h->sq.assign(P, 1.0);
+  if (calculateRMS)  // Diffractions::fillSquaredSums: the sum of each amplitude pattern
+    for (int i = 0; i < P; ++i) {
+      double t = 0;
+      for (size_t p = 0; p < NN; ++p) t += h->amp[size_t(i) * NN + p];
+      h->sq[i] = t;
+    }
+  return h;
+}
+
+// Runs the next iteration; err receives the iteration's error metric (ePIE with calculateRMS; 0 for DM).
+int orc_step(void* hp, double* err) {
+  auto* h = static_cast<OrcSession*>(hp);
+  int status = 0;
+  const int it = ++h->iter;
+  double e = 0;
+  if (h->algo == 0)
+    e = epie_iteration<double>(h->s, h->amp.data(), h->pos.data(), h->sq.data(), h->fl, it, h->rng, &status);
+  else
+    dm_iteration<double>(h->s, h->d, h->amp.data(), h->pos.data(), h->fl, it, h->nthreads);
+  if (err) *err = e;
+  return status;
+}
+
+// Copies out object (X*Y complex), probe (K*N*N complex) and {objMax, probeMax, fac0, fac1}.
+int orc_get(void* hp, double* obj, double* probe, double* scalars) {
+  auto* h = static_cast<OrcSession*>(hp);
+  store_state(h->s, obj, probe);
+  if (scalars) {
+    scalars[0] = h->s.objMax; scalars[1] = h->s.probeMax;
+    scalars[2] = h->d.fac[0]; scalars[3] = h->d.fac[1];
+  }
+  return 0;
+}
+
+// DM exit-wave state (P*N*N complex); zeros before the first DM iteration.
+int orc_get_psi(void* hp, double* psi) {
+  auto* h = static_cast<OrcSession*>(hp);
+  const size_t n = size_t(h->s.P) * h->s.N * h->s.N;
+  for (size_t i = 0; i < n; ++i) {
+    cx<double> v = h->d.psi.empty() ? cx<double>(0, 0) : h->d.psi[i];
+    psi[2 * i] = v.real(); psi[2 * i + 1] = v.imag();
+  }
+  return 0;
+}
+
+void orc_destroy(void* hp) { delete static_cast<OrcSession*>(hp); }
+
+// FP32 multithreaded DM over float inputs: the CPU baseline.  Same equations as orc_dm_run; runs `iters`
+// iterations from a zero object with the given probe and returns the wall time in seconds of those iterations.
+double orc_dm_baseline_f32(int N, int P, int X, int Y, const float* amp, const float* pos, const float* probe,
+                           int iters, int nthreads, float* obj_out) {
+  State<float> s;
+  const size_t NN = size_t(N) * N, XY = size_t(X) * Y;
+  s.N = N; s.K = 1; s.P = P; s.X = X; s.Y = Y;
+  s.O.assign(XY, cx<float>(0, 0)); s.Ocache.assign(XY, 0.f);
+  s.Pr.resize(NN); s.Pcache.assign(NN, 0.f);
+  for (size_t i = 0; i < NN; ++i) s.Pr[i] = cx<float>(probe[2 * i], probe[2 * i + 1]);
+  s.objMax = 0; s.probeMax = 1;
+  DMState<float> d;
+  Flags fl;
+  auto t0 = std::chrono::steady_clock::now();
+  for (int it = 0; it < iters; ++it) dm_iteration<float>(s, d, amp, pos, fl, it + 1, nthreads);
+  auto t1 = std::chrono::steady_clock::now();
+  if (obj_out)
+    for (size_t i = 0; i < XY; ++i) { obj_out[2 * i] = s.O[i].real(); obj_out[2 * i + 1] = s.O[i].imag(); }
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+}  // extern "C"

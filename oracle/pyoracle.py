@@ -1,0 +1,169 @@
+"""ctypes wrapper of the oracle (oracle/oracle.cpp).  TEST INFRASTRUCTURE ONLY: imported by tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker; never by the product.
+
+Parity status: unpinned by the reference (no reference golden vectors exist and the reference does not build);
+pinned to numpy.fft, hand-derived known answers and the committed fixtures under tests/golden/.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "oracle.cpp")
+LIB = os.path.join(HERE, "liboracle.so")
+
+
+def build(force=False, verbose=False):
+    """Compile the oracle (g++ only; no GPU needed)."""
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+        cmd = ["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-o", LIB, SRC, "-lpthread"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(LIB)
+        vp, i, d, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_float
+        u64 = ctypes.c_uint64
+        sig = {
+            "orc_fft2": ([vp, i, i], i),
+            "orc_sample_pixel": ([d, d, d, i], d),
+            "orc_cartesian_mesh": ([i, i, d, d, d, d, d, i, i, i, i, vp, vp], i),
+            "orc_list_mesh": ([vp, i, d, d, d, i, i, vp, vp], i),
+            "orc_probe_guess": ([vp, i, i, d, d, i, vp], i),
+            "orc_visiting_order": ([ctypes.POINTER(u64), i, vp], None),
+            "orc_extract_patch": ([vp, i, i, f, f, i, vp], i),
+            "orc_create": ([i, i, i, i, i, i, vp, vp, vp, vp, i, i, u64, i, i, i, i, i], vp),
+            "orc_step": ([vp, ctypes.POINTER(d)], i),
+            "orc_get": ([vp, vp, vp, vp], i),
+            "orc_get_psi": ([vp, vp], i),
+            "orc_destroy": ([vp], None),
+            "orc_dm_baseline_f32": ([i, i, i, i, vp, vp, vp, i, i, vp], d),
+        }
+        for name, (a, r) in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = a
+            fn.restype = r
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def fft2(a, inverse=False):
+    b = np.ascontiguousarray(a, dtype=np.complex128).copy()
+    assert lib().orc_fft2(_p(b), b.shape[0], int(inverse)) == 0
+    return b
+
+
+def sample_pixel(lambd, z, dx_d, N):
+    return lib().orc_sample_pixel(lambd, z, dx_d, N)
+
+
+def cartesian_mesh(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX=0, mirrorY=0, flip=0):
+    pos = np.zeros((nx * ny, 2), np.float32)
+    xy = np.zeros(2, np.int32)
+    assert lib().orc_cartesian_mesh(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX, mirrorY, flip, _p(pos),
+                                    _p(xy)) == 0
+    return pos, int(xy[0]), int(xy[1])
+
+
+def list_mesh(xy_m, lambd, z, dx_d, N, flip=0):
+    xy_m = np.ascontiguousarray(xy_m, np.float64)
+    pos = np.zeros((xy_m.shape[0], 2), np.float32)
+    xy = np.zeros(2, np.int32)
+    assert lib().orc_list_mesh(_p(xy_m), xy_m.shape[0], lambd, z, dx_d, N, flip, _p(pos), _p(xy)) == 0
+    return pos, int(xy[0]), int(xy[1])
+
+
+def probe_guess(amp, beamSize, dx_s, K=1):
+    amp = np.ascontiguousarray(amp, np.float64)
+    P, N = amp.shape[0], amp.shape[1]
+    out = np.zeros((K, N, N), np.complex128)
+    assert lib().orc_probe_guess(_p(amp), P, N, beamSize, dx_s, K, _p(out)) == 0
+    return out
+
+
+def visiting_order(state, P):
+    s = ctypes.c_uint64(state)
+    order = np.zeros(P, np.int32)
+    lib().orc_visiting_order(ctypes.byref(s), P, _p(order))
+    return order, s.value
+
+
+def extract_patch(obj, qx, qy, N):
+    o = np.ascontiguousarray(obj, np.complex128)
+    out = np.zeros((N, N), np.complex128)
+    assert lib().orc_extract_patch(_p(o), o.shape[0], o.shape[1], qx, qy, N, _p(out)) == 0
+    return out
+
+
+class OracleSession:
+    """FP64 restatement of one reconstruction (algo 'ePIE' or 'DM'), stepped one iteration at a time."""
+
+    def __init__(self, algo, amp, pos, obj, probe, *, probe_guess_path, modes_given=False, seed=0x5EED5EED,
+                 phaseConstraint=1, updateProbe=10, updateModes=20, calculateRMS=0, nthreads=1):
+        self.amp = np.ascontiguousarray(amp, np.float64)
+        self.pos = np.ascontiguousarray(pos, np.float32)
+        obj = np.ascontiguousarray(obj, np.complex128)
+        probe = np.ascontiguousarray(probe, np.complex128)
+        if probe.ndim == 2:
+            probe = probe[None]
+        self.X, self.Y = obj.shape
+        self.K, self.N = probe.shape[0], probe.shape[1]
+        self.P = self.amp.shape[0]
+        self.h = lib().orc_create(0 if algo == "ePIE" else 1, self.N, self.K, self.P, self.X, self.Y, _p(self.amp),
+                                  _p(self.pos), _p(obj), _p(probe), int(probe_guess_path), int(modes_given),
+                                  seed, phaseConstraint, updateProbe, updateModes, calculateRMS, nthreads)
+        if not self.h:
+            raise ValueError("oracle rejected the configuration")
+
+    def step(self):
+        e = ctypes.c_double(0)
+        rc = lib().orc_step(self.h, ctypes.byref(e))
+        if rc:
+            raise RuntimeError(f"oracle step failed ({rc})")
+        return e.value
+
+    def state(self):
+        o = np.zeros((self.X, self.Y), np.complex128)
+        p = np.zeros((self.K, self.N, self.N), np.complex128)
+        sc = np.zeros(4, np.float64)
+        lib().orc_get(self.h, _p(o), _p(p), _p(sc))
+        return o, p, sc
+
+    def psi(self):
+        out = np.zeros((self.P, self.N, self.N), np.complex128)
+        lib().orc_get_psi(self.h, _p(out))
+        return out
+
+    def close(self):
+        if self.h:
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def dm_baseline_f32(amp, pos, probe, X, Y, iters, nthreads):
+    """Multithreaded FP32 DM on the host (the CPU baseline).  Returns (seconds, object)."""
+    amp = np.ascontiguousarray(amp, np.float32)
+    pos = np.ascontiguousarray(pos, np.float32)
+    pr = np.ascontiguousarray(probe.reshape(-1, probe.shape[-1])[: probe.shape[-1]], np.complex64)
+    obj = np.zeros((X, Y), np.complex64)
+    N = amp.shape[1]
+    t = lib().orc_dm_baseline_f32(N, amp.shape[0], X, Y, _p(amp), _p(pos), _p(pr), iters, nthreads, _p(obj))
+    return t, obj

@@ -1,0 +1,197 @@
+// Register/shared-memory FFT building blocks for sm_100a.
+//
+// A length-L transform (L = E*T, E >= T, E % T == 0, both powers of two) is computed by T threads that each hold
+// E complex values in registers:
+//   stage 1  thread t holds x[t + T*e] (e < E), does an E-point DFT in registers and multiplies output k1 by
+//            w_L^(t*k1) (table in shared memory, laid out [k1][t] so a warp reads it conflict-free);
+//   exchange the E x T intermediate goes through a per-vector shared buffer with pitch T+1 (conflict-free for both
+//            the column write and the row read);
+//   stage 2  thread t takes k1 = t + T*m (m < E/T) and does T-point DFTs over the threads' values.
+// On return thread t holds X[t + T*e] in register v[m*T + k2] with e = m + (E/T)*k2, i.e. the same index set
+// it loaded, so transforms can be chained (forward -> pointwise -> inverse) with no data movement.
+//
+// The in-register DFTs are radix-2 decimation-in-frequency with compile-time twiddles (all indices resolve at
+// compile time, so everything stays in registers); trivial twiddles (multiples of pi/4) skip the multiplies.
+// Sign convention is cuFFT's: forward exp(-2*pi*i*k*n/L), inverse exp(+...), no scaling.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+namespace pty {
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+// conj(a) * b
+__device__ __forceinline__ float2 cconjmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+// cos(2*pi*q/32) for q in [0, 8]: exact values of the first octant, rounded to float.
+__host__ __device__ constexpr float cos32_octant(int q) {
+  return q == 0 ? 1.0f
+       : q == 1 ? 0.98078528040323044913f
+       : q == 2 ? 0.92387953251128675613f
+       : q == 3 ? 0.83146961230254523708f
+       : q == 4 ? 0.70710678118654752440f
+       : q == 5 ? 0.55557023301960222474f
+       : q == 6 ? 0.38268343236508977173f
+       : q == 7 ? 0.19509032201612826785f
+                : 0.0f;
+}
+// cos and sin of 2*pi*q/32 for any q in [0, 32) by octant symmetry.
+__host__ __device__ constexpr float cos32(int q) {
+  return q <= 8 ? cos32_octant(q) : q <= 16 ? -cos32_octant(16 - q) : q <= 24 ? -cos32_octant(q - 16)
+                                                                               : cos32_octant(32 - q);
+}
+__host__ __device__ constexpr float sin32(int q) { return cos32((q + 24) % 32); }
+
+// v * exp(-2*pi*i*Q/32) (forward) or v * exp(+2*pi*i*Q/32) (inverse), Q a compile-time constant.
+template <int Q, bool INV>
+__device__ __forceinline__ float2 twiddle32(float2 v) {
+  constexpr int q = Q % 32;
+  if constexpr (q == 0) {
+    return v;
+  } else if constexpr (q == 16) {
+    return make_float2(-v.x, -v.y);
+  } else if constexpr (q == 8) {  // exp(-i*pi/2) = -i
+    return INV ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
+  } else if constexpr (q == 24) {  // exp(-i*3pi/2) = +i
+    return INV ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
+  } else {
+    constexpr float c = cos32(q), s = sin32(q);
+    // forward: (x + iy)(c - is) = (xc + ys) + i(yc - xs); inverse: (x + iy)(c + is)
+    if constexpr (INV)
+      return make_float2(v.x * c - v.y * s, v.y * c + v.x * s);
+    else
+      return make_float2(v.x * c + v.y * s, v.y * c - v.x * s);
+  }
+}
+
+// Compile-time loop: f(std::integral_constant<int, I>) for I in [B, E).  Register-array indices computed from
+// the loop constant are then constant expressions, so the arrays never fall back to local memory.
+template <int B, int E, typename F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (B < E) {
+    f(std::integral_constant<int, B>{});
+    static_for<B + 1, E>(f);
+  }
+}
+
+__host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
+__host__ __device__ constexpr int bitrev(int i, int n) {
+  int r = 0;
+  for (int b = 0; b < ilog2(n); ++b) r |= ((i >> b) & 1) << (ilog2(n) - 1 - b);
+  return r;
+}
+
+// ---- compile-time radix-2 DIF DFT on a register array (output in bit-reversed order) -------------------
+template <int LEN, int S, int J, bool INV, int E>
+__device__ __forceinline__ void dif_butterflies(float2 (&a)[E]) {
+  if constexpr (J < LEN / 2) {
+    float2 u = a[S + J], w = a[S + J + LEN / 2];
+    a[S + J] = cadd(u, w);
+    a[S + J + LEN / 2] = twiddle32<J*(32 / LEN), INV>(csub(u, w));
+    dif_butterflies<LEN, S, J + 1, INV>(a);
+  }
+}
+template <int LEN, int S, bool INV, int E>
+__device__ __forceinline__ void dif_blocks(float2 (&a)[E]) {
+  if constexpr (S < E) {
+    dif_butterflies<LEN, S, 0, INV>(a);
+    dif_blocks<LEN, S + LEN, INV>(a);
+  }
+}
+template <int LEN, bool INV, int E>
+__device__ __forceinline__ void dif_stages(float2 (&a)[E]) {
+  if constexpr (LEN >= 2) {
+    dif_blocks<LEN, 0, INV>(a);
+    dif_stages<LEN / 2, INV>(a);
+  }
+}
+// In place: afterwards a[bitrev(k)] = sum_n a_in[n] w_E^(k*n).  E <= 32.
+template <bool INV, int E>
+__device__ __forceinline__ void dft_reg(float2 (&a)[E]) {
+  static_assert(E >= 2 && E <= 32 && (E & (E - 1)) == 0, "register DFT size");
+  dif_stages<E, INV>(a);
+}
+
+// Thread layout of a length-L transform.
+template <int L>
+struct FftShape {
+  static constexpr int T = (L == 1024) ? 32 : (L == 512) ? 16 : (L == 256) ? 16 : (L == 128) ? 8 : (L == 64) ? 8
+                          : (L == 32) ? 4 : 0;
+  static constexpr int E = L / T;      // registers (complex) per thread
+  static constexpr int M = E / T;      // stage-2 DFTs per thread
+  static constexpr int XCH = E * (T + 1);  // exchange buffer (float2) per vector
+  static_assert(T > 0, "unsupported FFT length");
+};
+
+// Twiddle table for stage 1: tw[k1*T + t] = exp(-2*pi*i*t*k1/L); filled by fill_twiddles (double precision).
+template <int L>
+__device__ __forceinline__ void load_twiddles(float2* s_tw, const float2* __restrict__ g_tw) {
+  for (int i = threadIdx.x; i < L; i += blockDim.x) s_tw[i] = g_tw[i];
+}
+
+// One length-L transform by T cooperating lanes of a warp (lane group `t` = 0..T-1).
+// v: on entry v[e] = x[t + T*e]; on exit v[m*T + k2] = X[t + T*(m + M*k2)].
+// xch: this vector's exchange buffer (XCH float2).  Ends with __syncwarp (xch reusable).
+template <int L, bool INV>
+__device__ __forceinline__ void fft_vec(float2 (&v)[FftShape<L>::E], int t, float2* xch, const float2* s_tw) {
+  constexpr int T = FftShape<L>::T, E = FftShape<L>::E, M = FftShape<L>::M;
+  dft_reg<INV>(v);
+  static_for<0, E>([&](auto k1c) {
+    constexpr int k1 = decltype(k1c)::value;
+    constexpr int src = bitrev(k1, E);
+    if constexpr (k1 == 0) {
+      xch[t] = v[src];
+    } else {
+      float2 w = s_tw[k1 * T + t];
+      if (INV) w.y = -w.y;
+      xch[k1 * (T + 1) + t] = cmul(v[src], w);
+    }
+  });
+  __syncwarp();
+  static_for<0, M>([&](auto mc) {
+    constexpr int m = decltype(mc)::value;
+    float2 c[T];
+#pragma unroll
+    for (int tt = 0; tt < T; ++tt) c[tt] = xch[(t + T * m) * (T + 1) + tt];
+    dft_reg<INV>(c);
+    static_for<0, T>([&](auto k2c) {
+      constexpr int k2 = decltype(k2c)::value;
+      v[m * T + k2] = c[bitrev(k2, T)];
+    });
+  });
+  __syncwarp();
+}
+
+// Register slot of element index n = t + T*e for this thread: slot(e) = m*T + k2 with e = m + M*k2.
+template <int L>
+__host__ __device__ constexpr int out_slot(int e) {
+  return (e % FftShape<L>::M) * FftShape<L>::T + (e / FftShape<L>::M);
+}
+
+// After fft_vec the thread holds element t + T*e in v[out_slot(e)].  To feed a second transform (which wants
+// v[e] = element t + T*e) reorder the registers (free at compile time).
+template <int L>
+__device__ __forceinline__ void to_input_order(float2 (&v)[FftShape<L>::E]) {
+  constexpr int E = FftShape<L>::E;
+  float2 tmp[E];
+  static_for<0, E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    tmp[e] = v[out_slot<L>(e)];
+  });
+#pragma unroll
+  for (int e = 0; e < E; ++e) v[e] = tmp[e];
+}
+
+}  // namespace pty

@@ -1,0 +1,483 @@
+// ePIE (src/ePIE.cpp:65-129) as ONE persistent kernel: a single thread-block cluster of C CTAs walks the
+// seeded visiting order serially; each position is five phases separated by cluster barriers.  The CTAs split
+// rows (row phases) and columns (column phase) of the N x N window; intermediates live in two small global
+// buffers that stay in L2 (Ka*N*N complex each).
+//
+//   A  rows     patch = bilinear O at (x+qx, y+qy) with 1/256-quantised weights (texture fetch,
+//               src/SampleKernels.cu:167-178), psi_old_k = patch * P_k (src/CXMath.h:49-58), FFT along y,
+//               stored transposed: W1[k][ky][x]
+//   B  columns  FFT along x, error term |A - |sum_k Psi_k|| (src/utilitiesKernels.cu:684-712), modulus
+//               (d_adjustFFT / d_adjustModalFFT, src/utilitiesKernels.cu:633-682), D_k = Psi'_k - Psi_k/N^2,
+//               inverse FFT along x, stored transposed: W2[k][x][ky]
+//   C  rows     inverse FFT along y gives dpsi_k = psi_k - psi_old_k; object update at the rounded offset
+//               O += (1/probeMax) sum_k conj(P_k) dpsi_k, phase clamp, |O|^2 cache (src/SampleKernels.cu:244-294)
+//   D  tiles    16x16 tile maxima of the |O|^2 cache are refreshed where the patch touched them; every CTA
+//               then takes the max over all tiles = max |O|^2 over the whole object (src/Sample.cpp:340-345)
+//   E  rows     probe update P_k += (1/objMax) conj(O_new) dpsi_k and |P_k|^2 cache (src/ProbeKernels.cu:425-458),
+//               per-CTA partial of Probe::getModalDoubleMax, combined after the barrier
+//
+// Cluster barriers (barrier.cluster arrive.release / wait.acquire, preceded by a device-scope fence) order the
+// global-memory hand-offs; there are no software spin-waits.
+#include <cooperative_groups.h>
+
+#include "fft_core.cuh"
+#include "kernel_util.cuh"
+#include "kernels_epie.h"
+
+namespace cg = cooperative_groups;
+
+namespace pty {
+
+__device__ __forceinline__ void cluster_barrier() {
+  __threadfence();
+  cg::this_cluster().sync();
+}
+
+// Texture-coordinate emulation for one axis: integer index idx plus fractional base; clamp addressing.
+__device__ __forceinline__ void tex_axis(float base, int idx, int extent, int& i0, int& i1, float& w) {
+  const float c = float(idx) + base;
+  const float tt = c + 0.5f;
+  const float xb = tt - 0.5f;
+  const float fl = floorf(xb);
+  const float fr = xb - fl;
+  w = floorf(fr * 256.f + 0.5f) * (1.f / 256.f);
+  int i = int(fl);
+  i0 = min(max(i, 0), extent - 1);
+  i1 = min(max(i + 1, 0), extent - 1);
+}
+
+template <int L, int R>
+__global__ void __launch_bounds__(R* FftShape<L>::T) k_epie(EpieArgs g) {
+  using S = FftShape<L>;
+  constexpr int T = S::T, E = S::E;
+  constexpr float nrm = 1.0f / float(L * L);
+  extern __shared__ float4 smem4[];
+  float2* smem = reinterpret_cast<float2*>(smem4);
+  float2* s_tw = smem;
+  float2* s_x = smem + L;                                   // exchange / staging
+  float* s_m2 = reinterpret_cast<float*>(s_x + (R * S::XCH > L * (R + 1) ? R * S::XCH : L * (R + 1)));  // R*L
+  float2* s_sum = reinterpret_cast<float2*>(s_m2 + R * L);  // R*L (error metric, Ka > 1)
+  __shared__ float s_objmax, s_probemax;
+
+  const int c = int(cg::this_cluster().block_rank());
+  const int C = g.C;
+  const int v = threadIdx.x / T, t = threadIdx.x % T;
+  const int rows_cta = L / C, passes = rows_cta / R;
+  const int Ka = g.Ka;
+  const size_t NN = size_t(L) * L;
+  const int nthreads = R * T;
+  load_twiddles<L>(s_tw, g.tw);
+  if (threadIdx.x == 0) {
+    s_objmax = g.sc->objMax;
+    s_probemax = g.sc->probeMax;
+  }
+  __syncthreads();
+  double err_acc = 0.0;
+
+  for (int s = 0; s < g.P; ++s) {
+    const int i = g.order[s];
+    const float2 q = g.pos[i];
+    const int ox = int(roundf(q.x)), oy = int(roundf(q.y));
+    const float* Ai = g.ampT + size_t(i) * NN;
+
+    // ---------------- A: bilinear patch * probe modes, row FFT, transposed store into W1 -------------------
+    for (int ps = 0; ps < passes; ++ps) {
+      const int x0 = c * rows_cta + ps * R, x = x0 + v;
+      int r0, r1;
+      float wb;
+      tex_axis(q.x, x, g.X, r0, r1, wb);
+      float2 patch[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int y = t + T * e;
+        int c0, c1;
+        float wa;
+        tex_axis(q.y, y, g.Y, c0, c1, wa);
+        const float2 v00 = g.obj[size_t(r0) * g.Y + c0], v01 = g.obj[size_t(r0) * g.Y + c1];
+        const float2 v10 = g.obj[size_t(r1) * g.Y + c0], v11 = g.obj[size_t(r1) * g.Y + c1];
+        const float w00 = (1.f - wa) * (1.f - wb), w01 = wa * (1.f - wb), w10 = (1.f - wa) * wb, w11 = wa * wb;
+        patch[e] = make_float2(v00.x * w00 + v01.x * w01 + v10.x * w10 + v11.x * w11,
+                               v00.y * w00 + v01.y * w01 + v10.y * w10 + v11.y * w11);
+      }
+      for (int k = 0; k < Ka; ++k) {
+        const float2* prow = g.probe + size_t(k) * NN + size_t(x) * L;
+        float2 a[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) a[e] = cmul(patch[e], prow[t + T * e]);
+        fft_vec<L, false>(a, t, s_x + v * S::XCH, s_tw);
+        store_rows_transposed<L, R>(a, g.W1 + size_t(k) * NN, x0, v, t, s_x);
+      }
+    }
+    cluster_barrier();
+
+    // ---------------- B: column FFT, modulus, inverse column FFT, transposed store into W2 -------------------
+    for (int ps = 0; ps < passes; ++ps) {
+      const int k0 = c * rows_cta + ps * R, ky = k0 + v;
+      const float* arow = Ai + size_t(ky) * L;
+      if (Ka == 1) {
+        float2 a[E];
+        const float2* row = g.W1 + size_t(ky) * L;
+#pragma unroll
+        for (int e = 0; e < E; ++e) a[e] = row[t + T * e];
+        fft_vec<L, false>(a, t, s_x + v * S::XCH, s_tw);
+        static_for<0, E>([&](auto ec) {
+          constexpr int e = decltype(ec)::value;
+          const float A = arow[t + T * e];
+          const float2 psi = a[out_slot<L>(e)];
+          if (g.rms) err_acc += fabsf(A - sqrtf(psi.x * psi.x + psi.y * psi.y));
+          float2 rep;
+          if (A - g.saturation >= 0.f)
+            rep = make_float2(psi.x * nrm, psi.y * nrm);  // floating pixel: no modulus
+          else
+            rep = modulus_replace(psi, A * nrm);
+          a[out_slot<L>(e)] = make_float2(rep.x - psi.x * nrm, rep.y - psi.y * nrm);
+        });
+        to_input_order<L>(a);
+        fft_vec<L, true>(a, t, s_x + v * S::XCH, s_tw);
+        store_rows_transposed<L, R>(a, g.W2, k0, v, t, s_x);
+      } else {
+        float* m2 = s_m2 + v * L;
+        float2* sm = s_sum + v * L;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          m2[t + T * e] = 0.f;
+          sm[t + T * e] = make_float2(0.f, 0.f);
+        }
+        for (int k = 0; k < Ka; ++k) {
+          float2 a[E];
+          float2* row = g.W1 + size_t(k) * NN + size_t(ky) * L;
+#pragma unroll
+          for (int e = 0; e < E; ++e) a[e] = row[t + T * e];
+          fft_vec<L, false>(a, t, s_x + v * S::XCH, s_tw);
+          static_for<0, E>([&](auto ec) {
+            constexpr int e = decltype(ec)::value;
+            const int n = t + T * e;
+            const float2 psi = a[out_slot<L>(e)];
+            row[n] = psi;  // spectrum kept in place for the second sweep
+            m2[n] += psi.x * psi.x + psi.y * psi.y;
+            sm[n] = cadd(sm[n], psi);
+          });
+        }
+        if (g.rms) {
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            const int n = t + T * e;
+            const float2 z = sm[n];
+            err_acc += fabsf(arow[n] - sqrtf(z.x * z.x + z.y * z.y));
+          }
+        }
+        for (int k = 0; k < Ka; ++k) {
+          float2 a[E];
+          const float2* row = g.W1 + size_t(k) * NN + size_t(ky) * L;
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            const int n = t + T * e;
+            const float2 psi = row[n];
+            const float A = arow[n];
+            const float tot = m2[n];
+            const float sc = (tot > 0.f) ? ((A - g.saturation >= 0.f) ? 1.f : A) * rsqrtf(tot) * nrm : 0.f;
+            a[e] = make_float2(psi.x * (sc - nrm), psi.y * (sc - nrm));
+          }
+          fft_vec<L, true>(a, t, s_x + v * S::XCH, s_tw);
+          store_rows_transposed<L, R>(a, g.W2 + size_t(k) * NN, k0, v, t, s_x);
+        }
+      }
+    }
+    if (g.rms) {
+      // per-position error: (sum over pixels)/Ka/sqsum_i, summed over CTAs
+      double e = block_reduce_sum(err_acc);
+      if (threadIdx.x == 0) atomicAdd(&g.sc->err, e / double(Ka) / double(g.sqsum[i]));
+      err_acc = 0.0;
+    }
+    cluster_barrier();
+
+    // ---------------- C: inverse row FFT -> dpsi; object update; |O|^2 cache ----------------------------
+    const float cO = 1.0f / s_probemax;
+    for (int ps = 0; ps < passes; ++ps) {
+      const int x0 = c * rows_cta + ps * R, x = x0 + v;
+      float2 inc[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) inc[e] = make_float2(0.f, 0.f);
+      for (int k = 0; k < Ka; ++k) {
+        float2 a[E];
+        const float2* row = g.W2 + size_t(k) * NN + size_t(x) * L;
+#pragma unroll
+        for (int e = 0; e < E; ++e) a[e] = row[t + T * e];
+        fft_vec<L, true>(a, t, s_x + v * S::XCH, s_tw);
+        const float2* prow = g.probe + size_t(k) * NN + size_t(x) * L;
+        float2* drow = g.W1 + size_t(k) * NN + size_t(x) * L;
+        static_for<0, E>([&](auto ec) {
+          constexpr int e = decltype(ec)::value;
+          const int n = t + T * e;
+          const float2 d = a[out_slot<L>(e)];
+          if (g.up) drow[n] = d;
+          inc[e] = cadd(inc[e], cconjmul(prow[n], d));
+        });
+      }
+      float2* orow = g.obj + size_t(x + ox) * g.Y + oy;
+      float* crow = g.ocache + size_t(x + ox) * g.Y + oy;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int n = t + T * e;
+        float2 o = orow[n];
+        o = make_float2(o.x + inc[e].x * cO, o.y + inc[e].y * cO);
+        const float mag = sqrtf(o.x * o.x + o.y * o.y);
+        if (g.pc) o = constrain_phase(o);
+        orow[n] = o;
+        crow[n] = mag * mag;
+      }
+    }
+    cluster_barrier();
+
+    if (!g.up) continue;  // the object max is only consumed by the probe update
+
+    // ---------------- D: refresh tile maxima under the patch, then the global object max ---------------------
+    {
+      const int tr0 = ox / 16, tr1 = (ox + L - 1) / 16, tc0 = oy / 16, tc1 = (oy + L - 1) / 16;
+      const int ntc = tc1 - tc0 + 1, ntiles = (tr1 - tr0 + 1) * ntc;
+      const int warps = nthreads / 32, gw = c * warps + int(threadIdx.x / 32), lane = threadIdx.x & 31;
+      for (int tile = gw; tile < ntiles; tile += C * warps) {
+        const int tr = tr0 + tile / ntc, tc = tc0 + tile % ntc;
+        float m = 0.f;
+        for (int j = lane; j < 256; j += 32) {
+          const int xr = tr * 16 + j / 16, yc = tc * 16 + j % 16;
+          if (xr < g.X && yc < g.Y) m = fmaxf(m, g.ocache[size_t(xr) * g.Y + yc]);
+        }
+        m = warp_reduce_maxf(m);
+        if (lane == 0) g.TM[size_t(tr) * g.TY + tc] = m;
+      }
+    }
+    cluster_barrier();
+    {
+      float m = 0.f;
+      const int nt = g.TX * g.TY;
+      for (int j = threadIdx.x; j < nt; j += nthreads) m = fmaxf(m, g.TM[j]);
+      m = block_reduce_maxf(m);
+      if (threadIdx.x == 0) s_objmax = m;
+      __syncthreads();
+    }
+
+    // ---------------- E: probe update and the modal max of the probe intensity cache -----------------------
+    {
+      const float cP = 1.0f / s_objmax;
+      float pmax = 0.f;
+      for (int ps = 0; ps < passes; ++ps) {
+        const int x0 = c * rows_cta + ps * R, x = x0 + v;
+        const float2* orow = g.obj + size_t(x + ox) * g.Y + oy;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int n = t + T * e;
+          const float2 oc = orow[n];
+          float modal = 0.f;
+          for (int k = 0; k < g.K; ++k) {
+            const size_t idx = size_t(k) * NN + size_t(x) * L + n;
+            float cache;
+            if (k < Ka) {
+              const float2 d = g.W1[idx];
+              const float2 u = cconjmul(oc, d);
+              float2 pv = g.probe[idx];
+              pv = make_float2(u.x * cP + pv.x, u.y * cP + pv.y);
+              const float mg = sqrtf(pv.x * pv.x + pv.y * pv.y);
+              g.probe[idx] = pv;
+              cache = mg * mg;
+              g.pcache[idx] = cache;
+            } else {
+              cache = g.pcache[idx];
+            }
+            if (g.useAll && g.K > 1)
+              modal += cache;
+            else
+              pmax = fmaxf(pmax, cache);
+          }
+          if (g.useAll && g.K > 1) pmax = fmaxf(pmax, modal);
+        }
+      }
+      pmax = block_reduce_maxf(pmax);
+      if (threadIdx.x == 0) g.pm[c] = pmax;
+      cluster_barrier();
+      if (threadIdx.x == 0) {
+        float m = 0.f;
+        for (int j = 0; j < C; ++j) m = fmaxf(m, g.pm[j]);
+        s_probemax = m;
+      }
+      __syncthreads();
+      cluster_barrier();  // pm is rewritten at the next position
+    }
+  }
+  if (c == 0 && threadIdx.x == 0) {
+    g.sc->objMax = s_objmax;
+    g.sc->probeMax = s_probemax;
+  }
+}
+
+// Rows per pass of a CTA (blockDim = R * T) for a length-L window.
+template <int L> struct EpieShape;
+template <> struct EpieShape<32> { static constexpr int R = 8; };
+template <> struct EpieShape<64> { static constexpr int R = 4; };
+template <> struct EpieShape<128> { static constexpr int R = 8; };
+template <> struct EpieShape<256> { static constexpr int R = 16; };
+template <> struct EpieShape<512> { static constexpr int R = 16; };
+
+template <int L>
+static size_t epie_smem(int) {
+  constexpr int R = EpieShape<L>::R, XCH = FftShape<L>::XCH;
+  constexpr int xs = R * XCH > L * (R + 1) ? R * XCH : L * (R + 1);
+  return sizeof(float2) * (L + xs) + sizeof(float) * R * L + sizeof(float2) * R * L;
+}
+
+template <int L>
+static cudaError_t epie_prepare_t(int* C_out) {
+  constexpr int R = EpieShape<L>::R, T = FftShape<L>::T;
+  auto kern = k_epie<L, R>;
+  const size_t smem = epie_smem<L>(0);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) return e;
+  // Largest cluster (<= 16, dividing the rows into whole passes, >= one warp per CTA) that can be resident.
+  int best = 0;
+  for (int C = 16; C >= 1; C /= 2) {
+    if (L % C || (L / C) % R) continue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C);
+    cfg.blockDim = dim3(R * T);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) == cudaSuccess && n >= 1) {
+      best = C;
+      break;
+    }
+    cudaGetLastError();
+  }
+  if (!best) return cudaErrorInvalidConfiguration;
+  *C_out = best;
+  return cudaSuccess;
+}
+
+cudaError_t epie_prepare(int N, int* C_out) {
+  switch (N) {
+    case 32: return epie_prepare_t<32>(C_out);
+    case 64: return epie_prepare_t<64>(C_out);
+    case 128: return epie_prepare_t<128>(C_out);
+    case 256: return epie_prepare_t<256>(C_out);
+    case 512: return epie_prepare_t<512>(C_out);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int L>
+static cudaError_t epie_launch_t(const EpieArgs& g, cudaStream_t st) {
+  constexpr int R = EpieShape<L>::R, T = FftShape<L>::T;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(g.C);
+  cfg.blockDim = dim3(R * T);
+  cfg.dynamicSmemBytes = epie_smem<L>(0);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = g.C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_epie<L, R>, g);
+}
+
+cudaError_t epie_launch(const EpieArgs& g, cudaStream_t st) {
+  switch (g.N) {
+    case 32: return epie_launch_t<32>(g, st);
+    case 64: return epie_launch_t<64>(g, st);
+    case 128: return epie_launch_t<128>(g, st);
+    case 256: return epie_launch_t<256>(g, st);
+    case 512: return epie_launch_t<512>(g, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+__global__ void k_tile_max_all(const float* __restrict__ ocache, int X, int Y, float* __restrict__ TM, int TY) {
+  const int tr = blockIdx.y, tc = blockIdx.x;
+  float m = 0.f;
+  for (int j = threadIdx.x; j < 256; j += blockDim.x) {
+    const int xr = tr * 16 + j / 16, yc = tc * 16 + j % 16;
+    if (xr < X && yc < Y) m = fmaxf(m, ocache[size_t(xr) * Y + yc]);
+  }
+  m = block_reduce_maxf(m);
+  if (threadIdx.x == 0) TM[size_t(tr) * TY + tc] = m;
+}
+
+cudaError_t tile_max_all(const float* ocache, int X, int Y, float* TM, int TX, int TY, cudaStream_t st) {
+  k_tile_max_all<<<dim3(TY, TX), 64, 0, st>>>(ocache, X, Y, TM, TY);
+  return cudaGetLastError();
+}
+
+// ---- modal set-up (Probe::initProbeModes / orthogonalize, src/Probe.cpp:229-242,320-330) ---------------
+__global__ void k_modes_from_base(float2* __restrict__ probe, float* __restrict__ pcache, int K, size_t NN,
+                                  float factor) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < NN; i += size_t(gridDim.x) * blockDim.x) {
+    const float2 b = probe[i];
+    const float2 v = make_float2(b.x * factor, b.y * factor);
+    const float m = sqrtf(v.x * v.x + v.y * v.y);
+    for (int k = 1; k < K; ++k) {
+      probe[size_t(k) * NN + i] = v;
+      pcache[size_t(k) * NN + i] = m * m;
+    }
+  }
+}
+
+// out[0..1] += sum conj(a) * b, out[2] += sum |a|^2 (double accumulation)
+__global__ void k_inner(const float2* __restrict__ a, const float2* __restrict__ b, size_t n, double* out) {
+  double re = 0, im = 0, aa = 0;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    const float2 x = a[i], y = b[i];
+    re += double(x.x) * y.x + double(x.y) * y.y;
+    im += double(x.x) * y.y - double(x.y) * y.x;
+    aa += double(x.x) * x.x + double(x.y) * x.y;
+  }
+  re = block_reduce_sum(re);
+  __syncthreads();
+  im = block_reduce_sum(im);
+  __syncthreads();
+  aa = block_reduce_sum(aa);
+  if (threadIdx.x == 0) {
+    atomicAdd(&out[0], re);
+    atomicAdd(&out[1], im);
+    atomicAdd(&out[2], aa);
+  }
+}
+
+// target -= f * u with f = conj(<u, v>) / <u, u> read from ip = {Re<u,v>, Im<u,v>, <u,u>} (h_projectUtoV:
+// factor = innerProduct(v, u) / innerProduct(u, u), innerProduct(a, b) = sum conj(a) b).
+__global__ void k_project_sub(float2* __restrict__ target, const float2* __restrict__ u, size_t n,
+                              const double* __restrict__ ip) {
+  const double fr = ip[0] / ip[2], fi = -ip[1] / ip[2];
+  const float2 f = make_float2(float(fr), float(fi));
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    target[i] = csub(target[i], cmul(f, u[i]));
+}
+
+cudaError_t epie_init_modes(float2* probe, float* pcache, int K, int N, float2* copy, double* scratch3,
+                            cudaStream_t st) {
+  const size_t NN = size_t(N) * N;
+  int grid = int((NN + 255) / 256);
+  if (grid > 1184) grid = 1184;
+  k_modes_from_base<<<grid, 256, 0, st>>>(probe, pcache, K, NN, 0.05f);
+  cudaError_t e = cudaMemcpyAsync(copy, probe, sizeof(float2) * NN * K, cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess) return e;
+  for (int i = 1; i < K; ++i)
+    for (int j = i - 1; j >= 0; --j) {
+      e = cudaMemsetAsync(scratch3, 0, 3 * sizeof(double), st);
+      if (e != cudaSuccess) return e;
+      k_inner<<<grid, 256, 0, st>>>(probe + size_t(j) * NN, copy + size_t(i) * NN, NN, scratch3);
+      k_project_sub<<<grid, 256, 0, st>>>(probe + size_t(i) * NN, probe + size_t(j) * NN, NN, scratch3);
+    }
+  return cudaGetLastError();
+}
+
+}  // namespace pty

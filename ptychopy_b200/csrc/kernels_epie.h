@@ -1,0 +1,45 @@
+// Persistent ePIE kernel interface (kernels_epie.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+namespace pty {
+
+// Device-resident scalars carried between positions and iterations.
+struct EpieScalars {
+  float objMax;    // Sample::m_maxObjectIntensity (max of the |O|^2 cache)
+  float probeMax;  // Probe::m_maxIntensity
+  double err;      // iteration error accumulator
+};
+
+struct EpieArgs {
+  const float* ampT;      // P x N x N amplitudes, each plane transposed ([ky][kx])
+  float2* obj;            // X x Y
+  float* ocache;          // X x Y |O|^2 cache
+  float2* probe;          // K x N x N
+  float* pcache;          // K x N x N |P_k|^2 cache
+  const float2* pos;      // P fractional positions (pixels)
+  const int* order;       // P visiting order of this iteration
+  float2* W1;             // Ka x N x N
+  float2* W2;             // Ka x N x N
+  float* TM;              // TX x TY tile maxima of ocache (16 x 16 tiles)
+  float* pm;              // C partial probe maxima
+  EpieScalars* sc;
+  const float2* tw;
+  const double* sqsum;    // per-pattern amplitude sums (error normaliser)
+  float saturation;       // pixels with A >= saturation float (no modulus)
+  int N, K, Ka, P, X, Y, TX, TY, C;
+  int pc, up, rms, useAll;
+};
+
+// Sets kernel attributes and picks the cluster size (largest resident of 16, 8, ...); returns it in C_out.
+cudaError_t epie_prepare(int N, int* C_out);
+cudaError_t epie_launch(const EpieArgs& g, cudaStream_t st);
+// Modes 1..K-1 = 0.05 * mode 0, then Gram-Schmidt against the original copies.
+cudaError_t epie_init_modes(float2* probe, float* pcache, int K, int N, float2* copy, double* scratch3,
+                            cudaStream_t st);
+// Tile maxima of the whole |O|^2 cache.
+cudaError_t tile_max_all(const float* ocache, int X, int Y, float* TM, int TX, int TY, cudaStream_t st);
+
+}  // namespace pty

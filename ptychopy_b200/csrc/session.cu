@@ -1,0 +1,914 @@
+// Host orchestration and the C ABI (include/ptychopy_b200.h).  One pty_session is one reconstruction: the
+// reference's IPhaser + CXParams pair (src/IPhaser.cpp:224-365, src/Parameters.cpp:380-653), with parameters
+// held per session instead of in a process-wide singleton.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <limits>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "kernels_epie.h"
+#include "session.h"
+
+namespace pty {
+
+static thread_local std::string g_last_error;
+
+[[noreturn]] void fail(int code, const std::string& msg) { throw Error{code, msg}; }
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  cudaGetLastError();
+  const int code = (e == cudaErrorMemoryAllocation) ? PTY_ERR_OOM : PTY_ERR_CUDA;
+  fail(code, std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+void DeviceBuf::alloc(size_t n, const char* what) {
+  free();
+  if (n == 0) n = 16;
+  check_cuda(cudaMalloc(&p, n), what);
+  bytes = n;
+}
+void DeviceBuf::free() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+// ---- geometry (FP32 like the reference's device code) -------------------------------------------------
+// dx_s = lambda*z/(N*dx_d) returned as real_t (float) by Parameters::samplePlanePixelSize (src/Parameters.h:175-179)
+double sample_pixel_size(double lambda, double z, double dx_d, int N) {
+  return double(float((lambda * z) / (double(N) * dx_d)));
+}
+
+// min/max, object size ceil(max - min + N) and the -min shift (src/IPtychoScanMesh.cpp:86-109).
+static void finish_geometry(const std::vector<float>& raw, int P, bool padZero, int N, bool flip, Geometry& g) {
+  float mnx = std::numeric_limits<float>::max(), mny = mnx, mxx = -mnx, mxy = -mnx;
+  for (int i = 0; i < P; ++i) {
+    mnx = std::min(mnx, raw[2 * i]);
+    mxx = std::max(mxx, raw[2 * i]);
+    mny = std::min(mny, raw[2 * i + 1]);
+    mxy = std::max(mxy, raw[2 * i + 1]);
+  }
+  if (padZero) {  // list meshes are padded to whole 1024-wide rows of (0,0) that join the min/max
+    mnx = std::min(mnx, 0.f);
+    mxx = std::max(mxx, 0.f);
+    mny = std::min(mny, 0.f);
+    mxy = std::max(mxy, 0.f);
+  }
+  volatile float ex = (mxx - mnx) + float(N);
+  volatile float ey = (mxy - mny) + float(N);
+  g.X = int(std::ceil(float(ex)));
+  g.Y = int(std::ceil(float(ey)));
+  g.pos.resize(2 * size_t(P));
+  for (int i = 0; i < P; ++i) {
+    const float tx = raw[2 * i], ty = raw[2 * i + 1];
+    g.pos[2 * i] = flip ? ty - mny : tx - mnx;
+    g.pos[2 * i + 1] = flip ? tx - mnx : ty - mny;
+  }
+}
+
+// Cartesian raster (d_generateMesh<1>, src/ScanMeshKernels.cu:46-93): index i*ny+j,
+// ((i - (nx-1)/2) * stepx) / dx_s in float.
+Geometry cartesian_geometry(int nx, int ny, double stepx, double stepy, double dx_s, int N, bool mirrorX,
+                            bool mirrorY, bool flip) {
+  const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
+  std::vector<float> raw(2 * size_t(nx) * ny);
+  const float mdx = float(nx - 1) * 0.5f, mdy = float(ny - 1) * 0.5f;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      volatile float dx = mirrorX ? (mdx - float(i)) : (float(i) - mdx);
+      volatile float vx = float(dx) * sx;
+      volatile float dy = mirrorY ? (mdy - float(j)) : (float(j) - mdy);
+      volatile float vy = float(dy) * sy;
+      volatile float px = float(vx) * inv, py = float(vy) * inv;
+      raw[2 * (size_t(i) * ny + j)] = px;
+      raw[2 * (size_t(i) * ny + j) + 1] = py;
+    }
+  Geometry g;
+  finish_geometry(raw, nx * ny, false, N, flip, g);
+  return g;
+}
+
+// Position list in metres (ListScanMesh::loadarr + d_generateMesh<2>, src/ListScanMesh.cpp:91-129).
+Geometry list_geometry(const std::vector<double>& xy_m, double dx_s, int N, bool flip) {
+  const int P = int(xy_m.size() / 2);
+  const float inv = float(1.0 / dx_s);
+  std::vector<float> raw(2 * size_t(P));
+  for (int i = 0; i < P; ++i) {
+    volatile float x = float(xy_m[2 * i]), y = float(xy_m[2 * i + 1]);
+    volatile float px = float(x) * inv, py = float(y) * inv;
+    raw[2 * i] = px;
+    raw[2 * i + 1] = py;
+  }
+  Geometry g;
+  finish_geometry(raw, P, (P % 1024) != 0, N, flip, g);
+  return g;
+}
+
+uint64_t splitmix64(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+void visiting_order(uint64_t& state, int P, std::vector<int>& order) {
+  std::vector<int> rem(P);
+  for (int i = 0; i < P; ++i) rem[i] = i;
+  order.resize(P);
+  for (int s = 0; s < P; ++s) {
+    const int k = int(splitmix64(state) % uint64_t(rem.size()));
+    order[s] = rem[k];
+    rem.erase(rem.begin() + k);
+  }
+}
+
+// Device state of the persistent ePIE kernel.
+struct EpieState {
+  DeviceBuf pos, order, W1, W2, TM, pm, sc, sq, modesCopy, ip;
+  int C = 1, TX = 0, TY = 0;
+  bool tm_valid = false;
+  int* order_h = nullptr;  // pinned
+  ~EpieState() {
+    if (order_h) cudaFreeHost(order_h);
+  }
+};
+
+}  // namespace pty
+
+using namespace pty;
+
+namespace {
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return PTY_OK;
+  } catch (const Error& e) {
+    g_last_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return PTY_ERR_OOM;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return PTY_ERR_INVALID;
+  }
+}
+
+void need(bool cond, const std::string& msg, int code = PTY_ERR_INVALID) {
+  if (!cond) fail(code, msg);
+}
+
+void set_device(pty_session* s) { check_cuda(cudaSetDevice(s->dev), "cudaSetDevice"); }
+
+Algo parse_algo(const char* a) {
+  std::string s(a);
+  if (s == "ePIE") return ALGO_EPIE;
+  if (s == "DM") return ALGO_DM;
+  if (s == "MLs") return ALGO_MLS;
+  fail(PTY_ERR_INVALID, "unknown algorithm '" + s + "' (expected ePIE, DM or MLs)");
+}
+
+// Float32 host->device copy of P*N*N values from float32 or float64 host data.
+void upload_patterns(pty_session* s, const void* host, int dtype, size_t n) {
+  s->amp.alloc(n * sizeof(float), "patterns");
+  if (dtype == PTY_F32) {
+    // cudaMemcpyDefault: the source may be host memory (pageable or pinned) or, through UVA, device memory
+    check_cuda(cudaMemcpyAsync(s->amp.p, host, n * sizeof(float), cudaMemcpyDefault, s->stream), "H2D patterns");
+  } else {
+    const double* src = static_cast<const double*>(host);
+    const size_t chunk = size_t(1) << 22;
+    float* stage = nullptr;
+    check_cuda(cudaMallocHost(&stage, chunk * sizeof(float)), "pinned staging");
+    try {
+      for (size_t off = 0; off < n; off += chunk) {
+        const size_t m = std::min(chunk, n - off);
+        check_cuda(cudaStreamSynchronize(s->stream), "staging sync");
+        for (size_t i = 0; i < m; ++i) stage[i] = float(src[off + i]);
+        check_cuda(cudaMemcpyAsync(s->amp.as<float>() + off, stage, m * sizeof(float), cudaMemcpyHostToDevice,
+                                   s->stream),
+                   "H2D patterns");
+      }
+      check_cuda(cudaStreamSynchronize(s->stream), "staging sync");
+    } catch (...) {
+      cudaFreeHost(stage);
+      throw;
+    }
+    cudaFreeHost(stage);
+  }
+}
+
+// Reference CSV cell: `re` then '+' when im >= 0, `im`, 'j' (src/Cuda2DArray.cpp:46-52); ", " between cells.
+void write_complex_file(const std::string& path, const float* c64, size_t rows, size_t cols, bool binary) {
+  std::ofstream f(path, binary ? std::ios::out | std::ios::binary : std::ios::out);
+  if (!f.is_open()) fail(PTY_ERR_IO, "cannot open " + path + " for writing");
+  if (binary) {
+    f.write(reinterpret_cast<const char*>(c64), std::streamsize(rows * cols * 2 * sizeof(float)));
+  } else {
+    for (size_t x = 0; x < rows; ++x) {
+      for (size_t y = 0; y < cols; ++y) {
+        const float re = c64[2 * (x * cols + y)], im = c64[2 * (x * cols + y) + 1];
+        f << re;
+        if (im >= 0) f << "+";
+        f << im << "j";
+        if (y + 1 < cols) f << ", ";
+      }
+      f << std::endl;
+    }
+  }
+  if (!f.good()) fail(PTY_ERR_IO, "write failed: " + path);
+}
+
+// Reads a complex CSV in the reference's format (probeGuess / objectGuess files).
+std::vector<float> read_complex_csv(const std::string& path, size_t& rows, size_t& cols) {
+  std::ifstream f(path);
+  if (!f.is_open()) fail(PTY_ERR_IO, "cannot open " + path);
+  std::vector<float> out;
+  std::string line;
+  rows = 0;
+  cols = 0;
+  while (std::getline(f, line)) {
+    if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
+    size_t n = 0;
+    std::stringstream ls(line);
+    std::string cell;
+    while (std::getline(ls, cell, ',')) {
+      std::string c;
+      for (char ch : cell)
+        if (ch != ' ' && ch != '(' && ch != ')' && ch != '\r') c += ch;
+      if (!c.empty() && (c.back() == 'j' || c.back() == 'i')) c.pop_back();
+      // split at the sign that starts the imaginary part (not an exponent sign, not the leading sign)
+      size_t cut = std::string::npos;
+      for (size_t k = c.size(); k-- > 1;)
+        if ((c[k] == '+' || c[k] == '-') && c[k - 1] != 'e' && c[k - 1] != 'E') {
+          cut = k;
+          break;
+        }
+      float re = 0, im = 0;
+      if (cut == std::string::npos) {
+        re = std::stof(c);
+      } else {
+        re = std::stof(c.substr(0, cut));
+        im = std::stof(c.substr(cut));
+      }
+      out.push_back(re);
+      out.push_back(im);
+      ++n;
+    }
+    if (cols == 0) cols = n;
+    if (n != cols) fail(PTY_ERR_INVALID, "ragged CSV rows in " + path);
+    ++rows;
+  }
+  return out;
+}
+
+// ---------------------------------------------------------------------------- initialisation
+void init_geometry(pty_session* s) {
+  const pty_params& p = s->prm;
+  const double dx_s = sample_pixel_size(p.lambd, p.z, p.dx_d, s->N);
+  if (!s->pos_m.empty()) {
+    s->geo = list_geometry(s->pos_m, dx_s, s->N, p.flipScanAxis != 0);
+  } else {
+    need(p.spiralScan == 0, "spiralScan is not supported by this engine; pass positionNP", PTY_ERR_UNSUPPORTED);
+    need(p.lf[0] == 0, "position list files (lf) are not supported by this engine; pass positionNP",
+         PTY_ERR_UNSUPPORTED);
+    need(p.jitterRadius == 0, "jitterRadius is not supported by this engine", PTY_ERR_UNSUPPORTED);
+    s->geo = cartesian_geometry(p.scanDimsx, p.scanDimsy, p.stepx, p.stepy, dx_s, s->N, p.mirror1stScanAxis != 0,
+                                p.mirror2ndScanAxis != 0, p.flipScanAxis != 0);
+  }
+  s->X = s->geo.X;
+  s->Y = s->geo.Y;
+  s->offs.resize(2 * size_t(s->P));
+  for (int i = 0; i < s->P; ++i) {
+    const float qx = s->geo.pos[2 * i], qy = s->geo.pos[2 * i + 1];
+    // src/ePIE.cpp:100-105 stops the process on a negative position; here it is an error status.
+    need(qx >= 0 && qy >= 0, "scan position " + std::to_string(i) + " is negative: object array too small");
+    const int ox = int(std::round(qx)), oy = int(std::round(qy));
+    need(ox + s->N <= s->X && oy + s->N <= s->Y,
+         "scan position " + std::to_string(i) + " places the probe window outside the object");
+    s->offs[2 * i] = ox;
+    s->offs[2 * i + 1] = oy;
+  }
+}
+
+void init_probe(pty_session* s, const float* avg_dev) {
+  const size_t NN = size_t(s->N) * s->N;
+  s->probe.alloc(sizeof(float2) * NN * s->K, "probe");
+  s->pcache.alloc(sizeof(float) * NN * s->K, "probe cache");
+  check_cuda(cudaMemsetAsync(s->probe.p, 0, s->probe.bytes, s->stream), "memset probe");
+  check_cuda(cudaMemsetAsync(s->pcache.p, 0, s->pcache.bytes, s->stream), "memset probe cache");
+  DeviceBuf d;
+  d.alloc(4 * sizeof(double), "scalars");
+  float pmax = 1.0f;
+  if (s->prm.probeGuess[0]) {
+    size_t r = 0, c = 0;
+    std::vector<float> h = read_complex_csv(s->prm.probeGuess, r, c);
+    need(r == size_t(s->N) && c == size_t(s->N), "probeGuess file is not N x N");
+    check_cuda(cudaMemcpyAsync(s->probe.p, h.data(), sizeof(float2) * NN, cudaMemcpyHostToDevice, s->stream),
+               "H2D probe");
+    check_cuda(cudaStreamSynchronize(s->stream), "sync");
+    // Probe::init file branch ends in updateIntensities() (src/Probe.cpp:344-353)
+    check_cuda(abs2(s->probe.as<float2>(), s->pcache.as<float>(), NN * s->K, s->stream), "abs2");
+    check_cuda(probe_modal_max(s->pcache.as<float>(), s->K, NN, 0, d.as<float>(), s->stream), "modal max");
+    check_cuda(cudaMemcpyAsync(&pmax, d.p, sizeof(float), cudaMemcpyDeviceToHost, s->stream), "D2H");
+  } else if (!s->probe_h.empty()) {
+    check_cuda(cudaMemcpyAsync(s->probe.p, s->probe_h.data(), sizeof(float2) * NN * s->probe_given_modes,
+                               cudaMemcpyHostToDevice, s->stream),
+               "H2D probe");
+    s->modesInitialized = s->probe_given_modes > 1;
+    pmax = 1.0f;  // Probe::m_maxIntensity keeps its constructor value; the intensity cache stays zero
+  } else {
+    // Probe guess (src/Probe.cpp:360-372): sinc*Gaussian, projected onto the mean amplitude, max|P| = 1.
+    const int N = s->N;
+    check_cuda(probe_start(s->probe.as<float2>(), N, float(double(N) / (2 * 2.35)),
+                           float(sample_pixel_size(s->prm.lambd, s->prm.z, s->prm.dx_d, N) / s->prm.beamSize),
+                           s->stream),
+               "probe start");
+    DeviceBuf work;
+    work.alloc(sizeof(float2) * NN, "fft work");
+    check_cuda(fft2(s->probe.as<float2>(), work.as<float2>(), s->tw.as<float2>(), 1, N, false, s->stream), "fft2");
+    check_cuda(modulus_project(s->probe.as<float2>(), avg_dev, int(NN), float(1.0 / double(NN)), s->stream),
+               "modulus");
+    check_cuda(fft2(s->probe.as<float2>(), work.as<float2>(), s->tw.as<float2>(), 1, N, true, s->stream), "ifft2");
+    check_cuda(reduce_abs_max(s->probe.as<float2>(), NN * s->K, d.as<double>(), s->stream), "max");
+    check_cuda(scale_by_inverse(s->probe.as<float2>(), NN * s->K, d.as<double>(), s->stream), "normalize");
+    check_cuda(abs2(s->probe.as<float2>(), s->pcache.as<float>(), NN * s->K, s->stream), "abs2");
+    check_cuda(probe_modal_max(s->pcache.as<float>(), s->K, NN, 0, d.as<float>() + 2, s->stream), "modal max");
+    check_cuda(cudaMemcpyAsync(&pmax, d.as<float>() + 2, sizeof(float), cudaMemcpyDeviceToHost, s->stream), "D2H");
+  }
+  check_cuda(cudaStreamSynchronize(s->stream), "probe init");
+  s->probeMax0 = pmax;
+}
+
+void init_object(pty_session* s) {
+  const size_t XY = size_t(s->X) * s->Y;
+  s->obj.alloc(sizeof(float2) * XY, "object");
+  check_cuda(cudaMemsetAsync(s->obj.p, 0, s->obj.bytes, s->stream), "memset object");
+  if (s->prm.objectGuess[0]) {
+    // Sample::loadGuess centres the guess in the object (h_setObjectArray, src/SampleKernels.cu:620-636)
+    size_t r = 0, c = 0;
+    std::vector<float> h = read_complex_csv(s->prm.objectGuess, r, c);
+    need(r <= size_t(s->X) && c <= size_t(s->Y), "objectGuess is larger than the object array");
+    const size_t offx = s->X / 2 - r / 2, offy = s->Y / 2 - c / 2;
+    check_cuda(cudaMemcpy2DAsync(s->obj.as<float2>() + offx * s->Y + offy, sizeof(float2) * s->Y, h.data(),
+                                 sizeof(float2) * c, sizeof(float2) * c, r, cudaMemcpyHostToDevice, s->stream),
+               "H2D object guess");
+    check_cuda(cudaStreamSynchronize(s->stream), "sync");
+  } else if (!s->obj_h.empty()) {
+    check_cuda(cudaMemcpyAsync(s->obj.p, s->obj_h.data(), sizeof(float2) * XY, cudaMemcpyHostToDevice, s->stream),
+               "H2D object");
+  }
+  s->objMax0 = 0;  // Sample::clearObjectArray (src/Sample.cpp:216-220); loadarr does not touch it
+}
+
+void init_epie(pty_session* s) {
+  auto* ep = new EpieState;
+  s->ep = ep;
+  const size_t NN = size_t(s->N) * s->N, XY = size_t(s->X) * s->Y;
+  check_cuda(epie_prepare(s->N, &ep->C), "ePIE kernel set-up (cluster size)");
+  ep->pos.alloc(sizeof(float2) * s->P, "positions");
+  check_cuda(cudaMemcpyAsync(ep->pos.p, s->geo.pos.data(), sizeof(float2) * s->P, cudaMemcpyHostToDevice, s->stream),
+             "H2D positions");
+  ep->order.alloc(sizeof(int) * s->P, "order");
+  check_cuda(cudaMallocHost(&ep->order_h, sizeof(int) * s->P), "pinned order");
+  ep->W1.alloc(sizeof(float2) * NN * s->K, "W1");
+  ep->W2.alloc(sizeof(float2) * NN * s->K, "W2");
+  ep->TX = (s->X + 15) / 16;
+  ep->TY = (s->Y + 15) / 16;
+  ep->TM.alloc(sizeof(float) * ep->TX * ep->TY, "tile maxima");
+  ep->pm.alloc(sizeof(float) * 16, "partial maxima");
+  ep->sc.alloc(sizeof(EpieScalars), "scalars");
+  ep->ip.alloc(4 * sizeof(double), "inner products");
+  s->ocache.alloc(sizeof(float) * XY, "object cache");
+  check_cuda(cudaMemsetAsync(s->ocache.p, 0, s->ocache.bytes, s->stream), "memset cache");
+  EpieScalars sc{float(s->objMax0), float(s->probeMax0), 0.0};
+  check_cuda(cudaMemcpyAsync(ep->sc.p, &sc, sizeof(sc), cudaMemcpyHostToDevice, s->stream), "H2D scalars");
+  ep->sq.alloc(sizeof(double) * s->P, "pattern sums");
+  std::vector<double> ones(s->P, 1.0);
+  if (s->prm.calculateRMS) {
+    check_cuda(plane_sums(s->amp.as<float>(), s->P, NN, ep->sq.as<double>(), s->stream), "pattern sums");
+  } else {
+    check_cuda(cudaMemcpyAsync(ep->sq.p, ones.data(), sizeof(double) * s->P, cudaMemcpyHostToDevice, s->stream),
+               "H2D sums");
+  }
+  check_cuda(cudaStreamSynchronize(s->stream), "ePIE init");
+}
+
+void init_dm(pty_session* s) {
+  const size_t NN = size_t(s->N) * s->N, XY = size_t(s->X) * s->Y;
+  s->psi.alloc(sizeof(float2) * NN * s->P, "DM exit waves");
+  check_cuda(cudaMemsetAsync(s->psi.p, 0, s->psi.bytes, s->stream), "memset psi");
+  s->dO.alloc(sizeof(float2) * XY, "dO");
+  check_cuda(cudaMemsetAsync(s->dO.p, 0, s->dO.bytes, s->stream), "memset dO");
+  s->dP.alloc(sizeof(float2) * NN, "dP");
+  check_cuda(cudaMemsetAsync(s->dP.p, 0, s->dP.bytes, s->stream), "memset dP");
+  // wave: patterns per pipeline pass; W1+W2 = 2 * wave * 8N^2 bytes, kept to ~64 MB so both stay in L2
+  int wave = s->prm.wave;
+  if (wave <= 0) wave = int(std::max<size_t>(1, (size_t(32) << 20) / (sizeof(float2) * NN)));
+  wave = std::min(wave, s->P);
+  s->wave = wave;
+  s->nwaves = (s->P + wave - 1) / wave;
+  s->W1.alloc(sizeof(float2) * NN * wave, "W1");
+  s->W2.alloc(sizeof(float2) * NN * wave, "W2");
+  std::vector<int> slots(s->P);
+  for (int i = 0; i < s->P; ++i) slots[i] = i;
+  s->slots.alloc(sizeof(int) * s->P, "slots");
+  check_cuda(cudaMemcpyAsync(s->slots.p, slots.data(), sizeof(int) * s->P, cudaMemcpyHostToDevice, s->stream),
+             "H2D slots");
+  s->scal.alloc(8 * sizeof(double), "DM scalars");
+  const double h[8] = {0, 0, 1.0 / s->objMax0, 1.0 / s->probeMax0, s->objMax0, s->probeMax0, 0, 0};
+  check_cuda(cudaMemcpyAsync(s->scal.p, h, sizeof(h), cudaMemcpyHostToDevice, s->stream), "H2D DM scalars");
+  check_cuda(dm_prepare(s->N), "DM kernel set-up");
+  check_cuda(cudaStreamSynchronize(s->stream), "DM init");
+}
+
+DMBuffers dm_buffers(pty_session* s) {
+  DMBuffers b;
+  b.psi = s->psi.as<float2>();
+  b.ampT = s->amp.as<float>();
+  b.obj = s->obj.as<float2>();
+  b.probe = s->probe.as<float2>();
+  b.dO = s->dO.as<float2>();
+  b.dP = s->dP.as<float2>();
+  b.W1 = s->W1.as<float2>();
+  b.W2 = s->W2.as<float2>();
+  b.offs = s->dOffs.as<int2>();
+  b.tw = s->tw.as<float2>();
+  b.sums = s->scal.as<double>();
+  b.fac = s->scal.as<double>() + 2;
+  b.N = s->N;
+  b.K = s->K;
+  b.X = s->X;
+  b.Y = s->Y;
+  return b;
+}
+
+// One DM iteration: waves of (fwd_rows, cols, inv_rows) then finalize, replayed from a CUDA graph per flag state.
+void step_dm(pty_session* s, int it) {
+  const bool pc = it <= s->prm.phaseConstraint, up = it >= s->prm.updateProbe;
+  const int gi = (pc ? 1 : 0) | (up ? 2 : 0);
+  if (!s->graphs[gi]) {
+    const DMBuffers b = dm_buffers(s);
+    cudaGraph_t graph = nullptr;
+    check_cuda(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t err = cudaSuccess;
+    for (int w = 0; w < s->nwaves && err == cudaSuccess; ++w) {
+      DMWave wv;
+      wv.slot_pat = s->slots.as<int>() + size_t(w) * s->wave;
+      wv.count = std::min(s->wave, s->P - w * s->wave);
+      err = dm_wave(b, wv, pc, up, s->stream, nullptr);
+    }
+    if (err == cudaSuccess) err = dm_finalize(b, up, s->stream, nullptr);
+    cudaError_t e2 = cudaStreamEndCapture(s->stream, &graph);
+    check_cuda(err, "DM capture");
+    check_cuda(e2, "end capture");
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e3 = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    check_cuda(e3, "graph instantiate");
+    s->graphs[gi] = exec;
+  }
+  check_cuda(cudaGraphLaunch(s->graphs[gi], s->stream), "DM graph launch");
+  s->launches += 3 * int64_t(s->nwaves) + 2;
+}
+
+// One ePIE iteration: the modal switch on the host side (beginModalReconstruction), then the persistent kernel.
+double step_epie(pty_session* s, int it, bool want_err) {
+  EpieState* ep = s->ep;
+  const bool pc = it <= s->prm.phaseConstraint, up = it >= s->prm.updateProbe, um = it >= s->prm.updateModes;
+  const size_t NN = size_t(s->N) * s->N;
+  DeviceBuf tmp;
+  if (um) {
+    s->useAll = true;
+    if (!s->modesInitialized) {  // initProbeModes (src/Probe.cpp:320-330)
+      if (s->K > 1) {
+        if (!ep->modesCopy.p) ep->modesCopy.alloc(sizeof(float2) * NN * s->K, "modes copy");
+        check_cuda(epie_init_modes(s->probe.as<float2>(), s->pcache.as<float>(), s->K, s->N,
+                                   ep->modesCopy.as<float2>(), ep->ip.as<double>(), s->stream),
+                   "mode init");
+        s->modesInitialized = true;
+        s->launches += 1 + 2 * (s->K * (s->K - 1) / 2);
+      }
+      // updateMaxIntensity(): probeMax = modal max of the cache
+      check_cuda(probe_modal_max(s->pcache.as<float>(), s->K, NN, 1, &reinterpret_cast<EpieScalars*>(ep->sc.p)->probeMax,
+                                 s->stream),
+                 "modal max");
+      s->launches += 1;
+    }
+  }
+  const int Ka = s->useAll ? s->K : 1;
+  std::vector<int> order;
+  visiting_order(s->rng, s->P, order);
+  check_cuda(cudaStreamSynchronize(s->stream), "order buffer reuse");
+  std::memcpy(ep->order_h, order.data(), sizeof(int) * s->P);
+  check_cuda(cudaMemcpyAsync(ep->order.p, ep->order_h, sizeof(int) * s->P, cudaMemcpyHostToDevice, s->stream),
+             "H2D order");
+  if (up && !ep->tm_valid) {
+    check_cuda(tile_max_all(s->ocache.as<float>(), s->X, s->Y, ep->TM.as<float>(), ep->TX, ep->TY, s->stream),
+               "tile maxima");
+    s->launches += 1;
+  }
+  ep->tm_valid = up;
+  check_cuda(cudaMemsetAsync(&reinterpret_cast<EpieScalars*>(ep->sc.p)->err, 0, sizeof(double), s->stream), "memset");
+  EpieArgs g;
+  g.ampT = s->amp.as<float>();
+  g.obj = s->obj.as<float2>();
+  g.ocache = s->ocache.as<float>();
+  g.probe = s->probe.as<float2>();
+  g.pcache = s->pcache.as<float>();
+  g.pos = ep->pos.as<float2>();
+  g.order = ep->order.as<int>();
+  g.W1 = ep->W1.as<float2>();
+  g.W2 = ep->W2.as<float2>();
+  g.TM = ep->TM.as<float>();
+  g.pm = ep->pm.as<float>();
+  g.sc = ep->sc.as<EpieScalars>();
+  g.tw = s->tw.as<float2>();
+  g.sqsum = ep->sq.as<double>();
+  g.saturation = s->prm.threshold > 0 || s->prm.sqrtData
+                     ? float(s->prm.sqrtData ? std::sqrt(4294967295.0 - s->prm.threshold)
+                                             : 4294967295.0 - s->prm.threshold)
+                     : std::numeric_limits<float>::infinity();
+  g.N = s->N;
+  g.K = s->K;
+  g.Ka = Ka;
+  g.P = s->P;
+  g.X = s->X;
+  g.Y = s->Y;
+  g.TX = ep->TX;
+  g.TY = ep->TY;
+  g.C = ep->C;
+  g.pc = pc;
+  g.up = up;
+  g.rms = s->prm.calculateRMS ? 1 : 0;
+  g.useAll = s->useAll ? 1 : 0;
+  check_cuda(epie_launch(g, s->stream), "ePIE kernel launch");
+  s->launches += 1;
+  if (!want_err || !s->prm.calculateRMS) return 0.0;
+  double e = 0;
+  check_cuda(cudaMemcpyAsync(&e, &reinterpret_cast<EpieScalars*>(ep->sc.p)->err, sizeof(double),
+                             cudaMemcpyDeviceToHost, s->stream),
+             "D2H error");
+  check_cuda(cudaStreamSynchronize(s->stream), "ePIE iteration");
+  return e / s->P;
+}
+
+void destroy_session(pty_session* s) {
+  if (!s) return;
+  cudaSetDevice(s->dev);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (auto& g : s->graphs)
+    if (g) cudaGraphExecDestroy(g);
+  delete s->ep;
+  s->ep = nullptr;
+  s->amp.free();
+  s->obj.free();
+  s->probe.free();
+  s->ocache.free();
+  s->pcache.free();
+  s->tw.free();
+  s->dOffs.free();
+  s->scal.free();
+  s->psi.free();
+  s->dO.free();
+  s->dP.free();
+  s->W1.free();
+  s->W2.free();
+  s->slots.free();
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+}  // namespace
+
+// ============================================================================== C ABI
+extern "C" {
+
+int pty_params_init(pty_params* p) {
+  if (!p) return PTY_ERR_INVALID;
+  std::memset(p, 0, sizeof(*p));
+  std::strcpy(p->algorithm, "ePIE");
+  p->fs = 0;
+  p->dpf = 1;
+  p->beamSize = 400e-9;
+  p->size = 512;
+  p->qx = 128;
+  p->qy = 128;
+  p->nx = 256;
+  p->ny = 256;
+  p->scanDimsx = 26;
+  p->scanDimsy = 26;
+  p->stepx = 40e-9;
+  p->stepy = 40e-9;
+  p->probeModes = 1;
+  p->lambd = 2.3843e-10;
+  p->dx_d = 172e-6;
+  p->z = 2.2;
+  p->iter = 100;
+  p->T = 0;
+  p->jitterRadius = 0;
+  p->delta_p = 0.1;
+  p->phaseConstraint = 1;
+  p->updateProbe = 10;
+  p->updateModes = 20;
+  p->PPS = 20;
+  p->seed = 0x5EED5EEDull;
+  p->calculateRMS = 0;
+  p->device = 0;
+  p->wave = 0;
+  return PTY_OK;
+}
+
+int pty_session_create(const pty_params* p, pty_session** out) {
+  if (!out) return PTY_ERR_INVALID;
+  *out = nullptr;
+  pty_session* s = nullptr;
+  int rc = guarded([&] {
+    need(p != nullptr, "null parameters");
+    s = new pty_session;
+    s->prm = *p;
+    s->algo = parse_algo(p->algorithm);
+    need(p->size > 16, "size must be larger than 16");  // src/Parameters.cpp:512-519
+    need(p->probeModes >= 1, "probeModes must be >= 1");
+    need(p->scanDimsx > 0 && p->scanDimsy > 0, "scanDimsx and scanDimsy must be positive");
+    need(p->lambd > 0 && p->z > 0 && p->dx_d > 0 && p->beamSize > 0, "lambd, z, dx_d, beamSize must be positive");
+    need(p->fp[0] == 0, "file ingest (fp) is not part of this engine; pass diffractionNP", PTY_ERR_UNSUPPORTED);
+    need(p->simulate == 0, "simulate mode is not part of this engine", PTY_ERR_UNSUPPORTED);
+    need(p->beamstopMask == 0, "beamstop masks from files are not part of this engine", PTY_ERR_UNSUPPORTED);
+    s->N = p->size;
+    s->K = p->probeModes;
+    s->rng = p->seed;
+    int ndev = 0;
+    check_cuda(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    need(p->device >= 0 && p->device < ndev, "device ordinal out of range");
+    s->dev = p->device;
+    set_device(s);
+    check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+    s->own_stream = true;
+  });
+  if (rc != PTY_OK) {
+    destroy_session(s);
+    return rc;
+  }
+  *out = s;
+  return PTY_OK;
+}
+
+int pty_session_destroy(pty_session* s) {
+  return guarded([&] { destroy_session(s); });
+}
+
+int pty_set_patterns(pty_session* s, const void* host, int dtype, int P, int N) {
+  return guarded([&] {
+    need(s && host, "null argument");
+    need(!s->initialized, "patterns must be set before pty_init", PTY_ERR_STATE);
+    need(dtype == PTY_F32 || dtype == PTY_F64, "dtype must be PTY_F32 or PTY_F64");
+    need(N == s->N, "pattern size " + std::to_string(N) + " differs from size=" + std::to_string(s->N));
+    need(fft_size_supported(N), "pattern size must be 32, 64, 128, 256 or 512");
+    need(P >= 1, "need at least one pattern");
+    set_device(s);
+    s->P = P;
+    upload_patterns(s, host, dtype, size_t(P) * N * N);
+    check_cuda(cudaStreamSynchronize(s->stream), "patterns");
+    s->have_patterns = true;
+  });
+}
+
+int pty_set_positions(pty_session* s, const double* xy_m, int P) {
+  return guarded([&] {
+    need(s && xy_m, "null argument");
+    need(!s->initialized, "positions must be set before pty_init", PTY_ERR_STATE);
+    need(P >= 1, "need at least one position");
+    s->pos_m.assign(xy_m, xy_m + 2 * size_t(P));
+  });
+}
+
+int pty_set_object(pty_session* s, const float* c64, int X, int Y) {
+  return guarded([&] {
+    need(s && c64, "null argument");
+    need(!s->initialized, "object must be set before pty_init", PTY_ERR_STATE);
+    need(X > 0 && Y > 0, "bad object shape");
+    s->obj_h.assign(c64, c64 + 2 * size_t(X) * Y);
+    s->X = X;
+    s->Y = Y;
+  });
+}
+
+int pty_set_probe(pty_session* s, const float* c64, int K, int N) {
+  return guarded([&] {
+    need(s && c64, "null argument");
+    need(!s->initialized, "probe must be set before pty_init", PTY_ERR_STATE);
+    need(N == s->N, "probe size differs from size");
+    need(K >= 1 && K <= s->K, "probe has more modes than probeModes");
+    s->probe_h.assign(c64, c64 + 2 * size_t(K) * N * N);
+    s->probe_given_modes = K;
+  });
+}
+
+int pty_init(pty_session* s) {
+  return guarded([&] {
+    need(s != nullptr, "null session");
+    need(!s->initialized, "session already initialised", PTY_ERR_STATE);
+    need(s->have_patterns, "no diffraction patterns (diffractionNP) were given", PTY_ERR_STATE);
+    need(s->algo != ALGO_MLS, "MLs is not available in this build", PTY_ERR_UNSUPPORTED);
+    set_device(s);
+    const pty_params& p = s->prm;
+    if (s->pos_m.empty())
+      need(s->P == p.scanDimsx * p.scanDimsy,
+           "pattern count " + std::to_string(s->P) + " differs from scanDimsx*scanDimsy = " +
+               std::to_string(p.scanDimsx * p.scanDimsy));
+    else
+      need(int(s->pos_m.size() / 2) == s->P, "positionNP and diffractionNP have different lengths");
+    const int gX = s->X, gY = s->Y;
+    init_geometry(s);
+    if (!s->obj_h.empty())
+      need(gX == s->X && gY == s->Y, "objectNP shape (" + std::to_string(gX) + ", " + std::to_string(gY) +
+                                         ") differs from the scan's object size (" + std::to_string(s->X) + ", " +
+                                         std::to_string(s->Y) + ")");
+    float2* twp = nullptr;
+    check_cuda(make_twiddles(s->N, &twp, s->stream), "twiddles");
+    s->tw.p = twp;
+    s->tw.bytes = sizeof(float2) * s->N;
+    s->dOffs.alloc(sizeof(int) * 2 * s->P, "offsets");
+    check_cuda(cudaMemcpyAsync(s->dOffs.p, s->offs.data(), sizeof(int) * 2 * s->P, cudaMemcpyHostToDevice, s->stream),
+               "H2D offsets");
+    const size_t NN = size_t(s->N) * s->N;
+    {
+      DeviceBuf avg;
+      if (p.probeGuess[0] == 0 && s->probe_h.empty()) {
+        avg.alloc(sizeof(float) * NN, "mean amplitude");
+        check_cuda(mean_amplitude(s->amp.as<float>(), s->P, s->N, avg.as<float>(), s->stream), "mean amplitude");
+      }
+      init_probe(s, avg.as<float>());
+    }
+    init_object(s);
+    // amplitudes are consumed column-wise by the column phase: transpose each plane once
+    {
+      DeviceBuf t;
+      t.alloc(s->amp.bytes, "transposed patterns");
+      check_cuda(transpose_planes(s->amp.as<float>(), t.as<float>(), s->P, s->N, s->stream), "transpose");
+      check_cuda(cudaStreamSynchronize(s->stream), "transpose");
+      std::swap(s->amp.p, t.p);
+      std::swap(s->amp.bytes, t.bytes);
+    }
+    if (s->algo == ALGO_EPIE)
+      init_epie(s);
+    else
+      init_dm(s);
+    s->initialized = true;
+  });
+}
+
+int pty_step(pty_session* s, double* err) {
+  return guarded([&] {
+    need(s && s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    set_device(s);
+    const int it = s->iter + 1;
+    double e = 0;
+    if (s->algo == ALGO_EPIE)
+      e = step_epie(s, it, err != nullptr);
+    else
+      step_dm(s, it);
+    s->iter = it;
+    if (err) *err = e;
+  });
+}
+
+int pty_run(pty_session* s, int iters, double* errs) {
+  return guarded([&] {
+    need(s && s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    need(iters >= 0, "negative iteration count");
+    set_device(s);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int i = 0; i < iters; ++i) {
+      const int it = s->iter + 1;
+      double e = 0;
+      if (s->algo == ALGO_EPIE)
+        e = step_epie(s, it, errs != nullptr);
+      else
+        step_dm(s, it);
+      s->iter = it;
+      if (errs) errs[i] = e;
+      if (s->prm.T > 0) {  // wall-time limit (src/IPhaser.cpp:386-387)
+        check_cuda(cudaStreamSynchronize(s->stream), "iteration");
+        if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >= s->prm.T) break;
+      }
+    }
+    check_cuda(cudaStreamSynchronize(s->stream), "pty_run");
+  });
+}
+
+int pty_get_dims(const pty_session* s, int* X, int* Y, int* K, int* N, int* P, int* iters_done) {
+  if (!s) return PTY_ERR_INVALID;
+  if (X) *X = s->X;
+  if (Y) *Y = s->Y;
+  if (K) *K = s->K;
+  if (N) *N = s->N;
+  if (P) *P = s->P;
+  if (iters_done) *iters_done = s->iter;
+  return PTY_OK;
+}
+
+int pty_get_object(pty_session* s, float* out, int X, int Y) {
+  return guarded([&] {
+    need(s && out, "null argument");
+    need(s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    need(X == s->X && Y == s->Y, "object buffer shape mismatch");
+    set_device(s);
+    check_cuda(cudaMemcpyAsync(out, s->obj.p, sizeof(float2) * size_t(X) * Y, cudaMemcpyDeviceToHost, s->stream),
+               "D2H object");
+    check_cuda(cudaStreamSynchronize(s->stream), "D2H object");
+  });
+}
+
+int pty_get_probe(pty_session* s, float* out, int K, int N) {
+  return guarded([&] {
+    need(s && out, "null argument");
+    need(s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    need(K == s->K && N == s->N, "probe buffer shape mismatch");
+    set_device(s);
+    check_cuda(cudaMemcpyAsync(out, s->probe.p, sizeof(float2) * size_t(K) * N * N, cudaMemcpyDeviceToHost,
+                               s->stream),
+               "D2H probe");
+    check_cuda(cudaStreamSynchronize(s->stream), "D2H probe");
+  });
+}
+
+int pty_get_positions(const pty_session* s, float* xy_px, int P) {
+  return guarded([&] {
+    need(s && xy_px, "null argument");
+    need(s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    need(P == s->P, "position buffer length mismatch");
+    std::memcpy(xy_px, s->geo.pos.data(), sizeof(float) * 2 * size_t(P));
+  });
+}
+
+int pty_write_results(pty_session* s, const char* dir, int r, int binary) {
+  return guarded([&] {
+    need(s && dir, "null argument");
+    need(s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    set_device(s);
+    std::vector<float> pr(2 * size_t(s->K) * s->N * s->N), ob(2 * size_t(s->X) * s->Y);
+    check_cuda(cudaMemcpyAsync(pr.data(), s->probe.p, pr.size() * sizeof(float), cudaMemcpyDeviceToHost, s->stream),
+               "D2H");
+    check_cuda(cudaMemcpyAsync(ob.data(), s->obj.p, ob.size() * sizeof(float), cudaMemcpyDeviceToHost, s->stream),
+               "D2H");
+    check_cuda(cudaStreamSynchronize(s->stream), "D2H results");
+    const std::string ext = binary ? "bin" : "csv";
+    const std::string base = std::string(dir) + "/" + s->prm.jobID;
+    write_complex_file(base + "_probes_" + std::to_string(r) + "." + ext, pr.data(), size_t(s->K) * s->N, s->N,
+                       binary != 0);
+    write_complex_file(base + "_object_" + std::to_string(r) + "." + ext, ob.data(), s->X, s->Y, binary != 0);
+  });
+}
+
+int pty_set_stream(pty_session* s, void* st) {
+  return guarded([&] {
+    need(s != nullptr, "null session");
+    set_device(s);
+    check_cuda(cudaStreamSynchronize(s->stream), "stream switch");
+    for (auto& g : s->graphs) {
+      if (g) cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+    if (st) {
+      if (s->own_stream) cudaStreamDestroy(s->stream);
+      s->stream = static_cast<cudaStream_t>(st);
+      s->own_stream = false;
+    } else if (!s->own_stream) {
+      check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+      s->own_stream = true;
+    }
+  });
+}
+
+int64_t pty_kernel_launches(const pty_session* s) { return s ? s->launches : -1; }
+
+const char* pty_last_error(void) { return g_last_error.c_str(); }
+
+int pty_fft2_dev(void* data_dev, void* work_dev, int batch, int N, int inverse, void* st) {
+  return guarded([&] {
+    need(data_dev && work_dev && batch >= 1, "bad argument");
+    need(fft_size_supported(N), "unsupported FFT size");
+    cudaStream_t stream = static_cast<cudaStream_t>(st);
+    float2* tw = nullptr;
+    check_cuda(make_twiddles(N, &tw, stream), "twiddles");
+    cudaError_t e = fft2(static_cast<float2*>(data_dev), static_cast<float2*>(work_dev), tw, batch, N, inverse != 0,
+                         stream);
+    cudaError_t e2 = cudaStreamSynchronize(stream);
+    cudaFree(tw);
+    check_cuda(e, "fft2");
+    check_cuda(e2, "fft2 sync");
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+// Host-side session state of one reconstruction (the engine's counterpart of the reference's IPhaser with its
+// Sample, Probe, Diffractions and scan-mesh members, src/IPhaser.h:58-115), owned through the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ptychopy_b200.h"
+
+namespace pty {
+
+enum Algo { ALGO_EPIE = 0, ALGO_DM = 1, ALGO_MLS = 2 };
+
+// Thrown inside the library and turned into a status code + message at the C boundary.
+struct Error {
+  int code;
+  std::string msg;
+};
+
+[[noreturn]] void fail(int code, const std::string& msg);
+void check_cuda(cudaError_t e, const char* what);
+
+// Scan geometry in pixels (IPtychoScanMesh): positions shifted by -min, object size ceil(max - min + N).
+struct Geometry {
+  std::vector<float> pos;  // 2*P (x = row, y = column)
+  int X = 0, Y = 0;
+};
+double sample_pixel_size(double lambda, double z, double dx_d, int N);
+Geometry cartesian_geometry(int nx, int ny, double stepx, double stepy, double dx_s, int N, bool mirrorX,
+                            bool mirrorY, bool flip);
+Geometry list_geometry(const std::vector<double>& xy_m, double dx_s, int N, bool flip);
+
+// SplitMix64 stream and the ePIE visiting order (pick `next % remaining`, erase; src/ePIE.cpp:93-97).
+uint64_t splitmix64(uint64_t& state);
+void visiting_order(uint64_t& state, int P, std::vector<int>& order);
+
+struct DeviceBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void alloc(size_t n, const char* what);
+  void free();
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+  ~DeviceBuf() { free(); }
+};
+
+struct EpieState;  // device state of the persistent ePIE kernel (kernels_epie.cu)
+
+}  // namespace pty
+
+struct pty_session {
+  pty_params prm{};
+  pty::Algo algo = pty::ALGO_EPIE;
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int N = 0, K = 1, P = 0, X = 0, Y = 0;
+  int iter = 0;
+  bool initialized = false;
+  int64_t launches = 0;
+
+  // inputs
+  bool have_patterns = false;
+  std::vector<double> pos_m;  // positions in metres (positionNP) or empty
+  std::vector<float> obj_h;   // objectNP (X*Y complex) or empty
+  std::vector<float> probe_h; // probeNP (Kg*N*N complex) or empty
+  int probe_given_modes = 0;
+
+  // geometry
+  pty::Geometry geo;
+  std::vector<int> offs;  // rounded offsets, 2*P
+
+  // device state
+  pty::DeviceBuf amp;    // P*N*N float (natural layout; DM keeps it transposed per plane)
+  pty::DeviceBuf obj, probe, ocache, pcache;
+  pty::DeviceBuf tw, dOffs, scal;
+  // DM
+  pty::DeviceBuf psi, dO, dP, W1, W2, slots;
+  int wave = 0, nwaves = 0;
+  cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
+  // ePIE
+  pty::EpieState* ep = nullptr;
+  uint64_t rng = 0;
+  double objMax0 = 0, probeMax0 = 1;
+  bool useAll = false, modesInitialized = false;
+  std::vector<double> sqsum;
+};

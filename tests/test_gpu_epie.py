@@ -1,0 +1,88 @@
+"""The persistent ePIE kernel against the FP64 oracle: same seeded visiting order, same update schedule."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from gpu_helpers import dataset, gpu_session
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+@pytest.mark.parametrize("N,nx", [(64, 5), (128, 4), (32, 6), (256, 3)])
+def test_epie_matches_oracle(oracle, N, nx):
+    d = dataset(N=N, nx=nx)
+    s = gpu_session(d, probe=d["probe"], updateProbe=2, calculateRMS=1, seed=77)
+    o = oracle.OracleSession("ePIE", d["amp"], d["pos"], np.zeros((d["X"], d["Y"])), d["probe"],
+                             probe_guess_path=False, updateProbe=2, calculateRMS=1, seed=77)
+    for it in range(1, 5):
+        eg = s.step()
+        eo = o.step()
+        ob, pr, _ = o.state()
+        assert rel_err(s.object(), ob) < TOL, f"object, iteration {it}"
+        assert rel_err(s.probe(), pr) < TOL, f"probe, iteration {it}"
+        assert abs(eg - eo) <= 1e-6 * max(abs(eo), 1e-12) + 1e-7, f"error metric, iteration {it}"
+
+
+def test_epie_probe_guess(oracle):
+    d = dataset(N=64, nx=5)
+    s = gpu_session(d, updateProbe=1, seed=3)
+    g = oracle.probe_guess(d["amp"], d["kw"]["beamSize"], d["dx_s"], K=1)
+    assert rel_err(s.probe(), g) < 1e-5
+    o = oracle.OracleSession("ePIE", d["amp"], d["pos"], np.zeros((d["X"], d["Y"])), g, probe_guess_path=True,
+                             updateProbe=1, seed=3)
+    for _ in range(3):
+        s.step()
+        o.step()
+    ob, pr, _ = o.state()
+    assert rel_err(s.object(), ob) < TOL and rel_err(s.probe(), pr) < TOL
+
+
+def test_epie_given_modes(oracle):
+    # probeNP with K modes (extension): single-mode iterations until updateModes, modal afterwards
+    d = dataset(N=64, nx=5, K=3)
+    s = gpu_session(d, probe=d["probe"], updateProbe=2, updateModes=3, calculateRMS=1, seed=9)
+    o = oracle.OracleSession("ePIE", d["amp"], d["pos"], np.zeros((d["X"], d["Y"])), d["probe"],
+                             probe_guess_path=False, modes_given=True, updateProbe=2, updateModes=3,
+                             calculateRMS=1, seed=9)
+    for it in range(1, 6):
+        s.step()
+        o.step()
+    ob, pr, _ = o.state()
+    assert rel_err(s.object(), ob) < TOL and rel_err(s.probe(), pr) < TOL
+
+
+def test_epie_mode_initialisation(oracle):
+    # modes created at updateModes from 0.05 * P0 and Gram-Schmidt: mode 0 and the object stay at parity
+    # (the extra modes start at round-off level, so they are compared loosely)
+    d = dataset(N=64, nx=5, K=2)
+    p0 = d["probe"][:1]
+    s = gpu_session(d, probe=p0, updateProbe=2, updateModes=2, seed=5)
+    o = oracle.OracleSession("ePIE", d["amp"], d["pos"], np.zeros((d["X"], d["Y"])),
+                             np.concatenate([p0, np.zeros_like(p0)]), probe_guess_path=False, updateProbe=2,
+                             updateModes=2, seed=5)
+    for _ in range(3):
+        s.step()
+        o.step()
+    ob, pr, _ = o.state()
+    assert rel_err(s.probe()[0], pr[0]) < 1e-3
+    assert rel_err(s.object(), ob) < 1e-3
+
+
+def test_epie_negative_position_is_an_error():
+    from ptychopy_b200 import abi
+
+    d = dataset(N=32, nx=3)
+    s = abi.Session(**d["kw"])
+    s.set_patterns(d["amp"])
+    xy = np.zeros((9, 2))
+    xy[:, 0] = np.arange(9) * 1e-8
+    s.set_positions(xy)
+    # list positions are shifted by their minimum, so they are valid; a too-small object is rejected instead
+    s.init()
+    s.close()
+    s2 = abi.Session(**d["kw"])
+    s2.set_patterns(d["amp"])
+    s2.set_object(np.ones((10, 10), np.complex64))
+    with pytest.raises(abi.PtyError):
+        s2.init()

@@ -1,0 +1,149 @@
+"""The oracle against numpy.fft, hand-derived known answers and the reference's geometry (CPU only)."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+
+@pytest.mark.parametrize("N", [8, 32, 64, 128])
+def test_fft_matches_numpy(oracle, N):
+    rng = np.random.default_rng(N)
+    a = rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))
+    assert rel_err(oracle.fft2(a), np.fft.fft2(a)) < 1e-13
+    assert rel_err(oracle.fft2(a, inverse=True), np.fft.ifft2(a) * N * N) < 1e-13
+
+
+def test_fft_known_answers(oracle):
+    N = 16
+    d = np.zeros((N, N), complex)
+    d[0, 0] = 1
+    assert np.allclose(oracle.fft2(d), 1.0)  # delta -> flat
+    x = np.arange(N)
+    pw = np.exp(2j * np.pi * (3 * x[:, None] + 5 * x[None, :]) / N)  # plane wave -> single bin (3, 5)
+    F = oracle.fft2(pw)
+    assert abs(F[3, 5] - N * N) < 1e-9 and np.abs(np.delete(F.ravel(), 3 * N + 5)).max() < 1e-9
+
+
+# object sizes and raster steps of the configurations (dx_s = lambda*z/(N*dx_d), object ceil(extent + N))
+@pytest.mark.parametrize("nx,step,lam,z,dxd,N,X,step_px", [
+    (10, 50e-9, 2.48e-10, 1.0, 172e-6, 128, 168, 4.4386),
+    (30, 50e-9, 2.48e-10, 1.0, 172e-6, 512, 1027, 17.7548),
+    (51, 100e-9, 1.409e-10, 1.92, 75e-6, 256, 611, 7.0972),
+    (64, 50e-9, 2.48e-10, 1.0, 172e-6, 128, 408, 4.4386),
+])
+def test_geometry_configs(oracle, nx, step, lam, z, dxd, N, X, step_px):
+    pos, gx, gy = oracle.cartesian_mesh(nx, nx, step, step, lam, z, dxd, N)
+    assert (gx, gy) == (X, X)
+    assert pos.min() == 0.0
+    assert abs(pos[1, 1] - pos[0, 1] - step_px) < 1e-3
+    assert abs(pos[nx, 0] - pos[0, 0] - step_px) < 1e-3
+
+
+def test_geometry_matches_synth(oracle):
+    from ptychopy_b200 import synth
+
+    dx_s = synth.sample_pixel(2.48e-10, 1.0, 172e-6, 128)
+    assert dx_s == oracle.sample_pixel(2.48e-10, 1.0, 172e-6, 128)
+    p1, X1, Y1 = synth.raster_positions(10, 7, 50e-9, 60e-9, dx_s, 128)
+    p2, X2, Y2 = oracle.cartesian_mesh(10, 7, 50e-9, 60e-9, 2.48e-10, 1.0, 172e-6, 128)
+    assert (X1, Y1) == (X2, Y2)
+    assert np.array_equal(p1, p2)
+
+
+def test_list_mesh_zero_padding(oracle):
+    # positions all > 0: the (0,0) padding entries of the 1024-wide list mesh join the min (P % 1024 != 0)
+    xy = np.array([[1e-6, 2e-6], [1.5e-6, 2.5e-6]])
+    pos, X, Y = oracle.list_mesh(xy, 2.48e-10, 1.0, 172e-6, 128)
+    dx_s = oracle.sample_pixel(2.48e-10, 1.0, 172e-6, 128)
+    assert abs(pos[0, 0] - 1e-6 / dx_s) < 1e-2
+    assert X == int(np.ceil(np.float32(1.5e-6 / dx_s) + 128))
+
+
+def test_patch_integer_and_half_offsets(oracle):
+    rng = np.random.default_rng(1)
+    O = rng.standard_normal((20, 24)) + 1j * rng.standard_normal((20, 24))
+    p = oracle.extract_patch(O, 3.0, 5.0, 8)
+    assert np.allclose(p, O[3:11, 5:13])
+    h = oracle.extract_patch(O, 3.0, 5.5, 8)  # weight exactly 1/2 between columns
+    assert np.allclose(h, 0.5 * (O[3:11, 5:13] + O[3:11, 6:14]))
+
+
+def test_patch_weights_quantised(oracle):
+    O = np.zeros((10, 10), complex)
+    O[:, 5] = 1.0
+    p = oracle.extract_patch(O, 0.0, 4.3, 4)  # fraction 0.3 -> round(0.3*256)/256 = 77/256
+    assert abs(p[0, 0].real - 77 / 256) < 1e-12
+
+
+def test_visiting_order_is_a_permutation(oracle):
+    order, s2 = oracle.visiting_order(1234, 50)
+    assert sorted(order.tolist()) == list(range(50))
+    order2, _ = oracle.visiting_order(s2, 50)
+    assert not np.array_equal(order, order2)
+    again, _ = oracle.visiting_order(1234, 50)
+    assert np.array_equal(order, again)
+
+
+def _toy(N=16, nx=3, seed=0, K=1):
+    from ptychopy_b200 import synth
+
+    rng = np.random.default_rng(seed)
+    dx_s = synth.sample_pixel(2.48e-10, 1.0, 172e-6, N)
+    pos, X, Y = synth.raster_positions(nx, nx, 30e-9, 30e-9, dx_s, N)
+    obj = synth.make_object(X, Y, rng, corr_px=3.0)
+    probe = synth.make_probe(N, dx_s, K=K, fwhm=8 * dx_s)
+    return pos, X, Y, obj, probe
+
+
+def test_epie_fixed_point(oracle):
+    # amplitudes generated from the current object and probe: the modulus projection is the identity and an
+    # iteration leaves object and probe unchanged
+    N = 16
+    pos, X, Y, obj, probe = _toy(N)
+    obj, probe = obj.astype(np.complex128), probe.astype(np.complex128)
+    amp = []
+    for q in pos:
+        o = np.round(q).astype(int)
+        amp.append(np.abs(np.fft.fft2(obj[o[0]:o[0] + N, o[1]:o[1] + N] * probe[0])))
+    amp = np.array(amp)
+    s = oracle.OracleSession("ePIE", amp, np.round(pos), obj, probe, probe_guess_path=False, updateProbe=1,
+                             phaseConstraint=0)
+    s.step()
+    o2, p2, _ = s.state()
+    assert rel_err(o2, obj) < 1e-12 and rel_err(p2, probe) < 1e-12
+
+
+def test_dm_first_iteration_known_answer(oracle):
+    # From a zero object and zero exit waves: Psi = 0, so Psi' = A/N^2 (phase 0), psi_1 = IFFT2(A)/N^2 and
+    # O_1 = (1/probeMax) * sum_j conj(P) psi_1,j placed at the rounded offsets (phase-clamped increments).
+    N = 16
+    pos, X, Y, obj, probe = _toy(N, seed=3)
+    rng = np.random.default_rng(5)
+    amp = rng.uniform(0.0, 2.0, size=(pos.shape[0], N, N))
+    s = oracle.OracleSession("DM", amp, pos, np.zeros((X, Y)), probe, probe_guess_path=False)
+    s.step()
+    o1, _, sc = s.state()
+    expect = np.zeros((X, Y), complex)
+    for j, q in enumerate(pos):
+        ox, oy = np.round(q).astype(int)
+        psi1 = np.fft.ifft2(amp[j])  # = IFFT_unnormalised(A)/N^2
+        inc = np.conj(probe[0]) * psi1 * 1.0  # probeMax = 1 for a supplied probe
+        inc = np.where(np.angle(inc) > 0, np.abs(inc), inc)  # phaseConstraint = 1 at iteration 1
+        expect[ox:ox + N, oy:oy + N] += inc
+    assert rel_err(o1, expect) < 1e-12
+    assert abs(sc[0] - np.sum(np.abs(expect) ** 2)) / sc[0] < 1e-12
+    psi = s.psi()
+    assert rel_err(psi[0], np.fft.ifft2(amp[0])) < 1e-12
+
+
+def test_probe_guess_matches_mean_amplitude(oracle):
+    rng = np.random.default_rng(2)
+    N = 32
+    amp = rng.uniform(0.1, 1.0, size=(6, N, N))
+    dx_s = oracle.sample_pixel(2.48e-10, 1.0, 172e-6, N)
+    P = oracle.probe_guess(amp, 110e-9, dx_s, K=2)
+    assert abs(np.abs(P[0]).max() - 1.0) < 1e-12 and np.abs(P[1]).max() == 0
+    F = np.abs(np.fft.fft2(P[0]))
+    avg = amp.mean(0)
+    ratio = F / avg
+    assert ratio.std() / ratio.mean() < 1e-10
