@@ -574,24 +574,58 @@ int orc_extract_patch(const double* obj, int X, int Y, float qx, float qy, int N
 // Oracle session: one reconstruction (algo 0 = ePIE, 1 = reference DM) driven one iteration at a time, so the
 // flag schedule (i <= phaseConstraint, i >= updateProbe, i >= updateModes) and all cached state (|O|^2 cache,
 // probe intensity cache, running maxima, DM factors, visiting-order stream) persist exactly as in a session.
-struct OrcSession {
-  int algo = 0, iter = 0, nthreads = 1;
-  State<double> s;
-  DMState<double> d;
-  Flags fl;
-  uint64_t rng = 0;
-  std::vector<double> amp, sq;
-  std::vector<float> pos;
+// precision 0 = FP64 (the oracle proper); 1 = the same code in FP32 (used to tell FP32 rounding from logic).
+}  // extern "C"
+
+namespace {
+struct OrcBase {
+  virtual ~OrcBase() {}
+  virtual int step(double* err) = 0;
+  virtual void get(double* obj, double* probe, double* scalars) = 0;
+  virtual void psi(double* out) = 0;
 };
 
-// probeGuessPath != 0: the probe came from the guess (its intensity cache and max are valid, as after
-// Probe::init's normalize()); otherwise it was supplied and the cache is zero with max 1 (src/Probe.cpp:354-358).
-// modesGiven != 0: modes >= 1 were supplied, so the modal switch does not re-initialise them.
-void* orc_create(int algo, int N, int K, int P, int X, int Y, const double* amp, const float* pos,
-                 const double* obj, const double* probe, int probeGuessPath, int modesGiven, uint64_t seed,
-                 int phaseConstraint, int updateProbe, int updateModes, int calculateRMS, int nthreads) {
-  if (N < 2 || (N & (N - 1)) || K < 1 || P < 1 || X < N || Y < N) return nullptr;
-  auto* h = new OrcSession;
+template <typename R> struct OrcSessionT : OrcBase {
+  int algo = 0, iter = 0, nthreads = 1;
+  State<R> s;
+  DMState<R> d;
+  Flags fl;
+  uint64_t rng = 0;
+  std::vector<R> amp, sq;
+  std::vector<float> pos;
+
+  int step(double* err) override {
+    int status = 0;
+    const int it = ++iter;
+    double e = 0;
+    if (algo == 0)
+      e = double(epie_iteration<R>(s, amp.data(), pos.data(), sq.data(), fl, it, rng, &status));
+    else
+      dm_iteration<R>(s, d, amp.data(), pos.data(), fl, it, nthreads);
+    if (err) *err = e;
+    return status;
+  }
+  void get(double* obj, double* probe, double* scalars) override {
+    store_state(s, obj, probe);
+    if (scalars) {
+      scalars[0] = double(s.objMax); scalars[1] = double(s.probeMax);
+      scalars[2] = d.fac[0]; scalars[3] = d.fac[1];
+    }
+  }
+  void psi(double* out) override {
+    const size_t n = size_t(s.P) * s.N * s.N;
+    for (size_t i = 0; i < n; ++i) {
+      cx<R> v = d.psi.empty() ? cx<R>(0, 0) : d.psi[i];
+      out[2 * i] = double(v.real()); out[2 * i + 1] = double(v.imag());
+    }
+  }
+};
+
+template <typename R>
+OrcBase* make_session(int algo, int N, int K, int P, int X, int Y, const double* amp, const float* pos,
+                      const double* obj, const double* probe, int probeGuessPath, int modesGiven, uint64_t seed,
+                      int phaseConstraint, int updateProbe, int updateModes, int calculateRMS, int nthreads) {
+  auto* h = new OrcSessionT<R>;
   h->algo = algo;
   h->nthreads = nthreads < 1 ? 1 : nthreads;
   load_state(h->s, N, K, P, X, Y, obj, probe, probeGuessPath);
@@ -600,55 +634,60 @@ void* orc_create(int algo, int N, int K, int P, int X, int Y, const double* amp,
   h->fl.calculateRMS = calculateRMS;
   h->rng = seed;
   const size_t NN = size_t(N) * N;
-  h->amp.assign(amp, amp + size_t(P) * NN);
+  h->amp.resize(size_t(P) * NN);
+  for (size_t i = 0; i < h->amp.size(); ++i) h->amp[i] = R(amp[i]);
   h->pos.assign(pos, pos + 2 * size_t(P));
-  h->sq.assign(P, 1.0);
+  h->sq.assign(P, R(1));
   if (calculateRMS)  // Diffractions::fillSquaredSums: the sum of each amplitude pattern
     for (int i = 0; i < P; ++i) {
       double t = 0;
-      for (size_t p = 0; p < NN; ++p) t += h->amp[size_t(i) * NN + p];
-      h->sq[i] = t;
+      for (size_t p = 0; p < NN; ++p) t += amp[size_t(i) * NN + p];
+      h->sq[i] = R(t);
     }
   return h;
 }
 
-// Runs the next iteration; err receives the iteration's error metric (ePIE with calculateRMS; 0 for DM).
-int orc_step(void* hp, double* err) {
-  auto* h = static_cast<OrcSession*>(hp);
-  int status = 0;
-  const int it = ++h->iter;
-  double e = 0;
-  if (h->algo == 0)
-    e = epie_iteration<double>(h->s, h->amp.data(), h->pos.data(), h->sq.data(), h->fl, it, h->rng, &status);
-  else
-    dm_iteration<double>(h->s, h->d, h->amp.data(), h->pos.data(), h->fl, it, h->nthreads);
-  if (err) *err = e;
-  return status;
+}  // namespace
+
+extern "C" {
+
+// probeGuessPath != 0: the probe came from the guess (its intensity cache and max are valid, as after
+// Probe::init's normalize()); otherwise it was supplied and the cache is zero with max 1 (src/Probe.cpp:354-358).
+// modesGiven != 0: modes >= 1 were supplied, so the modal switch does not re-initialise them.
+void* orc_create2(int precision, int algo, int N, int K, int P, int X, int Y, const double* amp, const float* pos,
+                  const double* obj, const double* probe, int probeGuessPath, int modesGiven, uint64_t seed,
+                  int phaseConstraint, int updateProbe, int updateModes, int calculateRMS, int nthreads) {
+  if (N < 2 || (N & (N - 1)) || K < 1 || P < 1 || X < N || Y < N) return nullptr;
+  if (precision == 1)
+    return make_session<float>(algo, N, K, P, X, Y, amp, pos, obj, probe, probeGuessPath, modesGiven, seed,
+                               phaseConstraint, updateProbe, updateModes, calculateRMS, nthreads);
+  return make_session<double>(algo, N, K, P, X, Y, amp, pos, obj, probe, probeGuessPath, modesGiven, seed,
+                              phaseConstraint, updateProbe, updateModes, calculateRMS, nthreads);
 }
+
+void* orc_create(int algo, int N, int K, int P, int X, int Y, const double* amp, const float* pos,
+                 const double* obj, const double* probe, int probeGuessPath, int modesGiven, uint64_t seed,
+                 int phaseConstraint, int updateProbe, int updateModes, int calculateRMS, int nthreads) {
+  return orc_create2(0, algo, N, K, P, X, Y, amp, pos, obj, probe, probeGuessPath, modesGiven, seed,
+                     phaseConstraint, updateProbe, updateModes, calculateRMS, nthreads);
+}
+
+// Runs the next iteration; err receives the iteration's error metric (ePIE with calculateRMS; 0 for DM).
+int orc_step(void* hp, double* err) { return static_cast<OrcBase*>(hp)->step(err); }
 
 // Copies out object (X*Y complex), probe (K*N*N complex) and {objMax, probeMax, fac0, fac1}.
 int orc_get(void* hp, double* obj, double* probe, double* scalars) {
-  auto* h = static_cast<OrcSession*>(hp);
-  store_state(h->s, obj, probe);
-  if (scalars) {
-    scalars[0] = h->s.objMax; scalars[1] = h->s.probeMax;
-    scalars[2] = h->d.fac[0]; scalars[3] = h->d.fac[1];
-  }
+  static_cast<OrcBase*>(hp)->get(obj, probe, scalars);
   return 0;
 }
 
 // DM exit-wave state (P*N*N complex); zeros before the first DM iteration.
 int orc_get_psi(void* hp, double* psi) {
-  auto* h = static_cast<OrcSession*>(hp);
-  const size_t n = size_t(h->s.P) * h->s.N * h->s.N;
-  for (size_t i = 0; i < n; ++i) {
-    cx<double> v = h->d.psi.empty() ? cx<double>(0, 0) : h->d.psi[i];
-    psi[2 * i] = v.real(); psi[2 * i + 1] = v.imag();
-  }
+  static_cast<OrcBase*>(hp)->psi(psi);
   return 0;
 }
 
-void orc_destroy(void* hp) { delete static_cast<OrcSession*>(hp); }
+void orc_destroy(void* hp) { delete static_cast<OrcBase*>(hp); }
 
 // FP32 multithreaded DM over float inputs: the CPU baseline.  Same equations as orc_dm_run; runs `iters`
 // iterations from a zero object with the given probe and returns the wall time in seconds of those iterations.

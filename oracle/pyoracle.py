@@ -44,6 +44,7 @@ def lib():
             "orc_visiting_order": ([ctypes.POINTER(u64), i, vp], None),
             "orc_extract_patch": ([vp, i, i, f, f, i, vp], i),
             "orc_create": ([i, i, i, i, i, i, vp, vp, vp, vp, i, i, u64, i, i, i, i, i], vp),
+            "orc_create2": ([i, i, i, i, i, i, i, vp, vp, vp, vp, i, i, u64, i, i, i, i, i], vp),
             "orc_step": ([vp, ctypes.POINTER(d)], i),
             "orc_get": ([vp, vp, vp, vp], i),
             "orc_get_psi": ([vp, vp], i),
@@ -114,7 +115,7 @@ class OracleSession:
     """FP64 restatement of one reconstruction (algo 'ePIE' or 'DM'), stepped one iteration at a time."""
 
     def __init__(self, algo, amp, pos, obj, probe, *, probe_guess_path, modes_given=False, seed=0x5EED5EED,
-                 phaseConstraint=1, updateProbe=10, updateModes=20, calculateRMS=0, nthreads=1):
+                 phaseConstraint=1, updateProbe=10, updateModes=20, calculateRMS=0, nthreads=1, fp32=False):
         self.amp = np.ascontiguousarray(amp, np.float64)
         self.pos = np.ascontiguousarray(pos, np.float32)
         obj = np.ascontiguousarray(obj, np.complex128)
@@ -124,7 +125,7 @@ class OracleSession:
         self.X, self.Y = obj.shape
         self.K, self.N = probe.shape[0], probe.shape[1]
         self.P = self.amp.shape[0]
-        self.h = lib().orc_create(0 if algo == "ePIE" else 1, self.N, self.K, self.P, self.X, self.Y, _p(self.amp),
+        self.h = lib().orc_create2(int(fp32), 0 if algo == "ePIE" else 1, self.N, self.K, self.P, self.X, self.Y, _p(self.amp),
                                   _p(self.pos), _p(obj), _p(probe), int(probe_guess_path), int(modes_given),
                                   seed, phaseConstraint, updateProbe, updateModes, calculateRMS, nthreads)
         if not self.h:

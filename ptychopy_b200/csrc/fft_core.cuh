@@ -132,6 +132,8 @@ struct FftShape {
   static constexpr int E = L / T;      // registers (complex) per thread
   static constexpr int M = E / T;      // stage-2 DFTs per thread
   static constexpr int XCH = E * (T + 1);  // exchange buffer (float2) per vector
+  static constexpr int RC = (256 / T < L) ? 256 / T : L;  // rows (vectors) of a row-transform CTA
+  static constexpr int THREADS = RC * T;                   // its block size (<= 256)
   static_assert(T > 0, "unsupported FFT length");
 };
 

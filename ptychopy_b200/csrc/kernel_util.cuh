@@ -7,10 +7,10 @@
 
 namespace pty {
 
-// Shared memory of a 256-thread row-transform CTA: twiddles + max(exchange buffers, transposed staging).
+// Shared memory of a row-transform CTA (FftShape<L>::RC rows): twiddles + max(exchange, transposed staging).
 template <int L>
 __host__ __device__ constexpr size_t rows_smem_bytes() {
-  constexpr int T = FftShape<L>::T, R = 256 / T;
+  constexpr int R = FftShape<L>::RC;
   constexpr int xch = R * FftShape<L>::XCH, stage = L * (R + 1);
   return sizeof(float2) * (L + (xch > stage ? xch : stage));
 }

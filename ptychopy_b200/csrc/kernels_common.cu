@@ -30,10 +30,11 @@ cudaError_t make_twiddles(int N, float2** d_tw, cudaStream_t st) {
 
 // ---- row transform + transposed store ------------------------------------------------------------------
 template <int L, bool INV>
-__global__ void __launch_bounds__(256) k_fft_rows_t(const float2* __restrict__ in, float2* __restrict__ out,
-                                                     const float2* __restrict__ g_tw) {
+__global__ void __launch_bounds__(FftShape<L>::THREADS) k_fft_rows_t(const float2* __restrict__ in,
+                                                                      float2* __restrict__ out,
+                                                                      const float2* __restrict__ g_tw) {
   using S = FftShape<L>;
-  constexpr int T = S::T, E = S::E, R = 256 / T;
+  constexpr int T = S::T, E = S::E, R = S::RC;
   extern __shared__ float4 smem4[];
   float2* smem = reinterpret_cast<float2*>(smem4);
   float2* s_tw = smem;
@@ -54,15 +55,15 @@ __global__ void __launch_bounds__(256) k_fft_rows_t(const float2* __restrict__ i
 template <int L>
 static cudaError_t launch_fft_pass(const float2* in, float2* out, const float2* tw, int batch, bool inverse,
                                    cudaStream_t st) {
-  constexpr int T = FftShape<L>::T, R = 256 / T;
+  constexpr int R = FftShape<L>::RC, NT = FftShape<L>::THREADS;
   const size_t smem = rows_smem_bytes<L>();
   dim3 grid(L / R, batch);
   if (inverse) {
     cudaFuncSetAttribute(k_fft_rows_t<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    k_fft_rows_t<L, true><<<grid, 256, smem, st>>>(in, out, tw);
+    k_fft_rows_t<L, true><<<grid, NT, smem, st>>>(in, out, tw);
   } else {
     cudaFuncSetAttribute(k_fft_rows_t<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    k_fft_rows_t<L, false><<<grid, 256, smem, st>>>(in, out, tw);
+    k_fft_rows_t<L, false><<<grid, NT, smem, st>>>(in, out, tw);
   }
   return cudaGetLastError();
 }

@@ -24,12 +24,12 @@
 namespace pty {
 
 template <int L>
-__global__ void __launch_bounds__(256) k_dm_fwd_rows(const float2* __restrict__ psi, const float2* __restrict__ obj,
+__global__ void __launch_bounds__(FftShape<L>::THREADS) k_dm_fwd_rows(const float2* __restrict__ psi, const float2* __restrict__ obj,
                                                       int objY, const float2* __restrict__ probe,
                                                       const int2* __restrict__ offs, const int* __restrict__ slot_pat,
                                                       float2* __restrict__ W1, const float2* __restrict__ g_tw) {
   using S = FftShape<L>;
-  constexpr int T = S::T, E = S::E, R = 256 / T;
+  constexpr int T = S::T, E = S::E, R = S::RC;
   extern __shared__ float4 smem4[];
   float2* smem = reinterpret_cast<float2*>(smem4);
   float2* s_tw = smem;
@@ -57,11 +57,11 @@ __global__ void __launch_bounds__(256) k_dm_fwd_rows(const float2* __restrict__ 
 }
 
 template <int L>
-__global__ void __launch_bounds__(256) k_dm_cols(const float2* __restrict__ W1, const float* __restrict__ ampT,
+__global__ void __launch_bounds__(FftShape<L>::THREADS) k_dm_cols(const float2* __restrict__ W1, const float* __restrict__ ampT,
                                                   const int* __restrict__ slot_pat, float2* __restrict__ W2,
                                                   const float2* __restrict__ g_tw) {
   using S = FftShape<L>;
-  constexpr int T = S::T, E = S::E, R = 256 / T;
+  constexpr int T = S::T, E = S::E, R = S::RC;
   extern __shared__ float4 smem4[];
   float2* smem = reinterpret_cast<float2*>(smem4);
   float2* s_tw = smem;
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(256) k_dm_cols(const float2* __restrict__ W1, 
 }
 
 template <int L>
-__global__ void __launch_bounds__(256) k_dm_inv_rows(const float2* __restrict__ W2, float2* __restrict__ psi,
+__global__ void __launch_bounds__(FftShape<L>::THREADS) k_dm_inv_rows(const float2* __restrict__ W2, float2* __restrict__ psi,
                                                       const float2* __restrict__ obj, int objY,
                                                       const float2* __restrict__ probe, const int2* __restrict__ offs,
                                                       const int* __restrict__ slot_pat, float2* __restrict__ dO,
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(256) k_dm_inv_rows(const float2* __restrict__ 
   float2* smem = reinterpret_cast<float2*>(smem4);
   float2* s_tw = smem;
   float2* s_x = smem + L;
-  constexpr int R = 256 / T;
+  constexpr int R = S::RC;
   const int slot = blockIdx.y;
   const int p = slot_pat[slot];
   const int v = threadIdx.x / T, t = threadIdx.x % T;
@@ -212,12 +212,12 @@ cudaError_t dm_prepare(int N) {
 template <int L>
 static cudaError_t dm_wave_t(const DMBuffers& b, const DMWave& w, bool pc, bool up, cudaStream_t st,
                              int64_t* launches) {
-  constexpr int T = FftShape<L>::T, R = 256 / T;
+  constexpr int R = FftShape<L>::RC, NT = FftShape<L>::THREADS;
   const size_t smem = rows_smem_bytes<L>();
   dim3 grid(L / R, w.count);
-  k_dm_fwd_rows<L><<<grid, 256, smem, st>>>(b.psi, b.obj, b.Y, b.probe, b.offs, w.slot_pat, b.W1, b.tw);
-  k_dm_cols<L><<<grid, 256, smem, st>>>(b.W1, b.ampT, w.slot_pat, b.W2, b.tw);
-  k_dm_inv_rows<L><<<grid, 256, smem, st>>>(b.W2, b.psi, b.obj, b.Y, b.probe, b.offs, w.slot_pat, b.dO, b.dP, b.fac,
+  k_dm_fwd_rows<L><<<grid, NT, smem, st>>>(b.psi, b.obj, b.Y, b.probe, b.offs, w.slot_pat, b.W1, b.tw);
+  k_dm_cols<L><<<grid, NT, smem, st>>>(b.W1, b.ampT, w.slot_pat, b.W2, b.tw);
+  k_dm_inv_rows<L><<<grid, NT, smem, st>>>(b.W2, b.psi, b.obj, b.Y, b.probe, b.offs, w.slot_pat, b.dO, b.dP, b.fac,
                                             pc ? 1 : 0, up ? 1 : 0, b.tw);
   if (launches) *launches += 3;
   return cudaGetLastError();
