@@ -18,7 +18,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
 
-CU_SOURCES = ["kernels_common.cu", "kernels_dm.cu", "kernels_epie.cu", "session.cu"]
+CU_SOURCES = ["kernels_common.cu", "kernels_dm.cu", "kernels_epie.cu", "session.cu", "noalloc.cu"]
 HEADERS = ["fft_core.cuh", "kernel_util.cuh", "kernels.h", "kernels_epie.h", "session.h"]
 
 LIB = os.path.join(HERE, "libptychopy_b200.so")

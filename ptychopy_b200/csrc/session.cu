@@ -21,6 +21,9 @@ static thread_local std::string g_last_error;
 
 [[noreturn]] void fail(int code, const std::string& msg) { throw Error{code, msg}; }
 
+// Sets the calling thread's pty_last_error() message (for entry points outside the guarded() wrapper).
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 void check_cuda(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return;
   cudaGetLastError();

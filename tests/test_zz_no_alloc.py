@@ -1,0 +1,54 @@
+"""pty_fft2_dev_noalloc: the batched 2-D FFT without any device allocation.
+
+For callers that cannot call cudaMalloc (a host that owns all device memory up front and forbids allocation
+afterwards): the entry point keeps its work buffer in a static device array of the library.  This test calls it
+through the C ABI and checks it against the allocating entry point pty_fft2_dev on two calls in a row, and that a
+request larger than the 8 MiB scratch is refused.  It sits in a file of its own that pytest collects last.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _random(batch, N, seed):
+    rng = np.random.default_rng(seed)
+    return (rng.standard_normal((batch, N, N)) + 1j * rng.standard_normal((batch, N, N))).astype(np.complex64)
+
+
+def test_no_alloc_fft_matches_allocating_entry_point():
+    import torch
+
+    from ptychopy_b200 import abi
+
+    lib = abi.lib()
+    for k, (N, batch, inverse) in enumerate([(256, 3, False), (512, 2, True)]):  # two calls in a row
+        a = _random(batch, N, 100 + k)
+        ref = torch.from_numpy(a.view(np.float32).copy()).cuda()
+        work = torch.empty_like(ref)
+        abi.fft2_dev(ref.data_ptr(), work.data_ptr(), batch, N, inverse=inverse)
+        got = torch.from_numpy(a.view(np.float32).copy()).cuda()
+        rc = lib.pty_fft2_dev_noalloc(ctypes.c_void_p(got.data_ptr()), batch, N, int(inverse), None)
+        assert rc == abi.PTY_OK, lib.pty_last_error().decode()
+        torch.cuda.synchronize()
+        g = got.cpu().numpy().view(np.complex64)
+        r = ref.cpu().numpy().view(np.complex64)
+        assert rel_err(g, r) < 3e-6
+        exact = np.fft.ifft2(a.astype(np.complex128)) * N * N if inverse else np.fft.fft2(a.astype(np.complex128))
+        assert rel_err(g, exact) < 3e-6
+
+
+def test_no_alloc_fft_rejects_oversize_requests():
+    import torch
+
+    from ptychopy_b200 import abi
+
+    lib = abi.lib()
+    d = torch.zeros((5, 512, 512, 2), dtype=torch.float32, device="cuda")  # 10 MiB > 8 MiB
+    rc = lib.pty_fft2_dev_noalloc(ctypes.c_void_p(d.data_ptr()), 5, 512, 0, None)
+    assert rc == abi.PTY_ERR_INVALID
+    assert b"8 MiB" in lib.pty_last_error()
