@@ -35,6 +35,9 @@ def parse():
     ap.add_argument("--e2e-calls", type=int, default=2)
     ap.add_argument("--e2e-iters", type=int, default=100, help="iterations per public-API call (the config's 100)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--nx", type=int, default=30, help="raster size (30 = the DM configuration; smaller for profiling)")
+    ap.add_argument("--wave", type=int, default=0, help="DM patterns per pipeline wave (0 = automatic)")
     return ap.parse_args()
 
 
@@ -120,13 +123,13 @@ def profiled_traffic():
     return None
 
 
-def dataset(device):
+def dataset(device, nx=30):
     """Seeded synthetic DM workload; patterns generated on `device` (torch) to keep set-up short."""
     import numpy as np
 
     from ptychopy_b200 import synth
 
-    cfg = synth.CONFIGS["dm512"]
+    cfg = dict(synth.CONFIGS["dm512"], nx=nx, ny=nx)
     rng = np.random.default_rng(20261204)
     N = cfg["N"]
     dx_s = synth.sample_pixel(cfg["lambd"], cfg["z"], cfg["dx_d"], N)
@@ -212,10 +215,10 @@ def run_b200(args, rank, world, local):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    ds = dataset("cuda")
+    ds = dataset("cuda", args.nx)
     N, P = ds["N"], ds["P"]
     stream = torch.cuda.Stream()
-    s = abi.Session(**dict(ds["kwargs"], algorithm="DM", device=local))
+    s = abi.Session(**dict(ds["kwargs"], algorithm="DM", device=local, wave=args.wave))
     s.set_stream(stream.cuda_stream)
     s.set_patterns_ptr(ds["amp"].data_ptr(), P, N)
     s.init()
@@ -251,6 +254,14 @@ def run_b200(args, rank, world, local):
     value = P * args.steps * world / (ms_max / 1000.0)
     ms_step = ms_max / args.steps
 
+    if args.no_e2e:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": ms_step, "steps": args.steps,
+                              "positions": P, "gpu_launches": int(launches), "finite": finite, "clocks": ck,
+                              "note": "partial run (--no-e2e)"}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
     # end to end through the public API: pinned host patterns -> dmnp(iter=...) -> object/probe on the host
     import ptychopy_b200
 
@@ -260,7 +271,7 @@ def run_b200(args, rank, world, local):
     amp_host = host.numpy()
     del ds["amp"]
     torch.cuda.empty_cache()
-    kw = dict(ds["kwargs"], iter=args.e2e_iters, returnResults=1, writeResults=0, device=local)
+    kw = dict(ds["kwargs"], iter=args.e2e_iters, returnResults=1, writeResults=0, device=local, wave=args.wave)
     pt.dmnp(diffractionNP=amp_host, **dict(kw, iter=2))  # warm-up call
     if dist:
         dist.barrier()
@@ -285,7 +296,8 @@ def run_b200(args, rank, world, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; object GRF phase, 110 nm probe, Poisson)",
-            "config": {"workload": WORKLOAD, "N": N, "positions": P, "object": [ds["X"], ds["Y"]],
+            "config": {"workload": WORKLOAD if args.nx == 30 else f"{WORKLOAD} (raster {args.nx}x{args.nx})",
+                       "N": N, "positions": P, "object": [ds["X"], ds["Y"]],
                        "step": "one DM iteration over all 900 patterns",
                        "l2": "inputs larger than L2 (exit waves 1.89 GB + amplitudes 0.94 GB per step)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},

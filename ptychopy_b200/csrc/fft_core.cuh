@@ -124,17 +124,24 @@ __device__ __forceinline__ void dft_reg(float2 (&a)[E]) {
   dif_stages<E, INV>(a);
 }
 
-// Thread layout of a length-L transform.
+// Thread layout of a length-L transform: L = E*T with T lanes per vector and E values per lane.
+// E >= T: stage 2 is M = E/T T-point DFTs per lane.  E < T (Q = T/E = 2): each T-point DFT of stage 2 is shared by
+// a lane pair through one radix-2 DIF step (L = 512 uses a whole warp per row with 16 values per lane, which keeps
+// registers low enough for several CTAs per SM).
+__host__ __device__ constexpr int fft_lanes(int L) {
+  return L == 1024 ? 32 : L == 512 ? 32 : L == 256 ? 16 : L == 128 ? 8 : L == 64 ? 8 : L == 32 ? 4 : 0;
+}
 template <int L>
 struct FftShape {
-  static constexpr int T = (L == 1024) ? 32 : (L == 512) ? 16 : (L == 256) ? 16 : (L == 128) ? 8 : (L == 64) ? 8
-                          : (L == 32) ? 4 : 0;
-  static constexpr int E = L / T;      // registers (complex) per thread
-  static constexpr int M = E / T;      // stage-2 DFTs per thread
-  static constexpr int XCH = E * (T + 1);  // exchange buffer (float2) per vector
+  static constexpr int T = fft_lanes(L);
+  static constexpr int E = L / T;                    // registers (complex) per lane
+  static constexpr int M = E >= T ? E / T : 1;       // stage-2 DFTs per lane (E >= T)
+  static constexpr int Q = E >= T ? 1 : T / E;       // lanes per stage-2 DFT (E < T)
+  static constexpr int XCH = E * (T + 1);            // exchange buffer (float2) per vector
   static constexpr int RC = (256 / T < L) ? 256 / T : L;  // rows (vectors) of a row-transform CTA
   static constexpr int THREADS = RC * T;                   // its block size (<= 256)
   static_assert(T > 0, "unsupported FFT length");
+  static_assert(Q == 1 || Q == 2, "stage-2 split supports lane pairs only");
 };
 
 // Twiddle table for stage 1: tw[k1*T + t] = exp(-2*pi*i*t*k1/L); filled by fill_twiddles (double precision).
@@ -143,12 +150,12 @@ __device__ __forceinline__ void load_twiddles(float2* s_tw, const float2* __rest
   for (int i = threadIdx.x; i < L; i += blockDim.x) s_tw[i] = g_tw[i];
 }
 
-// One length-L transform by T cooperating lanes of a warp (lane group `t` = 0..T-1).
-// v: on entry v[e] = x[t + T*e]; on exit v[m*T + k2] = X[t + T*(m + M*k2)].
+// One length-L transform by T cooperating lanes of a warp (lane index `t` = 0..T-1).
+// v: on entry v[e] = x[t + T*e]; on exit element t + T*e is in v[out_slot<L>(e)].
 // xch: this vector's exchange buffer (XCH float2).  Ends with __syncwarp (xch reusable).
 template <int L, bool INV>
 __device__ __forceinline__ void fft_vec(float2 (&v)[FftShape<L>::E], int t, float2* xch, const float2* s_tw) {
-  constexpr int T = FftShape<L>::T, E = FftShape<L>::E, M = FftShape<L>::M;
+  constexpr int T = FftShape<L>::T, E = FftShape<L>::E, M = FftShape<L>::M, Q = FftShape<L>::Q;
   dft_reg<INV>(v);
   static_for<0, E>([&](auto k1c) {
     constexpr int k1 = decltype(k1c)::value;
@@ -162,27 +169,49 @@ __device__ __forceinline__ void fft_vec(float2 (&v)[FftShape<L>::E], int t, floa
     }
   });
   __syncwarp();
-  static_for<0, M>([&](auto mc) {
-    constexpr int m = decltype(mc)::value;
-    float2 c[T];
+  if constexpr (Q == 1) {
+    static_for<0, M>([&](auto mc) {
+      constexpr int m = decltype(mc)::value;
+      float2 c[T];
 #pragma unroll
-    for (int tt = 0; tt < T; ++tt) c[tt] = xch[(t + T * m) * (T + 1) + tt];
-    dft_reg<INV>(c);
-    static_for<0, T>([&](auto k2c) {
-      constexpr int k2 = decltype(k2c)::value;
-      v[m * T + k2] = c[bitrev(k2, T)];
+      for (int tt = 0; tt < T; ++tt) c[tt] = xch[(t + T * m) * (T + 1) + tt];
+      dft_reg<INV>(c);
+      static_for<0, T>([&](auto k2c) {
+        constexpr int k2 = decltype(k2c)::value;
+        v[m * T + k2] = c[bitrev(k2, T)];
+      });
     });
-  });
+  } else {
+    // lane t = k1 + E*q: radix-2 DIF over the two halves of the T-point DFT for its k1, keeping half q:
+    // c[t'] = (b[t'] + (-1)^q b[t'+E]) * w_T^(q t'), then an E-point DFT gives outputs k2 = q + 2j.
+    const int k1 = t % E;
+    const bool odd = t >= E;
+    const float sgn = odd ? -1.f : 1.f;
+    const float2* row = xch + k1 * (T + 1);
+    float2 c[E];
+    static_for<0, E>([&](auto tc) {
+      constexpr int tp = decltype(tc)::value;
+      const float2 b0 = row[tp], b1 = row[tp + E];
+      const float2 d = make_float2(b0.x + sgn * b1.x, b0.y + sgn * b1.y);
+      const float2 dw = twiddle32<tp*(32 / T), INV>(d);
+      c[tp] = odd ? dw : d;
+    });
+    dft_reg<INV>(c);
+    static_for<0, E>([&](auto jc) {
+      constexpr int j = decltype(jc)::value;
+      v[j] = c[bitrev(j, E)];
+    });
+  }
   __syncwarp();
 }
 
-// Register slot of element index n = t + T*e for this thread: slot(e) = m*T + k2 with e = m + M*k2.
+// Register slot of element index n = t + T*e for this lane after fft_vec.
 template <int L>
 __host__ __device__ constexpr int out_slot(int e) {
-  return (e % FftShape<L>::M) * FftShape<L>::T + (e / FftShape<L>::M);
+  return FftShape<L>::Q > 1 ? e : (e % FftShape<L>::M) * FftShape<L>::T + (e / FftShape<L>::M);
 }
 
-// After fft_vec the thread holds element t + T*e in v[out_slot(e)].  To feed a second transform (which wants
+// After fft_vec the lane holds element t + T*e in v[out_slot(e)].  To feed a second transform (which wants
 // v[e] = element t + T*e) reorder the registers (free at compile time).
 template <int L>
 __device__ __forceinline__ void to_input_order(float2 (&v)[FftShape<L>::E]) {

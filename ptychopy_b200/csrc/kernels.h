@@ -57,6 +57,8 @@ struct DMBuffers {
 };
 // Sets the shared-memory attributes of the DM kernels for size N (call once, outside graph capture).
 cudaError_t dm_prepare(int N);
+// Patterns per pipeline wave for size N (balanced waves, W1 + W2 <= 1 GiB).
+int dm_wave_size(int N, int P);
 cudaError_t dm_wave(const DMBuffers& b, const DMWave& w, bool phaseConstraint, bool updateProbe, cudaStream_t st,
                     int64_t* launches);
 cudaError_t dm_finalize(const DMBuffers& b, bool updateProbe, cudaStream_t st, int64_t* launches);

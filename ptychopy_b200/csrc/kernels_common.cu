@@ -12,8 +12,8 @@ namespace pty {
 bool fft_size_supported(int N) { return N == 32 || N == 64 || N == 128 || N == 256 || N == 512; }
 
 cudaError_t make_twiddles(int N, float2** d_tw, cudaStream_t st) {
-  int T = N == 512 ? 16 : N == 256 ? 16 : N == 128 ? 8 : N == 64 ? 8 : N == 32 ? 4 : 0;
-  if (!T) return cudaErrorInvalidValue;
+  const int T = fft_lanes(N);
+  if (!T || N > 512) return cudaErrorInvalidValue;
   const int E = N / T;
   std::vector<float2> h(N);
   for (int k1 = 0; k1 < E; ++k1)

@@ -17,28 +17,37 @@
 // Object and probe updates use snapshot semantics: all increments of an iteration are computed from O and P
 // as they were at its start and summed (the reference adds them with atomics while other callbacks still read
 // O and P, which makes its result order-dependent).
+#include <algorithm>
+#include <cmath>
+
 #include "fft_core.cuh"
 #include "kernel_util.cuh"
 #include "kernels.h"
 
 namespace pty {
 
+// CTAs per SM the DM kernels are compiled for (caps registers so that many fit next to their shared memory).
+template <int L> struct DMOcc { static constexpr int MIN_BLOCKS = 4; };
+
+// Work items of a wave: (row block, slot) pairs; CTAs are persistent and stride over them (grid <= resident
+// slots), so a launch has no partially filled last round and CTAs drift out of lock-step (load / FFT overlap).
 template <int L>
-__global__ void __launch_bounds__(FftShape<L>::THREADS) k_dm_fwd_rows(const float2* __restrict__ psi, const float2* __restrict__ obj,
-                                                      int objY, const float2* __restrict__ probe,
-                                                      const int2* __restrict__ offs, const int* __restrict__ slot_pat,
-                                                      float2* __restrict__ W1, const float2* __restrict__ g_tw) {
+__global__ void __launch_bounds__(FftShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
+    k_dm_fwd_rows(const float2* __restrict__ psi, const float2* __restrict__ obj, int objY,
+                  const float2* __restrict__ probe, const int2* __restrict__ offs, const int* __restrict__ slot_pat,
+                  int count, float2* __restrict__ W1, const float2* __restrict__ g_tw) {
   using S = FftShape<L>;
-  constexpr int T = S::T, E = S::E, R = S::RC;
+  constexpr int T = S::T, E = S::E, R = S::RC, NB = L / S::RC;
   extern __shared__ float4 smem4[];
   float2* smem = reinterpret_cast<float2*>(smem4);
   float2* s_tw = smem;
   float2* s_x = smem + L;
-  const int slot = blockIdx.y;
-  const int p = slot_pat[slot];
   const int v = threadIdx.x / T, t = threadIdx.x % T;
-  const int x0 = blockIdx.x * R, x = x0 + v;
   load_twiddles<L>(s_tw, g_tw);
+  for (int item = blockIdx.x; item < NB * count; item += gridDim.x) {
+  const int slot = item / NB;
+  const int p = slot_pat[slot];
+  const int x0 = (item % NB) * R, x = x0 + v;
   const int2 o = offs[p];
   const float2* prow = probe + size_t(x) * L;
   const float2* orow = obj + size_t(x + o.x) * objY + o.y;
@@ -51,26 +60,28 @@ __global__ void __launch_bounds__(FftShape<L>::THREADS) k_dm_fwd_rows(const floa
     const float2 sv = ld_stream(srow + n);
     a[e] = make_float2(2.f * ph.x - sv.x, 2.f * ph.y - sv.y);
   }
-  __syncthreads();  // twiddles loaded
+  __syncthreads();  // twiddles loaded; previous item's staging reads done
   fft_vec<L, false>(a, t, s_x + v * S::XCH, s_tw);
   store_rows_transposed<L, R>(a, W1 + size_t(slot) * L * L, x0, v, t, s_x);
+  }
 }
 
 template <int L>
-__global__ void __launch_bounds__(FftShape<L>::THREADS) k_dm_cols(const float2* __restrict__ W1, const float* __restrict__ ampT,
-                                                  const int* __restrict__ slot_pat, float2* __restrict__ W2,
-                                                  const float2* __restrict__ g_tw) {
+__global__ void __launch_bounds__(FftShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
+    k_dm_cols(const float2* __restrict__ W1, const float* __restrict__ ampT, const int* __restrict__ slot_pat,
+              int count, float2* __restrict__ W2, const float2* __restrict__ g_tw) {
   using S = FftShape<L>;
-  constexpr int T = S::T, E = S::E, R = S::RC;
+  constexpr int T = S::T, E = S::E, R = S::RC, NB = L / S::RC;
   extern __shared__ float4 smem4[];
   float2* smem = reinterpret_cast<float2*>(smem4);
   float2* s_tw = smem;
   float2* s_x = smem + L;
-  const int slot = blockIdx.y;
-  const int p = slot_pat[slot];
   const int v = threadIdx.x / T, t = threadIdx.x % T;
-  const int k0 = blockIdx.x * R, ky = k0 + v;
   load_twiddles<L>(s_tw, g_tw);
+  for (int item = blockIdx.x; item < NB * count; item += gridDim.x) {
+  const int slot = item / NB;
+  const int p = slot_pat[slot];
+  const int k0 = (item % NB) * R, ky = k0 + v;
   const float2* row = W1 + (size_t(slot) * L + ky) * L;
   const float* arow = ampT + (size_t(p) * L + ky) * L;
   float2 a[E];
@@ -89,28 +100,27 @@ __global__ void __launch_bounds__(FftShape<L>::THREADS) k_dm_cols(const float2* 
   to_input_order<L>(a);
   fft_vec<L, true>(a, t, s_x + v * S::XCH, s_tw);
   store_rows_transposed<L, R>(a, W2 + size_t(slot) * L * L, k0, v, t, s_x);
+  }
 }
 
 template <int L>
-__global__ void __launch_bounds__(FftShape<L>::THREADS) k_dm_inv_rows(const float2* __restrict__ W2, float2* __restrict__ psi,
-                                                      const float2* __restrict__ obj, int objY,
-                                                      const float2* __restrict__ probe, const int2* __restrict__ offs,
-                                                      const int* __restrict__ slot_pat, float2* __restrict__ dO,
-                                                      float2* __restrict__ dP, const double* __restrict__ fac,
-                                                      int phaseConstraint, int updateProbe,
-                                                      const float2* __restrict__ g_tw) {
+__global__ void __launch_bounds__(FftShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
+    k_dm_inv_rows(const float2* __restrict__ W2, float2* __restrict__ psi, const float2* __restrict__ obj, int objY,
+                  const float2* __restrict__ probe, const int2* __restrict__ offs, const int* __restrict__ slot_pat,
+                  int count, float2* __restrict__ dO, float2* __restrict__ dP, const double* __restrict__ fac,
+                  int phaseConstraint, int updateProbe, const float2* __restrict__ g_tw) {
   using S = FftShape<L>;
-  constexpr int T = S::T, E = S::E;
+  constexpr int T = S::T, E = S::E, R = S::RC, NB = L / S::RC;
   extern __shared__ float4 smem4[];
   float2* smem = reinterpret_cast<float2*>(smem4);
   float2* s_tw = smem;
   float2* s_x = smem + L;
-  constexpr int R = S::RC;
-  const int slot = blockIdx.y;
-  const int p = slot_pat[slot];
   const int v = threadIdx.x / T, t = threadIdx.x % T;
-  const int x = blockIdx.x * R + v;
   load_twiddles<L>(s_tw, g_tw);
+  for (int item = blockIdx.x; item < NB * count; item += gridDim.x) {
+  const int slot = item / NB;
+  const int p = slot_pat[slot];
+  const int x = (item % NB) * R + v;
   const float2* row = W2 + (size_t(slot) * L + x) * L;
   float2 a[E];
 #pragma unroll
@@ -140,6 +150,7 @@ __global__ void __launch_bounds__(FftShape<L>::THREADS) k_dm_inv_rows(const floa
       atomicAdd(dprow + n, make_float2(pi.x * f0, pi.y * f0));
     }
   });
+  }
 }
 
 // O += dO, P += dP (mode 0), reset the accumulators, and sum |O|^2 and |P|^2 over all stacked probe modes.
@@ -210,17 +221,51 @@ cudaError_t dm_prepare(int N) {
 }
 
 template <int L>
+static int dm_grid(int items) {
+  static int slots = 0;
+  if (!slots) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_dm_fwd_rows<L>, FftShape<L>::THREADS, rows_smem_bytes<L>());
+    slots = sms * (per > 0 ? per : 1);
+  }
+  return items < slots ? items : slots;
+}
+
+template <int L>
 static cudaError_t dm_wave_t(const DMBuffers& b, const DMWave& w, bool pc, bool up, cudaStream_t st,
                              int64_t* launches) {
-  constexpr int R = FftShape<L>::RC, NT = FftShape<L>::THREADS;
+  constexpr int NT = FftShape<L>::THREADS, NB = L / FftShape<L>::RC;
   const size_t smem = rows_smem_bytes<L>();
-  dim3 grid(L / R, w.count);
-  k_dm_fwd_rows<L><<<grid, NT, smem, st>>>(b.psi, b.obj, b.Y, b.probe, b.offs, w.slot_pat, b.W1, b.tw);
-  k_dm_cols<L><<<grid, NT, smem, st>>>(b.W1, b.ampT, w.slot_pat, b.W2, b.tw);
-  k_dm_inv_rows<L><<<grid, NT, smem, st>>>(b.W2, b.psi, b.obj, b.Y, b.probe, b.offs, w.slot_pat, b.dO, b.dP, b.fac,
-                                            pc ? 1 : 0, up ? 1 : 0, b.tw);
+  const int grid = dm_grid<L>(NB * w.count);
+  k_dm_fwd_rows<L><<<grid, NT, smem, st>>>(b.psi, b.obj, b.Y, b.probe, b.offs, w.slot_pat, w.count, b.W1, b.tw);
+  k_dm_cols<L><<<grid, NT, smem, st>>>(b.W1, b.ampT, w.slot_pat, w.count, b.W2, b.tw);
+  k_dm_inv_rows<L><<<grid, NT, smem, st>>>(b.W2, b.psi, b.obj, b.Y, b.probe, b.offs, w.slot_pat, w.count, b.dO, b.dP,
+                                           b.fac, pc ? 1 : 0, up ? 1 : 0, b.tw);
   if (launches) *launches += 3;
   return cudaGetLastError();
+}
+
+// Patterns per wave: the largest balanced wave with W1 + W2 within 1 GiB.  The three kernels are bound by their
+// on-chip (L1/shared) traffic, so fewer, larger waves (less launch and tail overhead) beat L2-resident small ones.
+template <int L>
+static int dm_wave_size_t(int P) {
+  const size_t bytes_per_pattern = 2 * sizeof(float2) * size_t(L) * L;
+  const int maxwave = int(std::max<size_t>(1, (size_t(1) << 30) / bytes_per_pattern));
+  const int nwaves = (P + maxwave - 1) / maxwave;
+  return (P + nwaves - 1) / nwaves;
+}
+
+int dm_wave_size(int N, int P) {
+  switch (N) {
+    case 32: return dm_wave_size_t<32>(P);
+    case 64: return dm_wave_size_t<64>(P);
+    case 128: return dm_wave_size_t<128>(P);
+    case 256: return dm_wave_size_t<256>(P);
+    case 512: return dm_wave_size_t<512>(P);
+    default: return 1;
+  }
 }
 
 cudaError_t dm_wave(const DMBuffers& b, const DMWave& w, bool pc, bool up, cudaStream_t st, int64_t* launches) {

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/ptychopy_b200.h"
+#include "fft_core.cuh"
 #include "kernels.h"
 
 namespace pty {
@@ -36,7 +37,7 @@ std::mutex g_scratch_mu;
 
 // Stage-1 twiddles of a length-N transform in the [k1][t] layout the FFT kernels read (computed in double).
 void host_twiddles(int N, std::vector<float2>& out) {
-  const int T = N == 512 ? 16 : N == 256 ? 16 : N == 128 ? 8 : N == 64 ? 8 : 4;
+  const int T = fft_lanes(N);
   const int E = N / T;
   out.resize(N);
   for (int k1 = 0; k1 < E; ++k1)

@@ -414,9 +414,10 @@ void init_dm(pty_session* s) {
   check_cuda(cudaMemsetAsync(s->dO.p, 0, s->dO.bytes, s->stream), "memset dO");
   s->dP.alloc(sizeof(float2) * NN, "dP");
   check_cuda(cudaMemsetAsync(s->dP.p, 0, s->dP.bytes, s->stream), "memset dP");
-  // wave: patterns per pipeline pass; W1+W2 = 2 * wave * 8N^2 bytes, kept to ~64 MB so both stay in L2
+  // wave: patterns per pipeline pass (W1 + W2 = 2 * wave * 8N^2 bytes)
+  check_cuda(dm_prepare(s->N), "DM kernel set-up");
   int wave = s->prm.wave;
-  if (wave <= 0) wave = int(std::max<size_t>(1, (size_t(32) << 20) / (sizeof(float2) * NN)));
+  if (wave <= 0) wave = dm_wave_size(s->N, s->P);
   wave = std::min(wave, s->P);
   s->wave = wave;
   s->nwaves = (s->P + wave - 1) / wave;
@@ -430,7 +431,6 @@ void init_dm(pty_session* s) {
   s->scal.alloc(8 * sizeof(double), "DM scalars");
   const double h[8] = {0, 0, 1.0 / s->objMax0, 1.0 / s->probeMax0, s->objMax0, s->probeMax0, 0, 0};
   check_cuda(cudaMemcpyAsync(s->scal.p, h, sizeof(h), cudaMemcpyHostToDevice, s->stream), "H2D DM scalars");
-  check_cuda(dm_prepare(s->N), "DM kernel set-up");
   check_cuda(cudaStreamSynchronize(s->stream), "DM init");
 }
 
