@@ -482,6 +482,247 @@ template <typename R> void store_state(const State<R>& s, double* obj, double* p
   }
 }
 
+// ---------------------------------------------------------------- MLs core (src/MLS.cpp:74-490)
+// LSQ-ML with random groups, restated for one probe mode and one object, no variable probe, no sub-pixel shift,
+// no position search.  Geometry (ML mesh, src/CartesianScanMesh.cpp:94-177, src/IPtychoScanMesh.cpp:123-184):
+// raw centred positions, object Np_o_new = ceil(extent * 1.2), window starts round(pos + ceilvar) - 1.
+struct MlsGeometry {
+  int X = 0, Y = 0;
+  std::vector<int> r0, c0;   // window starts (0-based)
+  int roix0 = 0, roiy0 = 0, roinx = 0, roiny = 0;  // object ROI of calc_object_norm (0-based start, size)
+};
+
+// The ROI is kept inside the object (the reference indexes it unchecked); an empty range stays empty.
+void clamp_roi(int& a, int& n, int len) {
+  const int b = std::min(len, a + std::max(n, 0));
+  a = std::max(0, std::min(a, len));
+  n = std::max(0, b - a);
+}
+
+MlsGeometry mls_geometry(const std::vector<float>& raw, int P, int N) {
+  // raw: 2*P positions (x, y) in pixels, centred, as the ML mesh keeps them (no -min shift)
+  float mnx = std::numeric_limits<float>::max(), mny = mnx, mxx = -mnx, mxy = -mnx;
+  for (int i = 0; i < P; ++i) {
+    mnx = std::min(mnx, raw[2 * i]); mxx = std::max(mxx, raw[2 * i]);
+    mny = std::min(mny, raw[2 * i + 1]); mxy = std::max(mxy, raw[2 * i + 1]);
+  }
+  const float Np0 = 1e5f;
+  const float cv0x = std::ceil(Np0 * 1.0f / 2 - float(N) * 1.0f / 2), cv0y = cv0x;
+  const float rpx = (mxx + mnx) / 2, rpy = (mxy + mny) / 2;
+  long long minx = 1LL << 40, maxx = -1, miny = 1LL << 40, maxy = -1;
+  for (int i = 0; i < P; ++i) {  // tmpx from .y and tmpy from .x, as the reference's loop has them
+    long long tx = (long long)std::round(raw[2 * i + 1] - rpy + cv0x);
+    minx = std::min(minx, tx - 1); maxx = std::max(maxx, tx + N - 2);
+    long long ty = (long long)std::round(raw[2 * i] - rpx + cv0y);
+    miny = std::min(miny, ty - 1); maxy = std::max(maxy, ty + N - 2);
+  }
+  MlsGeometry g;
+  g.X = int(std::ceil(double(float(maxx - minx) * (1 + 0.2f))));
+  g.Y = int(std::ceil(double(float(maxy - miny) * (1 + 0.2f))));
+  const float cvx = std::ceil(float(g.X) * 1.0f / 2 - float(N) * 1.0f / 2);
+  const float cvy = std::ceil(float(g.Y) * 1.0f / 2 - float(N) * 1.0f / 2);
+  g.r0.resize(P); g.c0.resize(P);
+  for (int i = 0; i < P; ++i) {
+    g.r0[i] = int(std::round(raw[2 * i] + cvx)) - 1;
+    g.c0[i] = int(std::round(raw[2 * i + 1] + cvy)) - 1;
+  }
+  // precalculate_ROI: round(Np_o*0.5 + min) .. round(Np_o*0.5 + max) - 1, 1-based inclusive
+  const long long ax = (long long)std::round(g.X * 0.5 + mnx), bx = (long long)std::round(g.X * 0.5 + mxx) - 1;
+  const long long ay = (long long)std::round(g.Y * 0.5 + mny), by = (long long)std::round(g.Y * 0.5 + mxy) - 1;
+  g.roix0 = int(ax - 1); g.roinx = int(bx - ax + 1);
+  g.roiy0 = int(ay - 1); g.roiny = int(by - ay + 1);
+  clamp_roi(g.roix0, g.roinx, g.X);
+  clamp_roi(g.roiy0, g.roiny, g.Y);
+  return g;
+}
+
+// Group partition of one iteration: a SplitMix64 Fisher-Yates permutation cut into groups of G = max(1, P/100)
+// (src/IPtychoScanMesh.cpp:826-913), visited in a second shuffled order (src/MLS.cpp:106-113).
+void mls_groups(uint64_t& rng, int P, std::vector<std::vector<int>>& groups) {
+  std::vector<int> perm(P);
+  for (int i = 0; i < P; ++i) perm[i] = i;
+  for (int i = P - 1; i > 0; --i) std::swap(perm[i], perm[splitmix64(rng) % uint64_t(i + 1)]);
+  const int G = std::max(1, P / 100);
+  const int ng = (P + G - 1) / G;
+  std::vector<std::vector<int>> g(ng);
+  for (int k = 0; k < ng; ++k)
+    for (int m = k * G; m < std::min(P, (k + 1) * G); ++m) g[k].push_back(perm[m]);
+  std::vector<int> order(ng);
+  for (int i = 0; i < ng; ++i) order[i] = i;
+  for (int i = ng - 1; i > 0; --i) std::swap(order[i], order[splitmix64(rng) % uint64_t(i + 1)]);
+  groups.clear();
+  for (int i = 0; i < ng; ++i) groups.push_back(g[order[i]]);
+}
+
+template <typename R> struct MlsState {
+  int N = 0, P = 0;
+  MlsGeometry geo;
+  std::vector<cx<R>> O, Pr;
+  std::vector<R> A;           // sqrt(I), P*N*N
+  std::vector<R> pobj;        // illumination weights (p_object), X*Y
+  R maxIllum = 0;             // Probe::MAX_ILLUM from the set-up (src/Probe.cpp:507-613)
+  double delta_p = 0.1, beta_LSQ = 0.9, beta_object = 1, beta_probe = 1;
+};
+
+// p_object = sum_j |P|^2 placed at the windows (set_projections of aprobe2, src/Probe.cpp:701-729)
+template <typename R> void mls_illumination(MlsState<R>& s, std::vector<R>& out) {
+  const int N = s.N;
+  out.assign(size_t(s.geo.X) * s.geo.Y, R(0));
+  for (int j = 0; j < s.P; ++j)
+    for (int x = 0; x < N; ++x)
+      for (int y = 0; y < N; ++y)
+        out[size_t(s.geo.r0[j] + x) * s.geo.Y + (s.geo.c0[j] + y)] += std::norm(s.Pr[size_t(x) * N + y]);
+}
+
+// initEvo normalisations (src/Probe.cpp:563-608 with h_preCalillum, src/ProbeKernels.cu:697-741), no variable modes.
+template <typename R> void mls_setup(MlsState<R>& s, const std::vector<double>& intensitySums) {
+  const int N = s.N;
+  const size_t NN = size_t(N) * N;
+  std::vector<R> illum;
+  mls_illumination(s, illum);
+  double si = 0, soi = 0;
+  for (size_t i = 0; i < illum.size(); ++i) {
+    si += illum[i];
+    soi += double(std::norm(s.O[i])) * illum[i];
+  }
+  const R onorm = R(std::sqrt(soi / si));
+  for (auto& v : s.O) v *= R(1) / onorm;
+  double sp = 0;
+  for (size_t i = 0; i < NN; ++i) sp += std::norm(s.Pr[i]);
+  const double meanillum = sp / double(NN);
+  std::vector<double> corrv;
+  for (int i = 0; i < s.P; ++i) corrv.push_back(meanillum / (intensitySums[i] / double(NN)));
+  std::sort(corrv.begin(), corrv.end());
+  const size_t n = corrv.size();
+  double corr = (n % 2) ? corrv[n / 2] : 0.5 * (corrv[n / 2 - 1] + corrv[n / 2]);
+  corr = std::sqrt(corr * double(NN));
+  for (auto& v : s.Pr) v *= R(1.0 / corr);
+  s.pobj = illum;
+  for (auto& v : s.pobj) v /= R(corr * corr);
+  s.maxIllum = *std::max_element(s.pobj.begin(), s.pobj.end());
+}
+
+template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool want_err) {
+  const int N = s.N, X = s.geo.X, Y = s.geo.Y;
+  const size_t NN = size_t(N) * N, XY = size_t(X) * Y;
+  // calc_object_norm (src/Probe.cpp:671-699): ||W o O|| / ||W|| over the object ROI, W = p_object
+  {
+    double sw = 0, swo = 0;
+    for (int x = 0; x < s.geo.roinx; ++x)
+      for (int y = 0; y < s.geo.roiny; ++y) {
+        size_t i = size_t(s.geo.roix0 + x) * Y + (s.geo.roiy0 + y);
+        double w = s.pobj[i];
+        sw += w * w;
+        swo += w * w * double(std::norm(s.O[i]));
+      }
+    const R on = sw > 0 ? R(std::sqrt(swo) / std::sqrt(sw)) : R(1);  // empty / unlit ROI: no rescale
+    for (auto& v : s.Pr) v *= on;
+    for (auto& v : s.O) v *= R(1) / on;
+  }
+  // updated_cached_illumination: h_set_projections adds sum |P|^2 at the windows to p_object without clearing it,
+  // then /2, so p_object is a running average (MAX_ILLUM keeps its set-up value)
+  {
+    std::vector<R> il;
+    mls_illumination(s, il);
+    for (size_t i = 0; i < XY; ++i) s.pobj[i] = (s.pobj[i] + il[i]) / R(2);
+  }
+  std::vector<std::vector<int>> groups;
+  mls_groups(rng, s.P, groups);
+  Fft1<R> f(N);
+  std::vector<cx<R>> scr;
+  const R nrm = R(1.0 / double(NN));
+  const R lam = R(std::numeric_limits<float>::epsilon() / double(NN));
+  double errsum = 0;
+  std::vector<cx<R>> S(XY), pum(NN);
+  for (const auto& g : groups) {
+    const int G = int(g.size());
+    std::vector<std::vector<cx<R>>> op(G, std::vector<cx<R>>(NN)), chi(G, std::vector<cx<R>>(NN));
+    for (int k = 0; k < G; ++k) {
+      const int j = g[k];
+      for (int x = 0; x < N; ++x)
+        for (int y = 0; y < N; ++y) {
+          const size_t p = size_t(x) * N + y;
+          op[k][p] = s.O[size_t(s.geo.r0[j] + x) * Y + (s.geo.c0[j] + y)];
+          chi[k][p] = s.Pr[p] * op[k][p];  // get_illumination_probe: psi = P * obj_proj
+        }
+      fft2(f, chi[k].data(), false, scr);
+      const R* A = &s.A[size_t(j) * NN];
+      double e = 0;
+      for (size_t p = 0; p < NN; ++p) {  // modulus_constraint, R = A/(|Psi|+1e-9) - 1 (src/Diffractions.cpp:281-310)
+        const R ap = std::abs(chi[k][p]);
+        e += double(A[p] - ap) * double(A[p] - ap) * 0.25;
+        chi[k][p] *= (A[p] / (ap + R(1e-9)) - R(1));
+      }
+      errsum += std::sqrt(e / double(NN));
+      fft2(f, chi[k].data(), true, scr);
+      for (auto& v : chi[k]) v *= nrm;
+    }
+    // probe direction: mean_j W[window] * chi conj(obj_proj), W = p/(p + 0.01 MAX_ILLUM) (src/MLS.cpp:249-285)
+    std::fill(pum.begin(), pum.end(), cx<R>(0, 0));
+    for (int k = 0; k < G; ++k) {
+      const int j = g[k];
+      for (int x = 0; x < N; ++x)
+        for (int y = 0; y < N; ++y) {
+          const size_t p = size_t(x) * N + y;
+          const R w0 = s.pobj[size_t(s.geo.r0[j] + x) * Y + (s.geo.c0[j] + y)];
+          pum[p] += chi[k][p] * std::conj(op[k][p]) * (w0 / (w0 + s.maxIllum * R(0.01)));
+        }
+    }
+    for (auto& v : pum) v *= R(1.0 / G);
+    // object direction: set_projections of chi conj(P), preconditioned by p + delta_p MAX_ILLUM (src/MLS.cpp:287-347)
+    std::fill(S.begin(), S.end(), cx<R>(0, 0));
+    for (int k = 0; k < G; ++k) {
+      const int j = g[k];
+      for (int x = 0; x < N; ++x)
+        for (int y = 0; y < N; ++y) {
+          const size_t p = size_t(x) * N + y;
+          S[size_t(s.geo.r0[j] + x) * Y + (s.geo.c0[j] + y)] += chi[k][p] * std::conj(s.Pr[p]);
+        }
+    }
+    const R dmax = R(s.maxIllum * s.delta_p);
+    // LSQ step sizes (d_get_optimal_step_lsq, src/utilitiesKernels.cu:444-466, and the 2x2 solve, src/MLS.cpp:349-417)
+    std::vector<double> a1(G), a4(G), b1(G), b2(G);
+    std::vector<cx<double>> a2(G);
+    for (int k = 0; k < G; ++k) {
+      const int j = g[k];
+      double s1 = 0, s4 = 0, t1 = 0, t2 = 0;
+      cx<double> s2(0, 0);
+      for (int x = 0; x < N; ++x)
+        for (int y = 0; y < N; ++y) {
+          const size_t p = size_t(x) * N + y, o = size_t(s.geo.r0[j] + x) * Y + (s.geo.c0[j] + y);
+          const cx<R> oup = S[o] / (s.pobj[o] + dmax);
+          const cx<R> dOP = oup * s.Pr[p], dPO = pum[p] * op[k][p];
+          s1 += double(std::norm(dOP) + lam);
+          s4 += double(std::norm(dPO) + lam);
+          s2 += cx<double>(dOP * std::conj(dPO));
+          t1 += double((std::conj(dOP) * chi[k][p]).real());
+          t2 += double((std::conj(dPO) * chi[k][p]).real());
+        }
+      a1[k] = s1; a4[k] = s4; a2[k] = s2; b1[k] = t1; b2[k] = t2;
+    }
+    double m1 = 0, m4 = 0;
+    for (int k = 0; k < G; ++k) { m1 += a1[k]; m4 += a4[k]; }
+    m1 = 0.1 * m1 / G; m4 = 0.1 * m4 / G;
+    cx<double> bo(0, 0), bp(0, 0);
+    for (int k = 0; k < G; ++k) {
+      const double A11 = a1[k] + m1, A22 = a4[k] + m4;
+      const cx<double> A12 = a2[k], A21 = std::conj(a2[k]);
+      const cx<double> det = A11 * A22 - A12 * A21;
+      const cx<double> x0 = (b1[k] * A22 - A12 * b2[k]) / det;
+      const cx<double> x1 = (A11 * b2[k] - A21 * b1[k]) / det;
+      bo += x0 * (s.beta_object * s.beta_LSQ);
+      bp += x1 * (s.beta_probe * s.beta_LSQ);
+    }
+    bo /= double(G); bp /= double(G);
+    // update_object / update_probe with the group-mean steps (src/Sample.cpp:277-331, src/Probe.cpp:1339-1364)
+    const cx<R> bor(R(bo.real()), R(bo.imag())), bpr(R(bp.real()), R(bp.imag()));
+    for (size_t i = 0; i < XY; ++i)
+      if (S[i] != cx<R>(0, 0)) s.O[i] += bor * (S[i] / (s.pobj[i] + dmax));
+    for (size_t p = 0; p < NN; ++p) s.Pr[p] += bpr * pum[p];
+  }
+  return want_err ? errsum / s.P : 0.0;
+}
+
 }  // namespace
 
 // ============================================================================================================
@@ -710,4 +951,67 @@ double orc_dm_baseline_f32(int N, int P, int X, int Y, const float* amp, const f
   return std::chrono::duration<double>(t1 - t0).count();
 }
 
+// ---- MLs core oracle ----------------------------------------------------------------------------------------
+// raw_pos: 2*P centred pixel positions (x, y) of the ML mesh; intens: P*N*N intensities; probe N*N complex;
+// obj: object (X*Y complex, X/Y from orc_mls_geometry) or NULL for a flat start (ones).
+int orc_mls_geometry(const float* raw_pos, int P, int N, int* XY, int* starts, int* roi) {
+  std::vector<float> raw(raw_pos, raw_pos + 2 * size_t(P));
+  MlsGeometry g = mls_geometry(raw, P, N);
+  XY[0] = g.X; XY[1] = g.Y;
+  for (int i = 0; i < P; ++i) { starts[2 * i] = g.r0[i]; starts[2 * i + 1] = g.c0[i]; }
+  roi[0] = g.roix0; roi[1] = g.roiy0; roi[2] = g.roinx; roi[3] = g.roiny;
+  return 0;
+}
+
+struct OrcMls {
+  MlsState<double> s;
+  uint64_t rng = 0;
+};
+
+void* orc_mls_create(const float* raw_pos, int P, int N, const double* intens, const double* probe, const double* obj,
+                     uint64_t seed, double delta_p) {
+  auto* h = new OrcMls;
+  std::vector<float> raw(raw_pos, raw_pos + 2 * size_t(P));
+  h->s.geo = mls_geometry(raw, P, N);
+  h->s.N = N; h->s.P = P; h->s.delta_p = delta_p;
+  const size_t NN = size_t(N) * N, XY = size_t(h->s.geo.X) * h->s.geo.Y;
+  h->s.A.resize(size_t(P) * NN);
+  std::vector<double> sums(P, 0.0);
+  for (int i = 0; i < P; ++i)
+    for (size_t p = 0; p < NN; ++p) {
+      const double v = intens[size_t(i) * NN + p];
+      sums[i] += v;
+      h->s.A[size_t(i) * NN + p] = std::sqrt(v);
+    }
+  h->s.Pr.resize(NN);
+  for (size_t p = 0; p < NN; ++p) h->s.Pr[p] = cx<double>(probe[2 * p], probe[2 * p + 1]);
+  h->s.O.assign(XY, cx<double>(1, 0));
+  if (obj)
+    for (size_t i = 0; i < XY; ++i) h->s.O[i] = cx<double>(obj[2 * i], obj[2 * i + 1]);
+  mls_setup(h->s, sums);
+  h->rng = seed;
+  return h;
+}
+
+int orc_mls_step(void* hp, double* err) {
+  auto* h = static_cast<OrcMls*>(hp);
+  const double e = mls_iteration(h->s, h->rng, err != nullptr);
+  if (err) *err = e;
+  return 0;
+}
+
+int orc_mls_get(void* hp, double* obj, double* probe, double* scalars) {
+  auto* h = static_cast<OrcMls*>(hp);
+  for (size_t i = 0; i < h->s.O.size(); ++i) { obj[2 * i] = h->s.O[i].real(); obj[2 * i + 1] = h->s.O[i].imag(); }
+  for (size_t i = 0; i < h->s.Pr.size(); ++i) {
+    probe[2 * i] = h->s.Pr[i].real();
+    probe[2 * i + 1] = h->s.Pr[i].imag();
+  }
+  if (scalars) scalars[0] = h->s.maxIllum;
+  return 0;
+}
+
+void orc_mls_destroy(void* hp) { delete static_cast<OrcMls*>(hp); }
+
 }  // extern "C"
+

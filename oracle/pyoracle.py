@@ -50,6 +50,11 @@ def lib():
             "orc_get_psi": ([vp, vp], i),
             "orc_destroy": ([vp], None),
             "orc_dm_baseline_f32": ([i, i, i, i, vp, vp, vp, i, i, vp], d),
+            "orc_mls_geometry": ([vp, i, i, vp, vp, vp], i),
+            "orc_mls_create": ([vp, i, i, vp, vp, vp, u64, d], vp),
+            "orc_mls_step": ([vp, ctypes.POINTER(d)], i),
+            "orc_mls_get": ([vp, vp, vp, vp], i),
+            "orc_mls_destroy": ([vp], None),
         }
         for name, (a, r) in sig.items():
             fn = getattr(L, name)
@@ -168,3 +173,67 @@ def dm_baseline_f32(amp, pos, probe, X, Y, iters, nthreads):
     N = amp.shape[1]
     t = lib().orc_dm_baseline_f32(N, amp.shape[0], X, Y, _p(amp), _p(pos), _p(pr), iters, nthreads, _p(obj))
     return t, obj
+
+
+def mls_raw_positions(nx, ny, stepx, stepy, dx_s, mirror_x=False, mirror_y=False):
+    """Centred Cartesian positions of the ML mesh in pixels, FP32 like src/CartesianScanMesh.cpp:94-177:
+    ((i - (nx-1)/2) * step) * float(1/dx_s), row-major over (i, j), x = row, y = column."""
+    f = np.float32
+    i = np.arange(nx, dtype=f) - f(nx - 1) * f(0.5)
+    j = np.arange(ny, dtype=f) - f(ny - 1) * f(0.5)
+    if mirror_x:
+        i = -i
+    if mirror_y:
+        j = -j
+    inv = f(1.0 / dx_s)
+    px = (i * f(stepx)) * inv
+    py = (j * f(stepy)) * inv
+    out = np.zeros((nx, ny, 2), f)
+    out[:, :, 0] = px[:, None]
+    out[:, :, 1] = py[None, :]
+    return out.reshape(-1, 2)
+
+
+def mls_geometry(raw_pos, N):
+    """ML-mesh geometry from centred pixel positions: (X, Y), window starts (P, 2), object ROI (x0, y0, nx, ny)."""
+    raw = np.ascontiguousarray(raw_pos, np.float32)
+    P = raw.shape[0]
+    xy = np.zeros(2, np.int32)
+    starts = np.zeros((P, 2), np.int32)
+    roi = np.zeros(4, np.int32)
+    lib().orc_mls_geometry(_p(raw), P, N, _p(xy), _p(starts), _p(roi))
+    return int(xy[0]), int(xy[1]), starts, roi
+
+
+class OracleMls:
+    """FP64 MLs core (groups, preconditioned LSQ-ML, one probe mode), stepped one iteration at a time."""
+
+    def __init__(self, raw_pos, intens, probe, obj=None, seed=0x5EED5EED, delta_p=0.1):
+        self.raw = np.ascontiguousarray(raw_pos, np.float32)
+        self.I = np.ascontiguousarray(intens, np.float64)
+        self.P, self.N = self.I.shape[0], self.I.shape[1]
+        self.X, self.Y, self.starts, self.roi = mls_geometry(self.raw, self.N)
+        pr = np.ascontiguousarray(np.asarray(probe).reshape(self.N, self.N), np.complex128)
+        o = None if obj is None else np.ascontiguousarray(obj, np.complex128)
+        self.h = lib().orc_mls_create(_p(self.raw), self.P, self.N, _p(self.I), _p(pr),
+                                      _p(o) if o is not None else None, seed, delta_p)
+
+    def step(self):
+        e = ctypes.c_double(0)
+        lib().orc_mls_step(self.h, ctypes.byref(e))
+        return e.value
+
+    def state(self):
+        o = np.zeros((self.X, self.Y), np.complex128)
+        p = np.zeros((self.N, self.N), np.complex128)
+        sc = np.zeros(1)
+        lib().orc_mls_get(self.h, _p(o), _p(p), _p(sc))
+        return o, p, sc
+
+    def close(self):
+        if self.h:
+            lib().orc_mls_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

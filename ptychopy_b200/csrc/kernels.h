@@ -30,6 +30,8 @@ cudaError_t reduce_abs_max(const float2* a, size_t n, double* out, cudaStream_t 
 cudaError_t reduce_sum_sq(const float2* a, size_t n, double* out, cudaStream_t st);
 cudaError_t scale_by_inverse(float2* a, size_t n, const double* denom, cudaStream_t st);
 cudaError_t abs2(const float2* a, float* out, size_t n, cudaStream_t st);
+cudaError_t scale_complex(float2* a, size_t n, float s, cudaStream_t st);
+cudaError_t fill_complex(float2* a, size_t n, float2 v, cudaStream_t st);
 // out[p] = sum of plane p (P planes of NN floats), in double: Diffractions::fillSquaredSums.
 cudaError_t plane_sums(const float* a, int P, size_t NN, double* out, cudaStream_t st);
 // Probe::getModalDoubleMax over an intensity cache (K x NN): modal sum when useAll && K>1, else stacked max.

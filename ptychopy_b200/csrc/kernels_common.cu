@@ -240,6 +240,25 @@ cudaError_t probe_modal_max(const float* cache, int K, size_t NN, int useAll, fl
   return cudaGetLastError();
 }
 
+__global__ void k_scale_complex(float2* __restrict__ a, size_t n, float s) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    a[i] = cscale(a[i], s);
+}
+
+cudaError_t scale_complex(float2* a, size_t n, float s, cudaStream_t st) {
+  k_scale_complex<<<reduce_grid(n), 256, 0, st>>>(a, n, s);
+  return cudaGetLastError();
+}
+
+__global__ void k_fill_complex(float2* __restrict__ a, size_t n, float2 v) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) a[i] = v;
+}
+
+cudaError_t fill_complex(float2* a, size_t n, float2 v, cudaStream_t st) {
+  k_fill_complex<<<reduce_grid(n), 256, 0, st>>>(a, n, v);
+  return cudaGetLastError();
+}
+
 __global__ void k_plane_sums(const float* __restrict__ a, size_t NN, double* __restrict__ out) {
   const float* pl = a + size_t(blockIdx.x) * NN;
   double s = 0;

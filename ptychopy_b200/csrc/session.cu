@@ -13,6 +13,7 @@
 
 #include "kernels.h"
 #include "kernels_epie.h"
+#include "kernels_mls.h"
 #include "session.h"
 
 namespace pty {
@@ -114,6 +115,73 @@ Geometry list_geometry(const std::vector<double>& xy_m, double dx_s, int N, bool
   return g;
 }
 
+// Raw (centred, not shifted) Cartesian positions of the ML mesh: the same FP32 formula as cartesian_geometry.
+std::vector<float> raw_cartesian_positions(int nx, int ny, double stepx, double stepy, double dx_s, bool mirrorX,
+                                           bool mirrorY) {
+  const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
+  std::vector<float> raw(2 * size_t(nx) * ny);
+  const float mdx = float(nx - 1) * 0.5f, mdy = float(ny - 1) * 0.5f;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      volatile float dx = mirrorX ? (mdx - float(i)) : (float(i) - mdx);
+      volatile float vx = float(dx) * sx;
+      volatile float dy = mirrorY ? (mdy - float(j)) : (float(j) - mdy);
+      volatile float vy = float(dy) * sy;
+      volatile float px = float(vx) * inv, py = float(vy) * inv;
+      raw[2 * (size_t(i) * ny + j)] = px;
+      raw[2 * (size_t(i) * ny + j) + 1] = py;
+    }
+  return raw;
+}
+
+MlsGeometry mls_geometry(const std::vector<float>& raw, int N) {
+  const int P = int(raw.size() / 2);
+  float mnx = std::numeric_limits<float>::max(), mny = mnx, mxx = -mnx, mxy = -mnx;
+  for (int i = 0; i < P; ++i) {
+    mnx = std::min(mnx, raw[2 * i]);
+    mxx = std::max(mxx, raw[2 * i]);
+    mny = std::min(mny, raw[2 * i + 1]);
+    mxy = std::max(mxy, raw[2 * i + 1]);
+  }
+  // the extent loop works in a 1e5-wide frame; note its x bounds come from the positions' y and vice versa
+  const float frame = std::ceil(1e5f * 1.0f / 2 - float(N) * 1.0f / 2);
+  const float cx = (mxx + mnx) / 2, cy = (mxy + mny) / 2;
+  long long lox = 1LL << 40, hix = -1, loy = 1LL << 40, hiy = -1;
+  for (int i = 0; i < P; ++i) {
+    const long long tx = (long long)std::round(raw[2 * i + 1] - cy + frame);
+    lox = std::min(lox, tx - 1);
+    hix = std::max(hix, tx + N - 2);
+    const long long ty = (long long)std::round(raw[2 * i] - cx + frame);
+    loy = std::min(loy, ty - 1);
+    hiy = std::max(hiy, ty + N - 2);
+  }
+  MlsGeometry g;
+  g.X = int(std::ceil(double(float(hix - lox) * (1 + 0.2f))));
+  g.Y = int(std::ceil(double(float(hiy - loy) * (1 + 0.2f))));
+  const float ox = std::ceil(float(g.X) * 1.0f / 2 - float(N) * 1.0f / 2);
+  const float oy = std::ceil(float(g.Y) * 1.0f / 2 - float(N) * 1.0f / 2);
+  g.r0.resize(P);
+  g.c0.resize(P);
+  for (int i = 0; i < P; ++i) {
+    g.r0[i] = int(std::round(raw[2 * i] + ox)) - 1;
+    g.c0[i] = int(std::round(raw[2 * i + 1] + oy)) - 1;
+  }
+  const long long ax = (long long)std::round(g.X * 0.5 + mnx), bx = (long long)std::round(g.X * 0.5 + mxx) - 1;
+  const long long ay = (long long)std::round(g.Y * 0.5 + mny), by = (long long)std::round(g.Y * 0.5 + mxy) - 1;
+  g.roi[0] = int(ax - 1);
+  g.roi[1] = int(ay - 1);
+  g.roi[2] = int(bx - ax + 1);
+  g.roi[3] = int(by - ay + 1);
+  // kept inside the object (the reference indexes it unchecked); an empty range stays empty
+  for (int a = 0; a < 2; ++a) {
+    const int len = a == 0 ? g.X : g.Y;
+    const int end = std::min(len, g.roi[a] + std::max(g.roi[a + 2], 0));
+    g.roi[a] = std::max(0, std::min(g.roi[a], len));
+    g.roi[a + 2] = std::max(0, end - g.roi[a]);
+  }
+  return g;
+}
+
 uint64_t splitmix64(uint64_t& s) {
   uint64_t z = (s += 0x9E3779B97F4A7C15ull);
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -140,6 +208,17 @@ struct EpieState {
   int* order_h = nullptr;  // pinned
   ~EpieState() {
     if (order_h) cudaFreeHost(order_h);
+  }
+};
+
+// Device state of the MLs core.
+struct MlsState {
+  MlsGeometry geo;
+  DeviceBuf pobj, S, pum, objp, psi, work, starts, members, gsize, bbox, sums, errk, betas, err, norms, maxill;
+  int Gmax = 1, ng = 1;
+  cudaGraphExec_t graph = nullptr;
+  ~MlsState() {
+    if (graph) cudaGraphExecDestroy(graph);
   }
 };
 
@@ -434,6 +513,206 @@ void init_dm(pty_session* s) {
   check_cuda(cudaStreamSynchronize(s->stream), "DM init");
 }
 
+// MLs set-up: ML-mesh geometry, sqrt of the intensities, probe (given or the guess), flat or given object, and the
+// initEvo normalisations (src/Probe.cpp:507-613): object scaled by sqrt(sum |O|^2 illum / sum illum), probe by
+// 1/corr with corr = sqrt(median_i(mean|P|^2 / (sum I_i / N^2)) * N^2), p_object = illum / corr^2, MAX_ILLUM.
+void init_mls(pty_session* s) {
+  const pty_params& p = s->prm;
+  need(s->K == 1, "the MLs core supports one probe mode (probeModes=1)", PTY_ERR_UNSUPPORTED);
+  auto* ml = new MlsState;
+  s->ml = ml;
+  const int N = s->N, P = s->P;
+  const size_t NN = size_t(N) * N;
+  const double dx_s = sample_pixel_size(p.lambd, p.z, p.dx_d, N);
+  std::vector<float> raw;
+  if (!s->pos_m.empty()) {
+    const float inv = float(1.0 / dx_s);
+    raw.resize(2 * size_t(P));
+    for (int i = 0; i < 2 * P; ++i) raw[i] = float(s->pos_m[i]) * inv;
+  } else {
+    need(p.spiralScan == 0 && p.lf[0] == 0 && p.jitterRadius == 0, "MLs supports Cartesian or listed positions",
+         PTY_ERR_UNSUPPORTED);
+    raw = raw_cartesian_positions(p.scanDimsx, p.scanDimsy, p.stepx, p.stepy, dx_s, p.mirror1stScanAxis != 0,
+                                  p.mirror2ndScanAxis != 0);
+  }
+  ml->geo = mls_geometry(raw, N);
+  const int gX = s->X, gY = s->Y;
+  s->X = ml->geo.X;
+  s->Y = ml->geo.Y;
+  if (!s->obj_h.empty()) need(gX == s->X && gY == s->Y, "objectNP shape differs from the MLs object size");
+  std::vector<int2> st(P);
+  for (int i = 0; i < P; ++i) {
+    need(ml->geo.r0[i] >= 0 && ml->geo.c0[i] >= 0 && ml->geo.r0[i] + N <= s->X && ml->geo.c0[i] + N <= s->Y,
+         "MLs window " + std::to_string(i) + " lies outside the object");
+    st[i] = make_int2(ml->geo.r0[i], ml->geo.c0[i]);
+  }
+  s->geo.pos.assign(raw.begin(), raw.end());
+  ml->starts.alloc(sizeof(int2) * P, "MLs starts");
+  check_cuda(cudaMemcpyAsync(ml->starts.p, st.data(), sizeof(int2) * P, cudaMemcpyHostToDevice, s->stream), "H2D");
+  // intensity sums (Diffractions::fillSquaredSums) then amplitudes = sqrt(I) (Diffractions::squaredRoot)
+  DeviceBuf sq;
+  sq.alloc(sizeof(double) * P, "sums");
+  check_cuda(plane_sums(s->amp.as<float>(), P, NN, sq.as<double>(), s->stream), "intensity sums");
+  std::vector<double> isum(P);
+  check_cuda(cudaMemcpyAsync(isum.data(), sq.p, sizeof(double) * P, cudaMemcpyDeviceToHost, s->stream), "D2H");
+  check_cuda(sqrt_inplace(s->amp.as<float>(), size_t(P) * NN, s->stream), "sqrt");
+  {
+    DeviceBuf avg;
+    if (p.probeGuess[0] == 0 && s->probe_h.empty()) {
+      avg.alloc(sizeof(float) * NN, "mean amplitude");
+      check_cuda(mean_amplitude(s->amp.as<float>(), P, N, avg.as<float>(), s->stream), "mean amplitude");
+    }
+    init_probe(s, avg.as<float>());
+  }
+  const size_t XY = size_t(s->X) * s->Y;
+  s->obj.alloc(sizeof(float2) * XY, "object");
+  if (!s->obj_h.empty())
+    check_cuda(cudaMemcpyAsync(s->obj.p, s->obj_h.data(), sizeof(float2) * XY, cudaMemcpyHostToDevice, s->stream),
+               "H2D object");
+  else
+    check_cuda(fill_complex(s->obj.as<float2>(), XY, make_float2(1.f, 0.f), s->stream), "flat object");
+  ml->pobj.alloc(sizeof(float) * XY, "illumination");
+  ml->norms.alloc(2 * sizeof(double), "norm sums");
+  ml->maxill.alloc(sizeof(float), "max illumination");
+  check_cuda(cudaMemsetAsync(ml->pobj.p, 0, ml->pobj.bytes, s->stream), "memset");
+  check_cuda(mls_illum_add(ml->pobj.as<float>(), s->probe.as<float2>(), ml->starts.as<int2>(), P, N, s->Y, 1.f,
+                           s->stream),
+             "illumination");
+  check_cuda(mls_norm_sums(ml->pobj.as<float>(), s->obj.as<float2>(), s->Y, 0, 0, s->X, s->Y, 0, ml->norms.as<double>(),
+                           s->stream),
+             "object norm");
+  check_cuda(scale_by_norm(s->obj.as<float2>(), XY, ml->norms.as<double>(), 1, s->stream), "object norm");
+  DeviceBuf d;
+  d.alloc(sizeof(double), "sum");
+  check_cuda(reduce_sum_sq(s->probe.as<float2>(), NN, d.as<double>(), s->stream), "probe power");
+  double psum = 0;
+  check_cuda(cudaMemcpyAsync(&psum, d.p, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "D2H");
+  check_cuda(cudaStreamSynchronize(s->stream), "MLs set-up");
+  const double meanillum = psum / double(NN);
+  std::vector<double> corrv(P);
+  for (int i = 0; i < P; ++i) corrv[i] = meanillum / (isum[i] / double(NN));
+  std::sort(corrv.begin(), corrv.end());
+  double corr = (P % 2) ? corrv[P / 2] : 0.5 * (corrv[P / 2 - 1] + corrv[P / 2]);
+  corr = std::sqrt(corr * double(NN));
+  check_cuda(scale_complex(s->probe.as<float2>(), NN, float(1.0 / corr), s->stream), "probe scale");
+  check_cuda(scale_real(ml->pobj.as<float>(), XY, float(1.0 / (corr * corr)), s->stream), "illumination scale");
+  check_cuda(max_real(ml->pobj.as<float>(), XY, ml->maxill.as<float>(), s->stream), "MAX_ILLUM");
+  // group buffers
+  ml->Gmax = std::max(1, P / 100);
+  ml->ng = (P + ml->Gmax - 1) / ml->Gmax;
+  const size_t GN = size_t(ml->Gmax) * NN;
+  ml->S.alloc(sizeof(float2) * XY, "S");
+  ml->pum.alloc(sizeof(float2) * NN, "probe direction");
+  ml->objp.alloc(sizeof(float2) * GN, "windows");
+  ml->psi.alloc(sizeof(float2) * GN, "exit waves");
+  ml->work.alloc(sizeof(float2) * GN, "FFT work");
+  ml->members.alloc(sizeof(int) * ml->ng * ml->Gmax, "groups");
+  ml->gsize.alloc(sizeof(int) * ml->ng, "group sizes");
+  ml->bbox.alloc(sizeof(int) * 4 * ml->ng, "group boxes");
+  ml->sums.alloc(sizeof(double) * 6 * ml->Gmax, "LSQ sums");
+  ml->errk.alloc(sizeof(double) * ml->Gmax, "errors");
+  ml->betas.alloc(sizeof(double) * 4, "steps");
+  ml->err.alloc(sizeof(double), "error");
+  for (DeviceBuf* b : {&ml->S, &ml->pum, &ml->sums, &ml->errk})
+    check_cuda(cudaMemsetAsync(b->p, 0, b->bytes, s->stream), "memset");
+  check_cuda(cudaStreamSynchronize(s->stream), "MLs set-up");
+}
+
+MlsBuffers mls_buffers(pty_session* s) {
+  MlsState* ml = s->ml;
+  MlsBuffers b;
+  b.obj = s->obj.as<float2>();
+  b.probe = s->probe.as<float2>();
+  b.amp = s->amp.as<float>();
+  b.pobj = ml->pobj.as<float>();
+  b.S = ml->S.as<float2>();
+  b.pum = ml->pum.as<float2>();
+  b.objp = ml->objp.as<float2>();
+  b.psi = ml->psi.as<float2>();
+  b.work = ml->work.as<float2>();
+  b.starts = ml->starts.as<int2>();
+  b.members = ml->members.as<int>();
+  b.gsize = ml->gsize.as<int>();
+  b.bbox = ml->bbox.as<int>();
+  b.sums = ml->sums.as<double>();
+  b.errk = ml->errk.as<double>();
+  b.betas = ml->betas.as<double>();
+  b.err = ml->err.as<double>();
+  b.normsums = ml->norms.as<double>();
+  b.maxIllum = ml->maxill.as<float>();
+  b.tw = s->tw.as<float2>();
+  for (int i = 0; i < 4; ++i) b.roi[i] = ml->geo.roi[i];
+  b.N = s->N;
+  b.P = s->P;
+  b.X = s->X;
+  b.Y = s->Y;
+  b.Gmax = ml->Gmax;
+  b.delta_p = float(s->prm.delta_p);
+  b.beta_obj = 1.0 * 0.9;    // beta_object * beta_LSQ (src/Parameters.h:158-165 defaults)
+  b.beta_probe = 1.0 * 0.9;  // beta_probe * beta_LSQ
+  return b;
+}
+
+// One MLs iteration: the iteration's random groups (a SplitMix64 permutation cut into groups of max(1, P/100), in a
+// second shuffled order) are written to the device tables, then the iteration graph replays.
+double step_mls(pty_session* s, bool want_err) {
+  MlsState* ml = s->ml;
+  const int P = s->P, G = ml->Gmax, N = s->N;
+  std::vector<int> perm(P);
+  for (int i = 0; i < P; ++i) perm[i] = i;
+  for (int i = P - 1; i > 0; --i) std::swap(perm[i], perm[splitmix64(s->rng) % uint64_t(i + 1)]);
+  std::vector<int> order(ml->ng);
+  for (int i = 0; i < ml->ng; ++i) order[i] = i;
+  for (int i = ml->ng - 1; i > 0; --i) std::swap(order[i], order[splitmix64(s->rng) % uint64_t(i + 1)]);
+  std::vector<int> mem(size_t(ml->ng) * G, -1), gs(ml->ng), box(4 * size_t(ml->ng));
+  for (int gi = 0; gi < ml->ng; ++gi) {
+    const int g = order[gi];
+    const int lo = g * G, hi = std::min(P, (g + 1) * G);
+    gs[gi] = hi - lo;
+    int x0 = s->X, y0 = s->Y, x1 = 0, y1 = 0;
+    for (int m = lo; m < hi; ++m) {
+      const int j = perm[m];
+      mem[size_t(gi) * G + (m - lo)] = j;
+      x0 = std::min(x0, ml->geo.r0[j]);
+      y0 = std::min(y0, ml->geo.c0[j]);
+      x1 = std::max(x1, ml->geo.r0[j] + N);
+      y1 = std::max(y1, ml->geo.c0[j] + N);
+    }
+    box[4 * gi] = x0;
+    box[4 * gi + 1] = y0;
+    box[4 * gi + 2] = x1 - x0;
+    box[4 * gi + 3] = y1 - y0;
+  }
+  check_cuda(cudaStreamSynchronize(s->stream), "group table reuse");
+  check_cuda(cudaMemcpyAsync(ml->members.p, mem.data(), sizeof(int) * mem.size(), cudaMemcpyHostToDevice, s->stream),
+             "H2D groups");
+  check_cuda(cudaMemcpyAsync(ml->gsize.p, gs.data(), sizeof(int) * gs.size(), cudaMemcpyHostToDevice, s->stream),
+             "H2D groups");
+  check_cuda(cudaMemcpyAsync(ml->bbox.p, box.data(), sizeof(int) * box.size(), cudaMemcpyHostToDevice, s->stream),
+             "H2D groups");
+  check_cuda(cudaMemsetAsync(ml->err.p, 0, sizeof(double), s->stream), "memset");
+  if (!ml->graph) {
+    const MlsBuffers b = mls_buffers(s);
+    cudaGraph_t graph = nullptr;
+    check_cuda(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    const cudaError_t e = mls_iteration(b, ml->ng, s->stream);
+    const cudaError_t e2 = cudaStreamEndCapture(s->stream, &graph);
+    check_cuda(e, "MLs capture");
+    check_cuda(e2, "end capture");
+    const cudaError_t e3 = cudaGraphInstantiate(&ml->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    check_cuda(e3, "graph instantiate");
+  }
+  check_cuda(cudaGraphLaunch(ml->graph, s->stream), "MLs graph launch");
+  s->launches += mls_launches_per_iteration(ml->ng);
+  // the tables above are pageable host copies: wait before they go out of scope
+  double e = 0;
+  if (want_err && s->prm.calculateRMS)
+    check_cuda(cudaMemcpyAsync(&e, ml->err.p, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "D2H error");
+  check_cuda(cudaStreamSynchronize(s->stream), "MLs iteration");
+  return want_err && s->prm.calculateRMS ? e / P : 0.0;
+}
+
 DMBuffers dm_buffers(pty_session* s) {
   DMBuffers b;
   b.psi = s->psi.as<float2>();
@@ -573,6 +852,8 @@ void destroy_session(pty_session* s) {
     if (g) cudaGraphExecDestroy(g);
   delete s->ep;
   s->ep = nullptr;
+  delete s->ml;
+  s->ml = nullptr;
   s->amp.free();
   s->obj.free();
   s->probe.free();
@@ -722,7 +1003,6 @@ int pty_init(pty_session* s) {
     need(s != nullptr, "null session");
     need(!s->initialized, "session already initialised", PTY_ERR_STATE);
     need(s->have_patterns, "no diffraction patterns (diffractionNP) were given", PTY_ERR_STATE);
-    need(s->algo != ALGO_MLS, "MLs is not available in this build", PTY_ERR_UNSUPPORTED);
     set_device(s);
     const pty_params& p = s->prm;
     if (s->pos_m.empty())
@@ -731,16 +1011,21 @@ int pty_init(pty_session* s) {
                std::to_string(p.scanDimsx * p.scanDimsy));
     else
       need(int(s->pos_m.size() / 2) == s->P, "positionNP and diffractionNP have different lengths");
+    float2* twp = nullptr;
+    check_cuda(make_twiddles(s->N, &twp, s->stream), "twiddles");
+    s->tw.p = twp;
+    s->tw.bytes = sizeof(float2) * s->N;
+    if (s->algo == ALGO_MLS) {
+      init_mls(s);
+      s->initialized = true;
+      return;
+    }
     const int gX = s->X, gY = s->Y;
     init_geometry(s);
     if (!s->obj_h.empty())
       need(gX == s->X && gY == s->Y, "objectNP shape (" + std::to_string(gX) + ", " + std::to_string(gY) +
                                          ") differs from the scan's object size (" + std::to_string(s->X) + ", " +
                                          std::to_string(s->Y) + ")");
-    float2* twp = nullptr;
-    check_cuda(make_twiddles(s->N, &twp, s->stream), "twiddles");
-    s->tw.p = twp;
-    s->tw.bytes = sizeof(float2) * s->N;
     s->dOffs.alloc(sizeof(int) * 2 * s->P, "offsets");
     check_cuda(cudaMemcpyAsync(s->dOffs.p, s->offs.data(), sizeof(int) * 2 * s->P, cudaMemcpyHostToDevice, s->stream),
                "H2D offsets");
@@ -779,6 +1064,8 @@ int pty_step(pty_session* s, double* err) {
     double e = 0;
     if (s->algo == ALGO_EPIE)
       e = step_epie(s, it, err != nullptr);
+    else if (s->algo == ALGO_MLS)
+      e = step_mls(s, err != nullptr);
     else
       step_dm(s, it);
     s->iter = it;
@@ -797,6 +1084,8 @@ int pty_run(pty_session* s, int iters, double* errs) {
       double e = 0;
       if (s->algo == ALGO_EPIE)
         e = step_epie(s, it, errs != nullptr);
+      else if (s->algo == ALGO_MLS)
+        e = step_mls(s, errs != nullptr);
       else
         step_dm(s, it);
       s->iter = it;

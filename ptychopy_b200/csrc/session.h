@@ -46,6 +46,19 @@ struct DeviceBuf {
 };
 
 struct EpieState;  // device state of the persistent ePIE kernel (kernels_epie.cu)
+struct MlsState;   // device state of the MLs core (kernels_mls.cu)
+
+// ML-mesh geometry (src/CartesianScanMesh.cpp:94-177, src/IPtychoScanMesh.cpp:123-184): object ceil(extent * 1.2)
+// per axis, window starts round(pos + ceil(X/2 - N/2)) - 1 from the raw centred positions, and the object ROI that
+// calc_object_norm uses.
+struct MlsGeometry {
+  int X = 0, Y = 0;
+  std::vector<int> r0, c0;
+  int roi[4] = {0, 0, 0, 0};  // x0, y0, nx, ny (0-based)
+};
+MlsGeometry mls_geometry(const std::vector<float>& raw, int N);
+std::vector<float> raw_cartesian_positions(int nx, int ny, double stepx, double stepy, double dx_s, bool mirrorX,
+                                           bool mirrorY);
 
 }  // namespace pty
 
@@ -81,6 +94,8 @@ struct pty_session {
   cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
   // ePIE
   pty::EpieState* ep = nullptr;
+  // MLs
+  pty::MlsState* ml = nullptr;
   uint64_t rng = 0;
   double objMax0 = 0, probeMax0 = 1;
   bool useAll = false, modesInitialized = false;

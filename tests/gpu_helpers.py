@@ -28,3 +28,24 @@ def gpu_session(d, probe=None, obj=None, **params):
         s.set_object(obj)
     s.init()
     return s
+
+
+def mls_dataset(oracle, N=64, nx=5, step=40e-9, seed=3, pert=0.1):
+    """Noise-free MLs case on the ML mesh: intensities |FFT2(P O_true[window])|^2 at the ML window starts, the
+    start object O_true with a smooth perturbation of relative size `pert`.  Data consistent with the model keep
+    |Psi| far above FFT round-off wherever the data are non-zero, so FP32 and FP64 runs stay within round-off of each
+    other; with Poisson data and a flat start the modulus step A/(|Psi| + 1e-9) turns the round-off phase of
+    near-zero Psi into O(1) differences."""
+    rng = np.random.default_rng(seed)
+    lambd, z, dx_d = 2.48e-10, 1.0, 172e-6
+    dx_s = synth.sample_pixel(lambd, z, dx_d, N)
+    raw = oracle.mls_raw_positions(nx, nx, step, step, dx_s)
+    X, Y, starts, roi = oracle.mls_geometry(raw, N)
+    o_true = synth.make_object(X, Y, rng, corr_px=4.0).astype(np.complex128)
+    probe = synth.make_probe(N, dx_s, K=1, fwhm=10 * dx_s)[0].astype(np.complex128)
+    intens = np.stack([np.abs(np.fft.fft2(probe * o_true[r:r + N, c:c + N])) ** 2 for r, c in starts])
+    o0 = (o_true * (1 + pert * synth.make_object(X, Y, rng, corr_px=8.0) - pert)).astype(np.complex64)
+    kw = dict(size=N, scanDimsx=nx, scanDimsy=nx, stepx=step, stepy=step, lambd=lambd, z=z, dx_d=dx_d,
+              beamSize=10 * dx_s, probeModes=1, algorithm="MLs")
+    return dict(intens=intens.astype(np.float32), raw=raw, X=X, Y=Y, starts=starts, roi=roi, obj=o0,
+                probe=probe.astype(np.complex64), dx_s=dx_s, kw=kw)

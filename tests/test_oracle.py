@@ -147,3 +147,33 @@ def test_probe_guess_matches_mean_amplitude(oracle):
     avg = amp.mean(0)
     ratio = F / avg
     assert ratio.std() / ratio.mean() < 1e-10
+
+
+def test_mls_geometry_holds_every_window(oracle):
+    import math
+
+    from ptychopy_b200 import synth
+
+    N = 64
+    dx_s = synth.sample_pixel(2.48e-10, 1.0, 172e-6, N)
+    raw = oracle.mls_raw_positions(7, 5, 40e-9, 55e-9, dx_s)
+    assert raw.dtype == np.float32 and raw.shape == (35, 2)
+    assert abs(raw[:, 0].mean()) < 1e-4 and abs(raw[:, 1].mean()) < 1e-4
+    X, Y, starts, roi = oracle.mls_geometry(raw, N)
+    # object = ceil(1.2 * extent); the extent of axis x is measured on the positions' y and vice versa
+    ext_x = np.round(raw[:, 1]).max() - np.round(raw[:, 1]).min() + N - 1
+    ext_y = np.round(raw[:, 0]).max() - np.round(raw[:, 0]).min() + N - 1
+    assert abs(X - math.ceil(1.2 * ext_x)) <= 1 and abs(Y - math.ceil(1.2 * ext_y)) <= 1
+    assert starts.min() >= 0 and (starts[:, 0] + N).max() <= X and (starts[:, 1] + N).max() <= Y
+    assert roi[2] > 0 and roi[3] > 0 and roi[0] >= 0 and roi[1] >= 0
+
+
+def test_mls_oracle_reduces_the_fourier_error(oracle):
+    from gpu_helpers import dataset
+
+    d = dataset(N=32, nx=6, algorithm="MLs")
+    intens = d["amp"].astype(np.float64) ** 2
+    raw = oracle.mls_raw_positions(6, 6, d["kw"]["stepx"], d["kw"]["stepy"], d["dx_s"])
+    m = oracle.OracleMls(raw, intens, d["probe"][0])
+    errs = [m.step() for _ in range(8)]
+    assert np.isfinite(errs).all() and errs[-1] < 0.8 * errs[0]
