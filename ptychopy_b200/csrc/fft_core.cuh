@@ -205,6 +205,102 @@ __device__ __forceinline__ void fft_vec(float2 (&v)[FftShape<L>::E], int t, floa
   __syncwarp();
 }
 
+// ---- column transforms across a CTA ----------------------------------------------------------------------
+// A CTA of T*CB threads transforms CB adjacent columns of a row-major L x L plane along the first index.
+// Thread (s, c) holds column c at rows s + T*e (e < E), so every register load or store of the CTA touches CB
+// consecutive elements of 32/CB rows (coalesced) and stage 1 (E-point DFT over e) needs no data movement; the
+// exchange between the stages goes through `xch` (E x PK float2, PK = T*CB + 8: conflict-free for the stage-1
+// writes and the stage-2 reads).  The stage-1 twiddle depends on s only.  On return the thread holds the transform
+// at rows s + T*e in v[out_slot<L>(e)], the same index set it loaded, so forward -> pointwise -> inverse chains
+// with no extra data movement.  Starts with __syncthreads (so xch may be reused back to back); a caller that
+// reuses xch for anything else syncs first.
+template <int L>
+__host__ __device__ constexpr int cols_per_block() {
+  return FftShape<L>::T == 32 ? 8 : FftShape<L>::T == 16 ? 16 : (L < 32 ? L : 32);
+}
+template <int L>
+__host__ __device__ constexpr int cols_pitch() {
+  return FftShape<L>::T * cols_per_block<L>() + 8;
+}
+template <int L>
+__host__ __device__ constexpr int cols_threads() {
+  return FftShape<L>::T * cols_per_block<L>();
+}
+template <int L>
+__host__ __device__ constexpr int cols_xch_elems() {
+  return FftShape<L>::E * cols_pitch<L>();
+}
+
+// Thread -> (s, c) of a column CTA.  With T = 32 (CB = 8, four s per warp) the warp takes s in {2w, 2w+1, 2w+16,
+// 2w+17}, so the two lanes of a stage-2 pair (s and s+16) read the same exchange words in one instruction
+// (broadcast) while loads and stores still cover 64-byte row segments.
+template <int L>
+__device__ __forceinline__ void cols_thread(int tid, int& s, int& c) {
+  constexpr int CB = cols_per_block<L>();
+  c = tid % CB;
+  const int j = tid / CB;
+  if constexpr (FftShape<L>::Q == 2) {
+    static_assert(CB == 8 && FftShape<L>::T == 32, "pair mapping assumes four s per warp");
+    s = (j >> 2) * 2 + (j & 1) + 16 * ((j >> 1) & 1);
+  } else {
+    s = j;
+  }
+}
+
+template <int L, bool INV>
+__device__ __forceinline__ void fft_cols(float2 (&v)[FftShape<L>::E], int s, int c, float2* xch,
+                                         const float2* s_tw) {
+  constexpr int T = FftShape<L>::T, E = FftShape<L>::E, M = FftShape<L>::M, Q = FftShape<L>::Q;
+  constexpr int CB = cols_per_block<L>(), PK = cols_pitch<L>();
+  dft_reg<INV>(v);
+  __syncthreads();  // previous readers of xch are done
+  static_for<0, E>([&](auto k1c) {
+    constexpr int k1 = decltype(k1c)::value;
+    constexpr int src = bitrev(k1, E);
+    if constexpr (k1 == 0) {
+      xch[s * CB + c] = v[src];
+    } else {
+      float2 w = s_tw[k1 * T + s];
+      if (INV) w.y = -w.y;
+      xch[k1 * PK + s * CB + c] = cmul(v[src], w);
+    }
+  });
+  __syncthreads();
+  if constexpr (Q == 1) {
+    static_for<0, M>([&](auto mc) {
+      constexpr int m = decltype(mc)::value;
+      const float2* col = xch + (s + T * m) * PK + c;
+      float2 a[T];
+#pragma unroll
+      for (int tt = 0; tt < T; ++tt) a[tt] = col[tt * CB];
+      dft_reg<INV>(a);
+      static_for<0, T>([&](auto k2c) {
+        constexpr int k2 = decltype(k2c)::value;
+        v[m * T + k2] = a[bitrev(k2, T)];
+      });
+    });
+  } else {
+    // s = k1 + E*q: radix-2 DIF over the two halves of the T-point DFT of k1, keeping half q (as in fft_vec)
+    const int k1 = s % E;
+    const bool odd = s >= E;
+    const float sgn = odd ? -1.f : 1.f;
+    const float2* col = xch + k1 * PK + c;
+    float2 a[E];
+    static_for<0, E>([&](auto tc) {
+      constexpr int tp = decltype(tc)::value;
+      const float2 b0 = col[tp * CB], b1 = col[(tp + E) * CB];
+      const float2 d = make_float2(b0.x + sgn * b1.x, b0.y + sgn * b1.y);
+      const float2 dw = twiddle32<tp*(32 / T), INV>(d);
+      a[tp] = odd ? dw : d;
+    });
+    dft_reg<INV>(a);
+    static_for<0, E>([&](auto jc) {
+      constexpr int j = decltype(jc)::value;
+      v[j] = a[bitrev(j, E)];
+    });
+  }
+}
+
 // Register slot of element index n = t + T*e for this lane after fft_vec.
 template <int L>
 __host__ __device__ constexpr int out_slot(int e) {

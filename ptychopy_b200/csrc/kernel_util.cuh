@@ -47,8 +47,8 @@ __device__ __forceinline__ float2 modulus_replace(float2 psi, float amp) {
 // arg <= 0 is kept.  atan2(+0, x<0) = +pi counts as positive.
 __device__ __forceinline__ float2 constrain_phase(float2 v) {
   const bool pos = (v.y > 0.f) || (v.y == 0.f && !signbit(v.y) && v.x < 0.f);
-  if (!pos) return v;
-  return make_float2(sqrtf(v.x * v.x + v.y * v.y), 0.f);
+  const float m = sqrtf(v.x * v.x + v.y * v.y);  // branch-free: both results, then a select
+  return make_float2(pos ? m : v.x, pos ? 0.f : v.y);
 }
 
 __device__ __forceinline__ double warp_reduce_sum(double v) {

@@ -44,7 +44,7 @@ struct DMWave {
 };
 struct DMBuffers {
   float2* psi;          // P x N x N exit waves
-  const float* ampT;    // P x N x N amplitudes, each plane transposed ([ky][kx])
+  const float* amp;     // P x N x N amplitudes, natural layout ([kx][ky])
   float2* obj;          // X x Y
   float2* probe;        // K x N x N (mode 0 used)
   float2* dO;           // X x Y increment accumulator

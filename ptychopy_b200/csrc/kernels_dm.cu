@@ -1,18 +1,21 @@
 // Reference DM ("difference map" as ptychopy implements it, src/DM.cu:80-128 with the cuFFT callbacks of
-// src/SampleKernels.cu:416-490) as a three-kernel pipeline per wave of patterns plus a finalize step:
+// src/SampleKernels.cu:416-490) as three kernels per wave of patterns plus a finalize step:
 //
-//   fwd_rows   u = 2*P*O[x+ox][y+oy] - psi[x][y]  (load callback d_calculatePsi), FFT along y,
-//              stored transposed into W1[ky][x]                                   reads psi once from HBM
-//   cols       FFT along x (now contiguous), D = Psi' - Psi/N^2 with Psi' = A*Psi/|Psi|/N^2 (store callback
-//              d_modulusConstraint), inverse FFT along x, stored transposed into W2[x][ky]  reads A once
-//   inv_rows   inverse FFT along y gives psi_new = IFFT2(D) = psi + IFFT2(Psi') - 2*P*O (store callback
-//              d_updateObject), writes psi, and accumulates the object / probe increments   writes psi once
+//   rows   u = 2*P*O[x+ox][y+oy] - psi[x][y]  (load callback d_calculatePsi), FFT along y (one warp per row),
+//          W1[x][ky] row-major                                                  reads psi once from HBM
+//   cols   FFT along x of CB adjacent columns per CTA (fft_cols: coalesced row segments, no transpose),
+//          D = Psi' - Psi/N^2 with Psi' = A*Psi/|Psi|/N^2 (store callback d_modulusConstraint), inverse FFT along x,
+//          W2[x][ky] row-major                                                  reads A once
+//   inv    inverse FFT along y gives psi_new = IFFT2(D) = psi + IFFT2(Psi') - 2*P*O (store callback
+//          d_updateObject), writes psi, and accumulates the object / probe increments       writes psi once
 //   finalize   O += dO, P += dP, sums of |O|^2 and |P|^2, the hysteresis-cached factors (src/DM.cu:54-73)
 //
 // psi_new is formed as IFFT2(Psi' - Psi/N^2): by linearity IFFT2(Psi/N^2) = u = 2*P*O - psi, so
 // psi + IFFT2(Psi') - 2*P*O = IFFT2(Psi') - u.  This removes the second read of psi the callback form needs,
-// leaving the algorithmic minimum of HBM traffic, 20*N^2 bytes per pattern: psi read + write, A read.
-// W1/W2 hold one wave (a few tens of MB) and stay in L2 between the kernels.
+// leaving 20*N^2 bytes of algorithmic HBM traffic per pattern: psi read + write, A read.  Every global access is a
+// coalesced row segment and every plane keeps its natural row-major layout.
+//
+// The kernels are persistent (grid = resident CTA slots) and stride over the wave's work items (NB per pattern).
 //
 // Object and probe updates use snapshot semantics: all increments of an iteration are computed from O and P
 // as they were at its start and summed (the reference adds them with atomics while other callbacks still read
@@ -26,32 +29,33 @@
 
 namespace pty {
 
-// CTAs per SM the DM kernels are compiled for (caps registers so that many fit next to their shared memory).
+// CTAs per SM the DM kernels are compiled for (caps registers so that several fit next to their shared memory).
 template <int L> struct DMOcc { static constexpr int MIN_BLOCKS = 4; };
 
-// Work items of a wave: (row block, slot) pairs; CTAs are persistent and stride over them (grid <= resident
-// slots), so a launch has no partially filled last round and CTAs drift out of lock-step (load / FFT overlap).
+// Row and column work items use the same CTA size and item count per pattern for every supported L.
 template <int L>
-__global__ void __launch_bounds__(FftShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
-    k_dm_fwd_rows(const float2* __restrict__ psi, const float2* __restrict__ obj, int objY,
-                  const float2* __restrict__ probe, const int2* __restrict__ offs, const int* __restrict__ slot_pat,
-                  int count, float2* __restrict__ W1, const float2* __restrict__ g_tw) {
+struct DMShape {
+  static constexpr int THREADS = FftShape<L>::THREADS;
+  static constexpr int NB = L / FftShape<L>::RC;
+  static_assert(cols_threads<L>() == THREADS, "row and column items share the CTA size");
+  static_assert(L / cols_per_block<L>() == NB, "row and column items share the item count");
+  static constexpr size_t SMEM_ROWS = sizeof(float2) * (L + FftShape<L>::RC * FftShape<L>::XCH);
+  static constexpr size_t SMEM_COLS = sizeof(float2) * (L + cols_xch_elems<L>());
+  static constexpr size_t SMEM = SMEM_ROWS > SMEM_COLS ? SMEM_ROWS : SMEM_COLS;
+};
+
+// Rows x = sub*R .. sub*R + R-1 of pattern p (W slot `slot`).
+template <int L>
+__device__ __forceinline__ void dm_item_rows(const DMBuffers& b, int p, int slot, int sub, float2* s_x,
+                                             const float2* s_tw) {
   using S = FftShape<L>;
-  constexpr int T = S::T, E = S::E, R = S::RC, NB = L / S::RC;
-  extern __shared__ float4 smem4[];
-  float2* smem = reinterpret_cast<float2*>(smem4);
-  float2* s_tw = smem;
-  float2* s_x = smem + L;
+  constexpr int T = S::T, E = S::E, R = S::RC;
   const int v = threadIdx.x / T, t = threadIdx.x % T;
-  load_twiddles<L>(s_tw, g_tw);
-  for (int item = blockIdx.x; item < NB * count; item += gridDim.x) {
-  const int slot = item / NB;
-  const int p = slot_pat[slot];
-  const int x0 = (item % NB) * R, x = x0 + v;
-  const int2 o = offs[p];
-  const float2* prow = probe + size_t(x) * L;
-  const float2* orow = obj + size_t(x + o.x) * objY + o.y;
-  const float2* srow = psi + (size_t(p) * L + x) * L;
+  const int x = sub * R + v;
+  const int2 o = b.offs[p];
+  const float2* prow = b.probe + size_t(x) * L;
+  const float2* orow = b.obj + size_t(x + o.x) * b.Y + o.y;
+  const float2* srow = b.psi + (size_t(p) * L + x) * L;
   float2 a[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) {
@@ -60,80 +64,66 @@ __global__ void __launch_bounds__(FftShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
     const float2 sv = ld_stream(srow + n);
     a[e] = make_float2(2.f * ph.x - sv.x, 2.f * ph.y - sv.y);
   }
-  __syncthreads();  // twiddles loaded; previous item's staging reads done
   fft_vec<L, false>(a, t, s_x + v * S::XCH, s_tw);
-  store_rows_transposed<L, R>(a, W1 + size_t(slot) * L * L, x0, v, t, s_x);
-  }
+  float2* wrow = b.W1 + (size_t(slot) * L + x) * L;
+  static_for<0, E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    wrow[t + T * e] = a[out_slot<L>(e)];
+  });
 }
 
+// Columns sub*CB .. sub*CB + CB-1 of pattern p: forward FFT along x, modulus, inverse FFT along x.
 template <int L>
-__global__ void __launch_bounds__(FftShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
-    k_dm_cols(const float2* __restrict__ W1, const float* __restrict__ ampT, const int* __restrict__ slot_pat,
-              int count, float2* __restrict__ W2, const float2* __restrict__ g_tw) {
+__device__ __forceinline__ void dm_item_cols(const DMBuffers& b, int p, int slot, int sub, float2* s_x,
+                                             const float2* s_tw) {
   using S = FftShape<L>;
-  constexpr int T = S::T, E = S::E, R = S::RC, NB = L / S::RC;
-  extern __shared__ float4 smem4[];
-  float2* smem = reinterpret_cast<float2*>(smem4);
-  float2* s_tw = smem;
-  float2* s_x = smem + L;
-  const int v = threadIdx.x / T, t = threadIdx.x % T;
-  load_twiddles<L>(s_tw, g_tw);
-  for (int item = blockIdx.x; item < NB * count; item += gridDim.x) {
-  const int slot = item / NB;
-  const int p = slot_pat[slot];
-  const int k0 = (item % NB) * R, ky = k0 + v;
-  const float2* row = W1 + (size_t(slot) * L + ky) * L;
-  const float* arow = ampT + (size_t(p) * L + ky) * L;
+  constexpr int T = S::T, E = S::E, CB = cols_per_block<L>();
+  int s, c;
+  cols_thread<L>(threadIdx.x, s, c);
+  const int col = sub * CB + c;
+  const float2* w1 = b.W1 + size_t(slot) * L * L + col;
+  const float* A = b.amp + size_t(p) * L * L + col;
   float2 a[E];
 #pragma unroll
-  for (int e = 0; e < E; ++e) a[e] = row[t + T * e];
-  __syncthreads();
-  fft_vec<L, false>(a, t, s_x + v * S::XCH, s_tw);
+  for (int e = 0; e < E; ++e) a[e] = w1[size_t(s + T * e) * L];
+  fft_cols<L, false>(a, s, c, s_x, s_tw);
   constexpr float nrm = 1.0f / float(L * L);
   static_for<0, E>([&](auto ec) {
     constexpr int e = decltype(ec)::value;
-    const float A = ld_stream(arow + t + T * e);
-    const float2 psi = a[out_slot<L>(e)];
-    const float2 rep = modulus_replace(psi, A * nrm);
-    a[out_slot<L>(e)] = make_float2(rep.x - psi.x * nrm, rep.y - psi.y * nrm);
+    const float Av = ld_stream(A + size_t(s + T * e) * L);
+    const float2 ps = a[out_slot<L>(e)];
+    const float2 rep = modulus_replace(ps, Av * nrm);
+    a[out_slot<L>(e)] = make_float2(rep.x - ps.x * nrm, rep.y - ps.y * nrm);
   });
   to_input_order<L>(a);
-  fft_vec<L, true>(a, t, s_x + v * S::XCH, s_tw);
-  store_rows_transposed<L, R>(a, W2 + size_t(slot) * L * L, k0, v, t, s_x);
-  }
+  fft_cols<L, true>(a, s, c, s_x, s_tw);
+  float2* w2 = b.W2 + size_t(slot) * L * L + col;
+  static_for<0, E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    w2[size_t(s + T * e) * L] = a[out_slot<L>(e)];
+  });
 }
 
-template <int L>
-__global__ void __launch_bounds__(FftShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
-    k_dm_inv_rows(const float2* __restrict__ W2, float2* __restrict__ psi, const float2* __restrict__ obj, int objY,
-                  const float2* __restrict__ probe, const int2* __restrict__ offs, const int* __restrict__ slot_pat,
-                  int count, float2* __restrict__ dO, float2* __restrict__ dP, const double* __restrict__ fac,
-                  int phaseConstraint, int updateProbe, const float2* __restrict__ g_tw) {
+// Rows of pattern p: inverse FFT along y -> psi_new, psi write, object / probe increments.
+template <int L, bool PC, bool UP>
+__device__ __forceinline__ void dm_item_inv(const DMBuffers& b, int p, int slot, int sub, float2* s_x,
+                                            const float2* s_tw) {
   using S = FftShape<L>;
-  constexpr int T = S::T, E = S::E, R = S::RC, NB = L / S::RC;
-  extern __shared__ float4 smem4[];
-  float2* smem = reinterpret_cast<float2*>(smem4);
-  float2* s_tw = smem;
-  float2* s_x = smem + L;
+  constexpr int T = S::T, E = S::E, R = S::RC;
   const int v = threadIdx.x / T, t = threadIdx.x % T;
-  load_twiddles<L>(s_tw, g_tw);
-  for (int item = blockIdx.x; item < NB * count; item += gridDim.x) {
-  const int slot = item / NB;
-  const int p = slot_pat[slot];
-  const int x = (item % NB) * R + v;
-  const float2* row = W2 + (size_t(slot) * L + x) * L;
+  const int x = sub * R + v;
+  const float2* row = b.W2 + (size_t(slot) * L + x) * L;
   float2 a[E];
 #pragma unroll
   for (int e = 0; e < E; ++e) a[e] = row[t + T * e];
-  __syncthreads();
   fft_vec<L, true>(a, t, s_x + v * S::XCH, s_tw);
-  const float f0 = float(fac[0]), f1 = float(fac[1]);
-  const int2 o = offs[p];
-  const float2* prow = probe + size_t(x) * L;
-  const float2* orow = obj + size_t(x + o.x) * objY + o.y;
-  float2* dorow = dO + size_t(x + o.x) * objY + o.y;
-  float2* psrow = psi + (size_t(p) * L + x) * L;
-  float2* dprow = dP + size_t(x) * L;
+  const float f0 = float(b.fac[0]), f1 = float(b.fac[1]);
+  const int2 o = b.offs[p];
+  const float2* prow = b.probe + size_t(x) * L;
+  const float2* orow = b.obj + size_t(x + o.x) * b.Y + o.y;
+  float2* dorow = b.dO + size_t(x + o.x) * b.Y + o.y;
+  float2* psrow = b.psi + (size_t(p) * L + x) * L;
+  float2* dprow = b.dP + size_t(x) * L;
   static_for<0, E>([&](auto ec) {
     constexpr int e = decltype(ec)::value;
     const int n = t + T * e;
@@ -142,15 +132,49 @@ __global__ void __launch_bounds__(FftShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
     const float2 pv = prow[n];
     float2 inc = cconjmul(pv, pn);
     inc = make_float2(inc.x * f1, inc.y * f1);
-    if (phaseConstraint) inc = constrain_phase(inc);
+    if constexpr (PC) inc = constrain_phase(inc);
     atomicAdd(dorow + n, inc);
-    if (updateProbe) {
+    if constexpr (UP) {
       const float2 ov = orow[n];
-      float2 pi = cconjmul(ov, pn);
+      const float2 pi = cconjmul(ov, pn);
       atomicAdd(dprow + n, make_float2(pi.x * f0, pi.y * f0));
     }
   });
-  }
+}
+
+template <int L>
+__global__ void __launch_bounds__(DMShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
+    k_dm_rows(const DMBuffers b, const DMWave w) {
+  constexpr int NB = DMShape<L>::NB;
+  extern __shared__ float4 smem4[];
+  float2* smem = reinterpret_cast<float2*>(smem4);
+  load_twiddles<L>(smem, b.tw);
+  __syncthreads();
+  for (int item = blockIdx.x; item < NB * w.count; item += gridDim.x)
+    dm_item_rows<L>(b, w.slot_pat[item / NB], item / NB, item % NB, smem + L, smem);
+}
+
+template <int L>
+__global__ void __launch_bounds__(DMShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
+    k_dm_cols(const DMBuffers b, const DMWave w) {
+  constexpr int NB = DMShape<L>::NB;
+  extern __shared__ float4 smem4[];
+  float2* smem = reinterpret_cast<float2*>(smem4);
+  load_twiddles<L>(smem, b.tw);  // visible after fft_cols' first barrier
+  for (int item = blockIdx.x; item < NB * w.count; item += gridDim.x)
+    dm_item_cols<L>(b, w.slot_pat[item / NB], item / NB, item % NB, smem + L, smem);
+}
+
+template <int L, bool PC, bool UP>
+__global__ void __launch_bounds__(DMShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
+    k_dm_inv(const DMBuffers b, const DMWave w) {
+  constexpr int NB = DMShape<L>::NB;
+  extern __shared__ float4 smem4[];
+  float2* smem = reinterpret_cast<float2*>(smem4);
+  load_twiddles<L>(smem, b.tw);
+  __syncthreads();
+  for (int item = blockIdx.x; item < NB * w.count; item += gridDim.x)
+    dm_item_inv<L, PC, UP>(b, w.slot_pat[item / NB], item / NB, item % NB, smem + L, smem);
 }
 
 // O += dO, P += dP (mode 0), reset the accumulators, and sum |O|^2 and |P|^2 over all stacked probe modes.
@@ -202,11 +226,15 @@ __global__ void k_dm_factors(double* __restrict__ sums, double* __restrict__ fac
 
 template <int L>
 static cudaError_t dm_prepare_t() {
-  const int smem = int(rows_smem_bytes<L>());
-  cudaError_t e = cudaFuncSetAttribute(k_dm_fwd_rows<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_dm_cols<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_dm_inv_rows<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  return e;
+  const int sm = int(DMShape<L>::SMEM);
+  const void* fns[6] = {(const void*)k_dm_rows<L>, (const void*)k_dm_cols<L>, (const void*)k_dm_inv<L, false, false>,
+                        (const void*)k_dm_inv<L, false, true>, (const void*)k_dm_inv<L, true, false>,
+                        (const void*)k_dm_inv<L, true, true>};
+  for (const void* f : fns) {
+    const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t dm_prepare(int N) {
@@ -220,52 +248,47 @@ cudaError_t dm_prepare(int N) {
   }
 }
 
+// Resident CTA slots of the DM kernels (once per size; the three share block size and shared memory).
 template <int L>
-static int dm_grid(int items) {
-  static int slots = 0;
-  if (!slots) {
+static int dm_slots() {
+  static const int slots = [] {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_dm_fwd_rows<L>, FftShape<L>::THREADS, rows_smem_bytes<L>());
-    slots = sms * (per > 0 ? per : 1);
-  }
-  return items < slots ? items : slots;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_dm_rows<L>, DMShape<L>::THREADS, DMShape<L>::SMEM);
+    return sms * (per > 0 ? per : 1);
+  }();
+  return slots;
 }
 
 template <int L>
 static cudaError_t dm_wave_t(const DMBuffers& b, const DMWave& w, bool pc, bool up, cudaStream_t st,
                              int64_t* launches) {
-  constexpr int NT = FftShape<L>::THREADS, NB = L / FftShape<L>::RC;
-  const size_t smem = rows_smem_bytes<L>();
-  const int grid = dm_grid<L>(NB * w.count);
-  k_dm_fwd_rows<L><<<grid, NT, smem, st>>>(b.psi, b.obj, b.Y, b.probe, b.offs, w.slot_pat, w.count, b.W1, b.tw);
-  k_dm_cols<L><<<grid, NT, smem, st>>>(b.W1, b.ampT, w.slot_pat, w.count, b.W2, b.tw);
-  k_dm_inv_rows<L><<<grid, NT, smem, st>>>(b.W2, b.psi, b.obj, b.Y, b.probe, b.offs, w.slot_pat, w.count, b.dO, b.dP,
-                                           b.fac, pc ? 1 : 0, up ? 1 : 0, b.tw);
+  constexpr int NT = DMShape<L>::THREADS, NB = DMShape<L>::NB;
+  constexpr size_t SM = DMShape<L>::SMEM;
+  const int grid = std::min(dm_slots<L>(), NB * w.count);
+  k_dm_rows<L><<<grid, NT, SM, st>>>(b, w);
+  k_dm_cols<L><<<grid, NT, SM, st>>>(b, w);
+  if (pc && up)
+    k_dm_inv<L, true, true><<<grid, NT, SM, st>>>(b, w);
+  else if (pc)
+    k_dm_inv<L, true, false><<<grid, NT, SM, st>>>(b, w);
+  else if (up)
+    k_dm_inv<L, false, true><<<grid, NT, SM, st>>>(b, w);
+  else
+    k_dm_inv<L, false, false><<<grid, NT, SM, st>>>(b, w);
   if (launches) *launches += 3;
   return cudaGetLastError();
 }
 
-// Patterns per wave: the largest balanced wave with W1 + W2 within 1 GiB.  The three kernels are bound by their
-// on-chip (L1/shared) traffic, so fewer, larger waves (less launch and tail overhead) beat L2-resident small ones.
-template <int L>
-static int dm_wave_size_t(int P) {
-  const size_t bytes_per_pattern = 2 * sizeof(float2) * size_t(L) * L;
+// Patterns per wave: the largest balanced wave with W1 + W2 within 1 GiB.  The kernels are bound by their on-chip
+// work (shared memory, L1, issue), so fewer, larger waves (less launch and tail overhead) beat L2-resident small
+// ones.
+int dm_wave_size(int N, int P) {
+  const size_t bytes_per_pattern = 2 * sizeof(float2) * size_t(N) * N;
   const int maxwave = int(std::max<size_t>(1, (size_t(1) << 30) / bytes_per_pattern));
   const int nwaves = (P + maxwave - 1) / maxwave;
   return (P + nwaves - 1) / nwaves;
-}
-
-int dm_wave_size(int N, int P) {
-  switch (N) {
-    case 32: return dm_wave_size_t<32>(P);
-    case 64: return dm_wave_size_t<64>(P);
-    case 128: return dm_wave_size_t<128>(P);
-    case 256: return dm_wave_size_t<256>(P);
-    case 512: return dm_wave_size_t<512>(P);
-    default: return 1;
-  }
 }
 
 cudaError_t dm_wave(const DMBuffers& b, const DMWave& w, bool pc, bool up, cudaStream_t st, int64_t* launches) {

@@ -716,7 +716,7 @@ double step_mls(pty_session* s, bool want_err) {
 DMBuffers dm_buffers(pty_session* s) {
   DMBuffers b;
   b.psi = s->psi.as<float2>();
-  b.ampT = s->amp.as<float>();
+  b.amp = s->amp.as<float>();
   b.obj = s->obj.as<float2>();
   b.probe = s->probe.as<float2>();
   b.dO = s->dO.as<float2>();
@@ -1039,8 +1039,9 @@ int pty_init(pty_session* s) {
       init_probe(s, avg.as<float>());
     }
     init_object(s);
-    // amplitudes are consumed column-wise by the column phase: transpose each plane once
-    {
+    // ePIE's column phase consumes the amplitudes column-wise: transpose each plane once (DM reads them in their
+    // natural layout)
+    if (s->algo == ALGO_EPIE) {
       DeviceBuf t;
       t.alloc(s->amp.bytes, "transposed patterns");
       check_cuda(transpose_planes(s->amp.as<float>(), t.as<float>(), s->P, s->N, s->stream), "transpose");
