@@ -231,20 +231,13 @@ __host__ __device__ constexpr int cols_xch_elems() {
   return FftShape<L>::E * cols_pitch<L>();
 }
 
-// Thread -> (s, c) of a column CTA.  With T = 32 (CB = 8, four s per warp) the warp takes s in {2w, 2w+1, 2w+16,
-// 2w+17}, so the two lanes of a stage-2 pair (s and s+16) read the same exchange words in one instruction
-// (broadcast) while loads and stores still cover 64-byte row segments.
+// Thread -> (s, c) of a column CTA: c fastest, so a warp covers 32/CB values of s (for T = 32 all on the same side
+// of the stage-2 lane pairs, which keeps the pair branch warp-uniform and the twiddle reads contiguous).
 template <int L>
 __device__ __forceinline__ void cols_thread(int tid, int& s, int& c) {
   constexpr int CB = cols_per_block<L>();
   c = tid % CB;
-  const int j = tid / CB;
-  if constexpr (FftShape<L>::Q == 2) {
-    static_assert(CB == 8 && FftShape<L>::T == 32, "pair mapping assumes four s per warp");
-    s = (j >> 2) * 2 + (j & 1) + 16 * ((j >> 1) & 1);
-  } else {
-    s = j;
-  }
+  s = tid / CB;
 }
 
 template <int L, bool INV>

@@ -29,8 +29,12 @@
 
 namespace pty {
 
-// CTAs per SM the DM kernels are compiled for (caps registers so that several fit next to their shared memory).
-template <int L> struct DMOcc { static constexpr int MIN_BLOCKS = 4; };
+// CTAs per SM the DM kernels are compiled for (64 registers).  5 CTAs/SM (48 registers: no spills in the row and
+// column kernels) measured slower, 3.30 vs 3.12 ms per 900-pattern iteration at 512^2.
+template <int L> struct DMOcc {
+  static constexpr int MIN_BLOCKS = 4;
+  static constexpr int MIN_BLOCKS_INV = 4;
+};
 
 // Row and column work items use the same CTA size and item count per pattern for every supported L.
 template <int L>
@@ -166,7 +170,7 @@ __global__ void __launch_bounds__(DMShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
 }
 
 template <int L, bool PC, bool UP>
-__global__ void __launch_bounds__(DMShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
+__global__ void __launch_bounds__(DMShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS_INV)
     k_dm_inv(const DMBuffers b, const DMWave w) {
   constexpr int NB = DMShape<L>::NB;
   extern __shared__ float4 smem4[];
@@ -248,17 +252,29 @@ cudaError_t dm_prepare(int N) {
   }
 }
 
-// Resident CTA slots of the DM kernels (once per size; the three share block size and shared memory).
+// Resident CTA slots of a DM kernel (once per kernel and size).
+template <typename K>
+static int resident_slots(K kern, int threads, size_t smem) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem);
+  return sms * (per > 0 ? per : 1);
+}
 template <int L>
-static int dm_slots() {
-  static const int slots = [] {
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_dm_rows<L>, DMShape<L>::THREADS, DMShape<L>::SMEM);
-    return sms * (per > 0 ? per : 1);
-  }();
-  return slots;
+static int dm_slots_rows() {
+  static const int s = resident_slots(k_dm_rows<L>, DMShape<L>::THREADS, DMShape<L>::SMEM);
+  return s;
+}
+template <int L>
+static int dm_slots_cols() {
+  static const int s = resident_slots(k_dm_cols<L>, DMShape<L>::THREADS, DMShape<L>::SMEM);
+  return s;
+}
+template <int L>
+static int dm_slots_inv() {
+  static const int s = resident_slots(k_dm_inv<L, true, true>, DMShape<L>::THREADS, DMShape<L>::SMEM);
+  return s;
 }
 
 template <int L>
@@ -266,9 +282,10 @@ static cudaError_t dm_wave_t(const DMBuffers& b, const DMWave& w, bool pc, bool 
                              int64_t* launches) {
   constexpr int NT = DMShape<L>::THREADS, NB = DMShape<L>::NB;
   constexpr size_t SM = DMShape<L>::SMEM;
-  const int grid = std::min(dm_slots<L>(), NB * w.count);
-  k_dm_rows<L><<<grid, NT, SM, st>>>(b, w);
-  k_dm_cols<L><<<grid, NT, SM, st>>>(b, w);
+  const int items = NB * w.count;
+  const int grid = std::min(dm_slots_inv<L>(), items);
+  k_dm_rows<L><<<std::min(dm_slots_rows<L>(), items), NT, SM, st>>>(b, w);
+  k_dm_cols<L><<<std::min(dm_slots_cols<L>(), items), NT, SM, st>>>(b, w);
   if (pc && up)
     k_dm_inv<L, true, true><<<grid, NT, SM, st>>>(b, w);
   else if (pc)
