@@ -303,7 +303,7 @@ def run_b200(args, rank, world, local):
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": kind,
-                         "kernel": "DM iteration graph (fwd_rows, cols, inv_rows per wave + finalize)",
+                         "kernel": "DM iteration graph (k_dm_rows, k_dm_cols, k_dm_inv per wave + finalize)",
                          "algorithmic_bytes_per_step": bytes_step},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(amp_host.nbytes),
                     "d2h_bytes_per_step": int(d2h),
