@@ -7,6 +7,10 @@ stream, after `--warmup` untimed steps; `e2e` times the public API call (ptychop
 patterns in pinned host memory.  Multi-GPU runs (torchrun) are independent replicas, one per GPU.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+`--algo epie --cfg epie128|epie256k5` measures the ePIE configurations instead (10x10 raster at 128^2 with one probe
+mode; 51x51 raster at 256^2 with 5 modes): one step = one ePIE iteration over all positions, after enough warm-up
+iterations that the probe (iteration 10) and the modes (iteration 20) are being updated.
 """
 import argparse
 import json
@@ -38,6 +42,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--nx", type=int, default=30, help="raster size (30 = the DM configuration; smaller for profiling)")
     ap.add_argument("--wave", type=int, default=0, help="DM patterns per pipeline wave (0 = automatic)")
+    ap.add_argument("--algo", default="dm", choices=["dm", "epie"])
+    ap.add_argument("--cfg", default="epie128", choices=["epie128", "epie256k5"], help="ePIE configuration")
     return ap.parse_args()
 
 
@@ -319,10 +325,95 @@ def run_b200(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_epie(args, rank, local):
+    """ePIE throughput on one of the ePIE configurations (device-timed steps, oracle FP32 port as CPU baseline)."""
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+
+    from ptychopy_b200 import abi, synth
+
+    torch.cuda.set_device(local)
+    cfg = dict(synth.CONFIGS[args.cfg])
+    N, K = cfg["N"], cfg["K"]
+    rng = np.random.default_rng(20261205)
+    dx_s = synth.sample_pixel(cfg["lambd"], cfg["z"], cfg["dx_d"], N)
+    pos, X, Y = synth.raster_positions(cfg["nx"], cfg["ny"], cfg["step"], cfg["step"], dx_s, N)
+    obj = synth.make_object(X, Y, rng)
+    probe = synth.make_probe(N, dx_s, K=K)
+    amp = synth.make_patterns_torch(obj, probe, pos, N, cfg["photons"], seed=20261205, device="cuda")
+    P = pos.shape[0]
+    kwargs = dict(size=N, scanDimsx=cfg["nx"], scanDimsy=cfg["ny"], stepx=cfg["step"], stepy=cfg["step"],
+                  lambd=cfg["lambd"], z=cfg["z"], dx_d=cfg["dx_d"], beamSize=synth.BEAM_FWHM, probeModes=K,
+                  algorithm="ePIE", device=local)
+    stream = torch.cuda.Stream()
+    s = abi.Session(**kwargs)
+    s.set_stream(stream.cuda_stream)
+    s.set_patterns_ptr(amp.data_ptr(), P, N)
+    s.init()
+    warm = max(args.warmup, 21)
+    for _ in range(warm):
+        s.step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    l0 = s.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.start()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            s.step()
+        e1.record(stream)
+    stream.synchronize()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = s.launches() - l0
+    finite = bool(np.isfinite(s.object()).all())
+    s.close()
+    value = P * args.steps / (ms / 1000.0)
+    peak, kind = peaks()
+    bytes_pattern = 4 * N * N + 16 * N * N * (1 + K)  # A; object patch r+w; probe modes r+w (probe updating)
+    achieved = bytes_pattern * value / 1e9
+    out = {"metric": "ePIE patterns/s", "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+           "warmup": warm, "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "f32",
+           "data": "synthetic (seeded)",
+           "config": {"workload": f"ePIE {args.cfg}: {cfg['nx']}x{cfg['ny']} raster ({P} positions), {N}x{N} "
+                                  f"detector, {K} probe mode(s), object {X}x{Y}", "N": N, "positions": P, "modes": K},
+           "roofline": {"bound": "latency (serial positions)", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_kind": kind, "kernel": "k_epie (one persistent cluster)",
+                        "algorithmic_bytes_per_pattern": bytes_pattern},
+           "gpu_launches": int(launches), "clocks": ck, "finite": finite}
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+
+        amp_np = amp.cpu().numpy()
+        threads = 1  # the port's ePIE is serial over positions, like the method
+        n = min(P, 16)
+        o = pyoracle.OracleSession("ePIE", amp_np[:n], pos[:n], np.zeros((X, Y)), probe, probe_guess_path=False,
+                                   modes_given=K > 1, nthreads=threads, fp32=True)
+        t0 = time.perf_counter()
+        o.step()
+        per = (time.perf_counter() - t0) / n
+        n = int(min(P, max(n, 15.0 / max(per, 1e-9))))
+        o = pyoracle.OracleSession("ePIE", amp_np[:n], pos[:n], np.zeros((X, Y)), probe, probe_guess_path=False,
+                                   modes_given=K > 1, nthreads=threads, fp32=True)
+        t0 = time.perf_counter()
+        o.step()
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n / t, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"iteration 1 of ePIE over {n} of the {P} positions (FP32 C++ port, "
+                                         "no probe update yet)"}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
-    if args.impl == "reference":
+    if args.algo == "epie" and args.impl == "b200":
+        run_epie(args, rank, local)
+    elif args.impl == "reference":
         run_reference(args, rank)
     else:
         run_b200(args, rank, world, local)

@@ -16,8 +16,8 @@
 //   E  rows     probe update P_k += (1/objMax) conj(O_new) dpsi_k and |P_k|^2 cache (src/ProbeKernels.cu:425-458),
 //               per-CTA partial of Probe::getModalDoubleMax, combined after the barrier
 //
-// Cluster barriers (barrier.cluster arrive.release / wait.acquire, preceded by a device-scope fence) order the
-// global-memory hand-offs; there are no software spin-waits.
+// Cluster barriers (barrier.cluster arrive.release / wait.acquire) order the global-memory hand-offs at cluster
+// scope; there are no software spin-waits.
 #include <cooperative_groups.h>
 
 #include "fft_core.cuh"
@@ -28,9 +28,11 @@ namespace cg = cooperative_groups;
 
 namespace pty {
 
+// barrier.cluster.arrive (release) + barrier.cluster.wait (acquire): cluster-scope ordering of the global and
+// shared memory the CTAs hand to each other.  Every hand-off of this kernel stays inside its single cluster, so no
+// device-scope fence is needed.
 __device__ __forceinline__ void cluster_barrier() {
-  __threadfence();
-  cg::this_cluster().sync();
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
 // Texture-coordinate emulation for one axis: integer index idx plus fractional base; clamp addressing.
@@ -310,7 +312,9 @@ __global__ void __launch_bounds__(R* FftShape<L>::T) k_epie(EpieArgs g) {
   }
 }
 
-// Rows per pass of a CTA (blockDim = R * T) for a length-L window.
+// Rows per pass of a CTA (blockDim = R * T) for a length-L window; the cluster takes the largest size (<= 16)
+// whose CTAs hold whole passes.  Each position is a chain of short latency-bound phases: at L = 128, 4 CTAs of 8
+// warps (R = 32) measured no faster than 16 CTAs of 2 warps (3.43 vs 3.21 ms per 100-position iteration).
 template <int L> struct EpieShape;
 template <> struct EpieShape<32> { static constexpr int R = 8; };
 template <> struct EpieShape<64> { static constexpr int R = 4; };
