@@ -8,6 +8,10 @@ patterns in pinned host memory.  Multi-GPU runs (torchrun) are independent repli
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
+`--algo batch` measures the batched configuration: 16 independent scans of uneven sizes (8 DM, 8 MLs; detectors
+128-512, rasters 10x10-40x40, steps 30-100 nm), `--steps` iterations each, interleaved by pty_batch_run against
+the same scans run one after another.
+
 `--algo epie --cfg epie128|epie256k5` measures the ePIE configurations instead (10x10 raster at 128^2 with one probe
 mode; 51x51 raster at 256^2 with 5 modes): one step = one ePIE iteration over all positions, after enough warm-up
 iterations that the probe (iteration 10) and the modes (iteration 20) are being updated.
@@ -42,7 +46,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--nx", type=int, default=30, help="raster size (30 = the DM configuration; smaller for profiling)")
     ap.add_argument("--wave", type=int, default=0, help="DM patterns per pipeline wave (0 = automatic)")
-    ap.add_argument("--algo", default="dm", choices=["dm", "epie"])
+    ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch"])
     ap.add_argument("--cfg", default="epie128", choices=["epie128", "epie256k5"], help="ePIE configuration")
     return ap.parse_args()
 
@@ -408,11 +412,81 @@ def run_epie(args, rank, local):
     print(json.dumps(out), flush=True)
 
 
+BATCH_SCANS = [  # (algorithm, N, raster, step m)
+    ("DM", 128, 10, 30e-9), ("DM", 128, 20, 50e-9), ("DM", 256, 15, 60e-9), ("DM", 256, 25, 80e-9),
+    ("DM", 512, 10, 50e-9), ("DM", 512, 20, 100e-9), ("DM", 128, 40, 40e-9), ("DM", 256, 30, 70e-9),
+    ("MLs", 128, 12, 50e-9), ("MLs", 128, 24, 30e-9), ("MLs", 256, 10, 100e-9), ("MLs", 256, 20, 60e-9),
+    ("MLs", 512, 12, 80e-9), ("MLs", 128, 35, 40e-9), ("MLs", 256, 16, 50e-9), ("MLs", 512, 10, 100e-9),
+]
+
+
+def run_batch(args, rank, local):
+    """Aggregate patterns/s of 16 uneven scans run through pty_batch_run vs one after another."""
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+
+    from ptychopy_b200 import abi, synth
+
+    torch.cuda.set_device(local)
+    lambd, z, dx_d = 2.48e-10, 1.0, 172e-6
+    sessions, total_p, keep = [], 0, []
+    for i, (algo, N, nx, step) in enumerate(BATCH_SCANS):
+        rng = np.random.default_rng(20261206 + i)
+        dx_s = synth.sample_pixel(lambd, z, dx_d, N)
+        pos, X, Y = synth.raster_positions(nx, nx, step, step, dx_s, N)
+        obj = synth.make_object(X, Y, rng)
+        probe = synth.make_probe(N, dx_s, K=1)
+        amp = synth.make_patterns_torch(obj, probe, pos, N, 1e6, seed=20261206 + i, device="cuda",
+                                        intensities=(algo == "MLs"))
+        s = abi.Session(size=N, scanDimsx=nx, scanDimsy=nx, stepx=step, stepy=step, lambd=lambd, z=z, dx_d=dx_d,
+                        beamSize=synth.BEAM_FWHM, probeModes=1, algorithm=algo, delta_p=0.1, PPS=20, device=local)
+        s.set_patterns_ptr(amp.data_ptr(), pos.shape[0], N)
+        s.set_probe(probe)
+        s.init()
+        keep.append(amp)
+        sessions.append(s)
+        total_p += pos.shape[0]
+    abi.batch_run(sessions, 2)  # graph capture and warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in sessions:
+        s.run(args.steps)
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    clocks = Clocks(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    abi.batch_run(sessions, args.steps)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    ck = clocks.stop()
+    finite = all(bool(np.isfinite(s.object()).all()) for s in sessions)
+    work = total_p * args.steps
+    out = {"metric": "batched reconstructions, aggregate patterns/s", "value": work / t_batch, "unit": UNIT,
+           "n_gpus": 1, "steps": args.steps, "warmup": 2, "higher_is_better": True, "dtype": "f32",
+           "data": "synthetic (seeded)",
+           "config": {"workload": "16 scans: 8 DM + 8 MLs (delta_p 0.1), detectors 128-512, rasters 10x10-40x40, "
+                                  "steps 30-100 nm, 1e6 photons/pattern", "positions": total_p,
+                      "scans": [f"{a} {n}^2 {r}x{r} {st * 1e9:.0f} nm" for a, n, r, st in BATCH_SCANS]},
+           "sequential": {"value": work / t_seq, "unit": UNIT, "seconds": t_seq},
+           "batched_seconds": t_batch, "speedup_vs_sequential": t_seq / t_batch, "clocks": ck, "finite": finite,
+           "timing": "host wall clock around synchronised regions (includes each scan's host-side scheduling)",
+           "note": "MLs runs its core (no position search, sub-pixel shift or variable probe); PPS is accepted and "
+                   "has no effect"}
+    for s in sessions:
+        s.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.algo == "epie" and args.impl == "b200":
         run_epie(args, rank, local)
+    elif args.algo == "batch" and args.impl == "b200":
+        run_batch(args, rank, local)
     elif args.impl == "reference":
         run_reference(args, rank)
     else:

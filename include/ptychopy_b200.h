@@ -113,6 +113,13 @@ int pty_step(pty_session* s, double* err);
  * (src/IPhaser.cpp:367-389). */
 int pty_run(pty_session* s, int iters, double* errs);
 
+/* `iters` iterations of each of n initialised sessions (any mix of ePIE, DM and MLs on one device), interleaved:
+ * every round enqueues one iteration of every session on that session's own stream, without host
+ * synchronisation between DM and MLs steps, so independent scans of uneven sizes share the GPU.  Returns after all
+ * streams have finished.  No counterpart in the reference, which runs one reconstruction per process (its
+ * IPhaser::phaseLoop, src/IPhaser.cpp:367-389, per session); error metrics are not collected. */
+int pty_batch_run(pty_session* const* sessions, int n, int iters);
+
 /* Sizes: object X, Y; probe modes K, size N; pattern count P; iterations done. */
 int pty_get_dims(const pty_session* s, int* X, int* Y, int* K, int* N, int* P, int* iters_done);
 

@@ -28,7 +28,7 @@ EXPORTS = [
     "pty_params_init", "pty_session_create", "pty_session_destroy", "pty_set_patterns", "pty_set_positions",
     "pty_set_object", "pty_set_probe", "pty_init", "pty_step", "pty_run", "pty_get_dims", "pty_get_object",
     "pty_get_probe", "pty_get_positions", "pty_write_results", "pty_set_stream", "pty_kernel_launches",
-    "pty_last_error", "pty_fft2_dev", "pty_fft2_dev_noalloc",
+    "pty_last_error", "pty_fft2_dev", "pty_fft2_dev_noalloc", "pty_batch_run",
 ]
 
 
@@ -85,6 +85,7 @@ def lib():
             "pty_last_error": ([], ctypes.c_char_p),
             "pty_fft2_dev": ([vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
             "pty_fft2_dev_noalloc": ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
+            "pty_batch_run": ([ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int], ctypes.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -215,6 +216,12 @@ class Session:
 
     def launches(self):
         return int(lib().pty_kernel_launches(self.h))
+
+
+def batch_run(sessions, iters):
+    """Run `iters` iterations of every session, interleaved on their own streams (pty_batch_run)."""
+    arr = (ctypes.c_void_p * len(sessions))(*[s.h.value for s in sessions])
+    check(lib().pty_batch_run(arr, len(sessions), iters))
 
 
 def fft2_dev(data_ptr, work_ptr, batch, N, inverse=False, stream=0):

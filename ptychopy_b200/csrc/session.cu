@@ -212,13 +212,29 @@ struct EpieState {
 };
 
 // Device state of the MLs core.
+// Group tables of one iteration, packed: members (ng x Gmax, -1 padded) | sizes (ng) | boxes (4 ng).  Two sets
+// (device copy, pinned host staging, copy-done event, graph reading it) alternate between iterations, so the host
+// builds iteration i+1's tables while the GPU runs iteration i and a step needs no synchronisation.
+struct MlsTables {
+  DeviceBuf dev;
+  int* host = nullptr;
+  cudaEvent_t copied = nullptr;
+  cudaGraphExec_t graph = nullptr;
+};
+
 struct MlsState {
   MlsGeometry geo;
-  DeviceBuf pobj, S, pum, objp, psi, work, starts, members, gsize, bbox, sums, errk, betas, err, norms, maxill;
+  DeviceBuf pobj, S, pum, objp, psi, work, starts, sums, errk, betas, err, norms, maxill;
   int Gmax = 1, ng = 1;
-  cudaGraphExec_t graph = nullptr;
+  size_t table_ints = 0;
+  MlsTables tab[2];
+  int64_t steps = 0;
   ~MlsState() {
-    if (graph) cudaGraphExecDestroy(graph);
+    for (MlsTables& t : tab) {
+      if (t.graph) cudaGraphExecDestroy(t.graph);
+      if (t.copied) cudaEventDestroy(t.copied);
+      if (t.host) cudaFreeHost(t.host);
+    }
   }
 };
 
@@ -606,9 +622,12 @@ void init_mls(pty_session* s) {
   ml->objp.alloc(sizeof(float2) * GN, "windows");
   ml->psi.alloc(sizeof(float2) * GN, "exit waves");
   ml->work.alloc(sizeof(float2) * GN, "FFT work");
-  ml->members.alloc(sizeof(int) * ml->ng * ml->Gmax, "groups");
-  ml->gsize.alloc(sizeof(int) * ml->ng, "group sizes");
-  ml->bbox.alloc(sizeof(int) * 4 * ml->ng, "group boxes");
+  ml->table_ints = size_t(ml->ng) * ml->Gmax + 5 * size_t(ml->ng);
+  for (MlsTables& t : ml->tab) {
+    t.dev.alloc(sizeof(int) * ml->table_ints, "group tables");
+    check_cuda(cudaMallocHost(&t.host, sizeof(int) * ml->table_ints), "pinned group tables");
+    check_cuda(cudaEventCreateWithFlags(&t.copied, cudaEventDisableTiming), "event");
+  }
   ml->sums.alloc(sizeof(double) * 6 * ml->Gmax, "LSQ sums");
   ml->errk.alloc(sizeof(double) * ml->Gmax, "errors");
   ml->betas.alloc(sizeof(double) * 4, "steps");
@@ -618,7 +637,7 @@ void init_mls(pty_session* s) {
   check_cuda(cudaStreamSynchronize(s->stream), "MLs set-up");
 }
 
-MlsBuffers mls_buffers(pty_session* s) {
+MlsBuffers mls_buffers(pty_session* s, int parity) {
   MlsState* ml = s->ml;
   MlsBuffers b;
   b.obj = s->obj.as<float2>();
@@ -631,9 +650,9 @@ MlsBuffers mls_buffers(pty_session* s) {
   b.psi = ml->psi.as<float2>();
   b.work = ml->work.as<float2>();
   b.starts = ml->starts.as<int2>();
-  b.members = ml->members.as<int>();
-  b.gsize = ml->gsize.as<int>();
-  b.bbox = ml->bbox.as<int>();
+  b.members = ml->tab[parity].dev.as<int>();
+  b.gsize = b.members + size_t(ml->ng) * ml->Gmax;
+  b.bbox = b.gsize + ml->ng;
   b.sums = ml->sums.as<double>();
   b.errk = ml->errk.as<double>();
   b.betas = ml->betas.as<double>();
@@ -658,13 +677,20 @@ MlsBuffers mls_buffers(pty_session* s) {
 double step_mls(pty_session* s, bool want_err) {
   MlsState* ml = s->ml;
   const int P = s->P, G = ml->Gmax, N = s->N;
+  const int parity = int(ml->steps & 1);
+  MlsTables& tb = ml->tab[parity];
+  // this set's staging buffer was last copied two iterations ago
+  check_cuda(cudaEventSynchronize(tb.copied), "group table reuse");
   std::vector<int> perm(P);
   for (int i = 0; i < P; ++i) perm[i] = i;
   for (int i = P - 1; i > 0; --i) std::swap(perm[i], perm[splitmix64(s->rng) % uint64_t(i + 1)]);
   std::vector<int> order(ml->ng);
   for (int i = 0; i < ml->ng; ++i) order[i] = i;
   for (int i = ml->ng - 1; i > 0; --i) std::swap(order[i], order[splitmix64(s->rng) % uint64_t(i + 1)]);
-  std::vector<int> mem(size_t(ml->ng) * G, -1), gs(ml->ng), box(4 * size_t(ml->ng));
+  int* mem = tb.host;
+  int* gs = mem + size_t(ml->ng) * G;
+  int* box = gs + ml->ng;
+  std::fill(mem, mem + size_t(ml->ng) * G, -1);
   for (int gi = 0; gi < ml->ng; ++gi) {
     const int g = order[gi];
     const int lo = g * G, hi = std::min(P, (g + 1) * G);
@@ -683,34 +709,30 @@ double step_mls(pty_session* s, bool want_err) {
     box[4 * gi + 2] = x1 - x0;
     box[4 * gi + 3] = y1 - y0;
   }
-  check_cuda(cudaStreamSynchronize(s->stream), "group table reuse");
-  check_cuda(cudaMemcpyAsync(ml->members.p, mem.data(), sizeof(int) * mem.size(), cudaMemcpyHostToDevice, s->stream),
+  check_cuda(cudaMemcpyAsync(tb.dev.p, tb.host, sizeof(int) * ml->table_ints, cudaMemcpyHostToDevice, s->stream),
              "H2D groups");
-  check_cuda(cudaMemcpyAsync(ml->gsize.p, gs.data(), sizeof(int) * gs.size(), cudaMemcpyHostToDevice, s->stream),
-             "H2D groups");
-  check_cuda(cudaMemcpyAsync(ml->bbox.p, box.data(), sizeof(int) * box.size(), cudaMemcpyHostToDevice, s->stream),
-             "H2D groups");
+  check_cuda(cudaEventRecord(tb.copied, s->stream), "event");
   check_cuda(cudaMemsetAsync(ml->err.p, 0, sizeof(double), s->stream), "memset");
-  if (!ml->graph) {
-    const MlsBuffers b = mls_buffers(s);
+  if (!tb.graph) {
+    const MlsBuffers b = mls_buffers(s, parity);
     cudaGraph_t graph = nullptr;
     check_cuda(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     const cudaError_t e = mls_iteration(b, ml->ng, s->stream);
     const cudaError_t e2 = cudaStreamEndCapture(s->stream, &graph);
     check_cuda(e, "MLs capture");
     check_cuda(e2, "end capture");
-    const cudaError_t e3 = cudaGraphInstantiate(&ml->graph, graph, 0);
+    const cudaError_t e3 = cudaGraphInstantiate(&tb.graph, graph, 0);
     cudaGraphDestroy(graph);
     check_cuda(e3, "graph instantiate");
   }
-  check_cuda(cudaGraphLaunch(ml->graph, s->stream), "MLs graph launch");
+  check_cuda(cudaGraphLaunch(tb.graph, s->stream), "MLs graph launch");
   s->launches += mls_launches_per_iteration(ml->ng);
-  // the tables above are pageable host copies: wait before they go out of scope
+  ++ml->steps;
+  if (!(want_err && s->prm.calculateRMS)) return 0.0;
   double e = 0;
-  if (want_err && s->prm.calculateRMS)
-    check_cuda(cudaMemcpyAsync(&e, ml->err.p, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "D2H error");
+  check_cuda(cudaMemcpyAsync(&e, ml->err.p, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "D2H error");
   check_cuda(cudaStreamSynchronize(s->stream), "MLs iteration");
-  return want_err && s->prm.calculateRMS ? e / P : 0.0;
+  return e / P;
 }
 
 DMBuffers dm_buffers(pty_session* s) {
@@ -1097,6 +1119,34 @@ int pty_run(pty_session* s, int iters, double* errs) {
       }
     }
     check_cuda(cudaStreamSynchronize(s->stream), "pty_run");
+  });
+}
+
+int pty_batch_run(pty_session* const* sessions, int n, int iters) {
+  return guarded([&] {
+    need(sessions && n > 0, "no sessions");
+    need(iters >= 0, "negative iteration count");
+    for (int i = 0; i < n; ++i) {
+      need(sessions[i] != nullptr, "null session in the batch");
+      need(sessions[i]->initialized, "pty_init has not run for session " + std::to_string(i), PTY_ERR_STATE);
+      need(sessions[i]->dev == sessions[0]->dev, "batched sessions must share one device");
+    }
+    set_device(sessions[0]);
+    // round-robin: one iteration of every scan per round, each on its own stream, no host synchronisation for DM
+    // and MLs steps, so the scans' kernels run side by side
+    for (int it = 0; it < iters; ++it)
+      for (int i = 0; i < n; ++i) {
+        pty_session* s = sessions[i];
+        const int k = s->iter + 1;
+        if (s->algo == ALGO_EPIE)
+          step_epie(s, k, false);
+        else if (s->algo == ALGO_MLS)
+          step_mls(s, false);
+        else
+          step_dm(s, k);
+        s->iter = k;
+      }
+    for (int i = 0; i < n; ++i) check_cuda(cudaStreamSynchronize(sessions[i]->stream), "pty_batch_run");
   });
 }
 
