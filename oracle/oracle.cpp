@@ -723,6 +723,22 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
   return want_err ? errsum / s.P : 0.0;
 }
 
+// Position jitter (d_generateMesh, src/ScanMeshKernels.cu:53-60: jitter = r - u*2r per axis, u uniform in (0,1]
+// from curand with a time seed).  Restated with a seeded stream: SplitMix64 from seed ^ 0x6A09E667F3BCC909,
+// u = ((next >> 40) + 1) * 2^-24, x drawn before y, positions in generation order (padding included).
+void mesh_jitter(uint64_t seed, size_t n, unsigned radius, std::vector<float>& out) {
+  out.assign(2 * n, 0.f);
+  if (!radius) return;
+  uint64_t st = seed ^ 0x6A09E667F3BCC909ull;
+  const float r = float(radius);
+  for (size_t i = 0; i < 2 * n; ++i) {
+    const float u = float((splitmix64(st) >> 40) + 1) * (1.0f / 16777216.0f);
+    volatile float t = u * 2.0f;
+    volatile float t2 = t * r;
+    out[i] = r - t2;
+  }
+}
+
 }  // namespace
 
 // ============================================================================================================
@@ -745,10 +761,21 @@ int orc_fft2(double* data, int N, int inverse) {
 
 double orc_sample_pixel(double lambda, double z, double dx_d, int N) { return sample_pixel(lambda, z, dx_d, N); }
 
+int orc_cartesian_mesh_j(int nx, int ny, double stepx, double stepy, double lambda, double z, double dx_d, int N,
+                         int mirrorX, int mirrorY, int flip, unsigned jitter, uint64_t seed, float* pos, int* objXY);
+int orc_list_mesh_j(const double* xy_m, int P, double lambda, double z, double dx_d, int N, int flip, unsigned jitter,
+                    uint64_t seed, float* pos, int* objXY);
+
 // Cartesian raster mesh (d_generateMesh<1>, src/ScanMeshKernels.cu:46-93, launched at :153-160).
 // pos receives 2*nx*ny floats (raster order i*ny+j), objXY the object size.
 int orc_cartesian_mesh(int nx, int ny, double stepx, double stepy, double lambda, double z, double dx_d, int N,
                        int mirrorX, int mirrorY, int flip, float* pos, int* objXY) {
+  return orc_cartesian_mesh_j(nx, ny, stepx, stepy, lambda, z, dx_d, N, mirrorX, mirrorY, flip, 0, 0, pos, objXY);
+}
+
+int orc_cartesian_mesh_j(int nx, int ny, double stepx, double stepy, double lambda, double z, double dx_d, int N,
+                         int mirrorX, int mirrorY, int flip, unsigned jitter, uint64_t seed, float* pos,
+                         int* objXY) {
   if (nx < 1 || ny < 1 || N < 1) return -1;
   const double dx_s = sample_pixel(lambda, z, dx_d, N);
   const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
@@ -765,6 +792,12 @@ int orc_cartesian_mesh(int nx, int ny, double stepx, double stepy, double lambda
       raw[2 * (size_t(i) * ny + j)] = px;
       raw[2 * (size_t(i) * ny + j) + 1] = py;
     }
+  std::vector<float> jit;
+  mesh_jitter(seed, size_t(nx) * ny, jitter, jit);
+  for (size_t k = 0; k < raw.size(); ++k) {
+    volatile float v = raw[k] + jit[k];
+    raw[k] = v;
+  }
   Mesh m;
   finish_mesh(raw, nx * ny, false, N, flip != 0, m);
   std::memcpy(pos, m.pos.data(), m.pos.size() * sizeof(float));
@@ -775,19 +808,74 @@ int orc_cartesian_mesh(int nx, int ny, double stepx, double stepy, double lambda
 // List mesh from positions in metres (ListScanMesh::loadarr + d_generateMesh<2>, src/ListScanMesh.cpp:55-129).
 int orc_list_mesh(const double* xy_m, int P, double lambda, double z, double dx_d, int N, int flip, float* pos,
                   int* objXY) {
+  return orc_list_mesh_j(xy_m, P, lambda, z, dx_d, N, flip, 0, 0, pos, objXY);
+}
+
+// The mesh array holds whole 1024-wide rows: entries past P are (0, 0) plus their jitter and take part in the
+// min/max (calculateMeshDimensions reduces over the whole array).
+int orc_list_mesh_j(const double* xy_m, int P, double lambda, double z, double dx_d, int N, int flip, unsigned jitter,
+                    uint64_t seed, float* pos, int* objXY) {
   if (P < 1) return -1;
   const double dx_s = sample_pixel(lambda, z, dx_d, N);
   const float inv = float(1.0 / dx_s);
-  std::vector<float> raw(2 * size_t(P));
+  const size_t M = (size_t(P) + 1023) / 1024 * 1024;
+  std::vector<float> raw(2 * M, 0.f), jit;
   for (int i = 0; i < P; ++i) {
     volatile float x = float(xy_m[2 * i]), y = float(xy_m[2 * i + 1]);
     volatile float px = x * inv, py = y * inv;
     raw[2 * i] = px; raw[2 * i + 1] = py;
   }
+  mesh_jitter(seed, M, jitter, jit);
+  for (size_t k = 0; k < raw.size(); ++k) {
+    volatile float v = raw[k] + jit[k];
+    raw[k] = v;
+  }
   Mesh m;
-  finish_mesh(raw, P, (P % 1024) != 0, N, flip != 0, m);
+  finish_mesh(raw, int(M), false, N, flip != 0, m);
+  m.pos.resize(2 * size_t(P));
   std::memcpy(pos, m.pos.data(), m.pos.size() * sizeof(float));
   objXY[0] = m.X; objXY[1] = m.Y;
+  return 0;
+}
+
+// Spiral mesh (d_generateMesh<3>, src/ScanMeshKernels.cu:77-82, SpiralScanMesh::generateMesh,
+// src/SpiralScanMesh.cpp:57-84): point i at sqrt(i) * (cos, sin)(4 sqrt(i)) * step / dx_s.  The mesh array holds
+// whole 1024-wide rows and every entry is a spiral point, so the min/max (object size, shift) cover
+// ceil(P/1024)*1024 points while only the first P are scan positions.  cos/sin of the float argument in double,
+// rounded to float.
+int orc_spiral_mesh(int P, double stepx, double stepy, double lambda, double z, double dx_d, int N, int flip,
+                    unsigned jitter, uint64_t seed, float* pos, int* objXY) {
+  if (P < 1 || N < 1) return -1;
+  const double dx_s = sample_pixel(lambda, z, dx_d, N);
+  const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
+  const size_t M = (size_t(P) + 1023) / 1024 * 1024;
+  std::vector<float> raw(2 * M), jit;
+  mesh_jitter(seed, M, jitter, jit);
+  for (size_t i = 0; i < M; ++i) {
+    const float s = std::sqrt(float(i));
+    const float a = 4.0f * s;
+    const float c = float(std::cos(double(a))), sn = float(std::sin(double(a)));
+    volatile float vx = s * c;
+    volatile float vy = s * sn;
+    volatile float wx = vx * sx, wy = vy * sy;
+    volatile float px = wx * inv, py = wy * inv;
+    volatile float jx = px + jit[2 * i], jy = py + jit[2 * i + 1];
+    raw[2 * i] = jx;
+    raw[2 * i + 1] = jy;
+  }
+  Mesh m;
+  finish_mesh(raw, int(M), false, N, flip != 0, m);
+  m.pos.resize(2 * size_t(P));
+  std::memcpy(pos, m.pos.data(), m.pos.size() * sizeof(float));
+  objXY[0] = m.X; objXY[1] = m.Y;
+  return 0;
+}
+
+// The jitter stream itself (2*n floats: x, y per position).
+int orc_mesh_jitter(uint64_t seed, int n, unsigned radius, float* out) {
+  std::vector<float> j;
+  mesh_jitter(seed, size_t(n), radius, j);
+  std::memcpy(out, j.data(), j.size() * sizeof(float));
   return 0;
 }
 

@@ -40,6 +40,10 @@ def lib():
             "orc_sample_pixel": ([d, d, d, i], d),
             "orc_cartesian_mesh": ([i, i, d, d, d, d, d, i, i, i, i, vp, vp], i),
             "orc_list_mesh": ([vp, i, d, d, d, i, i, vp, vp], i),
+            "orc_cartesian_mesh_j": ([i, i, d, d, d, d, d, i, i, i, i, ctypes.c_uint, u64, vp, vp], i),
+            "orc_list_mesh_j": ([vp, i, d, d, d, i, i, ctypes.c_uint, u64, vp, vp], i),
+            "orc_spiral_mesh": ([i, d, d, d, d, d, i, i, ctypes.c_uint, u64, vp, vp], i),
+            "orc_mesh_jitter": ([u64, i, ctypes.c_uint, vp], i),
             "orc_probe_guess": ([vp, i, i, d, d, i, vp], i),
             "orc_visiting_order": ([ctypes.POINTER(u64), i, vp], None),
             "orc_extract_patch": ([vp, i, i, f, f, i, vp], i),
@@ -78,20 +82,36 @@ def sample_pixel(lambd, z, dx_d, N):
     return lib().orc_sample_pixel(lambd, z, dx_d, N)
 
 
-def cartesian_mesh(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX=0, mirrorY=0, flip=0):
+def cartesian_mesh(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX=0, mirrorY=0, flip=0, jitter=0, seed=0):
     pos = np.zeros((nx * ny, 2), np.float32)
     xy = np.zeros(2, np.int32)
-    assert lib().orc_cartesian_mesh(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX, mirrorY, flip, _p(pos),
-                                    _p(xy)) == 0
+    assert lib().orc_cartesian_mesh_j(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX, mirrorY, flip, jitter, seed,
+                                      _p(pos), _p(xy)) == 0
     return pos, int(xy[0]), int(xy[1])
 
 
-def list_mesh(xy_m, lambd, z, dx_d, N, flip=0):
+def list_mesh(xy_m, lambd, z, dx_d, N, flip=0, jitter=0, seed=0):
     xy_m = np.ascontiguousarray(xy_m, np.float64)
     pos = np.zeros((xy_m.shape[0], 2), np.float32)
     xy = np.zeros(2, np.int32)
-    assert lib().orc_list_mesh(_p(xy_m), xy_m.shape[0], lambd, z, dx_d, N, flip, _p(pos), _p(xy)) == 0
+    assert lib().orc_list_mesh_j(_p(xy_m), xy_m.shape[0], lambd, z, dx_d, N, flip, jitter, seed, _p(pos),
+                                 _p(xy)) == 0
     return pos, int(xy[0]), int(xy[1])
+
+
+def spiral_mesh(P, stepx, stepy, lambd, z, dx_d, N, flip=0, jitter=0, seed=0):
+    """Spiral scan positions (P, 2) in pixels after the -min shift, and the object size."""
+    pos = np.zeros((P, 2), np.float32)
+    xy = np.zeros(2, np.int32)
+    assert lib().orc_spiral_mesh(P, stepx, stepy, lambd, z, dx_d, N, flip, jitter, seed, _p(pos), _p(xy)) == 0
+    return pos, int(xy[0]), int(xy[1])
+
+
+def mesh_jitter(seed, n, radius):
+    """The seeded jitter stream: (n, 2) float32 offsets in pixels."""
+    out = np.zeros((n, 2), np.float32)
+    lib().orc_mesh_jitter(seed, n, radius, _p(out))
+    return out
 
 
 def probe_guess(amp, beamSize, dx_s, K=1):

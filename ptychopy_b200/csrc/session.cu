@@ -50,20 +50,15 @@ double sample_pixel_size(double lambda, double z, double dx_d, int N) {
   return double(float((lambda * z) / (double(N) * dx_d)));
 }
 
-// min/max, object size ceil(max - min + N) and the -min shift (src/IPtychoScanMesh.cpp:86-109).
-static void finish_geometry(const std::vector<float>& raw, int P, bool padZero, int N, bool flip, Geometry& g) {
+// min/max over the M entries of the mesh array, object size ceil(max - min + N) and the -min shift of the first P
+// (src/IPtychoScanMesh.cpp:86-109: calculateMeshDimensions reduces over the whole array).
+static void finish_geometry(const std::vector<float>& raw, int P, int M, int N, bool flip, Geometry& g) {
   float mnx = std::numeric_limits<float>::max(), mny = mnx, mxx = -mnx, mxy = -mnx;
-  for (int i = 0; i < P; ++i) {
+  for (int i = 0; i < M; ++i) {
     mnx = std::min(mnx, raw[2 * i]);
     mxx = std::max(mxx, raw[2 * i]);
     mny = std::min(mny, raw[2 * i + 1]);
     mxy = std::max(mxy, raw[2 * i + 1]);
-  }
-  if (padZero) {  // list meshes are padded to whole 1024-wide rows of (0,0) that join the min/max
-    mnx = std::min(mnx, 0.f);
-    mxx = std::max(mxx, 0.f);
-    mny = std::min(mny, 0.f);
-    mxy = std::max(mxy, 0.f);
   }
   volatile float ex = (mxx - mnx) + float(N);
   volatile float ey = (mxy - mny) + float(N);
@@ -77,10 +72,27 @@ static void finish_geometry(const std::vector<float>& raw, int P, bool padZero, 
   }
 }
 
+// Position jitter, r - u*2r per axis in pixels (src/ScanMeshKernels.cu:53-60, where u comes from curand with a
+// time seed).  Seeded here: SplitMix64 from seed ^ 0x6A09E667F3BCC909, u = ((next >> 40) + 1) * 2^-24 in (0, 1],
+// x before y, positions in mesh-array order (padding included).  Added to raw (already in pixels).
+static void add_jitter(std::vector<float>& raw, unsigned radius, uint64_t seed) {
+  if (!radius) return;
+  uint64_t st = seed ^ 0x6A09E667F3BCC909ull;
+  const float r = float(radius);
+  for (float& v : raw) {
+    const float u = float((splitmix64(st) >> 40) + 1) * (1.0f / 16777216.0f);
+    volatile float t = u * 2.0f;
+    volatile float t2 = t * r;
+    volatile float j = r - t2;
+    volatile float w = v + j;
+    v = w;
+  }
+}
+
 // Cartesian raster (d_generateMesh<1>, src/ScanMeshKernels.cu:46-93): index i*ny+j,
 // ((i - (nx-1)/2) * stepx) / dx_s in float.
 Geometry cartesian_geometry(int nx, int ny, double stepx, double stepy, double dx_s, int N, bool mirrorX,
-                            bool mirrorY, bool flip) {
+                            bool mirrorY, bool flip, unsigned jitter, uint64_t seed) {
   const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
   std::vector<float> raw(2 * size_t(nx) * ny);
   const float mdx = float(nx - 1) * 0.5f, mdy = float(ny - 1) * 0.5f;
@@ -94,25 +106,69 @@ Geometry cartesian_geometry(int nx, int ny, double stepx, double stepy, double d
       raw[2 * (size_t(i) * ny + j)] = px;
       raw[2 * (size_t(i) * ny + j) + 1] = py;
     }
+  add_jitter(raw, jitter, seed);
   Geometry g;
-  finish_geometry(raw, nx * ny, false, N, flip, g);
+  finish_geometry(raw, nx * ny, nx * ny, N, flip, g);
   return g;
 }
 
-// Position list in metres (ListScanMesh::loadarr + d_generateMesh<2>, src/ListScanMesh.cpp:91-129).
-Geometry list_geometry(const std::vector<double>& xy_m, double dx_s, int N, bool flip) {
+// Position list in metres (ListScanMesh::loadarr + d_generateMesh<2>, src/ListScanMesh.cpp:91-129).  The mesh
+// array holds whole 1024-wide rows; entries past P stay (0, 0) (plus jitter) and join the min/max.
+Geometry list_geometry(const std::vector<double>& xy_m, double dx_s, int N, bool flip, unsigned jitter,
+                       uint64_t seed) {
   const int P = int(xy_m.size() / 2);
+  const int M = (P + 1023) / 1024 * 1024;
   const float inv = float(1.0 / dx_s);
-  std::vector<float> raw(2 * size_t(P));
+  std::vector<float> raw(2 * size_t(M), 0.f);
   for (int i = 0; i < P; ++i) {
     volatile float x = float(xy_m[2 * i]), y = float(xy_m[2 * i + 1]);
     volatile float px = float(x) * inv, py = float(y) * inv;
     raw[2 * i] = px;
     raw[2 * i + 1] = py;
   }
+  add_jitter(raw, jitter, seed);
   Geometry g;
-  finish_geometry(raw, P, (P % 1024) != 0, N, flip, g);
+  finish_geometry(raw, P, M, N, flip, g);
   return g;
+}
+
+// Spiral (d_generateMesh<3>, src/ScanMeshKernels.cu:77-82; SpiralScanMesh::generateMesh,
+// src/SpiralScanMesh.cpp:57-84): point i at sqrt(i) * (cos, sin)(4 sqrt(i)) * step / dx_s.  Every entry of the
+// 1024-wide mesh array is a spiral point, so the min/max cover ceil(P/1024)*1024 points.  cos/sin of the float
+// argument are evaluated in double and rounded to float.
+Geometry spiral_geometry(int P, double stepx, double stepy, double dx_s, int N, bool flip, unsigned jitter,
+                         uint64_t seed) {
+  const int M = (P + 1023) / 1024 * 1024;
+  const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
+  std::vector<float> raw(2 * size_t(M));
+  for (int i = 0; i < M; ++i) {
+    const float r = std::sqrt(float(i));
+    const float a = 4.0f * r;
+    const float c = float(std::cos(double(a))), sn = float(std::sin(double(a)));
+    volatile float vx = r * c, vy = r * sn;
+    volatile float wx = vx * sx, wy = vy * sy;
+    volatile float px = wx * inv, py = wy * inv;
+    raw[2 * i] = px;
+    raw[2 * i + 1] = py;
+  }
+  add_jitter(raw, jitter, seed);
+  Geometry g;
+  finish_geometry(raw, P, M, N, flip, g);
+  return g;
+}
+
+// Position list file (ListScanMesh::loadList, src/ListScanMesh.cpp:65-89): P lines "x,y" in metres.
+std::vector<double> read_position_file(const std::string& path, int P) {
+  std::ifstream f(path);
+  if (!f.is_open()) fail(PTY_ERR_IO, "cannot open the position list file " + path);
+  std::vector<double> xy(2 * size_t(P));
+  for (int i = 0; i < P; ++i) {
+    char comma = 0;
+    if (!(f >> xy[2 * i]) || !(f >> comma) || comma != ',' || !(f >> xy[2 * i + 1]))
+      fail(PTY_ERR_INVALID, "position list file " + path + ": line " + std::to_string(i + 1) +
+                                " is not 'x,y' (expected " + std::to_string(P) + " lines)");
+  }
+  return xy;
 }
 
 // Raw (centred, not shifted) Cartesian positions of the ML mesh: the same FP32 formula as cartesian_geometry.
@@ -373,15 +429,19 @@ std::vector<float> read_complex_csv(const std::string& path, size_t& rows, size_
 void init_geometry(pty_session* s) {
   const pty_params& p = s->prm;
   const double dx_s = sample_pixel_size(p.lambd, p.z, p.dx_d, s->N);
+  // mesh choice of IPhaser::initScanMesh (src/IPhaser.cpp:128-152): positionNP, else a list file, else a spiral,
+  // else the Cartesian raster
+  need(p.jitterRadius >= 0, "jitterRadius must be >= 0");
+  const unsigned jit = unsigned(p.jitterRadius);
   if (!s->pos_m.empty()) {
-    s->geo = list_geometry(s->pos_m, dx_s, s->N, p.flipScanAxis != 0);
+    s->geo = list_geometry(s->pos_m, dx_s, s->N, p.flipScanAxis != 0, jit, p.seed);
+  } else if (p.lf[0]) {
+    s->geo = list_geometry(read_position_file(p.lf, s->P), dx_s, s->N, p.flipScanAxis != 0, jit, p.seed);
+  } else if (p.spiralScan) {
+    s->geo = spiral_geometry(s->P, p.stepx, p.stepy, dx_s, s->N, p.flipScanAxis != 0, jit, p.seed);
   } else {
-    need(p.spiralScan == 0, "spiralScan is not supported by this engine; pass positionNP", PTY_ERR_UNSUPPORTED);
-    need(p.lf[0] == 0, "position list files (lf) are not supported by this engine; pass positionNP",
-         PTY_ERR_UNSUPPORTED);
-    need(p.jitterRadius == 0, "jitterRadius is not supported by this engine", PTY_ERR_UNSUPPORTED);
     s->geo = cartesian_geometry(p.scanDimsx, p.scanDimsy, p.stepx, p.stepy, dx_s, s->N, p.mirror1stScanAxis != 0,
-                                p.mirror2ndScanAxis != 0, p.flipScanAxis != 0);
+                                p.mirror2ndScanAxis != 0, p.flipScanAxis != 0, jit, p.seed);
   }
   s->X = s->geo.X;
   s->Y = s->geo.Y;
@@ -541,12 +601,15 @@ void init_mls(pty_session* s) {
   const size_t NN = size_t(N) * N;
   const double dx_s = sample_pixel_size(p.lambd, p.z, p.dx_d, N);
   std::vector<float> raw;
-  if (!s->pos_m.empty()) {
+  if (!s->pos_m.empty() || p.lf[0]) {
+    const std::vector<double> xy = s->pos_m.empty() ? read_position_file(p.lf, P) : s->pos_m;
     const float inv = float(1.0 / dx_s);
     raw.resize(2 * size_t(P));
-    for (int i = 0; i < 2 * P; ++i) raw[i] = float(s->pos_m[i]) * inv;
+    for (int i = 0; i < 2 * P; ++i) raw[i] = float(xy[i]) * inv;
   } else {
-    need(p.spiralScan == 0 && p.lf[0] == 0 && p.jitterRadius == 0, "MLs supports Cartesian or listed positions",
+    // the reference's spiral mesh has no ML variant (SpiralScanMesh::generateMeshML is empty); jitter is not part
+    // of this engine's ML mesh
+    need(p.spiralScan == 0 && p.jitterRadius == 0, "MLs supports Cartesian or listed positions without jitter",
          PTY_ERR_UNSUPPORTED);
     raw = raw_cartesian_positions(p.scanDimsx, p.scanDimsy, p.stepx, p.stepy, dx_s, p.mirror1stScanAxis != 0,
                                   p.mirror2ndScanAxis != 0);

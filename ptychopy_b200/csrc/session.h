@@ -29,8 +29,12 @@ struct Geometry {
 };
 double sample_pixel_size(double lambda, double z, double dx_d, int N);
 Geometry cartesian_geometry(int nx, int ny, double stepx, double stepy, double dx_s, int N, bool mirrorX,
-                            bool mirrorY, bool flip);
-Geometry list_geometry(const std::vector<double>& xy_m, double dx_s, int N, bool flip);
+                            bool mirrorY, bool flip, unsigned jitter, uint64_t seed);
+Geometry list_geometry(const std::vector<double>& xy_m, double dx_s, int N, bool flip, unsigned jitter,
+                       uint64_t seed);
+Geometry spiral_geometry(int P, double stepx, double stepy, double dx_s, int N, bool flip, unsigned jitter,
+                         uint64_t seed);
+std::vector<double> read_position_file(const std::string& path, int P);
 
 // SplitMix64 stream and the ePIE visiting order (pick `next % remaining`, erase; src/ePIE.cpp:93-97).
 uint64_t splitmix64(uint64_t& state);

@@ -86,3 +86,26 @@ def test_epie_negative_position_is_an_error():
     s2.set_object(np.ones((10, 10), np.complex64))
     with pytest.raises(abi.PtyError):
         s2.init()
+
+
+def test_scan_meshes_match_oracle(oracle, tmp_path):
+    # spiral scan, jittered raster and a position list file: session geometry == oracle geometry, bit for bit
+    from gpu_helpers import dataset, gpu_session
+
+    d = dataset(N=64, nx=5, algorithm="ePIE")
+    kw = d["kw"]
+    lam, z, dxd = kw["lambd"], kw["z"], kw["dx_d"]
+    s = gpu_session(d, probe=d["probe"], spiralScan=1, seed=3)
+    pos, X, Y = oracle.spiral_mesh(25, kw["stepx"], kw["stepy"], lam, z, dxd, 64)
+    assert np.array_equal(s.positions(), pos) and (s.dims()["X"], s.dims()["Y"]) == (X, Y)
+    s = gpu_session(d, probe=d["probe"], jitterRadius=2, seed=11)
+    pos, X, Y = oracle.cartesian_mesh(5, 5, kw["stepx"], kw["stepy"], lam, z, dxd, 64, jitter=2, seed=11)
+    assert np.array_equal(s.positions(), pos) and (s.dims()["X"], s.dims()["Y"]) == (X, Y)
+    xy = (np.random.default_rng(1).random((25, 2)) * 0.4e-6).astype(np.float64)
+    f = tmp_path / "positions.csv"
+    f.write_text("".join(f"{float(a)!r},{float(b)!r}\n" for a, b in xy))
+    s = gpu_session(d, probe=d["probe"], lf=str(f))
+    pos, X, Y = oracle.list_mesh(xy, lam, z, dxd, 64)
+    assert np.array_equal(s.positions(), pos) and (s.dims()["X"], s.dims()["Y"]) == (X, Y)
+    s.step()
+    assert np.isfinite(s.object()).all()

@@ -177,3 +177,46 @@ def test_mls_oracle_reduces_the_fourier_error(oracle):
     m = oracle.OracleMls(raw, intens, d["probe"][0])
     errs = [m.step() for _ in range(8)]
     assert np.isfinite(errs).all() and errs[-1] < 0.8 * errs[0]
+
+
+def test_spiral_mesh(oracle):
+    lam, z, dxd, N = 2.48e-10, 1.0, 172e-6, 128
+    dx_s = oracle.lib().orc_sample_pixel(lam, z, dxd, N)
+    P = 100
+    pos, X, Y = oracle.spiral_mesh(P, 50e-9, 50e-9, lam, z, dxd, N)
+    # point i sits at sqrt(i)*(cos, sin)(4 sqrt(i))*step/dx_s before the shift; point 0 is the centre
+    i = np.arange(P, dtype=np.float64)
+    r = np.sqrt(i) * 50e-9 / dx_s
+    ref = np.stack([r * np.cos(4 * np.sqrt(i)), r * np.sin(4 * np.sqrt(i))], 1)
+    d = pos - pos[0]
+    assert np.allclose(d, ref - ref[0], atol=1e-3)
+    # the object covers the whole 1024-point spiral of the mesh array, not only the first P points
+    i2 = np.arange(1024, dtype=np.float64)
+    r2 = np.sqrt(i2) * 50e-9 / dx_s
+    ext = (r2 * np.cos(4 * np.sqrt(i2))).max() - (r2 * np.cos(4 * np.sqrt(i2))).min()
+    assert abs(X - np.ceil(ext + N)) <= 1
+    assert pos.min() >= 0 and (pos + N).max() <= max(X, Y) + 1
+
+
+def test_jitter_stream_and_bounds(oracle):
+    j1 = oracle.mesh_jitter(7, 500, 3)
+    j2 = oracle.mesh_jitter(7, 500, 3)
+    assert np.array_equal(j1, j2)
+    assert (np.abs(j1) <= 3).all() and j1.std() > 1.0
+    assert not np.array_equal(j1, oracle.mesh_jitter(8, 500, 3))
+    assert (oracle.mesh_jitter(7, 10, 0) == 0).all()
+    p0, X0, Y0 = oracle.cartesian_mesh(6, 6, 50e-9, 50e-9, 2.48e-10, 1.0, 172e-6, 64)
+    p1, X1, Y1 = oracle.cartesian_mesh(6, 6, 50e-9, 50e-9, 2.48e-10, 1.0, 172e-6, 64, jitter=2, seed=7)
+    # jitter moves each point by at most the radius relative to the others (the -min shift moves all together)
+    d = (p1 - p1[0]) - (p0 - p0[0])
+    assert np.abs(d).max() <= 4.0 + 1e-4 and np.abs(d).max() > 0.1
+
+
+def test_list_mesh_padding_joins_extent(oracle):
+    # positions far from the origin: the (0, 0) padding of the 1024-wide mesh array enlarges the object
+    xy = np.stack([np.linspace(1e-6, 2e-6, 20), np.linspace(1e-6, 1.5e-6, 20)], 1)
+    pos, X, Y = oracle.list_mesh(xy, 2.48e-10, 1.0, 172e-6, 64)
+    dx_s = oracle.lib().orc_sample_pixel(2.48e-10, 1.0, 172e-6, 64)
+    assert X == int(np.ceil(np.float32(2e-6 / dx_s) + 64))
+    # shifted by the padding's minimum (0), not by the list's own minimum
+    assert abs(pos[:, 0].min() - 1e-6 / dx_s) < 1e-3 and abs(pos[:, 1].min() - 1e-6 / dx_s) < 1e-3
