@@ -12,6 +12,10 @@ patterns in pinned host memory.  Multi-GPU runs (torchrun) are independent repli
 128-512, rasters 10x10-40x40, steps 30-100 nm), `--steps` iterations each, interleaved by pty_batch_run against
 the same scans run one after another.
 
+`--algo nrmse` measures the plain half of the warm-start comparison: ePIE from a flat (zero) object on the
+warm-start workload (64x64 raster at 128^2, 1e5 photons/pattern), iterations and GPU time until the phase NRMSE
+(after phase-ramp removal, central region) reaches 0.05.
+
 `--algo epie --cfg epie128|epie256k5` measures the ePIE configurations instead (10x10 raster at 128^2 with one probe
 mode; 51x51 raster at 256^2 with 5 modes): one step = one ePIE iteration over all positions, after enough warm-up
 iterations that the probe (iteration 10) and the modes (iteration 20) are being updated.
@@ -46,7 +50,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--nx", type=int, default=30, help="raster size (30 = the DM configuration; smaller for profiling)")
     ap.add_argument("--wave", type=int, default=0, help="DM patterns per pipeline wave (0 = automatic)")
-    ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch"])
+    ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch", "nrmse"])
     ap.add_argument("--cfg", default="epie128", choices=["epie128", "epie256k5"], help="ePIE configuration")
     return ap.parse_args()
 
@@ -412,6 +416,65 @@ def run_epie(args, rank, local):
     print(json.dumps(out), flush=True)
 
 
+def run_nrmse(args, rank, local):
+    """Plain ePIE from a flat start on the warm-start workload: iterations and GPU time to phase NRMSE <= 0.05."""
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+
+    from ptychopy_b200 import abi, synth
+
+    torch.cuda.set_device(local)
+    cfg = dict(synth.CONFIGS["warm128"])
+    N = cfg["N"]
+    rng = np.random.default_rng(20261207)
+    dx_s = synth.sample_pixel(cfg["lambd"], cfg["z"], cfg["dx_d"], N)
+    pos, X, Y = synth.raster_positions(cfg["nx"], cfg["ny"], cfg["step"], cfg["step"], dx_s, N)
+    obj = synth.make_object(X, Y, rng)
+    probe = synth.make_probe(N, dx_s, K=1)
+    amp = synth.make_patterns_torch(obj, probe, pos, N, cfg["photons"], seed=20261207, device="cuda")
+    P = pos.shape[0]
+    stream = torch.cuda.Stream()
+    s = abi.Session(size=N, scanDimsx=cfg["nx"], scanDimsy=cfg["ny"], stepx=cfg["step"], stepy=cfg["step"],
+                    lambd=cfg["lambd"], z=cfg["z"], dx_d=cfg["dx_d"], beamSize=synth.BEAM_FWHM, probeModes=1,
+                    algorithm="ePIE", device=local)
+    s.set_stream(stream.cuda_stream)
+    s.set_patterns_ptr(amp.data_ptr(), P, N)
+    s.set_probe(probe)
+    s.init()
+    mask = np.zeros((X, Y), bool)
+    mask[N // 2:X - N // 2, N // 2:Y - N // 2] = True
+    gpu_ms, history, reached = 0.0, [], None
+    max_iters, chunk = max(args.steps, 5), 5
+    it = 0
+    while it < max_iters:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(chunk):
+                s.step()
+            e1.record(stream)
+        stream.synchronize()
+        gpu_ms += e0.elapsed_time(e1)
+        it += chunk
+        err = synth.phase_nrmse(s.object(), obj, mask)
+        history.append([it, round(gpu_ms, 3), err])
+        if err <= 0.05 and reached is None:
+            reached = {"iterations": it, "gpu_ms": gpu_ms}
+            break
+    s.close()
+    print(json.dumps({"metric": "time to phase NRMSE <= 0.05, plain ePIE from a flat start", "unit": "ms",
+                      "value": reached["gpu_ms"] if reached else None, "higher_is_better": False,
+                      "reached": reached, "history": history, "positions": P,
+                      "config": {"workload": f"warm-start workload without the warm start: {cfg['nx']}x{cfg['ny']} "
+                                             f"raster ({P} positions), {N}^2, 1e5 photons/pattern, object {X}x{Y}, "
+                                             "true probe given, zero object",
+                                 "nrmse": "phase NRMSE after offset and linear-ramp removal over the central region "
+                                          "(N/2 margin), checked every 5 iterations"},
+                      "note": "the learned warm start (the other half of the comparison) is not built"}), flush=True)
+
+
 BATCH_SCANS = [  # (algorithm, N, raster, step m)
     ("DM", 128, 10, 30e-9), ("DM", 128, 20, 50e-9), ("DM", 256, 15, 60e-9), ("DM", 256, 25, 80e-9),
     ("DM", 512, 10, 50e-9), ("DM", 512, 20, 100e-9), ("DM", 128, 40, 40e-9), ("DM", 256, 30, 70e-9),
@@ -487,6 +550,8 @@ def main():
         run_epie(args, rank, local)
     elif args.algo == "batch" and args.impl == "b200":
         run_batch(args, rank, local)
+    elif args.algo == "nrmse" and args.impl == "b200":
+        run_nrmse(args, rank, local)
     elif args.impl == "reference":
         run_reference(args, rank)
     else:

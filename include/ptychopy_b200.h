@@ -61,10 +61,11 @@ typedef struct pty_params {
   char lf[256];           /* positions list file or "" */
   int PPS;
   /* --- additions --- */
-  uint64_t seed;          /* seed of the ePIE visiting-order stream (reference: time(NULL)) */
+  uint64_t seed;          /* seed of the ePIE visiting order, the MLs groups and the position jitter (reference:
+                             time(NULL) / rand() / curand) */
   int calculateRMS;       /* compute the per-iteration error metric (the reference's Python path never does) */
   int device;             /* CUDA device ordinal */
-  int wave;               /* DM patterns per pipeline wave (0 = automatic) */
+  int wave;               /* DM patterns per wave of its three kernels (0 = automatic) */
 } pty_params;
 
 typedef struct pty_session pty_session;
