@@ -312,6 +312,304 @@ __global__ void __launch_bounds__(R* FftShape<L>::T) k_epie(EpieArgs g) {
   }
 }
 
+// ---- shared-memory-resident ePIE for windows of L <= 128 with one probe mode -----------------------------------
+// A cluster of C = L/32 CTAs; CTA c owns rows [32c, 32c+32) of the window (and of the probe, which stays in its
+// shared memory for the whole launch) and columns [32c, 32c+32) of the column phase.  The row phase writes the row
+// spectra into the CTA's own slab; the column phase gathers its columns from every CTA's slab through distributed
+// shared memory (row r lives in CTA r/32), transforms, applies the modulus and writes the columns back in place; the inverse row phase reads the slab locally.  The amplitudes of the next position's
+// columns are copied into shared memory (cp.async, natural layout) while the current position runs.  Per position:
+// A rows -> barrier -> B columns -> barrier -> C rows (object update) -> barrier [-> D tile maxima -> barrier ->
+// E probe update in shared memory].  Same equations and order as k_epie (src/ePIE.cpp:65-129).
+template <int L>
+struct EpieSm {
+  static constexpr int T = FftShape<L>::T, E = FftShape<L>::E, R = 32, C = L / 32, NT = R * T;
+  static constexpr int XROWS = R * FftShape<L>::XCH, XCOLS = cols_xch_elems<L>();
+  static constexpr int XS = XROWS > XCOLS ? XROWS : XCOLS;
+  // float2 units: tw | probe | slab | xch, then 2 amplitude buffers (floats)
+  static constexpr size_t SMEM = sizeof(float2) * (L + 2 * size_t(R) * L + XS) + sizeof(float) * 2 * size_t(L) * 32;
+  static_assert(cols_threads<L>() == NT, "column phase uses the CTA's threads");
+  static_assert(cols_per_block<L>() == 32, "32 columns per CTA");
+};
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(NPEND) : "memory"); }
+
+// This CTA's 32 amplitude columns of pattern i (natural layout A[kx][ky]) into dst[kx*32 + cc].
+template <int L>
+__device__ __forceinline__ void epie_sm_fetch_amp(const float* __restrict__ amp, int i, int c, float* dst) {
+  constexpr int CHUNKS = L * 8;  // L rows x 128 bytes
+  const float* src = amp + size_t(i) * L * L + 32 * c;
+  for (int q = threadIdx.x; q < CHUNKS; q += EpieSm<L>::NT) {
+    const int kx = q >> 3, part = q & 7;
+    cp_async16(dst + kx * 32 + part * 4, src + size_t(kx) * L + part * 4);
+  }
+  cp_async_commit();
+}
+
+template <int L>
+__global__ void __launch_bounds__(EpieSm<L>::NT) k_epie_sm(EpieArgs g) {
+  using S = FftShape<L>;
+  using Z = EpieSm<L>;
+  constexpr int T = Z::T, E = Z::E, R = Z::R;
+  constexpr float nrm = 1.0f / float(L * L);
+  extern __shared__ float4 smem4[];
+  float2* s_tw = reinterpret_cast<float2*>(smem4);
+  float2* s_probe = s_tw + L;
+  float2* s_slab = s_probe + R * L;
+  float2* s_x = s_slab + R * L;
+  float* s_amp = reinterpret_cast<float*>(s_x + Z::XS);  // 2 x L x 32
+  __shared__ float s_objmax, s_probemax, s_pmpart;
+
+  cg::cluster_group cl = cg::this_cluster();
+  const int c = int(cl.block_rank());
+  const int v = threadIdx.x / T, t = threadIdx.x % T;  // row phases: local row v, lane t
+  int s, cc;                                            // column phase
+  cols_thread<L>(threadIdx.x, s, cc);
+  const int col = 32 * c + cc;
+  const int x = 32 * c + v;
+
+  load_twiddles<L>(s_tw, g.tw);
+#pragma unroll
+  for (int e = 0; e < E; ++e) s_probe[v * L + t + T * e] = g.probe[size_t(x) * L + t + T * e];
+  if (threadIdx.x == 0) {
+    s_objmax = g.sc->objMax;
+    s_probemax = g.sc->probeMax;
+    s_pmpart = 0.f;
+  }
+  bool pm_valid = false;
+  if (g.P > 0) epie_sm_fetch_amp<L>(g.amp, g.order[0], c, s_amp);
+  __syncthreads();
+  cluster_barrier();  // every CTA of the cluster is running before any distributed shared memory access
+  double err_acc = 0.0;
+  float2 onew[E];
+
+  for (int si = 0; si < g.P; ++si) {
+    const int i = g.order[si];
+    const float2 q = g.pos[i];
+    const int ox = int(roundf(q.x)), oy = int(roundf(q.y));
+    const float* s_A = s_amp + (si & 1) * L * 32;
+    if (si + 1 < g.P)
+      epie_sm_fetch_amp<L>(g.amp, g.order[si + 1], c, s_amp + ((si + 1) & 1) * L * 32);
+    else
+      cp_async_commit();  // keep one group per position so the wait below stays uniform
+
+    // ---------------- A: bilinear patch * probe, row FFT into the slab -------------------------------------------
+    {
+      int r0, r1;
+      float wb;
+      tex_axis(q.x, x, g.X, r0, r1, wb);
+      float2 a[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int y = t + T * e;
+        int c0, c1;
+        float wa;
+        tex_axis(q.y, y, g.Y, c0, c1, wa);
+        const float2 v00 = g.obj[size_t(r0) * g.Y + c0], v01 = g.obj[size_t(r0) * g.Y + c1];
+        const float2 v10 = g.obj[size_t(r1) * g.Y + c0], v11 = g.obj[size_t(r1) * g.Y + c1];
+        const float w00 = (1.f - wa) * (1.f - wb), w01 = wa * (1.f - wb), w10 = (1.f - wa) * wb, w11 = wa * wb;
+        const float2 pt = make_float2(v00.x * w00 + v01.x * w01 + v10.x * w10 + v11.x * w11,
+                                      v00.y * w00 + v01.y * w01 + v10.y * w10 + v11.y * w11);
+        a[e] = cmul(pt, s_probe[v * L + y]);
+      }
+      fft_vec<L, false>(a, t, s_x + v * S::XCH, s_tw);
+      static_for<0, E>([&](auto ec) {
+        constexpr int e = decltype(ec)::value;
+        s_slab[v * L + t + T * e] = a[out_slot<L>(e)];
+      });
+    }
+    cluster_barrier();
+
+    // ---------------- B: columns through distributed shared memory: FFT, modulus, inverse FFT ----------------
+    {
+      float2 a[E];
+      float2* src[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int r = s + T * e;
+        src[e] = cl.map_shared_rank(s_slab, r / 32) + (r % 32) * L + col;
+        a[e] = *src[e];
+      }
+      cp_async_wait<1>();  // this position's amplitudes (the next position's copy may still be in flight)
+      fft_cols<L, false>(a, s, cc, s_x, s_tw);  // its first barrier publishes every thread's amplitude copies
+      static_for<0, E>([&](auto ec) {
+        constexpr int e = decltype(ec)::value;
+        const float A = s_A[(s + T * e) * 32 + cc];
+        const float2 psi = a[out_slot<L>(e)];
+        if (g.rms) err_acc += fabsf(A - sqrtf(psi.x * psi.x + psi.y * psi.y));
+        float2 rep;
+        if (A - g.saturation >= 0.f)
+          rep = make_float2(psi.x * nrm, psi.y * nrm);  // floating pixel: no modulus
+        else
+          rep = modulus_replace(psi, A * nrm);
+        a[out_slot<L>(e)] = make_float2(rep.x - psi.x * nrm, rep.y - psi.y * nrm);
+      });
+      to_input_order<L>(a);
+      fft_cols<L, true>(a, s, cc, s_x, s_tw);
+      static_for<0, E>([&](auto ec) {
+        constexpr int e = decltype(ec)::value;
+        *src[e] = a[out_slot<L>(e)];
+      });
+      if (g.rms) {
+        const double er = block_reduce_sum(err_acc);
+        if (threadIdx.x == 0) atomicAdd(&g.sc->err, er / double(g.sqsum[i]));
+        err_acc = 0.0;
+      }
+    }
+    cluster_barrier();
+
+    // ---------------- C: inverse row FFT, dpsi, object update (global), |O|^2 cache -------------------------
+    {
+      if (pm_valid && threadIdx.x == 0) {  // probe maximum after the previous position's probe update
+        float m = 0.f;
+        for (int r = 0; r < Z::C; ++r) m = fmaxf(m, *cl.map_shared_rank(&s_pmpart, r));
+        s_probemax = m;
+      }
+      float2* orow = g.obj + size_t(x + ox) * g.Y + oy;
+      float* crow = g.ocache + size_t(x + ox) * g.Y + oy;
+      float2 a[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        onew[e] = orow[t + T * e];
+        a[e] = s_slab[v * L + t + T * e];
+      }
+      fft_vec<L, true>(a, t, s_x + v * S::XCH, s_tw);
+      __syncthreads();  // s_probemax
+      const float cO = 1.0f / s_probemax;
+      static_for<0, E>([&](auto ec) {
+        constexpr int e = decltype(ec)::value;
+        const int n = t + T * e;
+        const float2 pv = s_probe[v * L + n];
+        const float2 d = a[out_slot<L>(e)];  // IFFT2(Psi' - Psi/N^2) = psi_new - psi_old
+        s_slab[v * L + n] = d;
+        const float2 inc = cconjmul(pv, d);
+        float2 o = make_float2(onew[e].x + inc.x * cO, onew[e].y + inc.y * cO);
+        const float mag = sqrtf(o.x * o.x + o.y * o.y);
+        if (g.pc) o = constrain_phase(o);
+        orow[n] = o;
+        crow[n] = mag * mag;
+        onew[e] = o;
+      });
+    }
+    cluster_barrier();  // object writes visible to every CTA (next patch, tile maxima)
+    if (!g.up) continue;
+
+    // ---------------- D: refresh tile maxima under the patch, then the global object max ---------------------
+    {
+      const int tr0 = ox / 16, tr1 = (ox + L - 1) / 16, tc0 = oy / 16, tc1 = (oy + L - 1) / 16;
+      const int ntc = tc1 - tc0 + 1, ntiles = (tr1 - tr0 + 1) * ntc;
+      const int warps = Z::NT / 32, gw = c * warps + int(threadIdx.x / 32), lane = threadIdx.x & 31;
+      for (int tile = gw; tile < ntiles; tile += Z::C * warps) {
+        const int tr = tr0 + tile / ntc, tcc = tc0 + tile % ntc;
+        float m = 0.f;
+        for (int j = lane; j < 256; j += 32) {
+          const int xr = tr * 16 + j / 16, yc = tcc * 16 + j % 16;
+          if (xr < g.X && yc < g.Y) m = fmaxf(m, g.ocache[size_t(xr) * g.Y + yc]);
+        }
+        m = warp_reduce_maxf(m);
+        if (lane == 0) g.TM[size_t(tr) * g.TY + tcc] = m;
+      }
+    }
+    cluster_barrier();
+    {
+      float m = 0.f;
+      const int nt = g.TX * g.TY;
+      for (int j = threadIdx.x; j < nt; j += Z::NT) m = fmaxf(m, g.TM[j]);
+      m = block_reduce_maxf(m);
+      if (threadIdx.x == 0) s_objmax = m;
+      __syncthreads();
+    }
+
+    // ---------------- E: probe update in shared memory, partial max of |P|^2 --------------------------------
+    {
+      const float cP = 1.0f / s_objmax;
+      float pmax = 0.f;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int n = t + T * e;
+        const float2 u = cconjmul(onew[e], s_slab[v * L + n]);
+        float2 pv = s_probe[v * L + n];
+        pv = make_float2(u.x * cP + pv.x, u.y * cP + pv.y);
+        const float mg = sqrtf(pv.x * pv.x + pv.y * pv.y);
+        s_probe[v * L + n] = pv;
+        pmax = fmaxf(pmax, mg * mg);
+      }
+      pmax = block_reduce_maxf(pmax);
+      if (threadIdx.x == 0) s_pmpart = pmax;
+      pm_valid = true;
+    }
+  }
+  cp_async_wait<0>();
+  cluster_barrier();  // last partial maxima written
+  if (threadIdx.x == 0 && pm_valid) {
+    float m = 0.f;
+    for (int r = 0; r < Z::C; ++r) m = fmaxf(m, *cl.map_shared_rank(&s_pmpart, r));
+    s_probemax = m;
+  }
+  __syncthreads();
+  // probe rows and their |P|^2 cache back to global memory
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int n = t + T * e;
+    const float2 pv = s_probe[v * L + n];
+    const float mg = sqrtf(pv.x * pv.x + pv.y * pv.y);
+    g.probe[size_t(x) * L + n] = pv;
+    g.pcache[size_t(x) * L + n] = mg * mg;
+  }
+  if (c == 0 && threadIdx.x == 0) {
+    g.sc->objMax = s_objmax;
+    g.sc->probeMax = s_probemax;
+  }
+  cluster_barrier();  // no CTA leaves while another may still read its shared memory
+}
+
+bool epie_uses_smem(int N, int K) { return K == 1 && (N == 32 || N == 64 || N == 128); }
+
+template <int L>
+static cudaError_t epie_sm_prepare_t() {
+  return cudaFuncSetAttribute(k_epie_sm<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(EpieSm<L>::SMEM));
+}
+
+template <int L>
+static cudaError_t epie_sm_launch_t(const EpieArgs& g, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(EpieSm<L>::C);
+  cfg.blockDim = dim3(EpieSm<L>::NT);
+  cfg.dynamicSmemBytes = EpieSm<L>::SMEM;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = EpieSm<L>::C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_epie_sm<L>, g);
+}
+
+cudaError_t epie_sm_prepare(int N) {
+  switch (N) {
+    case 32: return epie_sm_prepare_t<32>();
+    case 64: return epie_sm_prepare_t<64>();
+    case 128: return epie_sm_prepare_t<128>();
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t epie_sm_launch(const EpieArgs& g, cudaStream_t st) {
+  switch (g.N) {
+    case 32: return epie_sm_launch_t<32>(g, st);
+    case 64: return epie_sm_launch_t<64>(g, st);
+    case 128: return epie_sm_launch_t<128>(g, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 // Rows per pass of a CTA (blockDim = R * T) for a length-L window; the cluster takes the largest size (<= 16)
 // whose CTAs hold whole passes.  Each position is a chain of short latency-bound phases: at L = 128, 4 CTAs of 8
 // warps (R = 32) measured no faster than 16 CTAs of 2 warps (3.43 vs 3.21 ms per 100-position iteration).

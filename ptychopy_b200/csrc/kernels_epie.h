@@ -14,7 +14,8 @@ struct EpieScalars {
 };
 
 struct EpieArgs {
-  const float* ampT;      // P x N x N amplitudes, each plane transposed ([ky][kx])
+  const float* ampT;      // P x N x N amplitudes, each plane transposed ([ky][kx]) (k_epie)
+  const float* amp;       // P x N x N amplitudes, natural layout (k_epie_sm)
   float2* obj;            // X x Y
   float* ocache;          // X x Y |O|^2 cache
   float2* probe;          // K x N x N
@@ -36,6 +37,11 @@ struct EpieArgs {
 // Sets kernel attributes and picks the cluster size (largest resident of 16, 8, ...); returns it in C_out.
 cudaError_t epie_prepare(int N, int* C_out);
 cudaError_t epie_launch(const EpieArgs& g, cudaStream_t st);
+// Shared-memory-resident variant for small windows with one probe mode (N = 32, 64, 128; K = 1): cluster of
+// N/32 CTAs, probe and window in (distributed) shared memory, natural-layout amplitudes.
+bool epie_uses_smem(int N, int K);
+cudaError_t epie_sm_prepare(int N);
+cudaError_t epie_sm_launch(const EpieArgs& g, cudaStream_t st);
 // Modes 1..K-1 = 0.05 * mode 0, then Gram-Schmidt against the original copies.
 cudaError_t epie_init_modes(float2* probe, float* pcache, int K, int N, float2* copy, double* scratch3,
                             cudaStream_t st);

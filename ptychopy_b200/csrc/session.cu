@@ -261,6 +261,7 @@ struct EpieState {
   DeviceBuf pos, order, W1, W2, TM, pm, sc, sq, modesCopy, ip;
   int C = 1, TX = 0, TY = 0;
   bool tm_valid = false;
+  bool sm = false;  // shared-memory-resident kernel (small windows, one mode)
   int* order_h = nullptr;  // pinned
   ~EpieState() {
     if (order_h) cudaFreeHost(order_h);
@@ -532,7 +533,11 @@ void init_epie(pty_session* s) {
   auto* ep = new EpieState;
   s->ep = ep;
   const size_t NN = size_t(s->N) * s->N, XY = size_t(s->X) * s->Y;
-  check_cuda(epie_prepare(s->N, &ep->C), "ePIE kernel set-up (cluster size)");
+  ep->sm = epie_uses_smem(s->N, s->K);
+  if (ep->sm)
+    check_cuda(epie_sm_prepare(s->N), "ePIE kernel set-up");
+  else
+    check_cuda(epie_prepare(s->N, &ep->C), "ePIE kernel set-up (cluster size)");
   ep->pos.alloc(sizeof(float2) * s->P, "positions");
   check_cuda(cudaMemcpyAsync(ep->pos.p, s->geo.pos.data(), sizeof(float2) * s->P, cudaMemcpyHostToDevice, s->stream),
              "H2D positions");
@@ -888,6 +893,7 @@ double step_epie(pty_session* s, int it, bool want_err) {
   check_cuda(cudaMemsetAsync(&reinterpret_cast<EpieScalars*>(ep->sc.p)->err, 0, sizeof(double), s->stream), "memset");
   EpieArgs g;
   g.ampT = s->amp.as<float>();
+  g.amp = s->amp.as<float>();
   g.obj = s->obj.as<float2>();
   g.ocache = s->ocache.as<float>();
   g.probe = s->probe.as<float2>();
@@ -918,7 +924,7 @@ double step_epie(pty_session* s, int it, bool want_err) {
   g.up = up;
   g.rms = s->prm.calculateRMS ? 1 : 0;
   g.useAll = s->useAll ? 1 : 0;
-  check_cuda(epie_launch(g, s->stream), "ePIE kernel launch");
+  check_cuda(ep->sm ? epie_sm_launch(g, s->stream) : epie_launch(g, s->stream), "ePIE kernel launch");
   s->launches += 1;
   if (!want_err || !s->prm.calculateRMS) return 0.0;
   double e = 0;
@@ -1124,9 +1130,9 @@ int pty_init(pty_session* s) {
       init_probe(s, avg.as<float>());
     }
     init_object(s);
-    // ePIE's column phase consumes the amplitudes column-wise: transpose each plane once (DM reads them in their
-    // natural layout)
-    if (s->algo == ALGO_EPIE) {
+    // the cluster ePIE kernel's column phase consumes the amplitudes column-wise: transpose each plane once (DM and
+    // the shared-memory ePIE kernel read them in their natural layout)
+    if (s->algo == ALGO_EPIE && !epie_uses_smem(s->N, s->K)) {
       DeviceBuf t;
       t.alloc(s->amp.bytes, "transposed patterns");
       check_cuda(transpose_planes(s->amp.as<float>(), t.as<float>(), s->P, s->N, s->stream), "transpose");
