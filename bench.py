@@ -12,6 +12,9 @@ patterns in pinned host memory.  Multi-GPU runs (torchrun) are independent repli
 128-512, rasters 10x10-40x40, steps 30-100 nm), `--steps` iterations each, interleaved by pty_batch_run against
 the same scans run one after another.
 
+`--algo mls` measures the MLs core on one scan of the batched configuration's MLs range (256^2, 20x20 raster,
+400 positions, groups of 4), with the FP64 oracle on a bounded sample as the CPU reference.
+
 `--algo nrmse` measures the plain half of the warm-start comparison: ePIE from a flat (zero) object on the
 warm-start workload (64x64 raster at 128^2, 1e5 photons/pattern), iterations and GPU time until the phase NRMSE
 (after phase-ramp removal, central region) reaches 0.05.
@@ -50,7 +53,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--nx", type=int, default=30, help="raster size (30 = the DM configuration; smaller for profiling)")
     ap.add_argument("--wave", type=int, default=0, help="DM patterns per pipeline wave (0 = automatic)")
-    ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch", "nrmse"])
+    ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch", "nrmse", "mls"])
     ap.add_argument("--cfg", default="epie128", choices=["epie128", "epie256k5"], help="ePIE configuration")
     return ap.parse_args()
 
@@ -416,6 +419,72 @@ def run_epie(args, rank, local):
     print(json.dumps(out), flush=True)
 
 
+def run_mls(args, rank, local):
+    """MLs core throughput on a 256^2, 20x20 scan (device-timed iterations), FP64 oracle sample as CPU reference."""
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+
+    from ptychopy_b200 import abi, synth
+
+    torch.cuda.set_device(local)
+    N, nx, step = 256, 20, 60e-9
+    lambd, z, dx_d = 2.48e-10, 1.0, 172e-6
+    rng = np.random.default_rng(20261208)
+    dx_s = synth.sample_pixel(lambd, z, dx_d, N)
+    pos, X, Y = synth.raster_positions(nx, nx, step, step, dx_s, N)
+    obj = synth.make_object(X, Y, rng)
+    probe = synth.make_probe(N, dx_s, K=1)
+    intens = synth.make_patterns_torch(obj, probe, pos, N, 1e6, seed=20261208, device="cuda", intensities=True)
+    P = pos.shape[0]
+    stream = torch.cuda.Stream()
+    s = abi.Session(size=N, scanDimsx=nx, scanDimsy=nx, stepx=step, stepy=step, lambd=lambd, z=z, dx_d=dx_d,
+                    beamSize=synth.BEAM_FWHM, probeModes=1, algorithm="MLs", delta_p=0.1, device=local)
+    s.set_stream(stream.cuda_stream)
+    s.set_patterns_ptr(intens.data_ptr(), P, N)
+    s.set_probe(probe)
+    s.init()
+    for _ in range(max(args.warmup, 3)):
+        s.run(1)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    l0 = s.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.start()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        s.run(args.steps)
+        e1.record(stream)
+    stream.synchronize()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = s.launches() - l0
+    finite = bool(np.isfinite(s.object()).all())
+    s.close()
+    out = {"metric": "MLs patterns/s", "value": P * args.steps / (ms / 1000.0), "unit": UNIT, "n_gpus": 1,
+           "steps": args.steps, "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "f32",
+           "data": "synthetic (seeded)",
+           "config": {"workload": f"MLs core, {N}^2, {nx}x{nx} raster ({P} positions, groups of {max(1, P // 100)}), "
+                                  f"delta_p 0.1", "N": N, "positions": P},
+           "gpu_launches": int(launches), "clocks": ck, "finite": finite,
+           "timing": "CUDA events around pty_run (the host builds each iteration's group tables while the GPU runs)"}
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+
+        raw = pyoracle.mls_raw_positions(nx, nx, step, step, dx_s)
+        n = 16
+        sub = intens[:n].cpu().numpy().astype(np.float64)
+        o = pyoracle.OracleMls(raw[:n], sub, probe[0])
+        t0 = time.perf_counter()
+        o.step()
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n / t, "unit": UNIT, "cores": 1, "kind": "port",
+                               "sample": f"1 MLs iteration of the FP64 oracle over {n} of the {P} positions"}
+    print(json.dumps(out), flush=True)
+
+
 def run_nrmse(args, rank, local):
     """Plain ePIE from a flat start on the warm-start workload: iterations and GPU time to phase NRMSE <= 0.05."""
     if rank != 0:
@@ -552,6 +621,8 @@ def main():
         run_batch(args, rank, local)
     elif args.algo == "nrmse" and args.impl == "b200":
         run_nrmse(args, rank, local)
+    elif args.algo == "mls" and args.impl == "b200":
+        run_mls(args, rank, local)
     elif args.impl == "reference":
         run_reference(args, rank)
     else:
