@@ -114,6 +114,14 @@ int pty_step(pty_session* s, double* err);
  * (src/IPhaser.cpp:367-389). */
 int pty_run(pty_session* s, int iters, double* errs);
 
+/* Forward model of simulation mode: amp_out[i] = |FFT2(O_bilinear(pos_px[i]) * P)| (P x N x N float32) for an
+ * object (X x Y complex64), one probe mode (N x N complex64) and pixel positions (P x 2, x = row; the fractional part
+ * is the bilinear texture offset).  Replaces Diffractions::simulate (src/Diffractions.cpp:80-117, d_simulatePSI
+ * src/SampleKernels.cu:113-122); the reference builds its object from PGM images, here the caller passes it.
+ * Pointers may be host or device memory; runs on the current device. */
+int pty_simulate(const float* obj_c64, int X, int Y, const float* probe_c64, int N, const float* pos_px, int P,
+                 float* amp_out);
+
 /* `iters` iterations of each of n initialised sessions (any mix of ePIE, DM and MLs on one device), interleaved:
  * every round enqueues one iteration of every session on that session's own stream, without host
  * synchronisation between DM and MLs steps, so independent scans of uneven sizes share the GPU.  Returns after all

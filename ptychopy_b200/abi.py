@@ -28,7 +28,7 @@ EXPORTS = [
     "pty_params_init", "pty_session_create", "pty_session_destroy", "pty_set_patterns", "pty_set_positions",
     "pty_set_object", "pty_set_probe", "pty_init", "pty_step", "pty_run", "pty_get_dims", "pty_get_object",
     "pty_get_probe", "pty_get_positions", "pty_write_results", "pty_set_stream", "pty_kernel_launches",
-    "pty_last_error", "pty_fft2_dev", "pty_fft2_dev_noalloc", "pty_batch_run",
+    "pty_last_error", "pty_fft2_dev", "pty_fft2_dev_noalloc", "pty_batch_run", "pty_simulate",
 ]
 
 
@@ -86,6 +86,7 @@ def lib():
             "pty_fft2_dev": ([vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
             "pty_fft2_dev_noalloc": ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
             "pty_batch_run": ([ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int], ctypes.c_int),
+            "pty_simulate": ([vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int, vp], ctypes.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -216,6 +217,18 @@ class Session:
 
     def launches(self):
         return int(lib().pty_kernel_launches(self.h))
+
+
+def simulate(obj, probe, pos_px):
+    """Diffraction amplitudes |FFT2(O_bilinear(pos) * P)| (P, N, N) float32 (pty_simulate)."""
+    o = np.ascontiguousarray(obj, np.complex64)
+    p = np.ascontiguousarray(probe, np.complex64)
+    if p.ndim == 3:
+        p = np.ascontiguousarray(p[0])
+    q = np.ascontiguousarray(pos_px, np.float32)
+    out = np.empty((q.shape[0], p.shape[0], p.shape[0]), np.float32)
+    check(lib().pty_simulate(_ptr(o), o.shape[0], o.shape[1], _ptr(p), p.shape[0], _ptr(q), q.shape[0], _ptr(out)))
+    return out
 
 
 def batch_run(sessions, iters):

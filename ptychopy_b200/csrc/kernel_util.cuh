@@ -34,6 +34,19 @@ __device__ __forceinline__ void store_rows_transposed(const float2 (&a)[FftShape
   }
 }
 
+// Texture-coordinate emulation for one axis: integer index idx plus fractional base; clamp addressing.
+__device__ __forceinline__ void tex_axis(float base, int idx, int extent, int& i0, int& i1, float& w) {
+  const float c = float(idx) + base;
+  const float tt = c + 0.5f;
+  const float xb = tt - 0.5f;
+  const float fl = floorf(xb);
+  const float fr = xb - fl;
+  w = floorf(fr * 256.f + 0.5f) * (1.f / 256.f);
+  int i = int(fl);
+  i0 = min(max(i, 0), extent - 1);
+  i1 = min(max(i + 1, 0), extent - 1);
+}
+
 // Modulus replacement amp * exp(i*arg(psi)) (src/SampleKernels.cu:436-450, src/utilitiesKernels.cu:626-631).
 // The reference takes arg through atan2; psi/|psi| is the same direction.  psi == 0 maps to phase 0.
 __device__ __forceinline__ float2 modulus_replace(float2 psi, float amp) {

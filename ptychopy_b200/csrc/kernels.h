@@ -30,6 +30,9 @@ cudaError_t reduce_abs_max(const float2* a, size_t n, double* out, cudaStream_t 
 cudaError_t reduce_sum_sq(const float2* a, size_t n, double* out, cudaStream_t st);
 cudaError_t scale_by_inverse(float2* a, size_t n, const double* denom, cudaStream_t st);
 cudaError_t abs2(const float2* a, float* out, size_t n, cudaStream_t st);
+// Forward model: amp[i] = |FFT2(bilinear O at pos[i] * probe)| for `count` positions (psi, work: count*N*N).
+cudaError_t simulate_patterns(const float2* obj, int X, int Y, const float2* probe, int N, const float2* pos,
+                              int count, float2* psi, float2* work, const float2* tw, float* amp, cudaStream_t st);
 cudaError_t scale_complex(float2* a, size_t n, float s, cudaStream_t st);
 cudaError_t fill_complex(float2* a, size_t n, float2 v, cudaStream_t st);
 // out[p] = sum of plane p (P planes of NN floats), in double: Diffractions::fillSquaredSums.

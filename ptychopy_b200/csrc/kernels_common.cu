@@ -272,4 +272,46 @@ cudaError_t plane_sums(const float* a, int P, size_t NN, double* out, cudaStream
   return cudaGetLastError();
 }
 
+// Forward model of simulation mode (Diffractions::simulate, src/Diffractions.cpp:80-117, with d_simulatePSI,
+// src/SampleKernels.cu:113-122): psi = bilinear O at (x + qx, y + qy) (texture fetch, 1/256 weights, clamp) times the
+// probe, then FFT2 and modulus.  This kernel writes psi for `count` positions starting at pos.
+__global__ void k_simulate_psi(const float2* __restrict__ obj, int X, int Y, const float2* __restrict__ probe, int N,
+                               const float2* __restrict__ pos, int count, float2* __restrict__ psi) {
+  const int i = blockIdx.y;
+  if (i >= count) return;
+  const float2 q = pos[i];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N * N; k += gridDim.x * blockDim.x) {
+    const int x = k / N, y = k % N;
+    int r0, r1, c0, c1;
+    float wb, wa;
+    tex_axis(q.x, x, X, r0, r1, wb);
+    tex_axis(q.y, y, Y, c0, c1, wa);
+    const float2 v00 = obj[size_t(r0) * Y + c0], v01 = obj[size_t(r0) * Y + c1];
+    const float2 v10 = obj[size_t(r1) * Y + c0], v11 = obj[size_t(r1) * Y + c1];
+    const float w00 = (1.f - wa) * (1.f - wb), w01 = wa * (1.f - wb), w10 = (1.f - wa) * wb, w11 = wa * wb;
+    const float2 pt = make_float2(v00.x * w00 + v01.x * w01 + v10.x * w10 + v11.x * w11,
+                                  v00.y * w00 + v01.y * w01 + v10.y * w10 + v11.y * w11);
+    psi[size_t(i) * N * N + k] = cmul(pt, probe[k]);
+  }
+}
+
+__global__ void k_abs(const float2* __restrict__ in, size_t n, float* __restrict__ out) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    const float2 v = in[i];
+    out[i] = sqrtf(v.x * v.x + v.y * v.y);
+  }
+}
+
+cudaError_t simulate_patterns(const float2* obj, int X, int Y, const float2* probe, int N, const float2* pos,
+                              int count, float2* psi, float2* work, const float2* tw, float* amp, cudaStream_t st) {
+  const int gx = (N * N + 255) / 256 < 64 ? (N * N + 255) / 256 : 64;
+  k_simulate_psi<<<dim3(gx, count), 256, 0, st>>>(obj, X, Y, probe, N, pos, count, psi);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if ((e = fft2(psi, work, tw, count, N, false, st)) != cudaSuccess) return e;
+  const size_t n = size_t(count) * N * N;
+  k_abs<<<reduce_grid(n), 256, 0, st>>>(psi, n, amp);
+  return cudaGetLastError();
+}
+
 }  // namespace pty

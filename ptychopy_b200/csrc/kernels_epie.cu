@@ -35,18 +35,6 @@ __device__ __forceinline__ void cluster_barrier() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
-// Texture-coordinate emulation for one axis: integer index idx plus fractional base; clamp addressing.
-__device__ __forceinline__ void tex_axis(float base, int idx, int extent, int& i0, int& i1, float& w) {
-  const float c = float(idx) + base;
-  const float tt = c + 0.5f;
-  const float xb = tt - 0.5f;
-  const float fl = floorf(xb);
-  const float fr = xb - fl;
-  w = floorf(fr * 256.f + 0.5f) * (1.f / 256.f);
-  int i = int(fl);
-  i0 = min(max(i, 0), extent - 1);
-  i1 = min(max(i + 1, 0), extent - 1);
-}
 
 template <int L, int R>
 __global__ void __launch_bounds__(R* FftShape<L>::T) k_epie(EpieArgs g) {

@@ -1191,6 +1191,52 @@ int pty_run(pty_session* s, int iters, double* errs) {
   });
 }
 
+int pty_simulate(const float* obj_c64, int X, int Y, const float* probe_c64, int N, const float* pos_px, int P,
+                 float* amp_out) {
+  return guarded([&] {
+    need(obj_c64 && probe_c64 && pos_px && amp_out, "null argument");
+    need(X >= N && Y >= N && P >= 0, "object smaller than the probe window or negative pattern count");
+    need(fft_size_supported(N), "N must be 32, 64, 128, 256 or 512");
+    for (int i = 0; i < P; ++i)
+      need(pos_px[2 * i] >= 0 && pos_px[2 * i + 1] >= 0, "position " + std::to_string(i) + " is negative");
+    const size_t NN = size_t(N) * N, XY = size_t(X) * Y;
+    const int chunk = int(std::max<size_t>(1, std::min<size_t>(size_t(P), (size_t(256) << 20) / (16 * NN))));
+    cudaStream_t st = nullptr;
+    check_cuda(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+    DeviceBuf obj, probe, pos, psi, work, amp;
+    float2* tw = nullptr;
+    try {
+      obj.alloc(sizeof(float2) * XY, "object");
+      probe.alloc(sizeof(float2) * NN, "probe");
+      pos.alloc(sizeof(float2) * std::max(P, 1), "positions");
+      psi.alloc(sizeof(float2) * NN * chunk, "exit waves");
+      work.alloc(sizeof(float2) * NN * chunk, "FFT work");
+      amp.alloc(sizeof(float) * NN * chunk, "amplitudes");
+      check_cuda(cudaMemcpyAsync(obj.p, obj_c64, obj.bytes, cudaMemcpyDefault, st), "copy object");
+      check_cuda(cudaMemcpyAsync(probe.p, probe_c64, probe.bytes, cudaMemcpyDefault, st), "copy probe");
+      if (P) check_cuda(cudaMemcpyAsync(pos.p, pos_px, sizeof(float2) * P, cudaMemcpyDefault, st), "copy positions");
+      check_cuda(make_twiddles(N, &tw, st), "twiddles");
+      for (int i0 = 0; i0 < P; i0 += chunk) {
+        const int cnt = std::min(chunk, P - i0);
+        check_cuda(simulate_patterns(obj.as<float2>(), X, Y, probe.as<float2>(), N, pos.as<float2>() + i0, cnt,
+                                     psi.as<float2>(), work.as<float2>(), tw, amp.as<float>(), st),
+                   "simulate");
+        check_cuda(cudaMemcpyAsync(amp_out + size_t(i0) * NN, amp.p, sizeof(float) * NN * cnt, cudaMemcpyDefault, st),
+                   "copy amplitudes");
+        check_cuda(cudaStreamSynchronize(st), "simulate");
+      }
+    } catch (...) {
+      cudaStreamSynchronize(st);
+      if (tw) cudaFree(tw);
+      cudaStreamDestroy(st);
+      throw;
+    }
+    cudaStreamSynchronize(st);
+    cudaFree(tw);
+    cudaStreamDestroy(st);
+  });
+}
+
 int pty_batch_run(pty_session* const* sessions, int n, int iters) {
   return guarded([&] {
     need(sessions && n > 0, "no sessions");
