@@ -114,6 +114,22 @@ int pty_step(pty_session* s, double* err);
  * (src/IPhaser.cpp:367-389). */
 int pty_run(pty_session* s, int iters, double* errs);
 
+/* Multi-GPU DM by position shards (one process per GPU).  The reference runs one GPU per reconstruction (its
+ * MPIPhaser stitches separate reconstructions and is not a counterpart); DM's increments are sums over positions, so
+ * a scan splits over GPUs with one reduction of the increments per iteration.
+ *
+ * pty_set_shard: this session holds positions [first, first + P) of a scan of `total` positions, P being the pattern
+ * count given to pty_set_patterns; geometry and object size are the whole scan's.  Call before pty_init; DM only; the
+ * probe must be given (probeNP or probeGuess).  Sharded sessions step with pty_dm_step_local (this shard's waves:
+ * the object / probe increments accumulate on the device), a sum of the increments over all shards in place on the
+ * session's stream (pty_dm_increments gives the complex64 buffers and their element counts; e.g. an NCCL
+ * all-reduce), then pty_dm_step_finish (apply, intensity sums, factors), after which every shard holds the same
+ * object and probe. */
+int pty_set_shard(pty_session* s, int first, int total);
+int pty_dm_step_local(pty_session* s);
+int pty_dm_increments(pty_session* s, void** dO, size_t* n_obj, void** dP, size_t* n_probe);
+int pty_dm_step_finish(pty_session* s);
+
 /* Forward model of simulation mode: amp_out[i] = |FFT2(O_bilinear(pos_px[i]) * P)| (P x N x N float32) for an
  * object (X x Y complex64), one probe mode (N x N complex64) and pixel positions (P x 2, x = row; the fractional part
  * is the bilinear texture offset).  Replaces Diffractions::simulate (src/Diffractions.cpp:80-117, d_simulatePSI

@@ -392,9 +392,13 @@ template <typename R> double sum_sq(const cx<R>* a, size_t n) {
   return t;
 }
 
+// Sum of the iteration's object / probe increments over position shards (interleaved re, im doubles), in place;
+// identity when the whole scan is in one session.
+typedef void (*DmReduceFn)(double* dO, size_t n_obj, double* dP, size_t n_probe, void* user);
+
 template <typename R>
 void dm_iteration(State<R>& s, DMState<R>& d, const R* amp, const float* pos, const Flags& fl, int iter,
-                  int nthreads) {
+                  int nthreads, DmReduceFn reduce = nullptr, void* reduce_user = nullptr) {
   const int N = s.N, P = s.P;
   const size_t NN = size_t(N) * N, XY = size_t(s.X) * s.Y;
   const bool pc = iter <= fl.phaseConstraint, up = iter >= fl.updateProbe;
@@ -450,11 +454,21 @@ void dm_iteration(State<R>& s, DMState<R>& d, const R* amp, const float* pos, co
     for (int t = 0; t < nthreads; ++t) th.emplace_back(work, t);
     for (auto& x : th) x.join();
   }
-  for (int t = 0; t < nthreads; ++t) {
-    for (size_t i = 0; i < XY; ++i) s.O[i] += dO[t][i];
-    if (up)
-      for (size_t i = 0; i < NN; ++i) s.Pr[i] += dP[t][i];
+  for (int t = 1; t < nthreads; ++t) {
+    for (size_t i = 0; i < XY; ++i) dO[0][i] += dO[t][i];
+    for (size_t i = 0; i < NN; ++i) dP[0][i] += dP[t][i];
   }
+  if (reduce) {  // position shards: every shard adds the others' increments before applying them
+    std::vector<double> bo(2 * XY), bp(2 * NN);
+    for (size_t i = 0; i < XY; ++i) { bo[2 * i] = double(dO[0][i].real()); bo[2 * i + 1] = double(dO[0][i].imag()); }
+    for (size_t i = 0; i < NN; ++i) { bp[2 * i] = double(dP[0][i].real()); bp[2 * i + 1] = double(dP[0][i].imag()); }
+    reduce(bo.data(), XY, bp.data(), NN, reduce_user);
+    for (size_t i = 0; i < XY; ++i) dO[0][i] = cx<R>(R(bo[2 * i]), R(bo[2 * i + 1]));
+    for (size_t i = 0; i < NN; ++i) dP[0][i] = cx<R>(R(bp[2 * i]), R(bp[2 * i + 1]));
+  }
+  for (size_t i = 0; i < XY; ++i) s.O[i] += dO[0][i];
+  if (up)
+    for (size_t i = 0; i < NN; ++i) s.Pr[i] += dP[0][i];
   // updateIntensities(true) on object and probe: sums of |.|^2 (all stacked modes for the probe)
   s.objMax = R(sum_sq(s.O.data(), XY));
   s.probeMax = R(sum_sq(s.Pr.data(), size_t(s.K) * NN));
@@ -909,6 +923,7 @@ int orc_extract_patch(const double* obj, int X, int Y, float qx, float qy, int N
 namespace {
 struct OrcBase {
   virtual ~OrcBase() {}
+  virtual void set_reduce(DmReduceFn fn, void* user) = 0;
   virtual int step(double* err) = 0;
   virtual void get(double* obj, double* probe, double* scalars) = 0;
   virtual void psi(double* out) = 0;
@@ -916,6 +931,8 @@ struct OrcBase {
 
 template <typename R> struct OrcSessionT : OrcBase {
   int algo = 0, iter = 0, nthreads = 1;
+  DmReduceFn reduce = nullptr;
+  void* reduce_user = nullptr;
   State<R> s;
   DMState<R> d;
   Flags fl;
@@ -930,9 +947,13 @@ template <typename R> struct OrcSessionT : OrcBase {
     if (algo == 0)
       e = double(epie_iteration<R>(s, amp.data(), pos.data(), sq.data(), fl, it, rng, &status));
     else
-      dm_iteration<R>(s, d, amp.data(), pos.data(), fl, it, nthreads);
+      dm_iteration<R>(s, d, amp.data(), pos.data(), fl, it, nthreads, reduce, reduce_user);
     if (err) *err = e;
     return status;
+  }
+  void set_reduce(DmReduceFn fn, void* user) override {
+    reduce = fn;
+    reduce_user = user;
   }
   void get(double* obj, double* probe, double* scalars) override {
     store_state(s, obj, probe);
@@ -992,6 +1013,13 @@ void* orc_create2(int precision, int algo, int N, int K, int P, int X, int Y, co
                                phaseConstraint, updateProbe, updateModes, calculateRMS, nthreads);
   return make_session<double>(algo, N, K, P, X, Y, amp, pos, obj, probe, probeGuessPath, modesGiven, seed,
                               phaseConstraint, updateProbe, updateModes, calculateRMS, nthreads);
+}
+
+// DM position shards: fn sums the increments over all shards in place (a host-side all-reduce); the session then
+// holds its shard's patterns and positions and the whole scan's object size.
+int orc_set_dm_reduce(void* h, DmReduceFn fn, void* user) {
+  static_cast<OrcBase*>(h)->set_reduce(fn, user);
+  return 0;
 }
 
 void* orc_create(int algo, int N, int K, int P, int X, int Y, const double* amp, const float* pos,

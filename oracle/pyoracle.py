@@ -44,6 +44,7 @@ def lib():
             "orc_list_mesh_j": ([vp, i, d, d, d, i, i, ctypes.c_uint, u64, vp, vp], i),
             "orc_spiral_mesh": ([i, d, d, d, d, d, i, i, ctypes.c_uint, u64, vp, vp], i),
             "orc_mesh_jitter": ([u64, i, ctypes.c_uint, vp], i),
+            "orc_set_dm_reduce": ([vp, vp, vp], i),
             "orc_probe_guess": ([vp, i, i, d, d, i, vp], i),
             "orc_visiting_order": ([ctypes.POINTER(u64), i, vp], None),
             "orc_extract_patch": ([vp, i, i, f, f, i, vp], i),
@@ -155,6 +156,19 @@ class OracleSession:
                                   seed, phaseConstraint, updateProbe, updateModes, calculateRMS, nthreads)
         if not self.h:
             raise ValueError("oracle rejected the configuration")
+
+    # DM position shards: fn(dO, dP) receives the iteration's increments as complex128 arrays (object, probe) and
+    # must sum them over all shards in place.
+    REDUCE = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t, ctypes.POINTER(ctypes.c_double),
+                              ctypes.c_size_t, ctypes.c_void_p)
+
+    def set_dm_reduce(self, fn):
+        def hook(po, no, pp, npr, _user):
+            dO = np.ctypeslib.as_array(po, shape=(2 * no,)).view(np.complex128)
+            dP = np.ctypeslib.as_array(pp, shape=(2 * npr,)).view(np.complex128)
+            fn(dO, dP)
+        self._reduce = self.REDUCE(hook)  # keep the callback alive
+        lib().orc_set_dm_reduce(self.h, ctypes.cast(self._reduce, ctypes.c_void_p), None)
 
     def step(self):
         e = ctypes.c_double(0)

@@ -29,6 +29,7 @@ EXPORTS = [
     "pty_set_object", "pty_set_probe", "pty_init", "pty_step", "pty_run", "pty_get_dims", "pty_get_object",
     "pty_get_probe", "pty_get_positions", "pty_write_results", "pty_set_stream", "pty_kernel_launches",
     "pty_last_error", "pty_fft2_dev", "pty_fft2_dev_noalloc", "pty_batch_run", "pty_simulate",
+    "pty_set_shard", "pty_dm_step_local", "pty_dm_increments", "pty_dm_step_finish",
 ]
 
 
@@ -87,6 +88,11 @@ def lib():
             "pty_fft2_dev_noalloc": ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
             "pty_batch_run": ([ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "pty_simulate": ([vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int, vp], ctypes.c_int),
+            "pty_set_shard": ([vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+            "pty_dm_step_local": ([vp], ctypes.c_int),
+            "pty_dm_increments": ([vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(vp),
+                                   ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
+            "pty_dm_step_finish": ([vp], ctypes.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -217,6 +223,23 @@ class Session:
 
     def launches(self):
         return int(lib().pty_kernel_launches(self.h))
+
+    # ---- DM position shards (multi-GPU) ----
+    def set_shard(self, first, total):
+        check(lib().pty_set_shard(self.h, first, total))
+
+    def step_local(self):
+        check(lib().pty_dm_step_local(self.h))
+
+    def increments(self):
+        """(dO pointer, object elements, dP pointer, probe elements): complex64 device buffers."""
+        o, p = ctypes.c_void_p(), ctypes.c_void_p()
+        no, npr = ctypes.c_size_t(), ctypes.c_size_t()
+        check(lib().pty_dm_increments(self.h, ctypes.byref(o), ctypes.byref(no), ctypes.byref(p), ctypes.byref(npr)))
+        return o.value, no.value, p.value, npr.value
+
+    def step_finish(self):
+        check(lib().pty_dm_step_finish(self.h))
 
 
 def simulate(obj, probe, pos_px):

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <limits>
 #include <sstream>
 #include <string>
@@ -434,16 +435,20 @@ void init_geometry(pty_session* s) {
   // else the Cartesian raster
   need(p.jitterRadius >= 0, "jitterRadius must be >= 0");
   const unsigned jit = unsigned(p.jitterRadius);
+  const int Ptot = s->shard_total > 0 ? s->shard_total : s->P;  // the whole scan's positions
   if (!s->pos_m.empty()) {
     s->geo = list_geometry(s->pos_m, dx_s, s->N, p.flipScanAxis != 0, jit, p.seed);
   } else if (p.lf[0]) {
-    s->geo = list_geometry(read_position_file(p.lf, s->P), dx_s, s->N, p.flipScanAxis != 0, jit, p.seed);
+    s->geo = list_geometry(read_position_file(p.lf, Ptot), dx_s, s->N, p.flipScanAxis != 0, jit, p.seed);
   } else if (p.spiralScan) {
-    s->geo = spiral_geometry(s->P, p.stepx, p.stepy, dx_s, s->N, p.flipScanAxis != 0, jit, p.seed);
+    s->geo = spiral_geometry(Ptot, p.stepx, p.stepy, dx_s, s->N, p.flipScanAxis != 0, jit, p.seed);
   } else {
     s->geo = cartesian_geometry(p.scanDimsx, p.scanDimsy, p.stepx, p.stepy, dx_s, s->N, p.mirror1stScanAxis != 0,
                                 p.mirror2ndScanAxis != 0, p.flipScanAxis != 0, jit, p.seed);
   }
+  if (s->shard_total > 0)  // keep this shard's positions; the object size stays the whole scan's
+    s->geo.pos = std::vector<float>(s->geo.pos.begin() + 2 * size_t(s->shard_first),
+                                    s->geo.pos.begin() + 2 * size_t(s->shard_first + s->P));
   s->X = s->geo.X;
   s->Y = s->geo.Y;
   s->offs.resize(2 * size_t(s->P));
@@ -853,6 +858,51 @@ void step_dm(pty_session* s, int it) {
   s->launches += 3 * int64_t(s->nwaves) + 2;
 }
 
+// Sharded DM: the waves of iteration `it` (increments accumulate in dO / dP) and, separately, their application.
+static cudaGraphExec_t capture_graph(pty_session* s, const std::function<cudaError_t()>& body) {
+  cudaGraph_t graph = nullptr;
+  check_cuda(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  const cudaError_t err = body();
+  const cudaError_t e2 = cudaStreamEndCapture(s->stream, &graph);
+  check_cuda(err, "capture");
+  check_cuda(e2, "end capture");
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t e3 = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  check_cuda(e3, "graph instantiate");
+  return exec;
+}
+
+void step_dm_local(pty_session* s, int it) {
+  const bool pc = it <= s->prm.phaseConstraint, up = it >= s->prm.updateProbe;
+  const int gi = (pc ? 1 : 0) | (up ? 2 : 0);
+  if (!s->graphs_local[gi]) {
+    const DMBuffers b = dm_buffers(s);
+    s->graphs_local[gi] = capture_graph(s, [&]() {
+      cudaError_t err = cudaSuccess;
+      for (int w = 0; w < s->nwaves && err == cudaSuccess; ++w) {
+        DMWave wv;
+        wv.slot_pat = s->slots.as<int>() + size_t(w) * s->wave;
+        wv.count = std::min(s->wave, s->P - w * s->wave);
+        err = dm_wave(b, wv, pc, up, s->stream, nullptr);
+      }
+      return err;
+    });
+  }
+  check_cuda(cudaGraphLaunch(s->graphs_local[gi], s->stream), "DM graph launch");
+  s->launches += 3 * int64_t(s->nwaves);
+}
+
+void step_dm_finish(pty_session* s, int it) {
+  const bool up = it >= s->prm.updateProbe;
+  if (!s->graphs_fin[up ? 1 : 0]) {
+    const DMBuffers b = dm_buffers(s);
+    s->graphs_fin[up ? 1 : 0] = capture_graph(s, [&]() { return dm_finalize(b, up, s->stream, nullptr); });
+  }
+  check_cuda(cudaGraphLaunch(s->graphs_fin[up ? 1 : 0], s->stream), "DM graph launch");
+  s->launches += 2;
+}
+
 // One ePIE iteration: the modal switch on the host side (beginModalReconstruction), then the persistent kernel.
 double step_epie(pty_session* s, int it, bool want_err) {
   EpieState* ep = s->ep;
@@ -940,6 +990,10 @@ void destroy_session(pty_session* s) {
   cudaSetDevice(s->dev);
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (auto& g : s->graphs)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto& g : s->graphs_local)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto& g : s->graphs_fin)
     if (g) cudaGraphExecDestroy(g);
   delete s->ep;
   s->ep = nullptr;
@@ -1096,12 +1150,22 @@ int pty_init(pty_session* s) {
     need(s->have_patterns, "no diffraction patterns (diffractionNP) were given", PTY_ERR_STATE);
     set_device(s);
     const pty_params& p = s->prm;
-    if (s->pos_m.empty())
+    const int Ptot = s->pos_m.empty() ? p.scanDimsx * p.scanDimsy : int(s->pos_m.size() / 2);
+    if (s->shard_total > 0) {
+      need(s->algo == ALGO_DM, "position shards are supported for DM only", PTY_ERR_UNSUPPORTED);
+      need(s->shard_total == Ptot, "the shard's scan has " + std::to_string(s->shard_total) +
+                                       " positions but the parameters describe " + std::to_string(Ptot));
+      need(s->shard_first + s->P <= Ptot, "shard [" + std::to_string(s->shard_first) + ", " +
+                                              std::to_string(s->shard_first + s->P) + ") exceeds the scan");
+      need(!s->probe_h.empty() || p.probeGuess[0],
+           "a DM shard needs the probe (probeNP or probeGuess): the guess uses every pattern of the scan");
+    } else if (s->pos_m.empty()) {
       need(s->P == p.scanDimsx * p.scanDimsy,
            "pattern count " + std::to_string(s->P) + " differs from scanDimsx*scanDimsy = " +
                std::to_string(p.scanDimsx * p.scanDimsy));
-    else
+    } else {
       need(int(s->pos_m.size() / 2) == s->P, "positionNP and diffractionNP have different lengths");
+    }
     float2* twp = nullptr;
     check_cuda(make_twiddles(s->N, &twp, s->stream), "twiddles");
     s->tw.p = twp;
@@ -1151,6 +1215,8 @@ int pty_init(pty_session* s) {
 int pty_step(pty_session* s, double* err) {
   return guarded([&] {
     need(s && s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    need(s->shard_total == 0, "a position shard steps with pty_dm_step_local, a reduction, pty_dm_step_finish",
+         PTY_ERR_STATE);
     set_device(s);
     const int it = s->iter + 1;
     double e = 0;
@@ -1168,6 +1234,8 @@ int pty_step(pty_session* s, double* err) {
 int pty_run(pty_session* s, int iters, double* errs) {
   return guarded([&] {
     need(s && s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    need(s->shard_total == 0, "a position shard steps with pty_dm_step_local, a reduction, pty_dm_step_finish",
+         PTY_ERR_STATE);
     need(iters >= 0, "negative iteration count");
     set_device(s);
     const auto t0 = std::chrono::steady_clock::now();
@@ -1188,6 +1256,50 @@ int pty_run(pty_session* s, int iters, double* errs) {
       }
     }
     check_cuda(cudaStreamSynchronize(s->stream), "pty_run");
+  });
+}
+
+int pty_set_shard(pty_session* s, int first, int total) {
+  return guarded([&] {
+    need(s != nullptr, "null session");
+    need(!s->initialized, "the shard must be set before pty_init", PTY_ERR_STATE);
+    need(first >= 0 && total >= 1, "shard start must be >= 0 and the scan size >= 1");
+    s->shard_first = first;
+    s->shard_total = total;
+  });
+}
+
+int pty_dm_step_local(pty_session* s) {
+  return guarded([&] {
+    need(s && s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    need(s->algo == ALGO_DM, "pty_dm_step_local is for DM sessions", PTY_ERR_STATE);
+    need(s->pending_iter == 0, "pty_dm_step_finish has not run for the previous local step", PTY_ERR_STATE);
+    set_device(s);
+    const int it = s->iter + 1;
+    step_dm_local(s, it);
+    s->pending_iter = it;
+  });
+}
+
+int pty_dm_increments(pty_session* s, void** dO, size_t* n_obj, void** dP, size_t* n_probe) {
+  return guarded([&] {
+    need(s && s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    need(s->algo == ALGO_DM, "increments exist for DM sessions only", PTY_ERR_STATE);
+    if (dO) *dO = s->dO.p;
+    if (n_obj) *n_obj = size_t(s->X) * s->Y;
+    if (dP) *dP = s->dP.p;
+    if (n_probe) *n_probe = size_t(s->N) * s->N;
+  });
+}
+
+int pty_dm_step_finish(pty_session* s) {
+  return guarded([&] {
+    need(s && s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    need(s->pending_iter > 0, "pty_dm_step_local has not run", PTY_ERR_STATE);
+    set_device(s);
+    step_dm_finish(s, s->pending_iter);
+    s->iter = s->pending_iter;
+    s->pending_iter = 0;
   });
 }
 
@@ -1245,6 +1357,7 @@ int pty_batch_run(pty_session* const* sessions, int n, int iters) {
       need(sessions[i] != nullptr, "null session in the batch");
       need(sessions[i]->initialized, "pty_init has not run for session " + std::to_string(i), PTY_ERR_STATE);
       need(sessions[i]->dev == sessions[0]->dev, "batched sessions must share one device");
+      need(sessions[i]->shard_total == 0, "position shards do not run in a batch", PTY_ERR_STATE);
     }
     set_device(sessions[0]);
     // round-robin: one iteration of every scan per round, each on its own stream, no host synchronisation for DM

@@ -96,6 +96,12 @@ struct pty_session {
   pty::DeviceBuf psi, dO, dP, W1, W2, slots;
   int wave = 0, nwaves = 0;
   cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
+  // position sharding (DM over several GPUs): this session holds positions [shard_first, shard_first + P) of a scan
+  // of shard_total positions; local step (waves) and finish (apply the summed increments) are separate graphs
+  int shard_first = 0, shard_total = 0;
+  cudaGraphExec_t graphs_local[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaGraphExec_t graphs_fin[2] = {nullptr, nullptr};
+  int pending_iter = 0;
   // ePIE
   pty::EpieState* ep = nullptr;
   // MLs
