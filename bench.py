@@ -8,6 +8,10 @@ patterns in pinned host memory.  Multi-GPU runs (torchrun) are independent repli
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
+`--shard` (with torchrun, N GPUs) splits the DM scan's positions over the ranks: each rank steps its share, the
+object / probe increments are summed with one NCCL all-reduce per iteration, and every rank applies the sum
+(strong scaling: the whole job is the 900-pattern iteration).
+
 `--algo batch` measures the batched configuration: 16 independent scans of uneven sizes (8 DM, 8 MLs; detectors
 128-512, rasters 10x10-40x40, steps 30-100 nm), `--steps` iterations each, interleaved by pty_batch_run against
 the same scans run one after another.
@@ -54,6 +58,9 @@ def parse():
     ap.add_argument("--nx", type=int, default=30, help="raster size (30 = the DM configuration; smaller for profiling)")
     ap.add_argument("--wave", type=int, default=0, help="DM patterns per pipeline wave (0 = automatic)")
     ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch", "nrmse", "mls"])
+    ap.add_argument("--shard", action="store_true",
+                    help="N>1: split the 900 positions over the GPUs (one NCCL all-reduce of the DM increments per "
+                         "iteration, strong scaling) instead of independent replicas")
     ap.add_argument("--cfg", default="epie128", choices=["epie128", "epie256k5"], help="ePIE configuration")
     return ap.parse_args()
 
@@ -218,6 +225,19 @@ def run_reference(args, rank):
     }))
 
 
+class _DeviceBuf:
+    """A float32 view of a complex64 device buffer (length 2n) for torch, through __cuda_array_interface__."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (2 * n,), "typestr": "<f4", "data": (ptr, False), "version": 3}
+
+
+def _device_view(ptr, n):
+    import torch
+
+    return torch.as_tensor(_DeviceBuf(ptr, n), device="cuda")
+
+
 def run_b200(args, rank, world, local):
     import numpy as np
     import torch
@@ -226,7 +246,7 @@ def run_b200(args, rank, world, local):
 
     torch.cuda.set_device(local)
     dist = None
-    if world > 1:
+    if world > 1 or args.shard:
         import datetime
 
         import torch.distributed as dist
@@ -235,12 +255,33 @@ def run_b200(args, rank, world, local):
     ds = dataset("cuda", args.nx)
     N, P = ds["N"], ds["P"]
     stream = torch.cuda.Stream()
+    shard = args.shard
     s = abi.Session(**dict(ds["kwargs"], algorithm="DM", device=local, wave=args.wave))
     s.set_stream(stream.cuda_stream)
-    s.set_patterns_ptr(ds["amp"].data_ptr(), P, N)
+    if shard:
+        bounds = [P * r // world for r in range(world + 1)]
+        first, count = bounds[rank], bounds[rank + 1] - bounds[rank]
+        s.set_shard(first, P)
+        s.set_patterns_ptr(ds["amp"][first:first + count].data_ptr(), count, N)
+        s.set_probe(ds["probe"])
+        dO_ptr, n_obj, dP_ptr, n_probe = None, 0, None, 0
+    else:
+        s.set_patterns_ptr(ds["amp"].data_ptr(), P, N)
     s.init()
+    if shard:
+        dO_ptr, n_obj, dP_ptr, n_probe = s.increments()
+        t_dO, t_dP = _device_view(dO_ptr, n_obj), _device_view(dP_ptr, n_probe)
+
+        def step():
+            s.step_local()
+            with torch.cuda.stream(stream):
+                dist.all_reduce(t_dO)
+                dist.all_reduce(t_dP)
+            s.step_finish()
+    else:
+        step = s.step
     for _ in range(args.warmup):
-        s.step()
+        step()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -252,7 +293,7 @@ def run_b200(args, rank, world, local):
     with torch.cuda.stream(stream):
         e0.record(stream)
         for _ in range(args.steps):
-            s.step()
+            step()
         e1.record(stream)
     stream.synchronize()
     ck = clocks.stop()
@@ -268,14 +309,17 @@ def run_b200(args, rank, world, local):
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
-    value = P * args.steps * world / (ms_max / 1000.0)
+    value = P * args.steps * (1 if shard else world) / (ms_max / 1000.0)
     ms_step = ms_max / args.steps
 
-    if args.no_e2e:
+    if args.no_e2e or shard:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "ms_per_step": ms_step, "steps": args.steps,
                               "positions": P, "gpu_launches": int(launches), "finite": finite, "clocks": ck,
-                              "note": "partial run (--no-e2e)"}), flush=True)
+                              "n_gpus": world, "scaling": "strong" if shard else "weak",
+                              "note": "partial run (--no-e2e)" if not shard else
+                                      "positions sharded over the GPUs, one NCCL all-reduce of the increments "
+                                      "per iteration"}), flush=True)
         if dist:
             dist.destroy_process_group()
         return
