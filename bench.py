@@ -23,6 +23,13 @@ the same scans run one after another.
 warm-start workload (64x64 raster at 128^2, 1e5 photons/pattern), iterations and GPU time until the phase NRMSE
 (after phase-ramp removal, central region) reaches 0.05.
 
+`--algo warm` measures the whole warm-start comparison on that workload: the encoder-decoder is trained first
+(20480 patterns from the forward model on objects of fresh seeds, 6 epochs; reported, not part of the timed
+comparison), then plain ePIE from a flat start against the warm start (inference over all 4096 patterns, stitching,
+phase integration, energy match, then ePIE iterations only if the warm object is still above 0.05), each as GPU time
+to phase NRMSE <= 0.05 checked after every iteration; DM from a flat start and from the warm object (exit waves
+P * O) are reported beside them.
+
 `--algo epie --cfg epie128|epie256k5` measures the ePIE configurations instead (10x10 raster at 128^2 with one probe
 mode; 51x51 raster at 256^2 with 5 modes): one step = one ePIE iteration over all positions, after enough warm-up
 iterations that the probe (iteration 10) and the modes (iteration 20) are being updated.
@@ -57,7 +64,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--nx", type=int, default=30, help="raster size (30 = the DM configuration; smaller for profiling)")
     ap.add_argument("--wave", type=int, default=0, help="DM patterns per pipeline wave (0 = automatic)")
-    ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch", "nrmse", "mls"])
+    ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch", "nrmse", "mls", "warm"])
     ap.add_argument("--shard", action="store_true",
                     help="N>1: split the 900 positions over the GPUs (one NCCL all-reduce of the DM increments per "
                          "iteration, strong scaling) instead of independent replicas")
@@ -588,6 +595,138 @@ def run_nrmse(args, rank, local):
                       "note": "the learned warm start (the other half of the comparison) is not built"}), flush=True)
 
 
+def run_warm(args, rank, local):
+    """Time to phase NRMSE <= 0.05 on the warm-start workload: learned warm start vs plain ePIE from a flat start."""
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+
+    from ptychopy_b200 import abi, synth, warmstart
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    cfg = dict(synth.CONFIGS["warm128"])
+    N, target = cfg["N"], 0.05
+    max_iters = max(args.steps, 10) if args.steps != 300 else 40
+    dx_s = synth.sample_pixel(cfg["lambd"], cfg["z"], cfg["dx_d"], N)
+    probe = synth.make_probe(N, dx_s, K=1)[0]
+    clocks = Clocks(local)
+    with torch.cuda.stream(stream):
+        # ---- training (one-off; wall clock) ----
+        t0 = time.time()
+        x, t = warmstart.training_set(probe, n_patterns=20480, N=N, seed=1000)
+        net = warmstart.Net(N=N, width=16, seed=0)
+        hist = warmstart.train(net, x, t, warmstart.loss_weight(probe, N // 4), epochs=6, batch=64)
+        stream.synchronize()
+        train_s = time.time() - t0
+        del x, t
+        # ---- the scan (same data as --algo nrmse) ----
+        rng = np.random.default_rng(20261207)
+        pos, X, Y = synth.raster_positions(cfg["nx"], cfg["ny"], cfg["step"], cfg["step"], dx_s, N)
+        obj = synth.make_object(X, Y, rng)
+        amp = synth.make_patterns_torch(obj, probe[None], pos, N, cfg["photons"], seed=20261207, device="cuda")
+        P = pos.shape[0]
+    mask = np.zeros((X, Y), bool)
+    mask[N // 2:X - N // 2, N // 2:Y - N // 2] = True
+
+    def session(alg, init=None):
+        s = abi.Session(size=N, scanDimsx=cfg["nx"], scanDimsy=cfg["ny"], stepx=cfg["step"], stepy=cfg["step"],
+                        lambd=cfg["lambd"], z=cfg["z"], dx_d=cfg["dx_d"], beamSize=synth.BEAM_FWHM, probeModes=1,
+                        algorithm=alg, device=local)
+        s.set_stream(stream.cuda_stream)
+        s.set_patterns_ptr(amp.data_ptr(), P, N)
+        s.set_probe(probe[None])
+        if init is not None:
+            s.set_object(init)
+        s.init()
+        return s
+
+    def iterate(s, gpu_ms, it0):
+        """Step until the phase NRMSE reaches the target (checked after every iteration) or max_iters."""
+        history, it = [], it0
+        while it < max_iters:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            with torch.cuda.stream(stream):
+                s.step()
+            e1.record(stream)
+            stream.synchronize()
+            gpu_ms += e0.elapsed_time(e1)
+            it += 1
+            err = synth.phase_nrmse(s.object(), obj, mask)
+            history.append([it, round(gpu_ms, 3), round(err, 5)])
+            if err <= target:
+                return {"iterations": it, "gpu_ms": round(gpu_ms, 3)}, history
+        return None, history
+
+    out = {"metric": "time to phase NRMSE <= 0.05: learned warm start vs plain ePIE from a flat start", "unit": "ms",
+           "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "data": "synthetic",
+           "positions": P}
+    clocks.start()
+    # plain ePIE from a flat start
+    s = session("ePIE")
+    spos = s.positions()
+    plain, plain_hist = iterate(s, 0.0, 0)
+    s.close()
+    # warm start: inference + assembly timed on the stream, then ePIE only while above the target
+    with torch.cuda.stream(stream):
+        for _ in range(3):  # warm-up
+            warmstart.assemble(warmstart.predict(net, amp), spos, probe, X, Y, amp)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        net_out = warmstart.predict(net, amp)
+        e1.record(stream)
+        o = warmstart.assemble(net_out, spos, probe, X, Y, amp)
+        e2.record(stream)
+        stream.synchronize()
+        t0 = time.time()
+        o0 = o.cpu().numpy().view(np.complex64)[..., 0].copy()
+        handoff_ms = (time.time() - t0) * 1e3
+    infer_ms, assemble_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    warm_err = synth.phase_nrmse(o0, obj, mask)
+    warm_ms = infer_ms + assemble_ms
+    if warm_err <= target:
+        warm = {"iterations": 0, "gpu_ms": round(warm_ms, 3)}
+        s = session("ePIE", o0)
+        _, warm_hist = iterate(s, warm_ms, 0)  # refinement trajectory, for the record
+        warm_hist = warm_hist[:10]
+    else:
+        s = session("ePIE", o0)
+        warm, warm_hist = iterate(s, warm_ms, 0)
+    s.close()
+    # DM beside them: flat start, and the warm object with exit waves P * O
+    dm = {}
+    for name, init in (("flat", None), ("warm", o0)):
+        s = session("DM", init)
+        if init is not None:
+            s.psi_from_object()
+        r, h = iterate(s, warm_ms if init is not None else 0.0, 0)
+        dm[name] = {"reached": r, "history": h if len(h) <= 8 else h[:5] + h[-3:]}
+        s.close()
+    clk = clocks.stop()
+    out.update({
+        "value": warm["gpu_ms"] if warm else None,
+        "plain": {"reached": plain, "history": plain_hist},
+        "warm": {"reached": warm, "infer_ms": round(infer_ms, 3), "assemble_ms": round(assemble_ms, 3),
+                 "warm_object_nrmse": round(warm_err, 5), "handoff_d2h_ms": round(handoff_ms, 3),
+                 "refinement_history": warm_hist},
+        "dm": dm,
+        "training": {"patterns": 20480, "epochs": 6, "batch": 64, "wall_s": round(train_s, 2),
+                     "loss_per_epoch": [round(v, 5) for v in hist], "parameters": net.n_params,
+                     "data": "pty_simulate at integer positions on objects of seeds 1000-1004, Poisson 1e5"},
+        "clocks": clk,
+        "config": {"workload": f"learned warm start: {cfg['nx']}x{cfg['ny']} raster ({P} positions), {N}^2, 50 nm "
+                               f"step, 1e5 photons/pattern, object {X}x{Y}, true probe given",
+                   "nrmse": "phase NRMSE after offset and linear-ramp removal over the central region (N/2 margin), "
+                            "after every iteration",
+                   "timing": "GPU time (CUDA events on the session's stream) of inference + assembly and of each "
+                             "iteration; session set-up and the object hand-off (host copy, reported) excluded in "
+                             "both arms"},
+    })
+    print(json.dumps(out), flush=True)
+
+
 BATCH_SCANS = [  # (algorithm, N, raster, step m)
     ("DM", 128, 10, 30e-9), ("DM", 128, 20, 50e-9), ("DM", 256, 15, 60e-9), ("DM", 256, 25, 80e-9),
     ("DM", 512, 10, 50e-9), ("DM", 512, 20, 100e-9), ("DM", 128, 40, 40e-9), ("DM", 256, 30, 70e-9),
@@ -667,6 +806,8 @@ def main():
         run_nrmse(args, rank, local)
     elif args.algo == "mls" and args.impl == "b200":
         run_mls(args, rank, local)
+    elif args.algo == "warm" and args.impl == "b200":
+        run_warm(args, rank, local)
     elif args.impl == "reference":
         run_reference(args, rank)
     else:

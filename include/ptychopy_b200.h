@@ -130,11 +130,57 @@ int pty_dm_step_local(pty_session* s);
 int pty_dm_increments(pty_session* s, void** dO, size_t* n_obj, void** dP, size_t* n_probe);
 int pty_dm_step_finish(pty_session* s);
 
+/* DM only, after pty_init: sets every exit wave to P * O at its position (probe mode 0, the object and probe as
+ * they are now).  The reference starts DM from zero exit waves (m_psiOld, src/DM.cu:95-98), which equals this for its
+ * zero object; for a given object (objectNP, a warm start) the zero start makes the first update
+ * P_F(2 P O) - P O ~ 0 and discards the object, while this start keeps it. */
+int pty_dm_psi_from_object(pty_session* s);
+
+/* Warm-start network kernels (no counterpart in the reference, which has no learned component): float32 NCHW
+ * device buffers, asynchronous on `stream`.  pty_nn_conv3x3: y = bias + 3x3 convolution of x (weights Cout x Cin x 3
+ * x 3, stride 1, zero padding 1; bias may be NULL), then max(y, 0) if relu != 0.  pty_nn_conv3x3_bwd: gradients of
+ * that convolution (without the ReLU) for dy: dx (may be NULL), dw and db (may be NULL), overwritten.
+ * pty_nn_relu (in place) / _bwd (g *= y > 0); pty_nn_pool2: 2x2 average to H x W; pty_nn_up2: nearest upsampling of
+ * H x W; their _bwd the gradients (H, W the small size, planes = batch x channels).  pty_nn_mse: weighted mean
+ * squared error, weight w[i % plane] (w may be NULL: all 1): g = 2 w (p - t) / n and *loss = sum w (p - t)^2 / n.
+ * pty_nn_adam: one Adam step (bias-corrected, step >= 1). */
+int pty_nn_conv3x3(const float* x, const float* w, const float* bias, float* y, int B, int Cin, int Cout, int H, int W,
+                   int relu, void* stream);
+int pty_nn_conv3x3_bwd(const float* x, const float* w, const float* dy, float* dx, float* dw, float* db, int B,
+                       int Cin, int Cout, int H, int W, void* stream);
+int pty_nn_relu(float* a, size_t n, void* stream);
+int pty_nn_relu_bwd(const float* y, float* g, size_t n, void* stream);
+int pty_nn_pool2(const float* x, float* y, size_t planes, int H, int W, void* stream);
+int pty_nn_pool2_bwd(const float* dy, float* dx, size_t planes, int H, int W, void* stream);
+int pty_nn_up2(const float* x, float* y, size_t planes, int H, int W, void* stream);
+int pty_nn_up2_bwd(const float* dy, float* dx, size_t planes, int H, int W, void* stream);
+int pty_nn_mse(const float* p, const float* t, const float* w, size_t plane, float* g, size_t n, double* loss,
+               void* stream);
+int pty_nn_adam(float* p, const float* g, float* m, float* v, size_t n, float lr, float b1, float b2, float eps,
+                int step, void* stream);
+
+/* Warm start of the object from the network's per-position predictions (no counterpart in the reference, which
+ * starts from a constant object, src/Sample.cpp:216-220, or a user-supplied objectNP).  Device pointers.
+ * pty_warm_input: network input x[b][i][j] = scale * log1p(amp[b][(i + N/2) % N][(j + N/2) % N]) (B x N x N).
+ * pty_warm_stitch: sums the network outputs out (P x 3 x S x S: amplitude, row and column phase differences
+ * phi(i+1,j) - phi(i,j) and phi(i,j+1) - phi(i,j), decoded as amp_mean + o * amp_scale and o * grad_scale) of the
+ * central S x S window of each position (pixel positions P x 2, rounded) into acc (4 x X x Y: weighted amplitude,
+ * row and column differences, and the weight), weighting by weight (S x S); deterministic.
+ * pty_warm_object: the object from acc: amplitude = weighted mean (amp_fill where the weight is <= wmin), phase = the
+ * least-squares integral of the mean differences (FFT Poisson solve on the periodic M x M grid, M the power of two
+ * >= max(X, Y), at most 512), then the whole object scaled so that sum_p sum |P O_p|^2 * N^2 equals the data's
+ * sum amp^2 (amp: P x N x N, probe N x N complex64).  work: 6 M^2 + 4 floats.  Returns after the stream is done. */
+int pty_warm_input(const float* amp, float* x, int B, int N, float scale, void* stream);
+int pty_warm_stitch(const float* out, const float* pos_px, int P, const float* weight, int S, int N, float amp_mean,
+                    float amp_scale, float grad_scale, float* acc, int X, int Y, void* stream);
+int pty_warm_object(const float* acc, int X, int Y, float wmin, float amp_fill, const float* probe_c64, int N,
+                    const float* pos_px, int P, const float* amp, float* work, float* obj_c64, void* stream);
+
 /* Forward model of simulation mode: amp_out[i] = |FFT2(O_bilinear(pos_px[i]) * P)| (P x N x N float32) for an
  * object (X x Y complex64), one probe mode (N x N complex64) and pixel positions (P x 2, x = row; the fractional part
  * is the bilinear texture offset).  Replaces Diffractions::simulate (src/Diffractions.cpp:80-117, d_simulatePSI
  * src/SampleKernels.cu:113-122); the reference builds its object from PGM images, here the caller passes it.
- * Pointers may be host or device memory; runs on the current device. */
+ * obj_c64, probe_c64 and amp_out may be host or device memory, pos_px is host memory; runs on the current device. */
 int pty_simulate(const float* obj_c64, int X, int Y, const float* probe_c64, int N, const float* pos_px, int P,
                  float* amp_out);
 

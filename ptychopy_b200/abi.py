@@ -30,6 +30,9 @@ EXPORTS = [
     "pty_get_probe", "pty_get_positions", "pty_write_results", "pty_set_stream", "pty_kernel_launches",
     "pty_last_error", "pty_fft2_dev", "pty_fft2_dev_noalloc", "pty_batch_run", "pty_simulate",
     "pty_set_shard", "pty_dm_step_local", "pty_dm_increments", "pty_dm_step_finish",
+    "pty_nn_conv3x3", "pty_nn_conv3x3_bwd", "pty_nn_relu", "pty_nn_relu_bwd", "pty_nn_pool2", "pty_nn_pool2_bwd",
+    "pty_nn_up2", "pty_nn_up2_bwd", "pty_nn_mse", "pty_nn_adam", "pty_warm_input", "pty_warm_stitch",
+    "pty_warm_object", "pty_dm_psi_from_object",
 ]
 
 
@@ -93,6 +96,23 @@ def lib():
             "pty_dm_increments": ([vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(vp),
                                    ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
             "pty_dm_step_finish": ([vp], ctypes.c_int),
+            "pty_dm_psi_from_object": ([vp], ctypes.c_int),
+            "pty_nn_conv3x3": ([vp, vp, vp, vp] + [ctypes.c_int] * 6 + [vp], ctypes.c_int),
+            "pty_nn_conv3x3_bwd": ([vp] * 6 + [ctypes.c_int] * 5 + [vp], ctypes.c_int),
+            "pty_nn_relu": ([vp, ctypes.c_size_t, vp], ctypes.c_int),
+            "pty_nn_relu_bwd": ([vp, vp, ctypes.c_size_t, vp], ctypes.c_int),
+            "pty_nn_pool2": ([vp, vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
+            "pty_nn_pool2_bwd": ([vp, vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
+            "pty_nn_up2": ([vp, vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
+            "pty_nn_up2_bwd": ([vp, vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
+            "pty_nn_mse": ([vp, vp, vp, ctypes.c_size_t, vp, ctypes.c_size_t, vp, vp], ctypes.c_int),
+            "pty_nn_adam": ([vp, vp, vp, vp, ctypes.c_size_t] + [ctypes.c_float] * 4 + [ctypes.c_int, vp],
+                            ctypes.c_int),
+            "pty_warm_input": ([vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, vp], ctypes.c_int),
+            "pty_warm_stitch": ([vp, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 3 +
+                                [vp, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
+            "pty_warm_object": ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, vp, ctypes.c_int,
+                                 vp, ctypes.c_int, vp, vp, vp, vp], ctypes.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -240,6 +260,10 @@ class Session:
 
     def step_finish(self):
         check(lib().pty_dm_step_finish(self.h))
+
+    def psi_from_object(self):
+        """DM: exit waves = P * O at every position (pty_dm_psi_from_object), for a given start object."""
+        check(lib().pty_dm_psi_from_object(self.h))
 
 
 def simulate(obj, probe, pos_px):

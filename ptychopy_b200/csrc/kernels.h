@@ -67,5 +67,7 @@ int dm_wave_size(int N, int P);
 cudaError_t dm_wave(const DMBuffers& b, const DMWave& w, bool phaseConstraint, bool updateProbe, cudaStream_t st,
                     int64_t* launches);
 cudaError_t dm_finalize(const DMBuffers& b, bool updateProbe, cudaStream_t st, int64_t* launches);
+// psi_p = P * O at every pattern's rounded offset (P patterns).
+cudaError_t dm_psi_from_object(const DMBuffers& b, int P, cudaStream_t st);
 
 }  // namespace pty

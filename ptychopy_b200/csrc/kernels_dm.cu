@@ -329,4 +329,22 @@ cudaError_t dm_finalize(const DMBuffers& b, bool up, cudaStream_t st, int64_t* l
   return cudaGetLastError();
 }
 
+// psi_p[x][y] = P[x][y] * O[x + ox_p][y + oy_p] for every pattern: the exit waves of the current object and probe
+// (mode 0), the usual start of the difference map for a given object.
+__global__ void k_dm_psi_from_object(const DMBuffers b, int P) {
+  const size_t NN = size_t(b.N) * b.N, n = size_t(P) * NN;
+  for (size_t q = blockIdx.x * size_t(blockDim.x) + threadIdx.x; q < n; q += size_t(gridDim.x) * blockDim.x) {
+    const int p = int(q / NN), k = int(q % NN), x = k / b.N, y = k % b.N;
+    const int2 o = b.offs[p];
+    b.psi[q] = cmul(b.probe[k], b.obj[size_t(x + o.x) * b.Y + o.y + y]);
+  }
+}
+
+cudaError_t dm_psi_from_object(const DMBuffers& b, int P, cudaStream_t st) {
+  const size_t n = size_t(P) * b.N * b.N;
+  const int grid = int(std::min<size_t>((n + 255) / 256, 148 * 16));
+  k_dm_psi_from_object<<<grid, 256, 0, st>>>(b, P);
+  return cudaGetLastError();
+}
+
 }  // namespace pty

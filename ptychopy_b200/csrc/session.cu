@@ -1303,6 +1303,17 @@ int pty_dm_step_finish(pty_session* s) {
   });
 }
 
+int pty_dm_psi_from_object(pty_session* s) {
+  return guarded([&] {
+    need(s && s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    need(s->algo == ALGO_DM, "exit waves exist for DM only", PTY_ERR_UNSUPPORTED);
+    need(s->pending_iter == 0, "a sharded step is in progress", PTY_ERR_STATE);
+    set_device(s);
+    check_cuda(dm_psi_from_object(dm_buffers(s), s->P, s->stream), "exit waves from the object");
+    check_cuda(cudaStreamSynchronize(s->stream), "exit waves from the object");
+  });
+}
+
 int pty_simulate(const float* obj_c64, int X, int Y, const float* probe_c64, int N, const float* pos_px, int P,
                  float* amp_out) {
   return guarded([&] {
