@@ -171,6 +171,34 @@ int pty_nn_adam(float* p, const float* g, float* m, float* v, size_t n, float lr
  * >= max(X, Y), at most 512), then the whole object scaled so that sum_p sum |P O_p|^2 * N^2 equals the data's
  * sum amp^2 (amp: P x N x N, probe N x N complex64).  work: 6 M^2 + 4 floats.  Returns after the stream is done. */
 int pty_warm_input(const float* amp, float* x, int B, int N, float scale, void* stream);
+
+/* Tensor-core (tcgen05) BF16 inference path of the warm-start network (no counterpart in the reference).
+ * Activations are NHWC BF16 device buffers.  pty_tc_weights_size: BF16 elements of a packed layer (Cout <= 256),
+ * -1 if unsupported; pty_tc_pack_weights: packs FP32 weights (Cout x Cin x 3 x 3) into that layout.
+ * pty_tc_conv3x3: y = bias + 3x3 convolution (output H x W) of the input, then max(y, 0) if relu; FP32 accumulation
+ * in tensor memory.  Input in_mode 0: x NHWC BF16 B x H x W x Cin (Cin a multiple of 8 or at most 8); 1: x NHWC BF16
+ * B x H/2 x W/2 x Cin, read 2x nearest-upsampled; 2: x FP32 amplitudes B x H x W (Cin = 1) read as
+ * in_scale * log1p(amp) with the zero frequency moved to the centre.  Output out_mode 0: y NHWC BF16 (Cout a
+ * multiple of 8); 1: y NCHW FP32; 2: y NHWC BF16 2x2-average-pooled to H/2 x W/2 (H even, W a multiple of 16).
+ * *err (device int, zero on entry) receives a non-zero code if a pipeline wait timed out.
+ * pty_tc_first_layer: the network's first layer on CUDA cores (K = 9 is too thin for tensor cores): y (NHWC BF16,
+ * B x H/2 x W/2 x 16) = pool2(relu(bias + conv3x3(in_scale * log1p(centred amp)))) for FP32 amplitudes amp
+ * (B x H x W) and FP32 weights (16 x 1 x 3 x 3), inputs and weights rounded to BF16 like the tensor-core layers.
+ * pty_tc_last_layer: the output layer on CUDA cores: y (NCHW FP32) = bias + conv3x3(x), x NHWC BF16 with Cin = 32,
+ * Cout <= 4, FP32 weights (rounded to BF16).
+ * pty_tc_pool2 / pty_tc_up2: 2x2 average pooling to H x W / nearest upsampling of H x W, NHWC BF16, C channels.
+ * pty_tc_to_bf16: n FP32 values to BF16.  All asynchronous on `stream`. */
+int pty_tc_weights_size(int Cin, int Cout);
+int pty_tc_pack_weights(const float* w, int Cin, int Cout, void* wpk, void* stream);
+int pty_tc_conv3x3(const void* x, const void* wpk, const float* bias, void* y, int B, int Cin, int Cout, int H, int W,
+                   int relu, int in_mode, int out_mode, float in_scale, int* err, void* stream);
+int pty_tc_first_layer(const float* amp, const float* w, const float* bias, void* y, int B, int Cout, int H, int W,
+                       float in_scale, void* stream);
+int pty_tc_last_layer(const void* x, const float* w, const float* bias, float* y, int B, int Cin, int Cout, int H,
+                      int W, void* stream);
+int pty_tc_pool2(const void* x, void* y, int B, int H, int W, int C, void* stream);
+int pty_tc_up2(const void* x, void* y, int B, int H, int W, int C, void* stream);
+int pty_tc_to_bf16(const float* x, void* y, size_t n, void* stream);
 int pty_warm_stitch(const float* out, const float* pos_px, int P, const float* weight, int S, int N, float amp_mean,
                     float amp_scale, float grad_scale, float* acc, int X, int Y, void* stream);
 int pty_warm_object(const float* acc, int X, int Y, float wmin, float amp_fill, const float* probe_c64, int N,

@@ -32,7 +32,8 @@ EXPORTS = [
     "pty_set_shard", "pty_dm_step_local", "pty_dm_increments", "pty_dm_step_finish",
     "pty_nn_conv3x3", "pty_nn_conv3x3_bwd", "pty_nn_relu", "pty_nn_relu_bwd", "pty_nn_pool2", "pty_nn_pool2_bwd",
     "pty_nn_up2", "pty_nn_up2_bwd", "pty_nn_mse", "pty_nn_adam", "pty_warm_input", "pty_warm_stitch",
-    "pty_warm_object", "pty_dm_psi_from_object",
+    "pty_warm_object", "pty_dm_psi_from_object", "pty_tc_weights_size", "pty_tc_pack_weights", "pty_tc_conv3x3",
+    "pty_tc_pool2", "pty_tc_up2", "pty_tc_to_bf16", "pty_tc_first_layer", "pty_tc_last_layer",
 ]
 
 
@@ -97,6 +98,14 @@ def lib():
                                    ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
             "pty_dm_step_finish": ([vp], ctypes.c_int),
             "pty_dm_psi_from_object": ([vp], ctypes.c_int),
+            "pty_tc_weights_size": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
+            "pty_tc_pack_weights": ([vp, ctypes.c_int, ctypes.c_int, vp, vp], ctypes.c_int),
+            "pty_tc_conv3x3": ([vp, vp, vp, vp] + [ctypes.c_int] * 8 + [ctypes.c_float, vp, vp], ctypes.c_int),
+            "pty_tc_pool2": ([vp, vp] + [ctypes.c_int] * 4 + [vp], ctypes.c_int),
+            "pty_tc_up2": ([vp, vp] + [ctypes.c_int] * 4 + [vp], ctypes.c_int),
+            "pty_tc_to_bf16": ([vp, vp, ctypes.c_size_t, vp], ctypes.c_int),
+            "pty_tc_first_layer": ([vp, vp, vp, vp] + [ctypes.c_int] * 4 + [ctypes.c_float, vp], ctypes.c_int),
+            "pty_tc_last_layer": ([vp, vp, vp, vp] + [ctypes.c_int] * 5 + [vp], ctypes.c_int),
             "pty_nn_conv3x3": ([vp, vp, vp, vp] + [ctypes.c_int] * 6 + [vp], ctypes.c_int),
             "pty_nn_conv3x3_bwd": ([vp] * 6 + [ctypes.c_int] * 5 + [vp], ctypes.c_int),
             "pty_nn_relu": ([vp, ctypes.c_size_t, vp], ctypes.c_int),

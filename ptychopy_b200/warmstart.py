@@ -181,6 +181,74 @@ class Net:
                                         b1, b2, eps, self.step_count, _stream()))
 
 
+class TcNet:
+    """BF16 tensor-core (tcgen05) inference copy of a trained Net: weights packed once, activations NHWC BF16,
+    FP32 accumulation, the output planes in FP32 NCHW like Net.forward."""
+
+    def __init__(self, net):
+        import torch
+
+        L = abi.lib()
+        self.net, self.plan, self.S, self.N = net, net.plan, net.S, net.N
+        self.device = net.device
+        self.wpk = []
+        st = _stream()
+        for l, (cin, cout, *_rest) in enumerate(self.plan):
+            n = L.pty_tc_weights_size(cin, cout)
+            if n < 0:
+                raise ValueError("layer %d not supported by the tensor-core path" % l)
+            w = torch.empty(n, dtype=torch.bfloat16, device=self.device)
+            abi.check(L.pty_tc_pack_weights(_p(net._w(net.params, l)), cin, cout, _p(w), st))
+            self.wpk.append(w)
+        self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._bufs, self._bufs_B = None, 0
+
+    def _buffers(self, B):
+        import torch
+
+        if self._bufs is not None and self._bufs_B >= B:
+            return self._bufs
+        f = dict(dtype=torch.bfloat16, device=self.device)
+        bufs = []
+        for cin, cout, H, relu, after in self.plan[:-1]:
+            side = H // 2 if after == "pool" else H  # pooling is fused into the convolution's epilogue
+            bufs.append(torch.empty((B, side, side, cout), **f))
+        self._bufs, self._bufs_B = bufs, B
+        return bufs
+
+    def forward_amp(self, amp, B, out):
+        """amp: B x N x N FP32 measured amplitudes (device); out: B x 3 x S x S FP32 (device), written.  The first
+        layer reads the amplitudes directly (log1p, centred zero frequency), pooling is fused into the epilogues and
+        upsampling into the next layer's loads."""
+        L = abi.lib()
+        bufs = self._buffers(B)
+        st = _stream()
+        cur, in_mode = amp, 2
+        last = len(self.plan) - 1
+        net = self.net
+        for l, (cin, cout, H, relu, after) in enumerate(self.plan):
+            y = out if l == last else bufs[l]
+            if l == 0 and cout == 16 and after == "pool" and relu:  # K = 9: CUDA cores
+                abi.check(L.pty_tc_first_layer(_p(cur), _p(net._w(net.params, l)), _p(net._b(net.params, l)), _p(y),
+                                               B, cout, H, H, INPUT_SCALE, st))
+            elif l == last and cin == 32 and cout <= 4 and in_mode == 0 and not relu:  # N = 3: CUDA cores
+                abi.check(L.pty_tc_last_layer(_p(cur), _p(net._w(net.params, l)), _p(net._b(net.params, l)), _p(y),
+                                              B, cin, cout, H, H, st))
+            else:
+                out_mode = 1 if l == last else (2 if after == "pool" else 0)
+                abi.check(L.pty_tc_conv3x3(_p(cur), _p(self.wpk[l]), _p(net._b(net.params, l)), _p(y), B, cin,
+                                           cout, H, H, int(relu), in_mode, out_mode, INPUT_SCALE, _p(self.err), st))
+            cur, in_mode = y, (1 if after == "up" else 0)
+        return out
+
+    def check(self):
+        """Raises if a tensor-core pipeline wait timed out since the last check."""
+        e = int(self.err.item())
+        if e:
+            self.err.zero_()
+            raise abi.PtyError(abi.PTY_ERR_CUDA, "tensor-core convolution: pipeline wait timed out (code %d)" % e)
+
+
 def loss_weight(probe, S):
     """Loss weight of the S x S output window: 0.1 + |P|^2 / max |P|^2 over the window, normalised to mean 1."""
     p = np.asarray(probe)
@@ -294,7 +362,8 @@ def train(net, x, t, weight, epochs=6, batch=64, lr=1e-3, seed=0, log=None):
 
 
 def predict(net, amp, chunk=256, out=None):
-    """Network outputs (P x 3 x S x S device tensor) for the amplitudes amp (P x N x N device tensor)."""
+    """Network outputs (P x 3 x S x S device tensor) for the amplitudes amp (P x N x N device tensor); `net` is a
+    Net (FP32 CUDA-core kernels) or a TcNet (BF16 tensor cores)."""
     import torch
 
     L = abi.lib()
@@ -302,6 +371,12 @@ def predict(net, amp, chunk=256, out=None):
     S = net.S
     if out is None:
         out = torch.empty((P, 3, S, S), dtype=torch.float32, device=amp.device)
+    if isinstance(net, TcNet):
+        for c0 in range(0, P, chunk):
+            cnt = min(chunk, P - c0)
+            net.forward_amp(amp[c0:c0 + cnt], cnt, out[c0:c0 + cnt])
+        net.check()
+        return out
     xb = torch.empty((min(chunk, P), 1, N, N), dtype=torch.float32, device=amp.device)
     for c0 in range(0, P, chunk):
         cnt = min(chunk, P - c0)
