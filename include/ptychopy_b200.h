@@ -130,6 +130,15 @@ int pty_dm_step_local(pty_session* s);
 int pty_dm_increments(pty_session* s, void** dO, size_t* n_obj, void** dP, size_t* n_probe);
 int pty_dm_step_finish(pty_session* s);
 
+/* Learned warm start (no counterpart in the reference, which starts from a constant object, src/Sample.cpp:216-220,
+ * or objectNP).  Before pty_init: the parameters (n_params floats, the layout ptychopy_b200/warmstart.py's Net
+ * trains: per layer the Cout x Cin x 3 x 3 weights then the Cout biases) of the width-`width` encoder-decoder for the
+ * session's N x N patterns; n_params = 0 removes it.  pty_init then runs the network on the session's patterns
+ * (BF16 tensor cores), stitches and integrates its predictions into the starting object (instead of the constant
+ * start; exclusive with objectNP / objectGuess) and, for DM, starts the exit waves at P * O.  ePIE and DM only;
+ * N a multiple of 16, the object at most 512 x 512. */
+int pty_set_warm_start(pty_session* s, const float* params, size_t n_params, int width);
+
 /* DM only, after pty_init: sets every exit wave to P * O at its position (probe mode 0, the object and probe as
  * they are now).  The reference starts DM from zero exit waves (m_psiOld, src/DM.cu:95-98), which equals this for its
  * zero object; for a given object (objectNP, a warm start) the zero start makes the first update

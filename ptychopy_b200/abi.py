@@ -33,7 +33,7 @@ EXPORTS = [
     "pty_nn_conv3x3", "pty_nn_conv3x3_bwd", "pty_nn_relu", "pty_nn_relu_bwd", "pty_nn_pool2", "pty_nn_pool2_bwd",
     "pty_nn_up2", "pty_nn_up2_bwd", "pty_nn_mse", "pty_nn_adam", "pty_warm_input", "pty_warm_stitch",
     "pty_warm_object", "pty_dm_psi_from_object", "pty_tc_weights_size", "pty_tc_pack_weights", "pty_tc_conv3x3",
-    "pty_tc_pool2", "pty_tc_up2", "pty_tc_to_bf16", "pty_tc_first_layer", "pty_tc_last_layer",
+    "pty_tc_pool2", "pty_tc_up2", "pty_tc_to_bf16", "pty_tc_first_layer", "pty_tc_last_layer", "pty_set_warm_start",
 ]
 
 
@@ -98,6 +98,7 @@ def lib():
                                    ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
             "pty_dm_step_finish": ([vp], ctypes.c_int),
             "pty_dm_psi_from_object": ([vp], ctypes.c_int),
+            "pty_set_warm_start": ([vp, vp, ctypes.c_size_t, ctypes.c_int], ctypes.c_int),
             "pty_tc_weights_size": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "pty_tc_pack_weights": ([vp, ctypes.c_int, ctypes.c_int, vp, vp], ctypes.c_int),
             "pty_tc_conv3x3": ([vp, vp, vp, vp] + [ctypes.c_int] * 8 + [ctypes.c_float, vp, vp], ctypes.c_int),
@@ -269,6 +270,15 @@ class Session:
 
     def step_finish(self):
         check(lib().pty_dm_step_finish(self.h))
+
+    def set_warm_start(self, params, width=16):
+        """Trained warm-start network parameters (warmstart.Net.state()); pty_init builds the start object from
+        them (pty_set_warm_start).  None removes them."""
+        if params is None:
+            check(lib().pty_set_warm_start(self.h, None, 0, 0))
+            return
+        self._warm = np.ascontiguousarray(params, np.float32)
+        check(lib().pty_set_warm_start(self.h, _ptr(self._warm), self._warm.size, int(width)))
 
     def psi_from_object(self):
         """DM: exit waves = P * O at every position (pty_dm_psi_from_object), for a given start object."""

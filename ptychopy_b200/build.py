@@ -19,7 +19,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
 
 CU_SOURCES = ["kernels_common.cu", "kernels_dm.cu", "kernels_epie.cu", "kernels_mls.cu", "session.cu",
-              "noalloc.cu", "kernels_nn.cu", "kernels_warm.cu", "kernels_tc.cu"]
+              "noalloc.cu", "kernels_nn.cu", "kernels_warm.cu", "kernels_tc.cu",
+              "warm_start.cu"]
 HEADERS = ["fft_core.cuh", "kernel_util.cuh", "kernels.h", "kernels_epie.h", "kernels_mls.h", "session.h"]
 
 LIB = os.path.join(HERE, "libptychopy_b200.so")

@@ -4,7 +4,8 @@
 //   * errors raise Python exceptions instead of printing and returning None/True or exiting the process;
 //   * result arrays are owned numpy arrays (the reference wraps leaked buffers, src/ptychopy.c:964-990);
 //   * objectNP/probeNP accept any complex or real dtype (the reference misreads complex64, src/ptychopy.c:383-471);
-//   * extra keywords: seed, calculateRMS, device, wave, returnResults, writeResults, outputDir;
+//   * extra keywords: seed, calculateRMS, device, wave, returnResults, writeResults, outputDir, warmStart (trained
+//     warm-start network parameters, float32) and warmStartWidth (its width, default 16);
 //     probeNP may be (K, N, N) to supply all probe modes.
 // Whole-mode file ingest (fp, hdf5path), simulate mode and CLI strings (cmdstr) are outside this engine and raise
 // NotImplementedError.
@@ -44,8 +45,8 @@ void copy_str(char* dst, size_t cap, const char* src) {
 
 struct Parsed {
   pty_params p;
-  PyObject *diff = nullptr, *pos = nullptr, *obj = nullptr, *probe = nullptr;
-  int returnResults = 0, writeResults = 1;
+  PyObject *diff = nullptr, *pos = nullptr, *obj = nullptr, *probe = nullptr, *warm = nullptr;
+  int returnResults = 0, writeResults = 1, warmWidth = 16;
   const char* outputDir = "data";
 };
 
@@ -68,7 +69,8 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
                                 "T", "jitterRadius", "delta_p", "threshold", "rotate90", "sqrtData", "fftShiftData",
                                 "binaryOutput", "simulate", "phaseConstraint", "updateProbe", "updateModes",
                                 "beamstopMask", "lf", "PPS", "seed", "calculateRMS", "device", "wave",
-                                "returnResults", "writeResults", "outputDir", nullptr};
+                                "returnResults", "writeResults", "outputDir", "warmStart", "warmStartWidth",
+                                nullptr};
   static const char* kw_file[] = {"jobID", "fp", "fs", "hdf5path", "dpf", "beamSize", "probeGuess", "objectGuess",
                                   "size", "qx", "qy", "nx", "ny", "scanDimsx", "scanDimsy", "spiralScan",
                                   "flipScanAxis", "mirror1stScanAxis", "mirror2ndScanAxis", "stepx", "stepy",
@@ -79,12 +81,13 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
   int ok;
   if (np) {
     ok = PyArg_ParseTupleAndKeywords(
-        args, kw, "|sOOOOsisidssiiiiiiiiiiiddidddiiidiiiiiiiiiisiKiiiiis", const_cast<char**>(kw_np), &jobID,
+        args, kw, "|sOOOOsisidssiiiiiiiiiiiddidddiiidiiiiiiiiiisiKiiiiisOi", const_cast<char**>(kw_np), &jobID,
         &out.diff, &out.pos, &out.obj, &out.probe, &fp, &fs, &hdf5path, &dpf, &beamSize, &probeGuess, &objectGuess,
         &size, &qx, &qy, &nx, &ny, &scanDimsx, &scanDimsy, &spiralScan, &flipScanAxis, &mirror1, &mirror2, &stepx,
         &stepy, &probeModes, &lambd, &dx_d, &z, &iter, &T, &jitter, &delta_p, &threshold, &rotate90, &sqrtData,
         &fftShiftData, &binaryOutput, &simulate, &phaseConstraint, &updateProbe, &updateModes, &beamstopMask, &lf,
-        &PPS, &seed, &calculateRMS, &device, &wave, &out.returnResults, &out.writeResults, &out.outputDir);
+        &PPS, &seed, &calculateRMS, &device, &wave, &out.returnResults, &out.writeResults, &out.outputDir, &out.warm,
+        &out.warmWidth);
   } else {
     ok = PyArg_ParseTupleAndKeywords(args, kw, "|ssisidssiiiiiiiiiiiddidddiiidiiiiiiiiiisi",
                                      const_cast<char**>(kw_file), &jobID, &fp, &fs, &hdf5path, &dpf, &beamSize,
@@ -189,6 +192,13 @@ pty_session* make_session(Parsed& a) {
     }
     rc = pty_set_probe(s, static_cast<const float*>(PyArray_DATA(pr)), K, pn);
     Py_DECREF(pr);
+    if (rc != PTY_OK) return bail(rc);
+  }
+  if (a.warm && a.warm != Py_None) {
+    PyArrayObject* wa = reinterpret_cast<PyArrayObject*>(PyArray_FROM_OTF(a.warm, NPY_FLOAT32, NPY_ARRAY_IN_ARRAY));
+    if (!wa) return bail(PTY_OK);
+    rc = pty_set_warm_start(s, static_cast<const float*>(PyArray_DATA(wa)), size_t(PyArray_SIZE(wa)), a.warmWidth);
+    Py_DECREF(wa);
     if (rc != PTY_OK) return bail(rc);
   }
   Py_BEGIN_ALLOW_THREADS rc = pty_init(s);

@@ -1171,6 +1171,7 @@ int pty_init(pty_session* s) {
     s->tw.p = twp;
     s->tw.bytes = sizeof(float2) * s->N;
     if (s->algo == ALGO_MLS) {
+      need(s->warm_params.empty(), "the learned warm start is for ePIE and DM sessions", PTY_ERR_UNSUPPORTED);
       init_mls(s);
       s->initialized = true;
       return;
@@ -1194,6 +1195,18 @@ int pty_init(pty_session* s) {
       init_probe(s, avg.as<float>());
     }
     init_object(s);
+    if (!s->warm_params.empty()) {
+      need(s->shard_total == 0, "the warm start needs the whole scan's patterns (not a position shard)",
+           PTY_ERR_UNSUPPORTED);
+      need(s->obj_h.empty() && !p.objectGuess[0], "warmStart and objectNP / objectGuess are exclusive");
+      need(s->N % 16 == 0, "the warm-start network needs N to be a multiple of 16");
+      const size_t want = warm_param_count(s->N, s->warm_width);
+      need(s->warm_params.size() == want, "warmStart has " + std::to_string(s->warm_params.size()) +
+                                              " parameters; the width-" + std::to_string(s->warm_width) +
+                                              " network for " + std::to_string(s->N) + "^2 patterns has " +
+                                              std::to_string(want));
+      run_warm_start(s);
+    }
     // the cluster ePIE kernel's column phase consumes the amplitudes column-wise: transpose each plane once (DM and
     // the shared-memory ePIE kernel read them in their natural layout)
     if (s->algo == ALGO_EPIE && !epie_uses_smem(s->N, s->K)) {
@@ -1204,10 +1217,15 @@ int pty_init(pty_session* s) {
       std::swap(s->amp.p, t.p);
       std::swap(s->amp.bytes, t.bytes);
     }
-    if (s->algo == ALGO_EPIE)
+    if (s->algo == ALGO_EPIE) {
       init_epie(s);
-    else
+    } else {
       init_dm(s);
+      if (!s->warm_params.empty()) {  // start DM from the warm object's exit waves, not from zero
+        check_cuda(dm_psi_from_object(dm_buffers(s), s->P, s->stream), "exit waves from the warm object");
+        check_cuda(cudaStreamSynchronize(s->stream), "exit waves from the warm object");
+      }
+    }
     s->initialized = true;
   });
 }
@@ -1300,6 +1318,21 @@ int pty_dm_step_finish(pty_session* s) {
     step_dm_finish(s, s->pending_iter);
     s->iter = s->pending_iter;
     s->pending_iter = 0;
+  });
+}
+
+int pty_set_warm_start(pty_session* s, const float* params, size_t n_params, int width) {
+  return guarded([&] {
+    need(s != nullptr, "null session");
+    need(!s->initialized, "the warm start must be set before pty_init", PTY_ERR_STATE);
+    if (n_params == 0 || !params) {
+      s->warm_params.clear();
+      s->warm_width = 0;
+      return;
+    }
+    need(width >= 1, "warm-start width must be positive");
+    s->warm_params.assign(params, params + n_params);
+    s->warm_width = width;
   });
 }
 

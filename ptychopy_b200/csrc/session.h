@@ -61,6 +61,11 @@ struct MlsGeometry {
   int roi[4] = {0, 0, 0, 0};  // x0, y0, nx, ny (0-based)
 };
 MlsGeometry mls_geometry(const std::vector<float>& raw, int N);
+// Learned warm start (warm_start.cu): parameter count of the width-w network for N x N patterns, and the
+// inference + assembly that writes the session's starting object inside pty_init.
+size_t warm_param_count(int N, int w);
+void run_warm_start(pty_session* s);
+
 std::vector<float> raw_cartesian_positions(int nx, int ny, double stepx, double stepy, double dx_s, bool mirrorX,
                                            bool mirrorY);
 
@@ -83,13 +88,15 @@ struct pty_session {
   std::vector<float> obj_h;   // objectNP (X*Y complex) or empty
   std::vector<float> probe_h; // probeNP (Kg*N*N complex) or empty
   int probe_given_modes = 0;
+  std::vector<float> warm_params;  // trained warm-start network (pty_set_warm_start) or empty
+  int warm_width = 0;
 
   // geometry
   pty::Geometry geo;
   std::vector<int> offs;  // rounded offsets, 2*P
 
   // device state
-  pty::DeviceBuf amp;    // P*N*N float (natural layout; DM keeps it transposed per plane)
+  pty::DeviceBuf amp;    // P*N*N float (natural layout; sessions of the cluster ePIE kernel transpose each plane)
   pty::DeviceBuf obj, probe, ocache, pcache;
   pty::DeviceBuf tw, dOffs, scal;
   // DM

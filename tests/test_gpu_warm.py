@@ -105,3 +105,57 @@ def test_warm_start_training_and_gain():
         res[name] = synth.phase_nrmse(s.object(), obj, mask)
         s.close()
     assert res["warm"] < res["flat"], res
+
+
+def test_native_warm_start_matches_python_path():
+    """pty_set_warm_start + pty_init (C++ inference and assembly inside the session) against warmstart.py on the
+    same network, patterns, probe and positions; also through the ptychopy module's warmStart keyword."""
+    import torch
+
+    from conftest import rel_err
+    from ptychopy_b200 import abi, synth, warmstart
+
+    cfg = dict(synth.CONFIGS["warm128"])
+    N, nx = cfg["N"], 12
+    dx_s = synth.sample_pixel(cfg["lambd"], cfg["z"], cfg["dx_d"], N)
+    probe = synth.make_probe(N, dx_s, K=1)[0]
+    rng = np.random.default_rng(31)
+    pos, X, Y = synth.raster_positions(nx, nx, cfg["step"], cfg["step"], dx_s, N)
+    obj = synth.make_object(X, Y, rng)
+    amp = synth.make_patterns_torch(obj, probe[None], pos, N, cfg["photons"], seed=31)
+    net = warmstart.Net(N=N, width=16, seed=9)
+    params = net.state()
+    s = _session("ePIE", amp, probe, cfg, nx)
+    spos = s.positions()
+    s.close()
+    ref = warmstart.initial_object(warmstart.TcNet(net), amp, spos, probe, X, Y)
+    for alg in ("ePIE", "DM"):
+        kw = dict(size=N, scanDimsx=nx, scanDimsy=nx, stepx=cfg["step"], stepy=cfg["step"], lambd=cfg["lambd"],
+                  z=cfg["z"], dx_d=cfg["dx_d"], beamSize=synth.BEAM_FWHM, probeModes=1, algorithm=alg)
+        s = abi.Session(**kw)
+        s.set_stream(torch.cuda.current_stream().cuda_stream)
+        s.set_patterns_ptr(amp.data_ptr(), amp.shape[0], N)
+        s.set_probe(probe[None])
+        s.set_warm_start(params, 16)
+        s.init()
+        got = s.object()
+        s.close()
+        assert rel_err(got, ref) < 1e-5, alg
+    # a parameter count that does not match the network is refused at pty_init
+    s = abi.Session(size=N, scanDimsx=nx, scanDimsy=nx, stepx=cfg["step"], stepy=cfg["step"], lambd=cfg["lambd"],
+                    z=cfg["z"], dx_d=cfg["dx_d"], beamSize=synth.BEAM_FWHM, probeModes=1, algorithm="ePIE")
+    s.set_patterns(amp.cpu().numpy())
+    s.set_warm_start(params[:-1], 16)
+    with pytest.raises(abi.PtyError):
+        s.init()
+    s.close()
+    # the reference-facing module: epienpinit(..., warmStart=params) starts from the same object
+    import ptychopy_b200
+
+    ptychopy = ptychopy_b200.import_ptychopy()
+    ptychopy.epienpinit(jobID="warm", diffractionNP=amp.cpu().numpy(), probeNP=probe, size=N, scanDimsx=nx,
+                        scanDimsy=nx, stepx=cfg["step"], stepy=cfg["step"], lambd=cfg["lambd"], z=cfg["z"],
+                        dx_d=cfg["dx_d"], beamSize=synth.BEAM_FWHM, iter=5, warmStart=params, warmStartWidth=16)
+    got = ptychopy.epieresobj()
+    ptychopy.epiepost()
+    assert rel_err(got, ref) < 1e-5
