@@ -30,6 +30,10 @@ phase integration, energy match, then ePIE iterations only if the warm object is
 to phase NRMSE <= 0.05 checked after every iteration; DM from a flat start and from the warm object (exit waves
 P * O) are reported beside them.
 
+`--algo infer` measures the warm-start network's BF16 tensor-core inference alone (the width-16 encoder-decoder,
+seeded random weights, on the 4096 patterns of the warm-start workload): patterns/s per forward pass, the FP32
+CUDA-core forward beside it, and the roofline of the dominant tcgen05 convolution against the measured BF16 peak.
+
 `--algo epie --cfg epie128|epie256k5` measures the ePIE configurations instead (10x10 raster at 128^2 with one probe
 mode; 51x51 raster at 256^2 with 5 modes): one step = one ePIE iteration over all positions, after enough warm-up
 iterations that the probe (iteration 10) and the modes (iteration 20) are being updated.
@@ -64,7 +68,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--nx", type=int, default=30, help="raster size (30 = the DM configuration; smaller for profiling)")
     ap.add_argument("--wave", type=int, default=0, help="DM patterns per pipeline wave (0 = automatic)")
-    ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch", "nrmse", "mls", "warm"])
+    ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch", "nrmse", "mls", "warm", "infer"])
     ap.add_argument("--shard", action="store_true",
                     help="N>1: split the 900 positions over the GPUs (one NCCL all-reduce of the DM increments per "
                          "iteration, strong scaling) instead of independent replicas")
@@ -739,6 +743,93 @@ def run_warm(args, rank, local):
     print(json.dumps(out), flush=True)
 
 
+def run_infer(args, rank, local):
+    """Warm-start network inference throughput: BF16 tcgen05 convolutions vs the FP32 CUDA-core network."""
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+
+    from ptychopy_b200 import abi, synth, warmstart
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    cfg = dict(synth.CONFIGS["warm128"])
+    N = cfg["N"]
+    steps, warmup = max(args.steps if args.steps != 300 else 20, 1), max(args.warmup if args.warmup != 30 else 3, 1)
+    dx_s = synth.sample_pixel(cfg["lambd"], cfg["z"], cfg["dx_d"], N)
+    probe = synth.make_probe(N, dx_s, K=1)
+    rng = np.random.default_rng(20261207)
+    pos, X, Y = synth.raster_positions(cfg["nx"], cfg["ny"], cfg["step"], cfg["step"], dx_s, N)
+    with torch.cuda.stream(stream):
+        amp = synth.make_patterns_torch(synth.make_object(X, Y, rng), probe, pos, N, cfg["photons"], seed=20261207)
+        P = amp.shape[0]
+        net = warmstart.Net(N=N, width=16, seed=0)
+        tc = warmstart.TcNet(net)
+        out = torch.empty((P, 3, N // 4, N // 4), device="cuda")
+        for _ in range(warmup):
+            warmstart.predict(tc, amp, chunk=P, out=out)
+        stream.synchronize()
+        clocks = Clocks(local)
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            tc.forward_amp(amp, P, out)
+        e1.record(stream)
+        stream.synchronize()
+        clk = clocks.stop()
+        tc.check()
+        ms = e0.elapsed_time(e1) / steps
+        # the dominant tensor-core layer (256 -> 256 channels at 8 x 8) timed alone for the roofline
+        L = abi.lib()
+        l5 = 5
+        cin, cout, H = net.plan[l5][0], net.plan[l5][1], net.plan[l5][2]
+        xin = torch.zeros((P, H, H, cin), dtype=torch.bfloat16, device="cuda")
+        y = torch.empty((P, H, H, cout), dtype=torch.bfloat16, device="cuda")
+
+        def layer():
+            abi.check(L.pty_tc_conv3x3(warmstart._p(xin), warmstart._p(tc.wpk[l5]),
+                                       warmstart._p(net._b(net.params, l5)), warmstart._p(y), P, cin, cout, H, H, 1,
+                                       0, 0, 1.0, warmstart._p(tc.err), warmstart._stream()))
+
+        for _ in range(3):
+            layer()
+        e0.record(stream)
+        for _ in range(10):
+            layer()
+        e1.record(stream)
+        stream.synchronize()
+        layer_ms = e0.elapsed_time(e1) / 10
+        flops = 2.0 * P * H * H * cout * cin * 9
+        e0.record(stream)
+        warmstart.predict(net, amp, chunk=256, out=out)
+        e1.record(stream)
+        stream.synchronize()
+        fp32_ms = e0.elapsed_time(e1)
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    pk = {"bf16_tflops": 1590.0, "source": "fallback"}
+    if os.path.exists(path):
+        with open(path) as f:
+            pk = {"bf16_tflops": float(json.load(f)["bf16_tflops"]), "source": "measured (burst)"}
+    achieved = flops / (layer_ms * 1e-3) / 1e12
+    total_flops = sum(2.0 * P * h * h * co * ci * 9 for ci, co, h, _r, _a in net.plan)
+    print(json.dumps({
+        "metric": "warm-start network inference, patterns/s (BF16 tcgen05)", "value": round(P / (ms * 1e-3), 1),
+        "unit": "patterns/s", "higher_is_better": True, "n_gpus": 1, "steps": steps, "warmup": warmup,
+        "ms_per_step": round(ms, 4), "dtype": "bf16", "data": "synthetic", "scaling": "weak", "vs_baseline": None,
+        "network_tflops": round(total_flops / (ms * 1e-3) / 1e12, 1),
+        "fp32_cuda_core_ms_per_step": round(fp32_ms, 3),
+        "roofline": {"bound": "tensor", "kernel": "k_conv_tc (256 -> 256 channels, 8 x 8, 4096 patterns)",
+                     "achieved": round(achieved, 1), "peak": pk["bf16_tflops"], "peak_source": pk["source"],
+                     "unit": "TFLOP/s", "frac": round(achieved / pk["bf16_tflops"], 4), "layer_ms": round(layer_ms, 4),
+                     "traffic": None},
+        "clocks": clk,
+        "config": {"workload": f"width-16 encoder-decoder (1.15 M parameters), {P} patterns of {N}^2, one batch",
+                   "timing": "CUDA events over one forward pass of all patterns, inputs resident in HBM"},
+    }), flush=True)
+
+
 BATCH_SCANS = [  # (algorithm, N, raster, step m)
     ("DM", 128, 10, 30e-9), ("DM", 128, 20, 50e-9), ("DM", 256, 15, 60e-9), ("DM", 256, 25, 80e-9),
     ("DM", 512, 10, 50e-9), ("DM", 512, 20, 100e-9), ("DM", 128, 40, 40e-9), ("DM", 256, 30, 70e-9),
@@ -820,6 +911,8 @@ def main():
         run_mls(args, rank, local)
     elif args.algo == "warm" and args.impl == "b200":
         run_warm(args, rank, local)
+    elif args.algo == "infer" and args.impl == "b200":
+        run_infer(args, rank, local)
     elif args.impl == "reference":
         run_reference(args, rank)
     else:

@@ -5,7 +5,8 @@
 // channel, k = tap * Cin + ci (tap = 3 * (dy + 1) + (dx + 1)), A[m][k] = x[pixel m shifted by the tap][ci] (zero
 // outside the image), B[n][k] = w[n][ci][tap].  A CTA owns 128 consecutive pixels and all N (<= 256) channels: the
 // accumulator is 128 lanes x N columns of FP32 in TMEM.  K runs in stages of 64: the 128 threads stage the im2col
-// rows of A with 16-byte cp.async (zero-fill outside the image) and the pre-packed B slice, both in the canonical
+// rows of A with 16-byte cp.async (zero-fill outside the image) and one thread bulk-copies the pre-packed B slice
+// (cp.async.bulk completing on an mbarrier), both in the canonical
 // K-major no-swizzle layout (8-row x 16-byte core matrices; SBO = 128 B between 8-row groups, LBO = one K-chunk
 // block between the two 8-element halves of a K=16 slice); one thread issues the stage's tcgen05.mma (M=128, K=16)
 // and a tcgen05.commit to the stage buffer's mbarrier, so the next stage's loads overlap the tensor core.  Every
@@ -49,11 +50,10 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
 }
 
-// 16-byte copies global -> shared.  cg (L2 only) for the weight slices; ca (allocating in L1) for the im2col rows,
-// whose nine taps (and the four readers of an upsampled pixel) re-read the same input lines.
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
-  const int n = valid ? 16 : 0;  // src-size 0: 16 zero bytes
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(n) : "memory");
+// 16-byte copy global -> shared for the im2col rows, allocating in L1 (ca): the nine taps (and the four readers of an
+// upsampled pixel) re-read the same input lines.  src-size 0 writes 16 zero bytes.
+__device__ __forceinline__ void cp_async16_cg(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async16_l1(uint32_t dst, const void* src, bool valid) {
   const int n = valid ? 16 : 0;
@@ -62,6 +62,15 @@ __device__ __forceinline__ void cp_async16_l1(uint32_t dst, const void* src, boo
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// One-thread bulk copy global -> shared (no tensor map, no multicast) completing on an mbarrier's transaction count.
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
 }
@@ -152,7 +161,7 @@ __device__ __forceinline__ bool tc_pixel(long long tile, int r, int H, int W, lo
 // in_mode 0: x NHWC BF16 (H x W x Cin); 1: x NHWC BF16 of H/2 x W/2, read 2x nearest-upsampled; 2: x FP32 amplitudes
 // (B x H x W, Cin = 1) read as in_scale * log1p(amp) with the zero frequency moved to the centre.
 // out_mode 0: y NHWC BF16 (Cout channels); 1: y NCHW FP32; 2: y NHWC BF16 2x2-average-pooled (H/2 x W/2).
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(TC_THREADS, 5)  // 5 CTAs per SM for the narrow layers (<= 96 registers)
     k_conv_tc(const void* __restrict__ x, const __nv_bfloat16* __restrict__ wpk, const float* __restrict__ bias,
               void* __restrict__ y, int B, int H, int W, int Cin, int Cout, int Npad, int Kp, int relu, int in_mode,
               int out_mode, float in_scale, int* __restrict__ err) {
@@ -162,7 +171,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t sbase = smem_u32(smem);
   const int STAGE = TcSmem::stage(Npad);
-  const uint32_t bar0 = sbase + 2 * STAGE, bar1 = bar0 + 8;
+  // bar0/bar1: MMAs of the buffer's item done (tcgen05.commit); full0/full1: the buffer's weight slice has landed
+  const uint32_t bar0 = sbase + 2 * STAGE, bar1 = bar0 + 8, full0 = bar0 + 16, full1 = bar0 + 24;
+  __shared__ int s_abort;
   const int HW = H * W;
   const long long Mtot = (long long)B * HW;
   const long long ntiles = (Mtot + TC_M - 1) / TC_M;
@@ -170,6 +181,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const int nstages = (Kp + TC_KC - 1) / TC_KC;
   const uint32_t ncols = Npad <= 32 ? 32u : (Npad <= 64 ? 64u : (Npad <= 128 ? 128u : 256u));
   const uint32_t idesc = umma_idesc_bf16(TC_M, Npad);
+  const bool b_bulk = Npad >= 128;  // weight slices of >= 16 KB per stage go through the bulk-copy unit
   if (tid == 0) s_skip = *reinterpret_cast<volatile int*>(err);
   __syncthreads();
   if (s_skip || (long long)blockIdx.x >= ntiles) return;  // uniform across the CTA
@@ -179,6 +191,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   if (tid == 0) {
     mbar_init(bar0, 1);
     mbar_init(bar1, 1);
+    mbar_init(full0, 1);
+    mbar_init(full1, 1);
+    s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {
@@ -202,6 +217,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const bool row_ok = tc_pixel(tile, tid, H, W, Mtot, out_mode == 2, pb, pi, pj);
     const __nv_bfloat16* xb = static_cast<const __nv_bfloat16*>(x);
     const int Hs = in_mode == 1 ? H / 2 : H, Ws = in_mode == 1 ? W / 2 : W;  // stored input size
+    const uint32_t dst0 = a_s + uint32_t(((tid >> 3) * 8 + (tid & 7)) * 16);
+    if (Cin % TC_KC == 0) {  // the stage's 64 k lie in one tap: one address, eight consecutive 16-byte chunks
+      const int tap = (s * TC_KC) / Cin, ci0 = s * TC_KC - tap * Cin;
+      int si = pi + tap / 3 - 1, sj = pj + tap % 3 - 1;
+      const bool v = row_ok && si >= 0 && si < H && sj >= 0 && sj < W;
+      if (in_mode == 1) {
+        si >>= 1;
+        sj >>= 1;
+      }
+      const __nv_bfloat16* src = v ? xb + (((long long)pb * Hs + si) * Ws + sj) * Cin + ci0 : xb;
+#pragma unroll
+      for (int c = 0; c < TC_KC / 8; ++c) cp_async16_l1(dst0 + uint32_t(c * (TC_M / 8) * 128), v ? src + 8 * c : xb, v);
+    } else
     for (int c = 0; c < kc / 8; ++c) {
       const int k0 = s * TC_KC + c * 8;
       const uint32_t dst = a_s + uint32_t(((c * (TC_M / 8) + (tid >> 3)) * 8 + (tid & 7)) * 16);
@@ -241,13 +269,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                      : "memory");
       }
     }
-    const __nv_bfloat16* wsrc = wpk + (size_t)Npad * TC_KC * s;  // the stage's shared-memory image
-    for (int q = tid; q < Npad * kc / 8; q += TC_THREADS) cp_async16(b_s + uint32_t(q * 16), wsrc + size_t(q) * 8, true);
+    // the packed weight slice is the stage's shared-memory image: one bulk copy by one thread for wide layers,
+    // 16-byte copies by all threads for narrow ones (whose small slices would serialise on the bulk-copy unit)
+    const __nv_bfloat16* wsrc = wpk + (size_t)Npad * TC_KC * s;
+    if (!b_bulk)
+      for (int q = tid; q < Npad * kc / 8; q += TC_THREADS)
+        cp_async16_cg(b_s + uint32_t(q * 16), wsrc + size_t(q) * 8);
     cp_async_commit();
+    if (b_bulk && tid == 0) {
+      const uint32_t fb = (i & 1) ? full1 : full0, bytes = uint32_t(Npad * kc * 2);
+      mbar_expect_tx(fb, bytes);
+      bulk_g2s(b_s, wsrc, bytes, fb);
+    }
   };
 
   bool ok = true;
-  long long issued = 0;  // items whose MMAs have been committed
+  long long issued = 0, loaded = 1;  // items whose MMAs have been committed / whose loads have been issued
   load_item(0);
   for (long long i = 0; i < nitems; ++i) {
     const int s = int(i % nstages);
@@ -256,15 +293,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     fence_async_smem();
     __syncthreads();
     if (tid == 0) {
-      tc_fence_after();
-      const uint32_t a_s = sbase + uint32_t((i & 1) * STAGE), b_s = a_s + TcSmem::A_BYTES;
-      const int kc = min(TC_KC, Kp - s * TC_KC);
-      for (int kk = 0; kk < kc / 16; ++kk) {
-        const uint64_t da = umma_desc(a_s + uint32_t(kk * 2 * (TC_M / 8) * 128), uint32_t((TC_M / 8) * 128), 128u);
-        const uint64_t db = umma_desc(b_s + uint32_t(kk * 2 * (Npad / 8) * 128), uint32_t((Npad / 8) * 128), 128u);
-        umma_bf16(tmem, da, db, idesc, s > 0 || kk > 0);
+      if (b_bulk && !mbar_wait((i & 1) ? full1 : full0, uint32_t((i >> 1) & 1))) {  // the weight slice of item i
+        atomicCAS(err, 0, 3);
+        s_abort = 1;
+      } else {
+        tc_fence_after();
+        const uint32_t a_s = sbase + uint32_t((i & 1) * STAGE), b_s = a_s + TcSmem::A_BYTES;
+        const int kc = min(TC_KC, Kp - s * TC_KC);
+        for (int kk = 0; kk < kc / 16; ++kk) {
+          const uint64_t da = umma_desc(a_s + uint32_t(kk * 2 * (TC_M / 8) * 128), uint32_t((TC_M / 8) * 128), 128u);
+          const uint64_t db = umma_desc(b_s + uint32_t(kk * 2 * (Npad / 8) * 128), uint32_t((Npad / 8) * 128), 128u);
+          umma_bf16(tmem, da, db, idesc, s > 0 || kk > 0);
+        }
       }
-      umma_commit(bar);
+      umma_commit(bar);  // committed either way, so every barrier keeps one phase per item
     }
     issued = i + 1;
     if (i + 1 < nitems) {
@@ -273,18 +315,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (tid == 0) atomicCAS(err, 0, 1);
         ok = false;
       }
-      if (__syncthreads_or(!ok)) {
+      if (__syncthreads_or(!ok || s_abort)) {
         ok = false;
         break;
       }
       load_item(i + 1);
+      loaded = i + 2;
     }
     if (s == nstages - 1) {
       if (!mbar_wait(bar, uint32_t((i >> 1) & 1))) {  // this tile's last commit covers all its MMAs
         if (tid == 0) atomicCAS(err, 0, 2);
         ok = false;
       }
-      if (__syncthreads_or(!ok)) {
+      if (__syncthreads_or(!ok || s_abort)) {
         ok = false;
         break;
       }
@@ -344,9 +387,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
   }
   cp_async_wait_all();
-  if (!ok && tid == 0 && issued > 0) {
-    // a wait gave up: give the MMAs already issued one more bounded wait before the accumulator is released
-    mbar_wait(((issued - 1) & 1) ? bar1 : bar0, uint32_t(((issued - 1) >> 1) & 1));
+  if (!ok && tid == 0) {
+    // a wait gave up: give the MMAs and the weight copies already issued one more bounded wait before the
+    // accumulator and the shared memory are released
+    if (issued > 0) mbar_wait(((issued - 1) & 1) ? bar1 : bar0, uint32_t(((issued - 1) >> 1) & 1));
+    if (b_bulk)
+      for (long long j = issued > 0 ? issued - 1 : 0; j < loaded; ++j)
+        mbar_wait((j & 1) ? full1 : full0, uint32_t((j >> 1) & 1));
   }
   tc_fence_before();
   __syncthreads();
