@@ -718,8 +718,48 @@ def run_warm(args, rank, local):
         r, h = iterate(s, warm_ms if init is not None else 0.0, 0)
         dm[name] = {"reached": r, "history": h if len(h) <= 8 else h[:5] + h[-3:]}
         s.close()
+    # end to end through the reference-facing module with host arrays: plain epienp for the iterations the plain
+    # arm needed vs epienpinit(warmStart=...) + epieresobj; host wall clock, one untimed call of each first
+    e2e = None
+    if plain and warm:
+        import ptychopy_b200
+
+        ptychopy = ptychopy_b200.import_ptychopy()
+        amp_h = amp.cpu().numpy()
+        params = net.state()
+        common = dict(jobID="warm_e2e", diffractionNP=amp_h, probeNP=probe, size=N, scanDimsx=cfg["nx"],
+                      scanDimsy=cfg["ny"], stepx=cfg["step"], stepy=cfg["step"], lambd=cfg["lambd"], z=cfg["z"],
+                      dx_d=cfg["dx_d"], beamSize=synth.BEAM_FWHM, probeModes=1, device=local)
+
+        def plain_call():
+            o, _ = ptychopy.epienp(iter=plain["iterations"], returnResults=1, writeResults=0, **common)
+            return o
+
+        def warm_call():
+            ptychopy.epienpinit(iter=max(warm["iterations"], 1), warmStart=params, warmStartWidth=16, writeResults=0,
+                                **common)
+            for _ in range(warm["iterations"]):
+                ptychopy.epiestep()
+            o = ptychopy.epieresobj()
+            ptychopy.epiepost(writeResults=0)
+            return o
+
+        times = {}
+        for name, fn in (("plain", plain_call), ("warm", warm_call)):
+            fn()
+            torch.cuda.synchronize()
+            t0 = time.time()
+            o = fn()
+            torch.cuda.synchronize()
+            times[name] = ((time.time() - t0) * 1e3, synth.phase_nrmse(o, obj, mask))
+        e2e = {"value": round(times["warm"][0], 2), "unit": "ms", "plain_ms": round(times["plain"][0], 2),
+               "warm_nrmse": round(times["warm"][1], 5), "plain_nrmse": round(times["plain"][1], 5),
+               "h2d_bytes_per_step": int(amp_h.nbytes), "d2h_bytes_per_step": int(X * Y * 8),
+               "call": "ptychopy.epienp(iter=plain iterations) vs ptychopy.epienpinit(warmStart=...) + epieresobj, "
+                       "host arrays, session set-up included"}
     clk = clocks.stop()
     out.update({
+        "e2e": e2e,
         "value": warm["gpu_ms"] if warm else None,
         "plain": {"reached": plain, "history": plain_hist},
         "warm": {"reached": warm, "infer_ms": round(infer_ms, 3), "assemble_ms": round(assemble_ms, 3),

@@ -229,6 +229,22 @@ __global__ void __launch_bounds__(TC_THREADS, 5)  // 5 CTAs per SM for the narro
       const __nv_bfloat16* src = v ? xb + (((long long)pb * Hs + si) * Ws + sj) * Cin + ci0 : xb;
 #pragma unroll
       for (int c = 0; c < TC_KC / 8; ++c) cp_async16_l1(dst0 + uint32_t(c * (TC_M / 8) * 128), v ? src + 8 * c : xb, v);
+    } else if ((Cin & 7) == 0) {  // Cin in {8, 16, 32, ...}: a stage spans several taps; one address per tap
+      for (int c = 0; c < kc / 8;) {
+        const int k0 = s * TC_KC + c * 8;
+        const int tap = k0 / Cin, ci0 = k0 - tap * Cin;
+        const int run = min((Cin - ci0) >> 3, kc / 8 - c);  // chunks of this tap inside the stage
+        int si = pi + tap / 3 - 1, sj = pj + tap % 3 - 1;
+        const bool v = row_ok && tap < 9 && si >= 0 && si < H && sj >= 0 && sj < W;
+        if (in_mode == 1) {
+          si >>= 1;
+          sj >>= 1;
+        }
+        const __nv_bfloat16* src = v ? xb + (((long long)pb * Hs + si) * Ws + sj) * Cin + ci0 : xb;
+        for (int q = 0; q < run; ++q)
+          cp_async16_l1(dst0 + uint32_t((c + q) * (TC_M / 8) * 128), v ? src + 8 * q : xb, v);
+        c += run;
+      }
     } else
     for (int c = 0; c < kc / 8; ++c) {
       const int k0 = s * TC_KC + c * 8;

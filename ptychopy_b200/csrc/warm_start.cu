@@ -63,9 +63,9 @@ void run_warm_start(pty_session* s) {
   prm.alloc(sizeof(float) * s->warm_params.size(), "warm-start parameters");
   check_cuda(cudaMemcpyAsync(prm.p, s->warm_params.data(), prm.bytes, cudaMemcpyHostToDevice, st), "H2D parameters");
   std::vector<const float*> wl(plan.size()), bl(plan.size());
-  std::vector<DeviceBuf> wpk(plan.size());
   std::vector<bool> cuda_core(plan.size(), false);
-  size_t off = 0;
+  std::vector<size_t> wpk_off(plan.size(), 0);
+  size_t off = 0, ws = 0;
   for (size_t l = 0; l < plan.size(); ++l) {
     const WarmLayer& L = plan[l];
     wl[l] = prm.as<float>() + off;
@@ -75,28 +75,44 @@ void run_warm_start(pty_session* s) {
     if (!cuda_core[l]) {
       const int n = pty_tc_weights_size(L.cin, L.cout);
       need(n > 0, "warm-start layer " + std::to_string(l) + " is not supported by the tensor-core path");
-      wpk[l].alloc(2 * size_t(n), "packed weights");
-      call(pty_tc_pack_weights(wl[l], L.cin, L.cout, wpk[l].p, st), "pack weights");
+      wpk_off[l] = ws;
+      ws += (2 * size_t(n) + 255) / 256 * 256;
     }
   }
-  // activations for one chunk of patterns (NHWC BF16, pooling fused into the producing layer)
+  // one workspace: the packed weights, the activations of one chunk of patterns (NHWC BF16, pooling fused into the
+  // producing layer), the network outputs of all patterns and the error flag
   const int chunk = std::min(P, 1024);
-  std::vector<DeviceBuf> act(plan.size());
+  std::vector<size_t> act_off(plan.size(), 0);
   for (int l = 0; l < last; ++l) {
     const int side = plan[l].after == 1 ? plan[l].H / 2 : plan[l].H;
-    act[l].alloc(2 * size_t(chunk) * side * side * plan[l].cout, "warm-start activations");
+    act_off[l] = ws;
+    ws += (2 * size_t(chunk) * side * side * plan[l].cout + 255) / 256 * 256;
   }
-  DeviceBuf out, err;
-  out.alloc(sizeof(float) * size_t(P) * 3 * S * S, "network outputs");
-  err.alloc(sizeof(int), "error flag");
-  check_cuda(cudaMemsetAsync(err.p, 0, sizeof(int), st), "memset flag");
+  const size_t out_off = ws;
+  ws += (sizeof(float) * size_t(P) * 3 * S * S + 255) / 256 * 256;
+  const size_t err_off = ws;
+  ws += 256;
+  DeviceBuf work_all;
+  work_all.alloc(ws, "warm-start workspace");
+  char* base = work_all.as<char>();
+  std::vector<void*> wpk(plan.size(), nullptr);
+  for (size_t l = 0; l < plan.size(); ++l)
+    if (!cuda_core[l]) {
+      wpk[l] = base + wpk_off[l];
+      call(pty_tc_pack_weights(wl[l], plan[l].cin, plan[l].cout, wpk[l], st), "pack weights");
+    }
+  std::vector<void*> act(plan.size(), nullptr);
+  for (int l = 0; l < last; ++l) act[l] = base + act_off[l];
+  float* out = reinterpret_cast<float*>(base + out_off);
+  int* err = reinterpret_cast<int*>(base + err_off);
+  check_cuda(cudaMemsetAsync(err, 0, sizeof(int), st), "memset flag");
   for (int c0 = 0; c0 < P; c0 += chunk) {
     const int B = std::min(chunk, P - c0);
     const void* cur = s->amp.as<float>() + size_t(c0) * NN;
     int in_mode = 2;
     for (int l = 0; l <= last; ++l) {
       const WarmLayer& L = plan[l];
-      void* y = l == last ? static_cast<void*>(out.as<float>() + size_t(c0) * 3 * S * S) : act[l].p;
+      void* y = l == last ? static_cast<void*>(out + size_t(c0) * 3 * S * S) : act[l];
       if (cuda_core[l] && l == 0) {
         call(pty_tc_first_layer(static_cast<const float*>(cur), wl[l], bl[l], y, B, L.cout, L.H, L.H,
                                 WARM_INPUT_SCALE, st),
@@ -106,8 +122,8 @@ void run_warm_start(pty_session* s) {
              "output layer");
       } else {
         const int out_mode = l == last ? 1 : (L.after == 1 ? 2 : 0);
-        call(pty_tc_conv3x3(cur, wpk[l].p, bl[l], y, B, L.cin, L.cout, L.H, L.H, L.relu ? 1 : 0, in_mode, out_mode,
-                            WARM_INPUT_SCALE, err.as<int>(), st),
+        call(pty_tc_conv3x3(cur, wpk[l], bl[l], y, B, L.cin, L.cout, L.H, L.H, L.relu ? 1 : 0, in_mode, out_mode,
+                            WARM_INPUT_SCALE, err, st),
              "convolution");
       }
       cur = y;
@@ -119,7 +135,7 @@ void run_warm_start(pty_session* s) {
   check_cuda(cudaMemcpyAsync(ph.data(), s->probe.p, sizeof(float2) * NN, cudaMemcpyDeviceToHost, st), "D2H probe");
   check_cuda(cudaStreamSynchronize(st), "warm-start network");
   int flag = 0;
-  check_cuda(cudaMemcpy(&flag, err.p, sizeof(int), cudaMemcpyDeviceToHost), "D2H flag");
+  check_cuda(cudaMemcpy(&flag, err, sizeof(int), cudaMemcpyDeviceToHost), "D2H flag");
   need(flag == 0, "warm-start network: a tensor-core pipeline wait timed out", PTY_ERR_CUDA);
   const int o = (N - S) / 2;
   std::vector<float> wgt(size_t(S) * S);
@@ -140,7 +156,7 @@ void run_warm_start(pty_session* s) {
   work.alloc(sizeof(float) * (6 * size_t(M) * M + 4), "phase integration");
   check_cuda(cudaMemcpyAsync(wd.p, wgt.data(), wd.bytes, cudaMemcpyHostToDevice, st), "H2D weights");
   check_cuda(cudaMemcpyAsync(pos.p, s->geo.pos.data(), pos.bytes, cudaMemcpyHostToDevice, st), "H2D positions");
-  call(pty_warm_stitch(out.as<float>(), pos.as<float>(), P, wd.as<float>(), S, N, WARM_AMP_MEAN, WARM_AMP_SCALE,
+  call(pty_warm_stitch(out, pos.as<float>(), P, wd.as<float>(), S, N, WARM_AMP_MEAN, WARM_AMP_SCALE,
                        WARM_GRAD_SCALE, acc.as<float>(), s->X, s->Y, st),
        "stitching");
   call(pty_warm_object(acc.as<float>(), s->X, s->Y, WARM_WMIN, WARM_AMP_MEAN, static_cast<const float*>(s->probe.p), N,
