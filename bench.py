@@ -34,8 +34,8 @@ P * O) are reported beside them.
 seeded random weights, on the 4096 patterns of the warm-start workload): patterns/s per forward pass, the FP32
 CUDA-core forward beside it, and the roofline of the dominant tcgen05 convolution against the measured BF16 peak.
 
-`--algo epie --cfg epie128|epie256k5` measures the ePIE configurations instead (10x10 raster at 128^2 with one probe
-mode; 51x51 raster at 256^2 with 5 modes): one step = one ePIE iteration over all positions, after enough warm-up
+`--algo epie --cfg epie128|epie256k5|dm512` measures the ePIE configurations instead (10x10 raster at 128^2 with one
+probe mode; 51x51 raster at 256^2 with 5 modes; ePIE on the 30x30 raster at 512^2 of the DM configuration): one step = one ePIE iteration over all positions, after enough warm-up
 iterations that the probe (iteration 10) and the modes (iteration 20) are being updated.
 """
 import argparse
@@ -72,7 +72,8 @@ def parse():
     ap.add_argument("--shard", action="store_true",
                     help="N>1: split the 900 positions over the GPUs (one NCCL all-reduce of the DM increments per "
                          "iteration, strong scaling) instead of independent replicas")
-    ap.add_argument("--cfg", default="epie128", choices=["epie128", "epie256k5"], help="ePIE configuration")
+    ap.add_argument("--cfg", default="epie128", choices=["epie128", "epie256k5", "dm512"],
+                    help="ePIE configuration (dm512: ePIE on the 512^2 DM configuration's scan)")
     return ap.parse_args()
 
 

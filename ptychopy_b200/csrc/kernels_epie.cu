@@ -606,7 +606,7 @@ template <> struct EpieShape<32> { static constexpr int R = 8; };
 template <> struct EpieShape<64> { static constexpr int R = 4; };
 template <> struct EpieShape<128> { static constexpr int R = 8; };
 template <> struct EpieShape<256> { static constexpr int R = 16; };
-template <> struct EpieShape<512> { static constexpr int R = 8; };
+template <> struct EpieShape<512> { static constexpr int R = 16; };
 
 template <int L>
 static size_t epie_smem(int) {

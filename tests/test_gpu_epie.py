@@ -9,7 +9,7 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-4
 
 
-@pytest.mark.parametrize("N,nx", [(64, 5), (128, 4), (32, 6), (256, 3)])
+@pytest.mark.parametrize("N,nx", [(64, 5), (128, 4), (32, 6), (256, 3), (512, 2)])
 def test_epie_matches_oracle(oracle, N, nx):
     d = dataset(N=N, nx=nx)
     s = gpu_session(d, probe=d["probe"], updateProbe=2, calculateRMS=1, seed=77)
