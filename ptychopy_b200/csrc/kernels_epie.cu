@@ -17,7 +17,8 @@
 //               per-CTA partial of Probe::getModalDoubleMax, combined after the barrier
 //
 // Cluster barriers (barrier.cluster arrive.release / wait.acquire) order the global-memory hand-offs at cluster
-// scope; there are no software spin-waits.
+// scope.  For 512 x 512 windows the same kernel runs as a whole-GPU cooperative launch of 128 CTAs whose phases are
+// separated by a device-scope grid barrier with a bounded wait (k_epie<L, R, true>).
 #include <cooperative_groups.h>
 
 #include "fft_core.cuh"
@@ -36,7 +37,44 @@ __device__ __forceinline__ void cluster_barrier() {
 }
 
 
-template <int L, int R>
+// Device-scope barrier over all CTAs of a cooperative launch (the whole-GPU variant): arrival count bar[0],
+// generation bar[1].  Thread 0 publishes its CTA's writes (fence), arrives, and the last arrival resets the count and
+// advances the generation; the others poll the generation (bounded: after EPIE_GRID_WAIT polls the CTA records
+// code 1 in *err and reports failure, so every CTA returns instead of waiting for good).
+constexpr unsigned EPIE_GRID_WAIT = 1u << 24;
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = bar + 1;
+    const unsigned gen = *vgen;
+    int ok = 1;
+    __threadfence();
+    if (atomicAdd(bar, 1u) + 1u == gridDim.x) {
+      bar[0] = 0;
+      __threadfence();
+      atomicExch(bar + 1, gen + 1u);
+    } else {
+      unsigned n = 0;
+      while (*vgen == gen) {
+        if (++n > EPIE_GRID_WAIT) {
+          ok = 0;
+          atomicCAS(err, 0, 1);
+          break;
+        }
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// GRID = false: one thread-block cluster (cluster barriers); GRID = true: all CTAs of a cooperative launch spread
+// over the GPU (grid barriers).  The phases, their work split (CTA c of C takes rows / columns [c L/C, (c+1) L/C))
+// and the global hand-offs are the same.
+template <int L, int R, bool GRID>
 __global__ void __launch_bounds__(R* FftShape<L>::T) k_epie(EpieArgs g) {
   using S = FftShape<L>;
   constexpr int T = S::T, E = S::E;
@@ -49,8 +87,17 @@ __global__ void __launch_bounds__(R* FftShape<L>::T) k_epie(EpieArgs g) {
   float2* s_sum = reinterpret_cast<float2*>(s_m2 + R * L);  // R*L (error metric, Ka > 1)
   __shared__ float s_objmax, s_probemax;
 
-  const int c = int(cg::this_cluster().block_rank());
+  const int c = GRID ? int(blockIdx.x) : int(cg::this_cluster().block_rank());
   const int C = g.C;
+  // phase separator; false only when a grid barrier timed out (then every CTA leaves the kernel)
+  auto sync_all = [&]() -> bool {
+    if constexpr (GRID) {
+      return grid_barrier(g.gbar, g.gerr);
+    } else {
+      cluster_barrier();
+      return true;
+    }
+  };
   const int v = threadIdx.x / T, t = threadIdx.x % T;
   const int rows_cta = L / C, passes = rows_cta / R;
   const int Ka = g.Ka;
@@ -98,7 +145,7 @@ __global__ void __launch_bounds__(R* FftShape<L>::T) k_epie(EpieArgs g) {
         store_rows_transposed<L, R>(a, g.W1 + size_t(k) * NN, x0, v, t, s_x);
       }
     }
-    cluster_barrier();
+    if (!sync_all()) return;
 
     // ---------------- B: column FFT, modulus, inverse column FFT, transposed store into W2 -------------------
     for (int ps = 0; ps < passes; ++ps) {
@@ -179,7 +226,7 @@ __global__ void __launch_bounds__(R* FftShape<L>::T) k_epie(EpieArgs g) {
       if (threadIdx.x == 0) atomicAdd(&g.sc->err, e / double(Ka) / double(g.sqsum[i]));
       err_acc = 0.0;
     }
-    cluster_barrier();
+    if (!sync_all()) return;
 
     // ---------------- C: inverse row FFT -> dpsi; object update; |O|^2 cache ----------------------------
     const float cO = 1.0f / s_probemax;
@@ -217,7 +264,7 @@ __global__ void __launch_bounds__(R* FftShape<L>::T) k_epie(EpieArgs g) {
         crow[n] = mag * mag;
       }
     }
-    cluster_barrier();
+    if (!sync_all()) return;
 
     if (!g.up) continue;  // the object max is only consumed by the probe update
 
@@ -237,7 +284,7 @@ __global__ void __launch_bounds__(R* FftShape<L>::T) k_epie(EpieArgs g) {
         if (lane == 0) g.TM[size_t(tr) * g.TY + tc] = m;
       }
     }
-    cluster_barrier();
+    if (!sync_all()) return;
     {
       float m = 0.f;
       const int nt = g.TX * g.TY;
@@ -284,14 +331,14 @@ __global__ void __launch_bounds__(R* FftShape<L>::T) k_epie(EpieArgs g) {
       }
       pmax = block_reduce_maxf(pmax);
       if (threadIdx.x == 0) g.pm[c] = pmax;
-      cluster_barrier();
+      if (!sync_all()) return;
       if (threadIdx.x == 0) {
         float m = 0.f;
         for (int j = 0; j < C; ++j) m = fmaxf(m, g.pm[j]);
         s_probemax = m;
       }
       __syncthreads();
-      cluster_barrier();  // pm is rewritten at the next position
+      if (!sync_all()) return;  // pm is rewritten at the next position
     }
   }
   if (c == 0 && threadIdx.x == 0) {
@@ -608,17 +655,53 @@ template <> struct EpieShape<128> { static constexpr int R = 8; };
 template <> struct EpieShape<256> { static constexpr int R = 16; };
 template <> struct EpieShape<512> { static constexpr int R = 16; };
 
-template <int L>
-static size_t epie_smem(int) {
-  constexpr int R = EpieShape<L>::R, XCH = FftShape<L>::XCH;
+// Whole-GPU variant (windows of 512): one pass of R rows per CTA, C = L / R = 128 CTAs in a cooperative launch.
+// Measured per 900-position iteration at 512^2: 47 ms against 74 ms for the 16-CTA cluster.  At 256^2 with 5
+// modes (64 CTAs of 4 rows) it measured 245 ms against 239 ms for the cluster: the row split gives both the same
+// 128 warps, and the grid barriers cost more than the cluster's, so 256 keeps the cluster.
+template <int L> struct EpieGridShape { static constexpr int R = 0; };
+template <> struct EpieGridShape<512> { static constexpr int R = 4; };
+
+template <int L, int R>
+static size_t epie_smem_r() {
+  constexpr int XCH = FftShape<L>::XCH;
   constexpr int xs = R * XCH > L * (R + 1) ? R * XCH : L * (R + 1);
   return sizeof(float2) * (L + xs) + sizeof(float) * R * L + sizeof(float2) * R * L;
+}
+template <int L>
+static size_t epie_smem(int) {
+  return epie_smem_r<L, EpieShape<L>::R>();
+}
+
+// Whole-GPU variant set-up: C = L / R CTAs must be co-resident (cooperative launch); returns C, or 0 if not possible.
+template <int L>
+static int epie_grid_prepare_t() {
+  constexpr int R = EpieGridShape<L>::R;
+  if constexpr (R == 0) {
+    return 0;
+  } else {
+    constexpr int T = FftShape<L>::T, C = L / R;
+    auto kern = k_epie<L, R, true>;
+    const size_t smem = epie_smem_r<L, R>();
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    int dev = 0, sms = 0, coop = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, R * T, smem) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    return (coop && per_sm * sms >= C) ? C : 0;
+  }
 }
 
 template <int L>
 static cudaError_t epie_prepare_t(int* C_out) {
   constexpr int R = EpieShape<L>::R, T = FftShape<L>::T;
-  auto kern = k_epie<L, R>;
+  auto kern = k_epie<L, R, false>;
   const size_t smem = epie_smem<L>(0);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
@@ -651,6 +734,8 @@ static cudaError_t epie_prepare_t(int* C_out) {
   return cudaSuccess;
 }
 
+int epie_grid_prepare(int N) { return N == 512 ? epie_grid_prepare_t<512>() : 0; }
+
 cudaError_t epie_prepare(int N, int* C_out) {
   switch (N) {
     case 32: return epie_prepare_t<32>(C_out);
@@ -664,6 +749,24 @@ cudaError_t epie_prepare(int N, int* C_out) {
 
 template <int L>
 static cudaError_t epie_launch_t(const EpieArgs& g, cudaStream_t st) {
+  if constexpr (EpieGridShape<L>::R > 0) {
+    if (g.grid) {
+      constexpr int R = EpieGridShape<L>::R, T = FftShape<L>::T;
+      cudaError_t e = cudaMemsetAsync(g.gbar, 0, 2 * sizeof(unsigned), st);
+      if (e != cudaSuccess) return e;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(g.C);
+      cfg.blockDim = dim3(R * T);
+      cfg.dynamicSmemBytes = epie_smem_r<L, R>();
+      cfg.stream = st;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeCooperative;
+      at[0].val.cooperative = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      return cudaLaunchKernelEx(&cfg, k_epie<L, R, true>, g);
+    }
+  }
   constexpr int R = EpieShape<L>::R, T = FftShape<L>::T;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(g.C);
@@ -677,7 +780,7 @@ static cudaError_t epie_launch_t(const EpieArgs& g, cudaStream_t st) {
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_epie<L, R>, g);
+  return cudaLaunchKernelEx(&cfg, k_epie<L, R, false>, g);
 }
 
 cudaError_t epie_launch(const EpieArgs& g, cudaStream_t st) {

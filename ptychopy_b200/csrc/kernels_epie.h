@@ -30,12 +30,17 @@ struct EpieArgs {
   const float2* tw;
   const double* sqsum;    // per-pattern amplitude sums (error normaliser)
   float saturation;       // pixels with A >= saturation float (no modulus)
+  unsigned* gbar;         // 2: grid-barrier count and generation (whole-GPU variant)
+  int* gerr;              // grid-barrier timeout flag (whole-GPU variant)
   int N, K, Ka, P, X, Y, TX, TY, C;
   int pc, up, rms, useAll;
+  int grid;               // 1: whole-GPU variant (C CTAs, cooperative launch); 0: one cluster of C CTAs
 };
 
 // Sets kernel attributes and picks the cluster size (largest resident of 16, 8, ...); returns it in C_out.
 cudaError_t epie_prepare(int N, int* C_out);
+// Whole-GPU variant for N = 512: the CTA count if a cooperative launch of it fits on this device, else 0.
+int epie_grid_prepare(int N);
 cudaError_t epie_launch(const EpieArgs& g, cudaStream_t st);
 // Shared-memory-resident variant for small windows with one probe mode (N = 32, 64, 128; K = 1): cluster of
 // N/32 CTAs, probe and window in (distributed) shared memory, natural-layout amplitudes.

@@ -259,10 +259,11 @@ void visiting_order(uint64_t& state, int P, std::vector<int>& order) {
 
 // Device state of the persistent ePIE kernel.
 struct EpieState {
-  DeviceBuf pos, order, W1, W2, TM, pm, sc, sq, modesCopy, ip;
+  DeviceBuf pos, order, W1, W2, TM, pm, sc, sq, modesCopy, ip, gsync;
   int C = 1, TX = 0, TY = 0;
   bool tm_valid = false;
-  bool sm = false;  // shared-memory-resident kernel (small windows, one mode)
+  bool sm = false;    // shared-memory-resident kernel (small windows, one mode)
+  bool grid = false;  // whole-GPU variant of k_epie (N = 256, 512): C CTAs in a cooperative launch
   int* order_h = nullptr;  // pinned
   ~EpieState() {
     if (order_h) cudaFreeHost(order_h);
@@ -539,10 +540,20 @@ void init_epie(pty_session* s) {
   s->ep = ep;
   const size_t NN = size_t(s->N) * s->N, XY = size_t(s->X) * s->Y;
   ep->sm = epie_uses_smem(s->N, s->K);
-  if (ep->sm)
+  if (ep->sm) {
     check_cuda(epie_sm_prepare(s->N), "ePIE kernel set-up");
-  else
-    check_cuda(epie_prepare(s->N, &ep->C), "ePIE kernel set-up (cluster size)");
+  } else {
+    const int Cg = epie_grid_prepare(s->N);
+    if (Cg > 0) {
+      ep->grid = true;
+      ep->C = Cg;
+    } else {
+      check_cuda(epie_prepare(s->N, &ep->C), "ePIE kernel set-up (cluster size)");
+    }
+  }
+  // grid-barrier count and generation, then the timeout flag
+  ep->gsync.alloc(4 * sizeof(unsigned), "grid barrier");
+  check_cuda(cudaMemsetAsync(ep->gsync.p, 0, ep->gsync.bytes, s->stream), "memset barrier");
   ep->pos.alloc(sizeof(float2) * s->P, "positions");
   check_cuda(cudaMemcpyAsync(ep->pos.p, s->geo.pos.data(), sizeof(float2) * s->P, cudaMemcpyHostToDevice, s->stream),
              "H2D positions");
@@ -553,7 +564,7 @@ void init_epie(pty_session* s) {
   ep->TX = (s->X + 15) / 16;
   ep->TY = (s->Y + 15) / 16;
   ep->TM.alloc(sizeof(float) * ep->TX * ep->TY, "tile maxima");
-  ep->pm.alloc(sizeof(float) * 16, "partial maxima");
+  ep->pm.alloc(sizeof(float) * 256, "partial maxima");  // one per CTA
   ep->sc.alloc(sizeof(EpieScalars), "scalars");
   ep->ip.alloc(4 * sizeof(double), "inner products");
   s->ocache.alloc(sizeof(float) * XY, "object cache");
@@ -974,8 +985,17 @@ double step_epie(pty_session* s, int it, bool want_err) {
   g.up = up;
   g.rms = s->prm.calculateRMS ? 1 : 0;
   g.useAll = s->useAll ? 1 : 0;
+  g.grid = ep->grid ? 1 : 0;
+  g.gbar = ep->gsync.as<unsigned>();
+  g.gerr = reinterpret_cast<int*>(ep->gsync.as<unsigned>() + 2);
   check_cuda(ep->sm ? epie_sm_launch(g, s->stream) : epie_launch(g, s->stream), "ePIE kernel launch");
   s->launches += 1;
+  if (ep->grid) {  // the whole-GPU variant reports a grid-barrier timeout through a device flag
+    int flag = 0;
+    check_cuda(cudaMemcpyAsync(&flag, g.gerr, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H flag");
+    check_cuda(cudaStreamSynchronize(s->stream), "ePIE iteration");
+    need(flag == 0, "ePIE: a grid barrier timed out (the iteration did not complete)", PTY_ERR_CUDA);
+  }
   if (!want_err || !s->prm.calculateRMS) return 0.0;
   double e = 0;
   check_cuda(cudaMemcpyAsync(&e, &reinterpret_cast<EpieScalars*>(ep->sc.p)->err, sizeof(double),
