@@ -206,6 +206,13 @@ int pty_tc_first_layer(const float* amp, const float* w, const float* bias, void
 int pty_tc_last_layer(const void* x, const float* w, const float* bias, float* y, int B, int Cin, int Cout, int H,
                       int W, void* stream);
 int pty_tc_pool2(const void* x, void* y, int B, int H, int W, int C, void* stream);
+
+/* Failure detection of the bounded device waits, without a GPU fault.  codes[0]: an mbarrier wait on a phase that
+ * nothing completes gave up (1 expected); codes[1]: the same wait after one arrival did not (0 expected);
+ * codes[2]: 64 grid barriers over 16 CTAs of a cooperative launch that reach their count timed out (0 expected);
+ * codes[3]: a grid barrier expecting one arrival too many timed out and every CTA returned (1 expected).
+ * Synchronous, on the current device, a few milliseconds. */
+int pty_selftest_bounded_waits(int* codes);
 int pty_tc_up2(const void* x, void* y, int B, int H, int W, int C, void* stream);
 int pty_tc_to_bf16(const float* x, void* y, size_t n, void* stream);
 int pty_warm_stitch(const float* out, const float* pos_px, int P, const float* weight, int S, int N, float amp_mean,

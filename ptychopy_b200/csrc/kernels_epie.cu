@@ -42,7 +42,9 @@ __device__ __forceinline__ void cluster_barrier() {
 // advances the generation; the others poll the generation (bounded: after EPIE_GRID_WAIT polls the CTA records
 // code 1 in *err and reports failure, so every CTA returns instead of waiting for good).
 constexpr unsigned EPIE_GRID_WAIT = 1u << 24;
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err) {
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned expected = 0,
+                                             unsigned limit = EPIE_GRID_WAIT) {
+  if (expected == 0) expected = gridDim.x;
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -50,14 +52,14 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err) {
     const unsigned gen = *vgen;
     int ok = 1;
     __threadfence();
-    if (atomicAdd(bar, 1u) + 1u == gridDim.x) {
+    if (atomicAdd(bar, 1u) + 1u == expected) {
       bar[0] = 0;
       __threadfence();
       atomicExch(bar + 1, gen + 1u);
     } else {
       unsigned n = 0;
       while (*vgen == gen) {
-        if (++n > EPIE_GRID_WAIT) {
+        if (++n > limit) {
           ok = 0;
           atomicCAS(err, 0, 1);
           break;
@@ -871,6 +873,31 @@ cudaError_t epie_init_modes(float2* probe, float* pcache, int K, int N, float2* 
       k_project_sub<<<grid, 256, 0, st>>>(probe + size_t(i) * NN, probe + size_t(j) * NN, NN, scratch3);
     }
   return cudaGetLastError();
+}
+
+// Self-test of the bounded grid barrier (failure detection without a GPU fault): a cooperative launch of C CTAs
+// passes `rounds` barriers expecting `expected` arrivals with at most `limit` polls each; a barrier whose count
+// cannot be reached (expected > C) must time out, set *err and let every CTA return.
+__global__ void k_selftest_grid_barrier(unsigned* bar, int* err, unsigned expected, unsigned limit, int rounds) {
+  for (int r = 0; r < rounds; ++r)
+    if (!grid_barrier(bar, err, expected, limit)) return;
+}
+
+cudaError_t selftest_grid_barrier(int ctas, unsigned expected, unsigned limit, int rounds, unsigned* bar, int* err,
+                                  cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ctas);
+  cfg.blockDim = dim3(64);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_selftest_grid_barrier, bar, err, expected, limit, rounds);
 }
 
 }  // namespace pty

@@ -50,6 +50,10 @@ cudaError_t epie_sm_launch(const EpieArgs& g, cudaStream_t st);
 // Modes 1..K-1 = 0.05 * mode 0, then Gram-Schmidt against the original copies.
 cudaError_t epie_init_modes(float2* probe, float* pcache, int K, int N, float2* copy, double* scratch3,
                             cudaStream_t st);
+// Self-test of the bounded grid barrier: `ctas` CTAs, `rounds` barriers expecting `expected` arrivals, at most
+// `limit` polls per wait; *err = 1 if a wait ran out.
+cudaError_t selftest_grid_barrier(int ctas, unsigned expected, unsigned limit, int rounds, unsigned* bar, int* err,
+                                  cudaStream_t st);
 // Tile maxima of the whole |O|^2 cache.
 cudaError_t tile_max_all(const float* ocache, int X, int Y, float* TM, int TX, int TY, cudaStream_t st);
 

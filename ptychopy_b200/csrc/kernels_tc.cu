@@ -20,6 +20,7 @@
 #include <string>
 
 #include "../../include/ptychopy_b200.h"
+#include "kernels_epie.h"
 
 namespace pty {
 void set_last_error(const std::string& msg);  // session.cu
@@ -75,8 +76,8 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
 }
 // true when the phase with the given parity has completed; gives up after TC_WAIT_LIMIT rounds
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (uint32_t i = 0; i < TC_WAIT_LIMIT; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit = TC_WAIT_LIMIT) {
+  for (uint32_t i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -573,6 +574,27 @@ __global__ void __launch_bounds__(256) k_tc_last(const __nv_bfloat16* __restrict
   }
 }
 
+// Self-test of the bounded mbarrier wait: out[0] = 1 when a wait on a phase nothing completes gives up after `limit`
+// rounds (the expected outcome), out[1] = 0 when the same wait succeeds after one arrival (the control).
+__global__ void k_selftest_mbar(int* out, uint32_t limit) {
+  __shared__ __align__(8) unsigned long long bar;
+  const uint32_t b = smem_u32(&bar);
+  if (threadIdx.x == 0) {
+    mbar_init(b, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  const bool completed = mbar_wait(b, 0, limit);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    out[0] = completed ? 0 : 1;
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(b) : "memory");
+  }
+  __syncthreads();
+  const bool after = mbar_wait(b, 0, limit);
+  if (threadIdx.x == 0) out[1] = after ? 0 : 1;
+}
+
 int grid1(size_t n) {
   const size_t g = (n + 255) / 256;
   return int(g < 1 ? 1 : (g > 8192 ? 8192 : g));
@@ -672,6 +694,29 @@ int pty_tc_last_layer(const void* x, const float* w, const float* bias, float* y
   k_tc_last<32><<<grid1(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const __nv_bfloat16*>(x), w,
                                                                           bias, y, B, H, W, Cout);
   return finish(cudaGetLastError(), "pty_tc_last_layer");
+}
+
+int pty_selftest_bounded_waits(int* codes) {
+  if (!codes) return fail("pty_selftest_bounded_waits: null argument", PTY_ERR_INVALID);
+  int* d = nullptr;
+  unsigned* bar = nullptr;
+  cudaError_t e = cudaMalloc(&d, 8 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&bar, 4 * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(d, 0xFF, 8 * sizeof(int));
+  if (e == cudaSuccess) {
+    k_selftest_mbar<<<1, 64>>>(d, 1u << 12);
+    e = cudaGetLastError();
+  }
+  // grid barrier: 16 CTAs, 64 rounds reaching their count (control), then one round expecting 17 arrivals
+  if (e == cudaSuccess) e = selftest_grid_barrier(16, 16, 1u << 16, 64, bar, d + 2, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(codes + 2, d + 2, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = selftest_grid_barrier(16, 17, 1u << 16, 1, bar, d + 3, nullptr);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(codes, d, 2 * sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(codes + 3, d + 3, sizeof(int), cudaMemcpyDeviceToHost);
+  if (d) cudaFree(d);
+  if (bar) cudaFree(bar);
+  return finish(e, "pty_selftest_bounded_waits");
 }
 
 int pty_tc_pool2(const void* x, void* y, int B, int H, int W, int C, void* stream) {
