@@ -34,6 +34,10 @@ P * O) are reported beside them.
 seeded random weights, on the 4096 patterns of the warm-start workload): patterns/s per forward pass, the FP32
 CUDA-core forward beside it, and the roofline of the dominant tcgen05 convolution against the measured BF16 peak.
 
+`--algo fft` measures the precision pattern: the batched 2-D FFT of 900 patterns of 256^2 as split-BF16 tensor-core
+GEMM stages (pty_fft2_tc) against the engine's FP32 FFT (pty_fft2_dev), each with its error against numpy's FP64
+FFT on a sample.
+
 `--algo epie --cfg epie128|epie256k5|dm512` measures the ePIE configurations instead (10x10 raster at 128^2 with one
 probe mode; 51x51 raster at 256^2 with 5 modes; ePIE on the 30x30 raster at 512^2 of the DM configuration): one step = one ePIE iteration over all positions, after enough warm-up
 iterations that the probe (iteration 10) and the modes (iteration 20) are being updated.
@@ -70,7 +74,7 @@ def parse():
                     help="skip the ePIE 512^2 and warm-start parts of the headline after the DM line")
     ap.add_argument("--nx", type=int, default=30, help="raster size (30 = the DM configuration; smaller for profiling)")
     ap.add_argument("--wave", type=int, default=0, help="DM patterns per pipeline wave (0 = automatic)")
-    ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch", "nrmse", "mls", "warm", "infer"])
+    ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch", "nrmse", "mls", "warm", "infer", "fft"])
     ap.add_argument("--shard", action="store_true",
                     help="N>1: split the 900 positions over the GPUs (one NCCL all-reduce of the DM increments per "
                          "iteration, strong scaling) instead of independent replicas")
@@ -909,6 +913,70 @@ def run_infer(args, rank, local):
     }), flush=True)
 
 
+def run_fft(args, rank, local):
+    """Split-BF16 tensor-core 2-D FFT vs the FP32 FFT: time per batch and error vs FP64."""
+    if rank != 0:
+        return
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from ptychopy_b200 import abi
+
+    torch.cuda.set_device(local)
+    L = abi.lib()
+    B, N = 900, 256
+    steps = args.steps if args.steps != 300 else 20
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20261209)
+    base = torch.randn((B, N, N, 2), generator=g, device="cuda")
+    d = base.clone()
+    w = torch.empty_like(d)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+
+    def tc():
+        abi.check(L.pty_fft2_tc(p(d), p(w), B, N, 0, p(err), ctypes.c_void_p(stream)))
+
+    def fp32():
+        abi.check(L.pty_fft2_dev(p(d), p(w), B, N, 0, ctypes.c_void_p(stream)))
+
+    res = {}
+    for name, fn in (("tensor_core_split_bf16", tc), ("fp32", fp32)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        # error on a 2-pattern sample against numpy's FP64 FFT
+        d.copy_(base)
+        fn()
+        torch.cuda.synchronize()
+        got = d[:2].cpu().numpy().view(np.complex64)[..., 0].astype(np.complex128)
+        src = base[:2].cpu().numpy().view(np.complex64)[..., 0].astype(np.complex128)
+        exact = np.fft.fft2(src)
+        rel = float(np.linalg.norm(got - exact) / np.linalg.norm(exact))
+        algo_bytes = 2 * 16.0 * N * N * B  # two passes, each reading and writing every element once
+        res[name] = {"ms_per_batch": round(ms, 4), "patterns_per_s": round(B / (ms * 1e-3), 1),
+                     "algorithmic_GBps": round(algo_bytes / (ms * 1e-3) / 1e9, 1), "rel_err_vs_fp64": rel}
+        d.copy_(base)
+    assert int(err.item()) == 0, "tensor-core FFT wait timed out"
+    print(json.dumps({"metric": "batched 2-D FFT, patterns/s (split-BF16 tensor cores vs FP32)",
+                      "value": res["tensor_core_split_bf16"]["patterns_per_s"], "unit": "patterns/s",
+                      "higher_is_better": True, "n_gpus": 1, "steps": steps, "dtype": "bf16x3 / f32",
+                      "data": "synthetic (seeded normal)", "results": res,
+                      "config": {"workload": f"{B} patterns of {N}^2 complex64, forward, unnormalised",
+                                 "timing": "CUDA events over repeated calls; pty_fft2_dev includes its twiddle "
+                                           "table set-up per call"}}), flush=True)
+
+
 BATCH_SCANS = [  # (algorithm, N, raster, step m)
     ("DM", 128, 10, 30e-9), ("DM", 128, 20, 50e-9), ("DM", 256, 15, 60e-9), ("DM", 256, 25, 80e-9),
     ("DM", 512, 10, 50e-9), ("DM", 512, 20, 100e-9), ("DM", 128, 40, 40e-9), ("DM", 256, 30, 70e-9),
@@ -992,6 +1060,8 @@ def main():
         run_warm(args, rank, local)
     elif args.algo == "infer" and args.impl == "b200":
         run_infer(args, rank, local)
+    elif args.algo == "fft" and args.impl == "b200":
+        run_fft(args, rank, local)
     elif args.impl == "reference":
         run_reference(args, rank)
     else:

@@ -268,6 +268,14 @@ const char* pty_last_error(void);
  * (src/CudaFFTPlan.cpp:72-101).  `work_dev` is a device buffer of batch*N*N complex64. */
 int pty_fft2_dev(void* data_dev, void* work_dev, int batch, int N, int inverse, void* cuda_stream);
 
+/* Mixed-precision batched 2-D FFT on the tensor cores (no counterpart in the reference, which calls cuFFT in FP32,
+ * src/CudaFFTPlan.cpp:91-101): every 256-point line transform is two radix-16 DFT stages computed as tcgen05 GEMMs
+ * with split-BF16 operands (x = x_hi + x_lo, the three products x_hi F_hi + x_lo F_hi + x_hi F_lo) and FP32
+ * accumulation, with FP32 twiddles between the stages.  In place on data (batch x N x N complex64, N = 256), work the
+ * same size; unnormalised like pty_fft2_dev.  *err (device int, zero on entry) receives a non-zero code if a
+ * tensor-core wait timed out.  Asynchronous on `stream`. */
+int pty_fft2_tc(void* data, void* work, int batch, int N, int inverse, int* err, void* stream);
+
 /* Allocation-free variant of pty_fft2_dev.  No counterpart in the reference (it has no entry point that avoids
  * allocation).  For callers that cannot call cudaMalloc: hosts that hand the library only buffers they allocated
  * up front and forbid allocation afterwards, such as an acquisition service that owns all device memory of the
