@@ -66,6 +66,9 @@ typedef struct pty_params {
   int calculateRMS;       /* compute the per-iteration error metric (the reference's Python path never does) */
   int device;             /* CUDA device ordinal */
   int wave;               /* DM patterns per wave of its three kernels (0 = automatic) */
+  int precision;          /* FFT arithmetic: 0 FP32 (default); 1 split-BF16 tensor-core stages (pty_fft2_tc) where a
+                             session's transforms are separate batched FFTs: MLs at N = 256.  DM and ePIE fuse their
+                             FP32 transforms into their kernels and refuse 1 (PTY_ERR_UNSUPPORTED). */
 } pty_params;
 
 typedef struct pty_session pty_session;

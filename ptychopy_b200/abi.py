@@ -55,7 +55,7 @@ class PtyParams(ctypes.Structure):
         ("simulate", ctypes.c_int), ("phaseConstraint", ctypes.c_int), ("updateProbe", ctypes.c_int),
         ("updateModes", ctypes.c_int), ("beamstopMask", ctypes.c_int), ("lf", ctypes.c_char * 256),
         ("PPS", ctypes.c_int), ("seed", ctypes.c_uint64), ("calculateRMS", ctypes.c_int),
-        ("device", ctypes.c_int), ("wave", ctypes.c_int),
+        ("device", ctypes.c_int), ("wave", ctypes.c_int), ("precision", ctypes.c_int),
     ]
 
 

@@ -15,6 +15,10 @@ cudaError_t make_twiddles(int N, float2** d_tw, cudaStream_t st);
 
 // Batched 2-D FFT in natural layout: data (batch x N x N) -> work (transposed) -> data.  Unnormalised.
 cudaError_t fft2(float2* data, float2* work, const float2* tw, int batch, int N, bool inverse, cudaStream_t st);
+// Split-BF16 tensor-core 2-D FFT (N = 256, kernels_fft_tc.cu): prepare once per device outside stream capture;
+// *err receives a non-zero code if a tensor-core wait timed out.
+cudaError_t fft2_tc_prepare();
+cudaError_t fft2_tc(float2* data, float2* work, int batch, int N, bool inverse, int* err, cudaStream_t st);
 
 // Transposes each N x N float plane: out[b][y][x] = in[b][x][y].
 cudaError_t transpose_planes(const float* in, float* out, int batch, int N, cudaStream_t st);

@@ -223,7 +223,28 @@ int fail(const std::string& msg, int code) {
   return code;
 }
 
+int g_fft_tc_sms = 0;  // SM count of the device the kernel was prepared on
+
 }  // namespace
+
+cudaError_t fft2_tc_prepare() {
+  cudaError_t e = cudaFuncSetAttribute(k_fft_tc_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, FT_SMEM);
+  int dev = 0;
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&g_fft_tc_sms, cudaDevAttrMultiProcessorCount, dev);
+  return e;
+}
+
+cudaError_t fft2_tc(float2* data, float2* work, int batch, int N, bool inverse, int* err, cudaStream_t st) {
+  if (N != FT_N || batch < 1 || g_fft_tc_sms == 0) return cudaErrorInvalidValue;
+  const int groups = batch * (FT_N / FT_LINES);
+  const int grid = groups < 4 * g_fft_tc_sms ? groups : 4 * g_fft_tc_sms;  // 4 CTAs per SM (48 KB, 32 TMEM columns)
+  const float sign = inverse ? 1.f : -1.f;
+  k_fft_tc_pass<<<grid, FT_THREADS, FT_SMEM, st>>>(data, work, groups, sign, err);
+  k_fft_tc_pass<<<grid, FT_THREADS, FT_SMEM, st>>>(work, data, groups, sign, err);
+  return cudaGetLastError();
+}
+
 }  // namespace pty
 
 using namespace pty;
@@ -231,25 +252,10 @@ using namespace pty;
 extern "C" int pty_fft2_tc(void* data, void* work, int batch, int N, int inverse, int* err, void* stream) {
   if (!data || !work || !err || batch < 1 || N != FT_N)
     return fail("pty_fft2_tc: bad argument (N must be 256)", PTY_ERR_INVALID);
-  static bool attr_set = false;
-  cudaError_t e = cudaSuccess;
-  if (!attr_set) {
-    e = cudaFuncSetAttribute(k_fft_tc_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, FT_SMEM);
-    if (e != cudaSuccess) return fail(std::string("pty_fft2_tc: ") + cudaGetErrorString(e), PTY_ERR_CUDA);
-    attr_set = true;
-  }
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int groups = batch * (FT_N / FT_LINES);
-  const int grid = groups < 4 * sms ? groups : 4 * sms;  // 4 CTAs per SM (48 KB shared memory, 32 TMEM columns each)
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const float sign = inverse ? 1.f : -1.f;
-  k_fft_tc_pass<<<grid, FT_THREADS, FT_SMEM, st>>>(static_cast<const float2*>(data), static_cast<float2*>(work),
-                                                    groups, sign, err);
-  k_fft_tc_pass<<<grid, FT_THREADS, FT_SMEM, st>>>(static_cast<const float2*>(work), static_cast<float2*>(data),
-                                                    groups, sign, err);
-  e = cudaGetLastError();
+  cudaError_t e = g_fft_tc_sms ? cudaSuccess : fft2_tc_prepare();
+  if (e == cudaSuccess)
+    e = fft2_tc(static_cast<float2*>(data), static_cast<float2*>(work), batch, N, inverse != 0, err,
+                static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return fail(std::string("pty_fft2_tc: ") + cudaGetErrorString(e), PTY_ERR_CUDA);
   return PTY_OK;
 }

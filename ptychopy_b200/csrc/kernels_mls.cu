@@ -301,9 +301,13 @@ cudaError_t mls_iteration(const MlsBuffers& b, int ngroups, cudaStream_t st) {
     const int* gs = b.gsize + g;
     dim3 grid(gb, b.Gmax);
     k_mls_exit<<<grid, 256, 0, st>>>(b.obj, b.probe, b.starts, mem, gs, N, b.Y, b.objp, b.psi);
-    if ((e = fft2(b.psi, b.work, b.tw, b.Gmax, N, false, st)) != cudaSuccess) return e;
+    if ((e = b.tc ? fft2_tc(b.psi, b.work, b.Gmax, N, false, b.tc_err, st)
+                  : fft2(b.psi, b.work, b.tw, b.Gmax, N, false, st)) != cudaSuccess)
+      return e;
     k_mls_modulus<<<grid, 256, 0, st>>>(b.psi, b.amp, mem, gs, N, b.errk);
-    if ((e = fft2(b.psi, b.work, b.tw, b.Gmax, N, true, st)) != cudaSuccess) return e;
+    if ((e = b.tc ? fft2_tc(b.psi, b.work, b.Gmax, N, true, b.tc_err, st)
+                  : fft2(b.psi, b.work, b.tw, b.Gmax, N, true, st)) != cudaSuccess)
+      return e;
     k_mls_dirs<<<grid, 256, 0, st>>>(b.psi, b.objp, b.probe, b.pobj, b.maxIllum, b.starts, mem, gs, N, b.Y, b.pum,
                                      b.S);
     k_mls_lsq<<<grid, 256, 0, st>>>(b.psi, b.objp, b.probe, b.pum, b.S, b.pobj, b.maxIllum, b.delta_p, b.starts, mem,

@@ -33,6 +33,8 @@ struct MlsBuffers {
   int N, P, X, Y, Gmax;
   float delta_p;
   double beta_obj, beta_probe;  // beta_object * beta_LSQ, beta_probe * beta_LSQ
+  int tc;                 // 1: the group FFTs run as split-BF16 tensor-core stages (fft2_tc)
+  int* tc_err;            // their wait-timeout flag
 };
 
 cudaError_t mls_illum_add(float* pobj, const float2* probe, const int2* starts, int P, int N, int Y, float scale,

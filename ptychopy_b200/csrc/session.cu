@@ -283,7 +283,7 @@ struct MlsTables {
 
 struct MlsState {
   MlsGeometry geo;
-  DeviceBuf pobj, S, pum, objp, psi, work, starts, sums, errk, betas, err, norms, maxill;
+  DeviceBuf pobj, S, pum, objp, psi, work, starts, sums, errk, betas, err, norms, maxill, tcerr;
   int Gmax = 1, ng = 1;
   size_t table_ints = 0;
   MlsTables tab[2];
@@ -616,8 +616,15 @@ void init_dm(pty_session* s) {
 void init_mls(pty_session* s) {
   const pty_params& p = s->prm;
   need(s->K == 1, "the MLs core supports one probe mode (probeModes=1)", PTY_ERR_UNSUPPORTED);
+  need(p.precision == 0 || s->N == 256, "precision=1 (tensor-core FFT stages) needs 256 x 256 patterns",
+       PTY_ERR_UNSUPPORTED);
   auto* ml = new MlsState;
   s->ml = ml;
+  if (p.precision) {
+    check_cuda(fft2_tc_prepare(), "tensor-core FFT set-up");
+    ml->tcerr.alloc(sizeof(int), "tensor-core flag");
+    check_cuda(cudaMemsetAsync(ml->tcerr.p, 0, sizeof(int), s->stream), "memset flag");
+  }
   const int N = s->N, P = s->P;
   const size_t NN = size_t(N) * N;
   const double dx_s = sample_pixel_size(p.lambd, p.z, p.dx_d, N);
@@ -753,6 +760,8 @@ MlsBuffers mls_buffers(pty_session* s, int parity) {
   b.delta_p = float(s->prm.delta_p);
   b.beta_obj = 1.0 * 0.9;    // beta_object * beta_LSQ (src/Parameters.h:158-165 defaults)
   b.beta_probe = 1.0 * 0.9;  // beta_probe * beta_LSQ
+  b.tc = s->prm.precision ? 1 : 0;
+  b.tc_err = ml->tcerr.as<int>();
   return b;
 }
 
@@ -812,6 +821,12 @@ double step_mls(pty_session* s, bool want_err) {
   check_cuda(cudaGraphLaunch(tb.graph, s->stream), "MLs graph launch");
   s->launches += mls_launches_per_iteration(ml->ng);
   ++ml->steps;
+  if (s->prm.precision) {  // the tensor-core FFT reports a wait timeout through its device flag
+    int flag = 0;
+    check_cuda(cudaMemcpyAsync(&flag, ml->tcerr.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H flag");
+    check_cuda(cudaStreamSynchronize(s->stream), "MLs iteration");
+    need(flag == 0, "MLs: a tensor-core FFT wait timed out", PTY_ERR_CUDA);
+  }
   if (!(want_err && s->prm.calculateRMS)) return 0.0;
   double e = 0;
   check_cuda(cudaMemcpyAsync(&e, ml->err.p, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "D2H error");
@@ -1190,6 +1205,8 @@ int pty_init(pty_session* s) {
     check_cuda(make_twiddles(s->N, &twp, s->stream), "twiddles");
     s->tw.p = twp;
     s->tw.bytes = sizeof(float2) * s->N;
+    need(s->algo == ALGO_MLS || p.precision == 0,
+         "precision=1 applies to MLs: DM and ePIE fuse their FP32 transforms into their kernels", PTY_ERR_UNSUPPORTED);
     if (s->algo == ALGO_MLS) {
       need(s->warm_params.empty(), "the learned warm start is for ePIE and DM sessions", PTY_ERR_UNSUPPORTED);
       init_mls(s);

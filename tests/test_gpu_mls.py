@@ -62,3 +62,33 @@ def test_mls_flat_start_poisson_data(oracle):
     errs_o = [o.step() for _ in range(6)]
     assert np.isfinite(errs).all() and errs[-1] < errs[0]
     np.testing.assert_allclose(errs, errs_o, rtol=2e-2)
+
+
+def test_mls_tensor_core_fft_precision(oracle):
+    """precision=1: the group FFTs run as split-BF16 tensor-core stages; error vs the FP64 oracle stated beside the
+    FP32 run's (the mixed-precision result is reported with its error, not held to the FP32 bound)."""
+    from ptychopy_b200 import abi
+
+    d = mls_dataset(oracle, N=256, nx=3)
+    runs = {}
+    for prec in (0, 1):
+        runs[prec] = gpu_session(dict(amp=d["intens"], kw=d["kw"]), probe=d["probe"], obj=d["obj"], calculateRMS=1,
+                                 precision=prec)
+    o = oracle.OracleMls(d["raw"], d["intens"], d["probe"], obj=d["obj"])
+    for _ in range(3):
+        for s in runs.values():
+            s.step()
+        o.step()
+    ob, pr, _ = o.state()
+    e32, etc = rel_err(runs[0].object(), ob), rel_err(runs[1].object(), ob)
+    p32, ptc = rel_err(runs[0].probe(), pr), rel_err(runs[1].probe(), pr)
+    print(f"MLs 256^2 after 3 iterations vs FP64: object FP32 {e32:.2e}, split-BF16 TC FFT {etc:.2e}; "
+          f"probe {p32:.2e}, {ptc:.2e}")
+    assert e32 < TOL and p32 < TOL
+    assert etc < 2e-3 and ptc < 2e-3
+    for s in runs.values():
+        s.close()
+    # DM and ePIE fuse their FP32 transforms: precision=1 is refused
+    dd = dataset(N=64, nx=3)
+    with pytest.raises(abi.PtyError):
+        gpu_session(dict(dd, kw=dict(dd["kw"], algorithm="DM")), probe=dd["probe"], precision=1)
