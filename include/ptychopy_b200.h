@@ -133,6 +133,13 @@ int pty_dm_step_local(pty_session* s);
 int pty_dm_increments(pty_session* s, void** dO, size_t* n_obj, void** dP, size_t* n_probe);
 int pty_dm_step_finish(pty_session* s);
 
+/* Autotuner (no counterpart in the reference, which has one launch configuration per kernel).  Before pty_init,
+ * with the patterns (and positions, probe, object) set: times the launch variants of the session's algorithm for
+ * `iters` iterations each on temporary sessions with the same inputs (DM: patterns per wave; ePIE: shared-memory
+ * cluster, cluster or whole-GPU kernel), keeps the fastest for this session, and writes a one-line summary with
+ * every candidate's ms per iteration into `report` (may be NULL).  MLs has no variants. */
+int pty_autotune(pty_session* s, int iters, char* report, int report_len);
+
 /* Learned warm start (no counterpart in the reference, which starts from a constant object, src/Sample.cpp:216-220,
  * or objectNP).  Before pty_init: the parameters (n_params floats, the layout ptychopy_b200/warmstart.py's Net
  * trains: per layer the Cout x Cin x 3 x 3 weights then the Cout biases) of the width-`width` encoder-decoder for the

@@ -34,7 +34,7 @@ EXPORTS = [
     "pty_nn_up2", "pty_nn_up2_bwd", "pty_nn_mse", "pty_nn_adam", "pty_warm_input", "pty_warm_stitch",
     "pty_warm_object", "pty_dm_psi_from_object", "pty_tc_weights_size", "pty_tc_pack_weights", "pty_tc_conv3x3",
     "pty_tc_pool2", "pty_tc_up2", "pty_tc_to_bf16", "pty_tc_first_layer", "pty_tc_last_layer", "pty_set_warm_start",
-    "pty_selftest_bounded_waits", "pty_fft2_tc",
+    "pty_selftest_bounded_waits", "pty_fft2_tc", "pty_autotune",
 ]
 
 
@@ -102,6 +102,7 @@ def lib():
             "pty_set_warm_start": ([vp, vp, ctypes.c_size_t, ctypes.c_int], ctypes.c_int),
             "pty_selftest_bounded_waits": ([vp], ctypes.c_int),
             "pty_fft2_tc": ([vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp], ctypes.c_int),
+            "pty_autotune": ([vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
             "pty_tc_weights_size": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "pty_tc_pack_weights": ([vp, ctypes.c_int, ctypes.c_int, vp, vp], ctypes.c_int),
             "pty_tc_conv3x3": ([vp, vp, vp, vp] + [ctypes.c_int] * 8 + [ctypes.c_float, vp, vp], ctypes.c_int),
@@ -282,6 +283,13 @@ class Session:
             return
         self._warm = np.ascontiguousarray(params, np.float32)
         check(lib().pty_set_warm_start(self.h, _ptr(self._warm), self._warm.size, int(width)))
+
+    def autotune(self, iters=2):
+        """Times the launch variants on temporary sessions and keeps the fastest (pty_autotune, before init);
+        returns the summary line."""
+        buf = ctypes.create_string_buffer(1024)
+        check(lib().pty_autotune(self.h, int(iters), buf, len(buf)))
+        return buf.value.decode()
 
     def psi_from_object(self):
         """DM: exit waves = P * O at every position (pty_dm_psi_from_object), for a given start object."""

@@ -657,11 +657,13 @@ template <> struct EpieShape<128> { static constexpr int R = 8; };
 template <> struct EpieShape<256> { static constexpr int R = 16; };
 template <> struct EpieShape<512> { static constexpr int R = 16; };
 
-// Whole-GPU variant (windows of 512): one pass of R rows per CTA, C = L / R = 128 CTAs in a cooperative launch.
+// Whole-GPU variant: one pass of R rows per CTA, C = L / R CTAs in a cooperative launch (the default at 512; at 256 only
+// when the autotuner asks for it).
 // Measured per 900-position iteration at 512^2: 47 ms against 74 ms for the 16-CTA cluster.  At 256^2 with 5
 // modes (64 CTAs of 4 rows) it measured 245 ms against 239 ms for the cluster: the row split gives both the same
 // 128 warps, and the grid barriers cost more than the cluster's, so 256 keeps the cluster.
 template <int L> struct EpieGridShape { static constexpr int R = 0; };
+template <> struct EpieGridShape<256> { static constexpr int R = 4; };
 template <> struct EpieGridShape<512> { static constexpr int R = 4; };
 
 template <int L, int R>
@@ -736,7 +738,11 @@ static cudaError_t epie_prepare_t(int* C_out) {
   return cudaSuccess;
 }
 
-int epie_grid_prepare(int N) { return N == 512 ? epie_grid_prepare_t<512>() : 0; }
+int epie_grid_prepare(int N, bool any_size) {
+  if (N == 512) return epie_grid_prepare_t<512>();
+  if (N == 256 && any_size) return epie_grid_prepare_t<256>();
+  return 0;
+}
 
 cudaError_t epie_prepare(int N, int* C_out) {
   switch (N) {

@@ -39,8 +39,9 @@ struct EpieArgs {
 
 // Sets kernel attributes and picks the cluster size (largest resident of 16, 8, ...); returns it in C_out.
 cudaError_t epie_prepare(int N, int* C_out);
-// Whole-GPU variant for N = 512: the CTA count if a cooperative launch of it fits on this device, else 0.
-int epie_grid_prepare(int N);
+// Whole-GPU variant (N = 512, and N = 256 when any_size): the CTA count if a cooperative launch of it fits on this
+// device, else 0.
+int epie_grid_prepare(int N, bool any_size = false);
 cudaError_t epie_launch(const EpieArgs& g, cudaStream_t st);
 // Shared-memory-resident variant for small windows with one probe mode (N = 32, 64, 128; K = 1): cluster of
 // N/32 CTAs, probe and window in (distributed) shared memory, natural-layout amplitudes.

@@ -539,11 +539,12 @@ void init_epie(pty_session* s) {
   auto* ep = new EpieState;
   s->ep = ep;
   const size_t NN = size_t(s->N) * s->N, XY = size_t(s->X) * s->Y;
-  ep->sm = epie_uses_smem(s->N, s->K);
+  const int var = s->epie_variant;
+  ep->sm = epie_uses_smem(s->N, s->K) && (var < 0 || var == 0);
   if (ep->sm) {
     check_cuda(epie_sm_prepare(s->N), "ePIE kernel set-up");
   } else {
-    const int Cg = epie_grid_prepare(s->N);
+    const int Cg = (var < 0 || var == 2) ? epie_grid_prepare(s->N, var == 2) : 0;
     if (Cg > 0) {
       ep->grid = true;
       ep->C = Cg;

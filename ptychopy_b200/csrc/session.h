@@ -90,6 +90,7 @@ struct pty_session {
   int probe_given_modes = 0;
   std::vector<float> warm_params;  // trained warm-start network (pty_set_warm_start) or empty
   int warm_width = 0;
+  int epie_variant = -1;  // ePIE kernel: -1 automatic, 0 shared-memory cluster, 1 cluster, 2 whole-GPU (autotuner)
 
   // geometry
   pty::Geometry geo;
