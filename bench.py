@@ -14,7 +14,8 @@ object / probe increments are summed with one NCCL all-reduce per iteration, and
 
 `--algo batch` measures the batched configuration: 16 independent scans of uneven sizes (8 DM, 8 MLs; detectors
 128-512, rasters 10x10-40x40, steps 30-100 nm), `--steps` iterations each, interleaved by pty_batch_run against
-the same scans run one after another.
+the same scans run one after another; each DM scan's wave size is chosen first by the autotuner (pty_autotune,
+reported; `--no-autotune` keeps the defaults).
 
 `--algo mls` measures the MLs core on one scan of the batched configuration's MLs range (256^2, 20x20 raster,
 400 positions, groups of 4), with the FP64 oracle on a bounded sample as the CPU reference.
@@ -70,6 +71,7 @@ def parse():
     ap.add_argument("--e2e-iters", type=int, default=100, help="iterations per public-API call (the config's 100)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="--algo batch: keep the default launch variants")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the ePIE 512^2 and warm-start parts of the headline after the DM line")
     ap.add_argument("--nx", type=int, default=30, help="raster size (30 = the DM configuration; smaller for profiling)")
@@ -996,7 +998,7 @@ def run_batch(args, rank, local):
 
     torch.cuda.set_device(local)
     lambd, z, dx_d = 2.48e-10, 1.0, 172e-6
-    sessions, total_p, keep = [], 0, []
+    sessions, total_p, keep, tuning = [], 0, [], []
     for i, (algo, N, nx, step) in enumerate(BATCH_SCANS):
         rng = np.random.default_rng(20261206 + i)
         dx_s = synth.sample_pixel(lambd, z, dx_d, N)
@@ -1009,6 +1011,10 @@ def run_batch(args, rank, local):
                         beamSize=synth.BEAM_FWHM, probeModes=1, algorithm=algo, delta_p=0.1, PPS=20, device=local)
         s.set_patterns_ptr(amp.data_ptr(), pos.shape[0], N)
         s.set_probe(probe)
+        if not args.no_autotune and algo != "MLs":
+            t0 = time.perf_counter()
+            tuning.append({"scan": f"{algo} {N}^2 {nx}x{nx}", "choice": s.autotune(iters=1),
+                           "seconds": round(time.perf_counter() - t0, 3)})
         s.init()
         keep.append(amp)
         sessions.append(s)
@@ -1038,6 +1044,7 @@ def run_batch(args, rank, local):
            "sequential": {"value": work / t_seq, "unit": UNIT, "seconds": t_seq},
            "batched_seconds": t_batch, "speedup_vs_sequential": t_seq / t_batch, "clocks": ck, "finite": finite,
            "timing": "host wall clock around synchronised regions (includes each scan's host-side scheduling)",
+           "autotune": tuning if tuning else "off (--no-autotune)",
            "note": "MLs runs its core (no position search, sub-pixel shift or variable probe); PPS is accepted and "
                    "has no effect"}
     for s in sessions:
