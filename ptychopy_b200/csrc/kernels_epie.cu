@@ -649,7 +649,8 @@ cudaError_t epie_sm_launch(const EpieArgs& g, cudaStream_t st) {
 
 // Rows per pass of a CTA (blockDim = R * T) for a length-L window; the cluster takes the largest size (<= 16)
 // whose CTAs hold whole passes.  Each position is a chain of short latency-bound phases: at L = 128, 4 CTAs of 8
-// warps (R = 32) measured no faster than 16 CTAs of 2 warps (3.43 vs 3.21 ms per 100-position iteration).
+// warps (R = 32) measured no faster than 16 CTAs of 2 warps (3.43 vs 3.21 ms per 100-position iteration).  At
+// L = 256 with 5 modes (2601 positions): R = 8 / 16 / 32 measured 415 / 237 / 308 ms per iteration.
 template <int L> struct EpieShape;
 template <> struct EpieShape<32> { static constexpr int R = 8; };
 template <> struct EpieShape<64> { static constexpr int R = 4; };

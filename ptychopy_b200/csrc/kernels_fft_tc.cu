@@ -19,6 +19,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <string>
 
@@ -223,22 +224,32 @@ int fail(const std::string& msg, int code) {
   return code;
 }
 
-int g_fft_tc_sms = 0;  // SM count of the device the kernel was prepared on
+constexpr int FT_MAX_DEV = 64;
+std::atomic<int> g_fft_tc_sms[FT_MAX_DEV];  // SM count per device the kernel was prepared on (0: not yet)
+
+int current_sms() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= FT_MAX_DEV) return 0;
+  return g_fft_tc_sms[dev].load();
+}
 
 }  // namespace
 
 cudaError_t fft2_tc_prepare() {
-  cudaError_t e = cudaFuncSetAttribute(k_fft_tc_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, FT_SMEM);
-  int dev = 0;
-  if (e == cudaSuccess) e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&g_fft_tc_sms, cudaDevAttrMultiProcessorCount, dev);
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess && (dev < 0 || dev >= FT_MAX_DEV)) e = cudaErrorInvalidDevice;
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fft_tc_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, FT_SMEM);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) g_fft_tc_sms[dev].store(sms);
   return e;
 }
 
 cudaError_t fft2_tc(float2* data, float2* work, int batch, int N, bool inverse, int* err, cudaStream_t st) {
-  if (N != FT_N || batch < 1 || g_fft_tc_sms == 0) return cudaErrorInvalidValue;
+  const int sms = current_sms();
+  if (N != FT_N || batch < 1 || sms == 0) return cudaErrorInvalidValue;
   const int groups = batch * (FT_N / FT_LINES);
-  const int grid = groups < 4 * g_fft_tc_sms ? groups : 4 * g_fft_tc_sms;  // 4 CTAs per SM (48 KB, 32 TMEM columns)
+  const int grid = groups < 4 * sms ? groups : 4 * sms;  // 4 CTAs per SM (48 KB, 32 TMEM columns)
   const float sign = inverse ? 1.f : -1.f;
   k_fft_tc_pass<<<grid, FT_THREADS, FT_SMEM, st>>>(data, work, groups, sign, err);
   k_fft_tc_pass<<<grid, FT_THREADS, FT_SMEM, st>>>(work, data, groups, sign, err);
@@ -252,7 +263,7 @@ using namespace pty;
 extern "C" int pty_fft2_tc(void* data, void* work, int batch, int N, int inverse, int* err, void* stream) {
   if (!data || !work || !err || batch < 1 || N != FT_N)
     return fail("pty_fft2_tc: bad argument (N must be 256)", PTY_ERR_INVALID);
-  cudaError_t e = g_fft_tc_sms ? cudaSuccess : fft2_tc_prepare();
+  cudaError_t e = current_sms() ? cudaSuccess : fft2_tc_prepare();
   if (e == cudaSuccess)
     e = fft2_tc(static_cast<float2*>(data), static_cast<float2*>(work), batch, N, inverse != 0, err,
                 static_cast<cudaStream_t>(stream));

@@ -16,6 +16,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <string>
 
@@ -569,12 +570,17 @@ int pty_tc_conv3x3(const void* x, const void* wpk, const float* bias, void* y, i
   if (in_mode == 1 && ((H & 1) || (W & 1))) return fail("pty_tc_conv3x3: upsampled input needs even H, W", PTY_ERR_INVALID);
   if (in_mode == 2 && (Cin != 1 || (H & 1) || (W & 1)))
     return fail("pty_tc_conv3x3: amplitude input needs Cin = 1 and even H, W", PTY_ERR_INVALID);
-  static bool attr_set = false;
-  if (!attr_set) {
+  // the kernel's shared-memory limit is a per-device attribute: set it once on every device that launches it
+  constexpr int MAX_DEV = 64;
+  static std::atomic<bool> attr_set[MAX_DEV];
+  int cur = 0;
+  cudaError_t ge = cudaGetDevice(&cur);
+  if (ge != cudaSuccess || cur < 0 || cur >= MAX_DEV) return finish(ge, "pty_tc_conv3x3: device");
+  if (!attr_set[cur].load()) {
     cudaError_t e = cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          TcSmem::total(TC_MAX_N));
     if (e != cudaSuccess) return finish(e, "pty_tc_conv3x3: shared memory attribute");
-    attr_set = true;
+    attr_set[cur].store(true);
   }
   const int Npad = pad16(Cout);
   const int smem = TcSmem::total(Npad);
