@@ -271,6 +271,11 @@ int finish(cudaError_t e, const char* what) {
   return PTY_OK;
 }
 
+int bad(const char* what) {
+  set_last_error(std::string(what) + ": bad argument (null pointer or empty size)");
+  return PTY_ERR_INVALID;
+}
+
 template <int T, bool FLIP>
 void launch_conv(const float* x, const float* w, const float* bias, float* y, int B, int Cin, int Cout, int H, int W,
                  int relu, cudaStream_t st) {
@@ -302,14 +307,15 @@ extern "C" {
 
 int pty_nn_conv3x3(const float* x, const float* w, const float* bias, float* y, int B, int Cin, int Cout, int H, int W,
                    int relu, void* stream) {
-  if (!x || !w || !y || B < 1 || Cin < 1 || Cout < 1 || H < 1 || W < 1 || B > 65535) return PTY_ERR_INVALID;
+  if (!x || !w || !y || B < 1 || Cin < 1 || Cout < 1 || H < 1 || W < 1 || B > 65535) return bad("pty_nn_conv3x3");
   conv<false>(x, w, bias, y, B, Cin, Cout, H, W, relu, static_cast<cudaStream_t>(stream));
   return finish(cudaGetLastError(), "pty_nn_conv3x3");
 }
 
 int pty_nn_conv3x3_bwd(const float* x, const float* w, const float* dy, float* dx, float* dw, float* db, int B,
                        int Cin, int Cout, int H, int W, void* stream) {
-  if (!x || !w || !dy || !dw || B < 1 || Cin < 1 || Cout < 1 || H < 1 || W < 1 || B > 65535) return PTY_ERR_INVALID;
+  if (!x || !w || !dy || !dw || B < 1 || Cin < 1 || Cout < 1 || H < 1 || W < 1 || B > 65535)
+    return bad("pty_nn_conv3x3_bwd");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(dw, 0, sizeof(float) * size_t(Cout) * Cin * 9, st);
   if (e == cudaSuccess && db) e = cudaMemsetAsync(db, 0, sizeof(float) * size_t(Cout), st);
@@ -332,32 +338,38 @@ int pty_nn_conv3x3_bwd(const float* x, const float* w, const float* dy, float* d
 }
 
 int pty_nn_relu(float* a, size_t n, void* stream) {
+  if (!a || n == 0) return bad("pty_nn_relu");
   k_relu<<<grid1(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(a, n);
   return finish(cudaGetLastError(), "pty_nn_relu");
 }
 int pty_nn_relu_bwd(const float* y, float* g, size_t n, void* stream) {
+  if (!y || !g || n == 0) return bad("pty_nn_relu_bwd");
   k_relu_bwd<<<grid1(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(y, g, n);
   return finish(cudaGetLastError(), "pty_nn_relu_bwd");
 }
 int pty_nn_pool2(const float* x, float* y, size_t planes, int H, int W, void* stream) {
+  if (!x || !y || planes == 0 || H < 1 || W < 1) return bad("pty_nn_pool2");
   k_pool2<<<grid1(planes * H * W), 256, 0, static_cast<cudaStream_t>(stream)>>>(x, y, planes, H, W);
   return finish(cudaGetLastError(), "pty_nn_pool2");
 }
 int pty_nn_pool2_bwd(const float* dy, float* dx, size_t planes, int H, int W, void* stream) {
+  if (!dy || !dx || planes == 0 || H < 1 || W < 1) return bad("pty_nn_pool2_bwd");
   k_pool2_bwd<<<grid1(planes * 4 * H * W), 256, 0, static_cast<cudaStream_t>(stream)>>>(dy, dx, planes, H, W);
   return finish(cudaGetLastError(), "pty_nn_pool2_bwd");
 }
 int pty_nn_up2(const float* x, float* y, size_t planes, int H, int W, void* stream) {
+  if (!x || !y || planes == 0 || H < 1 || W < 1) return bad("pty_nn_up2");
   k_up2<<<grid1(planes * 4 * H * W), 256, 0, static_cast<cudaStream_t>(stream)>>>(x, y, planes, H, W);
   return finish(cudaGetLastError(), "pty_nn_up2");
 }
 int pty_nn_up2_bwd(const float* dy, float* dx, size_t planes, int H, int W, void* stream) {
+  if (!dy || !dx || planes == 0 || H < 1 || W < 1) return bad("pty_nn_up2_bwd");
   k_up2_bwd<<<grid1(planes * H * W), 256, 0, static_cast<cudaStream_t>(stream)>>>(dy, dx, planes, H, W);
   return finish(cudaGetLastError(), "pty_nn_up2_bwd");
 }
 int pty_nn_mse(const float* p, const float* t, const float* w, size_t plane, float* g, size_t n, double* loss,
                void* stream) {
-  if (!p || !t || !g || !loss || n == 0 || (w && plane == 0)) return PTY_ERR_INVALID;
+  if (!p || !t || !g || !loss || n == 0 || (w && plane == 0)) return bad("pty_nn_mse");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(loss, 0, sizeof(double), st);
   if (e != cudaSuccess) return finish(e, "pty_nn_mse");
@@ -367,7 +379,7 @@ int pty_nn_mse(const float* p, const float* t, const float* w, size_t plane, flo
 }
 int pty_nn_adam(float* p, const float* g, float* m, float* v, size_t n, float lr, float b1, float b2, float eps,
                 int step, void* stream) {
-  if (step < 1) return PTY_ERR_INVALID;
+  if (!p || !g || !m || !v || n == 0 || step < 1) return bad("pty_nn_adam");
   const float c1 = 1.f - powf(b1, float(step)), c2 = 1.f - powf(b2, float(step));
   k_adam<<<grid1(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(p, g, m, v, n, lr, b1, b2, eps, c1, c2);
   return finish(cudaGetLastError(), "pty_nn_adam");

@@ -651,18 +651,21 @@ int pty_selftest_bounded_waits(int* codes) {
 }
 
 int pty_tc_pool2(const void* x, void* y, int B, int H, int W, int C, void* stream) {
+  if (!x || !y || B < 1 || H < 1 || W < 1 || C < 1) return fail("pty_tc_pool2: bad argument", PTY_ERR_INVALID);
   k_tc_pool2<<<grid1(size_t(B) * H * W * C), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const __nv_bfloat16*>(x), static_cast<__nv_bfloat16*>(y), B, H, W, C);
   return finish(cudaGetLastError(), "pty_tc_pool2");
 }
 
 int pty_tc_up2(const void* x, void* y, int B, int H, int W, int C, void* stream) {
+  if (!x || !y || B < 1 || H < 1 || W < 1 || C < 1) return fail("pty_tc_up2: bad argument", PTY_ERR_INVALID);
   k_tc_up2<<<grid1(size_t(B) * 4 * H * W * C), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const __nv_bfloat16*>(x), static_cast<__nv_bfloat16*>(y), B, H, W, C);
   return finish(cudaGetLastError(), "pty_tc_up2");
 }
 
 int pty_tc_to_bf16(const float* x, void* y, size_t n, void* stream) {
+  if (!x || !y || n == 0) return fail("pty_tc_to_bf16: bad argument", PTY_ERR_INVALID);
   k_to_bf16<<<grid1(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(x, static_cast<__nv_bfloat16*>(y), n);
   return finish(cudaGetLastError(), "pty_tc_to_bf16");
 }

@@ -56,3 +56,25 @@ def test_kernel_symbols_exported():
     for name in ["pty_nn_conv3x3", "pty_nn_conv3x3_bwd", "pty_nn_relu", "pty_nn_relu_bwd", "pty_nn_pool2",
                  "pty_nn_pool2_bwd", "pty_nn_up2", "pty_nn_up2_bwd", "pty_nn_mse", "pty_nn_adam"]:
         assert hasattr(L, name)
+
+
+def test_kernel_entry_points_reject_bad_arguments():
+    """Null pointers and empty sizes are refused before any launch (no GPU needed)."""
+    import ctypes
+
+    from ptychopy_b200 import abi
+
+    L = abi.lib()
+    assert L.pty_nn_relu(None, 10, None) == abi.PTY_ERR_INVALID
+    assert L.pty_nn_pool2(None, None, 1, 2, 2, None) == abi.PTY_ERR_INVALID
+    assert L.pty_nn_conv3x3(None, None, None, None, 1, 1, 1, 4, 4, 0, None) == abi.PTY_ERR_INVALID
+    assert L.pty_nn_adam(None, None, None, None, 0, 1e-3, 0.9, 0.999, 1e-8, 1, None) == abi.PTY_ERR_INVALID
+    assert L.pty_tc_conv3x3(None, None, None, None, 1, 16, 16, 8, 8, 0, 0, 0, 1.0, None, None) == abi.PTY_ERR_INVALID
+    assert L.pty_tc_pool2(None, None, 1, 2, 2, 8, None) == abi.PTY_ERR_INVALID
+    assert L.pty_tc_weights_size(16, 300) == -1  # Cout above 256
+    assert L.pty_warm_stitch(None, None, 0, None, 32, 128, 0.9, 0.1, 0.2, None, 10, 10, None) == abi.PTY_ERR_INVALID
+    assert L.pty_fft2_tc(None, None, 1, 128, 0, None, None) == abi.PTY_ERR_INVALID
+    assert b"bad argument" in L.pty_last_error()
+    codes = (ctypes.c_int * 4)()
+    assert L.pty_selftest_bounded_waits(None) == abi.PTY_ERR_INVALID
+    del codes
