@@ -801,6 +801,28 @@ def run_warm(args, rank, local, emit=True):
                "call": "ptychopy.epienp(iter=plain iterations) vs ptychopy.epienpinit(warmStart=...) + epieresobj, "
                        "host arrays, session set-up included"}
     clk = clocks.stop()
+    if plain and not args.no_cpu:
+        # the reference's method on the host: the oracle's FP32 ePIE port over a bounded sample of the positions,
+        # scaled to the positions x iterations the plain GPU arm needed to reach the target
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+
+        amp_np = amp.cpu().numpy()
+        n = min(P, 16)
+        for _ in range(2):
+            o = pyoracle.OracleSession("ePIE", amp_np[:n], pos[:n], np.zeros((X, Y)), probe[None],
+                                       probe_guess_path=False, modes_given=False, nthreads=1, fp32=True)
+            t0 = time.perf_counter()
+            o.step()
+            t = time.perf_counter() - t0
+            if t > 10.0 or n == P:
+                break
+            n = int(min(P, max(n, 15.0 * n / max(t, 1e-9))))
+        cpu_ms = t / n * P * plain["iterations"] * 1e3
+        out["cpu_baseline"] = {"value": round(cpu_ms, 1), "unit": "ms", "cores": 1, "kind": "port",
+                               "sample": f"iteration 1 of ePIE over {n} of the {P} positions (FP32 C++ port), "
+                                         f"scaled to {P} positions x the {plain['iterations']} iterations plain "
+                                         "ePIE needs to reach the target"}
     out.update({
         "e2e": e2e,
         "value": warm["gpu_ms"] if warm else None,

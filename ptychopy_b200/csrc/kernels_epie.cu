@@ -659,7 +659,8 @@ template <> struct EpieShape<256> { static constexpr int R = 16; };
 template <> struct EpieShape<512> { static constexpr int R = 16; };
 
 // Whole-GPU variant: one pass of R rows per CTA, C = L / R CTAs in a cooperative launch (the default at 512; at 256 only
-// when the autotuner asks for it).
+// when the autotuner asks for it).  At 512 (900 positions, 1 mode) R = 2 / 4 / 8 measured 50.6 / 47.4 / 47.0 ms per
+// iteration: the phases' latency chains, not the CTA count, bound it.
 // Measured per 900-position iteration at 512^2: 47 ms against 74 ms for the 16-CTA cluster.  At 256^2 with 5
 // modes (64 CTAs of 4 rows) it measured 245 ms against 239 ms for the cluster: the row split gives both the same
 // 128 warps, and the grid barriers cost more than the cluster's, so 256 keeps the cluster.
