@@ -17,8 +17,10 @@ object / probe increments are summed with one NCCL all-reduce per iteration, and
 the same scans run one after another; each DM scan's wave size is chosen first by the autotuner (pty_autotune,
 reported; `--no-autotune` keeps the defaults).
 
-`--algo mls` measures the MLs core on one scan of the batched configuration's MLs range (256^2, 20x20 raster,
-400 positions, groups of 4), with the FP64 oracle on a bounded sample as the CPU reference.
+`--algo mls` measures MLs on one scan of the batched configuration's MLs range (256^2, 20x20 raster, 400 positions,
+groups of 4): the reference's default path with every part active (variable probe and intensity, sub-pixel probe
+shift, position search), the fixed-probe core beside it, and the FP64 oracle on a bounded sample as the CPU
+reference.
 
 `--algo nrmse` measures the plain half of the warm-start comparison: ePIE from a flat (zero) object on the
 warm-start workload (64x64 raster at 128^2, 1e5 photons/pattern), iterations and GPU time until the phase NRMSE
@@ -518,7 +520,9 @@ def run_epie(args, rank, local, emit=True):
 
 
 def run_mls(args, rank, local):
-    """MLs core throughput on a 256^2, 20x20 scan (device-timed iterations), FP64 oracle sample as CPU reference."""
+    """MLs throughput on a 256^2, 20x20 scan (device-timed iterations): the reference's default path (variable probe
+    and intensity, sub-pixel probe shift, position search) with every part active, the fixed-probe core beside it;
+    the FP64 oracle's default path on a sample as CPU reference."""
     if rank != 0:
         return
     import numpy as np
@@ -537,34 +541,46 @@ def run_mls(args, rank, local):
     intens = synth.make_patterns_torch(obj, probe, pos, N, 1e6, seed=20261208, device="cuda", intensities=True)
     P = pos.shape[0]
     stream = torch.cuda.Stream()
-    s = abi.Session(size=N, scanDimsx=nx, scanDimsy=nx, stepx=step, stepy=step, lambd=lambd, z=z, dx_d=dx_d,
-                    beamSize=synth.BEAM_FWHM, probeModes=1, algorithm="MLs", delta_p=0.1, device=local)
-    s.set_stream(stream.cuda_stream)
-    s.set_patterns_ptr(intens.data_ptr(), P, N)
-    s.set_probe(probe)
-    s.init()
-    for _ in range(max(args.warmup, 3)):
-        s.run(1)
-    torch.cuda.synchronize()
-    clocks = Clocks(local)
-    l0 = s.launches()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clocks.start()
-    with torch.cuda.stream(stream):
-        e0.record(stream)
-        s.run(args.steps)
-        e1.record(stream)
-    stream.synchronize()
-    ck = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    launches = s.launches() - l0
-    finite = bool(np.isfinite(s.object()).all())
-    s.close()
+    pps = 3  # position search from iteration 3: with >= 3 warm-up iterations every timed one runs all parts
+
+    def timed(core):
+        s = abi.Session(size=N, scanDimsx=nx, scanDimsy=nx, stepx=step, stepy=step, lambd=lambd, z=z, dx_d=dx_d,
+                        beamSize=synth.BEAM_FWHM, probeModes=1, algorithm="MLs", delta_p=0.1, device=local,
+                        mlsCore=core, PPS=pps)
+        s.set_stream(stream.cuda_stream)
+        s.set_patterns_ptr(intens.data_ptr(), P, N)
+        s.set_probe(probe)
+        s.init()
+        for _ in range(max(args.warmup, 3)):
+            s.run(1)
+        torch.cuda.synchronize()
+        clocks = Clocks(local)
+        l0 = s.launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clocks.start()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            s.run(args.steps)
+            e1.record(stream)
+        stream.synchronize()
+        ck = clocks.stop()
+        ms = e0.elapsed_time(e1)
+        launches = s.launches() - l0
+        finite = bool(np.isfinite(s.object()).all())
+        s.close()
+        return ms, launches, ck, finite
+
+    ms, launches, ck, finite = timed(0)
+    ms_core, _, _, _ = timed(1)
+    G = max(1, P // 100)
     out = {"metric": "MLs patterns/s", "value": P * args.steps / (ms / 1000.0), "unit": UNIT, "n_gpus": 1,
            "steps": args.steps, "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "f32",
            "data": "synthetic (seeded)",
-           "config": {"workload": f"MLs core, {N}^2, {nx}x{nx} raster ({P} positions, groups of {max(1, P // 100)}), "
-                                  f"delta_p 0.1", "N": N, "positions": P},
+           "config": {"workload": f"MLs, the reference's default path (variable probe and intensity, sub-pixel probe "
+                                  f"shift, position search from iteration {pps}), {N}^2, {nx}x{nx} raster ({P} "
+                                  f"positions, groups of {G}), delta_p 0.1", "N": N, "positions": P},
+           "core": {"value": P * args.steps / (ms_core / 1000.0), "ms_per_step": ms_core / args.steps,
+                    "path": "fixed-probe core (mlsCore=1)"},
            "gpu_launches": int(launches), "clocks": ck, "finite": finite,
            "timing": "CUDA events around pty_run (the host builds each iteration's group tables while the GPU runs)"}
     if not args.no_cpu:
@@ -574,12 +590,13 @@ def run_mls(args, rank, local):
         raw = pyoracle.mls_raw_positions(nx, nx, step, step, dx_s)
         n = 16
         sub = intens[:n].cpu().numpy().astype(np.float64)
-        o = pyoracle.OracleMls(raw[:n], sub, probe[0])
+        o = pyoracle.OracleMls(raw[:n], sub, probe[0], variable=1, PPS=1)
         t0 = time.perf_counter()
         o.step()
         t = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": n / t, "unit": UNIT, "cores": 1, "kind": "port",
-                               "sample": f"1 MLs iteration of the FP64 oracle over {n} of the {P} positions"}
+                               "sample": f"1 MLs iteration of the FP64 oracle's default path (position search on) "
+                                         f"over {n} of the {P} positions"}
     print(json.dumps(out), flush=True)
 
 
@@ -1067,8 +1084,9 @@ def run_batch(args, rank, local):
            "batched_seconds": t_batch, "speedup_vs_sequential": t_seq / t_batch, "clocks": ck, "finite": finite,
            "timing": "host wall clock around synchronised regions (includes each scan's host-side scheduling)",
            "autotune": tuning if tuning else "off (--no-autotune)",
-           "note": "MLs runs its core (no position search, sub-pixel shift or variable probe); PPS is accepted and "
-                   "has no effect"}
+           "note": "MLs runs the reference's default path: variable probe and intensity, sub-pixel probe shift, "
+                   "position search from iteration PPS = 20 (the first 2 of the timed iterations run without it at "
+                   "--steps 50 after 2 warm-up ones: iterations 3-19 do not search, 20-52 do)"}
     for s in sessions:
         s.close()
     print(json.dumps(out), flush=True)

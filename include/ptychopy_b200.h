@@ -69,6 +69,10 @@ typedef struct pty_params {
   int precision;          /* FFT arithmetic: 0 FP32 (default); 1 split-BF16 tensor-core stages (pty_fft2_tc) where a
                              session's transforms are separate batched FFTs: MLs at N = 256.  DM and ePIE fuse their
                              FP32 transforms into their kernels and refuse 1 (PTY_ERR_UNSUPPORTED). */
+  int mlsCore;            /* MLs: 0 (default) the reference's path, which its Python API always runs
+                             (src/Parameters.h:162-163: variable probe with one extra mode, variable intensity,
+                             sub-pixel probe shift, position search from iteration PPS); 1 the fixed-probe core
+                             without them */
 } pty_params;
 
 typedef struct pty_session pty_session;
@@ -254,8 +258,14 @@ int pty_get_object(pty_session* s, float* c64_out, int X, int Y);
 /* Copy the probe stack (K x N x N complex64).  Replaces epieresprobe / mlsresprobe (src/ptychopy.c:978-990). */
 int pty_get_probe(pty_session* s, float* c64_out, int K, int N);
 
-/* Scan positions in pixels after the -min shift, P x 2 float32 (IPtychoScanMesh::getScanPositions). */
+/* Scan positions in pixels after the -min shift, P x 2 float32 (IPtychoScanMesh::getScanPositions).  MLs keeps
+ * the ML mesh's centred positions; on its default path these are the current, refined positions (m_positions). */
 int pty_get_positions(const pty_session* s, float* xy_px, int P);
+
+/* MLs default path: the extra (variable) probe mode E (N x N complex64) and the probe evolution weights evo0
+ * (intensity) and evo1 (extra mode), P doubles each (Probe::m_extramodes, m_probe_evolution).  Any pointer may be
+ * NULL.  PTY_ERR_STATE for other algorithms and for mlsCore = 1. */
+int pty_get_mls_state(const pty_session* s, float* E_c64, double* evo0, double* evo1, int N, int P);
 
 /* Write `<dir>/<jobID>_probes_<r>.{csv|bin}` and `<dir>/<jobID>_object_<r>.{csv|bin}`.  Replaces
  * IPhaser::writeResultsToDisk (src/IPhaser.cpp:417-428) with the CSV format of Cuda2DArray::save

@@ -496,9 +496,10 @@ template <typename R> void store_state(const State<R>& s, double* obj, double* p
   }
 }
 
-// ---------------------------------------------------------------- MLs core (src/MLS.cpp:74-490)
-// LSQ-ML with random groups, restated for one probe mode and one object, no variable probe, no sub-pixel shift,
-// no position search.  Geometry (ML mesh, src/CartesianScanMesh.cpp:94-177, src/IPtychoScanMesh.cpp:123-184):
+// ---------------------------------------------------------------- MLs (src/MLS.cpp:74-490)
+// LSQ-ML with random groups for one probe mode and one object.  Two paths: the reference's defaults
+// (src/Parameters.h:162-163: variable probe with one extra mode, variable intensity, sub-pixel probe shift,
+// position search from iteration PPS), and the fixed-probe core (none of these).  Geometry (ML mesh, src/CartesianScanMesh.cpp:94-177, src/IPtychoScanMesh.cpp:123-184):
 // raw centred positions, object Np_o_new = ceil(extent * 1.2), window starts round(pos + ceilvar) - 1.
 struct MlsGeometry {
   int X = 0, Y = 0;
@@ -576,7 +577,68 @@ template <typename R> struct MlsState {
   std::vector<R> pobj;        // illumination weights (p_object), X*Y
   R maxIllum = 0;             // Probe::MAX_ILLUM from the set-up (src/Probe.cpp:507-613)
   double delta_p = 0.1, beta_LSQ = 0.9, beta_object = 1, beta_probe = 1;
+  // the reference-default path
+  bool variable = false;
+  int PPS = 1 << 30;          // first iteration of the position search (probe_pos_search)
+  int iter = 0;               // iterations done
+  std::vector<cx<R>> E;       // extra probe mode (m_extramodes)
+  std::vector<double> evo0, evo1;       // probe evolution: intensity and variable-mode weights per position
+  std::vector<float> pos, pos_o, sub;   // 2*P: positions (x = rows), the originals, sub-pixel shifts (x = columns)
 };
+
+// Window starts and sub-pixel shifts from the positions (find_reconstruction_ROI, src/IPtychoScanMesh.cpp:122-171):
+// position + ceil(Np_o/2 - N/2) in FP32, rounded; the start is one below; the shift's x is the column remainder.
+// A start that would leave the object is clamped into it (the reference reads outside the array there).
+template <typename R> void mls_windows(MlsState<R>& s) {
+  const int N = s.N;
+  const float cvx = std::ceil(float(s.geo.X) * 1.0f / 2 - float(N) * 1.0f / 2);
+  const float cvy = std::ceil(float(s.geo.Y) * 1.0f / 2 - float(N) * 1.0f / 2);
+  for (int i = 0; i < s.P; ++i) {
+    const float p1 = s.pos[2 * i] + cvx, p2 = s.pos[2 * i + 1] + cvy;
+    const float t1 = std::round(p1), t2 = std::round(p2);
+    s.sub[2 * i] = p2 - t2;
+    s.sub[2 * i + 1] = p1 - t1;
+    s.geo.r0[i] = std::min(std::max(int(t1) - 1, 0), s.geo.X - N);
+    s.geo.c0[i] = std::min(std::max(int(t2) - 1, 0), s.geo.Y - N);
+  }
+}
+
+// Seeded stand-ins for the reference's time-seeded draws: curand uniforms for the extra mode (initVarModes,
+// src/Probe.cpp:497-505 with d_initVarMOdes, src/ProbeKernels.cu:99-110: r1 e^{2 pi i r2}, all r1 drawn before all
+// r2) and normalRandom for the variable-mode weights (1e-6 N(0,1), src/Probe.cpp:520-525).  SplitMix64 from
+// seed ^ 0x3C6EF372FE94F82B, u = (bits >> 11 + 0.5) 2^-53, Box-Muller cos branch, one normal per pair.
+void mls_variable_draws(uint64_t seed, int N, int P, std::vector<cx<double>>& E, std::vector<double>& evo1) {
+  uint64_t st = seed ^ 0x3C6EF372FE94F82Bull;
+  auto u = [&] { return (double(splitmix64(st) >> 11) + 0.5) * (1.0 / 9007199254740992.0); };
+  const size_t NN = size_t(N) * N;
+  std::vector<double> r1(NN), r2(NN);
+  for (auto& v : r1) v = u();
+  for (auto& v : r2) v = u();
+  E.resize(NN);
+  for (size_t i = 0; i < NN; ++i) E[i] = cx<double>(r1[i] * std::cos(2 * M_PI * r2[i]), r1[i] * std::sin(2 * M_PI * r2[i]));
+  evo1.resize(P);
+  for (auto& v : evo1) {
+    const double a = u(), b = u();
+    v = 1e-6 * (std::sqrt(-2.0 * std::log(a)) * std::cos(2 * M_PI * b));
+  }
+}
+
+// FFT frequency grid of the sub-pixel shift and the position gradient: fftshift(k/N - 0.5) (src/Probe.cpp:92-121),
+// i.e. k/N for k < N/2 and k/N - 1 above.
+inline double fft_freq(int k, int N) { return k < N / 2 ? double(k) / N : double(k) / N - 1.0; }
+
+// a <- IFFT2(FFT2(a) e^{-2 pi i (sx f[c] + sy f[r])}) / N^2 (shift_probe, src/Probe.cpp:1261-1337)
+template <typename R>
+void mls_shift(const Fft1<R>& f, cx<R>* a, double sx, double sy, std::vector<cx<R>>& scr) {
+  const int N = f.L;
+  fft2(f, a, false, scr);
+  for (int r = 0; r < N; ++r)
+    for (int c = 0; c < N; ++c) {
+      const double ph = -2.0 * M_PI * (sx * fft_freq(c, N) + sy * fft_freq(r, N));
+      a[size_t(r) * N + c] *= cx<R>(R(std::cos(ph) / (double(N) * N)), R(std::sin(ph) / (double(N) * N)));
+    }
+  fft2(f, a, true, scr);
+}
 
 // p_object = sum_j |P|^2 placed at the windows (set_projections of aprobe2, src/Probe.cpp:701-729)
 template <typename R> void mls_illumination(MlsState<R>& s, std::vector<R>& out) {
@@ -592,6 +654,14 @@ template <typename R> void mls_illumination(MlsState<R>& s, std::vector<R>& out)
 template <typename R> void mls_setup(MlsState<R>& s, const std::vector<double>& intensitySums) {
   const int N = s.N;
   const size_t NN = size_t(N) * N;
+  if (s.variable) {  // evolution weights; extra mode to unit RMS, its weights carry the norm (src/Probe.cpp:511-560)
+    s.evo0.assign(s.P, 1.0);
+    double se = 0;
+    for (const auto& v : s.E) se += double(std::norm(v));
+    const double rE = std::sqrt(se / double(NN));
+    for (auto& v : s.E) v *= R(1.0 / rE);
+    for (auto& v : s.evo1) v *= rE;
+  }
   std::vector<R> illum;
   mls_illumination(s, illum);
   double si = 0, soi = 0;
@@ -611,6 +681,7 @@ template <typename R> void mls_setup(MlsState<R>& s, const std::vector<double>& 
   double corr = (n % 2) ? corrv[n / 2] : 0.5 * (corrv[n / 2 - 1] + corrv[n / 2]);
   corr = std::sqrt(corr * double(NN));
   for (auto& v : s.Pr) v *= R(1.0 / corr);
+  for (auto& v : s.E) v *= R(1.0 / corr);
   s.pobj = illum;
   for (auto& v : s.pobj) v /= R(corr * corr);
   s.maxIllum = *std::max_element(s.pobj.begin(), s.pobj.end());
@@ -619,6 +690,9 @@ template <typename R> void mls_setup(MlsState<R>& s, const std::vector<double>& 
 template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool want_err) {
   const int N = s.N, X = s.geo.X, Y = s.geo.Y;
   const size_t NN = size_t(N) * N, XY = size_t(X) * Y;
+  const int iter = ++s.iter;  // 1-based, as MLS::iteration's iter
+  const bool var = s.variable;
+  if (var && (iter == 1 || iter >= s.PPS)) mls_windows(s);  // find_reconstruction_ROI_O (src/MLS.cpp:86-89)
   // calc_object_norm (src/Probe.cpp:671-699): ||W o O|| / ||W|| over the object ROI, W = p_object
   {
     double sw = 0, swo = 0;
@@ -631,7 +705,40 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
       }
     const R on = sw > 0 ? R(std::sqrt(swo) / std::sqrt(sw)) : R(1);  // empty / unlit ROI: no rescale
     for (auto& v : s.Pr) v *= on;
+    for (auto& v : s.E) v *= on;
     for (auto& v : s.O) v *= R(1) / on;
+  }
+  if (var) {
+    // updateScanPositionsDiff (src/IPtychoScanMesh.cpp:340-368): remove the mean drift from the originals
+    double s1x = 0, s1y = 0, s2x = 0, s2y = 0;
+    for (int i = 0; i < s.P; ++i) {
+      s1x += s.pos[2 * i]; s1y += s.pos[2 * i + 1];
+      s2x += s.pos_o[2 * i]; s2y += s.pos_o[2 * i + 1];
+    }
+    const float dx = float(s1x / s.P) - float(s2x / s.P), dy = float(s1y / s.P) - float(s2y / s.P);
+    for (int i = 0; i < s.P; ++i) { s.pos[2 * i] -= dx; s.pos[2 * i + 1] -= dy; }
+  }
+  if (var && iter > 1) {
+    // remove_extra_degree (src/Probe.cpp:615-669).  Its mean and norm loops run over m_probe_evolution.size() = 2
+    // entries (the number of evolution vectors), so only positions 0 and 1 are re-centred; kept as written.
+    double se = 0;
+    for (const auto& v : s.E) se += double(std::norm(v));
+    const double vn = std::sqrt(se / double(NN));
+    for (auto& v : s.E) v *= R(1.0 / vn);
+    for (auto& v : s.evo1) v *= vn;
+    const int len = std::min(2, s.P);
+    double a0 = 0, a1 = 0;
+    for (int i = 0; i < len; ++i) { a0 += s.evo0[i]; a1 += s.evo1[i]; }
+    const float m0 = float(a0 / len), m1 = float(a1 / len);
+    double sq = 0;
+    for (int i = 0; i < len; ++i) {
+      s.evo0[i] = (s.evo0[i] - m0) * 0.99 + 1;
+      s.evo1[i] = s.evo1[i] - m1;
+      sq += s.evo0[i] * s.evo0[i];
+    }
+    const double cn = std::sqrt(sq / len);
+    for (int i = 0; i < len; ++i) s.evo0[i] /= cn;
+    for (auto& v : s.Pr) v *= R(cn);
   }
   // updated_cached_illumination: h_set_projections adds sum |P|^2 at the windows to p_object without clearing it,
   // then /2, so p_object is a running average (MAX_ILLUM keeps its set-up value)
@@ -640,6 +747,7 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
     mls_illumination(s, il);
     for (size_t i = 0; i < XY; ++i) s.pobj[i] = (s.pobj[i] + il[i]) / R(2);
   }
+  const R pmax = *std::max_element(s.pobj.begin(), s.pobj.end());  // update_variable_probe's weight scale
   std::vector<std::vector<int>> groups;
   mls_groups(rng, s.P, groups);
   Fft1<R> f(N);
@@ -650,14 +758,19 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
   std::vector<cx<R>> S(XY), pum(NN);
   for (const auto& g : groups) {
     const int G = int(g.size());
-    std::vector<std::vector<cx<R>>> op(G, std::vector<cx<R>>(NN)), chi(G, std::vector<cx<R>>(NN));
+    std::vector<std::vector<cx<R>>> op(G, std::vector<cx<R>>(NN)), chi(G, std::vector<cx<R>>(NN)),
+        vp(G, std::vector<cx<R>>(NN)), pu(G, std::vector<cx<R>>(NN));
     for (int k = 0; k < G; ++k) {
       const int j = g[k];
+      // get_illumination_probe (src/Probe.cpp:887-954): the position's probe P evo0 + E evo1, sub-pixel shifted
+      for (size_t p = 0; p < NN; ++p)
+        vp[k][p] = var ? s.Pr[p] * R(s.evo0[j]) + s.E[p] * R(s.evo1[j]) : s.Pr[p];
+      if (var) mls_shift(f, vp[k].data(), s.sub[2 * j], s.sub[2 * j + 1], scr);
       for (int x = 0; x < N; ++x)
         for (int y = 0; y < N; ++y) {
           const size_t p = size_t(x) * N + y;
           op[k][p] = s.O[size_t(s.geo.r0[j] + x) * Y + (s.geo.c0[j] + y)];
-          chi[k][p] = s.Pr[p] * op[k][p];  // get_illumination_probe: psi = P * obj_proj
+          chi[k][p] = vp[k][p] * op[k][p];
         }
       fft2(f, chi[k].data(), false, scr);
       const R* A = &s.A[size_t(j) * NN];
@@ -670,8 +783,11 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
       errsum += std::sqrt(e / double(NN));
       fft2(f, chi[k].data(), true, scr);
       for (auto& v : chi[k]) v *= nrm;
+      // probe direction of this window, shifted back by the sub-pixel remainder (src/MLS.cpp:232-240)
+      for (size_t p = 0; p < NN; ++p) pu[k][p] = chi[k][p] * std::conj(op[k][p]);
+      if (var) mls_shift(f, pu[k].data(), -double(s.sub[2 * j]), -double(s.sub[2 * j + 1]), scr);
     }
-    // probe direction: mean_j W[window] * chi conj(obj_proj), W = p/(p + 0.01 MAX_ILLUM) (src/MLS.cpp:249-285)
+    // probe direction: mean_j W[window] * pu_j, W = p/(p + 0.01 MAX_ILLUM) (src/MLS.cpp:249-285)
     std::fill(pum.begin(), pum.end(), cx<R>(0, 0));
     for (int k = 0; k < G; ++k) {
       const int j = g[k];
@@ -679,18 +795,18 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
         for (int y = 0; y < N; ++y) {
           const size_t p = size_t(x) * N + y;
           const R w0 = s.pobj[size_t(s.geo.r0[j] + x) * Y + (s.geo.c0[j] + y)];
-          pum[p] += chi[k][p] * std::conj(op[k][p]) * (w0 / (w0 + s.maxIllum * R(0.01)));
+          pum[p] += pu[k][p] * (w0 / (w0 + s.maxIllum * R(0.01)));
         }
     }
     for (auto& v : pum) v *= R(1.0 / G);
-    // object direction: set_projections of chi conj(P), preconditioned by p + delta_p MAX_ILLUM (src/MLS.cpp:287-347)
+    // object direction: set_projections of chi conj(vp), preconditioned by p + delta_p MAX_ILLUM (src/MLS.cpp:287-347)
     std::fill(S.begin(), S.end(), cx<R>(0, 0));
     for (int k = 0; k < G; ++k) {
       const int j = g[k];
       for (int x = 0; x < N; ++x)
         for (int y = 0; y < N; ++y) {
           const size_t p = size_t(x) * N + y;
-          S[size_t(s.geo.r0[j] + x) * Y + (s.geo.c0[j] + y)] += chi[k][p] * std::conj(s.Pr[p]);
+          S[size_t(s.geo.r0[j] + x) * Y + (s.geo.c0[j] + y)] += chi[k][p] * std::conj(vp[k][p]);
         }
     }
     const R dmax = R(s.maxIllum * s.delta_p);
@@ -705,7 +821,7 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
         for (int y = 0; y < N; ++y) {
           const size_t p = size_t(x) * N + y, o = size_t(s.geo.r0[j] + x) * Y + (s.geo.c0[j] + y);
           const cx<R> oup = S[o] / (s.pobj[o] + dmax);
-          const cx<R> dOP = oup * s.Pr[p], dPO = pum[p] * op[k][p];
+          const cx<R> dOP = oup * vp[k][p], dPO = pum[p] * op[k][p];
           s1 += double(std::norm(dOP) + lam);
           s4 += double(std::norm(dPO) + lam);
           s2 += cx<double>(dOP * std::conj(dPO));
@@ -733,6 +849,89 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
     for (size_t i = 0; i < XY; ++i)
       if (S[i] != cx<R>(0, 0)) s.O[i] += bor * (S[i] / (s.pobj[i] + dmax));
     for (size_t p = 0; p < NN; ++p) s.Pr[p] += bpr * pum[p];
+    if (!var) continue;
+    if (iter >= s.PPS) {
+      // gradient_position_solver (src/Probe.cpp:956-1118): object gradients by the Fourier derivative, a least-
+      // squares shift per window clamped to 0.2 px.  The column-direction gradient (dX, the column frequency grid)
+      // moves the position's x (the row coordinate) and the row-direction one its y, as the reference pairs them.
+      for (int k = 0; k < G; ++k) {
+        const int j = g[k];
+        std::vector<cx<R>> img(op[k]), dX(NN), dY(NN);
+        fft2(f, img.data(), false, scr);
+        for (int r = 0; r < N; ++r)
+          for (int c = 0; c < N; ++c) {
+            const size_t p = size_t(r) * N + c;
+            const cx<R> d = img[p] * cx<R>(0, R(2.0 * M_PI));
+            dX[p] = d * R(fft_freq(c, N));
+            dY[p] = d * R(fft_freq(r, N));
+          }
+        fft2(f, dX.data(), true, scr);
+        fft2(f, dY.data(), true, scr);
+        double nx = 0, dnx = 0, ny = 0, dny = 0;
+        for (size_t p = 0; p < NN; ++p) {
+          const cx<R> gx = dX[p] * nrm * vp[k][p], gy = dY[p] * nrm * vp[k][p];
+          dnx += double(std::norm(gx));
+          nx += double((chi[k][p] * std::conj(gx)).real());
+          dny += double(std::norm(gy));
+          ny += double((chi[k][p] * std::conj(gy)).real());
+        }
+        const double ddx = nx / dnx, ddy = ny / dny;
+        const double shx = std::min(std::abs(ddx), 0.2) * double((0.0 < ddx) - (ddx < 0.0));
+        const double shy = std::min(std::abs(ddy), 0.2) * double((0.0 < ddy) - (ddy < 0.0));
+        s.pos[2 * j] = float(s.pos[2 * j] + shx);
+        s.pos[2 * j + 1] = float(s.pos[2 * j + 1] + shy);
+      }
+    }
+    if (iter > 2) {
+      // update_variable_probe (src/Probe.cpp:1366-1516): one SVD-like step of the extra mode on the weighted
+      // residual of the probe directions, then the variable-mode and intensity weights of the group's positions
+      const double relaxU = double(G) / s.P;
+      std::vector<double> ev(G);
+      double evn = 0;
+      for (int k = 0; k < G; ++k) { ev[k] = s.evo1[g[k]]; evn += ev[k] * ev[k]; }
+      std::vector<cx<R>> upd(NN, cx<R>(0, 0));
+      for (int k = 0; k < G; ++k) {
+        const int j = g[k];
+        std::vector<cx<R>> res(NN);
+        double pr = 0;
+        for (int x = 0; x < N; ++x)
+          for (int y = 0; y < N; ++y) {
+            const size_t p = size_t(x) * N + y;
+            const R w = s.pobj[size_t(s.geo.r0[j] + x) * Y + (s.geo.c0[j] + y)] / pmax;
+            res[p] = (pu[k][p] - pum[p]) * w;
+            pr += (double((s.E[p] * std::conj(res[p])).real()) + ev[k]) / evn;
+          }
+        pr /= double(NN);
+        for (size_t p = 0; p < NN; ++p) upd[p] += res[p] * R(pr);
+      }
+      double su = 0;
+      for (auto& v : upd) { v *= nrm; su += double(std::norm(v)); }
+      const double un = std::sqrt(su / double(NN));
+      const R us = R(relaxU / std::max(1.0, un));
+      double se = 0;
+      for (size_t p = 0; p < NN; ++p) { s.E[p] += upd[p] * us; se += double(std::norm(s.E[p])); }
+      const R en = R(1.0 / std::sqrt(se / double(NN)));
+      for (auto& v : s.E) v *= en;
+      std::vector<double> den(G), num(G), dI(G), nI(G);
+      double dsum = 0;
+      for (int k = 0; k < G; ++k) {
+        double a = 0, b = 0, c = 0, d = 0;
+        for (size_t p = 0; p < NN; ++p) {
+          const cx<R> v = op[k][p] * s.E[p], w = op[k][p] * s.Pr[p];
+          a += double(std::norm(v));
+          b += double((chi[k][p] * std::conj(v)).real());
+          c += double(std::norm(w));
+          d += double((chi[k][p] * std::conj(w)).real());
+        }
+        den[k] = a / double(NN); num[k] = b / double(NN); dI[k] = c; nI[k] = d;
+        dsum += den[k];
+      }
+      const double dmean = dsum / G;
+      for (int k = 0; k < G; ++k) {
+        s.evo1[g[k]] += num[k] / (den[k] + 0.1 * dmean);
+        s.evo0[g[k]] += 0.1 * nI[k] / dI[k];
+      }
+    }
   }
   return want_err ? errsum / s.P : 0.0;
 }
@@ -1084,12 +1283,22 @@ struct OrcMls {
   uint64_t rng = 0;
 };
 
+// variable: the reference-default path (variable probe and intensity, sub-pixel shift, position search from
+// iteration pps); 0 = the fixed-probe core.  The variable path's draws come from `seed` (mls_variable_draws).
 void* orc_mls_create(const float* raw_pos, int P, int N, const double* intens, const double* probe, const double* obj,
-                     uint64_t seed, double delta_p) {
+                     uint64_t seed, double delta_p, int variable, int pps) {
   auto* h = new OrcMls;
   std::vector<float> raw(raw_pos, raw_pos + 2 * size_t(P));
   h->s.geo = mls_geometry(raw, P, N);
   h->s.N = N; h->s.P = P; h->s.delta_p = delta_p;
+  h->s.variable = variable != 0;
+  h->s.PPS = pps;
+  if (h->s.variable) {
+    mls_variable_draws(seed, N, P, h->s.E, h->s.evo1);
+    h->s.pos = raw;
+    h->s.pos_o = raw;
+    h->s.sub.assign(2 * size_t(P), 0.f);
+  }
   const size_t NN = size_t(N) * N, XY = size_t(h->s.geo.X) * h->s.geo.Y;
   h->s.A.resize(size_t(P) * NN);
   std::vector<double> sums(P, 0.0);
@@ -1124,6 +1333,16 @@ int orc_mls_get(void* hp, double* obj, double* probe, double* scalars) {
     probe[2 * i + 1] = h->s.Pr[i].imag();
   }
   if (scalars) scalars[0] = h->s.maxIllum;
+  return 0;
+}
+
+// The variable path's state: extra mode E (N*N complex), evo0 / evo1 (P each), positions (2*P, x = rows).
+int orc_mls_get_var(void* hp, double* E, double* evo0, double* evo1, float* pos) {
+  auto* h = static_cast<OrcMls*>(hp);
+  if (!h->s.variable) return -1;
+  for (size_t i = 0; i < h->s.E.size(); ++i) { E[2 * i] = h->s.E[i].real(); E[2 * i + 1] = h->s.E[i].imag(); }
+  for (int i = 0; i < h->s.P; ++i) { evo0[i] = h->s.evo0[i]; evo1[i] = h->s.evo1[i]; }
+  for (size_t i = 0; i < h->s.pos.size(); ++i) pos[i] = h->s.pos[i];
   return 0;
 }
 

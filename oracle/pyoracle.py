@@ -56,7 +56,8 @@ def lib():
             "orc_destroy": ([vp], None),
             "orc_dm_baseline_f32": ([i, i, i, i, vp, vp, vp, i, i, vp], d),
             "orc_mls_geometry": ([vp, i, i, vp, vp, vp], i),
-            "orc_mls_create": ([vp, i, i, vp, vp, vp, u64, d], vp),
+            "orc_mls_create": ([vp, i, i, vp, vp, vp, u64, d, i, i], vp),
+            "orc_mls_get_var": ([vp, vp, vp, vp, vp], i),
             "orc_mls_step": ([vp, ctypes.POINTER(d)], i),
             "orc_mls_get": ([vp, vp, vp, vp], i),
             "orc_mls_destroy": ([vp], None),
@@ -240,17 +241,20 @@ def mls_geometry(raw_pos, N):
 
 
 class OracleMls:
-    """FP64 MLs core (groups, preconditioned LSQ-ML, one probe mode), stepped one iteration at a time."""
+    """FP64 MLs (groups, preconditioned LSQ-ML, one probe mode), stepped one iteration at a time.  variable=1 is the
+    reference's default path (variable probe and intensity, sub-pixel probe shift, position search from iteration
+    PPS); variable=0 the fixed-probe core."""
 
-    def __init__(self, raw_pos, intens, probe, obj=None, seed=0x5EED5EED, delta_p=0.1):
+    def __init__(self, raw_pos, intens, probe, obj=None, seed=0x5EED5EED, delta_p=0.1, variable=0, PPS=20):
         self.raw = np.ascontiguousarray(raw_pos, np.float32)
         self.I = np.ascontiguousarray(intens, np.float64)
         self.P, self.N = self.I.shape[0], self.I.shape[1]
         self.X, self.Y, self.starts, self.roi = mls_geometry(self.raw, self.N)
         pr = np.ascontiguousarray(np.asarray(probe).reshape(self.N, self.N), np.complex128)
         o = None if obj is None else np.ascontiguousarray(obj, np.complex128)
+        self.variable = int(variable)
         self.h = lib().orc_mls_create(_p(self.raw), self.P, self.N, _p(self.I), _p(pr),
-                                      _p(o) if o is not None else None, seed, delta_p)
+                                      _p(o) if o is not None else None, seed, delta_p, self.variable, int(PPS))
 
     def step(self):
         e = ctypes.c_double(0)
@@ -263,6 +267,15 @@ class OracleMls:
         sc = np.zeros(1)
         lib().orc_mls_get(self.h, _p(o), _p(p), _p(sc))
         return o, p, sc
+
+    def variable_state(self):
+        """(E, evo0, evo1, positions) of the variable path."""
+        E = np.zeros((self.N, self.N), np.complex128)
+        e0 = np.zeros(self.P)
+        e1 = np.zeros(self.P)
+        pos = np.zeros((self.P, 2), np.float32)
+        lib().orc_mls_get_var(self.h, _p(E), _p(e0), _p(e1), _p(pos))
+        return E, e0, e1, pos
 
     def close(self):
         if self.h:

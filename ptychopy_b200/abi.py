@@ -34,7 +34,7 @@ EXPORTS = [
     "pty_nn_up2", "pty_nn_up2_bwd", "pty_nn_mse", "pty_nn_adam", "pty_warm_input", "pty_warm_stitch",
     "pty_warm_object", "pty_dm_psi_from_object", "pty_tc_weights_size", "pty_tc_pack_weights", "pty_tc_conv3x3",
     "pty_tc_pool2", "pty_tc_up2", "pty_tc_to_bf16", "pty_tc_first_layer", "pty_tc_last_layer", "pty_set_warm_start",
-    "pty_selftest_bounded_waits", "pty_fft2_tc", "pty_autotune",
+    "pty_selftest_bounded_waits", "pty_fft2_tc", "pty_autotune", "pty_get_mls_state",
 ]
 
 
@@ -56,6 +56,7 @@ class PtyParams(ctypes.Structure):
         ("updateModes", ctypes.c_int), ("beamstopMask", ctypes.c_int), ("lf", ctypes.c_char * 256),
         ("PPS", ctypes.c_int), ("seed", ctypes.c_uint64), ("calculateRMS", ctypes.c_int),
         ("device", ctypes.c_int), ("wave", ctypes.c_int), ("precision", ctypes.c_int),
+        ("mlsCore", ctypes.c_int),
     ]
 
 
@@ -85,6 +86,7 @@ def lib():
             "pty_get_object": ([vp, vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "pty_get_probe": ([vp, vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "pty_get_positions": ([vp, vp, ctypes.c_int], ctypes.c_int),
+            "pty_get_mls_state": ([vp, vp, vp, vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "pty_write_results": ([vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "pty_set_stream": ([vp, vp], ctypes.c_int),
             "pty_kernel_launches": ([vp], ctypes.c_int64),
@@ -248,6 +250,15 @@ class Session:
         q = np.empty((d["P"], 2), np.float32)
         check(lib().pty_get_positions(self.h, _ptr(q), d["P"]))
         return q
+
+    def mls_state(self):
+        """MLs default path: (extra probe mode E, evo0, evo1)."""
+        d = self.dims()
+        E = np.empty((d["N"], d["N"]), np.complex64)
+        e0 = np.empty(d["P"])
+        e1 = np.empty(d["P"])
+        check(lib().pty_get_mls_state(self.h, _ptr(E), _ptr(e0), _ptr(e1), d["N"], d["P"]))
+        return E, e0, e1
 
     def write_results(self, directory, r=0, binary=False):
         check(lib().pty_write_results(self.h, directory.encode(), r, int(binary)))

@@ -14,7 +14,8 @@
 //   update    O += beta_o S/(p + delta_p MAX_ILLUM) over the group's bounding box, P += beta_p * mean direction
 //             (Sample::update_object, Probe::update_probe)
 // The whole iteration (calc_object_norm, cached illumination, all groups) is one CUDA graph; the random group
-// tables live in device memory and are rewritten before each replay.
+// tables live in device memory and are rewritten before each replay.  This is the fixed-probe core; the reference's
+// default path (variable probe, sub-pixel shift, position search) is kernels_mls_var.cu, built on the same kernels.
 #include "fft_core.cuh"
 #include "kernel_util.cuh"
 #include "kernels_mls.h"
@@ -129,8 +130,9 @@ __global__ void k_mls_dirs(const float2* __restrict__ chi, const float2* __restr
   }
 }
 
+// probe: one N x N probe for every window (pstride 0) or one per window (pstride N^2).
 __global__ void k_mls_lsq(const float2* __restrict__ chi, const float2* __restrict__ objp,
-                          const float2* __restrict__ probe, const float2* __restrict__ pum,
+                          const float2* __restrict__ probe, size_t pstride, const float2* __restrict__ pum,
                           const float2* __restrict__ S, const float* __restrict__ pobj,
                           const float* __restrict__ maxIllum, float delta_p, const int2* __restrict__ starts,
                           const int* __restrict__ members, const int* __restrict__ gsize, int N, int Y,
@@ -146,7 +148,7 @@ __global__ void k_mls_lsq(const float2* __restrict__ chi, const float2* __restri
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
     const size_t o = size_t(s.x + i / N) * Y + (s.y + i % N);
     const float2 oup = cscale(S[o], 1.f / (pobj[o] + dmax));
-    const float2 dOP = cmul(oup, probe[i]);
+    const float2 dOP = cmul(oup, probe[k * pstride + i]);
     const float2 dPO = cmul(cscale(pum[i], invG), objp[k * NN + i]);
     const float2 c = chi[k * NN + i];
     a1 += double(dOP.x * dOP.x + dOP.y * dOP.y + lam);
@@ -216,14 +218,34 @@ __global__ void k_mls_update_object(float2* __restrict__ obj, float2* __restrict
   }
 }
 
+// P += beta_p * pum / G; clear = 1 zeroes the accumulator for the next group's atomics.
 __global__ void k_mls_update_probe(float2* __restrict__ probe, float2* __restrict__ pum, const double* __restrict__ betas,
-                                   const int* __restrict__ gsize, int n) {
+                                   const int* __restrict__ gsize, int n, int clear) {
   const float2 b = make_float2(float(betas[2]), float(betas[3]));
   const float invG = 1.f / float(*gsize);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     probe[i] = cadd(probe[i], cmul(b, cscale(pum[i], invG)));
-    pum[i] = make_float2(0.f, 0.f);
+    if (clear) pum[i] = make_float2(0.f, 0.f);
   }
+}
+
+// Bounding box (x0, y0, nx, ny) of each group's windows.
+__global__ void k_mls_bbox(const int2* __restrict__ starts, const int* __restrict__ members,
+                           const int* __restrict__ gsize, int ngroups, int Gmax, int N, int* __restrict__ bbox) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  int x0 = 1 << 30, y0 = 1 << 30, x1 = 0, y1 = 0;
+  for (int m = 0; m < gsize[g]; ++m) {
+    const int2 s = starts[members[size_t(g) * Gmax + m]];
+    x0 = min(x0, s.x);
+    y0 = min(y0, s.y);
+    x1 = max(x1, s.x + N);
+    y1 = max(y1, s.y + N);
+  }
+  bbox[4 * g] = x0;
+  bbox[4 * g + 1] = y0;
+  bbox[4 * g + 2] = x1 - x0;
+  bbox[4 * g + 3] = y1 - y0;
 }
 
 static int grid_for(size_t n, int cap = 1184) {
@@ -310,16 +332,46 @@ cudaError_t mls_iteration(const MlsBuffers& b, int ngroups, cudaStream_t st) {
       return e;
     k_mls_dirs<<<grid, 256, 0, st>>>(b.psi, b.objp, b.probe, b.pobj, b.maxIllum, b.starts, mem, gs, N, b.Y, b.pum,
                                      b.S);
-    k_mls_lsq<<<grid, 256, 0, st>>>(b.psi, b.objp, b.probe, b.pum, b.S, b.pobj, b.maxIllum, b.delta_p, b.starts, mem,
-                                    gs, N, b.Y, b.sums);
-    k_mls_solve<<<1, 32, 0, st>>>(b.sums, b.errk, gs, N, b.beta_obj, b.beta_probe, b.betas, b.err);
-    k_mls_update_object<<<grid_for(size_t(2) * NN), 256, 0, st>>>(b.obj, b.S, b.pobj, b.maxIllum, b.delta_p, b.betas,
-                                                                   b.bbox + 4 * size_t(g), b.Y);
-    k_mls_update_probe<<<grid_for(NN), 256, 0, st>>>(b.probe, b.pum, b.betas, gs, NN);
+    if ((e = mls_lsq(b, b.probe, 0, mem, gs, st)) != cudaSuccess) return e;
+    if ((e = mls_solve_update(b, mem, gs, b.bbox + 4 * size_t(g), 1, st)) != cudaSuccess) return e;
   }
   return cudaGetLastError();
 }
 
 int mls_launches_per_iteration(int ngroups) { return 5 + ngroups * 11; }
+
+cudaError_t mls_group_boxes(const int2* starts, const int* members, const int* gsize, int ngroups, int Gmax, int N,
+                            int* bbox, cudaStream_t st) {
+  k_mls_bbox<<<(ngroups + 127) / 128, 128, 0, st>>>(starts, members, gsize, ngroups, Gmax, N, bbox);
+  return cudaGetLastError();
+}
+
+cudaError_t mls_modulus(const MlsBuffers& b, const int* members, const int* gsize, cudaStream_t st) {
+  const int NN = b.N * b.N;
+  dim3 grid((NN + 255) / 256 > 64 ? 64 : (NN + 255) / 256, b.Gmax);
+  k_mls_modulus<<<grid, 256, 0, st>>>(b.psi, b.amp, members, gsize, b.N, b.errk);
+  return cudaGetLastError();
+}
+
+cudaError_t mls_lsq(const MlsBuffers& b, const float2* probe, size_t pstride, const int* members, const int* gsize,
+                    cudaStream_t st) {
+  const int NN = b.N * b.N;
+  dim3 grid((NN + 255) / 256 > 64 ? 64 : (NN + 255) / 256, b.Gmax);
+  k_mls_lsq<<<grid, 256, 0, st>>>(b.psi, b.objp, probe, pstride, b.pum, b.S, b.pobj, b.maxIllum, b.delta_p, b.starts,
+                                  members, gsize, b.N, b.Y, b.sums);
+  return cudaGetLastError();
+}
+
+// 2x2 solves, object update over the group box, probe update.
+cudaError_t mls_solve_update(const MlsBuffers& b, const int* members, const int* gsize, const int* bbox,
+                             int clear_pum, cudaStream_t st) {
+  (void)members;
+  const int NN = b.N * b.N;
+  k_mls_solve<<<1, 32, 0, st>>>(b.sums, b.errk, gsize, b.N, b.beta_obj, b.beta_probe, b.betas, b.err);
+  k_mls_update_object<<<grid_for(size_t(2) * NN), 256, 0, st>>>(b.obj, b.S, b.pobj, b.maxIllum, b.delta_p, b.betas,
+                                                                 bbox, b.Y);
+  k_mls_update_probe<<<grid_for(NN), 256, 0, st>>>(b.probe, b.pum, b.betas, gsize, NN, clear_pum);
+  return cudaGetLastError();
+}
 
 }  // namespace pty

@@ -35,6 +35,29 @@ struct MlsBuffers {
   double beta_obj, beta_probe;  // beta_object * beta_LSQ, beta_probe * beta_LSQ
   int tc;                 // 1: the group FFTs run as split-BF16 tensor-core stages (fft2_tc)
   int* tc_err;            // their wait-timeout flag
+  // the reference-default path (kernels_mls_var.cu): variable probe and intensity, sub-pixel probe shift,
+  // position search
+  float2* E;              // N x N extra probe mode
+  double* evo;            // 2 x P probe evolution: intensity weights (evo0) | extra-mode weights (evo1)
+  float* pos;             // 2 x P current positions (x = rows)
+  const float* pos_o;     // 2 x P original positions
+  float2* sub;            // P sub-pixel shifts (x = column remainder, y = row remainder)
+  int2* win;              // P window starts, rewritten from pos (same array as `starts`)
+  int* boxw;              // ngroups x 4 group boxes, written on the device (same array as `bbox`)
+  float2* vp;             // Gmax x N x N probes of the group's positions
+  float2* pu;             // Gmax x N x N probe directions, shifted back
+  float2* aux;            // 2 Gmax x N x N gradient images of the position search; N x N extra-mode update
+  double* vs;             // scratch sums (mls_var_scratch_doubles(Gmax))
+  float* pmax;            // max of p_object in this iteration
+  float cvx, cvy;         // ceil(X/2 - N/2), ceil(Y/2 - N/2)
+};
+
+// Parts of one iteration of the reference-default path that depend on the iteration number.
+enum MlsVarFlags : unsigned {
+  MLS_WINDOWS = 1u,     // windows and sub-pixel shifts from the positions (iteration 1 and from PPS)
+  MLS_REMOVE = 2u,      // remove_extra_degree (from iteration 2)
+  MLS_VARUPD = 4u,      // update_variable_probe (from iteration 3)
+  MLS_POSSEARCH = 8u,   // gradient_position_solver (from PPS)
 };
 
 cudaError_t mls_illum_add(float* pobj, const float2* probe, const int2* starts, int P, int N, int Y, float scale,
@@ -49,5 +72,17 @@ cudaError_t max_real(const float* a, size_t n, float* out, cudaStream_t st);
 // One MLs iteration over `ngroups` groups (tables in b.members / b.gsize / b.bbox), enqueued on st.
 cudaError_t mls_iteration(const MlsBuffers& b, int ngroups, cudaStream_t st);
 int mls_launches_per_iteration(int ngroups);
+// One iteration of the reference-default path (kernels_mls_var.cu); flags from MlsVarFlags.
+cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, cudaStream_t st);
+int mls_var_launches_per_iteration(int ngroups, unsigned flags);
+size_t mls_var_scratch_doubles(int Gmax);
+// Kernels the two paths share (kernels_mls.cu).
+cudaError_t mls_group_boxes(const int2* starts, const int* members, const int* gsize, int ngroups, int Gmax, int N,
+                            int* bbox, cudaStream_t st);
+cudaError_t mls_modulus(const MlsBuffers& b, const int* members, const int* gsize, cudaStream_t st);
+cudaError_t mls_lsq(const MlsBuffers& b, const float2* probe, size_t pstride, const int* members, const int* gsize,
+                    cudaStream_t st);
+cudaError_t mls_solve_update(const MlsBuffers& b, const int* members, const int* gsize, const int* bbox,
+                             int clear_pum, cudaStream_t st);
 
 }  // namespace pty

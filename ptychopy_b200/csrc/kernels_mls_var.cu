@@ -1,0 +1,485 @@
+// MLs with the reference's defaults (src/Parameters.h:162-163: variable_probe, variable_intensity,
+// apply_subpix_shift on, probe_pos_search = PPS): one probe mode, one object, one extra (variable) probe mode.
+//
+// Per iteration (MLS::iteration, src/MLS.cpp:74-116):
+//   windows   from iteration 1 and PPS on: window starts and sub-pixel remainders from the current positions
+//             (find_reconstruction_ROI, src/IPtychoScanMesh.cpp:122-171); group boxes from the windows
+//   norm      calc_object_norm scales P, the extra mode E and O (src/Probe.cpp:671-699)
+//   recentre  positions lose their mean drift from the originals (updateScanPositionsDiff,
+//             src/IPtychoScanMesh.cpp:340-368)
+//   remove    from iteration 2: E to unit RMS, its weights carry the norm; the intensity weights' regularisation
+//             (remove_extra_degree, src/Probe.cpp:615-669)
+//   illum     p_object running average (updated_cached_illumination), and its maximum
+// Per group of G positions:
+//   probes    vp_j = P evo0_j + E evo1_j, shifted by the sub-pixel remainder: IFFT2(FFT2(vp) e^{-2 pi i s.f})/N^2
+//             (get_illumination_probe, shift_probe, src/Probe.cpp:887-954,1261-1337)
+//   exit      psi = O[window] vp_j; FFT2, modulus with error, IFFT2 -> chi   (kernels_mls.cu)
+//   dirs      pu_j = chi conj(O[window]) shifted back; pum = sum_j W pu_j; S += chi conj(vp_j) at the window
+//             (src/MLS.cpp:232-347)
+//   lsq/solve/update  as the core, with the position's own probe vp_j in dOP
+//   search    from PPS: Fourier gradients of the window, least-squares shift per position clamped to 0.2 px
+//             (gradient_position_solver, src/Probe.cpp:956-1118)
+//   variable  from iteration 3: extra-mode step on the weighted residual of the probe directions, then the
+//             extra-mode and intensity weights of the group's positions (update_variable_probe, src/Probe.cpp:1366-1516)
+// Scalar bookkeeping (2x2 solves, position and weight updates) runs in one thread on the device, so the iteration
+// is one CUDA graph with no host round trip.
+#include "fft_core.cuh"
+#include "kernel_util.cuh"
+#include "kernels_mls.h"
+
+namespace pty {
+
+namespace {
+
+constexpr float kTwoPi = 6.283185307179586f;
+
+// Offsets into MlsBuffers::vs (doubles).
+struct VsLayout {
+  int G;
+  __host__ __device__ size_t pos() const { return 0; }             // 4 G: position-search sums
+  __host__ __device__ size_t proj() const { return 4 * size_t(G); }  // G: residual projections
+  __host__ __device__ size_t prj() const { return 5 * size_t(G); }   // G: per-position weights of the update
+  __host__ __device__ size_t evs() const { return 6 * size_t(G); }   // 4 G: weight-update sums
+  __host__ __device__ size_t sc() const { return 10 * size_t(G); }   // 8 scalars
+};
+enum { SC_ESUM = 0, SC_USUM = 1, SC_ENEW = 2, SC_EFAC = 3, SC_PFAC = 4 };
+
+__device__ __forceinline__ float fft_freq(int k, int N) {
+  return k < N / 2 ? float(k) / float(N) : float(k) / float(N) - 1.f;
+}
+
+__global__ void k_var_windows(const float* __restrict__ pos, int P, int N, int X, int Y, float cvx, float cvy,
+                              int2* __restrict__ win, float2* __restrict__ sub) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P) return;
+  const float p1 = pos[2 * i] + cvx, p2 = pos[2 * i + 1] + cvy;
+  const float t1 = roundf(p1), t2 = roundf(p2);
+  sub[i] = make_float2(p2 - t2, p1 - t1);
+  win[i] = make_int2(min(max(int(t1) - 1, 0), X - N), min(max(int(t2) - 1, 0), Y - N));
+}
+
+// Positions minus their mean drift from the originals (one block).
+__global__ void k_var_recentre(float* __restrict__ pos, const float* __restrict__ pos_o, int P) {
+  double s[4] = {0, 0, 0, 0};
+  for (int i = threadIdx.x; i < P; i += blockDim.x) {
+    s[0] += pos[2 * i];
+    s[1] += pos[2 * i + 1];
+    s[2] += pos_o[2 * i];
+    s[3] += pos_o[2 * i + 1];
+  }
+  __shared__ float d[2];
+  for (int m = 0; m < 4; ++m) {
+    s[m] = block_reduce_sum(s[m]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    d[0] = float(s[0] / P) - float(s[2] / P);
+    d[1] = float(s[1] / P) - float(s[3] / P);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < P; i += blockDim.x) {
+    pos[2 * i] -= d[0];
+    pos[2 * i + 1] -= d[1];
+  }
+}
+
+// out += sum |a|^2 (FP64)
+__global__ void k_var_sumsq(const float2* __restrict__ a, size_t n, double* __restrict__ out) {
+  double s = 0;
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    s += double(a[i].x) * a[i].x + double(a[i].y) * a[i].y;
+  s = block_reduce_sum(s);
+  if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
+// remove_extra_degree's scalars (one thread).  Its mean and norm loops run over m_probe_evolution.size() = 2 entries,
+// so only positions 0 and 1 are re-centred; kept as written.
+__global__ void k_var_remove(double* __restrict__ sc, double* __restrict__ evo, int P, int NN) {
+  if (threadIdx.x != 0) return;
+  double* e0 = evo;
+  double* e1 = evo + P;
+  const double vn = sqrt(sc[SC_ESUM] / NN);
+  for (int i = 0; i < P; ++i) e1[i] *= vn;
+  const int len = P < 2 ? P : 2;
+  double a0 = 0, a1 = 0;
+  for (int i = 0; i < len; ++i) {
+    a0 += e0[i];
+    a1 += e1[i];
+  }
+  const float m0 = float(a0 / len), m1 = float(a1 / len);
+  double sq = 0;
+  for (int i = 0; i < len; ++i) {
+    e0[i] = (e0[i] - m0) * 0.99 + 1;
+    e1[i] = e1[i] - m1;
+    sq += e0[i] * e0[i];
+  }
+  const double cn = sqrt(sq / len);
+  for (int i = 0; i < len; ++i) e0[i] /= cn;
+  sc[SC_EFAC] = 1.0 / vn;
+  sc[SC_PFAC] = cn;
+  sc[SC_ESUM] = 0.0;
+}
+
+__global__ void k_var_scale(float2* __restrict__ a, size_t n, const double* __restrict__ f) {
+  const float s = float(*f);
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    a[i] = cscale(a[i], s);
+}
+
+// objp = O[window], vp = P evo0 + E evo1 (zeros past the group's size)
+__global__ void k_var_exit(const float2* __restrict__ obj, const float2* __restrict__ probe,
+                           const float2* __restrict__ E, const double* __restrict__ evo, int P,
+                           const int2* __restrict__ win, const int* __restrict__ members,
+                           const int* __restrict__ gsize, int N, int Y, float2* __restrict__ objp,
+                           float2* __restrict__ vp) {
+  const int k = blockIdx.y;
+  const size_t NN = size_t(N) * N;
+  const bool live = k < *gsize;
+  const int j = live ? members[k] : 0;
+  const int2 s = live ? win[j] : make_int2(0, 0);
+  const float f0 = live ? float(evo[j]) : 0.f, f1 = live ? float(evo[P + j]) : 0.f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    float2 o = make_float2(0.f, 0.f), v = make_float2(0.f, 0.f);
+    if (live) {
+      o = obj[size_t(s.x + i / N) * Y + (s.y + i % N)];
+      v = cadd(cscale(probe[i], f0), cscale(E[i], f1));
+    }
+    objp[k * NN + i] = o;
+    vp[k * NN + i] = v;
+  }
+}
+
+// a_k *= e^{-2 pi i sign (s.x f[c] + s.y f[r])} / N^2 on the spectra of the group's windows (shift_probe)
+__global__ void k_var_phase(float2* __restrict__ a, const float2* __restrict__ sub, const int* __restrict__ members,
+                            const int* __restrict__ gsize, int N, float sign) {
+  const int k = blockIdx.y;
+  if (k >= *gsize) return;
+  const size_t NN = size_t(N) * N;
+  const float2 s = sub[members[k]];
+  const float sx = sign * s.x, sy = sign * s.y, nrm = 1.f / float(NN);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    const float t = sx * fft_freq(i % N, N) + sy * fft_freq(i / N, N);
+    float sn, cs;
+    sincosf(-kTwoPi * t, &sn, &cs);
+    a[k * NN + i] = cmul(a[k * NN + i], make_float2(cs * nrm, sn * nrm));
+  }
+}
+
+__global__ void k_var_psi(const float2* __restrict__ objp, const float2* __restrict__ vp, float2* __restrict__ psi,
+                          size_t n) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    psi[i] = cmul(objp[i], vp[i]);
+}
+
+// pu = chi conj(objp); S += chi conj(vp) at the window
+__global__ void k_var_dirs(const float2* __restrict__ chi, const float2* __restrict__ objp,
+                           const float2* __restrict__ vp, const int2* __restrict__ win,
+                           const int* __restrict__ members, const int* __restrict__ gsize, int N, int Y,
+                           float2* __restrict__ pu, float2* __restrict__ S) {
+  const int k = blockIdx.y;
+  const size_t NN = size_t(N) * N;
+  if (k >= *gsize) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x)
+      pu[k * NN + i] = make_float2(0.f, 0.f);
+    return;
+  }
+  const int2 s = win[members[k]];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    const float2 c = chi[k * NN + i];
+    pu[k * NN + i] = cmulc(c, objp[k * NN + i]);
+    atomicAdd(&S[size_t(s.x + i / N) * Y + (s.y + i % N)], cmulc(c, vp[k * NN + i]));
+  }
+}
+
+// pum = sum_j W_j pu_j, W = p/(p + 0.01 MAX_ILLUM) at the window (a sum over the group per pixel: no atomics)
+__global__ void k_var_pum(const float2* __restrict__ pu, const float* __restrict__ pobj,
+                          const float* __restrict__ maxIllum, const int2* __restrict__ win,
+                          const int* __restrict__ members, const int* __restrict__ gsize, int N, int Y,
+                          float2* __restrict__ pum) {
+  const int G = *gsize;
+  const size_t NN = size_t(N) * N;
+  const float damp = 0.01f * *maxIllum;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    float2 acc = make_float2(0.f, 0.f);
+    for (int k = 0; k < G; ++k) {
+      const int2 s = win[members[k]];
+      const float w = pobj[size_t(s.x + i / N) * Y + (s.y + i % N)];
+      acc = cadd(acc, cscale(pu[k * NN + i], w / (w + damp)));
+    }
+    pum[i] = acc;
+  }
+}
+
+// Gradient spectra of the windows: from FFT2(objp) in aux[k], dX -> aux[k] (column frequencies), dY -> aux[Gmax + k]
+__global__ void k_var_grad(float2* __restrict__ aux, int Gmax, int N) {
+  const int k = blockIdx.y;
+  const size_t NN = size_t(N) * N;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    const float2 v = aux[k * NN + i];
+    const float2 d = cmul(v, make_float2(0.f, kTwoPi));
+    aux[(Gmax + k) * NN + i] = cscale(d, fft_freq(i / N, N));
+    aux[k * NN + i] = cscale(d, fft_freq(i % N, N));
+  }
+}
+
+// Per window: sum |dX vp|^2, Re(chi conj(dX vp)), the same for dY (gradient images still unnormalised by N^2)
+__global__ void k_var_possums(const float2* __restrict__ aux, const float2* __restrict__ vp,
+                              const float2* __restrict__ chi, const int* __restrict__ gsize, int Gmax, int N,
+                              double* __restrict__ out) {
+  const int k = blockIdx.y;
+  if (k >= *gsize) return;
+  const size_t NN = size_t(N) * N;
+  const float nrm = 1.f / float(NN);
+  double v[4] = {0, 0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    const float2 p = vp[k * NN + i], c = chi[k * NN + i];
+    const float2 gx = cmul(cscale(aux[k * NN + i], nrm), p);
+    const float2 gy = cmul(cscale(aux[(Gmax + k) * NN + i], nrm), p);
+    v[0] += double(gx.x) * gx.x + double(gx.y) * gx.y;
+    v[1] += double(c.x) * gx.x + double(c.y) * gx.y;  // Re(chi conj(g))
+    v[2] += double(gy.x) * gy.x + double(gy.y) * gy.y;
+    v[3] += double(c.x) * gy.x + double(c.y) * gy.y;
+  }
+  for (int m = 0; m < 4; ++m) {
+    const double r = block_reduce_sum(v[m]);
+    if (threadIdx.x == 0) atomicAdd(&out[4 * k + m], r);
+    __syncthreads();
+  }
+}
+
+// Position updates (one thread): shift = clamp(num/den, +-0.2); the column-gradient shift moves x (the row
+// coordinate) and the row-gradient one y, as gradient_position_solver pairs them.
+__global__ void k_var_posupd(double* __restrict__ s, const int* __restrict__ members, const int* __restrict__ gsize,
+                             float* __restrict__ pos) {
+  if (threadIdx.x != 0) return;
+  const int G = *gsize;
+  for (int k = 0; k < G; ++k) {
+    const double dx = s[4 * k + 1] / s[4 * k], dy = s[4 * k + 3] / s[4 * k + 2];
+    const double shx = fmin(fabs(dx), 0.2) * double((0.0 < dx) - (dx < 0.0));
+    const double shy = fmin(fabs(dy), 0.2) * double((0.0 < dy) - (dy < 0.0));
+    const int j = members[k];
+    pos[2 * j] = float(double(pos[2 * j]) + shx);
+    pos[2 * j + 1] = float(double(pos[2 * j + 1]) + shy);
+    for (int m = 0; m < 4; ++m) s[4 * k + m] = 0.0;
+  }
+}
+
+// Residual of window k at pixel i: (pu_k - pum/G) p/max(p)
+__device__ __forceinline__ float2 var_resid(const float2* pu, const float2* pum, const float* pobj, float inv_pmax,
+                                            int2 s, int k, int i, int N, int Y, float invG) {
+  const float w = pobj[size_t(s.x + i / N) * Y + (s.y + i % N)] * inv_pmax;
+  const float2 r = make_float2(pu[size_t(k) * N * N + i].x - pum[i].x * invG, pu[size_t(k) * N * N + i].y - pum[i].y * invG);
+  return cscale(r, w);
+}
+
+// proj_k += sum Re(E conj(resid_k))
+__global__ void k_var_proj(const float2* __restrict__ pu, const float2* __restrict__ pum,
+                           const float* __restrict__ pobj, const float* __restrict__ pmax,
+                           const float2* __restrict__ E, const int2* __restrict__ win, const int* __restrict__ members,
+                           const int* __restrict__ gsize, int N, int Y, double* __restrict__ proj) {
+  const int k = blockIdx.y;
+  const int G = *gsize;
+  if (k >= G) return;
+  const int2 s = win[members[k]];
+  const float ip = 1.f / *pmax, invG = 1.f / float(G);
+  double acc = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    const float2 r = var_resid(pu, pum, pobj, ip, s, k, i, N, Y, invG);
+    const float2 e = E[i];
+    acc += double(e.x) * r.x + double(e.y) * r.y;
+  }
+  acc = block_reduce_sum(acc);
+  if (threadIdx.x == 0) atomicAdd(&proj[k], acc);
+}
+
+// prj_k = (mean_pixels Re(E conj(resid_k)) + evo1_k) / sum_group evo1^2 (one thread); clears proj
+__global__ void k_var_prj(double* __restrict__ proj, double* __restrict__ prj, const double* __restrict__ evo, int P,
+                          const int* __restrict__ members, const int* __restrict__ gsize, int NN) {
+  if (threadIdx.x != 0) return;
+  const int G = *gsize;
+  double evn = 0;
+  for (int k = 0; k < G; ++k) evn += evo[P + members[k]] * evo[P + members[k]];
+  for (int k = 0; k < G; ++k) {
+    prj[k] = (proj[k] / NN + evo[P + members[k]]) / evn;
+    proj[k] = 0.0;
+  }
+}
+
+// upd = sum_k resid_k prj_k / N^2; usum += sum |upd|^2
+__global__ void k_var_upd(const float2* __restrict__ pu, const float2* __restrict__ pum,
+                          const float* __restrict__ pobj, const float* __restrict__ pmax,
+                          const double* __restrict__ prj, const int2* __restrict__ win, const int* __restrict__ members,
+                          const int* __restrict__ gsize, int N, int Y, float2* __restrict__ upd,
+                          double* __restrict__ usum) {
+  const int G = *gsize;
+  const float ip = 1.f / *pmax, invG = 1.f / float(G), nrm = 1.f / float(N * N);
+  double acc = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    float2 u = make_float2(0.f, 0.f);
+    for (int k = 0; k < G; ++k) {
+      const float2 r = var_resid(pu, pum, pobj, ip, win[members[k]], k, i, N, Y, invG);
+      u = cadd(u, cscale(r, float(prj[k])));
+    }
+    u = cscale(u, nrm);
+    upd[i] = u;
+    acc += double(u.x) * u.x + double(u.y) * u.y;
+  }
+  acc = block_reduce_sum(acc);
+  if (threadIdx.x == 0) atomicAdd(usum, acc);
+}
+
+// E += upd relax_U / max(1, rms(upd)); enew += sum |E|^2
+__global__ void k_var_eapply(float2* __restrict__ E, const float2* __restrict__ upd, int NN, const int* __restrict__ gsize,
+                             int P, const double* __restrict__ usum, double* __restrict__ enew) {
+  const double rms = sqrt(*usum / NN);
+  const float us = float((double(*gsize) / P) / (rms > 1.0 ? rms : 1.0));
+  double acc = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += gridDim.x * blockDim.x) {
+    const float2 e = cadd(E[i], cscale(upd[i], us));
+    E[i] = e;
+    acc += double(e.x) * e.x + double(e.y) * e.y;
+  }
+  acc = block_reduce_sum(acc);
+  if (threadIdx.x == 0) atomicAdd(enew, acc);
+}
+
+__global__ void k_var_enorm(float2* __restrict__ E, int NN, const double* __restrict__ enew) {
+  const float f = float(1.0 / sqrt(*enew / NN));
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += gridDim.x * blockDim.x) E[i] = cscale(E[i], f);
+}
+
+// Per window: sum |objp E|^2, Re(chi conj(objp E)), |objp P|^2, Re(chi conj(objp P))
+__global__ void k_var_evosums(const float2* __restrict__ objp, const float2* __restrict__ E,
+                              const float2* __restrict__ probe, const float2* __restrict__ chi,
+                              const int* __restrict__ gsize, int N, double* __restrict__ out) {
+  const int k = blockIdx.y;
+  if (k >= *gsize) return;
+  const size_t NN = size_t(N) * N;
+  double v[4] = {0, 0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    const float2 o = objp[k * NN + i], c = chi[k * NN + i];
+    const float2 a = cmul(o, E[i]), b = cmul(o, probe[i]);
+    v[0] += double(a.x) * a.x + double(a.y) * a.y;
+    v[1] += double(c.x) * a.x + double(c.y) * a.y;
+    v[2] += double(b.x) * b.x + double(b.y) * b.y;
+    v[3] += double(c.x) * b.x + double(c.y) * b.y;
+  }
+  for (int m = 0; m < 4; ++m) {
+    const double r = block_reduce_sum(v[m]);
+    if (threadIdx.x == 0) atomicAdd(&out[4 * k + m], r);
+    __syncthreads();
+  }
+}
+
+// evo1 += mean num / (mean den + 0.1 group mean of mean den); evo0 += 0.1 sum num / sum den (one thread);
+// clears the sums of this group's variable update
+__global__ void k_var_evoupd(double* __restrict__ s, double* __restrict__ sc, double* __restrict__ evo, int P,
+                             const int* __restrict__ members, const int* __restrict__ gsize, int NN) {
+  if (threadIdx.x != 0) return;
+  const int G = *gsize;
+  double dm = 0;
+  for (int k = 0; k < G; ++k) dm += s[4 * k] / NN;
+  dm /= G;
+  for (int k = 0; k < G; ++k) {
+    const int j = members[k];
+    evo[P + j] += (s[4 * k + 1] / NN) / (s[4 * k] / NN + 0.1 * dm);
+    evo[j] += 0.1 * s[4 * k + 3] / s[4 * k + 2];
+    for (int m = 0; m < 4; ++m) s[4 * k + m] = 0.0;
+  }
+  sc[SC_USUM] = 0.0;
+  sc[SC_ENEW] = 0.0;
+}
+
+int grid_n(size_t n, int cap = 1184) {
+  size_t g = (n + 255) / 256;
+  return int(g < 1 ? 1 : (g > size_t(cap) ? cap : g));
+}
+
+}  // namespace
+
+size_t mls_var_scratch_doubles(int Gmax) { return 10 * size_t(Gmax) + 8; }
+
+int mls_var_launches_per_iteration(int ngroups, unsigned flags) {
+  int pre = 2 + 3 + 1 + 3 + 2;  // windows?, boxes, norm (3 + E), recentre, illumination, max
+  if (flags & MLS_WINDOWS) ++pre;
+  if (flags & MLS_REMOVE) pre += 4;
+  // per group: exit, 2 FFT2 + phase, psi, 2 FFT2 + modulus, dirs, 2 FFT2 + phase, pum, lsq, solve + 2 updates
+  int per = 1 + 5 + 1 + 5 + 1 + 5 + 1 + 1 + 3;
+  if (flags & MLS_POSSEARCH) per += 2 + 1 + 2 + 1 + 1;  // FFT2, grad, FFT2 (2 G), sums, update
+  if (flags & MLS_VARUPD) per += 7;
+  return pre + ngroups * per;
+}
+
+cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, cudaStream_t st) {
+  const int N = b.N, NN = N * N, P = b.P;
+  const size_t XY = size_t(b.X) * b.Y, GN = size_t(b.Gmax) * NN;
+  const VsLayout L{b.Gmax};
+  double* sc = b.vs + L.sc();
+  cudaError_t e;
+  auto fft = [&](float2* d, int batch, bool inv) {
+    return b.tc ? fft2_tc(d, b.work, batch, N, inv, b.tc_err, st) : fft2(d, b.work, b.tw, batch, N, inv, st);
+  };
+  if (flags & MLS_WINDOWS)
+    k_var_windows<<<(P + 255) / 256, 256, 0, st>>>(b.pos, P, N, b.X, b.Y, b.cvx, b.cvy, b.win, b.sub);
+  if ((e = mls_group_boxes(b.win, b.members, b.gsize, ngroups, b.Gmax, N, b.boxw, st)) != cudaSuccess) return e;
+  // calc_object_norm over the object ROI with the current illumination weights: P, E scaled by on, O by 1/on
+  if ((e = mls_norm_sums(b.pobj, b.obj, b.Y, b.roi[0], b.roi[1], b.roi[2], b.roi[3], 1, b.normsums, st)) != cudaSuccess)
+    return e;
+  if ((e = scale_by_norm(b.probe, NN, b.normsums, 0, st)) != cudaSuccess) return e;
+  if ((e = scale_by_norm(b.E, NN, b.normsums, 0, st)) != cudaSuccess) return e;
+  if ((e = scale_by_norm(b.obj, XY, b.normsums, 1, st)) != cudaSuccess) return e;
+  k_var_recentre<<<1, 256, 0, st>>>(b.pos, b.pos_o, P);
+  if (flags & MLS_REMOVE) {
+    k_var_sumsq<<<grid_n(NN, 64), 256, 0, st>>>(b.E, NN, sc + SC_ESUM);
+    k_var_remove<<<1, 32, 0, st>>>(sc, b.evo, P, NN);
+    k_var_scale<<<grid_n(NN), 256, 0, st>>>(b.E, NN, sc + SC_EFAC);
+    k_var_scale<<<grid_n(NN), 256, 0, st>>>(b.probe, NN, sc + SC_PFAC);
+  }
+  // updated_cached_illumination: p = (p + sum |P|^2 at the windows) / 2; its maximum for the variable update
+  if ((e = scale_real(b.pobj, XY, 0.5f, st)) != cudaSuccess) return e;
+  if ((e = mls_illum_add(b.pobj, b.probe, b.win, P, N, b.Y, 0.5f, st)) != cudaSuccess) return e;
+  if ((e = max_real(b.pobj, XY, b.pmax, st)) != cudaSuccess) return e;
+  const int gb = (NN + 255) / 256 > 64 ? 64 : (NN + 255) / 256;
+  const dim3 grid(gb, b.Gmax);
+  for (int g = 0; g < ngroups; ++g) {
+    const int* mem = b.members + size_t(g) * b.Gmax;
+    const int* gs = b.gsize + g;
+    k_var_exit<<<grid, 256, 0, st>>>(b.obj, b.probe, b.E, b.evo, P, b.win, mem, gs, N, b.Y, b.objp, b.vp);
+    if ((e = fft(b.vp, b.Gmax, false)) != cudaSuccess) return e;
+    k_var_phase<<<grid, 256, 0, st>>>(b.vp, b.sub, mem, gs, N, 1.f);
+    if ((e = fft(b.vp, b.Gmax, true)) != cudaSuccess) return e;
+    k_var_psi<<<grid_n(GN), 256, 0, st>>>(b.objp, b.vp, b.psi, GN);
+    if ((e = fft(b.psi, b.Gmax, false)) != cudaSuccess) return e;
+    if ((e = mls_modulus(b, mem, gs, st)) != cudaSuccess) return e;
+    if ((e = fft(b.psi, b.Gmax, true)) != cudaSuccess) return e;
+    k_var_dirs<<<grid, 256, 0, st>>>(b.psi, b.objp, b.vp, b.win, mem, gs, N, b.Y, b.pu, b.S);
+    if ((e = fft(b.pu, b.Gmax, false)) != cudaSuccess) return e;
+    k_var_phase<<<grid, 256, 0, st>>>(b.pu, b.sub, mem, gs, N, -1.f);
+    if ((e = fft(b.pu, b.Gmax, true)) != cudaSuccess) return e;
+    k_var_pum<<<grid_n(NN, 256), 256, 0, st>>>(b.pu, b.pobj, b.maxIllum, b.win, mem, gs, N, b.Y, b.pum);
+    if ((e = mls_lsq(b, b.vp, NN, mem, gs, st)) != cudaSuccess) return e;
+    if ((e = mls_solve_update(b, mem, gs, b.boxw + 4 * size_t(g), 0, st)) != cudaSuccess) return e;
+    if (flags & MLS_POSSEARCH) {
+      if ((e = cudaMemcpyAsync(b.aux, b.objp, GN * sizeof(float2), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+        return e;
+      if ((e = fft(b.aux, b.Gmax, false)) != cudaSuccess) return e;
+      k_var_grad<<<grid, 256, 0, st>>>(b.aux, b.Gmax, N);
+      if ((e = fft(b.aux, 2 * b.Gmax, true)) != cudaSuccess) return e;
+      k_var_possums<<<grid, 256, 0, st>>>(b.aux, b.vp, b.psi, gs, b.Gmax, N, b.vs + L.pos());
+      k_var_posupd<<<1, 32, 0, st>>>(b.vs + L.pos(), mem, gs, b.pos);
+    }
+    if (flags & MLS_VARUPD) {
+      k_var_proj<<<grid, 256, 0, st>>>(b.pu, b.pum, b.pobj, b.pmax, b.E, b.win, mem, gs, N, b.Y, b.vs + L.proj());
+      k_var_prj<<<1, 32, 0, st>>>(b.vs + L.proj(), b.vs + L.prj(), b.evo, P, mem, gs, NN);
+      k_var_upd<<<grid_n(NN, 256), 256, 0, st>>>(b.pu, b.pum, b.pobj, b.pmax, b.vs + L.prj(), b.win, mem, gs, N, b.Y,
+                                                  b.aux, sc + SC_USUM);
+      k_var_eapply<<<grid_n(NN, 256), 256, 0, st>>>(b.E, b.aux, NN, gs, P, sc + SC_USUM, sc + SC_ENEW);
+      k_var_enorm<<<grid_n(NN, 256), 256, 0, st>>>(b.E, NN, sc + SC_ENEW);
+      k_var_evosums<<<grid, 256, 0, st>>>(b.objp, b.E, b.probe, b.psi, gs, N, b.vs + L.evs());
+      k_var_evoupd<<<1, 32, 0, st>>>(b.vs + L.evs(), sc, b.evo, P, mem, gs, NN);
+    }
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace pty

@@ -6,7 +6,8 @@
 //   * objectNP/probeNP accept any complex or real dtype (the reference misreads complex64, src/ptychopy.c:383-471);
 //   * extra keywords: seed, calculateRMS, device, wave, returnResults, writeResults, outputDir, warmStart (trained
 //     warm-start network parameters, float32) and warmStartWidth (its width, default 16), precision (0 FP32 FFT,
-//     1 split-BF16 tensor-core FFT stages for MLs at 256 x 256);
+//     1 split-BF16 tensor-core FFT stages for MLs at 256 x 256), mlsCore (1: MLs without the reference's variable
+//     probe, sub-pixel shift and position search);
 //     probeNP may be (K, N, N) to supply all probe modes.
 // Whole-mode file ingest (fp, hdf5path), simulate mode and CLI strings (cmdstr) are outside this engine and raise
 // NotImplementedError.
@@ -62,7 +63,7 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
   int phaseConstraint = 1, updateProbe = 10, updateModes = 20, beamstopMask = 0, PPS = 20;
   double beamSize = 400e-9, stepx = 40e-9, stepy = 40e-9, lambd = 2.3843e-10, dx_d = 172e-6, z = 2.2, delta_p = 0.1;
   unsigned long long seed = out.p.seed;
-  int calculateRMS = 0, device = 0, wave = 0, precision = 0;
+  int calculateRMS = 0, device = 0, wave = 0, precision = 0, mlsCore = 0;
   static const char* kw_np[] = {"jobID", "diffractionNP", "positionNP", "objectNP", "probeNP", "fp", "fs",
                                 "hdf5path", "dpf", "beamSize", "probeGuess", "objectGuess", "size", "qx", "qy", "nx",
                                 "ny", "scanDimsx", "scanDimsy", "spiralScan", "flipScanAxis", "mirror1stScanAxis",
@@ -71,7 +72,7 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
                                 "binaryOutput", "simulate", "phaseConstraint", "updateProbe", "updateModes",
                                 "beamstopMask", "lf", "PPS", "seed", "calculateRMS", "device", "wave",
                                 "returnResults", "writeResults", "outputDir", "warmStart", "warmStartWidth",
-                                "precision", nullptr};
+                                "precision", "mlsCore", nullptr};
   static const char* kw_file[] = {"jobID", "fp", "fs", "hdf5path", "dpf", "beamSize", "probeGuess", "objectGuess",
                                   "size", "qx", "qy", "nx", "ny", "scanDimsx", "scanDimsy", "spiralScan",
                                   "flipScanAxis", "mirror1stScanAxis", "mirror2ndScanAxis", "stepx", "stepy",
@@ -82,13 +83,13 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
   int ok;
   if (np) {
     ok = PyArg_ParseTupleAndKeywords(
-        args, kw, "|sOOOOsisidssiiiiiiiiiiiddidddiiidiiiiiiiiiisiKiiiiisOii", const_cast<char**>(kw_np), &jobID,
+        args, kw, "|sOOOOsisidssiiiiiiiiiiiddidddiiidiiiiiiiiiisiKiiiiisOiii", const_cast<char**>(kw_np), &jobID,
         &out.diff, &out.pos, &out.obj, &out.probe, &fp, &fs, &hdf5path, &dpf, &beamSize, &probeGuess, &objectGuess,
         &size, &qx, &qy, &nx, &ny, &scanDimsx, &scanDimsy, &spiralScan, &flipScanAxis, &mirror1, &mirror2, &stepx,
         &stepy, &probeModes, &lambd, &dx_d, &z, &iter, &T, &jitter, &delta_p, &threshold, &rotate90, &sqrtData,
         &fftShiftData, &binaryOutput, &simulate, &phaseConstraint, &updateProbe, &updateModes, &beamstopMask, &lf,
         &PPS, &seed, &calculateRMS, &device, &wave, &out.returnResults, &out.writeResults, &out.outputDir, &out.warm,
-        &out.warmWidth, &precision);
+        &out.warmWidth, &precision, &mlsCore);
   } else {
     ok = PyArg_ParseTupleAndKeywords(args, kw, "|ssisidssiiiiiiiiiiiddidddiiidiiiiiiiiiisi",
                                      const_cast<char**>(kw_file), &jobID, &fp, &fs, &hdf5path, &dpf, &beamSize,
@@ -116,6 +117,7 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
   p.beamstopMask = beamstopMask; p.PPS = PPS; p.seed = seed; p.calculateRMS = calculateRMS; p.device = device;
   p.wave = wave;
   p.precision = precision;
+  p.mlsCore = mlsCore;
   return true;
 }
 

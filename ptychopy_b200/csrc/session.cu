@@ -8,6 +8,7 @@
 #include <fstream>
 #include <functional>
 #include <limits>
+#include <map>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -284,9 +285,15 @@ struct MlsTables {
 struct MlsState {
   MlsGeometry geo;
   DeviceBuf pobj, S, pum, objp, psi, work, starts, sums, errk, betas, err, norms, maxill, tcerr;
+  // the reference-default path: extra mode, evolution weights, positions, sub-pixel shifts, per-position probes and
+  // directions, gradient images, scratch sums, max of p_object
+  bool variable = false;
+  DeviceBuf E, evo, pos, pos_o, sub, vp, pu, aux, vs, pmax;
   int Gmax = 1, ng = 1;
   size_t table_ints = 0;
   MlsTables tab[2];
+  // the default path's graphs differ by iteration regime (MlsVarFlags): one per (table set, flags)
+  std::map<unsigned, cudaGraphExec_t> var_graphs;
   int64_t steps = 0;
   ~MlsState() {
     for (MlsTables& t : tab) {
@@ -294,8 +301,30 @@ struct MlsState {
       if (t.copied) cudaEventDestroy(t.copied);
       if (t.host) cudaFreeHost(t.host);
     }
+    for (auto& kv : var_graphs) cudaGraphExecDestroy(kv.second);
   }
 };
+
+// Seeded stand-ins for the reference's time-seeded draws of the MLs default path: curand uniforms for the extra
+// mode (initVarModes, src/Probe.cpp:497-505, d_initVarMOdes src/ProbeKernels.cu:99-110: r1 e^{2 pi i r2}, all r1
+// drawn before all r2) and normalRandom for the extra-mode weights (1e-6 N(0,1), src/Probe.cpp:520-525).  SplitMix64
+// from seed ^ 0x3C6EF372FE94F82B, u = (bits >> 11 + 0.5) 2^-53, Box-Muller's cos branch, one normal per pair.
+void mls_variable_draws(uint64_t seed, int N, int P, std::vector<float2>& E, std::vector<double>& evo1) {
+  uint64_t st = seed ^ 0x3C6EF372FE94F82Bull;
+  auto u = [&] { return (double(splitmix64(st) >> 11) + 0.5) * (1.0 / 9007199254740992.0); };
+  const size_t NN = size_t(N) * N;
+  std::vector<double> r1(NN), r2(NN);
+  for (auto& v : r1) v = u();
+  for (auto& v : r2) v = u();
+  E.resize(NN);
+  for (size_t i = 0; i < NN; ++i)
+    E[i] = make_float2(float(r1[i] * std::cos(2 * M_PI * r2[i])), float(r1[i] * std::sin(2 * M_PI * r2[i])));
+  evo1.resize(P);
+  for (auto& v : evo1) {
+    const double a = u(), b = u();
+    v = 1e-6 * (std::sqrt(-2.0 * std::log(a)) * std::cos(2 * M_PI * b));
+  }
+}
 
 }  // namespace pty
 
@@ -655,6 +684,11 @@ void init_mls(pty_session* s) {
     st[i] = make_int2(ml->geo.r0[i], ml->geo.c0[i]);
   }
   s->geo.pos.assign(raw.begin(), raw.end());
+  ml->variable = p.mlsCore == 0;
+  // remove_extra_degree re-centres the extra-mode weights of the first min(2, P) positions; with one position that
+  // zeroes its only weight and update_variable_probe then divides by zero
+  need(!ml->variable || P >= 2, "the MLs default path needs at least 2 positions (mlsCore=1 runs one)",
+       PTY_ERR_UNSUPPORTED);
   ml->starts.alloc(sizeof(int2) * P, "MLs starts");
   check_cuda(cudaMemcpyAsync(ml->starts.p, st.data(), sizeof(int2) * P, cudaMemcpyHostToDevice, s->stream), "H2D");
   // intensity sums (Diffractions::fillSquaredSums) then amplitudes = sqrt(I) (Diffractions::squaredRoot)
@@ -679,6 +713,28 @@ void init_mls(pty_session* s) {
                "H2D object");
   else
     check_cuda(fill_complex(s->obj.as<float2>(), XY, make_float2(1.f, 0.f), s->stream), "flat object");
+  std::vector<float2> Eh;
+  if (ml->variable) {
+    // initEvo (src/Probe.cpp:511-560): intensity weights 1; the extra mode to unit RMS, its weights carry the norm
+    std::vector<double> evo(2 * size_t(P), 1.0), evo1;
+    mls_variable_draws(p.seed, N, P, Eh, evo1);
+    double se = 0;
+    for (const float2& v : Eh) se += double(v.x) * v.x + double(v.y) * v.y;
+    const double rE = std::sqrt(se / double(NN));
+    for (float2& v : Eh) v = make_float2(float(v.x * (1.0 / rE)), float(v.y * (1.0 / rE)));
+    for (int i = 0; i < P; ++i) evo[P + i] = evo1[i] * rE;
+    ml->E.alloc(sizeof(float2) * NN, "extra probe mode");
+    ml->evo.alloc(sizeof(double) * 2 * P, "probe evolution");
+    ml->pos.alloc(sizeof(float) * 2 * P, "MLs positions");
+    ml->pos_o.alloc(sizeof(float) * 2 * P, "MLs original positions");
+    ml->sub.alloc(sizeof(float2) * P, "sub-pixel shifts");
+    check_cuda(cudaMemcpyAsync(ml->E.p, Eh.data(), ml->E.bytes, cudaMemcpyHostToDevice, s->stream), "H2D");
+    check_cuda(cudaMemcpyAsync(ml->evo.p, evo.data(), ml->evo.bytes, cudaMemcpyHostToDevice, s->stream), "H2D");
+    check_cuda(cudaMemcpyAsync(ml->pos.p, raw.data(), ml->pos.bytes, cudaMemcpyHostToDevice, s->stream), "H2D");
+    check_cuda(cudaMemcpyAsync(ml->pos_o.p, raw.data(), ml->pos_o.bytes, cudaMemcpyHostToDevice, s->stream), "H2D");
+    check_cuda(cudaMemsetAsync(ml->sub.p, 0, ml->sub.bytes, s->stream), "memset");
+    check_cuda(cudaStreamSynchronize(s->stream), "MLs set-up");  // Eh, evo and raw are host temporaries
+  }
   ml->pobj.alloc(sizeof(float) * XY, "illumination");
   ml->norms.alloc(2 * sizeof(double), "norm sums");
   ml->maxill.alloc(sizeof(float), "max illumination");
@@ -703,6 +759,7 @@ void init_mls(pty_session* s) {
   double corr = (P % 2) ? corrv[P / 2] : 0.5 * (corrv[P / 2 - 1] + corrv[P / 2]);
   corr = std::sqrt(corr * double(NN));
   check_cuda(scale_complex(s->probe.as<float2>(), NN, float(1.0 / corr), s->stream), "probe scale");
+  if (ml->variable) check_cuda(scale_complex(ml->E.as<float2>(), NN, float(1.0 / corr), s->stream), "extra mode scale");
   check_cuda(scale_real(ml->pobj.as<float>(), XY, float(1.0 / (corr * corr)), s->stream), "illumination scale");
   check_cuda(max_real(ml->pobj.as<float>(), XY, ml->maxill.as<float>(), s->stream), "MAX_ILLUM");
   // group buffers
@@ -713,7 +770,16 @@ void init_mls(pty_session* s) {
   ml->pum.alloc(sizeof(float2) * NN, "probe direction");
   ml->objp.alloc(sizeof(float2) * GN, "windows");
   ml->psi.alloc(sizeof(float2) * GN, "exit waves");
-  ml->work.alloc(sizeof(float2) * GN, "FFT work");
+  ml->work.alloc(sizeof(float2) * GN * (ml->variable ? 2 : 1), "FFT work");
+  if (ml->variable) {
+    ml->vp.alloc(sizeof(float2) * GN, "position probes");
+    ml->pu.alloc(sizeof(float2) * GN, "probe directions");
+    ml->aux.alloc(sizeof(float2) * 2 * GN, "gradient images");
+    ml->vs.alloc(sizeof(double) * mls_var_scratch_doubles(ml->Gmax), "MLs sums");
+    ml->pmax.alloc(sizeof(float), "illumination maximum");
+    for (DeviceBuf* b : {&ml->vp, &ml->pu, &ml->aux, &ml->vs})
+      check_cuda(cudaMemsetAsync(b->p, 0, b->bytes, s->stream), "memset");
+  }
   ml->table_ints = size_t(ml->ng) * ml->Gmax + 5 * size_t(ml->ng);
   for (MlsTables& t : ml->tab) {
     t.dev.alloc(sizeof(int) * ml->table_ints, "group tables");
@@ -763,6 +829,22 @@ MlsBuffers mls_buffers(pty_session* s, int parity) {
   b.beta_probe = 1.0 * 0.9;  // beta_probe * beta_LSQ
   b.tc = s->prm.precision ? 1 : 0;
   b.tc_err = ml->tcerr.as<int>();
+  if (ml->variable) {
+    b.E = ml->E.as<float2>();
+    b.evo = ml->evo.as<double>();
+    b.pos = ml->pos.as<float>();
+    b.pos_o = ml->pos_o.as<float>();
+    b.sub = ml->sub.as<float2>();
+    b.win = ml->starts.as<int2>();
+    b.boxw = const_cast<int*>(b.bbox);
+    b.vp = ml->vp.as<float2>();
+    b.pu = ml->pu.as<float2>();
+    b.aux = ml->aux.as<float2>();
+    b.vs = ml->vs.as<double>();
+    b.pmax = ml->pmax.as<float>();
+    b.cvx = std::ceil(float(s->X) * 1.0f / 2 - float(s->N) * 1.0f / 2);
+    b.cvy = std::ceil(float(s->Y) * 1.0f / 2 - float(s->N) * 1.0f / 2);
+  }
   return b;
 }
 
@@ -807,6 +889,34 @@ double step_mls(pty_session* s, bool want_err) {
              "H2D groups");
   check_cuda(cudaEventRecord(tb.copied, s->stream), "event");
   check_cuda(cudaMemsetAsync(ml->err.p, 0, sizeof(double), s->stream), "memset");
+  if (ml->variable) {
+    // iteration regime (src/MLS.cpp:86-89,99-102,470-475): windows at iteration 1 and from PPS, remove_extra_degree
+    // from 2, update_variable_probe from 3, position search from PPS
+    const int64_t it = ml->steps + 1;
+    const int pps = s->prm.PPS;
+    unsigned flags = 0;
+    if (it == 1 || it >= pps) flags |= MLS_WINDOWS;
+    if (it > 1) flags |= MLS_REMOVE;
+    if (it > 2) flags |= MLS_VARUPD;
+    if (it >= pps) flags |= MLS_POSSEARCH;
+    const unsigned key = unsigned(parity) | (flags << 1);
+    cudaGraphExec_t& ge = ml->var_graphs[key];
+    if (!ge) {
+      const MlsBuffers b = mls_buffers(s, parity);
+      cudaGraph_t graph = nullptr;
+      check_cuda(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+      const cudaError_t e = mls_iteration_var(b, ml->ng, flags, s->stream);
+      const cudaError_t e2 = cudaStreamEndCapture(s->stream, &graph);
+      check_cuda(e, "MLs capture");
+      check_cuda(e2, "end capture");
+      const cudaError_t e3 = cudaGraphInstantiate(&ge, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e3 != cudaSuccess) ml->var_graphs.erase(key);
+      check_cuda(e3, "graph instantiate");
+    }
+    check_cuda(cudaGraphLaunch(ge, s->stream), "MLs graph launch");
+    s->launches += mls_var_launches_per_iteration(ml->ng, flags);
+  } else {
   if (!tb.graph) {
     const MlsBuffers b = mls_buffers(s, parity);
     cudaGraph_t graph = nullptr;
@@ -821,6 +931,7 @@ double step_mls(pty_session* s, bool want_err) {
   }
   check_cuda(cudaGraphLaunch(tb.graph, s->stream), "MLs graph launch");
   s->launches += mls_launches_per_iteration(ml->ng);
+  }
   ++ml->steps;
   if (s->prm.precision) {  // the tensor-core FFT reports a wait timeout through its device flag
     int flag = 0;
@@ -1501,7 +1612,35 @@ int pty_get_positions(const pty_session* s, float* xy_px, int P) {
     need(s && xy_px, "null argument");
     need(s->initialized, "pty_init has not run", PTY_ERR_STATE);
     need(P == s->P, "position buffer length mismatch");
+    if (s->ml && s->ml->variable) {  // the refined positions
+      check_cuda(cudaSetDevice(s->dev), "cudaSetDevice");
+      check_cuda(cudaMemcpyAsync(xy_px, s->ml->pos.p, sizeof(float) * 2 * size_t(P), cudaMemcpyDeviceToHost,
+                                 s->stream),
+                 "D2H positions");
+      check_cuda(cudaStreamSynchronize(s->stream), "D2H positions");
+      return;
+    }
     std::memcpy(xy_px, s->geo.pos.data(), sizeof(float) * 2 * size_t(P));
+  });
+}
+
+int pty_get_mls_state(const pty_session* s, float* E_c64, double* evo0, double* evo1, int N, int P) {
+  return guarded([&] {
+    need(s != nullptr, "null argument");
+    need(s->initialized, "pty_init has not run", PTY_ERR_STATE);
+    need(s->ml && s->ml->variable, "no MLs default-path state (another algorithm, or mlsCore = 1)", PTY_ERR_STATE);
+    need(N == s->N && P == s->P, "buffer size mismatch");
+    check_cuda(cudaSetDevice(s->dev), "cudaSetDevice");
+    const size_t NN = size_t(N) * N;
+    if (E_c64)
+      check_cuda(cudaMemcpyAsync(E_c64, s->ml->E.p, sizeof(float2) * NN, cudaMemcpyDeviceToHost, s->stream), "D2H");
+    if (evo0)
+      check_cuda(cudaMemcpyAsync(evo0, s->ml->evo.p, sizeof(double) * P, cudaMemcpyDeviceToHost, s->stream), "D2H");
+    if (evo1)
+      check_cuda(cudaMemcpyAsync(evo1, s->ml->evo.as<double>() + P, sizeof(double) * P, cudaMemcpyDeviceToHost,
+                                 s->stream),
+                 "D2H");
+    check_cuda(cudaStreamSynchronize(s->stream), "D2H MLs state");
   });
 }
 

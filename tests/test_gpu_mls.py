@@ -1,6 +1,7 @@
-"""MLs core (LSQ-ML with random groups, one probe mode) on the GPU against the FP64 oracle.
+"""MLs (LSQ-ML with random groups, one probe mode) on the GPU against the FP64 oracle: the reference's default path
+(variable probe and intensity, sub-pixel probe shift, position search from PPS) and the fixed-probe core (mlsCore=1).
 
-Both sides start from the same intensities, probe, object and group stream (SplitMix64 seed).  Parity cases use
+Both sides start from the same intensities, probe, object, group stream and draws (SplitMix64 seed).  Parity cases use
 noise-free data consistent with the model (gpu_helpers.mls_dataset), where the iteration is well conditioned; the
 Poisson / flat-start case is chaotic in the reference algorithm itself (FFT round-off of near-zero Psi decides the
 phase the modulus step gives to non-zero data), so it is checked through the error metric only."""
@@ -15,10 +16,67 @@ TOL = 1e-4
 
 
 def _pair(oracle, d, **params):
-    s = gpu_session(dict(amp=d["intens"], kw=d["kw"]), probe=d["probe"], obj=d["obj"], calculateRMS=1, **params)
+    s = gpu_session(dict(amp=d["intens"], kw=d["kw"]), probe=d["probe"], obj=d["obj"], calculateRMS=1, mlsCore=1,
+                    **params)
     o = oracle.OracleMls(d["raw"], d["intens"], d["probe"], obj=d["obj"], delta_p=params.get("delta_p", 0.1),
                          seed=params.get("seed", 0x5EED5EED))
     return s, o
+
+
+def _pair_default(oracle, d, PPS, **params):
+    s = gpu_session(dict(amp=d["intens"], kw=d["kw"]), probe=d["probe"], obj=d["obj"], calculateRMS=1, PPS=PPS,
+                    **params)
+    o = oracle.OracleMls(d["raw"], d["intens"], d["probe"], obj=d["obj"], delta_p=params.get("delta_p", 0.1),
+                         seed=params.get("seed", 0x5EED5EED), variable=1, PPS=PPS)
+    return s, o
+
+
+def _check_default(s, o, what):
+    ob, pr, _ = o.state()
+    E, e0, e1, pos = o.variable_state()
+    gE, g0, g1 = s.mls_state()
+    assert rel_err(s.object(), ob) < TOL, f"object, {what}"
+    assert rel_err(s.probe(), pr) < TOL, f"probe, {what}"
+    # E moves only by steps built from the residuals of the probe directions (one per group: 484 steps after four
+    # iterations of 121 groups of one), so FP32 rounding of those residuals accumulates in it: bound 1e-3
+    assert rel_err(gE, E) < 1e-3, f"extra mode, {what}"
+    assert rel_err(g0, e0) < 1e-5, f"intensity weights, {what}"
+    # the extra-mode weights (~1e-6..1e-5) are sums of Re(chi conj(O E)) over the residual chi, which carries the FP32
+    # cancellation of a small difference of large terms: bound 1e-2 (their effect on the probes, E evo1, is ~1e-5 of P)
+    assert rel_err(g1, e1) < 1e-2, f"extra-mode weights, {what}"
+    assert np.abs(s.positions() - pos).max() < 1e-4, f"positions, {what}"
+    return pos
+
+
+@pytest.mark.parametrize("N,nx,PPS", [(64, 6, 3), (32, 11, 2), (128, 4, 3), (64, 2, 1)])
+def test_mls_default_path_matches_oracle(oracle, N, nx, PPS):
+    """The reference's default MLs path: windows and sub-pixel shifts from the positions, the shifted position
+    probes P evo0 + E evo1, the extra-mode and weight updates from iteration 3, the position search from PPS."""
+    d = mls_dataset(oracle, N=N, nx=nx, shifted=True)
+    s, o = _pair_default(oracle, d, PPS)
+    assert np.array_equal(s.positions(), d["raw"])
+    _check_default(s, o, "set-up")
+    for it in range(1, 6):
+        e = s.step()
+        eo = o.step()
+        pos = _check_default(s, o, f"iteration {it}")
+        assert abs(e - eo) <= 1e-3 * abs(eo), f"error, iteration {it}"
+        moved = np.abs(pos - d["raw"]).max()
+        if it < PPS:
+            assert moved == 0.0, "positions move only from PPS"
+    assert moved > 0.0
+    s.close()
+
+
+def test_mls_default_path_groups_of_several(oracle):
+    # 15x15 = 225 positions: groups of 2 and one of 1, delta_p 0.2, another seed; position search from iteration 2
+    d = mls_dataset(oracle, N=32, nx=15, seed=4, shifted=True)
+    s, o = _pair_default(oracle, d, 2, delta_p=0.2, seed=77)
+    for it in range(4):
+        s.step()
+        o.step()
+    _check_default(s, o, "iteration 4")
+    s.close()
 
 
 @pytest.mark.parametrize("N,nx", [(64, 6), (32, 11), (128, 4), (64, 2)])
@@ -55,13 +113,15 @@ def test_mls_flat_start_poisson_data(oracle):
     # Poisson data and a flat object: compare the Fourier-error trajectory, which is stable, and its decrease
     d = dataset(N=64, nx=8, algorithm="MLs")
     intens = (d["amp"].astype(np.float64) ** 2).astype(np.float32)
-    s = gpu_session(dict(d, amp=intens), probe=d["probe"], calculateRMS=1)
     raw = oracle.mls_raw_positions(8, 8, d["kw"]["stepx"], d["kw"]["stepy"], d["dx_s"])
-    o = oracle.OracleMls(raw, intens, d["probe"][0])
-    errs = [s.step() for _ in range(6)]
-    errs_o = [o.step() for _ in range(6)]
-    assert np.isfinite(errs).all() and errs[-1] < errs[0]
-    np.testing.assert_allclose(errs, errs_o, rtol=2e-2)
+    for core in (1, 0):
+        s = gpu_session(dict(d, amp=intens), probe=d["probe"], calculateRMS=1, mlsCore=core, PPS=4)
+        o = oracle.OracleMls(raw, intens, d["probe"][0], variable=1 - core, PPS=4)
+        errs = [s.step() for _ in range(6)]
+        errs_o = [o.step() for _ in range(6)]
+        assert np.isfinite(errs).all() and errs[-1] < errs[0]
+        np.testing.assert_allclose(errs, errs_o, rtol=2e-2)
+        s.close()
 
 
 def test_mls_tensor_core_fft_precision(oracle):
@@ -73,7 +133,7 @@ def test_mls_tensor_core_fft_precision(oracle):
     runs = {}
     for prec in (0, 1):
         runs[prec] = gpu_session(dict(amp=d["intens"], kw=d["kw"]), probe=d["probe"], obj=d["obj"], calculateRMS=1,
-                                 precision=prec)
+                                 precision=prec, mlsCore=1)
     o = oracle.OracleMls(d["raw"], d["intens"], d["probe"], obj=d["obj"])
     for _ in range(3):
         for s in runs.values():

@@ -179,6 +179,42 @@ def test_mls_oracle_reduces_the_fourier_error(oracle):
     assert np.isfinite(errs).all() and errs[-1] < 0.8 * errs[0]
 
 
+def test_mls_default_path_forward_model_matches_numpy_shift(oracle):
+    """The default MLs path shifts each position's probe by its sub-pixel remainder.  On data made with numpy's
+    Fourier-shift model (gpu_helpers.shifted_probe) it converges far below the same data without the shift in the
+    model (the core path), and below its own error on unshifted data: the shift's sign and axes match numpy's."""
+    from gpu_helpers import mls_dataset
+
+    res = {}
+    for shifted in (True, False):
+        d = mls_dataset(oracle, N=32, nx=6, shifted=shifted, pert=0.0)
+        for var in (1, 0):
+            m = oracle.OracleMls(d["raw"], d["intens"], d["probe"], obj=d["obj"], variable=var, PPS=100)
+            res[shifted, var] = [m.step() for _ in range(8)][-1]
+    assert res[True, 1] < 0.3 * res[True, 0], res
+    assert res[True, 1] < 0.3 * res[False, 1], res
+
+
+def test_mls_default_path_position_search_starts_at_pps(oracle):
+    from gpu_helpers import mls_dataset
+
+    d = mls_dataset(oracle, N=32, nx=5, shifted=True)
+    for pps in (3, 100):
+        m = oracle.OracleMls(d["raw"], d["intens"], d["probe"], obj=d["obj"], variable=1, PPS=pps)
+        moved = []
+        for _ in range(4):
+            m.step()
+            moved.append(float(np.abs(m.variable_state()[3] - d["raw"]).max()))
+        if pps == 3:
+            assert moved[0] == moved[1] == 0.0 and moved[2] > 0.0, moved
+            assert max(moved) < 0.2 * 4 * d["raw"].shape[0]  # at most 0.2 px per visit
+        else:
+            assert max(moved) == 0.0, moved
+        E, e0, e1, _ = m.variable_state()
+        assert abs(np.sqrt(np.mean(np.abs(E) ** 2)) - 1.0) < 1e-6  # unit-RMS extra mode after each update
+        assert np.isfinite(e0).all() and np.isfinite(e1).all()
+
+
 def test_spiral_mesh(oracle):
     lam, z, dxd, N = 2.48e-10, 1.0, 172e-6, 128
     dx_s = oracle.lib().orc_sample_pixel(lam, z, dxd, N)
