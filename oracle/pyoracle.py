@@ -240,6 +240,29 @@ def mls_geometry(raw_pos, N):
     return int(xy[0]), int(xy[1]), starts, roi
 
 
+def mls_zone_plate_probe(N, lambd, dx_s, beamSize):
+    """MLs probe start without a given probe, FP64: the zone-plate guess of Probe::initMLH (src/Probe.cpp:376-420,
+    d_initProbeMLH / d_endProbeMLH / d_shiftEnd, src/ProbeKernels.cu:220-360, h_initProbeMLH :592-628):
+    fftshift(FFT2(fftshift(kern)) * pf) with kern the apertured zone plate (outer radius D_FZP/2, central stop D_H/2)
+    times the Fresnel kernel to z = fl + beamSize, pf the detector-side phase, fl = 2 Rn dRn / lambda."""
+    Rn, dRn, D_FZP, D_H = 90e-6, 50e-9, 180e-6, 60e-6
+    fl = 2 * Rn * dRn / lambd
+    dx_fzp = lambd * fl / (N * dx_s)
+    k = 2 * np.pi / lambd
+    z = fl + beamSize
+    g = -dx_fzp * N / 2 + dx_fzp * N / (N - 1) * np.arange(N)
+    s2 = g[None, :] ** 2 + g[:, None] ** 2
+    r = np.sqrt(s2)
+    kern = ((r <= D_FZP / 2) & (r >= D_H / 2)) * np.exp(1j * (-2 / (lambd * 2 * fl) * np.pi) * s2) \
+        * np.exp(1j * (k / (2 * z)) * s2)
+    fu = lambd * (fl + beamSize) / dx_fzp
+    fs = fu / (N - 1)
+    i = np.arange(N)
+    lu = np.where(i < N // 2, -fu / 2 + fs * (N // 2) + fs * i, -fu / 2 + fs * (i - N // 2))
+    pf = np.exp(1j * k * z) * np.exp(1j * (k / (2 * z)) * (lu[None, :] ** 2 + lu[:, None] ** 2))
+    return np.fft.fftshift(np.fft.fft2(np.fft.fftshift(kern)) * pf)
+
+
 class OracleMls:
     """FP64 MLs (groups, preconditioned LSQ-ML, one probe mode), stepped one iteration at a time.  variable=1 is the
     reference's default path (variable probe and intensity, sub-pixel probe shift, position search from iteration

@@ -76,6 +76,9 @@ int mls_launches_per_iteration(int ngroups);
 cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, cudaStream_t st);
 int mls_var_launches_per_iteration(int ngroups, unsigned flags);
 size_t mls_var_scratch_doubles(int Gmax);
+// MLs probe start without a given probe: the zone-plate guess of initMLH (N x N into probe; pf and work N x N each).
+cudaError_t mls_zone_plate_probe(float2* probe, float2* pf, float2* work, const float2* tw, int N, double lambda,
+                                 double dx_recon, double beamSize, cudaStream_t st);
 // Kernels the two paths share (kernels_mls.cu).
 cudaError_t mls_group_boxes(const int2* starts, const int* members, const int* gsize, int ngroups, int Gmax, int N,
                             int* bbox, cudaStream_t st);

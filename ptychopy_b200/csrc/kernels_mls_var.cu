@@ -23,6 +23,8 @@
 //             extra-mode and intensity weights of the group's positions (update_variable_probe, src/Probe.cpp:1366-1516)
 // Scalar bookkeeping (2x2 solves, position and weight updates) runs in one thread on the device, so the iteration
 // is one CUDA graph with no host round trip.
+#include <cmath>
+
 #include "fft_core.cuh"
 #include "kernel_util.cuh"
 #include "kernels_mls.h"
@@ -390,6 +392,46 @@ __global__ void k_var_evoupd(double* __restrict__ s, double* __restrict__ sc, do
   sc[SC_ENEW] = 0.0;
 }
 
+// Zone-plate probe start (initMLH, src/Probe.cpp:376-420 with d_initProbeMLH, src/ProbeKernels.cu:220-315):
+// kern = C(r <= D_FZP/2) H(r >= D_H/2) e^{i lens r^2} e^{i kdz r^2} on the linspace(-dx N/2, dx N/2, N) grid of the
+// zone plate, written fftshifted; pf = e^{ikz} e^{i kdz (u^2 + v^2)} on the detector frequencies in ifftshifted order.
+// FP64 phases (the lens and propagation phases reach ~1e3 rad and nearly cancel).
+struct ZonePlate {
+  double start, step, lens, rC, rH, fu, startFU, fustep, kdz, kzc, kzs;
+};
+
+__global__ void k_fzp_start(float2* __restrict__ probe, float2* __restrict__ pf, int N, ZonePlate z) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    const int r = i / N, c = i % N;
+    const double x = z.start + z.step * c, y = z.start + z.step * r;
+    const double s2 = x * x + y * y, rad = sqrt(s2);
+    const double on = (rad <= z.rC ? 1.0 : 0.0) * (rad >= z.rH ? 1.0 : 0.0);
+    double s1, c1, s3, c3;
+    sincos(z.lens * s2, &s1, &c1);
+    sincos(z.kdz * s2, &s3, &c3);
+    const double kr = on * (c1 * c3 - s1 * s3), ki = on * (c1 * s3 + s1 * c3);
+    probe[size_t((r + N / 2) % N) * N + (c + N / 2) % N] = make_float2(float(kr), float(ki));
+    const double u = c < N / 2 ? z.startFU + z.fustep * c : -z.fu / 2 + z.fustep * (c - N / 2);
+    const double v = r < N / 2 ? z.startFU + z.fustep * r : -z.fu / 2 + z.fustep * (r - N / 2);
+    double sp, cp;
+    sincos(z.kdz * (u * u + v * v), &sp, &cp);
+    pf[i] = make_float2(float(z.kzc * cp - z.kzs * sp), float(z.kzc * sp + z.kzs * cp));
+  }
+}
+
+// pf = FFT2(kern) pf
+__global__ void k_fzp_mul(const float2* __restrict__ spec, float2* __restrict__ pf, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) pf[i] = cmul(spec[i], pf[i]);
+}
+
+// probe = fftshift(pf)
+__global__ void k_fzp_shift(const float2* __restrict__ pf, float2* __restrict__ probe, int N) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    const int r = i / N, c = i % N;
+    probe[size_t((r + N / 2) % N) * N + (c + N / 2) % N] = pf[i];
+  }
+}
+
 int grid_n(size_t n, int cap = 1184) {
   size_t g = (n + 255) / 256;
   return int(g < 1 ? 1 : (g > size_t(cap) ? cap : g));
@@ -398,6 +440,33 @@ int grid_n(size_t n, int cap = 1184) {
 }  // namespace
 
 size_t mls_var_scratch_doubles(int Gmax) { return 10 * size_t(Gmax) + 8; }
+
+cudaError_t mls_zone_plate_probe(float2* probe, float2* pf, float2* work, const float2* tw, int N, double lambda,
+                                 double dx_recon, double beamSize, cudaStream_t st) {
+  const double Rn = 90e-6, dRn = 50e-9, D_FZP = 180e-6, D_H = 60e-6;
+  const double fl = 2 * Rn * dRn / lambda;
+  const double dx_fzp = lambda * fl / (N * dx_recon);
+  const double k = 2 * M_PI / lambda, zz = fl + beamSize;
+  ZonePlate z;
+  z.step = dx_fzp * N / (N - 1);
+  z.start = -dx_fzp * N / 2;
+  z.lens = -2 / (lambda * 2 * fl) * M_PI;
+  z.rC = D_FZP / 2;
+  z.rH = D_H / 2;
+  z.fu = lambda * (fl + beamSize) / dx_fzp;
+  z.fustep = z.fu / (N - 1);
+  z.startFU = -z.fu / 2 + z.fustep * (N / 2);
+  z.kdz = k / (2 * zz);
+  z.kzc = std::cos(k * zz);
+  z.kzs = std::sin(k * zz);
+  const int NN = N * N;
+  k_fzp_start<<<grid_n(NN), 256, 0, st>>>(probe, pf, N, z);
+  cudaError_t e = fft2(probe, work, tw, 1, N, false, st);
+  if (e != cudaSuccess) return e;
+  k_fzp_mul<<<grid_n(NN), 256, 0, st>>>(probe, pf, NN);
+  k_fzp_shift<<<grid_n(NN), 256, 0, st>>>(pf, probe, N);
+  return cudaGetLastError();
+}
 
 int mls_var_launches_per_iteration(int ngroups, unsigned flags) {
   int pre = 2 + 3 + 1 + 3 + 2;  // windows?, boxes, norm (3 + E), recentre, illumination, max

@@ -698,13 +698,20 @@ void init_mls(pty_session* s) {
   std::vector<double> isum(P);
   check_cuda(cudaMemcpyAsync(isum.data(), sq.p, sizeof(double) * P, cudaMemcpyDeviceToHost, s->stream), "D2H");
   check_cuda(sqrt_inplace(s->amp.as<float>(), size_t(P) * NN, s->stream), "sqrt");
-  {
-    DeviceBuf avg;
-    if (p.probeGuess[0] == 0 && s->probe_h.empty()) {
-      avg.alloc(sizeof(float) * NN, "mean amplitude");
-      check_cuda(mean_amplitude(s->amp.as<float>(), P, N, avg.as<float>(), s->stream), "mean amplitude");
-    }
-    init_probe(s, avg.as<float>());
+  if (p.probeGuess[0] == 0 && s->probe_h.empty()) {
+    // no probe given: the zone-plate guess of initMLH (src/IPhaser.cpp:283-291, src/Probe.cpp:376-420)
+    s->probe.alloc(sizeof(float2) * NN, "probe");
+    s->pcache.alloc(sizeof(float) * NN, "probe cache");
+    check_cuda(cudaMemsetAsync(s->pcache.p, 0, s->pcache.bytes, s->stream), "memset probe cache");
+    DeviceBuf pf, work;
+    pf.alloc(sizeof(float2) * NN, "zone-plate propagator");
+    work.alloc(sizeof(float2) * NN, "fft work");
+    check_cuda(mls_zone_plate_probe(s->probe.as<float2>(), pf.as<float2>(), work.as<float2>(), s->tw.as<float2>(), N,
+                                    p.lambd, dx_s, p.beamSize, s->stream),
+               "zone-plate probe");
+    check_cuda(cudaStreamSynchronize(s->stream), "zone-plate probe");
+  } else {
+    init_probe(s, nullptr);
   }
   const size_t XY = size_t(s->X) * s->Y;
   s->obj.alloc(sizeof(float2) * XY, "object");

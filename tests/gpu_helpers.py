@@ -48,7 +48,7 @@ def shifted_probe(probe, sx, sy):
     return np.fft.ifft2(np.fft.fft2(probe) * np.exp(-2j * np.pi * (sx * f[None, :] + sy * f[:, None])))
 
 
-def mls_dataset(oracle, N=64, nx=5, step=40e-9, seed=3, pert=0.1, shifted=False):
+def mls_dataset(oracle, N=64, nx=5, step=40e-9, seed=3, pert=0.1, shifted=False, probe=None):
     """Noise-free MLs case on the ML mesh: intensities |FFT2(P O_true[window])|^2 at the ML window starts, the
     start object O_true with a smooth perturbation of relative size `pert`.  Data consistent with the model keep
     |Psi| far above FFT round-off wherever the data are non-zero, so FP32 and FP64 runs stay within round-off of each
@@ -61,7 +61,9 @@ def mls_dataset(oracle, N=64, nx=5, step=40e-9, seed=3, pert=0.1, shifted=False)
     raw = oracle.mls_raw_positions(nx, nx, step, step, dx_s)
     X, Y, starts, roi = oracle.mls_geometry(raw, N)
     o_true = synth.make_object(X, Y, rng, corr_px=4.0).astype(np.complex128)
-    probe = synth.make_probe(N, dx_s, K=1, fwhm=10 * dx_s)[0].astype(np.complex128)
+    if probe is None:
+        probe = synth.make_probe(N, dx_s, K=1, fwhm=10 * dx_s)[0]
+    probe = np.asarray(probe, np.complex128)
     if shifted:
         sx, sy = subpixel_shifts(raw, X, Y, N)
         intens = np.stack([np.abs(np.fft.fft2(shifted_probe(probe, sx[k], sy[k]) * o_true[r:r + N, c:c + N])) ** 2

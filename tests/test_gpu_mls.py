@@ -68,6 +68,26 @@ def test_mls_default_path_matches_oracle(oracle, N, nx, PPS):
     s.close()
 
 
+def test_mls_zone_plate_probe_start(oracle):
+    """No probe given: MLs starts from the zone-plate guess of initMLH (the ePIE paths use the mean-amplitude guess).
+    The data are made with that probe, so the run is consistent with its model."""
+    from ptychopy_b200 import synth
+
+    N, lambd = 64, 2.48e-10
+    dx_s = synth.sample_pixel(lambd, 1.0, 172e-6, N)
+    beam = 10 * dx_s
+    fzp = oracle.mls_zone_plate_probe(N, lambd, dx_s, beam)
+    d = mls_dataset(oracle, N=N, nx=5, shifted=True, probe=fzp / np.abs(fzp).max())
+    s = gpu_session(dict(amp=d["intens"], kw=d["kw"]), obj=d["obj"], calculateRMS=1, PPS=3)
+    o = oracle.OracleMls(d["raw"], d["intens"], fzp, obj=d["obj"], variable=1, PPS=3)
+    _check_default(s, o, "set-up")
+    for it in range(1, 4):
+        s.step()
+        o.step()
+        _check_default(s, o, f"iteration {it}")
+    s.close()
+
+
 def test_mls_default_path_groups_of_several(oracle):
     # 15x15 = 225 positions: groups of 2 and one of 1, delta_p 0.2, another seed; position search from iteration 2
     d = mls_dataset(oracle, N=32, nx=15, seed=4, shifted=True)
