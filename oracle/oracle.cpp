@@ -581,6 +581,8 @@ template <typename R> struct MlsState {
   bool variable = false;
   int PPS = 1 << 30;          // first iteration of the position search (probe_pos_search)
   int iter = 0;               // iterations done
+  int K = 1;                  // probe modes (default path only)
+  std::vector<cx<R>> Pk;      // modes 1..K-1, (K-1)*N*N (mode 0 is Pr)
   std::vector<cx<R>> E;       // extra probe mode (m_extramodes)
   std::vector<double> evo0, evo1;       // probe evolution: intensity and variable-mode weights per position
   std::vector<float> pos, pos_o, sub;   // 2*P: positions (x = rows), the originals, sub-pixel shifts (x = columns)
@@ -607,7 +609,10 @@ template <typename R> void mls_windows(MlsState<R>& s) {
 // src/Probe.cpp:497-505 with d_initVarMOdes, src/ProbeKernels.cu:99-110: r1 e^{2 pi i r2}, all r1 drawn before all
 // r2) and normalRandom for the variable-mode weights (1e-6 N(0,1), src/Probe.cpp:520-525).  SplitMix64 from
 // seed ^ 0x3C6EF372FE94F82B, u = (bits >> 11 + 0.5) 2^-53, Box-Muller cos branch, one normal per pair.
-void mls_variable_draws(uint64_t seed, int N, int P, std::vector<cx<double>>& E, std::vector<double>& evo1) {
+// With K > 1 probe modes, 2 (K - 1) normals for the modes' phase tilts (initMLH, src/Probe.cpp:422-431) are drawn
+// after the extra mode and before the weights.
+void mls_variable_draws(uint64_t seed, int N, int P, int K, std::vector<cx<double>>& E, std::vector<double>& tilts,
+                        std::vector<double>& evo1) {
   uint64_t st = seed ^ 0x3C6EF372FE94F82Bull;
   auto u = [&] { return (double(splitmix64(st) >> 11) + 0.5) * (1.0 / 9007199254740992.0); };
   const size_t NN = size_t(N) * N;
@@ -616,11 +621,144 @@ void mls_variable_draws(uint64_t seed, int N, int P, std::vector<cx<double>>& E,
   for (auto& v : r2) v = u();
   E.resize(NN);
   for (size_t i = 0; i < NN; ++i) E[i] = cx<double>(r1[i] * std::cos(2 * M_PI * r2[i]), r1[i] * std::sin(2 * M_PI * r2[i]));
-  evo1.resize(P);
-  for (auto& v : evo1) {
+  auto normal = [&] {
     const double a = u(), b = u();
-    v = 1e-6 * (std::sqrt(-2.0 * std::log(a)) * std::cos(2 * M_PI * b));
+    return std::sqrt(-2.0 * std::log(a)) * std::cos(2 * M_PI * b);
+  };
+  tilts.resize(2 * size_t(K > 1 ? K - 1 : 0));
+  for (auto& v : tilts) v = normal();
+  evo1.resize(P);
+  for (auto& v : evo1) v = 1e-6 * normal();
+}
+
+// Eigen-decomposition of a Hermitian K x K matrix (row-major) by cyclic complex Jacobi rotations, FP64.  Eigenpairs
+// in descending |eigenvalue|; each eigenvector (a column of V, unit norm) is turned so that its first component of at
+// least half the largest magnitude is real and positive (robust to the equal-magnitude components that equal-power
+// modes give).
+void hermitian_eigen(int K, std::vector<cx<double>> A, std::vector<double>& lam, std::vector<cx<double>>& V) {
+  V.assign(size_t(K) * K, cx<double>(0, 0));
+  for (int i = 0; i < K; ++i) V[size_t(i) * K + i] = 1;
+  double scale = 0;
+  for (const auto& v : A) scale += std::norm(v);
+  for (int sweep = 0; sweep < 64; ++sweep) {
+    double off = 0;
+    for (int p = 0; p < K; ++p)
+      for (int q = p + 1; q < K; ++q) off += std::norm(A[size_t(p) * K + q]);
+    if (off <= 1e-30 * scale) break;
+    for (int p = 0; p < K; ++p)
+      for (int q = p + 1; q < K; ++q) {
+        const cx<double> apq = A[size_t(p) * K + q];
+        const double m = std::abs(apq);
+        if (m == 0.0) continue;
+        const double app = A[size_t(p) * K + p].real(), aqq = A[size_t(q) * K + q].real();
+        const double th = 0.5 * std::atan2(2 * m, aqq - app);
+        const double c = std::cos(th), s = std::sin(th);
+        const cx<double> em = std::conj(apq) / m;  // e^{-i phi}
+        // A <- A G, G = [[c, s], [-s e^{-i phi}, c e^{-i phi}]] on columns p, q; then A <- G^H A; V <- V G
+        for (int k = 0; k < K; ++k) {
+          const cx<double> x = A[size_t(k) * K + p], y = A[size_t(k) * K + q];
+          A[size_t(k) * K + p] = c * x - s * em * y;
+          A[size_t(k) * K + q] = s * x + c * em * y;
+          const cx<double> vx = V[size_t(k) * K + p], vy = V[size_t(k) * K + q];
+          V[size_t(k) * K + p] = c * vx - s * em * vy;
+          V[size_t(k) * K + q] = s * vx + c * em * vy;
+        }
+        for (int k = 0; k < K; ++k) {
+          const cx<double> x = A[size_t(p) * K + k], y = A[size_t(q) * K + k];
+          A[size_t(p) * K + k] = c * x - s * std::conj(em) * y;
+          A[size_t(q) * K + k] = s * x + c * std::conj(em) * y;
+        }
+      }
   }
+  std::vector<int> idx(K);
+  for (int i = 0; i < K; ++i) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+    return std::abs(A[size_t(x) * K + x].real()) > std::abs(A[size_t(y) * K + y].real());
+  });
+  std::vector<cx<double>> W(size_t(K) * K);
+  lam.resize(K);
+  for (int j = 0; j < K; ++j) {
+    const int c = idx[j];
+    lam[j] = A[size_t(c) * K + c].real();
+    double mx = 0;
+    for (int k = 0; k < K; ++k) mx = std::max(mx, std::abs(V[size_t(k) * K + c]));
+    int best = 0;
+    while (best < K - 1 && std::abs(V[size_t(best) * K + c]) < 0.5 * mx) ++best;
+    const cx<double> v = V[size_t(best) * K + c];
+    const cx<double> ph = std::abs(v) > 0 ? std::conj(v) / std::abs(v) : cx<double>(1, 0);
+    for (int k = 0; k < K; ++k) W[size_t(k) * K + j] = V[size_t(k) * K + c] * ph;
+  }
+  V = W;
+}
+
+// The MLs probe modes 1..K-1 (initMLH, src/Probe.cpp:422-490): mode 0 times the phase tilt
+// e^{-2 pi i (t1 (c/N - 0.5) + t2 (r/N - 0.5))} (h_initVarProbe: fftshift, d_imshift_fft, fftshift back), then the
+// modes are recombined by the eigenvectors of their Gram matrix G_ij = sum conj(m_i) m_j, in descending eigenvalue
+// order (the reference's assignment m[sigma(i)] = combination i equals this when its eigen solver returns descending
+// order; eigenvector phases are pinned by hermitian_eigen's convention).
+template <typename R> void mls_init_modes(MlsState<R>& s, const std::vector<double>& tilts) {
+  const int N = s.N, K = s.K;
+  const size_t NN = size_t(N) * N;
+  std::vector<std::vector<cx<R>>> m(K, std::vector<cx<R>>(NN));
+  m[0] = s.Pr;
+  for (int k = 1; k < K; ++k) {
+    const double t1 = double(float(tilts[2 * (k - 1)])), t2 = double(float(tilts[2 * (k - 1) + 1]));
+    for (int r = 0; r < N; ++r)
+      for (int c = 0; c < N; ++c) {
+        const double ph = -2 * M_PI * (t1 * (double(c) / N - 0.5) + t2 * (double(r) / N - 0.5));
+        m[k][size_t(r) * N + c] = s.Pr[size_t(r) * N + c] * cx<R>(R(std::cos(ph)), R(std::sin(ph)));
+      }
+  }
+  std::vector<cx<double>> G(size_t(K) * K);
+  for (int i = 0; i < K; ++i)
+    for (int j = 0; j < K; ++j) {
+      cx<double> acc(0, 0);
+      for (size_t p = 0; p < NN; ++p) acc += std::conj(cx<double>(m[i][p])) * cx<double>(m[j][p]);
+      G[size_t(i) * K + j] = acc;
+    }
+  std::vector<double> lam;
+  std::vector<cx<double>> V;
+  hermitian_eigen(K, G, lam, V);
+  std::vector<std::vector<cx<R>>> out(K, std::vector<cx<R>>(NN, cx<R>(0, 0)));
+  for (int i = 0; i < K; ++i)
+    for (int q = 0; q < K; ++q) {
+      const cx<R> v(R(V[size_t(q) * K + i].real()), R(V[size_t(q) * K + i].imag()));
+      for (size_t p = 0; p < NN; ++p) out[i][p] += m[q][p] * v;
+    }
+  s.Pr = out[0];
+  s.Pk.resize(size_t(K - 1) * NN);
+  for (int k = 1; k < K; ++k) std::copy(out[k].begin(), out[k].end(), s.Pk.begin() + size_t(k - 1) * NN);
+}
+
+// ortho_modes (src/Probe.cpp:244-294), run after each iteration when K > 1: Gram-Schmidt in mode order (each mode
+// minus its projections on the already orthogonalised earlier ones), then modes 1..K-1 are replaced by the modes
+// ranked 1..K-1 by their power before the Gram-Schmidt; mode 0 is never replaced, as written.
+template <typename R> void mls_ortho_modes(MlsState<R>& s) {
+  const int K = s.K;
+  const size_t NN = size_t(s.N) * s.N;
+  auto mode = [&](int k) { return k == 0 ? s.Pr.data() : s.Pk.data() + size_t(k - 1) * NN; };
+  std::vector<std::pair<double, int>> rank;
+  for (int i = 0; i < K; ++i) {
+    double pw = 0;
+    for (size_t p = 0; p < NN; ++p) pw += std::norm(mode(i)[p]);
+    rank.push_back({-pw, i});
+    for (int j = 0; j < i; ++j) {
+      double nj = 0;
+      cx<double> sl(0, 0);
+      for (size_t p = 0; p < NN; ++p) {
+        nj += std::norm(mode(j)[p]);
+        sl += cx<double>(mode(i)[p] * std::conj(mode(j)[p]));
+      }
+      const cx<R> pr(R(sl.real() / nj), R(sl.imag() / nj));
+      for (size_t p = 0; p < NN; ++p) mode(i)[p] -= pr * mode(j)[p];
+    }
+  }
+  std::sort(rank.begin(), rank.end());
+  std::vector<cx<R>> all(s.Pr);
+  all.insert(all.end(), s.Pk.begin(), s.Pk.end());
+  for (int i = 1; i < K; ++i)
+    std::copy(all.begin() + size_t(rank[i].second) * NN, all.begin() + size_t(rank[i].second + 1) * NN,
+              s.Pk.begin() + size_t(i - 1) * NN);
 }
 
 // FFT frequency grid of the sub-pixel shift and the position gradient: fftshift(k/N - 0.5) (src/Probe.cpp:92-121),
@@ -673,6 +811,7 @@ template <typename R> void mls_setup(MlsState<R>& s, const std::vector<double>& 
   for (auto& v : s.O) v *= R(1) / onorm;
   double sp = 0;
   for (size_t i = 0; i < NN; ++i) sp += std::norm(s.Pr[i]);
+  for (const auto& v : s.Pk) sp += std::norm(v);  // the mean illumination counts every mode
   const double meanillum = sp / double(NN);
   std::vector<double> corrv;
   for (int i = 0; i < s.P; ++i) corrv.push_back(meanillum / (intensitySums[i] / double(NN)));
@@ -681,11 +820,16 @@ template <typename R> void mls_setup(MlsState<R>& s, const std::vector<double>& 
   double corr = (n % 2) ? corrv[n / 2] : 0.5 * (corrv[n / 2 - 1] + corrv[n / 2]);
   corr = std::sqrt(corr * double(NN));
   for (auto& v : s.Pr) v *= R(1.0 / corr);
+  for (auto& v : s.Pk) v *= R(1.0 / corr);
   for (auto& v : s.E) v *= R(1.0 / corr);
   s.pobj = illum;
   for (auto& v : s.pobj) v /= R(corr * corr);
   s.maxIllum = *std::max_element(s.pobj.begin(), s.pobj.end());
 }
+
+template <typename R>
+void mls_mode_updates(MlsState<R>& s, const std::vector<int>& g, const std::vector<std::vector<cx<R>>>& op,
+                      const std::vector<std::vector<std::vector<cx<R>>>>& chm, cx<R> bpr);
 
 template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool want_err) {
   const int N = s.N, X = s.geo.X, Y = s.geo.Y;
@@ -705,6 +849,7 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
       }
     const R on = sw > 0 ? R(std::sqrt(swo) / std::sqrt(sw)) : R(1);  // empty / unlit ROI: no rescale
     for (auto& v : s.Pr) v *= on;
+    for (auto& v : s.Pk) v *= on;
     for (auto& v : s.E) v *= on;
     for (auto& v : s.O) v *= R(1) / on;
   }
@@ -760,6 +905,7 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
     const int G = int(g.size());
     std::vector<std::vector<cx<R>>> op(G, std::vector<cx<R>>(NN)), chi(G, std::vector<cx<R>>(NN)),
         vp(G, std::vector<cx<R>>(NN)), pu(G, std::vector<cx<R>>(NN));
+    std::vector<std::vector<std::vector<cx<R>>>> chm(s.K - 1, std::vector<std::vector<cx<R>>>(G, std::vector<cx<R>>(NN)));
     for (int k = 0; k < G; ++k) {
       const int j = g[k];
       // get_illumination_probe (src/Probe.cpp:887-954): the position's probe P evo0 + E evo1, sub-pixel shifted
@@ -773,16 +919,30 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
           chi[k][p] = vp[k][p] * op[k][p];
         }
       fft2(f, chi[k].data(), false, scr);
+      for (int m = 1; m < s.K; ++m) {  // the other modes' exit waves, unshifted (get_illumination_probe)
+        auto& c = chm[m - 1][k];
+        const cx<R>* Pm = s.Pk.data() + size_t(m - 1) * NN;
+        for (size_t p = 0; p < NN; ++p) c[p] = Pm[p] * op[k][p];
+        fft2(f, c.data(), false, scr);
+      }
       const R* A = &s.A[size_t(j) * NN];
       double e = 0;
       for (size_t p = 0; p < NN; ++p) {  // modulus_constraint, R = A/(|Psi|+1e-9) - 1 (src/Diffractions.cpp:281-310)
-        const R ap = std::abs(chi[k][p]);
+        R a2 = std::norm(chi[k][p]);
+        for (int m = 1; m < s.K; ++m) a2 += std::norm(chm[m - 1][k][p]);
+        const R ap = s.K > 1 ? std::sqrt(a2) : std::abs(chi[k][p]);
         e += double(A[p] - ap) * double(A[p] - ap) * 0.25;
-        chi[k][p] *= (A[p] / (ap + R(1e-9)) - R(1));
+        const R rr = A[p] / (ap + R(1e-9)) - R(1);
+        chi[k][p] *= rr;
+        for (int m = 1; m < s.K; ++m) chm[m - 1][k][p] *= rr;
       }
       errsum += std::sqrt(e / double(NN));
       fft2(f, chi[k].data(), true, scr);
       for (auto& v : chi[k]) v *= nrm;
+      for (int m = 1; m < s.K; ++m) {
+        fft2(f, chm[m - 1][k].data(), true, scr);
+        for (auto& v : chm[m - 1][k]) v *= nrm;
+      }
       // probe direction of this window, shifted back by the sub-pixel remainder (src/MLS.cpp:232-240)
       for (size_t p = 0; p < NN; ++p) pu[k][p] = chi[k][p] * std::conj(op[k][p]);
       if (var) mls_shift(f, pu[k].data(), -double(s.sub[2 * j]), -double(s.sub[2 * j + 1]), scr);
@@ -849,8 +1009,7 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
     for (size_t i = 0; i < XY; ++i)
       if (S[i] != cx<R>(0, 0)) s.O[i] += bor * (S[i] / (s.pobj[i] + dmax));
     for (size_t p = 0; p < NN; ++p) s.Pr[p] += bpr * pum[p];
-    if (!var) continue;
-    if (iter >= s.PPS) {
+    if (var && iter >= s.PPS) {
       // gradient_position_solver (src/Probe.cpp:956-1118): object gradients by the Fourier derivative, a least-
       // squares shift per window clamped to 0.2 px.  The column-direction gradient (dX, the column frequency grid)
       // moves the position's x (the row coordinate) and the row-direction one its y, as the reference pairs them.
@@ -882,7 +1041,7 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
         s.pos[2 * j + 1] = float(s.pos[2 * j + 1] + shy);
       }
     }
-    if (iter > 2) {
+    if (var && iter > 2) {
       // update_variable_probe (src/Probe.cpp:1366-1516): one SVD-like step of the extra mode on the weighted
       // residual of the probe directions, then the variable-mode and intensity weights of the group's positions
       const double relaxU = double(G) / s.P;
@@ -932,8 +1091,33 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
         s.evo0[g[k]] += 0.1 * nI[k] / dI[k];
       }
     }
+    if (s.K > 1) mls_mode_updates(s, g, op, chm, bpr);
   }
+  if (s.K > 1) mls_ortho_modes(s);
   return want_err ? errsum / s.P : 0.0;
+}
+
+// ll = 2..K of MLS::iteration's mode loop for one group (src/MLS.cpp:241-285,465-469): mode m's direction
+// mean_j W chi_m conj(obj_proj) (no sub-pixel shift, no object step) with the group's LSQ probe step.
+template <typename R>
+void mls_mode_updates(MlsState<R>& s, const std::vector<int>& g, const std::vector<std::vector<cx<R>>>& op,
+                      const std::vector<std::vector<std::vector<cx<R>>>>& chm, cx<R> bpr) {
+  const int N = s.N, Y = s.geo.Y, G = int(g.size());
+  const size_t NN = size_t(N) * N;
+  for (int m = 1; m < s.K; ++m) {
+    std::vector<cx<R>> pm(NN, cx<R>(0, 0));
+    for (int k = 0; k < G; ++k) {
+      const int j = g[k];
+      for (int x = 0; x < N; ++x)
+        for (int y = 0; y < N; ++y) {
+          const size_t p = size_t(x) * N + y;
+          const R w0 = s.pobj[size_t(s.geo.r0[j] + x) * Y + (s.geo.c0[j] + y)];
+          pm[p] += chm[m - 1][k][p] * std::conj(op[k][p]) * (w0 / (w0 + s.maxIllum * R(0.01)));
+        }
+    }
+    cx<R>* Pm = s.Pk.data() + size_t(m - 1) * NN;
+    for (size_t p = 0; p < NN; ++p) Pm[p] += bpr * (pm[p] * R(1.0 / G));
+  }
 }
 
 // Position jitter (d_generateMesh, src/ScanMeshKernels.cu:53-60: jitter = r - u*2r per axis, u uniform in (0,1]
@@ -1285,16 +1469,19 @@ struct OrcMls {
 
 // variable: the reference-default path (variable probe and intensity, sub-pixel shift, position search from
 // iteration pps); 0 = the fixed-probe core.  The variable path's draws come from `seed` (mls_variable_draws).
+// probe: K modes of N*N complex (K > 1 only on the variable path; modes 1..K-1 are initialised from mode 0).
 void* orc_mls_create(const float* raw_pos, int P, int N, const double* intens, const double* probe, const double* obj,
-                     uint64_t seed, double delta_p, int variable, int pps) {
+                     uint64_t seed, double delta_p, int variable, int pps, int K) {
   auto* h = new OrcMls;
   std::vector<float> raw(raw_pos, raw_pos + 2 * size_t(P));
   h->s.geo = mls_geometry(raw, P, N);
   h->s.N = N; h->s.P = P; h->s.delta_p = delta_p;
   h->s.variable = variable != 0;
   h->s.PPS = pps;
+  std::vector<double> tilts;
+  h->s.K = h->s.variable ? std::max(1, K) : 1;
   if (h->s.variable) {
-    mls_variable_draws(seed, N, P, h->s.E, h->s.evo1);
+    mls_variable_draws(seed, N, P, h->s.K, h->s.E, tilts, h->s.evo1);
     h->s.pos = raw;
     h->s.pos_o = raw;
     h->s.sub.assign(2 * size_t(P), 0.f);
@@ -1310,6 +1497,7 @@ void* orc_mls_create(const float* raw_pos, int P, int N, const double* intens, c
     }
   h->s.Pr.resize(NN);
   for (size_t p = 0; p < NN; ++p) h->s.Pr[p] = cx<double>(probe[2 * p], probe[2 * p + 1]);
+  if (h->s.K > 1) mls_init_modes(h->s, tilts);
   h->s.O.assign(XY, cx<double>(1, 0));
   if (obj)
     for (size_t i = 0; i < XY; ++i) h->s.O[i] = cx<double>(obj[2 * i], obj[2 * i + 1]);
@@ -1331,6 +1519,10 @@ int orc_mls_get(void* hp, double* obj, double* probe, double* scalars) {
   for (size_t i = 0; i < h->s.Pr.size(); ++i) {
     probe[2 * i] = h->s.Pr[i].real();
     probe[2 * i + 1] = h->s.Pr[i].imag();
+  }
+  for (size_t i = 0; i < h->s.Pk.size(); ++i) {  // modes 1..K-1 follow mode 0
+    probe[2 * (h->s.Pr.size() + i)] = h->s.Pk[i].real();
+    probe[2 * (h->s.Pr.size() + i) + 1] = h->s.Pk[i].imag();
   }
   if (scalars) scalars[0] = h->s.maxIllum;
   return 0;

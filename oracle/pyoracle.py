@@ -56,7 +56,7 @@ def lib():
             "orc_destroy": ([vp], None),
             "orc_dm_baseline_f32": ([i, i, i, i, vp, vp, vp, i, i, vp], d),
             "orc_mls_geometry": ([vp, i, i, vp, vp, vp], i),
-            "orc_mls_create": ([vp, i, i, vp, vp, vp, u64, d, i, i], vp),
+            "orc_mls_create": ([vp, i, i, vp, vp, vp, u64, d, i, i, i], vp),
             "orc_mls_get_var": ([vp, vp, vp, vp, vp], i),
             "orc_mls_step": ([vp, ctypes.POINTER(d)], i),
             "orc_mls_get": ([vp, vp, vp, vp], i),
@@ -268,16 +268,17 @@ class OracleMls:
     reference's default path (variable probe and intensity, sub-pixel probe shift, position search from iteration
     PPS); variable=0 the fixed-probe core."""
 
-    def __init__(self, raw_pos, intens, probe, obj=None, seed=0x5EED5EED, delta_p=0.1, variable=0, PPS=20):
+    def __init__(self, raw_pos, intens, probe, obj=None, seed=0x5EED5EED, delta_p=0.1, variable=0, PPS=20, K=1):
         self.raw = np.ascontiguousarray(raw_pos, np.float32)
         self.I = np.ascontiguousarray(intens, np.float64)
         self.P, self.N = self.I.shape[0], self.I.shape[1]
         self.X, self.Y, self.starts, self.roi = mls_geometry(self.raw, self.N)
-        pr = np.ascontiguousarray(np.asarray(probe).reshape(self.N, self.N), np.complex128)
+        pr = np.ascontiguousarray(np.asarray(probe).reshape(-1, self.N, self.N)[0], np.complex128)  # mode 0
         o = None if obj is None else np.ascontiguousarray(obj, np.complex128)
         self.variable = int(variable)
+        self.K = int(K) if self.variable else 1
         self.h = lib().orc_mls_create(_p(self.raw), self.P, self.N, _p(self.I), _p(pr),
-                                      _p(o) if o is not None else None, seed, delta_p, self.variable, int(PPS))
+                                      _p(o) if o is not None else None, seed, delta_p, self.variable, int(PPS), self.K)
 
     def step(self):
         e = ctypes.c_double(0)
@@ -286,10 +287,10 @@ class OracleMls:
 
     def state(self):
         o = np.zeros((self.X, self.Y), np.complex128)
-        p = np.zeros((self.N, self.N), np.complex128)
+        p = np.zeros((self.K, self.N, self.N), np.complex128)
         sc = np.zeros(1)
         lib().orc_mls_get(self.h, _p(o), _p(p), _p(sc))
-        return o, p, sc
+        return o, (p[0] if self.K == 1 else p), sc
 
     def variable_state(self):
         """(E, evo0, evo1, positions) of the variable path."""

@@ -50,6 +50,9 @@ struct MlsBuffers {
   double* vs;             // scratch sums (mls_var_scratch_doubles(Gmax))
   float* pmax;            // max of p_object in this iteration
   float cvx, cvy;         // ceil(X/2 - N/2), ceil(Y/2 - N/2)
+  int K;                  // probe modes (probe holds K x N x N)
+  float2* psik;           // (K-1) x Gmax x N x N exit waves of modes 1..K-1
+  float2* mtmp;           // K x N x N scratch of the mode orthogonalisation
 };
 
 // Parts of one iteration of the reference-default path that depend on the iteration number.
@@ -75,7 +78,14 @@ int mls_launches_per_iteration(int ngroups);
 // One iteration of the reference-default path (kernels_mls_var.cu); flags from MlsVarFlags.
 cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, cudaStream_t st);
 int mls_var_launches_per_iteration(int ngroups, unsigned flags);
+int mls_var_mode_launches(int ngroups, int K);
 size_t mls_var_scratch_doubles(int Gmax);
+// MLs probe modes 1..K-1 from mode 0 (initMLH): phase tilts (2 (K-1) values, device), then the Gram matrix
+// G_ij = sum conj(m_i) m_j (K x K double2, device) for the host's eigen-decomposition, then modes <- modes V
+// (V: K x K double2 on the device, column i = combination i); tmp holds K x N x N.
+cudaError_t mls_mode_tilts(float2* probe, int K, int N, const double* tilts, cudaStream_t st);
+cudaError_t mls_mode_gram(const float2* probe, int K, int N, double2* gram, cudaStream_t st);
+cudaError_t mls_mode_combine(float2* probe, float2* tmp, int K, int N, const double2* V, cudaStream_t st);
 // MLs probe start without a given probe: the zone-plate guess of initMLH (N x N into probe; pf and work N x N each).
 cudaError_t mls_zone_plate_probe(float2* probe, float2* pf, float2* work, const float2* tw, int N, double lambda,
                                  double dx_recon, double beamSize, cudaStream_t st);

@@ -432,6 +432,163 @@ __global__ void k_fzp_shift(const float2* __restrict__ pf, float2* __restrict__ 
   }
 }
 
+// Exit waves of modes 1..K-1: psik[m-1][k] = P_m objp_k
+__global__ void k_var_psik(const float2* __restrict__ probe, const float2* __restrict__ objp, float2* __restrict__ psik,
+                           int K, int Gmax, size_t NN) {
+  const size_t n = size_t(K - 1) * Gmax * NN;
+  for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < n; t += size_t(gridDim.x) * blockDim.x) {
+    const size_t i = t % NN, k = (t / NN) % Gmax, m = t / (NN * Gmax) + 1;
+    psik[t] = cmul(probe[m * NN + i], objp[k * NN + i]);
+  }
+}
+
+// Modal modulus: |Psi| = sqrt(sum_m |Psi_m|^2) over all modes, every mode scaled by (A/(|Psi| + 1e-9) - 1)/N^2,
+// Fourier error from |Psi| (modulus_constraint, get_fourier_error)
+__global__ void k_var_modulus(float2* __restrict__ spec, float2* __restrict__ psik, const float* __restrict__ amp,
+                              const int* __restrict__ members, const int* __restrict__ gsize, int N, int K, int Gmax,
+                              double* __restrict__ err) {
+  const int k = blockIdx.y;
+  if (k >= *gsize) return;
+  const size_t NN = size_t(N) * N, GN = size_t(Gmax) * NN;
+  const float* A = amp + size_t(members[k]) * NN;
+  const float nrm = 1.f / float(NN);
+  double e = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    const float2 v = spec[k * NN + i];
+    float a2 = v.x * v.x + v.y * v.y;
+    for (int m = 0; m < K - 1; ++m) {
+      const float2 w = psik[m * GN + k * NN + i];
+      a2 += w.x * w.x + w.y * w.y;
+    }
+    const float ap = sqrtf(a2);
+    const float a = A[i];
+    e += double(a - ap) * double(a - ap) * 0.25;
+    const float r = (a / (ap + 1e-9f) - 1.f) * nrm;
+    spec[k * NN + i] = cscale(v, r);
+    for (int m = 0; m < K - 1; ++m) psik[m * GN + k * NN + i] = cscale(psik[m * GN + k * NN + i], r);
+  }
+  e = block_reduce_sum(e);
+  if (threadIdx.x == 0) atomicAdd(&err[k], e);
+}
+
+// Mode m >= 1: P_m += beta_p mean_j W chi_m,j conj(objp_j) (no sub-pixel shift for modes past the first)
+__global__ void k_var_mode_update(const float2* __restrict__ chim, const float2* __restrict__ objp,
+                                  const float* __restrict__ pobj, const float* __restrict__ maxIllum,
+                                  const int2* __restrict__ win, const int* __restrict__ members,
+                                  const int* __restrict__ gsize, int N, int Y, const double* __restrict__ betas,
+                                  float2* __restrict__ mode) {
+  const int G = *gsize;
+  const size_t NN = size_t(N) * N;
+  const float damp = 0.01f * *maxIllum, invG = 1.f / float(G);
+  const float2 b = make_float2(float(betas[2]), float(betas[3]));
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    float2 acc = make_float2(0.f, 0.f);
+    for (int k = 0; k < G; ++k) {
+      const int2 s = win[members[k]];
+      const float w = pobj[size_t(s.x + i / N) * Y + (s.y + i % N)];
+      acc = cadd(acc, cscale(cmulc(chim[k * NN + i], objp[k * NN + i]), w / (w + damp)));
+    }
+    mode[i] = cadd(mode[i], cmul(b, cscale(acc, invG)));
+  }
+}
+
+// ortho_modes (src/Probe.cpp:244-294) in one block: Gram-Schmidt in mode order with powers taken before each mode's
+// projections, then modes 1..K-1 take the modes ranked 1..K-1 by that power (mode 0 stays, as written)
+__global__ void k_var_ortho(float2* __restrict__ modes, float2* __restrict__ tmp, int K, int NN) {
+  __shared__ double pw[64];
+  __shared__ float2 proj;
+  __shared__ int rank[64];
+  for (int i = 0; i < K; ++i) {
+    float2* mi = modes + size_t(i) * NN;
+    double p = 0;
+    for (int t = threadIdx.x; t < NN; t += blockDim.x) p += double(mi[t].x) * mi[t].x + double(mi[t].y) * mi[t].y;
+    p = block_reduce_sum(p);
+    if (threadIdx.x == 0) pw[i] = p;
+    __syncthreads();
+    for (int j = 0; j < i; ++j) {
+      const float2* mj = modes + size_t(j) * NN;
+      double nj = 0, sr = 0, si = 0;
+      for (int t = threadIdx.x; t < NN; t += blockDim.x) {
+        const float2 a = mi[t], b = mj[t];
+        nj += double(b.x) * b.x + double(b.y) * b.y;
+        sr += double(a.x) * b.x + double(a.y) * b.y;  // a conj(b)
+        si += double(a.y) * b.x - double(a.x) * b.y;
+      }
+      nj = block_reduce_sum(nj);
+      __syncthreads();
+      sr = block_reduce_sum(sr);
+      __syncthreads();
+      si = block_reduce_sum(si);
+      if (threadIdx.x == 0) proj = make_float2(float(sr / nj), float(si / nj));
+      __syncthreads();
+      const float2 pr = proj;
+      for (int t = threadIdx.x; t < NN; t += blockDim.x) mi[t] = make_float2(mi[t].x - (pr.x * mj[t].x - pr.y * mj[t].y),
+                                                                             mi[t].y - (pr.x * mj[t].y + pr.y * mj[t].x));
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) {  // order by power, descending; ties by index
+    for (int i = 0; i < K; ++i) rank[i] = i;
+    for (int i = 1; i < K; ++i)
+      for (int j = i; j > 0 && pw[rank[j]] > pw[rank[j - 1]]; --j) {
+        const int t = rank[j];
+        rank[j] = rank[j - 1];
+        rank[j - 1] = t;
+      }
+  }
+  for (size_t t = threadIdx.x; t < size_t(K) * NN; t += blockDim.x) tmp[t] = modes[t];
+  __syncthreads();
+  for (int i = 1; i < K; ++i)
+    for (int t = threadIdx.x; t < NN; t += blockDim.x) modes[size_t(i) * NN + t] = tmp[size_t(rank[i]) * NN + t];
+}
+
+// m_k = m_0 e^{-2 pi i (t1 (c/N - 0.5) + t2 (r/N - 0.5))}, k >= 1 (FP64 phase)
+__global__ void k_mode_tilts(float2* __restrict__ probe, int K, int N, const double* __restrict__ tilts) {
+  const size_t NN = size_t(N) * N;
+  for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < size_t(K - 1) * NN;
+       t += size_t(gridDim.x) * blockDim.x) {
+    const int k = int(t / NN) + 1;
+    const int i = int(t % NN), r = i / N, c = i % N;
+    const double t1 = double(float(tilts[2 * (k - 1)])), t2 = double(float(tilts[2 * (k - 1) + 1]));
+    double sn, cs;
+    sincos(-2 * M_PI * (t1 * (double(c) / N - 0.5) + t2 * (double(r) / N - 0.5)), &sn, &cs);
+    const float2 p = probe[i];
+    probe[size_t(k) * NN + i] = make_float2(float(p.x * cs - p.y * sn), float(p.x * sn + p.y * cs));
+  }
+}
+
+// gram[i K + j] = sum conj(m_i) m_j, one block per pair
+__global__ void k_mode_gram(const float2* __restrict__ probe, int K, int NN, double2* __restrict__ gram) {
+  const int i = blockIdx.x / K, j = blockIdx.x % K;
+  double sr = 0, si = 0;
+  for (int t = threadIdx.x; t < NN; t += blockDim.x) {
+    const float2 a = probe[size_t(i) * NN + t], b = probe[size_t(j) * NN + t];
+    sr += double(a.x) * b.x + double(a.y) * b.y;
+    si += double(a.x) * b.y - double(a.y) * b.x;
+  }
+  sr = block_reduce_sum(sr);
+  __syncthreads();
+  si = block_reduce_sum(si);
+  if (threadIdx.x == 0) gram[blockIdx.x] = make_double2(sr, si);
+}
+
+// tmp_i = sum_q V(q, i) m_q, then copied back
+__global__ void k_mode_combine(const float2* __restrict__ probe, float2* __restrict__ tmp, int K, int NN,
+                               const double2* __restrict__ V) {
+  for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < size_t(K) * NN; t += size_t(gridDim.x) * blockDim.x) {
+    const int i = int(t / NN);
+    const size_t p = t % NN;
+    double re = 0, im = 0;
+    for (int q = 0; q < K; ++q) {
+      const double2 v = V[size_t(q) * K + i];
+      const float2 m = probe[size_t(q) * NN + p];
+      re += m.x * v.x - m.y * v.y;
+      im += m.x * v.y + m.y * v.x;
+    }
+    tmp[t] = make_float2(float(re), float(im));
+  }
+}
+
 int grid_n(size_t n, int cap = 1184) {
   size_t g = (n + 255) / 256;
   return int(g < 1 ? 1 : (g > size_t(cap) ? cap : g));
@@ -440,6 +597,25 @@ int grid_n(size_t n, int cap = 1184) {
 }  // namespace
 
 size_t mls_var_scratch_doubles(int Gmax) { return 10 * size_t(Gmax) + 8; }
+
+cudaError_t mls_mode_tilts(float2* probe, int K, int N, const double* tilts, cudaStream_t st) {
+  if (K < 2) return cudaSuccess;
+  k_mode_tilts<<<grid_n(size_t(K - 1) * N * N), 256, 0, st>>>(probe, K, N, tilts);
+  return cudaGetLastError();
+}
+
+cudaError_t mls_mode_gram(const float2* probe, int K, int N, double2* gram, cudaStream_t st) {
+  k_mode_gram<<<K * K, 256, 0, st>>>(probe, K, N * N, gram);
+  return cudaGetLastError();
+}
+
+cudaError_t mls_mode_combine(float2* probe, float2* tmp, int K, int N, const double2* V, cudaStream_t st) {
+  const size_t n = size_t(K) * N * N;
+  k_mode_combine<<<grid_n(n), 256, 0, st>>>(probe, tmp, K, N * N, V);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyAsync(probe, tmp, n * sizeof(float2), cudaMemcpyDeviceToDevice, st);
+}
 
 cudaError_t mls_zone_plate_probe(float2* probe, float2* pf, float2* work, const float2* tw, int N, double lambda,
                                  double dx_recon, double beamSize, cudaStream_t st) {
@@ -479,6 +655,12 @@ int mls_var_launches_per_iteration(int ngroups, unsigned flags) {
   return pre + ngroups * per;
 }
 
+int mls_var_mode_launches(int ngroups, int K) {
+  // per group: other modes' exit waves, their FFT2 and inverse, the modal modulus in place of the plain one, one
+  // update per extra mode; one orthogonalisation per iteration
+  return K > 1 ? ngroups * (1 + 2 + 2 + (K - 1)) + 1 : 0;
+}
+
 cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, cudaStream_t st) {
   const int N = b.N, NN = N * N, P = b.P;
   const size_t XY = size_t(b.X) * b.Y, GN = size_t(b.Gmax) * NN;
@@ -494,7 +676,7 @@ cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, 
   // calc_object_norm over the object ROI with the current illumination weights: P, E scaled by on, O by 1/on
   if ((e = mls_norm_sums(b.pobj, b.obj, b.Y, b.roi[0], b.roi[1], b.roi[2], b.roi[3], 1, b.normsums, st)) != cudaSuccess)
     return e;
-  if ((e = scale_by_norm(b.probe, NN, b.normsums, 0, st)) != cudaSuccess) return e;
+  if ((e = scale_by_norm(b.probe, size_t(b.K) * NN, b.normsums, 0, st)) != cudaSuccess) return e;
   if ((e = scale_by_norm(b.E, NN, b.normsums, 0, st)) != cudaSuccess) return e;
   if ((e = scale_by_norm(b.obj, XY, b.normsums, 1, st)) != cudaSuccess) return e;
   k_var_recentre<<<1, 256, 0, st>>>(b.pos, b.pos_o, P);
@@ -519,7 +701,14 @@ cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, 
     if ((e = fft(b.vp, b.Gmax, true)) != cudaSuccess) return e;
     k_var_psi<<<grid_n(GN), 256, 0, st>>>(b.objp, b.vp, b.psi, GN);
     if ((e = fft(b.psi, b.Gmax, false)) != cudaSuccess) return e;
-    if ((e = mls_modulus(b, mem, gs, st)) != cudaSuccess) return e;
+    if (b.K > 1) {
+      k_var_psik<<<grid_n(size_t(b.K - 1) * GN), 256, 0, st>>>(b.probe, b.objp, b.psik, b.K, b.Gmax, NN);
+      if ((e = fft(b.psik, (b.K - 1) * b.Gmax, false)) != cudaSuccess) return e;
+      k_var_modulus<<<grid, 256, 0, st>>>(b.psi, b.psik, b.amp, mem, gs, N, b.K, b.Gmax, b.errk);
+      if ((e = fft(b.psik, (b.K - 1) * b.Gmax, true)) != cudaSuccess) return e;
+    } else if ((e = mls_modulus(b, mem, gs, st)) != cudaSuccess) {
+      return e;
+    }
     if ((e = fft(b.psi, b.Gmax, true)) != cudaSuccess) return e;
     k_var_dirs<<<grid, 256, 0, st>>>(b.psi, b.objp, b.vp, b.win, mem, gs, N, b.Y, b.pu, b.S);
     if ((e = fft(b.pu, b.Gmax, false)) != cudaSuccess) return e;
@@ -547,7 +736,11 @@ cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, 
       k_var_evosums<<<grid, 256, 0, st>>>(b.objp, b.E, b.probe, b.psi, gs, N, b.vs + L.evs());
       k_var_evoupd<<<1, 32, 0, st>>>(b.vs + L.evs(), sc, b.evo, P, mem, gs, NN);
     }
+    for (int m = 1; m < b.K; ++m)  // modes past the first: their directions with the group's probe step
+      k_var_mode_update<<<grid_n(NN, 256), 256, 0, st>>>(b.psik + size_t(m - 1) * GN, b.objp, b.pobj, b.maxIllum,
+                                                          b.win, mem, gs, N, b.Y, b.betas, b.probe + size_t(m) * NN);
   }
+  if (b.K > 1) k_var_ortho<<<1, 1024, 0, st>>>(b.probe, b.mtmp, b.K, NN);
   return cudaGetLastError();
 }
 

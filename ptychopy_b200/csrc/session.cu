@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <fstream>
 #include <functional>
@@ -288,7 +289,7 @@ struct MlsState {
   // the reference-default path: extra mode, evolution weights, positions, sub-pixel shifts, per-position probes and
   // directions, gradient images, scratch sums, max of p_object
   bool variable = false;
-  DeviceBuf E, evo, pos, pos_o, sub, vp, pu, aux, vs, pmax;
+  DeviceBuf E, evo, pos, pos_o, sub, vp, pu, aux, vs, pmax, psik, mtmp;
   int Gmax = 1, ng = 1;
   size_t table_ints = 0;
   MlsTables tab[2];
@@ -309,7 +310,10 @@ struct MlsState {
 // mode (initVarModes, src/Probe.cpp:497-505, d_initVarMOdes src/ProbeKernels.cu:99-110: r1 e^{2 pi i r2}, all r1
 // drawn before all r2) and normalRandom for the extra-mode weights (1e-6 N(0,1), src/Probe.cpp:520-525).  SplitMix64
 // from seed ^ 0x3C6EF372FE94F82B, u = (bits >> 11 + 0.5) 2^-53, Box-Muller's cos branch, one normal per pair.
-void mls_variable_draws(uint64_t seed, int N, int P, std::vector<float2>& E, std::vector<double>& evo1) {
+// With K > 1 probe modes, 2 (K - 1) normals for the modes' phase tilts (initMLH, src/Probe.cpp:422-431) are drawn
+// after the extra mode and before the weights.
+void mls_variable_draws(uint64_t seed, int N, int P, int K, std::vector<float2>& E, std::vector<double>& tilts,
+                        std::vector<double>& evo1) {
   uint64_t st = seed ^ 0x3C6EF372FE94F82Bull;
   auto u = [&] { return (double(splitmix64(st) >> 11) + 0.5) * (1.0 / 9007199254740992.0); };
   const size_t NN = size_t(N) * N;
@@ -319,10 +323,74 @@ void mls_variable_draws(uint64_t seed, int N, int P, std::vector<float2>& E, std
   E.resize(NN);
   for (size_t i = 0; i < NN; ++i)
     E[i] = make_float2(float(r1[i] * std::cos(2 * M_PI * r2[i])), float(r1[i] * std::sin(2 * M_PI * r2[i])));
-  evo1.resize(P);
-  for (auto& v : evo1) {
+  auto normal = [&] {
     const double a = u(), b = u();
-    v = 1e-6 * (std::sqrt(-2.0 * std::log(a)) * std::cos(2 * M_PI * b));
+    return std::sqrt(-2.0 * std::log(a)) * std::cos(2 * M_PI * b);
+  };
+  tilts.resize(2 * size_t(K > 1 ? K - 1 : 0));
+  for (auto& v : tilts) v = normal();
+  evo1.resize(P);
+  for (auto& v : evo1) v = 1e-6 * normal();
+}
+
+// Eigen-decomposition of a Hermitian K x K matrix (row-major, complex as double2) by cyclic complex Jacobi
+// rotations.  Eigenvectors (columns of V, unit norm) in descending |eigenvalue|, each turned so that its first
+// component of at least half the largest magnitude is real and positive (robust to the equal-magnitude components
+// of equal-power modes): the reference's ComplexEigenSolver fixes no phase.
+void hermitian_eigen(int K, const std::vector<double2>& Ain, std::vector<double2>& Vout) {
+  using C = std::complex<double>;
+  std::vector<C> A(size_t(K) * K), V(size_t(K) * K, C(0, 0));
+  for (size_t i = 0; i < A.size(); ++i) A[i] = C(Ain[i].x, Ain[i].y);
+  for (int i = 0; i < K; ++i) V[size_t(i) * K + i] = 1;
+  double scale = 0;
+  for (const C& v : A) scale += std::norm(v);
+  for (int sweep = 0; sweep < 64; ++sweep) {
+    double off = 0;
+    for (int p = 0; p < K; ++p)
+      for (int q = p + 1; q < K; ++q) off += std::norm(A[size_t(p) * K + q]);
+    if (off <= 1e-30 * scale) break;
+    for (int p = 0; p < K; ++p)
+      for (int q = p + 1; q < K; ++q) {
+        const C apq = A[size_t(p) * K + q];
+        const double m = std::abs(apq);
+        if (m == 0.0) continue;
+        const double app = A[size_t(p) * K + p].real(), aqq = A[size_t(q) * K + q].real();
+        const double th = 0.5 * std::atan2(2 * m, aqq - app);
+        const double c = std::cos(th), s = std::sin(th);
+        const C em = std::conj(apq) / m;
+        for (int k = 0; k < K; ++k) {
+          const C x = A[size_t(k) * K + p], y = A[size_t(k) * K + q];
+          A[size_t(k) * K + p] = c * x - s * em * y;
+          A[size_t(k) * K + q] = s * x + c * em * y;
+          const C vx = V[size_t(k) * K + p], vy = V[size_t(k) * K + q];
+          V[size_t(k) * K + p] = c * vx - s * em * vy;
+          V[size_t(k) * K + q] = s * vx + c * em * vy;
+        }
+        for (int k = 0; k < K; ++k) {
+          const C x = A[size_t(p) * K + k], y = A[size_t(q) * K + k];
+          A[size_t(p) * K + k] = c * x - s * std::conj(em) * y;
+          A[size_t(q) * K + k] = s * x + c * std::conj(em) * y;
+        }
+      }
+  }
+  std::vector<int> idx(K);
+  for (int i = 0; i < K; ++i) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+    return std::abs(A[size_t(x) * K + x].real()) > std::abs(A[size_t(y) * K + y].real());
+  });
+  Vout.resize(size_t(K) * K);
+  for (int j = 0; j < K; ++j) {
+    const int c = idx[j];
+    double mx = 0;
+    for (int k = 0; k < K; ++k) mx = std::max(mx, std::abs(V[size_t(k) * K + c]));
+    int best = 0;
+    while (best < K - 1 && std::abs(V[size_t(best) * K + c]) < 0.5 * mx) ++best;
+    const C v = V[size_t(best) * K + c];
+    const C ph = std::abs(v) > 0 ? std::conj(v) / std::abs(v) : C(1, 0);
+    for (int k = 0; k < K; ++k) {
+      const C w = V[size_t(k) * K + c] * ph;
+      Vout[size_t(k) * K + j] = make_double2(w.real(), w.imag());
+    }
   }
 }
 
@@ -645,7 +713,9 @@ void init_dm(pty_session* s) {
 // 1/corr with corr = sqrt(median_i(mean|P|^2 / (sum I_i / N^2)) * N^2), p_object = illum / corr^2, MAX_ILLUM.
 void init_mls(pty_session* s) {
   const pty_params& p = s->prm;
-  need(s->K == 1, "the MLs core supports one probe mode (probeModes=1)", PTY_ERR_UNSUPPORTED);
+  need(s->K == 1 || p.mlsCore == 0, "the MLs core (mlsCore=1) supports one probe mode (probeModes=1)",
+       PTY_ERR_UNSUPPORTED);
+  need(s->K <= 64, "MLs supports up to 64 probe modes", PTY_ERR_UNSUPPORTED);
   need(p.precision == 0 || s->N == 256, "precision=1 (tensor-core FFT stages) needs 256 x 256 patterns",
        PTY_ERR_UNSUPPORTED);
   auto* ml = new MlsState;
@@ -700,8 +770,9 @@ void init_mls(pty_session* s) {
   check_cuda(sqrt_inplace(s->amp.as<float>(), size_t(P) * NN, s->stream), "sqrt");
   if (p.probeGuess[0] == 0 && s->probe_h.empty()) {
     // no probe given: the zone-plate guess of initMLH (src/IPhaser.cpp:283-291, src/Probe.cpp:376-420)
-    s->probe.alloc(sizeof(float2) * NN, "probe");
-    s->pcache.alloc(sizeof(float) * NN, "probe cache");
+    s->probe.alloc(sizeof(float2) * NN * s->K, "probe");
+    s->pcache.alloc(sizeof(float) * NN * s->K, "probe cache");
+    check_cuda(cudaMemsetAsync(s->probe.p, 0, s->probe.bytes, s->stream), "memset probe");
     check_cuda(cudaMemsetAsync(s->pcache.p, 0, s->pcache.bytes, s->stream), "memset probe cache");
     DeviceBuf pf, work;
     pf.alloc(sizeof(float2) * NN, "zone-plate propagator");
@@ -723,8 +794,28 @@ void init_mls(pty_session* s) {
   std::vector<float2> Eh;
   if (ml->variable) {
     // initEvo (src/Probe.cpp:511-560): intensity weights 1; the extra mode to unit RMS, its weights carry the norm
-    std::vector<double> evo(2 * size_t(P), 1.0), evo1;
-    mls_variable_draws(p.seed, N, P, Eh, evo1);
+    std::vector<double> evo(2 * size_t(P), 1.0), evo1, tilts;
+    mls_variable_draws(p.seed, N, P, s->K, Eh, tilts, evo1);
+    if (s->K > 1) {
+      // modes 1..K-1 from mode 0 (initMLH, src/Probe.cpp:422-490): phase tilts, then recombination by the
+      // eigenvectors of their Gram matrix
+      const int K = s->K;
+      DeviceBuf dt, dg, tmp;
+      dt.alloc(sizeof(double) * tilts.size(), "mode tilts");
+      dg.alloc(sizeof(double2) * K * K, "mode Gram matrix");
+      tmp.alloc(sizeof(float2) * NN * K, "modes");
+      check_cuda(cudaMemcpyAsync(dt.p, tilts.data(), dt.bytes, cudaMemcpyHostToDevice, s->stream), "H2D");
+      check_cuda(mls_mode_tilts(s->probe.as<float2>(), K, N, dt.as<double>(), s->stream), "mode tilts");
+      check_cuda(mls_mode_gram(s->probe.as<float2>(), K, N, dg.as<double2>(), s->stream), "mode Gram matrix");
+      std::vector<double2> gram(size_t(K) * K), V;
+      check_cuda(cudaMemcpyAsync(gram.data(), dg.p, dg.bytes, cudaMemcpyDeviceToHost, s->stream), "D2H");
+      check_cuda(cudaStreamSynchronize(s->stream), "mode Gram matrix");
+      hermitian_eigen(K, gram, V);
+      check_cuda(cudaMemcpyAsync(dg.p, V.data(), dg.bytes, cudaMemcpyHostToDevice, s->stream), "H2D");
+      check_cuda(mls_mode_combine(s->probe.as<float2>(), tmp.as<float2>(), K, N, dg.as<double2>(), s->stream),
+                 "mode recombination");
+      check_cuda(cudaStreamSynchronize(s->stream), "probe modes");
+    }
     double se = 0;
     for (const float2& v : Eh) se += double(v.x) * v.x + double(v.y) * v.y;
     const double rE = std::sqrt(se / double(NN));
@@ -755,7 +846,7 @@ void init_mls(pty_session* s) {
   check_cuda(scale_by_norm(s->obj.as<float2>(), XY, ml->norms.as<double>(), 1, s->stream), "object norm");
   DeviceBuf d;
   d.alloc(sizeof(double), "sum");
-  check_cuda(reduce_sum_sq(s->probe.as<float2>(), NN, d.as<double>(), s->stream), "probe power");
+  check_cuda(reduce_sum_sq(s->probe.as<float2>(), NN * s->K, d.as<double>(), s->stream), "probe power");
   double psum = 0;
   check_cuda(cudaMemcpyAsync(&psum, d.p, sizeof(double), cudaMemcpyDeviceToHost, s->stream), "D2H");
   check_cuda(cudaStreamSynchronize(s->stream), "MLs set-up");
@@ -765,7 +856,7 @@ void init_mls(pty_session* s) {
   std::sort(corrv.begin(), corrv.end());
   double corr = (P % 2) ? corrv[P / 2] : 0.5 * (corrv[P / 2 - 1] + corrv[P / 2]);
   corr = std::sqrt(corr * double(NN));
-  check_cuda(scale_complex(s->probe.as<float2>(), NN, float(1.0 / corr), s->stream), "probe scale");
+  check_cuda(scale_complex(s->probe.as<float2>(), NN * s->K, float(1.0 / corr), s->stream), "probe scale");
   if (ml->variable) check_cuda(scale_complex(ml->E.as<float2>(), NN, float(1.0 / corr), s->stream), "extra mode scale");
   check_cuda(scale_real(ml->pobj.as<float>(), XY, float(1.0 / (corr * corr)), s->stream), "illumination scale");
   check_cuda(max_real(ml->pobj.as<float>(), XY, ml->maxill.as<float>(), s->stream), "MAX_ILLUM");
@@ -777,13 +868,17 @@ void init_mls(pty_session* s) {
   ml->pum.alloc(sizeof(float2) * NN, "probe direction");
   ml->objp.alloc(sizeof(float2) * GN, "windows");
   ml->psi.alloc(sizeof(float2) * GN, "exit waves");
-  ml->work.alloc(sizeof(float2) * GN * (ml->variable ? 2 : 1), "FFT work");
+  ml->work.alloc(sizeof(float2) * GN * (ml->variable ? std::max(2, s->K - 1) : 1), "FFT work");
   if (ml->variable) {
     ml->vp.alloc(sizeof(float2) * GN, "position probes");
     ml->pu.alloc(sizeof(float2) * GN, "probe directions");
     ml->aux.alloc(sizeof(float2) * 2 * GN, "gradient images");
     ml->vs.alloc(sizeof(double) * mls_var_scratch_doubles(ml->Gmax), "MLs sums");
     ml->pmax.alloc(sizeof(float), "illumination maximum");
+    if (s->K > 1) {
+      ml->psik.alloc(sizeof(float2) * GN * (s->K - 1), "exit waves of the other modes");
+      ml->mtmp.alloc(sizeof(float2) * NN * s->K, "mode scratch");
+    }
     for (DeviceBuf* b : {&ml->vp, &ml->pu, &ml->aux, &ml->vs})
       check_cuda(cudaMemsetAsync(b->p, 0, b->bytes, s->stream), "memset");
   }
@@ -804,7 +899,7 @@ void init_mls(pty_session* s) {
 
 MlsBuffers mls_buffers(pty_session* s, int parity) {
   MlsState* ml = s->ml;
-  MlsBuffers b;
+  MlsBuffers b{};
   b.obj = s->obj.as<float2>();
   b.probe = s->probe.as<float2>();
   b.amp = s->amp.as<float>();
@@ -851,6 +946,9 @@ MlsBuffers mls_buffers(pty_session* s, int parity) {
     b.pmax = ml->pmax.as<float>();
     b.cvx = std::ceil(float(s->X) * 1.0f / 2 - float(s->N) * 1.0f / 2);
     b.cvy = std::ceil(float(s->Y) * 1.0f / 2 - float(s->N) * 1.0f / 2);
+    b.K = s->K;
+    b.psik = ml->psik.as<float2>();
+    b.mtmp = ml->mtmp.as<float2>();
   }
   return b;
 }
@@ -922,7 +1020,7 @@ double step_mls(pty_session* s, bool want_err) {
       check_cuda(e3, "graph instantiate");
     }
     check_cuda(cudaGraphLaunch(ge, s->stream), "MLs graph launch");
-    s->launches += mls_var_launches_per_iteration(ml->ng, flags);
+    s->launches += mls_var_launches_per_iteration(ml->ng, flags) + mls_var_mode_launches(ml->ng, s->K);
   } else {
   if (!tb.graph) {
     const MlsBuffers b = mls_buffers(s, parity);

@@ -88,6 +88,31 @@ def test_mls_zone_plate_probe_start(oracle):
     s.close()
 
 
+@pytest.mark.parametrize("K", [2, 3])
+def test_mls_probe_modes_match_oracle(oracle, K):
+    """probeModes > 1: modes 1..K-1 from phase tilts of mode 0 recombined by the eigenvectors of their Gram matrix,
+    the modal modulus over sum |Psi_k|^2, per-mode probe steps, and ortho_modes after each iteration."""
+    d = mls_dataset(oracle, N=64, nx=6, shifted=True)
+    s = gpu_session(dict(amp=d["intens"], kw=d["kw"]), probe=d["probe"], obj=d["obj"], calculateRMS=1, PPS=3,
+                    probeModes=K)
+    o = oracle.OracleMls(d["raw"], d["intens"], d["probe"], obj=d["obj"], variable=1, PPS=3, K=K)
+    for it in range(0, 5):
+        if it:
+            e = s.step()
+            eo = o.step()
+            assert abs(e - eo) <= 1e-3 * abs(eo), f"error, iteration {it}"
+        ob, pr, _ = o.state()
+        gp = s.probe()
+        assert gp.shape == (K, 64, 64)
+        assert rel_err(s.object(), ob) < TOL, f"object, iteration {it}"
+        for k in range(K):  # the weaker modes carry a few % of the power: each checked on its own scale
+            assert rel_err(gp[k], pr[k]) < (TOL if k == 0 else 1e-3), f"mode {k}, iteration {it}"
+        G = np.einsum("kxy,lxy->kl", gp.conj().astype(np.complex128), gp.astype(np.complex128))
+        off = np.abs(G - np.diag(np.diag(G))).max() / np.abs(np.diag(G)).max()
+        assert off < 1e-5, f"modes not orthogonal, iteration {it}"
+    s.close()
+
+
 def test_mls_default_path_groups_of_several(oracle):
     # 15x15 = 225 positions: groups of 2 and one of 1, delta_p 0.2, another seed; position search from iteration 2
     d = mls_dataset(oracle, N=32, nx=15, seed=4, shifted=True)
