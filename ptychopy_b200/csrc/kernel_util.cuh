@@ -7,6 +7,18 @@
 
 namespace pty {
 
+// Programmatic dependent launch: a kernel launched with launch_pdl (pdl.cuh) may start while its predecessor in the
+// stream still runs; it waits here until that grid has completed and its memory is visible, then lets its own
+// dependent launch begin.  Outside such a launch both instructions return at once.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+}  // namespace pty
+
+namespace pty {
+
 // Shared memory of a row-transform CTA (FftShape<L>::RC rows): twiddles + max(exchange, transposed staging).
 template <int L>
 __host__ __device__ constexpr size_t rows_smem_bytes() {

@@ -19,12 +19,14 @@
 #include "fft_core.cuh"
 #include "kernel_util.cuh"
 #include "kernels_mls.h"
+#include "pdl.cuh"
 
 namespace pty {
 
 // p[r0+x][c0+y] += scale * |P[x][y]|^2 for every window (set_projections of |P|^2).
 __global__ void k_mls_illum_add(float* __restrict__ pobj, const float2* __restrict__ probe,
                                 const int2* __restrict__ starts, int N, int Y, float scale) {
+  pdl_enter();
   const int j = blockIdx.y;
   const int2 s = starts[j];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
@@ -36,6 +38,7 @@ __global__ void k_mls_illum_add(float* __restrict__ pobj, const float2* __restri
 }
 
 __global__ void k_scale_real(float* __restrict__ a, size_t n, float s) {
+  pdl_enter();
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
     a[i] *= s;
 }
@@ -43,6 +46,7 @@ __global__ void k_scale_real(float* __restrict__ a, size_t n, float s) {
 // out[0] += sum w^q, out[1] += sum w^q |O|^2 over the rectangle [x0, x0+nx) x [y0, y0+ny), q = 2 (squared) or 1
 __global__ void k_mls_norm_sums(const float* __restrict__ w, const float2* __restrict__ obj, int Y, int x0, int y0,
                                 int nx, int ny, int squared, double* __restrict__ out) {
+  pdl_enter();
   double sw = 0, so = 0;
   const int n = nx * ny;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -64,6 +68,7 @@ __global__ void k_mls_norm_sums(const float* __restrict__ w, const float2* __res
 // calc_object_norm: on = sqrt(sum w^2|O|^2 / sum w^2); P *= on, O /= on (mode 0: multiply a by on, 1: divide).
 // An empty or unlit ROI (sum w^2 = 0, e.g. a single scan line) leaves both unscaled.
 __global__ void k_scale_by_norm(float2* __restrict__ a, size_t n, const double* __restrict__ sums, int divide) {
+  pdl_enter();
   const double on = sums[0] > 0.0 ? sqrt(sums[1]) / sqrt(sums[0]) : 1.0;
   const float s = divide ? float(1.0 / on) : float(on);
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
@@ -74,6 +79,7 @@ __global__ void k_mls_exit(const float2* __restrict__ obj, const float2* __restr
                            const int2* __restrict__ starts, const int* __restrict__ members,
                            const int* __restrict__ gsize, int N, int Y, float2* __restrict__ objp,
                            float2* __restrict__ psi) {
+  pdl_enter();
   const int k = blockIdx.y;
   const size_t NN = size_t(N) * N;
   const bool live = k < *gsize;
@@ -92,6 +98,7 @@ __global__ void k_mls_exit(const float2* __restrict__ obj, const float2* __restr
 __global__ void k_mls_modulus(float2* __restrict__ spec, const float* __restrict__ amp,
                               const int* __restrict__ members, const int* __restrict__ gsize, int N,
                               double* __restrict__ err) {
+  pdl_enter();
   const int k = blockIdx.y;
   if (k >= *gsize) return;
   const size_t NN = size_t(N) * N;
@@ -115,6 +122,7 @@ __global__ void k_mls_dirs(const float2* __restrict__ chi, const float2* __restr
                            const float* __restrict__ maxIllum, const int2* __restrict__ starts,
                            const int* __restrict__ members, const int* __restrict__ gsize, int N, int Y,
                            float2* __restrict__ pum, float2* __restrict__ S) {
+  pdl_enter();
   const int k = blockIdx.y;
   if (k >= *gsize) return;
   const size_t NN = size_t(N) * N;
@@ -137,6 +145,7 @@ __global__ void k_mls_lsq(const float2* __restrict__ chi, const float2* __restri
                           const float* __restrict__ maxIllum, float delta_p, const int2* __restrict__ starts,
                           const int* __restrict__ members, const int* __restrict__ gsize, int N, int Y,
                           double* __restrict__ sums) {
+  pdl_enter();
   const int k = blockIdx.y;
   const int G = *gsize;
   if (k >= G) return;
@@ -171,6 +180,7 @@ __global__ void k_mls_lsq(const float2* __restrict__ chi, const float2* __restri
 __global__ void k_mls_solve(double* __restrict__ sums, double* __restrict__ errk, const int* __restrict__ gsize,
                             int N, double beta_obj, double beta_probe, double* __restrict__ betas,
                             double* __restrict__ err_total) {
+  pdl_enter();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int G = *gsize;
   double m1 = 0, m4 = 0;
@@ -205,6 +215,7 @@ __global__ void k_mls_solve(double* __restrict__ sums, double* __restrict__ errk
 __global__ void k_mls_update_object(float2* __restrict__ obj, float2* __restrict__ S, const float* __restrict__ pobj,
                                     const float* __restrict__ maxIllum, float delta_p, const double* __restrict__ betas,
                                     const int* __restrict__ bbox, int Y) {
+  pdl_enter();
   const int x0 = bbox[0], y0 = bbox[1], nx = bbox[2], ny = bbox[3];
   const float2 b = make_float2(float(betas[0]), float(betas[1]));
   const float dmax = *maxIllum * delta_p;
@@ -221,6 +232,7 @@ __global__ void k_mls_update_object(float2* __restrict__ obj, float2* __restrict
 // P += beta_p * pum / G; clear = 1 zeroes the accumulator for the next group's atomics.
 __global__ void k_mls_update_probe(float2* __restrict__ probe, float2* __restrict__ pum, const double* __restrict__ betas,
                                    const int* __restrict__ gsize, int n, int clear) {
+  pdl_enter();
   const float2 b = make_float2(float(betas[2]), float(betas[3]));
   const float invG = 1.f / float(*gsize);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -232,6 +244,7 @@ __global__ void k_mls_update_probe(float2* __restrict__ probe, float2* __restric
 // Bounding box (x0, y0, nx, ny) of each group's windows.
 __global__ void k_mls_bbox(const int2* __restrict__ starts, const int* __restrict__ members,
                            const int* __restrict__ gsize, int ngroups, int Gmax, int N, int* __restrict__ bbox) {
+  pdl_enter();
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ngroups) return;
   int x0 = 1 << 30, y0 = 1 << 30, x1 = 0, y1 = 0;
@@ -256,17 +269,17 @@ static int grid_for(size_t n, int cap = 1184) {
 cudaError_t mls_illum_add(float* pobj, const float2* probe, const int2* starts, int P, int N, int Y, float scale,
                           cudaStream_t st) {
   dim3 grid((N * N + 255) / 256, P);
-  k_mls_illum_add<<<grid, 256, 0, st>>>(pobj, probe, starts, N, Y, scale);
+  launch_pdl(k_mls_illum_add, grid, 256, 0, st, pobj, probe, starts, N, Y, scale);
   return cudaGetLastError();
 }
 
 cudaError_t scale_real(float* a, size_t n, float s, cudaStream_t st) {
-  k_scale_real<<<grid_for(n), 256, 0, st>>>(a, n, s);
+  launch_pdl(k_scale_real, grid_for(n), 256, 0, st, a, n, s);
   return cudaGetLastError();
 }
 
 cudaError_t scale_by_norm(float2* a, size_t n, const double* sums, int divide, cudaStream_t st) {
-  k_scale_by_norm<<<grid_for(n), 256, 0, st>>>(a, n, sums, divide);
+  launch_pdl(k_scale_by_norm, grid_for(n), 256, 0, st, a, n, sums, divide);
   return cudaGetLastError();
 }
 
@@ -274,21 +287,23 @@ cudaError_t mls_norm_sums(const float* w, const float2* obj, int Y, int x0, int 
                           double* out, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(out, 0, 2 * sizeof(double), st);
   if (e != cudaSuccess) return e;
-  k_mls_norm_sums<<<grid_for(size_t(nx) * ny), 256, 0, st>>>(w, obj, Y, x0, y0, nx, ny, squared, out);
+  launch_pdl(k_mls_norm_sums, grid_for(size_t(nx) * ny), 256, 0, st, w, obj, Y, x0, y0, nx, ny, squared, out);
   return cudaGetLastError();
 }
 
 __global__ void k_sqrt_inplace(float* __restrict__ a, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
     a[i] = sqrtf(a[i]);
 }
 
 cudaError_t sqrt_inplace(float* a, size_t n, cudaStream_t st) {
-  k_sqrt_inplace<<<grid_for(n), 256, 0, st>>>(a, n);
+  launch_pdl(k_sqrt_inplace, grid_for(n), 256, 0, st, a, n);
   return cudaGetLastError();
 }
 
 __global__ void k_max_real(const float* __restrict__ a, size_t n, float* out) {
+  pdl_enter();
   float m = 0.f;
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
     m = fmaxf(m, a[i]);
@@ -299,7 +314,7 @@ __global__ void k_max_real(const float* __restrict__ a, size_t n, float* out) {
 cudaError_t max_real(const float* a, size_t n, float* out, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float), st);
   if (e != cudaSuccess) return e;
-  k_max_real<<<grid_for(n), 256, 0, st>>>(a, n, out);
+  launch_pdl(k_max_real, grid_for(n), 256, 0, st, a, n, out);
   return cudaGetLastError();
 }
 
@@ -309,28 +324,28 @@ cudaError_t mls_iteration(const MlsBuffers& b, int ngroups, cudaStream_t st) {
   cudaError_t e;
   // calc_object_norm over the object ROI with the current illumination weights
   if ((e = cudaMemsetAsync(b.normsums, 0, 2 * sizeof(double), st)) != cudaSuccess) return e;
-  k_mls_norm_sums<<<grid_for(size_t(b.roi[2]) * b.roi[3]), 256, 0, st>>>(b.pobj, b.obj, b.Y, b.roi[0], b.roi[1],
+  launch_pdl(k_mls_norm_sums, grid_for(size_t(b.roi[2]) * b.roi[3]), 256, 0, st, b.pobj, b.obj, b.Y, b.roi[0], b.roi[1],
                                                                            b.roi[2], b.roi[3], 1, b.normsums);
-  k_scale_by_norm<<<grid_for(NN), 256, 0, st>>>(b.probe, NN, b.normsums, 0);
-  k_scale_by_norm<<<grid_for(XY), 256, 0, st>>>(b.obj, XY, b.normsums, 1);
+  launch_pdl(k_scale_by_norm, grid_for(NN), 256, 0, st, b.probe, NN, b.normsums, 0);
+  launch_pdl(k_scale_by_norm, grid_for(XY), 256, 0, st, b.obj, XY, b.normsums, 1);
   // updated_cached_illumination: p = (p + sum |P|^2 at the windows) / 2
-  k_scale_real<<<grid_for(XY), 256, 0, st>>>(b.pobj, XY, 0.5f);
+  launch_pdl(k_scale_real, grid_for(XY), 256, 0, st, b.pobj, XY, 0.5f);
   dim3 gi((NN + 255) / 256, b.P);
-  k_mls_illum_add<<<gi, 256, 0, st>>>(b.pobj, b.probe, b.starts, N, b.Y, 0.5f);
+  launch_pdl(k_mls_illum_add, gi, 256, 0, st, b.pobj, b.probe, b.starts, N, b.Y, 0.5f);
   const int gb = (NN + 255) / 256 > 64 ? 64 : (NN + 255) / 256;
   for (int g = 0; g < ngroups; ++g) {
     const int* mem = b.members + size_t(g) * b.Gmax;
     const int* gs = b.gsize + g;
     dim3 grid(gb, b.Gmax);
-    k_mls_exit<<<grid, 256, 0, st>>>(b.obj, b.probe, b.starts, mem, gs, N, b.Y, b.objp, b.psi);
+    launch_pdl(k_mls_exit, grid, 256, 0, st, b.obj, b.probe, b.starts, mem, gs, N, b.Y, b.objp, b.psi);
     if ((e = b.tc ? fft2_tc(b.psi, b.work, b.Gmax, N, false, b.tc_err, st)
-                  : fft2(b.psi, b.work, b.tw, b.Gmax, N, false, st)) != cudaSuccess)
+                  : fft2_pdl(b.psi, b.work, b.tw, b.Gmax, N, false, st)) != cudaSuccess)
       return e;
-    k_mls_modulus<<<grid, 256, 0, st>>>(b.psi, b.amp, mem, gs, N, b.errk);
+    launch_pdl(k_mls_modulus, grid, 256, 0, st, b.psi, b.amp, mem, gs, N, b.errk);
     if ((e = b.tc ? fft2_tc(b.psi, b.work, b.Gmax, N, true, b.tc_err, st)
-                  : fft2(b.psi, b.work, b.tw, b.Gmax, N, true, st)) != cudaSuccess)
+                  : fft2_pdl(b.psi, b.work, b.tw, b.Gmax, N, true, st)) != cudaSuccess)
       return e;
-    k_mls_dirs<<<grid, 256, 0, st>>>(b.psi, b.objp, b.probe, b.pobj, b.maxIllum, b.starts, mem, gs, N, b.Y, b.pum,
+    launch_pdl(k_mls_dirs, grid, 256, 0, st, b.psi, b.objp, b.probe, b.pobj, b.maxIllum, b.starts, mem, gs, N, b.Y, b.pum,
                                      b.S);
     if ((e = mls_lsq(b, b.probe, 0, mem, gs, st)) != cudaSuccess) return e;
     if ((e = mls_solve_update(b, mem, gs, b.bbox + 4 * size_t(g), 1, st)) != cudaSuccess) return e;
@@ -342,14 +357,14 @@ int mls_launches_per_iteration(int ngroups) { return 5 + ngroups * 11; }
 
 cudaError_t mls_group_boxes(const int2* starts, const int* members, const int* gsize, int ngroups, int Gmax, int N,
                             int* bbox, cudaStream_t st) {
-  k_mls_bbox<<<(ngroups + 127) / 128, 128, 0, st>>>(starts, members, gsize, ngroups, Gmax, N, bbox);
+  launch_pdl(k_mls_bbox, (ngroups + 127) / 128, 128, 0, st, starts, members, gsize, ngroups, Gmax, N, bbox);
   return cudaGetLastError();
 }
 
 cudaError_t mls_modulus(const MlsBuffers& b, const int* members, const int* gsize, cudaStream_t st) {
   const int NN = b.N * b.N;
   dim3 grid((NN + 255) / 256 > 64 ? 64 : (NN + 255) / 256, b.Gmax);
-  k_mls_modulus<<<grid, 256, 0, st>>>(b.psi, b.amp, members, gsize, b.N, b.errk);
+  launch_pdl(k_mls_modulus, grid, 256, 0, st, b.psi, b.amp, members, gsize, b.N, b.errk);
   return cudaGetLastError();
 }
 
@@ -357,7 +372,7 @@ cudaError_t mls_lsq(const MlsBuffers& b, const float2* probe, size_t pstride, co
                     cudaStream_t st) {
   const int NN = b.N * b.N;
   dim3 grid((NN + 255) / 256 > 64 ? 64 : (NN + 255) / 256, b.Gmax);
-  k_mls_lsq<<<grid, 256, 0, st>>>(b.psi, b.objp, probe, pstride, b.pum, b.S, b.pobj, b.maxIllum, b.delta_p, b.starts,
+  launch_pdl(k_mls_lsq, grid, 256, 0, st, b.psi, b.objp, probe, pstride, b.pum, b.S, b.pobj, b.maxIllum, b.delta_p, b.starts,
                                   members, gsize, b.N, b.Y, b.sums);
   return cudaGetLastError();
 }
@@ -367,10 +382,10 @@ cudaError_t mls_solve_update(const MlsBuffers& b, const int* members, const int*
                              int clear_pum, cudaStream_t st) {
   (void)members;
   const int NN = b.N * b.N;
-  k_mls_solve<<<1, 32, 0, st>>>(b.sums, b.errk, gsize, b.N, b.beta_obj, b.beta_probe, b.betas, b.err);
-  k_mls_update_object<<<grid_for(size_t(2) * NN), 256, 0, st>>>(b.obj, b.S, b.pobj, b.maxIllum, b.delta_p, b.betas,
+  launch_pdl(k_mls_solve, 1, 32, 0, st, b.sums, b.errk, gsize, b.N, b.beta_obj, b.beta_probe, b.betas, b.err);
+  launch_pdl(k_mls_update_object, grid_for(size_t(2) * NN), 256, 0, st, b.obj, b.S, b.pobj, b.maxIllum, b.delta_p, b.betas,
                                                                  bbox, b.Y);
-  k_mls_update_probe<<<grid_for(NN), 256, 0, st>>>(b.probe, b.pum, b.betas, gsize, NN, clear_pum);
+  launch_pdl(k_mls_update_probe, grid_for(NN), 256, 0, st, b.probe, b.pum, b.betas, gsize, NN, clear_pum);
   return cudaGetLastError();
 }
 

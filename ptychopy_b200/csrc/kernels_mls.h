@@ -73,12 +73,13 @@ cudaError_t scale_by_norm(float2* a, size_t n, const double* sums, int divide, c
 cudaError_t sqrt_inplace(float* a, size_t n, cudaStream_t st);
 cudaError_t max_real(const float* a, size_t n, float* out, cudaStream_t st);
 // One MLs iteration over `ngroups` groups (tables in b.members / b.gsize / b.bbox), enqueued on st.
+// fft2 with both passes launched by programmatic dependent launch (kernels_mls_var.cu)
+cudaError_t fft2_pdl(float2* data, float2* work, const float2* tw, int batch, int N, bool inverse, cudaStream_t st);
 cudaError_t mls_iteration(const MlsBuffers& b, int ngroups, cudaStream_t st);
 int mls_launches_per_iteration(int ngroups);
 // One iteration of the reference-default path (kernels_mls_var.cu); flags from MlsVarFlags.
 cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, cudaStream_t st);
-int mls_var_launches_per_iteration(int ngroups, unsigned flags);
-int mls_var_mode_launches(int ngroups, int K);
+int mls_var_launches_per_iteration(int ngroups, unsigned flags, int K, bool tc);
 size_t mls_var_scratch_doubles(int Gmax);
 // MLs probe modes 1..K-1 from mode 0 (initMLH): phase tilts (2 (K-1) values, device), then the Gram matrix
 // G_ij = sum conj(m_i) m_j (K x K double2, device) for the host's eigen-decomposition, then modes <- modes V

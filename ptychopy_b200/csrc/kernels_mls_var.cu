@@ -28,6 +28,7 @@
 #include "fft_core.cuh"
 #include "kernel_util.cuh"
 #include "kernels_mls.h"
+#include "pdl.cuh"
 
 namespace pty {
 
@@ -52,6 +53,7 @@ __device__ __forceinline__ float fft_freq(int k, int N) {
 
 __global__ void k_var_windows(const float* __restrict__ pos, int P, int N, int X, int Y, float cvx, float cvy,
                               int2* __restrict__ win, float2* __restrict__ sub) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
   const float p1 = pos[2 * i] + cvx, p2 = pos[2 * i + 1] + cvy;
@@ -62,6 +64,7 @@ __global__ void k_var_windows(const float* __restrict__ pos, int P, int N, int X
 
 // Positions minus their mean drift from the originals (one block).
 __global__ void k_var_recentre(float* __restrict__ pos, const float* __restrict__ pos_o, int P) {
+  pdl_enter();
   double s[4] = {0, 0, 0, 0};
   for (int i = threadIdx.x; i < P; i += blockDim.x) {
     s[0] += pos[2 * i];
@@ -87,6 +90,7 @@ __global__ void k_var_recentre(float* __restrict__ pos, const float* __restrict_
 
 // out += sum |a|^2 (FP64)
 __global__ void k_var_sumsq(const float2* __restrict__ a, size_t n, double* __restrict__ out) {
+  pdl_enter();
   double s = 0;
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
     s += double(a[i].x) * a[i].x + double(a[i].y) * a[i].y;
@@ -97,6 +101,7 @@ __global__ void k_var_sumsq(const float2* __restrict__ a, size_t n, double* __re
 // remove_extra_degree's scalars (one thread).  Its mean and norm loops run over m_probe_evolution.size() = 2 entries,
 // so only positions 0 and 1 are re-centred; kept as written.
 __global__ void k_var_remove(double* __restrict__ sc, double* __restrict__ evo, int P, int NN) {
+  pdl_enter();
   if (threadIdx.x != 0) return;
   double* e0 = evo;
   double* e1 = evo + P;
@@ -123,6 +128,7 @@ __global__ void k_var_remove(double* __restrict__ sc, double* __restrict__ evo, 
 }
 
 __global__ void k_var_scale(float2* __restrict__ a, size_t n, const double* __restrict__ f) {
+  pdl_enter();
   const float s = float(*f);
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
     a[i] = cscale(a[i], s);
@@ -134,6 +140,7 @@ __global__ void k_var_exit(const float2* __restrict__ obj, const float2* __restr
                            const int2* __restrict__ win, const int* __restrict__ members,
                            const int* __restrict__ gsize, int N, int Y, float2* __restrict__ objp,
                            float2* __restrict__ vp) {
+  pdl_enter();
   const int k = blockIdx.y;
   const size_t NN = size_t(N) * N;
   const bool live = k < *gsize;
@@ -154,6 +161,7 @@ __global__ void k_var_exit(const float2* __restrict__ obj, const float2* __restr
 // a_k *= e^{-2 pi i sign (s.x f[c] + s.y f[r])} / N^2 on the spectra of the group's windows (shift_probe)
 __global__ void k_var_phase(float2* __restrict__ a, const float2* __restrict__ sub, const int* __restrict__ members,
                             const int* __restrict__ gsize, int N, float sign) {
+  pdl_enter();
   const int k = blockIdx.y;
   if (k >= *gsize) return;
   const size_t NN = size_t(N) * N;
@@ -169,6 +177,7 @@ __global__ void k_var_phase(float2* __restrict__ a, const float2* __restrict__ s
 
 __global__ void k_var_psi(const float2* __restrict__ objp, const float2* __restrict__ vp, float2* __restrict__ psi,
                           size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
     psi[i] = cmul(objp[i], vp[i]);
 }
@@ -178,6 +187,7 @@ __global__ void k_var_dirs(const float2* __restrict__ chi, const float2* __restr
                            const float2* __restrict__ vp, const int2* __restrict__ win,
                            const int* __restrict__ members, const int* __restrict__ gsize, int N, int Y,
                            float2* __restrict__ pu, float2* __restrict__ S) {
+  pdl_enter();
   const int k = blockIdx.y;
   const size_t NN = size_t(N) * N;
   if (k >= *gsize) {
@@ -198,6 +208,7 @@ __global__ void k_var_pum(const float2* __restrict__ pu, const float* __restrict
                           const float* __restrict__ maxIllum, const int2* __restrict__ win,
                           const int* __restrict__ members, const int* __restrict__ gsize, int N, int Y,
                           float2* __restrict__ pum) {
+  pdl_enter();
   const int G = *gsize;
   const size_t NN = size_t(N) * N;
   const float damp = 0.01f * *maxIllum;
@@ -214,6 +225,7 @@ __global__ void k_var_pum(const float2* __restrict__ pu, const float* __restrict
 
 // Gradient spectra of the windows: from FFT2(objp) in aux[k], dX -> aux[k] (column frequencies), dY -> aux[Gmax + k]
 __global__ void k_var_grad(float2* __restrict__ aux, int Gmax, int N) {
+  pdl_enter();
   const int k = blockIdx.y;
   const size_t NN = size_t(N) * N;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
@@ -228,6 +240,7 @@ __global__ void k_var_grad(float2* __restrict__ aux, int Gmax, int N) {
 __global__ void k_var_possums(const float2* __restrict__ aux, const float2* __restrict__ vp,
                               const float2* __restrict__ chi, const int* __restrict__ gsize, int Gmax, int N,
                               double* __restrict__ out) {
+  pdl_enter();
   const int k = blockIdx.y;
   if (k >= *gsize) return;
   const size_t NN = size_t(N) * N;
@@ -253,6 +266,7 @@ __global__ void k_var_possums(const float2* __restrict__ aux, const float2* __re
 // coordinate) and the row-gradient one y, as gradient_position_solver pairs them.
 __global__ void k_var_posupd(double* __restrict__ s, const int* __restrict__ members, const int* __restrict__ gsize,
                              float* __restrict__ pos) {
+  pdl_enter();
   if (threadIdx.x != 0) return;
   const int G = *gsize;
   for (int k = 0; k < G; ++k) {
@@ -279,6 +293,7 @@ __global__ void k_var_proj(const float2* __restrict__ pu, const float2* __restri
                            const float* __restrict__ pobj, const float* __restrict__ pmax,
                            const float2* __restrict__ E, const int2* __restrict__ win, const int* __restrict__ members,
                            const int* __restrict__ gsize, int N, int Y, double* __restrict__ proj) {
+  pdl_enter();
   const int k = blockIdx.y;
   const int G = *gsize;
   if (k >= G) return;
@@ -297,6 +312,7 @@ __global__ void k_var_proj(const float2* __restrict__ pu, const float2* __restri
 // prj_k = (mean_pixels Re(E conj(resid_k)) + evo1_k) / sum_group evo1^2 (one thread); clears proj
 __global__ void k_var_prj(double* __restrict__ proj, double* __restrict__ prj, const double* __restrict__ evo, int P,
                           const int* __restrict__ members, const int* __restrict__ gsize, int NN) {
+  pdl_enter();
   if (threadIdx.x != 0) return;
   const int G = *gsize;
   double evn = 0;
@@ -313,6 +329,7 @@ __global__ void k_var_upd(const float2* __restrict__ pu, const float2* __restric
                           const double* __restrict__ prj, const int2* __restrict__ win, const int* __restrict__ members,
                           const int* __restrict__ gsize, int N, int Y, float2* __restrict__ upd,
                           double* __restrict__ usum) {
+  pdl_enter();
   const int G = *gsize;
   const float ip = 1.f / *pmax, invG = 1.f / float(G), nrm = 1.f / float(N * N);
   double acc = 0;
@@ -333,6 +350,7 @@ __global__ void k_var_upd(const float2* __restrict__ pu, const float2* __restric
 // E += upd relax_U / max(1, rms(upd)); enew += sum |E|^2
 __global__ void k_var_eapply(float2* __restrict__ E, const float2* __restrict__ upd, int NN, const int* __restrict__ gsize,
                              int P, const double* __restrict__ usum, double* __restrict__ enew) {
+  pdl_enter();
   const double rms = sqrt(*usum / NN);
   const float us = float((double(*gsize) / P) / (rms > 1.0 ? rms : 1.0));
   double acc = 0;
@@ -346,6 +364,7 @@ __global__ void k_var_eapply(float2* __restrict__ E, const float2* __restrict__ 
 }
 
 __global__ void k_var_enorm(float2* __restrict__ E, int NN, const double* __restrict__ enew) {
+  pdl_enter();
   const float f = float(1.0 / sqrt(*enew / NN));
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += gridDim.x * blockDim.x) E[i] = cscale(E[i], f);
 }
@@ -354,6 +373,7 @@ __global__ void k_var_enorm(float2* __restrict__ E, int NN, const double* __rest
 __global__ void k_var_evosums(const float2* __restrict__ objp, const float2* __restrict__ E,
                               const float2* __restrict__ probe, const float2* __restrict__ chi,
                               const int* __restrict__ gsize, int N, double* __restrict__ out) {
+  pdl_enter();
   const int k = blockIdx.y;
   if (k >= *gsize) return;
   const size_t NN = size_t(N) * N;
@@ -377,6 +397,7 @@ __global__ void k_var_evosums(const float2* __restrict__ objp, const float2* __r
 // clears the sums of this group's variable update
 __global__ void k_var_evoupd(double* __restrict__ s, double* __restrict__ sc, double* __restrict__ evo, int P,
                              const int* __restrict__ members, const int* __restrict__ gsize, int NN) {
+  pdl_enter();
   if (threadIdx.x != 0) return;
   const int G = *gsize;
   double dm = 0;
@@ -401,6 +422,7 @@ struct ZonePlate {
 };
 
 __global__ void k_fzp_start(float2* __restrict__ probe, float2* __restrict__ pf, int N, ZonePlate z) {
+  pdl_enter();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
     const int r = i / N, c = i % N;
     const double x = z.start + z.step * c, y = z.start + z.step * r;
@@ -421,11 +443,13 @@ __global__ void k_fzp_start(float2* __restrict__ probe, float2* __restrict__ pf,
 
 // pf = FFT2(kern) pf
 __global__ void k_fzp_mul(const float2* __restrict__ spec, float2* __restrict__ pf, int n) {
+  pdl_enter();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) pf[i] = cmul(spec[i], pf[i]);
 }
 
 // probe = fftshift(pf)
 __global__ void k_fzp_shift(const float2* __restrict__ pf, float2* __restrict__ probe, int N) {
+  pdl_enter();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
     const int r = i / N, c = i % N;
     probe[size_t((r + N / 2) % N) * N + (c + N / 2) % N] = pf[i];
@@ -435,6 +459,7 @@ __global__ void k_fzp_shift(const float2* __restrict__ pf, float2* __restrict__ 
 // Exit waves of modes 1..K-1: psik[m-1][k] = P_m objp_k
 __global__ void k_var_psik(const float2* __restrict__ probe, const float2* __restrict__ objp, float2* __restrict__ psik,
                            int K, int Gmax, size_t NN) {
+  pdl_enter();
   const size_t n = size_t(K - 1) * Gmax * NN;
   for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < n; t += size_t(gridDim.x) * blockDim.x) {
     const size_t i = t % NN, k = (t / NN) % Gmax, m = t / (NN * Gmax) + 1;
@@ -447,6 +472,7 @@ __global__ void k_var_psik(const float2* __restrict__ probe, const float2* __res
 __global__ void k_var_modulus(float2* __restrict__ spec, float2* __restrict__ psik, const float* __restrict__ amp,
                               const int* __restrict__ members, const int* __restrict__ gsize, int N, int K, int Gmax,
                               double* __restrict__ err) {
+  pdl_enter();
   const int k = blockIdx.y;
   if (k >= *gsize) return;
   const size_t NN = size_t(N) * N, GN = size_t(Gmax) * NN;
@@ -477,6 +503,7 @@ __global__ void k_var_mode_update(const float2* __restrict__ chim, const float2*
                                   const int2* __restrict__ win, const int* __restrict__ members,
                                   const int* __restrict__ gsize, int N, int Y, const double* __restrict__ betas,
                                   float2* __restrict__ mode) {
+  pdl_enter();
   const int G = *gsize;
   const size_t NN = size_t(N) * N;
   const float damp = 0.01f * *maxIllum, invG = 1.f / float(G);
@@ -495,6 +522,7 @@ __global__ void k_var_mode_update(const float2* __restrict__ chim, const float2*
 // ortho_modes (src/Probe.cpp:244-294) in one block: Gram-Schmidt in mode order with powers taken before each mode's
 // projections, then modes 1..K-1 take the modes ranked 1..K-1 by that power (mode 0 stays, as written)
 __global__ void k_var_ortho(float2* __restrict__ modes, float2* __restrict__ tmp, int K, int NN) {
+  pdl_enter();
   __shared__ double pw[64];
   __shared__ float2 proj;
   __shared__ int rank[64];
@@ -544,6 +572,7 @@ __global__ void k_var_ortho(float2* __restrict__ modes, float2* __restrict__ tmp
 
 // m_k = m_0 e^{-2 pi i (t1 (c/N - 0.5) + t2 (r/N - 0.5))}, k >= 1 (FP64 phase)
 __global__ void k_mode_tilts(float2* __restrict__ probe, int K, int N, const double* __restrict__ tilts) {
+  pdl_enter();
   const size_t NN = size_t(N) * N;
   for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < size_t(K - 1) * NN;
        t += size_t(gridDim.x) * blockDim.x) {
@@ -559,6 +588,7 @@ __global__ void k_mode_tilts(float2* __restrict__ probe, int K, int N, const dou
 
 // gram[i K + j] = sum conj(m_i) m_j, one block per pair
 __global__ void k_mode_gram(const float2* __restrict__ probe, int K, int NN, double2* __restrict__ gram) {
+  pdl_enter();
   const int i = blockIdx.x / K, j = blockIdx.x % K;
   double sr = 0, si = 0;
   for (int t = threadIdx.x; t < NN; t += blockDim.x) {
@@ -575,6 +605,7 @@ __global__ void k_mode_gram(const float2* __restrict__ probe, int K, int NN, dou
 // tmp_i = sum_q V(q, i) m_q, then copied back
 __global__ void k_mode_combine(const float2* __restrict__ probe, float2* __restrict__ tmp, int K, int NN,
                                const double2* __restrict__ V) {
+  pdl_enter();
   for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < size_t(K) * NN; t += size_t(gridDim.x) * blockDim.x) {
     const int i = int(t / NN);
     const size_t p = t % NN;
@@ -589,6 +620,218 @@ __global__ void k_mode_combine(const float2* __restrict__ probe, float2* __restr
   }
 }
 
+// ---- FFT passes with fused loads and stores -------------------------------------------------------------------
+// One row-transform pass of the batched 2-D FFT (the k_fft_rows_t scheme: R rows per CTA, transposed store) with a
+// prologue that produces each loaded element (plane b, row x, column y) and an epilogue that maps each stored element
+// (plane b, row x, column y of the natural layout after the second pass) and may accumulate per-plane sums, finished
+// once per CTA.  The first pass of a 2-D transform takes a prologue and stores plainly into the transposed work
+// plane; the second loads plainly and takes an epilogue.
+struct ProLoad {
+  const float2* in;
+  __device__ float2 operator()(int b, int x, int y, int L) const { return in[(size_t(b) * L + x) * L + y]; }
+};
+struct EpiStore {
+  __device__ float2 operator()(int, int, int, int, float2 v) { return v; }
+  __device__ void finish(int) {}
+};
+
+template <int L, bool INV, class Pro, class Epi>
+__global__ void __launch_bounds__(FftShape<L>::THREADS) k_fftx_pass(float2* __restrict__ out,
+                                                                    const float2* __restrict__ g_tw, Pro pro, Epi epi) {
+  pdl_enter();
+  using S = FftShape<L>;
+  constexpr int T = S::T, E = S::E, R = S::RC;
+  extern __shared__ float4 smem4[];
+  float2* smem = reinterpret_cast<float2*>(smem4);
+  float2* s_tw = smem;
+  float2* s_x = smem + L;
+  const int v = threadIdx.x / T, t = threadIdx.x % T, b = blockIdx.y;
+  const int x0 = blockIdx.x * R;
+  load_twiddles<L>(s_tw, g_tw);
+  __syncthreads();
+  float2 a[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) a[e] = pro(b, x0 + v, t + T * e, L);
+  fft_vec<L, INV>(a, t, s_x + v * S::XCH, s_tw);
+  __syncthreads();  // the staging tile aliases the exchange buffers of other warps
+  static_for<0, E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    s_x[(t + T * e) * (R + 1) + v] = a[out_slot<L>(e)];
+  });
+  __syncthreads();
+  float2* o = out + size_t(b) * L * L;
+  for (int i = threadIdx.x; i < L * R; i += blockDim.x) {
+    const int vv = i % R, n = i / R;
+    o[size_t(n) * L + x0 + vv] = epi(b, n, x0 + vv, L, s_x[n * (R + 1) + vv]);
+  }
+  epi.finish(b);
+}
+
+template <int L, bool INV, class Pro, class Epi>
+cudaError_t launch_fftx(float2* out, const float2* tw, int batch, Pro pro, Epi epi, cudaStream_t st) {
+  constexpr int R = FftShape<L>::RC, NT = FftShape<L>::THREADS;
+  const size_t smem = rows_smem_bytes<L>();
+  cudaError_t e = cudaFuncSetAttribute(k_fftx_pass<L, INV, Pro, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem));
+  if (e != cudaSuccess) return e;
+  return launch_pdl(k_fftx_pass<L, INV, Pro, Epi>, dim3(L / R, batch), NT, smem, st, out, tw, pro, epi);
+}
+
+// 2-D transform data-in (through pro) -> work (transposed) -> out (through epi)
+template <bool INV, class Pro, class Epi>
+cudaError_t fftx2(int N, float2* work, float2* out, const float2* tw, int batch, Pro pro, Epi epi, cudaStream_t st) {
+  cudaError_t e;
+#define PTY_FFTX(L)                                                                            \
+  case L:                                                                                      \
+    if ((e = launch_fftx<L, INV>(work, tw, batch, pro, EpiStore{}, st)) != cudaSuccess) return e; \
+    return launch_fftx<L, INV>(out, tw, batch, ProLoad{work}, epi, st);
+  switch (N) {
+    PTY_FFTX(32)
+    PTY_FFTX(64)
+    PTY_FFTX(128)
+    PTY_FFTX(256)
+    PTY_FFTX(512)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef PTY_FFTX
+}
+
+// Batched 2-D FFT in natural layout like fft2, both passes launched with programmatic dependent launch.
+cudaError_t fft2_pdl_impl(float2* data, float2* work, const float2* tw, int batch, int N, bool inverse, cudaStream_t st) {
+  return inverse ? fftx2<true>(N, work, data, tw, batch, ProLoad{data}, EpiStore{}, st)
+                 : fftx2<false>(N, work, data, tw, batch, ProLoad{data}, EpiStore{}, st);
+}
+
+// Prologue of the probes' forward transform: objp_b = O[window_b] (stored on the side) and vp_b = P evo0 + E evo1
+struct ProExit {
+  const float2 *obj, *probe, *E;
+  const double* evo;
+  const int2* win;
+  const int *members, *gsize;
+  float2* objp;
+  int P, Y;
+  __device__ float2 operator()(int b, int x, int y, int L) const {
+    const size_t i = size_t(x) * L + y, k = size_t(b) * L * L + i;
+    if (b >= *gsize) {
+      objp[k] = make_float2(0.f, 0.f);
+      return make_float2(0.f, 0.f);
+    }
+    const int j = members[b];
+    const int2 s = win[j];
+    objp[k] = obj[size_t(s.x + x) * Y + (s.y + y)];
+    return cadd(cscale(probe[i], float(evo[j])), cscale(E[i], float(evo[P + j])));
+  }
+};
+
+// Spectrum times e^{-2 pi i sign (s.x f[y] + s.y f[x])} / N^2 (shift_probe)
+struct EpiPhase {
+  const float2* sub;
+  const int *members, *gsize;
+  float sign;
+  __device__ float2 operator()(int b, int x, int y, int L, float2 v) {
+    if (b >= *gsize) return v;
+    const float2 s = sub[members[b]];
+    const float tt = sign * (s.x * fft_freq(y, L) + s.y * fft_freq(x, L));
+    float sn, cs;
+    sincosf(-kTwoPi * tt, &sn, &cs);
+    const float nrm = 1.f / float(L * L);
+    return cmul(v, make_float2(cs * nrm, sn * nrm));
+  }
+  __device__ void finish(int) {}
+};
+
+// The shifted probe is stored; the exit wave psi = objp vp goes on the side
+struct EpiVpPsi {
+  const float2* objp;
+  float2* psi;
+  __device__ float2 operator()(int b, int x, int y, int L, float2 v) {
+    const size_t k = (size_t(b) * L + x) * L + y;
+    psi[k] = cmul(objp[k], v);
+    return v;
+  }
+  __device__ void finish(int) {}
+};
+
+// Modulus (one probe mode): Psi (A/(|Psi| + 1e-9) - 1)/N^2 and the Fourier error of the window
+struct EpiModulus {
+  const float* amp;
+  const int *members, *gsize;
+  double* err;
+  double e;
+  __device__ float2 operator()(int b, int x, int y, int L, float2 v) {
+    if (b >= *gsize) return v;
+    const float ap = sqrtf(v.x * v.x + v.y * v.y);
+    const float A = amp[size_t(members[b]) * L * L + size_t(x) * L + y];
+    e += double(A - ap) * double(A - ap) * 0.25;
+    return cscale(v, (A / (ap + 1e-9f) - 1.f) * (1.f / float(L * L)));
+  }
+  __device__ void finish(int b) {
+    const double r = block_reduce_sum(e);
+    if (threadIdx.x == 0 && b < *gsize) atomicAdd(&err[b], r);
+  }
+};
+
+// chi is stored; pu = chi conj(objp) and S += chi conj(vp) at the window go on the side
+struct EpiChi {
+  const float2 *objp, *vp;
+  const int2* win;
+  const int *members, *gsize;
+  float2 *pu, *S;
+  int Y;
+  __device__ float2 operator()(int b, int x, int y, int L, float2 v) {
+    const size_t k = (size_t(b) * L + x) * L + y;
+    if (b >= *gsize) {
+      pu[k] = make_float2(0.f, 0.f);
+      return v;
+    }
+    pu[k] = cmulc(v, objp[k]);
+    const int2 s = win[members[b]];
+    atomicAdd(&S[size_t(s.x + x) * Y + (s.y + y)], cmulc(v, vp[k]));
+    return v;
+  }
+  __device__ void finish(int) {}
+};
+
+// Gradient spectra: d = 2 pi i FFT2(objp); dX = d f[y] stored, dY = d f[x] into plane Gmax + b
+struct EpiGrad {
+  float2* dy;  // aux + Gmax N^2
+  __device__ float2 operator()(int b, int x, int y, int L, float2 v) {
+    const float2 d = cmul(v, make_float2(0.f, kTwoPi));
+    dy[(size_t(b) * L + x) * L + y] = cscale(d, fft_freq(x, L));
+    return cscale(d, fft_freq(y, L));
+  }
+  __device__ void finish(int) {}
+};
+
+// Position-search sums of the gradient images (planes b < Gmax: dX of window b, else dY of window b - Gmax)
+struct EpiPosSums {
+  const float2 *vp, *chi;
+  const int* gsize;
+  double* out;
+  int Gmax;
+  double s0, s1;
+  __device__ float2 operator()(int b, int x, int y, int L, float2 v) {
+    const int k = b < Gmax ? b : b - Gmax;
+    if (k >= *gsize) return v;
+    const size_t i = (size_t(k) * L + x) * L + y;
+    const float2 g = cmul(cscale(v, 1.f / float(L * L)), vp[i]), c = chi[i];
+    s0 += double(g.x) * g.x + double(g.y) * g.y;
+    s1 += double(c.x) * g.x + double(c.y) * g.y;
+    return v;
+  }
+  __device__ void finish(int b) {
+    const double r0 = block_reduce_sum(s0);
+    __syncthreads();
+    const double r1 = block_reduce_sum(s1);
+    const int k = b < Gmax ? b : b - Gmax, m = b < Gmax ? 0 : 2;
+    if (threadIdx.x == 0 && k < *gsize) {
+      atomicAdd(&out[4 * k + m], r0);
+      atomicAdd(&out[4 * k + m + 1], r1);
+    }
+  }
+};
+
 int grid_n(size_t n, int cap = 1184) {
   size_t g = (n + 255) / 256;
   return int(g < 1 ? 1 : (g > size_t(cap) ? cap : g));
@@ -598,20 +841,24 @@ int grid_n(size_t n, int cap = 1184) {
 
 size_t mls_var_scratch_doubles(int Gmax) { return 10 * size_t(Gmax) + 8; }
 
+cudaError_t fft2_pdl(float2* data, float2* work, const float2* tw, int batch, int N, bool inverse, cudaStream_t st) {
+  return fft2_pdl_impl(data, work, tw, batch, N, inverse, st);
+}
+
 cudaError_t mls_mode_tilts(float2* probe, int K, int N, const double* tilts, cudaStream_t st) {
   if (K < 2) return cudaSuccess;
-  k_mode_tilts<<<grid_n(size_t(K - 1) * N * N), 256, 0, st>>>(probe, K, N, tilts);
+  launch_pdl(k_mode_tilts, grid_n(size_t(K - 1) * N * N), 256, 0, st, probe, K, N, tilts);
   return cudaGetLastError();
 }
 
 cudaError_t mls_mode_gram(const float2* probe, int K, int N, double2* gram, cudaStream_t st) {
-  k_mode_gram<<<K * K, 256, 0, st>>>(probe, K, N * N, gram);
+  launch_pdl(k_mode_gram, K * K, 256, 0, st, probe, K, N * N, gram);
   return cudaGetLastError();
 }
 
 cudaError_t mls_mode_combine(float2* probe, float2* tmp, int K, int N, const double2* V, cudaStream_t st) {
   const size_t n = size_t(K) * N * N;
-  k_mode_combine<<<grid_n(n), 256, 0, st>>>(probe, tmp, K, N * N, V);
+  launch_pdl(k_mode_combine, grid_n(n), 256, 0, st, probe, tmp, K, N * N, V);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return cudaMemcpyAsync(probe, tmp, n * sizeof(float2), cudaMemcpyDeviceToDevice, st);
@@ -636,29 +883,27 @@ cudaError_t mls_zone_plate_probe(float2* probe, float2* pf, float2* work, const 
   z.kzc = std::cos(k * zz);
   z.kzs = std::sin(k * zz);
   const int NN = N * N;
-  k_fzp_start<<<grid_n(NN), 256, 0, st>>>(probe, pf, N, z);
+  launch_pdl(k_fzp_start, grid_n(NN), 256, 0, st, probe, pf, N, z);
   cudaError_t e = fft2(probe, work, tw, 1, N, false, st);
   if (e != cudaSuccess) return e;
-  k_fzp_mul<<<grid_n(NN), 256, 0, st>>>(probe, pf, NN);
-  k_fzp_shift<<<grid_n(NN), 256, 0, st>>>(pf, probe, N);
+  launch_pdl(k_fzp_mul, grid_n(NN), 256, 0, st, probe, pf, NN);
+  launch_pdl(k_fzp_shift, grid_n(NN), 256, 0, st, pf, probe, N);
   return cudaGetLastError();
 }
 
-int mls_var_launches_per_iteration(int ngroups, unsigned flags) {
-  int pre = 2 + 3 + 1 + 3 + 2;  // windows?, boxes, norm (3 + E), recentre, illumination, max
+int mls_var_launches_per_iteration(int ngroups, unsigned flags, int K, bool tc) {
+  int pre = 1 + 4 + 1 + 2 + 1;  // boxes, norm (sums + 3 scales), recentre, illumination (2), max
   if (flags & MLS_WINDOWS) ++pre;
   if (flags & MLS_REMOVE) pre += 4;
-  // per group: exit, 2 FFT2 + phase, psi, 2 FFT2 + modulus, dirs, 2 FFT2 + phase, pum, lsq, solve + 2 updates
-  int per = 1 + 5 + 1 + 5 + 1 + 5 + 1 + 1 + 3;
-  if (flags & MLS_POSSEARCH) per += 2 + 1 + 2 + 1 + 1;  // FFT2, grad, FFT2 (2 G), sums, update
+  // per group: six 2-D transforms of two passes; FP32 fuses exit, both phase ramps, psi, the one-mode modulus and
+  // the directions into them, the tensor-core path runs them as 6 kernels (the modulus only for one mode); then
+  // pum, lsq, solve and the two updates
+  int per = 12 + 5 + (tc ? 6 + (K == 1 ? 1 : 0) : 0);
+  if (flags & MLS_POSSEARCH) per += tc ? 2 + 1 + 2 + 1 + 1 : 2 + 2 + 1;
   if (flags & MLS_VARUPD) per += 7;
-  return pre + ngroups * per;
-}
-
-int mls_var_mode_launches(int ngroups, int K) {
-  // per group: other modes' exit waves, their FFT2 and inverse, the modal modulus in place of the plain one, one
-  // update per extra mode; one orthogonalisation per iteration
-  return K > 1 ? ngroups * (1 + 2 + 2 + (K - 1)) + 1 : 0;
+  // other modes: exit waves, forward and inverse 2-D transforms, the modal modulus, one update each
+  if (K > 1) per += 1 + 2 + 1 + 2 + (K - 1);
+  return pre + ngroups * per + (K > 1 ? 1 : 0);
 }
 
 cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, cudaStream_t st) {
@@ -668,10 +913,10 @@ cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, 
   double* sc = b.vs + L.sc();
   cudaError_t e;
   auto fft = [&](float2* d, int batch, bool inv) {
-    return b.tc ? fft2_tc(d, b.work, batch, N, inv, b.tc_err, st) : fft2(d, b.work, b.tw, batch, N, inv, st);
+    return b.tc ? fft2_tc(d, b.work, batch, N, inv, b.tc_err, st) : fft2_pdl(d, b.work, b.tw, batch, N, inv, st);
   };
   if (flags & MLS_WINDOWS)
-    k_var_windows<<<(P + 255) / 256, 256, 0, st>>>(b.pos, P, N, b.X, b.Y, b.cvx, b.cvy, b.win, b.sub);
+    launch_pdl(k_var_windows, (P + 255) / 256, 256, 0, st, b.pos, P, N, b.X, b.Y, b.cvx, b.cvy, b.win, b.sub);
   if ((e = mls_group_boxes(b.win, b.members, b.gsize, ngroups, b.Gmax, N, b.boxw, st)) != cudaSuccess) return e;
   // calc_object_norm over the object ROI with the current illumination weights: P, E scaled by on, O by 1/on
   if ((e = mls_norm_sums(b.pobj, b.obj, b.Y, b.roi[0], b.roi[1], b.roi[2], b.roi[3], 1, b.normsums, st)) != cudaSuccess)
@@ -679,12 +924,12 @@ cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, 
   if ((e = scale_by_norm(b.probe, size_t(b.K) * NN, b.normsums, 0, st)) != cudaSuccess) return e;
   if ((e = scale_by_norm(b.E, NN, b.normsums, 0, st)) != cudaSuccess) return e;
   if ((e = scale_by_norm(b.obj, XY, b.normsums, 1, st)) != cudaSuccess) return e;
-  k_var_recentre<<<1, 256, 0, st>>>(b.pos, b.pos_o, P);
+  launch_pdl(k_var_recentre, 1, 256, 0, st, b.pos, b.pos_o, P);
   if (flags & MLS_REMOVE) {
-    k_var_sumsq<<<grid_n(NN, 64), 256, 0, st>>>(b.E, NN, sc + SC_ESUM);
-    k_var_remove<<<1, 32, 0, st>>>(sc, b.evo, P, NN);
-    k_var_scale<<<grid_n(NN), 256, 0, st>>>(b.E, NN, sc + SC_EFAC);
-    k_var_scale<<<grid_n(NN), 256, 0, st>>>(b.probe, NN, sc + SC_PFAC);
+    launch_pdl(k_var_sumsq, grid_n(NN, 64), 256, 0, st, b.E, NN, sc + SC_ESUM);
+    launch_pdl(k_var_remove, 1, 32, 0, st, sc, b.evo, P, NN);
+    launch_pdl(k_var_scale, grid_n(NN), 256, 0, st, b.E, NN, sc + SC_EFAC);
+    launch_pdl(k_var_scale, grid_n(NN), 256, 0, st, b.probe, NN, sc + SC_PFAC);
   }
   // updated_cached_illumination: p = (p + sum |P|^2 at the windows) / 2; its maximum for the variable update
   if ((e = scale_real(b.pobj, XY, 0.5f, st)) != cudaSuccess) return e;
@@ -695,52 +940,81 @@ cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, 
   for (int g = 0; g < ngroups; ++g) {
     const int* mem = b.members + size_t(g) * b.Gmax;
     const int* gs = b.gsize + g;
-    k_var_exit<<<grid, 256, 0, st>>>(b.obj, b.probe, b.E, b.evo, P, b.win, mem, gs, N, b.Y, b.objp, b.vp);
-    if ((e = fft(b.vp, b.Gmax, false)) != cudaSuccess) return e;
-    k_var_phase<<<grid, 256, 0, st>>>(b.vp, b.sub, mem, gs, N, 1.f);
-    if ((e = fft(b.vp, b.Gmax, true)) != cudaSuccess) return e;
-    k_var_psi<<<grid_n(GN), 256, 0, st>>>(b.objp, b.vp, b.psi, GN);
-    if ((e = fft(b.psi, b.Gmax, false)) != cudaSuccess) return e;
+    if (b.tc) {  // tensor-core transforms: separate pointwise kernels around fft2_tc
+      launch_pdl(k_var_exit, grid, 256, 0, st, b.obj, b.probe, b.E, b.evo, P, b.win, mem, gs, N, b.Y, b.objp, b.vp);
+      if ((e = fft(b.vp, b.Gmax, false)) != cudaSuccess) return e;
+      launch_pdl(k_var_phase, grid, 256, 0, st, b.vp, b.sub, mem, gs, N, 1.f);
+      if ((e = fft(b.vp, b.Gmax, true)) != cudaSuccess) return e;
+      launch_pdl(k_var_psi, grid_n(GN), 256, 0, st, b.objp, b.vp, b.psi, GN);
+      if ((e = fft(b.psi, b.Gmax, false)) != cudaSuccess) return e;
+    } else {  // FP32 transforms with the pointwise steps fused into their loads and stores
+      const ProExit pe{b.obj, b.probe, b.E, b.evo, b.win, mem, gs, b.objp, P, b.Y};
+      if ((e = fftx2<false>(N, b.work, b.vp, b.tw, b.Gmax, pe, EpiPhase{b.sub, mem, gs, 1.f}, st)) != cudaSuccess)
+        return e;
+      if ((e = fftx2<true>(N, b.work, b.vp, b.tw, b.Gmax, ProLoad{b.vp}, EpiVpPsi{b.objp, b.psi}, st)) != cudaSuccess)
+        return e;
+      if (b.K == 1) {
+        if ((e = fftx2<false>(N, b.work, b.psi, b.tw, b.Gmax, ProLoad{b.psi}, EpiModulus{b.amp, mem, gs, b.errk, 0.0},
+                              st)) != cudaSuccess)
+          return e;
+      } else if ((e = fft(b.psi, b.Gmax, false)) != cudaSuccess) {
+        return e;
+      }
+    }
     if (b.K > 1) {
-      k_var_psik<<<grid_n(size_t(b.K - 1) * GN), 256, 0, st>>>(b.probe, b.objp, b.psik, b.K, b.Gmax, NN);
+      launch_pdl(k_var_psik, grid_n(size_t(b.K - 1) * GN), 256, 0, st, b.probe, b.objp, b.psik, b.K, b.Gmax, NN);
       if ((e = fft(b.psik, (b.K - 1) * b.Gmax, false)) != cudaSuccess) return e;
-      k_var_modulus<<<grid, 256, 0, st>>>(b.psi, b.psik, b.amp, mem, gs, N, b.K, b.Gmax, b.errk);
+      launch_pdl(k_var_modulus, grid, 256, 0, st, b.psi, b.psik, b.amp, mem, gs, N, b.K, b.Gmax, b.errk);
       if ((e = fft(b.psik, (b.K - 1) * b.Gmax, true)) != cudaSuccess) return e;
-    } else if ((e = mls_modulus(b, mem, gs, st)) != cudaSuccess) {
+    } else if (b.tc && (e = mls_modulus(b, mem, gs, st)) != cudaSuccess) {
       return e;
     }
-    if ((e = fft(b.psi, b.Gmax, true)) != cudaSuccess) return e;
-    k_var_dirs<<<grid, 256, 0, st>>>(b.psi, b.objp, b.vp, b.win, mem, gs, N, b.Y, b.pu, b.S);
-    if ((e = fft(b.pu, b.Gmax, false)) != cudaSuccess) return e;
-    k_var_phase<<<grid, 256, 0, st>>>(b.pu, b.sub, mem, gs, N, -1.f);
+    if (b.tc) {
+      if ((e = fft(b.psi, b.Gmax, true)) != cudaSuccess) return e;
+      launch_pdl(k_var_dirs, grid, 256, 0, st, b.psi, b.objp, b.vp, b.win, mem, gs, N, b.Y, b.pu, b.S);
+      if ((e = fft(b.pu, b.Gmax, false)) != cudaSuccess) return e;
+      launch_pdl(k_var_phase, grid, 256, 0, st, b.pu, b.sub, mem, gs, N, -1.f);
+    } else {
+      const EpiChi ec{b.objp, b.vp, b.win, mem, gs, b.pu, b.S, b.Y};
+      if ((e = fftx2<true>(N, b.work, b.psi, b.tw, b.Gmax, ProLoad{b.psi}, ec, st)) != cudaSuccess) return e;
+      if ((e = fftx2<false>(N, b.work, b.pu, b.tw, b.Gmax, ProLoad{b.pu}, EpiPhase{b.sub, mem, gs, -1.f}, st)) !=
+          cudaSuccess)
+        return e;
+    }
     if ((e = fft(b.pu, b.Gmax, true)) != cudaSuccess) return e;
-    k_var_pum<<<grid_n(NN, 256), 256, 0, st>>>(b.pu, b.pobj, b.maxIllum, b.win, mem, gs, N, b.Y, b.pum);
+    launch_pdl(k_var_pum, grid_n(NN, 256), 256, 0, st, b.pu, b.pobj, b.maxIllum, b.win, mem, gs, N, b.Y, b.pum);
     if ((e = mls_lsq(b, b.vp, NN, mem, gs, st)) != cudaSuccess) return e;
     if ((e = mls_solve_update(b, mem, gs, b.boxw + 4 * size_t(g), 0, st)) != cudaSuccess) return e;
-    if (flags & MLS_POSSEARCH) {
+    if ((flags & MLS_POSSEARCH) && b.tc) {
       if ((e = cudaMemcpyAsync(b.aux, b.objp, GN * sizeof(float2), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
         return e;
       if ((e = fft(b.aux, b.Gmax, false)) != cudaSuccess) return e;
-      k_var_grad<<<grid, 256, 0, st>>>(b.aux, b.Gmax, N);
+      launch_pdl(k_var_grad, grid, 256, 0, st, b.aux, b.Gmax, N);
       if ((e = fft(b.aux, 2 * b.Gmax, true)) != cudaSuccess) return e;
-      k_var_possums<<<grid, 256, 0, st>>>(b.aux, b.vp, b.psi, gs, b.Gmax, N, b.vs + L.pos());
-      k_var_posupd<<<1, 32, 0, st>>>(b.vs + L.pos(), mem, gs, b.pos);
+      launch_pdl(k_var_possums, grid, 256, 0, st, b.aux, b.vp, b.psi, gs, b.Gmax, N, b.vs + L.pos());
+      launch_pdl(k_var_posupd, 1, 32, 0, st, b.vs + L.pos(), mem, gs, b.pos);
+    } else if (flags & MLS_POSSEARCH) {
+      if ((e = fftx2<false>(N, b.work, b.aux, b.tw, b.Gmax, ProLoad{b.objp}, EpiGrad{b.aux + GN}, st)) != cudaSuccess)
+        return e;
+      const EpiPosSums ps{b.vp, b.psi, gs, b.vs + L.pos(), b.Gmax, 0.0, 0.0};
+      if ((e = fftx2<true>(N, b.work, b.aux, b.tw, 2 * b.Gmax, ProLoad{b.aux}, ps, st)) != cudaSuccess) return e;
+      launch_pdl(k_var_posupd, 1, 32, 0, st, b.vs + L.pos(), mem, gs, b.pos);
     }
     if (flags & MLS_VARUPD) {
-      k_var_proj<<<grid, 256, 0, st>>>(b.pu, b.pum, b.pobj, b.pmax, b.E, b.win, mem, gs, N, b.Y, b.vs + L.proj());
-      k_var_prj<<<1, 32, 0, st>>>(b.vs + L.proj(), b.vs + L.prj(), b.evo, P, mem, gs, NN);
-      k_var_upd<<<grid_n(NN, 256), 256, 0, st>>>(b.pu, b.pum, b.pobj, b.pmax, b.vs + L.prj(), b.win, mem, gs, N, b.Y,
+      launch_pdl(k_var_proj, grid, 256, 0, st, b.pu, b.pum, b.pobj, b.pmax, b.E, b.win, mem, gs, N, b.Y, b.vs + L.proj());
+      launch_pdl(k_var_prj, 1, 32, 0, st, b.vs + L.proj(), b.vs + L.prj(), b.evo, P, mem, gs, NN);
+      launch_pdl(k_var_upd, grid_n(NN, 256), 256, 0, st, b.pu, b.pum, b.pobj, b.pmax, b.vs + L.prj(), b.win, mem, gs, N, b.Y,
                                                   b.aux, sc + SC_USUM);
-      k_var_eapply<<<grid_n(NN, 256), 256, 0, st>>>(b.E, b.aux, NN, gs, P, sc + SC_USUM, sc + SC_ENEW);
-      k_var_enorm<<<grid_n(NN, 256), 256, 0, st>>>(b.E, NN, sc + SC_ENEW);
-      k_var_evosums<<<grid, 256, 0, st>>>(b.objp, b.E, b.probe, b.psi, gs, N, b.vs + L.evs());
-      k_var_evoupd<<<1, 32, 0, st>>>(b.vs + L.evs(), sc, b.evo, P, mem, gs, NN);
+      launch_pdl(k_var_eapply, grid_n(NN, 256), 256, 0, st, b.E, b.aux, NN, gs, P, sc + SC_USUM, sc + SC_ENEW);
+      launch_pdl(k_var_enorm, grid_n(NN, 256), 256, 0, st, b.E, NN, sc + SC_ENEW);
+      launch_pdl(k_var_evosums, grid, 256, 0, st, b.objp, b.E, b.probe, b.psi, gs, N, b.vs + L.evs());
+      launch_pdl(k_var_evoupd, 1, 32, 0, st, b.vs + L.evs(), sc, b.evo, P, mem, gs, NN);
     }
     for (int m = 1; m < b.K; ++m)  // modes past the first: their directions with the group's probe step
-      k_var_mode_update<<<grid_n(NN, 256), 256, 0, st>>>(b.psik + size_t(m - 1) * GN, b.objp, b.pobj, b.maxIllum,
+      launch_pdl(k_var_mode_update, grid_n(NN, 256), 256, 0, st, b.psik + size_t(m - 1) * GN, b.objp, b.pobj, b.maxIllum,
                                                           b.win, mem, gs, N, b.Y, b.betas, b.probe + size_t(m) * NN);
   }
-  if (b.K > 1) k_var_ortho<<<1, 1024, 0, st>>>(b.probe, b.mtmp, b.K, NN);
+  if (b.K > 1) launch_pdl(k_var_ortho, 1, 1024, 0, st, b.probe, b.mtmp, b.K, NN);
   return cudaGetLastError();
 }
 

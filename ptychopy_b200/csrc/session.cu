@@ -1020,7 +1020,7 @@ double step_mls(pty_session* s, bool want_err) {
       check_cuda(e3, "graph instantiate");
     }
     check_cuda(cudaGraphLaunch(ge, s->stream), "MLs graph launch");
-    s->launches += mls_var_launches_per_iteration(ml->ng, flags) + mls_var_mode_launches(ml->ng, s->K);
+    s->launches += mls_var_launches_per_iteration(ml->ng, flags, s->K, s->prm.precision != 0);
   } else {
   if (!tb.graph) {
     const MlsBuffers b = mls_buffers(s, parity);

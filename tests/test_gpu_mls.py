@@ -88,6 +88,27 @@ def test_mls_zone_plate_probe_start(oracle):
     s.close()
 
 
+def test_mls_default_path_tensor_core_fft(oracle):
+    """precision=1 on the default path: the transforms run as split-BF16 tensor-core stages with the pointwise steps
+    as separate kernels (the FP32 path fuses them into its FFT passes); both against the FP64 oracle."""
+    d = mls_dataset(oracle, N=256, nx=3, shifted=True)
+    runs = {prec: gpu_session(dict(amp=d["intens"], kw=d["kw"]), probe=d["probe"], obj=d["obj"], calculateRMS=1,
+                              PPS=2, precision=prec) for prec in (0, 1)}
+    o = oracle.OracleMls(d["raw"], d["intens"], d["probe"], obj=d["obj"], variable=1, PPS=2)
+    for _ in range(3):
+        for s in runs.values():
+            s.step()
+        o.step()
+    ob, pr, _ = o.state()
+    e32, etc = rel_err(runs[0].object(), ob), rel_err(runs[1].object(), ob)
+    p32, ptc = rel_err(runs[0].probe(), pr), rel_err(runs[1].probe(), pr)
+    print(f"MLs default path 256^2, 3 iterations vs FP64: object FP32 {e32:.2e}, TC {etc:.2e}; probe {p32:.2e}, {ptc:.2e}")
+    assert e32 < TOL and p32 < TOL
+    assert etc < 2e-3 and ptc < 2e-3
+    for s in runs.values():
+        s.close()
+
+
 @pytest.mark.parametrize("K", [2, 3])
 def test_mls_probe_modes_match_oracle(oracle, K):
     """probeModes > 1: modes 1..K-1 from phase tilts of mode 0 recombined by the eigenvectors of their Gram matrix,
