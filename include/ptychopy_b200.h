@@ -258,6 +258,11 @@ int pty_get_object(pty_session* s, float* c64_out, int X, int Y);
 /* Copy the probe stack (K x N x N complex64).  Replaces epieresprobe / mlsresprobe (src/ptychopy.c:978-990). */
 int pty_get_probe(pty_session* s, float* c64_out, int K, int N);
 
+/* Device memory freed by destroyed sessions stays cached for the next session of this process (unmapping the
+ * buffers of a large DM session took up to 160 ms).  This returns the cache of `device` (-1: every device) to the
+ * driver.  No reference counterpart (the reference frees with cudaFree). */
+int pty_release_cached_memory(int device);
+
 /* Scan positions in pixels after the -min shift, P x 2 float32 (IPtychoScanMesh::getScanPositions).  MLs keeps
  * the ML mesh's centred positions; on its default path these are the current, refined positions (m_positions). */
 int pty_get_positions(const pty_session* s, float* xy_px, int P);

@@ -35,6 +35,7 @@ EXPORTS = [
     "pty_warm_object", "pty_dm_psi_from_object", "pty_tc_weights_size", "pty_tc_pack_weights", "pty_tc_conv3x3",
     "pty_tc_pool2", "pty_tc_up2", "pty_tc_to_bf16", "pty_tc_first_layer", "pty_tc_last_layer", "pty_set_warm_start",
     "pty_selftest_bounded_waits", "pty_fft2_tc", "pty_autotune", "pty_get_mls_state",
+    "pty_release_cached_memory",
 ]
 
 
@@ -87,6 +88,7 @@ def lib():
             "pty_get_probe": ([vp, vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "pty_get_positions": ([vp, vp, ctypes.c_int], ctypes.c_int),
             "pty_get_mls_state": ([vp, vp, vp, vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+            "pty_release_cached_memory": ([ctypes.c_int], ctypes.c_int),
             "pty_write_results": ([vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "pty_set_stream": ([vp, vp], ctypes.c_int),
             "pty_kernel_launches": ([vp], ctypes.c_int64),

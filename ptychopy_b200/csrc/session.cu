@@ -10,6 +10,7 @@
 #include <functional>
 #include <limits>
 #include <map>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -35,16 +36,92 @@ void check_cuda(cudaError_t e, const char* what) {
   fail(code, std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
 }
 
+void need_device_index(int d) {
+  if (d < 0 || d >= 64) fail(PTY_ERR_UNSUPPORTED, "device ordinal " + std::to_string(d) + " above the buffer cache's 64");
+}
+
+// Freed device blocks are kept per device and handed to the next request of at least their size and at most a
+// quarter more: cudaFree of a DM session's buffers (about 3 GB at 512^2 x 900 patterns) unmaps the memory and took
+// 10-160 ms, up to a third of a 100-iteration dmnp call, and the next session mapped it again.  A block enters the
+// cache after a device synchronisation (the ordering cudaFree gives).  pty_release_cached_memory returns the cache
+// to the driver; so does an allocation that fails, before its one retry.
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_cache_mu;
+std::multimap<size_t, void*> g_cache[kMaxDevices];
+
+void* cache_take(int dev, size_t n, size_t* cap) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  auto& c = g_cache[dev];
+  auto it = c.lower_bound(n);
+  if (it == c.end() || it->first > n + n / 4) return nullptr;
+  void* q = it->second;
+  *cap = it->first;
+  c.erase(it);
+  return q;
+}
+
+void cache_release(int dev) {
+  std::multimap<size_t, void*> blocks;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    blocks.swap(g_cache[dev]);
+  }
+  if (blocks.empty()) return;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != dev) cudaSetDevice(dev);
+  for (auto& kv : blocks) cudaFree(kv.second);
+  if (cur != dev) cudaSetDevice(cur);
+}
+}  // namespace
+
 void DeviceBuf::alloc(size_t n, const char* what) {
   free();
   if (n == 0) n = 16;
-  check_cuda(cudaMalloc(&p, n), what);
+  int d = 0;
+  check_cuda(cudaGetDevice(&d), what);
+  need_device_index(d);
+  size_t got = 0;
+  void* q = cache_take(d, n, &got);
+  if (q) {
+    // a fresh cudaMalloc block reads as zeros (the driver clears new pages); a recycled one is cleared to match,
+    // complete before return (the memset runs on the legacy stream, which the sessions' non-blocking streams do not
+    // order against)
+    check_cuda(cudaMemset(q, 0, n), what);
+    check_cuda(cudaDeviceSynchronize(), what);
+  } else {
+    cudaError_t e = cudaMalloc(&q, n);
+    if (e == cudaErrorMemoryAllocation) {  // give the cache back and try once more
+      cudaGetLastError();
+      cache_release(d);
+      e = cudaMalloc(&q, n);
+    }
+    check_cuda(e, what);
+    got = n;
+  }
+  p = q;
   bytes = n;
+  cap = got;
+  dev = d;
 }
 void DeviceBuf::free() {
-  if (p) cudaFree(p);
+  if (p && dev < 0) {  // not from alloc: owned plainly
+    cudaFree(p);
+  } else if (p) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
+    cudaDeviceSynchronize();
+    {
+      std::lock_guard<std::mutex> lk(g_cache_mu);
+      g_cache[dev].emplace(cap, p);
+    }
+    if (cur != dev) cudaSetDevice(cur);
+  }
   p = nullptr;
   bytes = 0;
+  cap = 0;
 }
 
 // ---- geometry (FP32 like the reference's device code) -------------------------------------------------
@@ -1348,6 +1425,14 @@ int pty_session_destroy(pty_session* s) {
   return guarded([&] { destroy_session(s); });
 }
 
+int pty_release_cached_memory(int device) {
+  return guarded([&] {
+    need(device >= -1 && device < 64, "device must be -1 (all) or an ordinal below 64");
+    for (int d = 0; d < 64; ++d)
+      if (device == -1 || device == d) cache_release(d);
+  });
+}
+
 int pty_set_patterns(pty_session* s, const void* host, int dtype, int P, int N) {
   return guarded([&] {
     need(s && host, "null argument");
@@ -1420,8 +1505,9 @@ int pty_init(pty_session* s) {
     }
     float2* twp = nullptr;
     check_cuda(make_twiddles(s->N, &twp, s->stream), "twiddles");
-    s->tw.p = twp;
-    s->tw.bytes = sizeof(float2) * s->N;
+    s->tw.p = twp;  // allocated by make_twiddles; the cache takes it back like any block
+    s->tw.bytes = s->tw.cap = sizeof(float2) * s->N;
+    s->tw.dev = s->dev;
     need(s->algo == ALGO_MLS || p.precision == 0,
          "precision=1 applies to MLs: DM and ePIE fuse their FP32 transforms into their kernels", PTY_ERR_UNSUPPORTED);
     if (s->algo == ALGO_MLS) {

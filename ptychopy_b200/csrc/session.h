@@ -40,9 +40,12 @@ std::vector<double> read_position_file(const std::string& path, int P);
 uint64_t splitmix64(uint64_t& state);
 void visiting_order(uint64_t& state, int P, std::vector<int>& order);
 
+// Device buffer.  Its memory comes from and returns to a per-device cache of freed blocks (session.cu).
 struct DeviceBuf {
   void* p = nullptr;
-  size_t bytes = 0;
+  size_t bytes = 0;      // requested size
+  size_t cap = 0;        // size of the underlying block
+  int dev = -1;
   void alloc(size_t n, const char* what);
   void free();
   template <typename T> T* as() const { return static_cast<T*>(p); }
