@@ -50,6 +50,10 @@ struct MlsBuffers {
   double* vs;             // scratch sums (mls_var_scratch_doubles(Gmax))
   float* pmax;            // max of p_object in this iteration
   float cvx, cvy;         // ceil(X/2 - N/2), ceil(Y/2 - N/2)
+  float2* vupd;           // N x N extra-mode update
+  float2* work2;          // 2 Gmax x N x N FFT work of the position search
+  cudaStream_t side;      // the position search runs on this stream beside the rest of its group
+  cudaEvent_t ev_fork, ev_join;
   int K;                  // probe modes (probe holds K x N x N)
   float2* psik;           // (K-1) x Gmax x N x N exit waves of modes 1..K-1
   float2* mtmp;           // K x N x N scratch of the mode orthogonalisation

@@ -41,9 +41,8 @@ struct VsLayout {
   int G;
   __host__ __device__ size_t pos() const { return 0; }             // 4 G: position-search sums
   __host__ __device__ size_t proj() const { return 4 * size_t(G); }  // G: residual projections
-  __host__ __device__ size_t prj() const { return 5 * size_t(G); }   // G: per-position weights of the update
-  __host__ __device__ size_t evs() const { return 6 * size_t(G); }   // 4 G: weight-update sums
-  __host__ __device__ size_t sc() const { return 10 * size_t(G); }   // 8 scalars
+  __host__ __device__ size_t evs() const { return 5 * size_t(G); }   // 4 G: weight-update sums
+  __host__ __device__ size_t sc() const { return 9 * size_t(G); }    // 8 scalars
 };
 enum { SC_ESUM = 0, SC_USUM = 1, SC_ENEW = 2, SC_EFAC = 3, SC_PFAC = 4 };
 
@@ -309,35 +308,30 @@ __global__ void k_var_proj(const float2* __restrict__ pu, const float2* __restri
   if (threadIdx.x == 0) atomicAdd(&proj[k], acc);
 }
 
-// prj_k = (mean_pixels Re(E conj(resid_k)) + evo1_k) / sum_group evo1^2 (one thread); clears proj
-__global__ void k_var_prj(double* __restrict__ proj, double* __restrict__ prj, const double* __restrict__ evo, int P,
-                          const int* __restrict__ members, const int* __restrict__ gsize, int NN) {
-  pdl_enter();
-  if (threadIdx.x != 0) return;
-  const int G = *gsize;
-  double evn = 0;
-  for (int k = 0; k < G; ++k) evn += evo[P + members[k]] * evo[P + members[k]];
-  for (int k = 0; k < G; ++k) {
-    prj[k] = (proj[k] / NN + evo[P + members[k]]) / evn;
-    proj[k] = 0.0;
-  }
-}
-
-// upd = sum_k resid_k prj_k / N^2; usum += sum |upd|^2
+// upd = sum_k resid_k prj_k / N^2 with prj_k = (mean_pixels Re(E conj(resid_k)) + evo1_k) / sum_group evo1^2 (each
+// block computes the group's prj into shared memory); usum += sum |upd|^2
 __global__ void k_var_upd(const float2* __restrict__ pu, const float2* __restrict__ pum,
                           const float* __restrict__ pobj, const float* __restrict__ pmax,
-                          const double* __restrict__ prj, const int2* __restrict__ win, const int* __restrict__ members,
+                          const double* __restrict__ proj, const double* __restrict__ evo, int P,
+                          const int2* __restrict__ win, const int* __restrict__ members,
                           const int* __restrict__ gsize, int N, int Y, float2* __restrict__ upd,
                           double* __restrict__ usum) {
   pdl_enter();
+  extern __shared__ float s_prj[];
   const int G = *gsize;
+  if (threadIdx.x == 0) {
+    double evn = 0;
+    for (int k = 0; k < G; ++k) evn += evo[P + members[k]] * evo[P + members[k]];
+    for (int k = 0; k < G; ++k) s_prj[k] = float((proj[k] / (double(N) * N) + evo[P + members[k]]) / evn);
+  }
+  __syncthreads();
   const float ip = 1.f / *pmax, invG = 1.f / float(G), nrm = 1.f / float(N * N);
   double acc = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
     float2 u = make_float2(0.f, 0.f);
     for (int k = 0; k < G; ++k) {
       const float2 r = var_resid(pu, pum, pobj, ip, win[members[k]], k, i, N, Y, invG);
-      u = cadd(u, cscale(r, float(prj[k])));
+      u = cadd(u, cscale(r, s_prj[k]));
     }
     u = cscale(u, nrm);
     upd[i] = u;
@@ -347,40 +341,42 @@ __global__ void k_var_upd(const float2* __restrict__ pu, const float2* __restric
   if (threadIdx.x == 0) atomicAdd(usum, acc);
 }
 
-// E += upd relax_U / max(1, rms(upd)); enew += sum |E|^2
-__global__ void k_var_eapply(float2* __restrict__ E, const float2* __restrict__ upd, int NN, const int* __restrict__ gsize,
-                             int P, const double* __restrict__ usum, double* __restrict__ enew) {
+// u <- E + u relax_U / max(1, rms(u)) (the new extra mode before its normalisation, kept in the update buffer);
+// enew += sum |E_new|^2; clears the residual projections
+__global__ void k_var_eapply(const float2* __restrict__ E, float2* __restrict__ upd, int NN,
+                             const int* __restrict__ gsize, int P, const double* __restrict__ usum,
+                             double* __restrict__ enew, double* __restrict__ proj) {
   pdl_enter();
   const double rms = sqrt(*usum / NN);
   const float us = float((double(*gsize) / P) / (rms > 1.0 ? rms : 1.0));
+  if (blockIdx.x == 0 && threadIdx.x < *gsize) proj[threadIdx.x] = 0.0;
   double acc = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += gridDim.x * blockDim.x) {
     const float2 e = cadd(E[i], cscale(upd[i], us));
-    E[i] = e;
+    upd[i] = e;
     acc += double(e.x) * e.x + double(e.y) * e.y;
   }
   acc = block_reduce_sum(acc);
   if (threadIdx.x == 0) atomicAdd(enew, acc);
 }
 
-__global__ void k_var_enorm(float2* __restrict__ E, int NN, const double* __restrict__ enew) {
-  pdl_enter();
-  const float f = float(1.0 / sqrt(*enew / NN));
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += gridDim.x * blockDim.x) E[i] = cscale(E[i], f);
-}
-
-// Per window: sum |objp E|^2, Re(chi conj(objp E)), |objp P|^2, Re(chi conj(objp P))
-__global__ void k_var_evosums(const float2* __restrict__ objp, const float2* __restrict__ E,
+// E = E_new / rms(E_new) (stored by window 0's blocks); per window: sum |objp E|^2, Re(chi conj(objp E)),
+// |objp P|^2, Re(chi conj(objp P))
+__global__ void k_var_evosums(const float2* __restrict__ objp, const float2* __restrict__ Enew,
+                              float2* __restrict__ E, const double* __restrict__ enew,
                               const float2* __restrict__ probe, const float2* __restrict__ chi,
                               const int* __restrict__ gsize, int N, double* __restrict__ out) {
   pdl_enter();
   const int k = blockIdx.y;
   if (k >= *gsize) return;
   const size_t NN = size_t(N) * N;
+  const float f = float(1.0 / sqrt(*enew / double(NN)));
   double v[4] = {0, 0, 0, 0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    const float2 e = cscale(Enew[i], f);
+    if (k == 0) E[i] = e;
     const float2 o = objp[k * NN + i], c = chi[k * NN + i];
-    const float2 a = cmul(o, E[i]), b = cmul(o, probe[i]);
+    const float2 a = cmul(o, e), b = cmul(o, probe[i]);
     v[0] += double(a.x) * a.x + double(a.y) * a.y;
     v[1] += double(c.x) * a.x + double(c.y) * a.y;
     v[2] += double(b.x) * b.x + double(b.y) * b.y;
@@ -839,7 +835,7 @@ int grid_n(size_t n, int cap = 1184) {
 
 }  // namespace
 
-size_t mls_var_scratch_doubles(int Gmax) { return 10 * size_t(Gmax) + 8; }
+size_t mls_var_scratch_doubles(int Gmax) { return 9 * size_t(Gmax) + 8; }
 
 cudaError_t fft2_pdl(float2* data, float2* work, const float2* tw, int batch, int N, bool inverse, cudaStream_t st) {
   return fft2_pdl_impl(data, work, tw, batch, N, inverse, st);
@@ -900,7 +896,7 @@ int mls_var_launches_per_iteration(int ngroups, unsigned flags, int K, bool tc) 
   // pum, lsq, solve and the two updates
   int per = 12 + 5 + (tc ? 6 + (K == 1 ? 1 : 0) : 0);
   if (flags & MLS_POSSEARCH) per += tc ? 2 + 1 + 2 + 1 + 1 : 2 + 2 + 1;
-  if (flags & MLS_VARUPD) per += 7;
+  if (flags & MLS_VARUPD) per += 5;
   // other modes: exit waves, forward and inverse 2-D transforms, the modal modulus, one update each
   if (K > 1) per += 1 + 2 + 1 + 2 + (K - 1);
   return pre + ngroups * per + (K > 1 ? 1 : 0);
@@ -977,6 +973,21 @@ cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, 
     } else {
       const EpiChi ec{b.objp, b.vp, b.win, mem, gs, b.pu, b.S, b.Y};
       if ((e = fftx2<true>(N, b.work, b.psi, b.tw, b.Gmax, ProLoad{b.psi}, ec, st)) != cudaSuccess) return e;
+      if (flags & MLS_POSSEARCH) {
+        // the position search needs this group's windows, probes and chi only, and writes positions that no kernel
+        // reads before the next iteration: it runs on the side stream while the group goes on, and joins before
+        // the next group rewrites those buffers
+        if ((e = cudaEventRecord(b.ev_fork, st)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(b.side, b.ev_fork, 0)) != cudaSuccess) return e;
+        if ((e = fftx2<false>(N, b.work2, b.aux, b.tw, b.Gmax, ProLoad{b.objp}, EpiGrad{b.aux + GN}, b.side)) !=
+            cudaSuccess)
+          return e;
+        const EpiPosSums ps{b.vp, b.psi, gs, b.vs + L.pos(), b.Gmax, 0.0, 0.0};
+        if ((e = fftx2<true>(N, b.work2, b.aux, b.tw, 2 * b.Gmax, ProLoad{b.aux}, ps, b.side)) != cudaSuccess)
+          return e;
+        launch_pdl(k_var_posupd, 1, 32, 0, b.side, b.vs + L.pos(), mem, gs, b.pos);
+        if ((e = cudaEventRecord(b.ev_join, b.side)) != cudaSuccess) return e;
+      }
       if ((e = fftx2<false>(N, b.work, b.pu, b.tw, b.Gmax, ProLoad{b.pu}, EpiPhase{b.sub, mem, gs, -1.f}, st)) !=
           cudaSuccess)
         return e;
@@ -993,26 +1004,21 @@ cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, 
       if ((e = fft(b.aux, 2 * b.Gmax, true)) != cudaSuccess) return e;
       launch_pdl(k_var_possums, grid, 256, 0, st, b.aux, b.vp, b.psi, gs, b.Gmax, N, b.vs + L.pos());
       launch_pdl(k_var_posupd, 1, 32, 0, st, b.vs + L.pos(), mem, gs, b.pos);
-    } else if (flags & MLS_POSSEARCH) {
-      if ((e = fftx2<false>(N, b.work, b.aux, b.tw, b.Gmax, ProLoad{b.objp}, EpiGrad{b.aux + GN}, st)) != cudaSuccess)
-        return e;
-      const EpiPosSums ps{b.vp, b.psi, gs, b.vs + L.pos(), b.Gmax, 0.0, 0.0};
-      if ((e = fftx2<true>(N, b.work, b.aux, b.tw, 2 * b.Gmax, ProLoad{b.aux}, ps, st)) != cudaSuccess) return e;
-      launch_pdl(k_var_posupd, 1, 32, 0, st, b.vs + L.pos(), mem, gs, b.pos);
     }
     if (flags & MLS_VARUPD) {
       launch_pdl(k_var_proj, grid, 256, 0, st, b.pu, b.pum, b.pobj, b.pmax, b.E, b.win, mem, gs, N, b.Y, b.vs + L.proj());
-      launch_pdl(k_var_prj, 1, 32, 0, st, b.vs + L.proj(), b.vs + L.prj(), b.evo, P, mem, gs, NN);
-      launch_pdl(k_var_upd, grid_n(NN, 256), 256, 0, st, b.pu, b.pum, b.pobj, b.pmax, b.vs + L.prj(), b.win, mem, gs, N, b.Y,
-                                                  b.aux, sc + SC_USUM);
-      launch_pdl(k_var_eapply, grid_n(NN, 256), 256, 0, st, b.E, b.aux, NN, gs, P, sc + SC_USUM, sc + SC_ENEW);
-      launch_pdl(k_var_enorm, grid_n(NN, 256), 256, 0, st, b.E, NN, sc + SC_ENEW);
-      launch_pdl(k_var_evosums, grid, 256, 0, st, b.objp, b.E, b.probe, b.psi, gs, N, b.vs + L.evs());
+      launch_pdl(k_var_upd, grid_n(NN, 256), 256, sizeof(float) * b.Gmax, st, b.pu, b.pum, b.pobj, b.pmax,
+                 b.vs + L.proj(), b.evo, P, b.win, mem, gs, N, b.Y, b.vupd, sc + SC_USUM);
+      launch_pdl(k_var_eapply, grid_n(NN, 256), 256, 0, st, b.E, b.vupd, NN, gs, P, sc + SC_USUM, sc + SC_ENEW,
+                 b.vs + L.proj());
+      launch_pdl(k_var_evosums, grid, 256, 0, st, b.objp, b.vupd, b.E, sc + SC_ENEW, b.probe, b.psi, gs, N,
+                 b.vs + L.evs());
       launch_pdl(k_var_evoupd, 1, 32, 0, st, b.vs + L.evs(), sc, b.evo, P, mem, gs, NN);
     }
     for (int m = 1; m < b.K; ++m)  // modes past the first: their directions with the group's probe step
       launch_pdl(k_var_mode_update, grid_n(NN, 256), 256, 0, st, b.psik + size_t(m - 1) * GN, b.objp, b.pobj, b.maxIllum,
                                                           b.win, mem, gs, N, b.Y, b.betas, b.probe + size_t(m) * NN);
+    if ((flags & MLS_POSSEARCH) && !b.tc && (e = cudaStreamWaitEvent(st, b.ev_join, 0)) != cudaSuccess) return e;
   }
   if (b.K > 1) launch_pdl(k_var_ortho, 1, 1024, 0, st, b.probe, b.mtmp, b.K, NN);
   return cudaGetLastError();

@@ -366,7 +366,9 @@ struct MlsState {
   // the reference-default path: extra mode, evolution weights, positions, sub-pixel shifts, per-position probes and
   // directions, gradient images, scratch sums, max of p_object
   bool variable = false;
-  DeviceBuf E, evo, pos, pos_o, sub, vp, pu, aux, vs, pmax, psik, mtmp;
+  DeviceBuf E, evo, pos, pos_o, sub, vp, pu, aux, vs, pmax, psik, mtmp, vupd, work2;
+  cudaStream_t side = nullptr;  // the position search's stream
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int Gmax = 1, ng = 1;
   size_t table_ints = 0;
   MlsTables tab[2];
@@ -380,6 +382,9 @@ struct MlsState {
       if (t.host) cudaFreeHost(t.host);
     }
     for (auto& kv : var_graphs) cudaGraphExecDestroy(kv.second);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
   }
 };
 
@@ -952,6 +957,11 @@ void init_mls(pty_session* s) {
     ml->aux.alloc(sizeof(float2) * 2 * GN, "gradient images");
     ml->vs.alloc(sizeof(double) * mls_var_scratch_doubles(ml->Gmax), "MLs sums");
     ml->pmax.alloc(sizeof(float), "illumination maximum");
+    ml->vupd.alloc(sizeof(float2) * NN, "extra-mode update");
+    ml->work2.alloc(sizeof(float2) * 2 * GN, "position-search FFT work");
+    check_cuda(cudaStreamCreateWithFlags(&ml->side, cudaStreamNonBlocking), "position-search stream");
+    check_cuda(cudaEventCreateWithFlags(&ml->ev_fork, cudaEventDisableTiming), "event");
+    check_cuda(cudaEventCreateWithFlags(&ml->ev_join, cudaEventDisableTiming), "event");
     if (s->K > 1) {
       ml->psik.alloc(sizeof(float2) * GN * (s->K - 1), "exit waves of the other modes");
       ml->mtmp.alloc(sizeof(float2) * NN * s->K, "mode scratch");
@@ -1023,6 +1033,11 @@ MlsBuffers mls_buffers(pty_session* s, int parity) {
     b.pmax = ml->pmax.as<float>();
     b.cvx = std::ceil(float(s->X) * 1.0f / 2 - float(s->N) * 1.0f / 2);
     b.cvy = std::ceil(float(s->Y) * 1.0f / 2 - float(s->N) * 1.0f / 2);
+    b.vupd = ml->vupd.as<float2>();
+    b.work2 = ml->work2.as<float2>();
+    b.side = ml->side;
+    b.ev_fork = ml->ev_fork;
+    b.ev_join = ml->ev_join;
     b.K = s->K;
     b.psik = ml->psik.as<float2>();
     b.mtmp = ml->mtmp.as<float2>();
