@@ -30,6 +30,12 @@ CASES = {
 }
 
 
+# MLs on the reference's default path: name -> (N, nx, probe modes, PPS, iterations)
+MLS_CASES = {
+    "mls_default_n32": (32, 6, 2, 2, 4),
+}
+
+
 def inputs(N, nx, K, seed=4242):
     rng = np.random.default_rng(seed)
     lambd, z, dx_d, step = 2.48e-10, 1.0, 172e-6, 40e-9
@@ -64,7 +70,28 @@ def make(name):
                         params=np.array(repr(dict(params, algorithm=algo, **sched))))
 
 
+def make_mls(name):
+    """Noise-free intensities of the shifted-probe model (gpu_helpers.mls_dataset), the oracle's default MLs path with
+    probe modes, the position search from iteration PPS and the variable-probe update from iteration 3."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    from gpu_helpers import mls_dataset
+
+    N, nx, K, pps, iters = MLS_CASES[name]
+    d = mls_dataset(pyoracle, N=N, nx=nx, shifted=True, seed=8)
+    o = pyoracle.OracleMls(d["raw"], d["intens"], d["probe"], obj=d["obj"], variable=1, PPS=pps, K=K)
+    errs = [o.step() for _ in range(iters)]
+    ob, pr, _ = o.state()
+    E, e0, e1, pos = o.variable_state()
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), intens=d["intens"], raw=d["raw"],
+                        probe_start=d["probe"].astype(np.complex64), obj_start=d["obj"], object=ob, probe=pr,
+                        extra_mode=E, evo0=e0, evo1=e1, positions=pos, errors=np.array(errs), iterations=iters,
+                        params=np.array(repr(dict(d["kw"], probeModes=K, PPS=pps, calculateRMS=1))))
+
+
 if __name__ == "__main__":
     for n in CASES:
         make(n)
+        print("wrote", n)
+    for n in MLS_CASES:
+        make_mls(n)
         print("wrote", n)

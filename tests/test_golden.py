@@ -13,7 +13,9 @@ import pytest
 from conftest import rel_err
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CASES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(HERE, "golden", "*.npz")))
+ALL = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(HERE, "golden", "*.npz")))
+CASES = [c for c in ALL if not c.startswith("mls_")]
+MLS_CASES = [c for c in ALL if c.startswith("mls_")]
 
 
 def load(name):
@@ -24,6 +26,46 @@ def load(name):
 
 def test_fixtures_present():
     assert {"epie_n32", "dm_n32", "epie_modes_n32", "epie_guess_n64"} <= set(CASES)
+    assert {"mls_default_n32"} <= set(MLS_CASES)
+
+
+def _mls_oracle(oracle, z, params):
+    return oracle.OracleMls(z["raw"], z["intens"], z["probe_start"], obj=z["obj_start"], variable=1,
+                            PPS=params["PPS"], K=params["probeModes"])
+
+
+@pytest.mark.parametrize("name", MLS_CASES)
+def test_oracle_reproduces_mls_fixture(oracle, name):
+    z, params = load(name)
+    o = _mls_oracle(oracle, z, params)
+    errs = [o.step() for _ in range(int(z["iterations"]))]
+    ob, pr, _ = o.state()
+    E, e0, e1, pos = o.variable_state()
+    for got, want in ((ob, z["object"]), (pr, z["probe"]), (E, z["extra_mode"]), (e0, z["evo0"]), (e1, z["evo1"])):
+        assert rel_err(got, want) < 1e-12
+    assert np.array_equal(pos, z["positions"])
+    assert np.allclose(errs, z["errors"], rtol=1e-12, atol=0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", MLS_CASES)
+def test_cuda_matches_mls_fixture(name):
+    """The default MLs path (modes, position search, variable probe) against the stored FP64 results: object and the
+    dominant mode 1e-4, the weaker mode, the extra mode and the refined positions as in test_gpu_mls."""
+    from gpu_helpers import gpu_session
+
+    z, params = load(name)
+    s = gpu_session(dict(amp=z["intens"], kw=params), probe=z["probe_start"], obj=z["obj_start"])
+    errs = [s.step() for _ in range(int(z["iterations"]))]
+    gp = s.probe()
+    assert rel_err(s.object(), z["object"]) < 1e-4
+    assert rel_err(gp[0], z["probe"][0]) < 1e-4
+    assert rel_err(gp[1], z["probe"][1]) < 1e-3
+    E, e0, e1 = s.mls_state()
+    assert rel_err(E, z["extra_mode"]) < 1e-3 and rel_err(e0, z["evo0"]) < 1e-5 and rel_err(e1, z["evo1"]) < 1e-2
+    assert np.abs(s.positions() - z["positions"]).max() < 1e-4
+    assert np.allclose(errs, z["errors"], rtol=1e-3)
+    s.close()
 
 
 @pytest.mark.parametrize("name", CASES)
