@@ -331,16 +331,19 @@ __global__ void __launch_bounds__(R* FftShape<L>::T) k_epie(EpieArgs g) {
           if (g.useAll && g.K > 1) pmax = fmaxf(pmax, modal);
         }
       }
+      // partial maxima double-buffered by position parity: the next position writes the other half, and the one
+      // after it cannot reach this half before every CTA has passed the next position's first barrier, i.e. has
+      // read it here
+      float* pm = g.pm + (s & 1) * 256;
       pmax = block_reduce_maxf(pmax);
-      if (threadIdx.x == 0) g.pm[c] = pmax;
+      if (threadIdx.x == 0) pm[c] = pmax;
       if (!sync_all()) return;
       if (threadIdx.x == 0) {
         float m = 0.f;
-        for (int j = 0; j < C; ++j) m = fmaxf(m, g.pm[j]);
+        for (int j = 0; j < C; ++j) m = fmaxf(m, pm[j]);
         s_probemax = m;
       }
       __syncthreads();
-      if (!sync_all()) return;  // pm is rewritten at the next position
     }
   }
   if (c == 0 && threadIdx.x == 0) {

@@ -744,7 +744,7 @@ void init_epie(pty_session* s) {
   ep->TX = (s->X + 15) / 16;
   ep->TY = (s->Y + 15) / 16;
   ep->TM.alloc(sizeof(float) * ep->TX * ep->TY, "tile maxima");
-  ep->pm.alloc(sizeof(float) * 256, "partial maxima");  // one per CTA
+  ep->pm.alloc(sizeof(float) * 512, "partial maxima");  // one per CTA, two sets (position parity)
   ep->sc.alloc(sizeof(EpieScalars), "scalars");
   ep->ip.alloc(4 * sizeof(double), "inner products");
   s->ocache.alloc(sizeof(float) * XY, "object cache");
