@@ -73,7 +73,8 @@ def parse():
     ap.add_argument("--e2e-iters", type=int, default=100, help="iterations per public-API call (the config's 100)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-autotune", action="store_true", help="--algo batch: keep the default launch variants")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="--algo batch / epie: keep the default launch variants")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the ePIE 512^2 and warm-start parts of the headline after the DM line")
     ap.add_argument("--nx", type=int, default=30, help="raster size (30 = the DM configuration; smaller for profiling)")
@@ -82,6 +83,8 @@ def parse():
     ap.add_argument("--shard", action="store_true",
                     help="N>1: split the 900 positions over the GPUs (one NCCL all-reduce of the DM increments per "
                          "iteration, strong scaling) instead of independent replicas")
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
+                    help="--algo epie: 1 runs the transforms as split-BF16 tensor-core stages (256^2)")
     ap.add_argument("--cfg", default="epie128", choices=["epie128", "epie256k5", "dm512"],
                     help="ePIE configuration (dm512: ePIE on the 512^2 DM configuration's scan)")
     return ap.parse_args()
@@ -455,11 +458,15 @@ def run_epie(args, rank, local, emit=True):
     P = pos.shape[0]
     kwargs = dict(size=N, scanDimsx=cfg["nx"], scanDimsy=cfg["ny"], stepx=cfg["step"], stepy=cfg["step"],
                   lambd=cfg["lambd"], z=cfg["z"], dx_d=cfg["dx_d"], beamSize=synth.BEAM_FWHM, probeModes=K,
-                  algorithm="ePIE", device=local)
+                  algorithm="ePIE", device=local, precision=args.precision)
     stream = torch.cuda.Stream()
     s = abi.Session(**kwargs)
     s.set_stream(stream.cuda_stream)
     s.set_patterns_ptr(amp.data_ptr(), P, N)
+    tuning = None
+    if not args.no_autotune and not args.precision:  # pick the launch variant (pty_autotune), reported
+        t0 = time.perf_counter()
+        tuning = {"choice": s.autotune(iters=1), "seconds": round(time.perf_counter() - t0, 3)}
     s.init()
     warm = max(args.warmup, 21)
     for _ in range(warm):
@@ -485,14 +492,17 @@ def run_epie(args, rank, local, emit=True):
     bytes_pattern = 4 * N * N + 16 * N * N * (1 + K)  # A; object patch r+w; probe modes r+w (probe updating)
     achieved = bytes_pattern * value / 1e9
     out = {"metric": "ePIE patterns/s", "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-           "warmup": warm, "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "f32",
+           "warmup": warm, "ms_per_step": ms / args.steps, "higher_is_better": True,
+           "dtype": "f32 (transforms split-BF16 on tensor cores)" if args.precision else "f32",
            "data": "synthetic (seeded)",
            "config": {"workload": f"ePIE {args.cfg}: {cfg['nx']}x{cfg['ny']} raster ({P} positions), {N}x{N} "
                                   f"detector, {K} probe mode(s), object {X}x{Y}", "N": N, "positions": P, "modes": K},
            "roofline": {"bound": "latency (serial positions)", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "peak_kind": kind, "kernel": "k_epie (one persistent cluster)",
+                        "frac": achieved / peak, "peak_kind": kind, "kernel": ("per-position kernel chain with tensor-core transforms" if args.precision
+                                                           else "the autotuned ePIE launch variant"),
                         "algorithmic_bytes_per_pattern": bytes_pattern},
-           "gpu_launches": int(launches), "clocks": ck, "finite": finite}
+           "gpu_launches": int(launches), "clocks": ck, "finite": finite,
+           "autotune": tuning if tuning else ("tensor-core chain (precision=1)" if args.precision else "off")}
     if not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import pyoracle

@@ -102,6 +102,7 @@ extern "C" int pty_autotune(pty_session* s, int iters, char* report, int report_
     if (epie_uses_smem(N, s->K)) cands.push_back({0, 0, "shared-memory cluster"});
     cands.push_back({0, 1, "cluster"});
     if (N == 256 || N == 512) cands.push_back({0, 2, "whole-GPU"});
+    cands.push_back({0, 3, "kernel chain"});
   }
   std::string rep = s->algo == ALGO_DM ? "DM" : (s->algo == ALGO_EPIE ? "ePIE" : "MLs");
   int best = -1;

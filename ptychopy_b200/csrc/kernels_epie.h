@@ -37,6 +37,30 @@ struct EpieArgs {
   int grid;               // 1: whole-GPU variant (C CTAs, cooperative launch); 0: one cluster of C CTAs
 };
 
+// ePIE as a chain of whole-GPU kernels per position (kernels_epie_chain.cu): the precision = 1 path, whose 2-D
+// transforms run as split-BF16 tensor-core stages (tc = 1, N = 256).  Same update as k_epie.
+struct EpieChainArgs {
+  const float* ampT;      // P x N x N amplitudes, transposed (A(x, y) at [y N + x])
+  float2* obj;
+  float* ocache;
+  float2* probe;
+  float* pcache;
+  const float2* pos;
+  const int* order;
+  float2* psi;            // Ka x N x N exit waves, spectra, updates
+  float2* work;           // Ka x N x N FFT work
+  float* TM;
+  EpieScalars* sc;
+  const double* sqsum;
+  float* pmax2;           // 2: probe maximum after each position (position parity)
+  int* tcerr;             // tensor-core wait-timeout flag
+  const float2* tw;       // twiddles of the FP32 transforms (tc = 0)
+  float saturation;
+  int N, K, Ka, P, X, Y, TX, TY, pc, up, rms, useAll, tc;
+};
+cudaError_t epie_chain_iteration(const EpieChainArgs& g, cudaStream_t st);
+int epie_chain_launches(int P, bool up);
+
 // Sets kernel attributes and picks the cluster size (largest resident of 16, 8, ...); returns it in C_out.
 cudaError_t epie_prepare(int N, int* C_out);
 // Whole-GPU variant (N = 512, and N = 256 when any_size): the CTA count if a cooperative launch of it fits on this

@@ -1,0 +1,219 @@
+// ePIE as a chain of whole-GPU kernels per position (ePIE::iteration, src/ePIE.cpp:65-129): launch variant 3 with FP32
+// transforms (fft2_pdl), and the precision = 1 path, whose 2-D transforms run as split-BF16 tensor-core stages
+// (fft2_tc, N = 256).  The pointwise steps follow the fused kernel k_epie phase by phase (kernels_epie.cu), so the
+// paths compute the same update; the chain spreads every step over the whole GPU, where the fused kernel runs one
+// thread-block cluster (it wins with several probe modes).  Per position s of the visiting order:
+//   exit      psi_k = bilinear patch (Q2) x P_k, k < Ka                       (get projections, a3/a4)
+//   FFT2      Psi_k
+//   modulus   d_k = (Psi'_k - Psi_k)/N^2 with the modal modulus and the error metric (a5, a9); by linearity the
+//             inverse transform of d_k is psi_new - psi_old
+//   IFFT2     dpsi_k
+//   object    O += (1/max |P|^2) sum_k conj(P_k) dpsi_k at the rounded position, phase constraint, |O|^2 cache (a6)
+//   tiles     16 x 16 tile maxima of |O|^2 under the patch                    (probe update only)
+//   probe     object max from the tiles; P_k += (1/max |O|^2) conj(O) dpsi_k; |P_k|^2 cache and the probe maximum
+//             for the next position (a7)
+// Every kernel is launched with programmatic dependent launch.
+#include "fft_core.cuh"
+#include "kernel_util.cuh"
+#include "kernels.h"
+#include "kernels_epie.h"
+#include "kernels_mls.h"
+#include "pdl.cuh"
+
+namespace pty {
+
+namespace {
+
+int grid_e(size_t n) {
+  size_t g = (n + 255) / 256;
+  return int(g < 1 ? 1 : (g > 1184 ? 1184 : g));
+}
+
+__global__ void k_ec_exit(EpieChainArgs g, int s) {
+  pdl_enter();
+  const int i = g.order[s];
+  const float2 q = g.pos[i];
+  const int N = g.N;
+  const size_t NN = size_t(N) * N;
+  if (g.up && blockIdx.x == 0 && threadIdx.x == 0) g.pmax2[s & 1] = 0.f;  // this position's probe maximum
+  for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
+    const int x = int(idx / N), y = int(idx % N);
+    int r0, r1, c0, c1;
+    float wb, wa;
+    tex_axis(q.x, x, g.X, r0, r1, wb);
+    tex_axis(q.y, y, g.Y, c0, c1, wa);
+    const float2 v00 = g.obj[size_t(r0) * g.Y + c0], v01 = g.obj[size_t(r0) * g.Y + c1];
+    const float2 v10 = g.obj[size_t(r1) * g.Y + c0], v11 = g.obj[size_t(r1) * g.Y + c1];
+    const float w00 = (1.f - wa) * (1.f - wb), w01 = wa * (1.f - wb), w10 = (1.f - wa) * wb, w11 = wa * wb;
+    const float2 patch = make_float2(v00.x * w00 + v01.x * w01 + v10.x * w10 + v11.x * w11,
+                                     v00.y * w00 + v01.y * w01 + v10.y * w10 + v11.y * w11);
+    for (int k = 0; k < g.Ka; ++k) g.psi[k * NN + idx] = cmul(patch, g.probe[k * NN + idx]);
+  }
+}
+
+__global__ void k_ec_modulus(EpieChainArgs g, int s) {
+  pdl_enter();
+  const int i = g.order[s];
+  const int N = g.N;
+  const size_t NN = size_t(N) * N;
+  const float nrm = 1.f / float(NN);
+  const float* Ai = g.ampT + size_t(i) * NN;  // transposed: A(x, y) at [y N + x]
+  double err = 0.0;
+  for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
+    const int x = int(idx / N), y = int(idx % N);
+    const float A = Ai[size_t(y) * N + x];
+    if (g.Ka == 1) {
+      const float2 psi = g.psi[idx];
+      if (g.rms) err += fabsf(A - sqrtf(psi.x * psi.x + psi.y * psi.y));
+      float2 rep;
+      if (A - g.saturation >= 0.f)
+        rep = make_float2(psi.x * nrm, psi.y * nrm);  // floating pixel: no modulus
+      else
+        rep = modulus_replace(psi, A * nrm);
+      g.psi[idx] = make_float2(rep.x - psi.x * nrm, rep.y - psi.y * nrm);
+    } else {
+      float tot = 0.f;
+      float2 sum = make_float2(0.f, 0.f);
+      for (int k = 0; k < g.Ka; ++k) {
+        const float2 psi = g.psi[k * NN + idx];
+        tot += psi.x * psi.x + psi.y * psi.y;
+        sum = cadd(sum, psi);
+      }
+      if (g.rms) err += fabsf(A - sqrtf(sum.x * sum.x + sum.y * sum.y));
+      const float sc = (tot > 0.f) ? ((A - g.saturation >= 0.f) ? 1.f : A) * rsqrtf(tot) * nrm : 0.f;
+      for (int k = 0; k < g.Ka; ++k) {
+        const float2 psi = g.psi[k * NN + idx];
+        g.psi[k * NN + idx] = make_float2(psi.x * (sc - nrm), psi.y * (sc - nrm));
+      }
+    }
+  }
+  if (g.rms) {
+    const double e = block_reduce_sum(err);
+    if (threadIdx.x == 0) atomicAdd(&g.sc->err, e / double(g.Ka) / double(g.sqsum[i]));
+  }
+}
+
+__global__ void k_ec_object(EpieChainArgs g, int s) {
+  pdl_enter();
+  const int i = g.order[s];
+  const float2 q = g.pos[i];
+  const int ox = int(roundf(q.x)), oy = int(roundf(q.y));
+  const int N = g.N;
+  const size_t NN = size_t(N) * N;
+  const float pmax = (g.up && s > 0) ? g.pmax2[(s - 1) & 1] : g.sc->probeMax;
+  const float cO = 1.0f / pmax;
+  for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
+    const int x = int(idx / N), y = int(idx % N);
+    float2 inc = make_float2(0.f, 0.f);
+    for (int k = 0; k < g.Ka; ++k) inc = cadd(inc, cconjmul(g.probe[k * NN + idx], g.psi[k * NN + idx]));
+    const size_t o_i = size_t(x + ox) * g.Y + (y + oy);
+    float2 o = g.obj[o_i];
+    o = make_float2(o.x + inc.x * cO, o.y + inc.y * cO);
+    const float mag = sqrtf(o.x * o.x + o.y * o.y);
+    if (g.pc) o = constrain_phase(o);
+    g.obj[o_i] = o;
+    g.ocache[o_i] = mag * mag;
+  }
+}
+
+// 16 x 16 tile maxima of |O|^2 under the patch (one warp per tile)
+__global__ void k_ec_tiles(EpieChainArgs g, int s) {
+  pdl_enter();
+  const int i = g.order[s];
+  const float2 q = g.pos[i];
+  const int ox = int(roundf(q.x)), oy = int(roundf(q.y)), N = g.N;
+  const int tr0 = ox / 16, tr1 = (ox + N - 1) / 16, tc0 = oy / 16, tc1 = (oy + N - 1) / 16;
+  const int ntc = tc1 - tc0 + 1, ntiles = (tr1 - tr0 + 1) * ntc;
+  const int lane = threadIdx.x & 31;
+  for (int tile = int((blockIdx.x * blockDim.x + threadIdx.x) / 32); tile < ntiles;
+       tile += int(gridDim.x * blockDim.x / 32)) {
+    const int tr = tr0 + tile / ntc, tc = tc0 + tile % ntc;
+    float m = 0.f;
+    for (int j = lane; j < 256; j += 32) {
+      const int xr = tr * 16 + j / 16, yc = tc * 16 + j % 16;
+      if (xr < g.X && yc < g.Y) m = fmaxf(m, g.ocache[size_t(xr) * g.Y + yc]);
+    }
+    m = warp_reduce_maxf(m);
+    if (lane == 0) g.TM[size_t(tr) * g.TY + tc] = m;
+  }
+}
+
+__global__ void k_ec_probe(EpieChainArgs g, int s) {
+  pdl_enter();
+  __shared__ float s_om;
+  float m = 0.f;
+  for (int j = threadIdx.x; j < g.TX * g.TY; j += blockDim.x) m = fmaxf(m, g.TM[j]);
+  m = block_reduce_maxf(m);
+  if (threadIdx.x == 0) {
+    s_om = m;
+    if (blockIdx.x == 0) g.sc->objMax = m;
+  }
+  __syncthreads();
+  const float cP = 1.0f / s_om;
+  const int i = g.order[s];
+  const float2 q = g.pos[i];
+  const int ox = int(roundf(q.x)), oy = int(roundf(q.y));
+  const int N = g.N;
+  const size_t NN = size_t(N) * N;
+  float pmax = 0.f;
+  for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
+    const int x = int(idx / N), y = int(idx % N);
+    const float2 oc = g.obj[size_t(x + ox) * g.Y + (y + oy)];
+    float modal = 0.f;
+    for (int k = 0; k < g.K; ++k) {
+      float cache;
+      if (k < g.Ka) {
+        const float2 u = cconjmul(oc, g.psi[k * NN + idx]);
+        float2 pv = g.probe[k * NN + idx];
+        pv = make_float2(u.x * cP + pv.x, u.y * cP + pv.y);
+        const float mg = sqrtf(pv.x * pv.x + pv.y * pv.y);
+        g.probe[k * NN + idx] = pv;
+        cache = mg * mg;
+        g.pcache[k * NN + idx] = cache;
+      } else {
+        cache = g.pcache[k * NN + idx];
+      }
+      if (g.useAll && g.K > 1)
+        modal += cache;
+      else
+        pmax = fmaxf(pmax, cache);
+    }
+    if (g.useAll && g.K > 1) pmax = fmaxf(pmax, modal);
+  }
+  pmax = block_reduce_maxf(pmax);
+  if (threadIdx.x == 0) atomicMax(reinterpret_cast<int*>(&g.pmax2[s & 1]), __float_as_int(pmax));
+}
+
+__global__ void k_ec_finish(EpieChainArgs g) {
+  pdl_enter();
+  if (threadIdx.x == 0 && blockIdx.x == 0 && g.up && g.P > 0) g.sc->probeMax = g.pmax2[(g.P - 1) & 1];
+}
+
+}  // namespace
+
+cudaError_t epie_chain_iteration(const EpieChainArgs& g, cudaStream_t st) {
+  const size_t NN = size_t(g.N) * g.N;
+  const int gb = grid_e(NN);
+  const int tiles = ((g.N + 15) / 16 + 1) * ((g.N + 15) / 16 + 1);
+  cudaError_t e;
+  auto fft = [&](bool inv) {
+    return g.tc ? fft2_tc(g.psi, g.work, g.Ka, g.N, inv, g.tcerr, st)
+                : fft2_pdl(g.psi, g.work, g.tw, g.Ka, g.N, inv, st);
+  };
+  for (int s = 0; s < g.P; ++s) {
+    if ((e = launch_pdl(k_ec_exit, gb, 256, 0, st, g, s)) != cudaSuccess) return e;
+    if ((e = fft(false)) != cudaSuccess) return e;
+    if ((e = launch_pdl(k_ec_modulus, gb, 256, 0, st, g, s)) != cudaSuccess) return e;
+    if ((e = fft(true)) != cudaSuccess) return e;
+    if ((e = launch_pdl(k_ec_object, gb, 256, 0, st, g, s)) != cudaSuccess) return e;
+    if (g.up) {
+      if ((e = launch_pdl(k_ec_tiles, (tiles * 32 + 255) / 256, 256, 0, st, g, s)) != cudaSuccess) return e;
+      if ((e = launch_pdl(k_ec_probe, gb, 256, 0, st, g, s)) != cudaSuccess) return e;
+    }
+  }
+  return launch_pdl(k_ec_finish, 1, 32, 0, st, g);
+}
+
+int epie_chain_launches(int P, bool up) { return P * (up ? 9 : 7) + 1; }
+
+}  // namespace pty

@@ -339,6 +339,9 @@ void visiting_order(uint64_t& state, int P, std::vector<int>& order) {
 // Device state of the persistent ePIE kernel.
 struct EpieState {
   DeviceBuf pos, order, W1, W2, TM, pm, sc, sq, modesCopy, ip, gsync;
+  bool chain = false;     // the per-position kernel chain (variant 3, or precision = 1)
+  bool chain_tc = false;  // its transforms on the tensor cores (precision = 1)
+  DeviceBuf cpsi, cwork, pmax2, tcerr;
   int C = 1, TX = 0, TY = 0;
   bool tm_valid = false;
   bool sm = false;    // shared-memory-resident kernel (small windows, one mode)
@@ -719,8 +722,21 @@ void init_epie(pty_session* s) {
   s->ep = ep;
   const size_t NN = size_t(s->N) * s->N, XY = size_t(s->X) * s->Y;
   const int var = s->epie_variant;
-  ep->sm = epie_uses_smem(s->N, s->K) && (var < 0 || var == 0);
-  if (ep->sm) {
+  ep->chain_tc = s->prm.precision != 0;
+  // the chain spreads each step over the whole GPU; with several probe modes at 256^2 and up it measured 2.5x the
+  // fused cluster kernel (5 modes at 256^2: 93 vs 237 ms per iteration), so it is the automatic choice there
+  ep->chain = ep->chain_tc || var == 3 || (var < 0 && s->K > 1 && s->N >= 256);
+  ep->sm = !ep->chain && epie_uses_smem(s->N, s->K) && (var < 0 || var == 0);
+  if (ep->chain) {
+    if (ep->chain_tc) {
+      need(s->N == 256, "precision=1 (tensor-core FFT stages) needs 256 x 256 patterns", PTY_ERR_UNSUPPORTED);
+      check_cuda(fft2_tc_prepare(), "tensor-core FFT set-up");
+    }
+    ep->cpsi.alloc(sizeof(float2) * NN * s->K, "exit waves");
+    ep->cwork.alloc(sizeof(float2) * NN * s->K, "FFT work");
+    ep->pmax2.alloc(2 * sizeof(float), "probe maxima");
+    ep->tcerr.alloc(sizeof(int), "tensor-core flag");
+  } else if (ep->sm) {
     check_cuda(epie_sm_prepare(s->N), "ePIE kernel set-up");
   } else {
     const int Cg = (var < 0 || var == 2) ? epie_grid_prepare(s->N, var == 2) : 0;
@@ -1312,8 +1328,49 @@ double step_epie(pty_session* s, int it, bool want_err) {
   g.grid = ep->grid ? 1 : 0;
   g.gbar = ep->gsync.as<unsigned>();
   g.gerr = reinterpret_cast<int*>(ep->gsync.as<unsigned>() + 2);
-  check_cuda(ep->sm ? epie_sm_launch(g, s->stream) : epie_launch(g, s->stream), "ePIE kernel launch");
-  s->launches += 1;
+  if (ep->chain) {
+    EpieChainArgs cg;
+    cg.ampT = g.ampT;
+    cg.obj = g.obj;
+    cg.ocache = g.ocache;
+    cg.probe = g.probe;
+    cg.pcache = g.pcache;
+    cg.pos = g.pos;
+    cg.order = g.order;
+    cg.psi = ep->cpsi.as<float2>();
+    cg.work = ep->cwork.as<float2>();
+    cg.TM = g.TM;
+    cg.sc = g.sc;
+    cg.sqsum = g.sqsum;
+    cg.pmax2 = ep->pmax2.as<float>();
+    cg.tcerr = ep->tcerr.as<int>();
+    cg.tw = g.tw;
+    cg.saturation = g.saturation;
+    cg.N = g.N;
+    cg.K = g.K;
+    cg.Ka = g.Ka;
+    cg.P = g.P;
+    cg.X = g.X;
+    cg.Y = g.Y;
+    cg.TX = g.TX;
+    cg.TY = g.TY;
+    cg.pc = g.pc;
+    cg.up = g.up;
+    cg.rms = g.rms;
+    cg.useAll = g.useAll;
+    cg.tc = ep->chain_tc ? 1 : 0;
+    check_cuda(epie_chain_iteration(cg, s->stream), "ePIE chain");
+    s->launches += epie_chain_launches(s->P, up);
+    if (ep->chain_tc) {  // the tensor-core transforms report a wait timeout through their device flag
+      int flag = 0;
+      check_cuda(cudaMemcpyAsync(&flag, cg.tcerr, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H flag");
+      check_cuda(cudaStreamSynchronize(s->stream), "ePIE iteration");
+      need(flag == 0, "ePIE: a tensor-core FFT wait timed out", PTY_ERR_CUDA);
+    }
+  } else {
+    check_cuda(ep->sm ? epie_sm_launch(g, s->stream) : epie_launch(g, s->stream), "ePIE kernel launch");
+    s->launches += 1;
+  }
   if (ep->grid) {  // the whole-GPU variant reports a grid-barrier timeout through a device flag
     int flag = 0;
     check_cuda(cudaMemcpyAsync(&flag, g.gerr, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H flag");
@@ -1523,8 +1580,8 @@ int pty_init(pty_session* s) {
     s->tw.p = twp;  // allocated by make_twiddles; the cache takes it back like any block
     s->tw.bytes = s->tw.cap = sizeof(float2) * s->N;
     s->tw.dev = s->dev;
-    need(s->algo == ALGO_MLS || p.precision == 0,
-         "precision=1 applies to MLs: DM and ePIE fuse their FP32 transforms into their kernels", PTY_ERR_UNSUPPORTED);
+    need(s->algo != ALGO_DM || p.precision == 0,
+         "precision=1 applies to MLs and ePIE: DM fuses its FP32 transforms into its kernels", PTY_ERR_UNSUPPORTED);
     if (s->algo == ALGO_MLS) {
       need(s->warm_params.empty(), "the learned warm start is for ePIE and DM sessions", PTY_ERR_UNSUPPORTED);
       init_mls(s);

@@ -109,3 +109,30 @@ def test_scan_meshes_match_oracle(oracle, tmp_path):
     assert np.array_equal(s.positions(), pos) and (s.dims()["X"], s.dims()["Y"]) == (X, Y)
     s.step()
     assert np.isfinite(s.object()).all()
+
+
+@pytest.mark.parametrize("K", [1, 3])
+def test_epie_tensor_core_fft_chain(oracle, K):
+    """precision=1: ePIE as a per-position kernel chain whose transforms run as split-BF16 tensor-core stages
+    (256^2); FP32 fused kernel and the chain both against the FP64 oracle, error stated, with the probe updating
+    from iteration 2 and (K = 3) the modes from iteration 3."""
+    d = dataset(N=256, nx=3, K=K)
+    kw = dict(updateProbe=2, updateModes=3, calculateRMS=1, seed=21)
+    runs = {prec: gpu_session(d, probe=d["probe"], precision=prec, **kw) for prec in (0, 1)}
+    o = oracle.OracleSession("ePIE", d["amp"], d["pos"], np.zeros((d["X"], d["Y"])), d["probe"],
+                             probe_guess_path=False, modes_given=K > 1, **kw)
+    errs = {0: [], 1: []}
+    for _ in range(4):
+        for prec, s in runs.items():
+            errs[prec].append(s.step())
+        eo = o.step()
+    ob, pr, _ = o.state()
+    e32, etc = rel_err(runs[0].object(), ob), rel_err(runs[1].object(), ob)
+    p32, ptc = rel_err(runs[0].probe(), pr), rel_err(runs[1].probe(), pr)
+    print(f"ePIE 256^2 K={K}, 4 iterations vs FP64: object FP32 {e32:.2e}, TC chain {etc:.2e}; "
+          f"probe {p32:.2e}, {ptc:.2e}; error metric {errs[0][-1]:.6e} / {errs[1][-1]:.6e} / {eo:.6e}")
+    assert e32 < TOL and p32 < TOL
+    assert etc < 2e-3 and ptc < 2e-3
+    assert abs(errs[1][-1] - eo) <= 2e-3 * abs(eo)
+    for s in runs.values():
+        s.close()

@@ -214,7 +214,9 @@ def test_mls_tensor_core_fft_precision(oracle):
     assert etc < 2e-3 and ptc < 2e-3
     for s in runs.values():
         s.close()
-    # DM and ePIE fuse their FP32 transforms: precision=1 is refused
+    # DM fuses its FP32 transforms: precision=1 is refused; ePIE takes it at 256^2 only
     dd = dataset(N=64, nx=3)
     with pytest.raises(abi.PtyError):
         gpu_session(dict(dd, kw=dict(dd["kw"], algorithm="DM")), probe=dd["probe"], precision=1)
+    with pytest.raises(abi.PtyError):
+        gpu_session(dict(dd, kw=dict(dd["kw"], algorithm="ePIE")), probe=dd["probe"], precision=1)
