@@ -32,6 +32,10 @@ struct Candidate {
 double time_candidate(const pty_session* s, const Candidate& c, int iters) {
   pty_params p = s->prm;
   p.wave = c.wave;
+  // time the steady state: the probe (and, with several modes, the modes) update from the first iteration, as they
+  // do for most of a run (from updateProbe = 10 and updateModes = 20 of 100 by default)
+  p.updateProbe = std::min(p.updateProbe, 1);
+  p.updateModes = std::min(p.updateModes, 1);
   pty_session* t = nullptr;
   if (pty_session_create(&p, &t) != PTY_OK) return -1.0;
   double ms = -1.0;

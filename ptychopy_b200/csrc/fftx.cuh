@@ -1,0 +1,90 @@
+// Row-transform passes of the batched 2-D FFT with fused loads and stores, launched with programmatic dependent
+// launch.  Header-only templates, shared by the MLs default path (kernels_mls_var.cu) and the ePIE kernel chain
+// (kernels_epie_chain.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fft_core.cuh"
+#include "kernel_util.cuh"
+#include "pdl.cuh"
+
+namespace pty {
+
+// ---- FFT passes with fused loads and stores -------------------------------------------------------------------
+// One row-transform pass of the batched 2-D FFT (the k_fft_rows_t scheme: R rows per CTA, transposed store) with a
+// prologue that produces each loaded element (plane b, row x, column y) and an epilogue that maps each stored element
+// (plane b, row x, column y of the natural layout after the second pass) and may accumulate per-plane sums, finished
+// once per CTA.  The first pass of a 2-D transform takes a prologue and stores plainly into the transposed work
+// plane; the second loads plainly and takes an epilogue.
+struct ProLoad {
+  const float2* in;
+  __device__ float2 operator()(int b, int x, int y, int L) const { return in[(size_t(b) * L + x) * L + y]; }
+};
+struct EpiStore {
+  __device__ float2 operator()(int, int, int, int, float2 v) { return v; }
+  __device__ void finish(int) {}
+};
+
+template <int L, bool INV, class Pro, class Epi>
+__global__ void __launch_bounds__(FftShape<L>::THREADS) k_fftx_pass(float2* __restrict__ out,
+                                                                    const float2* __restrict__ g_tw, Pro pro, Epi epi) {
+  pdl_enter();
+  using S = FftShape<L>;
+  constexpr int T = S::T, E = S::E, R = S::RC;
+  extern __shared__ float4 smem4[];
+  float2* smem = reinterpret_cast<float2*>(smem4);
+  float2* s_tw = smem;
+  float2* s_x = smem + L;
+  const int v = threadIdx.x / T, t = threadIdx.x % T, b = blockIdx.y;
+  const int x0 = blockIdx.x * R;
+  load_twiddles<L>(s_tw, g_tw);
+  __syncthreads();
+  float2 a[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) a[e] = pro(b, x0 + v, t + T * e, L);
+  fft_vec<L, INV>(a, t, s_x + v * S::XCH, s_tw);
+  __syncthreads();  // the staging tile aliases the exchange buffers of other warps
+  static_for<0, E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    s_x[(t + T * e) * (R + 1) + v] = a[out_slot<L>(e)];
+  });
+  __syncthreads();
+  float2* o = out + size_t(b) * L * L;
+  for (int i = threadIdx.x; i < L * R; i += blockDim.x) {
+    const int vv = i % R, n = i / R;
+    o[size_t(n) * L + x0 + vv] = epi(b, n, x0 + vv, L, s_x[n * (R + 1) + vv]);
+  }
+  epi.finish(b);
+}
+
+template <int L, bool INV, class Pro, class Epi>
+inline cudaError_t launch_fftx(float2* out, const float2* tw, int batch, Pro pro, Epi epi, cudaStream_t st) {
+  constexpr int R = FftShape<L>::RC, NT = FftShape<L>::THREADS;
+  const size_t smem = rows_smem_bytes<L>();
+  cudaError_t e = cudaFuncSetAttribute(k_fftx_pass<L, INV, Pro, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem));
+  if (e != cudaSuccess) return e;
+  return launch_pdl(k_fftx_pass<L, INV, Pro, Epi>, dim3(L / R, batch), NT, smem, st, out, tw, pro, epi);
+}
+
+// 2-D transform data-in (through pro) -> work (transposed) -> out (through epi)
+template <bool INV, class Pro, class Epi>
+inline cudaError_t fftx2(int N, float2* work, float2* out, const float2* tw, int batch, Pro pro, Epi epi, cudaStream_t st) {
+  cudaError_t e;
+#define PTY_FFTX(L)                                                                            \
+  case L:                                                                                      \
+    if ((e = launch_fftx<L, INV>(work, tw, batch, pro, EpiStore{}, st)) != cudaSuccess) return e; \
+    return launch_fftx<L, INV>(out, tw, batch, ProLoad{work}, epi, st);
+  switch (N) {
+    PTY_FFTX(32)
+    PTY_FFTX(64)
+    PTY_FFTX(128)
+    PTY_FFTX(256)
+    PTY_FFTX(512)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef PTY_FFTX
+}
+
+}  // namespace pty
