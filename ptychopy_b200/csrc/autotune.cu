@@ -36,6 +36,7 @@ double time_candidate(const pty_session* s, const Candidate& c, int iters) {
   // do for most of a run (from updateProbe = 10 and updateModes = 20 of 100 by default)
   p.updateProbe = std::min(p.updateProbe, 1);
   p.updateModes = std::min(p.updateModes, 1);
+  p.phaseConstraint = 0;  // one schedule regime throughout: graphs captured in the warm-up replay in the timed part
   pty_session* t = nullptr;
   if (pty_session_create(&p, &t) != PTY_OK) return -1.0;
   double ms = -1.0;

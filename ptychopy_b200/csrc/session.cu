@@ -342,6 +342,9 @@ struct EpieState {
   bool chain = false;     // the per-position kernel chain (variant 3, or precision = 1)
   bool chain_tc = false;  // its transforms on the tensor cores (precision = 1)
   DeviceBuf cpsi, cwork, pmax2, tcerr;
+  // the chain's iteration as a CUDA graph per schedule regime (active modes, probe update, phase constraint,
+  // error metric); the visiting order is read from device memory at each replay
+  std::map<unsigned, cudaGraphExec_t> chain_graphs;
   int C = 1, TX = 0, TY = 0;
   bool tm_valid = false;
   bool sm = false;    // shared-memory-resident kernel (small windows, one mode)
@@ -349,6 +352,7 @@ struct EpieState {
   int* order_h = nullptr;  // pinned
   ~EpieState() {
     if (order_h) cudaFreeHost(order_h);
+    for (auto& kv : chain_graphs) cudaGraphExecDestroy(kv.second);
   }
 };
 
@@ -1359,7 +1363,21 @@ double step_epie(pty_session* s, int it, bool want_err) {
     cg.rms = g.rms;
     cg.useAll = g.useAll;
     cg.tc = ep->chain_tc ? 1 : 0;
-    check_cuda(epie_chain_iteration(cg, s->stream), "ePIE chain");
+    const unsigned key = unsigned(Ka) | (unsigned(up) << 8) | (unsigned(pc) << 9) | (unsigned(cg.rms) << 10);
+    cudaGraphExec_t& ge = ep->chain_graphs[key];
+    if (!ge) {
+      cudaGraph_t graph = nullptr;
+      check_cuda(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+      const cudaError_t e1 = epie_chain_iteration(cg, s->stream);
+      const cudaError_t e2 = cudaStreamEndCapture(s->stream, &graph);
+      check_cuda(e1, "ePIE chain capture");
+      check_cuda(e2, "end capture");
+      const cudaError_t e3 = cudaGraphInstantiate(&ge, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e3 != cudaSuccess) ep->chain_graphs.erase(key);
+      check_cuda(e3, "graph instantiate");
+    }
+    check_cuda(cudaGraphLaunch(ge, s->stream), "ePIE chain");
     s->launches += epie_chain_launches(s->P, up);
     if (ep->chain_tc) {  // the tensor-core transforms report a wait timeout through their device flag
       int flag = 0;
