@@ -9,9 +9,10 @@
 //             inverse transform of d_k is psi_new - psi_old
 //   IFFT2     dpsi_k
 //   object    O += (1/max |P|^2) sum_k conj(P_k) dpsi_k at the rounded position, phase constraint, |O|^2 cache (a6)
-//   tiles     16 x 16 tile maxima of |O|^2 under the patch                    (probe update only)
+//             with the 16 x 16 tile maxima of |O|^2 under the patch, one block per tile (probe update only)
 //   probe     object max from the tiles; P_k += (1/max |O|^2) conj(O) dpsi_k; |P_k|^2 cache and the probe maximum
-//             for the next position (a7)
+//             (a7): pixel-local, so it runs at the start of the next position's exit kernel, by the threads that
+//             then read those probe pixels (the last position's in a final kernel)
 // Every kernel is launched with programmatic dependent launch.
 #include "fft_core.cuh"
 #include "kernel_util.cuh"
@@ -29,8 +30,56 @@ int grid_e(size_t n) {
   return int(g < 1 ? 1 : (g > 1184 ? 1184 : g));
 }
 
+// Probe update of position sp at the pixels of this thread's grid-stride loop (a7): the object max from TM (all
+// blocks compute it), P_k += (1/max |O|^2) conj(O) dpsi_k, |P_k|^2 cache, and the probe maximum into its slot.
+// The same loop as the exit wave's, so that a thread updates exactly the probe pixels it then reads.
+__device__ void ec_probe_update(const EpieChainArgs& g, int sp) {
+  __shared__ float s_om;
+  float m = 0.f;
+  for (int j = threadIdx.x; j < g.TX * g.TY; j += blockDim.x) m = fmaxf(m, g.TM[j]);
+  m = block_reduce_maxf(m);
+  if (threadIdx.x == 0) {
+    s_om = m;
+    if (blockIdx.x == 0) g.sc->objMax = m;
+  }
+  __syncthreads();
+  const float cP = 1.0f / s_om;
+  const float2 q = g.pos[g.order[sp]];
+  const int ox = int(roundf(q.x)), oy = int(roundf(q.y));
+  const int N = g.N;
+  const size_t NN = size_t(N) * N;
+  float pmax = 0.f;
+  for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
+    const int x = int(idx / N), y = int(idx % N);
+    const float2 oc = g.obj[size_t(x + ox) * g.Y + (y + oy)];
+    float modal = 0.f;
+    for (int k = 0; k < g.K; ++k) {
+      float cache;
+      if (k < g.Ka) {
+        const float2 u = cconjmul(oc, g.psi[k * NN + idx]);
+        float2 pv = g.probe[k * NN + idx];
+        pv = make_float2(u.x * cP + pv.x, u.y * cP + pv.y);
+        const float mg = sqrtf(pv.x * pv.x + pv.y * pv.y);
+        g.probe[k * NN + idx] = pv;
+        cache = mg * mg;
+        g.pcache[k * NN + idx] = cache;
+      } else {
+        cache = g.pcache[k * NN + idx];
+      }
+      if (g.useAll && g.K > 1)
+        modal += cache;
+      else
+        pmax = fmaxf(pmax, cache);
+    }
+    if (g.useAll && g.K > 1) pmax = fmaxf(pmax, modal);
+  }
+  pmax = block_reduce_maxf(pmax);
+  if (threadIdx.x == 0) atomicMax(reinterpret_cast<int*>(&g.pmax2[sp & 1]), __float_as_int(pmax));
+}
+
 __global__ void k_ec_exit(EpieChainArgs g, int s) {
   pdl_enter();
+  if (g.up && s > 0) ec_probe_update(g, s - 1);  // the previous position's probe update, pixel by pixel
   const int i = g.order[s];
   const float2 q = g.pos[i];
   const int N = g.N;
@@ -93,98 +142,53 @@ __global__ void k_ec_modulus(EpieChainArgs g, int s) {
   }
 }
 
-__global__ void k_ec_object(EpieChainArgs g, int s) {
-  pdl_enter();
-  const int i = g.order[s];
-  const float2 q = g.pos[i];
-  const int ox = int(roundf(q.x)), oy = int(roundf(q.y));
-  const int N = g.N;
-  const size_t NN = size_t(N) * N;
-  const float pmax = (g.up && s > 0) ? g.pmax2[(s - 1) & 1] : g.sc->probeMax;
-  const float cO = 1.0f / pmax;
-  for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
-    const int x = int(idx / N), y = int(idx % N);
-    float2 inc = make_float2(0.f, 0.f);
-    for (int k = 0; k < g.Ka; ++k) inc = cadd(inc, cconjmul(g.probe[k * NN + idx], g.psi[k * NN + idx]));
-    const size_t o_i = size_t(x + ox) * g.Y + (y + oy);
-    float2 o = g.obj[o_i];
-    o = make_float2(o.x + inc.x * cO, o.y + inc.y * cO);
-    const float mag = sqrtf(o.x * o.x + o.y * o.y);
-    if (g.pc) o = constrain_phase(o);
-    g.obj[o_i] = o;
-    g.ocache[o_i] = mag * mag;
-  }
-}
-
-// 16 x 16 tile maxima of |O|^2 under the patch (one warp per tile)
-__global__ void k_ec_tiles(EpieChainArgs g, int s) {
+// Object update and tile maxima in one pass: one block per 16 x 16 object tile under the patch; each thread updates
+// its cell when the patch covers it (as k_ec_object), then the block writes the tile's maximum of |O|^2 (cells
+// outside the patch unchanged) into TM
+__global__ void __launch_bounds__(256) k_ec_object_tiles(EpieChainArgs g, int s) {
   pdl_enter();
   const int i = g.order[s];
   const float2 q = g.pos[i];
   const int ox = int(roundf(q.x)), oy = int(roundf(q.y)), N = g.N;
-  const int tr0 = ox / 16, tr1 = (ox + N - 1) / 16, tc0 = oy / 16, tc1 = (oy + N - 1) / 16;
-  const int ntc = tc1 - tc0 + 1, ntiles = (tr1 - tr0 + 1) * ntc;
-  const int lane = threadIdx.x & 31;
-  for (int tile = int((blockIdx.x * blockDim.x + threadIdx.x) / 32); tile < ntiles;
-       tile += int(gridDim.x * blockDim.x / 32)) {
-    const int tr = tr0 + tile / ntc, tc = tc0 + tile % ntc;
-    float m = 0.f;
-    for (int j = lane; j < 256; j += 32) {
-      const int xr = tr * 16 + j / 16, yc = tc * 16 + j % 16;
-      if (xr < g.X && yc < g.Y) m = fmaxf(m, g.ocache[size_t(xr) * g.Y + yc]);
-    }
-    m = warp_reduce_maxf(m);
-    if (lane == 0) g.TM[size_t(tr) * g.TY + tc] = m;
-  }
-}
-
-__global__ void k_ec_probe(EpieChainArgs g, int s) {
-  pdl_enter();
-  __shared__ float s_om;
-  float m = 0.f;
-  for (int j = threadIdx.x; j < g.TX * g.TY; j += blockDim.x) m = fmaxf(m, g.TM[j]);
-  m = block_reduce_maxf(m);
-  if (threadIdx.x == 0) {
-    s_om = m;
-    if (blockIdx.x == 0) g.sc->objMax = m;
-  }
-  __syncthreads();
-  const float cP = 1.0f / s_om;
-  const int i = g.order[s];
-  const float2 q = g.pos[i];
-  const int ox = int(roundf(q.x)), oy = int(roundf(q.y));
-  const int N = g.N;
+  const int tr0 = ox / 16, tc0 = oy / 16, ntc = (oy + N - 1) / 16 - tc0 + 1, ntr = (ox + N - 1) / 16 - tr0 + 1;
+  if (int(blockIdx.x) >= ntr * ntc) return;  // the grid covers the most tiles a patch can touch
+  const int tr = tr0 + int(blockIdx.x) / ntc, tc = tc0 + int(blockIdx.x) % ntc;
+  const int xr = tr * 16 + int(threadIdx.x) / 16, yc = tc * 16 + int(threadIdx.x) % 16;
   const size_t NN = size_t(N) * N;
-  float pmax = 0.f;
-  for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
-    const int x = int(idx / N), y = int(idx % N);
-    const float2 oc = g.obj[size_t(x + ox) * g.Y + (y + oy)];
-    float modal = 0.f;
-    for (int k = 0; k < g.K; ++k) {
-      float cache;
-      if (k < g.Ka) {
-        const float2 u = cconjmul(oc, g.psi[k * NN + idx]);
-        float2 pv = g.probe[k * NN + idx];
-        pv = make_float2(u.x * cP + pv.x, u.y * cP + pv.y);
-        const float mg = sqrtf(pv.x * pv.x + pv.y * pv.y);
-        g.probe[k * NN + idx] = pv;
-        cache = mg * mg;
-        g.pcache[k * NN + idx] = cache;
-      } else {
-        cache = g.pcache[k * NN + idx];
-      }
-      if (g.useAll && g.K > 1)
-        modal += cache;
-      else
-        pmax = fmaxf(pmax, cache);
+  float m2 = 0.f;
+  if (xr < g.X && yc < g.Y) {
+    const size_t o_i = size_t(xr) * g.Y + yc;
+    const int x = xr - ox, y = yc - oy;
+    if (x >= 0 && x < N && y >= 0 && y < N) {
+      const float pmax = (g.up && s > 0) ? g.pmax2[(s - 1) & 1] : g.sc->probeMax;
+      const float cO = 1.0f / pmax;
+      const size_t idx = size_t(x) * N + y;
+      float2 inc = make_float2(0.f, 0.f);
+      for (int k = 0; k < g.Ka; ++k) inc = cadd(inc, cconjmul(g.probe[k * NN + idx], g.psi[k * NN + idx]));
+      float2 o = g.obj[o_i];
+      o = make_float2(o.x + inc.x * cO, o.y + inc.y * cO);
+      const float mag = sqrtf(o.x * o.x + o.y * o.y);
+      if (g.pc) o = constrain_phase(o);
+      g.obj[o_i] = o;
+      m2 = mag * mag;
+      g.ocache[o_i] = m2;
+    } else {
+      m2 = g.ocache[o_i];
     }
-    if (g.useAll && g.K > 1) pmax = fmaxf(pmax, modal);
   }
-  pmax = block_reduce_maxf(pmax);
-  if (threadIdx.x == 0) atomicMax(reinterpret_cast<int*>(&g.pmax2[s & 1]), __float_as_int(pmax));
+  if (!g.up) return;  // the tile maxima are only consumed by the probe update
+  m2 = block_reduce_maxf(m2);
+  if (threadIdx.x == 0) g.TM[size_t(tr) * g.TY + tc] = m2;
 }
 
+// The last position's probe update and the probe maximum for the next iteration
 __global__ void k_ec_finish(EpieChainArgs g) {
+  pdl_enter();
+  if (!g.up || g.P == 0) return;
+  ec_probe_update(g, g.P - 1);
+}
+
+__global__ void k_ec_scalars(EpieChainArgs g) {
   pdl_enter();
   if (threadIdx.x == 0 && blockIdx.x == 0 && g.up && g.P > 0) g.sc->probeMax = g.pmax2[(g.P - 1) & 1];
 }
@@ -205,15 +209,14 @@ cudaError_t epie_chain_iteration(const EpieChainArgs& g, cudaStream_t st) {
     if ((e = fft(false)) != cudaSuccess) return e;
     if ((e = launch_pdl(k_ec_modulus, gb, 256, 0, st, g, s)) != cudaSuccess) return e;
     if ((e = fft(true)) != cudaSuccess) return e;
-    if ((e = launch_pdl(k_ec_object, gb, 256, 0, st, g, s)) != cudaSuccess) return e;
-    if (g.up) {
-      if ((e = launch_pdl(k_ec_tiles, (tiles * 32 + 255) / 256, 256, 0, st, g, s)) != cudaSuccess) return e;
-      if ((e = launch_pdl(k_ec_probe, gb, 256, 0, st, g, s)) != cudaSuccess) return e;
-    }
+    // one block per tile the patch touches: the tile count depends on the position's offset within a tile, so the
+    // grid covers the most a patch can touch and blocks past this position's tiles return
+    if ((e = launch_pdl(k_ec_object_tiles, tiles, 256, 0, st, g, s)) != cudaSuccess) return e;
   }
-  return launch_pdl(k_ec_finish, 1, 32, 0, st, g);
+  if ((e = launch_pdl(k_ec_finish, gb, 256, 0, st, g)) != cudaSuccess) return e;
+  return launch_pdl(k_ec_scalars, 1, 32, 0, st, g);
 }
 
-int epie_chain_launches(int P, bool up) { return P * (up ? 9 : 7) + 1; }
+int epie_chain_launches(int P, bool) { return P * 7 + 2; }
 
 }  // namespace pty

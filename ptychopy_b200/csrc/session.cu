@@ -727,9 +727,10 @@ void init_epie(pty_session* s) {
   const size_t NN = size_t(s->N) * s->N, XY = size_t(s->X) * s->Y;
   const int var = s->epie_variant;
   ep->chain_tc = s->prm.precision != 0;
-  // the chain spreads each step over the whole GPU; with several probe modes at 256^2 and up it measured 2.5x the
-  // fused cluster kernel (5 modes at 256^2: 93 vs 237 ms per iteration), so it is the automatic choice there
-  ep->chain = ep->chain_tc || var == 3 || (var < 0 && s->K > 1 && s->N >= 256);
+  // the chain spreads each step over the whole GPU: with several probe modes at 256^2 it measured 3.1x the fused
+  // cluster kernel (5 modes: 76.8 vs 237 ms per iteration), at 512^2 with one mode 1.15x the whole-GPU kernel
+  // (39.8 vs 45.7 ms), so it is the automatic choice there
+  ep->chain = ep->chain_tc || var == 3 || (var < 0 && ((s->K > 1 && s->N >= 256) || s->N >= 512));
   ep->sm = !ep->chain && epie_uses_smem(s->N, s->K) && (var < 0 || var == 0);
   if (ep->chain) {
     if (ep->chain_tc) {
