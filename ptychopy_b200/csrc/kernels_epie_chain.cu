@@ -14,6 +14,8 @@
 //             (a7): pixel-local, so it runs at the start of the next position's exit kernel, by the threads that
 //             then read those probe pixels (the last position's in a final kernel)
 // Every kernel is launched with programmatic dependent launch.
+#include <algorithm>
+
 #include "fft_core.cuh"
 #include "kernel_util.cuh"
 #include "kernels.h"
@@ -204,8 +206,16 @@ cudaError_t epie_chain_iteration(const EpieChainArgs& g, cudaStream_t st) {
     return g.tc ? fft2_tc(g.psi, g.work, g.Ka, g.N, inv, g.tcerr, st)
                 : fft2_pdl(g.psi, g.work, g.tw, g.Ka, g.N, inv, st);
   };
+  // the exit kernel carries the previous position's probe update, whose blocks each reduce the tile maxima of the
+  // whole object first: two blocks per SM keep that reduction from dominating its one-pixel-per-thread work
+  int sms = 148;
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const int gx = g.up ? std::min(gb, 2 * sms) : gb;
   for (int s = 0; s < g.P; ++s) {
-    if ((e = launch_pdl(k_ec_exit, gb, 256, 0, st, g, s)) != cudaSuccess) return e;
+    if ((e = launch_pdl(k_ec_exit, gx, 256, 0, st, g, s)) != cudaSuccess) return e;
     if ((e = fft(false)) != cudaSuccess) return e;
     if ((e = launch_pdl(k_ec_modulus, gb, 256, 0, st, g, s)) != cudaSuccess) return e;
     if ((e = fft(true)) != cudaSuccess) return e;
@@ -213,7 +223,7 @@ cudaError_t epie_chain_iteration(const EpieChainArgs& g, cudaStream_t st) {
     // grid covers the most a patch can touch and blocks past this position's tiles return
     if ((e = launch_pdl(k_ec_object_tiles, tiles, 256, 0, st, g, s)) != cudaSuccess) return e;
   }
-  if ((e = launch_pdl(k_ec_finish, gb, 256, 0, st, g)) != cudaSuccess) return e;
+  if ((e = launch_pdl(k_ec_finish, gx, 256, 0, st, g)) != cudaSuccess) return e;
   return launch_pdl(k_ec_scalars, 1, 32, 0, st, g);
 }
 
