@@ -513,6 +513,17 @@ void need(bool cond, const std::string& msg, int code = PTY_ERR_INVALID) {
 
 void set_device(pty_session* s) { check_cuda(cudaSetDevice(s->dev), "cudaSetDevice"); }
 
+// A session's own stream.  MLs and ePIE are chains of small dependent kernels whose time is their latency; DM runs
+// few large kernels.  The chains get the device's highest stream priority, so that beside other sessions (a batch)
+// their blocks are dispatched ahead of queued bulk work.  (The batched 8 DM + 8 MLs configuration measured the same
+// with and without it, 195 K vs 194 K patterns/s: its long MLs chains were not waiting behind the DM kernels.)
+void create_session_stream(pty_session* s, cudaStream_t* st) {
+  int least = 0, greatest = 0;
+  check_cuda(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
+  const int prio = (s->algo == ALGO_MLS || s->algo == ALGO_EPIE) ? greatest : least;
+  check_cuda(cudaStreamCreateWithPriority(st, cudaStreamNonBlocking, prio), "stream");
+}
+
 Algo parse_algo(const char* a) {
   std::string s(a);
   if (s == "ePIE") return ALGO_EPIE;
@@ -980,7 +991,7 @@ void init_mls(pty_session* s) {
     ml->pmax.alloc(sizeof(float), "illumination maximum");
     ml->vupd.alloc(sizeof(float2) * NN, "extra-mode update");
     ml->work2.alloc(sizeof(float2) * 2 * GN, "position-search FFT work");
-    check_cuda(cudaStreamCreateWithFlags(&ml->side, cudaStreamNonBlocking), "position-search stream");
+    create_session_stream(s, &ml->side);  // the position search's stream
     check_cuda(cudaEventCreateWithFlags(&ml->ev_fork, cudaEventDisableTiming), "event");
     check_cuda(cudaEventCreateWithFlags(&ml->ev_join, cudaEventDisableTiming), "event");
     if (s->K > 1) {
@@ -1501,7 +1512,7 @@ int pty_session_create(const pty_params* p, pty_session** out) {
     need(p->device >= 0 && p->device < ndev, "device ordinal out of range");
     s->dev = p->device;
     set_device(s);
-    check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+    create_session_stream(s, &s->stream);
     s->own_stream = true;
   });
   if (rc != PTY_OK) {
@@ -1959,7 +1970,7 @@ int pty_set_stream(pty_session* s, void* st) {
       s->stream = static_cast<cudaStream_t>(st);
       s->own_stream = false;
     } else if (!s->own_stream) {
-      check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+      create_session_stream(s, &s->stream);
       s->own_stream = true;
     }
   });
