@@ -25,19 +25,15 @@ struct EpiStore {
   __device__ void finish(int) {}
 };
 
+// Rows x0 .. x0 + RC - 1 of plane b: load through pro, transform, store transposed through epi.  s_tw holds the
+// twiddles, s_x the exchange / staging buffers (rows_smem_bytes<L> with s_tw); starts with a CTA barrier so that
+// calls may follow each other.
 template <int L, bool INV, class Pro, class Epi>
-__global__ void __launch_bounds__(FftShape<L>::THREADS) k_fftx_pass(float2* __restrict__ out,
-                                                                    const float2* __restrict__ g_tw, Pro pro, Epi epi) {
-  pdl_enter();
+__device__ __forceinline__ void fftx_rows(float2* out, const float2* s_tw, float2* s_x, int b, int x0, const Pro& pro,
+                                          Epi& epi) {
   using S = FftShape<L>;
   constexpr int T = S::T, E = S::E, R = S::RC;
-  extern __shared__ float4 smem4[];
-  float2* smem = reinterpret_cast<float2*>(smem4);
-  float2* s_tw = smem;
-  float2* s_x = smem + L;
-  const int v = threadIdx.x / T, t = threadIdx.x % T, b = blockIdx.y;
-  const int x0 = blockIdx.x * R;
-  load_twiddles<L>(s_tw, g_tw);
+  const int v = threadIdx.x / T, t = threadIdx.x % T;
   __syncthreads();
   float2 a[E];
 #pragma unroll
@@ -54,7 +50,17 @@ __global__ void __launch_bounds__(FftShape<L>::THREADS) k_fftx_pass(float2* __re
     const int vv = i % R, n = i / R;
     o[size_t(n) * L + x0 + vv] = epi(b, n, x0 + vv, L, s_x[n * (R + 1) + vv]);
   }
-  epi.finish(b);
+}
+
+template <int L, bool INV, class Pro, class Epi>
+__global__ void __launch_bounds__(FftShape<L>::THREADS) k_fftx_pass(float2* __restrict__ out,
+                                                                    const float2* __restrict__ g_tw, Pro pro, Epi epi) {
+  pdl_enter();
+  extern __shared__ float4 smem4[];
+  float2* smem = reinterpret_cast<float2*>(smem4);
+  load_twiddles<L>(smem, g_tw);
+  fftx_rows<L, INV>(out, smem, smem + L, blockIdx.y, blockIdx.x * FftShape<L>::RC, pro, epi);
+  epi.finish(blockIdx.y);
 }
 
 template <int L, bool INV, class Pro, class Epi>
@@ -85,6 +91,30 @@ inline cudaError_t fftx2(int N, float2* work, float2* out, const float2* tw, int
       return cudaErrorInvalidValue;
   }
 #undef PTY_FFTX
+}
+
+// ---- whole 2-D transforms inside one thread-block cluster ------------------------------------------------------
+// A cluster of C CTAs owns one plane: CTA `rank` transforms row blocks rank, rank + C, ... of each pass, and the
+// passes hand the plane to each other through global memory (L2) across cluster barriers, so that a chain of 2-D
+// transforms with pointwise steps between them runs as one launch.
+// barrier.cluster.arrive (release) + wait (acquire): cluster-scope ordering of the global-memory hand-offs.
+__device__ __forceinline__ void cluster_sync_acqrel() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// in (through pro) -> work (transposed) -> out (through epi); ends with a cluster barrier, so out is complete for
+// every CTA of the cluster on return
+template <int L, bool INV, class Pro, class Epi>
+__device__ __forceinline__ void fftx2_cluster(float2* work, float2* out, int b, int rank, int C, const float2* s_tw,
+                                              float2* s_x, const Pro& pro, Epi epi) {
+  constexpr int R = FftShape<L>::RC;
+  EpiStore plain;
+  for (int x0 = rank * R; x0 < L; x0 += C * R) fftx_rows<L, INV>(work, s_tw, s_x, b, x0, pro, plain);
+  cluster_sync_acqrel();
+  const ProLoad lw{work};
+  for (int x0 = rank * R; x0 < L; x0 += C * R) fftx_rows<L, INV>(out, s_tw, s_x, b, x0, lw, epi);
+  epi.finish(b);
+  cluster_sync_acqrel();
 }
 
 }  // namespace pty

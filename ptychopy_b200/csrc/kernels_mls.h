@@ -83,8 +83,12 @@ cudaError_t mls_iteration(const MlsBuffers& b, int ngroups, cudaStream_t st);
 int mls_launches_per_iteration(int ngroups);
 // One iteration of the reference-default path (kernels_mls_var.cu); flags from MlsVarFlags.
 cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, cudaStream_t st);
-int mls_var_launches_per_iteration(int ngroups, unsigned flags, int K, bool tc);
+int mls_var_launches_per_iteration(int ngroups, unsigned flags, int K, bool tc, int N);
 size_t mls_var_scratch_doubles(int Gmax);
+// One mode in FP32 up to 256^2: the group's six 2-D transforms run as one cluster launch; mls_var_prepare sets that
+// launch up for N x N windows (outside graph capture).
+bool mls_var_fused(int N, int K, bool tc);
+cudaError_t mls_var_prepare(int N);
 // MLs probe modes 1..K-1 from mode 0 (initMLH): phase tilts (2 (K-1) values, device), then the Gram matrix
 // G_ij = sum conj(m_i) m_j (K x K double2, device) for the host's eigen-decomposition, then modes <- modes V
 // (V: K x K double2 on the device, column i = combination i); tmp holds K x N x N.

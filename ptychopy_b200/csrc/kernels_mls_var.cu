@@ -23,6 +23,7 @@
 //             extra-mode and intensity weights of the group's positions (update_variable_probe, src/Probe.cpp:1366-1516)
 // Scalar bookkeeping (2x2 solves, position and weight updates) runs in one thread on the device, so the iteration
 // is one CUDA graph with no host round trip.
+#include <algorithm>
 #include <cmath>
 
 #include "fft_core.cuh"
@@ -752,12 +753,127 @@ struct EpiPosSums {
   }
 };
 
+// The group's six FP32 2-D transforms with one probe mode, from the exit waves to the shifted-back probe direction,
+// as one launch: a thread-block cluster per window runs the twelve row passes with the pointwise steps in their loads
+// and stores (the same functors as the separate passes) and cluster barriers between the passes.  Every step of the
+// chain reads only its own window, so no hand-off leaves the cluster.
+struct VarFront {
+  ProExit exit;
+  EpiPhase shift;
+  EpiVpPsi vpsi;
+  EpiModulus modulus;
+  EpiChi chi;
+  EpiPhase unshift;
+  float2 *work, *vp, *psi, *pu;
+  const float2* tw;
+};
+
+template <int L>
+__global__ void __launch_bounds__(FftShape<L>::THREADS) k_var_front(VarFront a) {
+  pdl_enter();
+  extern __shared__ float4 smem4[];
+  float2* s_tw = reinterpret_cast<float2*>(smem4);
+  float2* s_x = s_tw + L;
+  load_twiddles<L>(s_tw, a.tw);  // each row block starts with a CTA barrier
+  const int b = blockIdx.y, rank = blockIdx.x, C = gridDim.x;
+  fftx2_cluster<L, false>(a.work, a.vp, b, rank, C, s_tw, s_x, a.exit, a.shift);         // shifted probe
+  fftx2_cluster<L, true>(a.work, a.vp, b, rank, C, s_tw, s_x, ProLoad{a.vp}, a.vpsi);    // vp, psi = objp vp
+  fftx2_cluster<L, false>(a.work, a.psi, b, rank, C, s_tw, s_x, ProLoad{a.psi}, a.modulus);
+  fftx2_cluster<L, true>(a.work, a.psi, b, rank, C, s_tw, s_x, ProLoad{a.psi}, a.chi);   // chi, pu, S
+  fftx2_cluster<L, false>(a.work, a.pu, b, rank, C, s_tw, s_x, ProLoad{a.pu}, a.unshift);
+  fftx2_cluster<L, true>(a.work, a.pu, b, rank, C, s_tw, s_x, ProLoad{a.pu}, EpiStore{});
+}
+
+// Cluster size: one CTA per row block of a plane up to 16 (the largest cluster, opted into), halved while no such
+// cluster fits on an SM group
+template <int L>
+int var_front_cluster() {
+  constexpr int R = FftShape<L>::RC, NT = FftShape<L>::THREADS;
+  const int smem = int(rows_smem_bytes<L>());
+  if (cudaFuncSetAttribute(k_var_front<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_var_front<L>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    return 0;
+  for (int C = std::min(L / R, 16); C >= 1; C /= 2) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C, 1);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = size_t(smem);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_var_front<L>, &cfg) == cudaSuccess && n >= 1) return C;
+    cudaGetLastError();
+  }
+  return 0;
+}
+
+// chosen once per process (the first session sets it up outside any graph capture, mls_var_prepare)
+template <int L>
+int front_cluster() {
+  static const int C = var_front_cluster<L>();
+  return C;
+}
+
+template <int L>
+cudaError_t launch_var_front(const VarFront& a, int planes, cudaStream_t st) {
+  const int C = front_cluster<L>();
+  if (C < 1) return cudaErrorInvalidConfiguration;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C, planes);
+  cfg.blockDim = dim3(FftShape<L>::THREADS);
+  cfg.dynamicSmemBytes = rows_smem_bytes<L>();
+  cfg.stream = st;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 2;
+  return cudaLaunchKernelEx(&cfg, k_var_front<L>, a);
+}
+
+cudaError_t var_front(const VarFront& a, int N, int planes, cudaStream_t st) {
+  switch (N) {
+    case 32: return launch_var_front<32>(a, planes, st);
+    case 64: return launch_var_front<64>(a, planes, st);
+    case 128: return launch_var_front<128>(a, planes, st);
+    case 256: return launch_var_front<256>(a, planes, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 int grid_n(size_t n, int cap = 1184) {
   size_t g = (n + 255) / 256;
   return int(g < 1 ? 1 : (g > size_t(cap) ? cap : g));
 }
 
 }  // namespace
+
+// The one-launch group transforms pay where a window's row blocks fill its cluster (one per CTA, N <= 256); at
+// 512^2 a 16-CTA cluster per window leaves most SMs idle (measured 2.2x slower with one window per group), and the
+// separate passes, 64 CTAs per window, stay.
+bool mls_var_fused(int N, int K, bool tc) { return !tc && K == 1 && N <= 256; }
+
+cudaError_t mls_var_prepare(int N) {
+  int C = 0;
+  switch (N) {
+    case 32: C = front_cluster<32>(); break;
+    case 64: C = front_cluster<64>(); break;
+    case 128: C = front_cluster<128>(); break;
+    case 256: C = front_cluster<256>(); break;
+    default: break;
+  }
+  cudaGetLastError();
+  return C >= 1 ? cudaSuccess : cudaErrorInvalidConfiguration;
+}
 
 size_t mls_var_scratch_doubles(int Gmax) { return 9 * size_t(Gmax) + 8; }
 
@@ -811,14 +927,14 @@ cudaError_t mls_zone_plate_probe(float2* probe, float2* pf, float2* work, const 
   return cudaGetLastError();
 }
 
-int mls_var_launches_per_iteration(int ngroups, unsigned flags, int K, bool tc) {
+int mls_var_launches_per_iteration(int ngroups, unsigned flags, int K, bool tc, int N) {
   int pre = 1 + 4 + 1 + 2 + 1;  // boxes, norm (sums + 3 scales), recentre, illumination (2), max
   if (flags & MLS_WINDOWS) ++pre;
   if (flags & MLS_REMOVE) pre += 4;
   // per group: six 2-D transforms of two passes; FP32 fuses exit, both phase ramps, psi, the one-mode modulus and
-  // the directions into them, the tensor-core path runs them as 6 kernels (the modulus only for one mode); then
-  // pum, lsq, solve and the two updates
-  int per = 12 + 5 + (tc ? 6 + (K == 1 ? 1 : 0) : 0);
+  // the directions into them (one mode up to 256^2: all twelve passes in one cluster launch), the tensor-core path
+  // runs them as 6 kernels (the modulus only for one mode); then pum, lsq, solve and the two updates
+  int per = (mls_var_fused(N, K, tc) ? 1 : 12) + 5 + (tc ? 6 + (K == 1 ? 1 : 0) : 0);
   if (flags & MLS_POSSEARCH) per += tc ? 2 + 1 + 2 + 1 + 1 : 2 + 2 + 1;
   if (flags & MLS_VARUPD) per += 5;
   // other modes: exit waves, forward and inverse 2-D transforms, the modal modulus, one update each
@@ -857,66 +973,81 @@ cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, 
   if ((e = max_real(b.pobj, XY, b.pmax, st)) != cudaSuccess) return e;
   const int gb = (NN + 255) / 256 > 64 ? 64 : (NN + 255) / 256;
   const dim3 grid(gb, b.Gmax);
+  const bool fused = mls_var_fused(N, b.K, b.tc);
   for (int g = 0; g < ngroups; ++g) {
     const int* mem = b.members + size_t(g) * b.Gmax;
     const int* gs = b.gsize + g;
-    if (b.tc) {  // tensor-core transforms: separate pointwise kernels around fft2_tc
-      launch_pdl(k_var_exit, grid, 256, 0, st, b.obj, b.probe, b.E, b.evo, P, b.win, mem, gs, N, b.Y, b.objp, b.vp);
-      if ((e = fft(b.vp, b.Gmax, false)) != cudaSuccess) return e;
-      launch_pdl(k_var_phase, grid, 256, 0, st, b.vp, b.sub, mem, gs, N, 1.f);
-      if ((e = fft(b.vp, b.Gmax, true)) != cudaSuccess) return e;
-      launch_pdl(k_var_psi, grid_n(GN), 256, 0, st, b.objp, b.vp, b.psi, GN);
-      if ((e = fft(b.psi, b.Gmax, false)) != cudaSuccess) return e;
-    } else {  // FP32 transforms with the pointwise steps fused into their loads and stores
-      const ProExit pe{b.obj, b.probe, b.E, b.evo, b.win, mem, gs, b.objp, P, b.Y};
-      if ((e = fftx2<false>(N, b.work, b.vp, b.tw, b.Gmax, pe, EpiPhase{b.sub, mem, gs, 1.f}, st)) != cudaSuccess)
-        return e;
-      if ((e = fftx2<true>(N, b.work, b.vp, b.tw, b.Gmax, ProLoad{b.vp}, EpiVpPsi{b.objp, b.psi}, st)) != cudaSuccess)
-        return e;
-      if (b.K == 1) {
-        if ((e = fftx2<false>(N, b.work, b.psi, b.tw, b.Gmax, ProLoad{b.psi}, EpiModulus{b.amp, mem, gs, b.errk, 0.0},
-                              st)) != cudaSuccess)
-          return e;
-      } else if ((e = fft(b.psi, b.Gmax, false)) != cudaSuccess) {
-        return e;
-      }
-    }
-    if (b.K > 1) {
-      launch_pdl(k_var_psik, grid_n(size_t(b.K - 1) * GN), 256, 0, st, b.probe, b.objp, b.psik, b.K, b.Gmax, NN);
-      if ((e = fft(b.psik, (b.K - 1) * b.Gmax, false)) != cudaSuccess) return e;
-      launch_pdl(k_var_modulus, grid, 256, 0, st, b.psi, b.psik, b.amp, mem, gs, N, b.K, b.Gmax, b.errk);
-      if ((e = fft(b.psik, (b.K - 1) * b.Gmax, true)) != cudaSuccess) return e;
-    } else if (b.tc && (e = mls_modulus(b, mem, gs, st)) != cudaSuccess) {
-      return e;
-    }
-    if (b.tc) {
-      if ((e = fft(b.psi, b.Gmax, true)) != cudaSuccess) return e;
-      launch_pdl(k_var_dirs, grid, 256, 0, st, b.psi, b.objp, b.vp, b.win, mem, gs, N, b.Y, b.pu, b.S);
-      if ((e = fft(b.pu, b.Gmax, false)) != cudaSuccess) return e;
-      launch_pdl(k_var_phase, grid, 256, 0, st, b.pu, b.sub, mem, gs, N, -1.f);
+    // the position search needs this group's windows, probes and chi only, and writes positions that no kernel
+    // reads before the next iteration: it runs on the side stream while the group goes on, and joins before the
+    // next group rewrites those buffers
+    auto possearch_fork = [&]() -> cudaError_t {
+      cudaError_t r;
+      if ((r = cudaEventRecord(b.ev_fork, st)) != cudaSuccess) return r;
+      if ((r = cudaStreamWaitEvent(b.side, b.ev_fork, 0)) != cudaSuccess) return r;
+      if ((r = fftx2<false>(N, b.work2, b.aux, b.tw, b.Gmax, ProLoad{b.objp}, EpiGrad{b.aux + GN}, b.side)) !=
+          cudaSuccess)
+        return r;
+      const EpiPosSums ps{b.vp, b.psi, gs, b.vs + L.pos(), b.Gmax, 0.0, 0.0};
+      if ((r = fftx2<true>(N, b.work2, b.aux, b.tw, 2 * b.Gmax, ProLoad{b.aux}, ps, b.side)) != cudaSuccess) return r;
+      launch_pdl(k_var_posupd, 1, 32, 0, b.side, b.vs + L.pos(), mem, gs, b.pos);
+      return cudaEventRecord(b.ev_join, b.side);
+    };
+    if (fused) {  // FP32, one mode: the six transforms and their pointwise steps in one cluster launch
+      const VarFront a{ProExit{b.obj, b.probe, b.E, b.evo, b.win, mem, gs, b.objp, P, b.Y},
+                       EpiPhase{b.sub, mem, gs, 1.f},
+                       EpiVpPsi{b.objp, b.psi},
+                       EpiModulus{b.amp, mem, gs, b.errk, 0.0},
+                       EpiChi{b.objp, b.vp, b.win, mem, gs, b.pu, b.S, b.Y},
+                       EpiPhase{b.sub, mem, gs, -1.f},
+                       b.work, b.vp, b.psi, b.pu, b.tw};
+      if ((e = var_front(a, N, b.Gmax, st)) != cudaSuccess) return e;
+      if ((flags & MLS_POSSEARCH) && (e = possearch_fork()) != cudaSuccess) return e;
     } else {
-      const EpiChi ec{b.objp, b.vp, b.win, mem, gs, b.pu, b.S, b.Y};
-      if ((e = fftx2<true>(N, b.work, b.psi, b.tw, b.Gmax, ProLoad{b.psi}, ec, st)) != cudaSuccess) return e;
-      if (flags & MLS_POSSEARCH) {
-        // the position search needs this group's windows, probes and chi only, and writes positions that no kernel
-        // reads before the next iteration: it runs on the side stream while the group goes on, and joins before
-        // the next group rewrites those buffers
-        if ((e = cudaEventRecord(b.ev_fork, st)) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(b.side, b.ev_fork, 0)) != cudaSuccess) return e;
-        if ((e = fftx2<false>(N, b.work2, b.aux, b.tw, b.Gmax, ProLoad{b.objp}, EpiGrad{b.aux + GN}, b.side)) !=
+      if (b.tc) {  // tensor-core transforms: separate pointwise kernels around fft2_tc
+        launch_pdl(k_var_exit, grid, 256, 0, st, b.obj, b.probe, b.E, b.evo, P, b.win, mem, gs, N, b.Y, b.objp, b.vp);
+        if ((e = fft(b.vp, b.Gmax, false)) != cudaSuccess) return e;
+        launch_pdl(k_var_phase, grid, 256, 0, st, b.vp, b.sub, mem, gs, N, 1.f);
+        if ((e = fft(b.vp, b.Gmax, true)) != cudaSuccess) return e;
+        launch_pdl(k_var_psi, grid_n(GN), 256, 0, st, b.objp, b.vp, b.psi, GN);
+        if ((e = fft(b.psi, b.Gmax, false)) != cudaSuccess) return e;
+      } else {  // FP32 transforms with the pointwise steps fused into their loads and stores
+        const ProExit pe{b.obj, b.probe, b.E, b.evo, b.win, mem, gs, b.objp, P, b.Y};
+        if ((e = fftx2<false>(N, b.work, b.vp, b.tw, b.Gmax, pe, EpiPhase{b.sub, mem, gs, 1.f}, st)) != cudaSuccess)
+          return e;
+        if ((e = fftx2<true>(N, b.work, b.vp, b.tw, b.Gmax, ProLoad{b.vp}, EpiVpPsi{b.objp, b.psi}, st)) !=
             cudaSuccess)
           return e;
-        const EpiPosSums ps{b.vp, b.psi, gs, b.vs + L.pos(), b.Gmax, 0.0, 0.0};
-        if ((e = fftx2<true>(N, b.work2, b.aux, b.tw, 2 * b.Gmax, ProLoad{b.aux}, ps, b.side)) != cudaSuccess)
+        if (b.K == 1) {
+          if ((e = fftx2<false>(N, b.work, b.psi, b.tw, b.Gmax, ProLoad{b.psi},
+                                EpiModulus{b.amp, mem, gs, b.errk, 0.0}, st)) != cudaSuccess)
+            return e;
+        } else if ((e = fft(b.psi, b.Gmax, false)) != cudaSuccess) {
           return e;
-        launch_pdl(k_var_posupd, 1, 32, 0, b.side, b.vs + L.pos(), mem, gs, b.pos);
-        if ((e = cudaEventRecord(b.ev_join, b.side)) != cudaSuccess) return e;
+        }
       }
-      if ((e = fftx2<false>(N, b.work, b.pu, b.tw, b.Gmax, ProLoad{b.pu}, EpiPhase{b.sub, mem, gs, -1.f}, st)) !=
-          cudaSuccess)
+      if (b.K > 1) {
+        launch_pdl(k_var_psik, grid_n(size_t(b.K - 1) * GN), 256, 0, st, b.probe, b.objp, b.psik, b.K, b.Gmax, NN);
+        if ((e = fft(b.psik, (b.K - 1) * b.Gmax, false)) != cudaSuccess) return e;
+        launch_pdl(k_var_modulus, grid, 256, 0, st, b.psi, b.psik, b.amp, mem, gs, N, b.K, b.Gmax, b.errk);
+        if ((e = fft(b.psik, (b.K - 1) * b.Gmax, true)) != cudaSuccess) return e;
+      } else if (b.tc && (e = mls_modulus(b, mem, gs, st)) != cudaSuccess) {
         return e;
+      }
+      if (b.tc) {
+        if ((e = fft(b.psi, b.Gmax, true)) != cudaSuccess) return e;
+        launch_pdl(k_var_dirs, grid, 256, 0, st, b.psi, b.objp, b.vp, b.win, mem, gs, N, b.Y, b.pu, b.S);
+        if ((e = fft(b.pu, b.Gmax, false)) != cudaSuccess) return e;
+        launch_pdl(k_var_phase, grid, 256, 0, st, b.pu, b.sub, mem, gs, N, -1.f);
+      } else {
+        const EpiChi ec{b.objp, b.vp, b.win, mem, gs, b.pu, b.S, b.Y};
+        if ((e = fftx2<true>(N, b.work, b.psi, b.tw, b.Gmax, ProLoad{b.psi}, ec, st)) != cudaSuccess) return e;
+        if ((flags & MLS_POSSEARCH) && (e = possearch_fork()) != cudaSuccess) return e;
+        if ((e = fftx2<false>(N, b.work, b.pu, b.tw, b.Gmax, ProLoad{b.pu}, EpiPhase{b.sub, mem, gs, -1.f}, st)) !=
+            cudaSuccess)
+          return e;
+      }
+      if ((e = fft(b.pu, b.Gmax, true)) != cudaSuccess) return e;
     }
-    if ((e = fft(b.pu, b.Gmax, true)) != cudaSuccess) return e;
     launch_pdl(k_var_pum, grid_n(NN, 256), 256, 0, st, b.pu, b.pobj, b.maxIllum, b.win, mem, gs, N, b.Y, b.pum);
     if ((e = mls_lsq(b, b.vp, NN, mem, gs, st)) != cudaSuccess) return e;
     if ((e = mls_solve_update(b, mem, gs, b.boxw + 4 * size_t(g), 0, st)) != cudaSuccess) return e;

@@ -994,6 +994,8 @@ void init_mls(pty_session* s) {
     create_session_stream(s, &ml->side);  // the position search's stream
     check_cuda(cudaEventCreateWithFlags(&ml->ev_fork, cudaEventDisableTiming), "event");
     check_cuda(cudaEventCreateWithFlags(&ml->ev_join, cudaEventDisableTiming), "event");
+    if (mls_var_fused(s->N, s->K, s->prm.precision != 0))
+      check_cuda(mls_var_prepare(s->N), "MLs cluster launch set-up");
     if (s->K > 1) {
       ml->psik.alloc(sizeof(float2) * GN * (s->K - 1), "exit waves of the other modes");
       ml->mtmp.alloc(sizeof(float2) * NN * s->K, "mode scratch");
@@ -1144,7 +1146,7 @@ double step_mls(pty_session* s, bool want_err) {
       check_cuda(e3, "graph instantiate");
     }
     check_cuda(cudaGraphLaunch(ge, s->stream), "MLs graph launch");
-    s->launches += mls_var_launches_per_iteration(ml->ng, flags, s->K, s->prm.precision != 0);
+    s->launches += mls_var_launches_per_iteration(ml->ng, flags, s->K, s->prm.precision != 0, s->N);
   } else {
   if (!tb.graph) {
     const MlsBuffers b = mls_buffers(s, parity);
