@@ -4,6 +4,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <utility>
+
 #include "fft_core.cuh"
 #include "kernel_util.cuh"
 #include "pdl.cuh"
@@ -115,6 +117,56 @@ __device__ __forceinline__ void fftx2_cluster(float2* work, float2* out, int b, 
   for (int x0 = rank * R; x0 < L; x0 += C * R) fftx_rows<L, INV>(out, s_tw, s_x, b, x0, lw, epi);
   epi.finish(b);
   cluster_sync_acqrel();
+}
+
+// Largest cluster of `kernel` (at most one CTA per row block of a plane and at most 16, the largest size, opted
+// into) of which one fits on the device; 0 if none.  Sets the kernel's shared-memory and cluster attributes.
+template <class Kern>
+inline int fit_cluster(Kern* kernel, int row_blocks, int threads, size_t smem) {
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  for (int C = row_blocks < 16 ? row_blocks : 16; C >= 1; C /= 2) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C, 1);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kernel, &cfg) == cudaSuccess && n >= 1) return C;
+    cudaGetLastError();
+  }
+  return 0;
+}
+
+// Launch of a grid of (C, planes) CTAs in clusters of C along x, with programmatic stream serialisation
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_cluster_pdl(void (*kernel)(KArgs...), int C, int planes, int threads, size_t smem,
+                                      cudaStream_t st, Args&&... args) {
+  if (C < 1) return cudaErrorInvalidConfiguration;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C, planes);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 2;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 }  // namespace pty

@@ -784,60 +784,17 @@ __global__ void __launch_bounds__(FftShape<L>::THREADS) k_var_front(VarFront a) 
   fftx2_cluster<L, true>(a.work, a.pu, b, rank, C, s_tw, s_x, ProLoad{a.pu}, EpiStore{});
 }
 
-// Cluster size: one CTA per row block of a plane up to 16 (the largest cluster, opted into), halved while no such
-// cluster fits on an SM group
-template <int L>
-int var_front_cluster() {
-  constexpr int R = FftShape<L>::RC, NT = FftShape<L>::THREADS;
-  const int smem = int(rows_smem_bytes<L>());
-  if (cudaFuncSetAttribute(k_var_front<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
-      cudaFuncSetAttribute(k_var_front<L>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
-    return 0;
-  for (int C = std::min(L / R, 16); C >= 1; C /= 2) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(C, 1);
-    cfg.blockDim = dim3(NT);
-    cfg.dynamicSmemBytes = size_t(smem);
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = C;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, k_var_front<L>, &cfg) == cudaSuccess && n >= 1) return C;
-    cudaGetLastError();
-  }
-  return 0;
-}
-
 // chosen once per process (the first session sets it up outside any graph capture, mls_var_prepare)
 template <int L>
 int front_cluster() {
-  static const int C = var_front_cluster<L>();
+  static const int C = fit_cluster(k_var_front<L>, L / FftShape<L>::RC, FftShape<L>::THREADS, rows_smem_bytes<L>());
   return C;
 }
 
 template <int L>
 cudaError_t launch_var_front(const VarFront& a, int planes, cudaStream_t st) {
-  const int C = front_cluster<L>();
-  if (C < 1) return cudaErrorInvalidConfiguration;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(C, planes);
-  cfg.blockDim = dim3(FftShape<L>::THREADS);
-  cfg.dynamicSmemBytes = rows_smem_bytes<L>();
-  cfg.stream = st;
-  cudaLaunchAttribute at[2];
-  at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = C;
-  at[0].val.clusterDim.y = 1;
-  at[0].val.clusterDim.z = 1;
-  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[1].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 2;
-  return cudaLaunchKernelEx(&cfg, k_var_front<L>, a);
+  return launch_cluster_pdl(k_var_front<L>, front_cluster<L>(), planes, FftShape<L>::THREADS, rows_smem_bytes<L>(),
+                            st, a);
 }
 
 cudaError_t var_front(const VarFront& a, int N, int planes, cudaStream_t st) {
