@@ -65,6 +65,8 @@ enum MlsVarFlags : unsigned {
   MLS_REMOVE = 2u,      // remove_extra_degree (from iteration 2)
   MLS_VARUPD = 4u,      // update_variable_probe (from iteration 3)
   MLS_POSSEARCH = 8u,   // gradient_position_solver (from PPS)
+  MLS_SEPARATE = 16u,   // separate transform passes even where one cluster launch per window would serve (the
+                        // step shares the GPU with other scans, whose kernels hold SMs the clusters wait for)
 };
 
 cudaError_t mls_illum_add(float* pobj, const float2* probe, const int2* starts, int P, int N, int Y, float scale,

@@ -816,7 +816,8 @@ int grid_n(size_t n, int cap = 1184) {
 
 // The one-launch group transforms pay where a window's row blocks fill its cluster (one per CTA, N <= 256); at
 // 512^2 a 16-CTA cluster per window leaves most SMs idle (measured 2.2x slower with one window per group), and the
-// separate passes, 64 CTAs per window, stay.
+// separate passes, 64 CTAs per window, stay.  Beside other scans' kernels (MLS_SEPARATE) the separate passes stay
+// too: 16 scans of the batched workload measured 163.5 K patterns/s with the cluster launches, 193.3 K without.
 bool mls_var_fused(int N, int K, bool tc) { return !tc && K == 1 && N <= 256; }
 
 cudaError_t mls_var_prepare(int N) {
@@ -891,7 +892,7 @@ int mls_var_launches_per_iteration(int ngroups, unsigned flags, int K, bool tc, 
   // per group: six 2-D transforms of two passes; FP32 fuses exit, both phase ramps, psi, the one-mode modulus and
   // the directions into them (one mode up to 256^2: all twelve passes in one cluster launch), the tensor-core path
   // runs them as 6 kernels (the modulus only for one mode); then pum, lsq, solve and the two updates
-  int per = (mls_var_fused(N, K, tc) ? 1 : 12) + 5 + (tc ? 6 + (K == 1 ? 1 : 0) : 0);
+  int per = (mls_var_fused(N, K, tc) && !(flags & MLS_SEPARATE) ? 1 : 12) + 5 + (tc ? 6 + (K == 1 ? 1 : 0) : 0);
   if (flags & MLS_POSSEARCH) per += tc ? 2 + 1 + 2 + 1 + 1 : 2 + 2 + 1;
   if (flags & MLS_VARUPD) per += 5;
   // other modes: exit waves, forward and inverse 2-D transforms, the modal modulus, one update each
@@ -930,7 +931,7 @@ cudaError_t mls_iteration_var(const MlsBuffers& b, int ngroups, unsigned flags, 
   if ((e = max_real(b.pobj, XY, b.pmax, st)) != cudaSuccess) return e;
   const int gb = (NN + 255) / 256 > 64 ? 64 : (NN + 255) / 256;
   const dim3 grid(gb, b.Gmax);
-  const bool fused = mls_var_fused(N, b.K, b.tc);
+  const bool fused = mls_var_fused(N, b.K, b.tc) && !(flags & MLS_SEPARATE);
   for (int g = 0; g < ngroups; ++g) {
     const int* mem = b.members + size_t(g) * b.Gmax;
     const int* gs = b.gsize + g;

@@ -1081,7 +1081,9 @@ MlsBuffers mls_buffers(pty_session* s, int parity) {
 
 // One MLs iteration: the iteration's random groups (a SplitMix64 permutation cut into groups of max(1, P/100), in a
 // second shuffled order) are written to the device tables, then the iteration graph replays.
-double step_mls(pty_session* s, bool want_err) {
+// shared_gpu: the step runs beside other scans' kernels (pty_batch_run), where the MLs groups use their separate
+// transform passes (MLS_SEPARATE) rather than one launch of 16-CTA clusters, which waits for whole SM groups to free up
+double step_mls(pty_session* s, bool want_err, bool shared_gpu = false) {
   MlsState* ml = s->ml;
   const int P = s->P, G = ml->Gmax, N = s->N;
   const int parity = int(ml->steps & 1);
@@ -1130,6 +1132,7 @@ double step_mls(pty_session* s, bool want_err) {
     if (it > 1) flags |= MLS_REMOVE;
     if (it > 2) flags |= MLS_VARUPD;
     if (it >= pps) flags |= MLS_POSSEARCH;
+    if (shared_gpu) flags |= MLS_SEPARATE;
     const unsigned key = unsigned(parity) | (flags << 1);
     cudaGraphExec_t& ge = ml->var_graphs[key];
     if (!ge) {
@@ -1857,7 +1860,7 @@ int pty_batch_run(pty_session* const* sessions, int n, int iters) {
         if (s->algo == ALGO_EPIE)
           step_epie(s, k, false);
         else if (s->algo == ALGO_MLS)
-          step_mls(s, false);
+          step_mls(s, false, true);
         else
           step_dm(s, k);
         s->iter = k;
