@@ -104,6 +104,25 @@ __device__ __forceinline__ double block_reduce_sum(double v) {
   if (w == 0) v = warp_reduce_sum(v);
   return v;
 }
+// M block-wide sums at once, with the same additions in the same order as M calls of block_reduce_sum but two CTA
+// barriers in all; the results are valid in thread 0.
+template <int M>
+__device__ __forceinline__ void block_reduce_sum_n(double (&v)[M]) {
+  __shared__ double s[M][32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int m = 0; m < M; ++m) v[m] = warp_reduce_sum(v[m]);
+  __syncthreads();
+  if (l == 0) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) s[m][w] = v[m];
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) v[m] = warp_reduce_sum(threadIdx.x < (blockDim.x >> 5) ? s[m][l] : 0.0);
+  }
+}
 __device__ __forceinline__ double block_reduce_max(double v) {
   __shared__ double s[32];
   v = warp_reduce_max(v);

@@ -138,17 +138,47 @@ __global__ void k_mls_dirs(const float2* __restrict__ chi, const float2* __restr
   }
 }
 
-// probe: one N x N probe for every window (pstride 0) or one per window (pstride N^2).
-__global__ void k_mls_lsq(const float2* __restrict__ chi, const float2* __restrict__ objp,
-                          const float2* __restrict__ probe, size_t pstride, const float2* __restrict__ pum,
-                          const float2* __restrict__ S, const float* __restrict__ pobj,
-                          const float* __restrict__ maxIllum, float delta_p, const int2* __restrict__ starts,
-                          const int* __restrict__ members, const int* __restrict__ gsize, int N, int Y,
-                          double* __restrict__ sums) {
-  pdl_enter();
-  const int k = blockIdx.y;
-  const int G = *gsize;
-  if (k >= G) return;
+// Regularised 2x2 solves, group-mean steps, Fourier error; clears the per-group accumulators (one thread; sums and
+// errk read from L2, where the atomics of the group's blocks landed).
+__device__ void mls_solve_group(double* sums, double* errk, int G, int N, double beta_obj, double beta_probe,
+                                double* betas, double* err_total) {
+  double m1 = 0, m4 = 0;
+  for (int k = 0; k < G; ++k) {
+    m1 += __ldcg(&sums[k * 6 + 0]);
+    m4 += __ldcg(&sums[k * 6 + 1]);
+  }
+  m1 = 0.1 * m1 / G;
+  m4 = 0.1 * m4 / G;
+  double bor = 0, boi = 0, bpr = 0, bpi = 0, e = 0;
+  for (int k = 0; k < G; ++k) {
+    const double A11 = __ldcg(&sums[k * 6 + 0]) + m1, A22 = __ldcg(&sums[k * 6 + 1]) + m4;
+    const double cr = __ldcg(&sums[k * 6 + 2]), ci = __ldcg(&sums[k * 6 + 3]);  // A12 = c, A21 = conj(c)
+    const double b1 = __ldcg(&sums[k * 6 + 4]), b2 = __ldcg(&sums[k * 6 + 5]);
+    const double det = A11 * A22 - (cr * cr + ci * ci);      // real for a Hermitian 2x2
+    // x0 = (b1 A22 - c b2)/det, x1 = (A11 b2 - conj(c) b1)/det
+    bor += (b1 * A22 - cr * b2) / det;
+    boi += (-ci * b2) / det;
+    bpr += (A11 * b2 - cr * b1) / det;
+    bpi += (ci * b1) / det;
+    e += sqrt(__ldcg(&errk[k]) / (double(N) * N));
+    for (int m = 0; m < 6; ++m) sums[k * 6 + m] = 0.0;
+    errk[k] = 0.0;
+  }
+  betas[0] = beta_obj * bor / G;
+  betas[1] = beta_obj * boi / G;
+  betas[2] = beta_probe * bpr / G;
+  betas[3] = beta_probe * bpi / G;
+  *err_total += e;
+}
+
+// LSQ sums of window k of the group (its blocks' share), added into sums[k * 6 ..]
+__device__ __forceinline__ void lsq_window_sums(const float2* __restrict__ chi, const float2* __restrict__ objp,
+                                                const float2* __restrict__ probe, size_t pstride,
+                                                const float2* __restrict__ pum, const float2* __restrict__ S,
+                                                const float* __restrict__ pobj, const float* __restrict__ maxIllum,
+                                                float delta_p, const int2* __restrict__ starts,
+                                                const int* __restrict__ members, int G, int k, int N, int Y,
+                                                double* sums) {
   const size_t NN = size_t(N) * N;
   const int2 s = starts[members[k]];
   const float dmax = *maxIllum * delta_p, invG = 1.f / float(G);
@@ -169,47 +199,37 @@ __global__ void k_mls_lsq(const float2* __restrict__ chi, const float2* __restri
     b2 += double(dPO.x * c.x + dPO.y * c.y);
   }
   double v[6] = {a1, a4, a2r, a2i, b1, b2};
-  for (int m = 0; m < 6; ++m) {
-    const double r = block_reduce_sum(v[m]);
-    if (threadIdx.x == 0) atomicAdd(&sums[k * 6 + m], r);
-    __syncthreads();
-  }
+  block_reduce_sum_n(v);
+  if (threadIdx.x == 0)
+    for (int m = 0; m < 6; ++m) atomicAdd(&sums[k * 6 + m], v[m]);
 }
 
-// One thread: regularised 2x2 solves, group-mean steps, Fourier error; clears the per-group accumulators.
-__global__ void k_mls_solve(double* __restrict__ sums, double* __restrict__ errk, const int* __restrict__ gsize,
-                            int N, double beta_obj, double beta_probe, double* __restrict__ betas,
-                            double* __restrict__ err_total) {
+// probe: one N x N probe for every window (pstride 0) or one per window (pstride N^2).
+__global__ void k_mls_lsq(const float2* __restrict__ chi, const float2* __restrict__ objp,
+                          const float2* __restrict__ probe, size_t pstride, const float2* __restrict__ pum,
+                          const float2* __restrict__ S, const float* __restrict__ pobj,
+                          const float* __restrict__ maxIllum, float delta_p, const int2* __restrict__ starts,
+                          const int* __restrict__ members, const int* __restrict__ gsize, int N, int Y,
+                          double* __restrict__ sums, unsigned* __restrict__ done, double* __restrict__ errk,
+                          double beta_obj, double beta_probe, double* __restrict__ betas,
+                          double* __restrict__ err_total) {
   pdl_enter();
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int k = blockIdx.y;
   const int G = *gsize;
-  double m1 = 0, m4 = 0;
-  for (int k = 0; k < G; ++k) {
-    m1 += sums[k * 6 + 0];
-    m4 += sums[k * 6 + 1];
+  if (k < G) lsq_window_sums(chi, objp, probe, pstride, pum, S, pobj, maxIllum, delta_p, starts, members, G, k, N, Y,
+                             sums);
+  // the last block to finish solves the group on the completed sums (no separate one-thread launch)
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x * gridDim.y - 1;
   }
-  m1 = 0.1 * m1 / G;
-  m4 = 0.1 * m4 / G;
-  double bor = 0, boi = 0, bpr = 0, bpi = 0, e = 0;
-  for (int k = 0; k < G; ++k) {
-    const double A11 = sums[k * 6 + 0] + m1, A22 = sums[k * 6 + 1] + m4;
-    const double cr = sums[k * 6 + 2], ci = sums[k * 6 + 3];  // A12 = c, A21 = conj(c)
-    const double b1 = sums[k * 6 + 4], b2 = sums[k * 6 + 5];
-    const double det = A11 * A22 - (cr * cr + ci * ci);      // real for a Hermitian 2x2
-    // x0 = (b1 A22 - c b2)/det, x1 = (A11 b2 - conj(c) b1)/det
-    bor += (b1 * A22 - cr * b2) / det;
-    boi += (-ci * b2) / det;
-    bpr += (A11 * b2 - cr * b1) / det;
-    bpi += (ci * b1) / det;
-    e += sqrt(errk[k] / (double(N) * N));
-    for (int m = 0; m < 6; ++m) sums[k * 6 + m] = 0.0;
-    errk[k] = 0.0;
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    *done = 0u;
+    mls_solve_group(sums, errk, G, N, beta_obj, beta_probe, betas, err_total);
   }
-  betas[0] = beta_obj * bor / G;
-  betas[1] = beta_obj * boi / G;
-  betas[2] = beta_probe * bpr / G;
-  betas[3] = beta_probe * bpi / G;
-  *err_total += e;
 }
 
 __global__ void k_mls_update_object(float2* __restrict__ obj, float2* __restrict__ S, const float* __restrict__ pobj,
@@ -353,7 +373,7 @@ cudaError_t mls_iteration(const MlsBuffers& b, int ngroups, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-int mls_launches_per_iteration(int ngroups) { return 5 + ngroups * 11; }
+int mls_launches_per_iteration(int ngroups) { return 5 + ngroups * 10; }
 
 cudaError_t mls_group_boxes(const int2* starts, const int* members, const int* gsize, int ngroups, int Gmax, int N,
                             int* bbox, cudaStream_t st) {
@@ -373,16 +393,16 @@ cudaError_t mls_lsq(const MlsBuffers& b, const float2* probe, size_t pstride, co
   const int NN = b.N * b.N;
   dim3 grid((NN + 255) / 256 > 64 ? 64 : (NN + 255) / 256, b.Gmax);
   launch_pdl(k_mls_lsq, grid, 256, 0, st, b.psi, b.objp, probe, pstride, b.pum, b.S, b.pobj, b.maxIllum, b.delta_p, b.starts,
-                                  members, gsize, b.N, b.Y, b.sums);
+                                  members, gsize, b.N, b.Y, b.sums, b.lsq_done, b.errk, b.beta_obj, b.beta_probe, b.betas,
+                                  b.err);
   return cudaGetLastError();
 }
 
-// 2x2 solves, object update over the group box, probe update.
+// Object update over the group box, probe update (the 2x2 solves ran at the end of mls_lsq).
 cudaError_t mls_solve_update(const MlsBuffers& b, const int* members, const int* gsize, const int* bbox,
                              int clear_pum, cudaStream_t st) {
   (void)members;
   const int NN = b.N * b.N;
-  launch_pdl(k_mls_solve, 1, 32, 0, st, b.sums, b.errk, gsize, b.N, b.beta_obj, b.beta_probe, b.betas, b.err);
   launch_pdl(k_mls_update_object, grid_for(size_t(2) * NN), 256, 0, st, b.obj, b.S, b.pobj, b.maxIllum, b.delta_p, b.betas,
                                                                  bbox, b.Y);
   launch_pdl(k_mls_update_probe, grid_for(NN), 256, 0, st, b.probe, b.pum, b.betas, gsize, NN, clear_pum);

@@ -23,6 +23,7 @@ struct MlsBuffers {
   const int* gsize;       // ngroups
   const int* bbox;        // ngroups x 4 (x0, y0, nx, ny)
   double* sums;           // Gmax x 6 LSQ sums
+  unsigned* lsq_done;     // blocks of the LSQ launch that have finished (the last one solves and resets it)
   double* errk;           // Gmax Fourier-error sums
   double* betas;          // 4: group-mean object step (re, im), probe step (re, im)
   double* err;            // iteration error accumulator

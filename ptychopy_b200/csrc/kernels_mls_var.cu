@@ -74,10 +74,7 @@ __global__ void k_var_recentre(float* __restrict__ pos, const float* __restrict_
     s[3] += pos_o[2 * i + 1];
   }
   __shared__ float d[2];
-  for (int m = 0; m < 4; ++m) {
-    s[m] = block_reduce_sum(s[m]);
-    __syncthreads();
-  }
+  block_reduce_sum_n(s);
   if (threadIdx.x == 0) {
     d[0] = float(s[0] / P) - float(s[2] / P);
     d[1] = float(s[1] / P) - float(s[3] / P);
@@ -256,11 +253,9 @@ __global__ void k_var_possums(const float2* __restrict__ aux, const float2* __re
     v[2] += double(gy.x) * gy.x + double(gy.y) * gy.y;
     v[3] += double(c.x) * gy.x + double(c.y) * gy.y;
   }
-  for (int m = 0; m < 4; ++m) {
-    const double r = block_reduce_sum(v[m]);
-    if (threadIdx.x == 0) atomicAdd(&out[4 * k + m], r);
-    __syncthreads();
-  }
+  block_reduce_sum_n(v);
+  if (threadIdx.x == 0)
+    for (int m = 0; m < 4; ++m) atomicAdd(&out[4 * k + m], v[m]);
 }
 
 // Position updates (one thread): shift = clamp(num/den, +-0.2); the column-gradient shift moves x (the row
@@ -384,11 +379,9 @@ __global__ void k_var_evosums(const float2* __restrict__ objp, const float2* __r
     v[2] += double(b.x) * b.x + double(b.y) * b.y;
     v[3] += double(c.x) * b.x + double(c.y) * b.y;
   }
-  for (int m = 0; m < 4; ++m) {
-    const double r = block_reduce_sum(v[m]);
-    if (threadIdx.x == 0) atomicAdd(&out[4 * k + m], r);
-    __syncthreads();
-  }
+  block_reduce_sum_n(v);
+  if (threadIdx.x == 0)
+    for (int m = 0; m < 4; ++m) atomicAdd(&out[4 * k + m], v[m]);
 }
 
 // evo1 += mean num / (mean den + 0.1 group mean of mean den); evo0 += 0.1 sum num / sum den (one thread);
@@ -742,9 +735,9 @@ struct EpiPosSums {
     return v;
   }
   __device__ void finish(int b) {
-    const double r0 = block_reduce_sum(s0);
-    __syncthreads();
-    const double r1 = block_reduce_sum(s1);
+    double r[2] = {s0, s1};
+    block_reduce_sum_n(r);
+    const double r0 = r[0], r1 = r[1];
     const int k = b < Gmax ? b : b - Gmax, m = b < Gmax ? 0 : 2;
     if (threadIdx.x == 0 && k < *gsize) {
       atomicAdd(&out[4 * k + m], r0);
@@ -891,8 +884,8 @@ int mls_var_launches_per_iteration(int ngroups, unsigned flags, int K, bool tc, 
   if (flags & MLS_REMOVE) pre += 4;
   // per group: six 2-D transforms of two passes; FP32 fuses exit, both phase ramps, psi, the one-mode modulus and
   // the directions into them (one mode up to 256^2: all twelve passes in one cluster launch), the tensor-core path
-  // runs them as 6 kernels (the modulus only for one mode); then pum, lsq, solve and the two updates
-  int per = (mls_var_fused(N, K, tc) && !(flags & MLS_SEPARATE) ? 1 : 12) + 5 + (tc ? 6 + (K == 1 ? 1 : 0) : 0);
+  // runs them as 6 kernels (the modulus only for one mode); then pum, lsq with the solves, and the two updates
+  int per = (mls_var_fused(N, K, tc) && !(flags & MLS_SEPARATE) ? 1 : 12) + 4 + (tc ? 6 + (K == 1 ? 1 : 0) : 0);
   if (flags & MLS_POSSEARCH) per += tc ? 2 + 1 + 2 + 1 + 1 : 2 + 2 + 1;
   if (flags & MLS_VARUPD) per += 5;
   // other modes: exit waves, forward and inverse 2-D transforms, the modal modulus, one update each

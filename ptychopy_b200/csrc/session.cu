@@ -1009,7 +1009,7 @@ void init_mls(pty_session* s) {
     check_cuda(cudaMallocHost(&t.host, sizeof(int) * ml->table_ints), "pinned group tables");
     check_cuda(cudaEventCreateWithFlags(&t.copied, cudaEventDisableTiming), "event");
   }
-  ml->sums.alloc(sizeof(double) * 6 * ml->Gmax, "LSQ sums");
+  ml->sums.alloc(sizeof(double) * (6 * ml->Gmax + 1), "LSQ sums");  // + the LSQ launch's block counter
   ml->errk.alloc(sizeof(double) * ml->Gmax, "errors");
   ml->betas.alloc(sizeof(double) * 4, "steps");
   ml->err.alloc(sizeof(double), "error");
@@ -1035,6 +1035,7 @@ MlsBuffers mls_buffers(pty_session* s, int parity) {
   b.gsize = b.members + size_t(ml->ng) * ml->Gmax;
   b.bbox = b.gsize + ml->ng;
   b.sums = ml->sums.as<double>();
+  b.lsq_done = reinterpret_cast<unsigned*>(b.sums + 6 * ml->Gmax);
   b.errk = ml->errk.as<double>();
   b.betas = ml->betas.as<double>();
   b.err = ml->err.as<double>();
