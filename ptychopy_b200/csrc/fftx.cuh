@@ -119,12 +119,20 @@ __device__ __forceinline__ void fftx2_cluster(float2* work, float2* out, int b, 
   cluster_sync_acqrel();
 }
 
+// The shared-memory size and the opt-in to 16-CTA clusters of a cluster kernel, on the current device (function
+// attributes are per device: set them on every device that launches the kernel)
+template <class Kern>
+inline cudaError_t set_cluster_attributes(Kern* kernel, size_t smem) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  return e;
+}
+
 // Largest cluster of `kernel` (at most one CTA per row block of a plane and at most 16, the largest size, opted
-// into) of which one fits on the device; 0 if none.  Sets the kernel's shared-memory and cluster attributes.
+// into) of which one fits on the device; 0 if none.  Sets the kernel's attributes on the current device.
 template <class Kern>
 inline int fit_cluster(Kern* kernel, int row_blocks, int threads, size_t smem) {
-  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess ||
-      cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+  if (set_cluster_attributes(kernel, smem) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }

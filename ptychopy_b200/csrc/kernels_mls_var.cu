@@ -813,16 +813,27 @@ int grid_n(size_t n, int cap = 1184) {
 // too: 16 scans of the batched workload measured 163.5 K patterns/s with the cluster launches, 193.3 K without.
 bool mls_var_fused(int N, int K, bool tc) { return !tc && K == 1 && N <= 256; }
 
+// Per session, on its device: the cluster size is chosen once per process, the kernel's attributes are set on every
+// device that runs it
 cudaError_t mls_var_prepare(int N) {
   int C = 0;
+  cudaError_t e = cudaErrorInvalidValue;
+#define PTY_FRONT(L)                                                          \
+  case L:                                                                     \
+    C = front_cluster<L>();                                                   \
+    e = set_cluster_attributes(k_var_front<L>, rows_smem_bytes<L>());         \
+    break;
   switch (N) {
-    case 32: C = front_cluster<32>(); break;
-    case 64: C = front_cluster<64>(); break;
-    case 128: C = front_cluster<128>(); break;
-    case 256: C = front_cluster<256>(); break;
-    default: break;
+    PTY_FRONT(32)
+    PTY_FRONT(64)
+    PTY_FRONT(128)
+    PTY_FRONT(256)
+    default:
+      break;
   }
+#undef PTY_FRONT
   cudaGetLastError();
+  if (e != cudaSuccess) return e;
   return C >= 1 ? cudaSuccess : cudaErrorInvalidConfiguration;
 }
 
