@@ -84,13 +84,7 @@ void DeviceBuf::alloc(size_t n, const char* what) {
   need_device_index(d);
   size_t got = 0;
   void* q = cache_take(d, n, &got);
-  if (q) {
-    // a fresh cudaMalloc block reads as zeros (the driver clears new pages); a recycled one is cleared to match,
-    // complete before return (the memset runs on the legacy stream, which the sessions' non-blocking streams do not
-    // order against)
-    check_cuda(cudaMemset(q, 0, n), what);
-    check_cuda(cudaDeviceSynchronize(), what);
-  } else {
+  if (!q) {
     cudaError_t e = cudaMalloc(&q, n);
     if (e == cudaErrorMemoryAllocation) {  // give the cache back and try once more
       cudaGetLastError();
@@ -100,6 +94,11 @@ void DeviceBuf::alloc(size_t n, const char* what) {
     check_cuda(e, what);
     got = n;
   }
+  // every buffer starts at zero (accumulators, counters and padding rely on it), whether recycled or fresh (cudaMalloc
+  // does not promise cleared memory: pages this process freed may come back as they were); complete before return,
+  // as the memset runs on the legacy stream, which the sessions' non-blocking streams do not order against
+  check_cuda(cudaMemset(q, 0, n), what);
+  check_cuda(cudaDeviceSynchronize(), what);
   p = q;
   bytes = n;
   cap = got;
