@@ -28,6 +28,8 @@ def _scans(oracle):
 
 
 def test_batch_matches_individual_runs(oracle):
+    # the lone MLs sessions run each group's transforms as one cluster launch per window, the batched ones as
+    # separate passes, so this also compares the two forms of the MLs group
     make = _scans(oracle)
     alone = make()
     for s in alone:
