@@ -256,3 +256,31 @@ def test_list_mesh_padding_joins_extent(oracle):
     assert X == int(np.ceil(np.float32(2e-6 / dx_s) + 64))
     # shifted by the padding's minimum (0), not by the list's own minimum
     assert abs(pos[:, 0].min() - 1e-6 / dx_s) < 1e-3 and abs(pos[:, 1].min() - 1e-6 / dx_s) < 1e-3
+
+
+def test_mls_default_path_position_steps_are_clamped(oracle):
+    """Each iteration moves every position by one common recentring shift (positions minus their mean drift from
+    the originals) plus its own least-squares step, clamped to 0.2 px per axis: per axis, the moves of one iteration
+    spread over at most 0.4 px.  The data are made at positions up to 1 px away from the nominal ones, so the search
+    takes steps near the clamp."""
+    from gpu_helpers import mls_dataset, shifted_probe, subpixel_shifts
+
+    N = 32
+    d = mls_dataset(oracle, N=N, nx=5, shifted=True, pert=0.0)
+    sx, sy = subpixel_shifts(d["raw"], d["X"], d["Y"], N)
+    ex, ey = np.random.default_rng(7).uniform(-1.0, 1.0, (2, len(sx)))
+    o, p = d["obj"].astype(np.complex128), np.asarray(d["probe"], np.complex128)
+    intens = np.stack([np.abs(np.fft.fft2(shifted_probe(p, sx[k] + ex[k], sy[k] + ey[k]) * o[r:r + N, c:c + N])) ** 2
+                       for k, (r, c) in enumerate(d["starts"])]).astype(np.float32)
+    m = oracle.OracleMls(d["raw"], intens, d["probe"], obj=d["obj"], variable=1, PPS=2)
+    prev = m.variable_state()[3].astype(np.float64)
+    spreads = []
+    for _ in range(5):
+        m.step()
+        cur = m.variable_state()[3].astype(np.float64)
+        step = cur - prev
+        spreads.append(float((step.max(axis=0) - step.min(axis=0)).max()))
+        prev = cur
+    assert spreads[0] == 0.0, spreads  # no search before iteration PPS
+    assert max(spreads) <= 0.4 + 1e-4, spreads
+    assert max(spreads) > 0.2, spreads  # the search takes steps of the clamp's order
