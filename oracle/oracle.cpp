@@ -5,11 +5,13 @@
 // tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker.  The product (libptychopy_b200)
 // never links, loads or calls anything in this directory.
 //
-// Parity status: UNPINNED by the reference.  The reference ships no tests, golden vectors or known-answer
-// fixtures, and its CUDA sources do not build with CUDA 12.9 (removed texture-reference API, missing
-// CUDA-samples headers), so this restatement cannot be checked against reference outputs.  It is pinned instead
-// by (a) numpy.fft for the FFT convention, (b) hand-derived known-answer cases in tests/, and (c) committed
-// golden fixtures generated from this file (tests/golden/make_golden.py).
+// Parity status: pinned to the reference's own device code.  oracle/ref_build.py compiles the reference's
+// hot-path device functions unchanged (DM callbacks, ePIE modulus / object / probe updates and error metric, the
+// texture gather, the forward model, the MLs step-length terms and modulus factor, the raster mesh) and
+// tests/test_gpu_refstages.py runs them on the GPU against this file's stages and whole iterations (DM and ePIE
+// to FP32 round-off; the raster mesh and the texture filter weights bit for bit).  The reference ships no golden
+// vectors; numpy.fft, hand-derived known answers (tests/test_oracle.py) and committed fixtures generated from this
+// file (tests/golden/make_golden.py) pin the rest.
 //
 // Numerics: templated on the real type.  `double` is the FP64 oracle; `float` + std::thread is the multithreaded
 // FP32 CPU baseline that bench.py times.  Scan geometry is computed in FP32 exactly as the reference does it
@@ -183,6 +185,24 @@ template <typename R> inline cx<R> constrain_phase(cx<R> v) {
   R mag = std::abs(v), arg = std::atan2(v.imag(), v.real());
   arg = arg <= R(0) ? arg : R(0);
   return cx<R>(mag * std::cos(arg), mag * std::sin(arg));
+}
+
+// MLs modulus factor (d_modulus_amplitude with R_offset = 1, src/DiffractionsKernels.cu:127-137, called from
+// Diffractions::modulus_constraint, src/Diffractions.cpp:281-310): A / (|Psi| + 1e-9) - 1.
+template <typename R> inline R mls_modulus_factor(R A, R ap) { return A / (ap + R(1e-9)) - R(1); }
+
+// Per-pixel terms of the MLs 2x2 step-length system (d_get_optimal_step_lsq, src/utilitiesKernels.cu:444-466):
+// dOP = oup * probe; AA1 = |dOP|^2 + lambda, AA2 = dOP conj(dPO), AA4 = |dPO|^2 + lambda, Atb1 = Re(conj(dOP) chi),
+// Atb2 = Re(conj(dPO) chi).
+template <typename R>
+inline void mls_lsq_terms(cx<R> chi, cx<R> oup, cx<R> dPO, cx<R> probe, R lam, R& a1, cx<R>& a2, R& a4, R& b1,
+                          R& b2) {
+  const cx<R> dOP = oup * probe;
+  a1 = std::norm(dOP) + lam;
+  a2 = dOP * std::conj(dPO);
+  a4 = std::norm(dPO) + lam;
+  b1 = (std::conj(dOP) * chi).real();
+  b2 = (std::conj(dPO) * chi).real();
 }
 
 template <typename R> inline cx<R> modulus_phase(cx<R> psi, R amp) {
@@ -932,7 +952,7 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
         for (int m = 1; m < s.K; ++m) a2 += std::norm(chm[m - 1][k][p]);
         const R ap = s.K > 1 ? std::sqrt(a2) : std::abs(chi[k][p]);
         e += double(A[p] - ap) * double(A[p] - ap) * 0.25;
-        const R rr = A[p] / (ap + R(1e-9)) - R(1);
+        const R rr = mls_modulus_factor(A[p], ap);
         chi[k][p] *= rr;
         for (int m = 1; m < s.K; ++m) chm[m - 1][k][p] *= rr;
       }
@@ -981,12 +1001,14 @@ template <typename R> double mls_iteration(MlsState<R>& s, uint64_t& rng, bool w
         for (int y = 0; y < N; ++y) {
           const size_t p = size_t(x) * N + y, o = size_t(s.geo.r0[j] + x) * Y + (s.geo.c0[j] + y);
           const cx<R> oup = S[o] / (s.pobj[o] + dmax);
-          const cx<R> dOP = oup * vp[k][p], dPO = pum[p] * op[k][p];
-          s1 += double(std::norm(dOP) + lam);
-          s4 += double(std::norm(dPO) + lam);
-          s2 += cx<double>(dOP * std::conj(dPO));
-          t1 += double((std::conj(dOP) * chi[k][p]).real());
-          t2 += double((std::conj(dPO) * chi[k][p]).real());
+          R a1p, a4p, b1p, b2p;
+          cx<R> a2p;
+          mls_lsq_terms(chi[k][p], oup, pum[p] * op[k][p], vp[k][p], lam, a1p, a2p, a4p, b1p, b2p);
+          s1 += double(a1p);
+          s4 += double(a4p);
+          s2 += cx<double>(a2p);
+          t1 += double(b1p);
+          t2 += double(b2p);
         }
       a1[k] = s1; a4[k] = s4; a2[k] = s2; b1[k] = t1; b2[k] = t2;
     }
@@ -1141,6 +1163,25 @@ void mesh_jitter(uint64_t seed, size_t n, unsigned radius, std::vector<float>& o
 // ============================================================================================================
 // C ABI of the oracle (ctypes from tests/ and bench.py).  Complex arrays are interleaved (re, im) doubles.
 // ============================================================================================================
+// Raw pixel positions of an nx x ny raster before the -min shift (d_generateMesh<1>, src/ScanMeshKernels.cu:46-93,
+// launched at :153-160 with one_over_dxs = (float)(1.0/dx_s)): ((i - (nx-1)/2) * stepx) * one_over_dxs in float,
+// index i*ny + j.
+static void cartesian_raw(int nx, int ny, double stepx, double stepy, double dx_s, int mirrorX, int mirrorY, float* raw) {
+  const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      volatile float mi = float(i), md = float(nx - 1) * 0.5f;
+      volatile float dxv = mirrorX ? (md - mi) : (mi - md);
+      volatile float vx = dxv * sx;
+      volatile float mj = float(j), mdy = float(ny - 1) * 0.5f;
+      volatile float dyv = mirrorY ? (mdy - mj) : (mj - mdy);
+      volatile float vy = dyv * sy;
+      volatile float px = vx * inv, py = vy * inv;
+      raw[2 * (size_t(i) * ny + j)] = px;
+      raw[2 * (size_t(i) * ny + j) + 1] = py;
+    }
+}
+
 extern "C" {
 
 int orc_version() { return 1; }
@@ -1174,21 +1215,8 @@ int orc_cartesian_mesh_j(int nx, int ny, double stepx, double stepy, double lamb
                          int mirrorX, int mirrorY, int flip, unsigned jitter, uint64_t seed, float* pos,
                          int* objXY) {
   if (nx < 1 || ny < 1 || N < 1) return -1;
-  const double dx_s = sample_pixel(lambda, z, dx_d, N);
-  const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
   std::vector<float> raw(2 * size_t(nx) * ny);
-  for (int i = 0; i < nx; ++i)
-    for (int j = 0; j < ny; ++j) {
-      volatile float mi = float(i), md = float(nx - 1) * 0.5f;
-      volatile float dxv = mirrorX ? (md - mi) : (mi - md);
-      volatile float vx = dxv * sx;
-      volatile float mj = float(j), mdy = float(ny - 1) * 0.5f;
-      volatile float dyv = mirrorY ? (mdy - mj) : (mj - mdy);
-      volatile float vy = dyv * sy;
-      volatile float px = vx * inv, py = vy * inv;
-      raw[2 * (size_t(i) * ny + j)] = px;
-      raw[2 * (size_t(i) * ny + j) + 1] = py;
-    }
+  cartesian_raw(nx, ny, stepx, stepy, sample_pixel(lambda, z, dx_d, N), mirrorX, mirrorY, raw.data());
   std::vector<float> jit;
   mesh_jitter(seed, size_t(nx) * ny, jitter, jit);
   for (size_t k = 0; k < raw.size(); ++k) {
@@ -1199,6 +1227,14 @@ int orc_cartesian_mesh_j(int nx, int ny, double stepx, double stepy, double lamb
   finish_mesh(raw, nx * ny, false, N, flip != 0, m);
   std::memcpy(pos, m.pos.data(), m.pos.size() * sizeof(float));
   objXY[0] = m.X; objXY[1] = m.Y;
+  return 0;
+}
+
+// The raw raster before the -min shift (2*nx*ny floats, raw[2*(i*ny+j)] = x, +1 = y).
+int orc_cartesian_mesh_raw(int nx, int ny, double stepx, double stepy, double lambda, double z, double dx_d, int N,
+                           int mirrorX, int mirrorY, float* raw) {
+  if (nx < 1 || ny < 1 || N < 1) return -1;
+  cartesian_raw(nx, ny, stepx, stepy, sample_pixel(lambda, z, dx_d, N), mirrorX, mirrorY, raw);
   return 0;
 }
 
@@ -1539,6 +1575,24 @@ int orc_mls_get_var(void* hp, double* E, double* evo0, double* evo1, float* pos)
 }
 
 void orc_mls_destroy(void* hp) { delete static_cast<OrcMls*>(hp); }
+
+// Stage entry points of the MLs helpers (n pixels; complex arrays interleaved re, im doubles).
+int orc_mls_modulus_factor(const double* A, const double* ap, int n, double* out) {
+  for (int i = 0; i < n; ++i) out[i] = mls_modulus_factor(A[i], ap[i]);
+  return 0;
+}
+
+int orc_mls_lsq_terms(const double* chi, const double* oup, const double* dPO, const double* probe, double lam, int n,
+                      double* a1, double* a2, double* a4, double* b1, double* b2) {
+  auto c = [](const double* v, int i) { return cx<double>(v[2 * i], v[2 * i + 1]); };
+  for (int i = 0; i < n; ++i) {
+    cx<double> t;
+    mls_lsq_terms(c(chi, i), c(oup, i), c(dPO, i), c(probe, i), lam, a1[i], t, a4[i], b1[i], b2[i]);
+    a2[2 * i] = t.real();
+    a2[2 * i + 1] = t.imag();
+  }
+  return 0;
+}
 
 }  // extern "C"
 

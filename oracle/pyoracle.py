@@ -1,8 +1,9 @@
 """ctypes wrapper of the oracle (oracle/oracle.cpp).  TEST INFRASTRUCTURE ONLY: imported by tests/,
 __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker; never by the product.
 
-Parity status: unpinned by the reference (no reference golden vectors exist and the reference does not build);
-pinned to numpy.fft, hand-derived known answers and the committed fixtures under tests/golden/.
+Parity status: pinned to the reference's own device functions, compiled unchanged by oracle/ref_build.py and
+compared stage by stage and iteration by iteration in tests/test_gpu_refstages.py; also pinned to numpy.fft,
+hand-derived known answers and the committed fixtures under tests/golden/.
 """
 import ctypes
 import os
@@ -61,6 +62,9 @@ def lib():
             "orc_mls_step": ([vp, ctypes.POINTER(d)], i),
             "orc_mls_get": ([vp, vp, vp, vp], i),
             "orc_mls_destroy": ([vp], None),
+            "orc_cartesian_mesh_raw": ([i, i, d, d, d, d, d, i, i, i, vp], i),
+            "orc_mls_modulus_factor": ([vp, vp, i, vp], i),
+            "orc_mls_lsq_terms": ([vp, vp, vp, vp, d, i, vp, vp, vp, vp, vp], i),
         }
         for name, (a, r) in sig.items():
             fn = getattr(L, name)
@@ -90,6 +94,32 @@ def cartesian_mesh(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX=0, mirrorY=0
     assert lib().orc_cartesian_mesh_j(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX, mirrorY, flip, jitter, seed,
                                       _p(pos), _p(xy)) == 0
     return pos, int(xy[0]), int(xy[1])
+
+
+def cartesian_mesh_raw(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX=0, mirrorY=0):
+    """Raw raster positions (nx*ny, 2) float32 in pixels, before the -min shift."""
+    raw = np.zeros((nx * ny, 2), np.float32)
+    assert lib().orc_cartesian_mesh_raw(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX, mirrorY, _p(raw)) == 0
+    return raw
+
+
+def mls_modulus_factor(A, ap):
+    """A / (|Psi| + 1e-9) - 1 per pixel (the oracle's MLs modulus helper)."""
+    A = np.ascontiguousarray(A, np.float64).ravel()
+    ap = np.ascontiguousarray(ap, np.float64).ravel()
+    out = np.zeros_like(A)
+    assert lib().orc_mls_modulus_factor(_p(A), _p(ap), A.size, _p(out)) == 0
+    return out
+
+
+def mls_lsq_terms(chi, oup, dPO, probe, lam):
+    """Per-pixel (AA1, AA2, AA4, Atb1, Atb2) of the MLs step-length system (the oracle's helper)."""
+    c = [np.ascontiguousarray(v, np.complex128).ravel() for v in (chi, oup, dPO, probe)]
+    n = c[0].size
+    a1, a4, b1, b2 = (np.zeros(n) for _ in range(4))
+    a2 = np.zeros(n, np.complex128)
+    assert lib().orc_mls_lsq_terms(*(_p(v) for v in c), lam, n, _p(a1), _p(a2), _p(a4), _p(b1), _p(b2)) == 0
+    return a1, a2, a4, b1, b2
 
 
 def list_mesh(xy_m, lambd, z, dx_d, N, flip=0, jitter=0, seed=0):
