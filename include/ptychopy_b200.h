@@ -306,14 +306,19 @@ int pty_fft2_tc(void* data, void* work, int batch, int N, int inverse, int* err,
  * allocation).  For callers that cannot call cudaMalloc: hosts that hand the library only buffers they allocated
  * up front and forbid allocation afterwards, such as an acquisition service that owns all device memory of the
  * GPU for the length of a run.  The work buffer and twiddle tables live in a static device array inside this
- * library (8 MiB plus 8 KiB, held on every GPU that loads the library until the process exits), so the call
- * allocates nothing; the caller passes only the data, transformed in place (batch x N x N complex64,
- * N in {32, 64, 128, 256, 512}).  Requests with batch*N*N*8 > 8 MiB are rejected with PTY_ERR_INVALID.
- * The first call on a device sets that device's scratch up (resolves its address, fills the twiddles with a
- * synchronous copy); make that first call before any stream capture.  The launch is asynchronous on
- * `cuda_stream`.  All calls on a device share the one scratch array, which keeps the last call's contents (it is
- * fully overwritten before it is read, so nothing needs clearing); calls that overlap on the GPU, e.g. on two
- * streams at once, race on it and must be serialised by the caller. */
+ * library (8 MiB plus 8 KiB), so the call allocates nothing; the caller passes only the data, transformed in place
+ * (batch x N x N complex64, N in {32, 64, 128, 256, 512}).  Requests with batch*N*N*8 > 8 MiB are rejected with
+ * PTY_ERR_INVALID.
+ * The static array occupies device memory from the moment the CUDA runtime loads this library's device code onto
+ * a GPU until the process exits.  With the runtime's default lazy loading that happens on the first call on that
+ * device (which also resolves the array's address and fills the twiddles with a synchronous copy), and each
+ * transform size's kernels are loaded on the first call with that size, so those first calls need free device
+ * memory (~8 MiB, then the code): make one call per size the host will use at start-up, before it claims the
+ * GPU's memory and before any stream capture (or run with CUDA_MODULE_LOADING=EAGER, which loads everything when
+ * the CUDA context is created).  Later calls allocate nothing.  The launch is asynchronous on `cuda_stream`.  All
+ * calls on a device share the one scratch array, which keeps the last call's contents (it is fully overwritten
+ * before it is read, so nothing needs clearing); calls that overlap on the GPU, e.g. on two streams at once, race
+ * on it and must be serialised by the caller. */
 int pty_fft2_dev_noalloc(void* data_dev, int batch, int N, int inverse, void* cuda_stream);
 
 #ifdef __cplusplus

@@ -91,6 +91,63 @@ template <typename R> void fft2(const Fft1<R>& f, cx<R>* a, bool inverse, std::v
   for (int c = 0; c < N; ++c) f.run(a + c, N, inverse, scratch.data());
 }
 
+// The same transform with the rows, then the columns, split over nthreads threads (same arithmetic per line, so
+// the result is identical to fft2).
+template <typename R> void fft2_mt(const Fft1<R>& f, cx<R>* a, bool inverse, int nthreads) {
+  const int N = f.L;
+  if (nthreads <= 1 || N < 256) {
+    std::vector<cx<R>> scr;
+    fft2(f, a, inverse, scr);
+    return;
+  }
+  for (int pass = 0; pass < 2; ++pass) {
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; ++t)
+      th.emplace_back([&, t, pass] {
+        std::vector<cx<R>> scr(N);
+        for (int l = t; l < N; l += nthreads) {
+          if (pass == 0)
+            f.run(a + size_t(l) * N, 1, inverse, scr.data());
+          else
+            f.run(a + l, N, inverse, scr.data());
+        }
+      });
+    for (auto& x : th) x.join();
+  }
+}
+
+// K stacked N x N transforms: one thread per mode when there are several, else the rows / columns of the one
+// transform split over the threads.  Each line sees the same arithmetic as fft2.
+template <typename R> void fft2_modes(const Fft1<R>& f, cx<R>* a, int K, bool inverse, int nthreads) {
+  const size_t NN = size_t(f.L) * f.L;
+  if (K == 1 || nthreads <= 1) {
+    for (int k = 0; k < K; ++k) fft2_mt(f, a + k * NN, inverse, nthreads);
+    return;
+  }
+  const int T = std::min(K, nthreads);
+  std::vector<std::thread> th;
+  for (int t = 0; t < T; ++t)
+    th.emplace_back([&, t] {
+      std::vector<cx<R>> scr;
+      for (int k = t; k < K; k += T) fft2(f, a + k * NN, inverse, scr);
+    });
+  for (auto& x : th) x.join();
+}
+
+// fn(i) for i in [0, n), split into contiguous chunks over nthreads threads (serial when nthreads <= 1).
+template <typename F> void parallel_rows(int n, int nthreads, F&& fn) {
+  if (nthreads <= 1 || n < 2 * nthreads) {
+    for (int i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 0; t < nthreads; ++t)
+    th.emplace_back([&, t] {
+      for (int i = int(int64_t(n) * t / nthreads); i < int(int64_t(n) * (t + 1) / nthreads); ++i) fn(i);
+    });
+  for (auto& x : th) x.join();
+}
+
 // ---------------------------------------------------------------- geometry (FP32 like the reference)
 // src/Parameters.h:175-179 returns real_t (float): dx_s = (float)(lambda*z/(N*dx_d)).
 double sample_pixel(double lambda, double z, double dx_d, int N) {
@@ -320,7 +377,7 @@ template <typename R> void begin_modal(State<R>& s) {
 // ---------------------------------------------------------------- ePIE iteration (src/ePIE.cpp:65-129)
 template <typename R>
 R epie_iteration(State<R>& s, const R* amp, const float* pos, const R* sqsum, const Flags& fl, int iter,
-                 uint64_t& rng, int* status) {
+                 uint64_t& rng, int* status, int nthreads = 1) {
   const int N = s.N, K = s.K, P = s.P;
   const size_t NN = size_t(N) * N;
   const bool pc = iter <= fl.phaseConstraint, up = iter >= fl.updateProbe, um = iter >= fl.updateModes;
@@ -329,7 +386,7 @@ R epie_iteration(State<R>& s, const R* amp, const float* pos, const R* sqsum, co
   std::vector<int> order(P);
   visiting_order(rng, P, order.data());
   Fft1<R> f(N);
-  std::vector<cx<R>> scr, patch(NN), psiOld(size_t(Ka) * NN), Psi(size_t(Ka) * NN), psi(size_t(Ka) * NN);
+  std::vector<cx<R>> patch(NN), psiOld(size_t(Ka) * NN), Psi(size_t(Ka) * NN), psi(size_t(Ka) * NN);
   const R nrm = R(1.0 / double(N * N));
   double err = 0;
   for (int step = 0; step < P; ++step) {
@@ -339,10 +396,8 @@ R epie_iteration(State<R>& s, const R* amp, const float* pos, const R* sqsum, co
     extract_patch(s.O.data(), s.X, s.Y, qx, qy, N, patch.data());
     for (int k = Ka - 1; k >= 0; --k)
       for (size_t p = 0; p < NN; ++p) psiOld[k * NN + p] = patch[p] * s.Pr[k * NN + p];
-    for (int k = 0; k < Ka; ++k) {
-      std::copy(&psiOld[k * NN], &psiOld[k * NN] + NN, &Psi[k * NN]);
-      fft2(f, &Psi[k * NN], false, scr);
-    }
+    for (int k = 0; k < Ka; ++k) std::copy(&psiOld[k * NN], &psiOld[k * NN] + NN, &Psi[k * NN]);
+    fft2_modes(f, Psi.data(), Ka, false, nthreads);
     const R* A = amp + size_t(i) * NN;
     if (Ka == 1) {
       for (size_t p = 0; p < NN; ++p) psi[p] = modulus_phase(Psi[p], A[p]) * nrm;
@@ -364,11 +419,11 @@ R epie_iteration(State<R>& s, const R* amp, const float* pos, const R* sqsum, co
       }
       err += (e / Ka) / double(sqsum[i]);
     }
-    for (int k = 0; k < Ka; ++k) fft2(f, &psi[k * NN], true, scr);
+    fft2_modes(f, psi.data(), Ka, true, nthreads);
     const int ox = int(std::round(qx)), oy = int(std::round(qy));
     // Object update (d_updateObjectArray[M], src/SampleKernels.cu:244-294), c = 1/probeMax.
     const R cO = R(1.0 / double(s.probeMax));
-    for (int r = 0; r < N; ++r)
+    parallel_rows(N, nthreads, [&](int r) {
       for (int c = 0; c < N; ++c) {
         size_t p = size_t(r) * N + c, o = size_t(r + ox) * s.Y + (c + oy);
         cx<R> inc(0, 0);
@@ -379,10 +434,11 @@ R epie_iteration(State<R>& s, const R* amp, const float* pos, const R* sqsum, co
         s.O[o] = v;
         s.Ocache[o] = mag * mag;
       }
+    });
     s.objMax = *std::max_element(s.Ocache.begin(), s.Ocache.end());
     if (up) {  // d_updateProbe[M] (src/ProbeKernels.cu:425-458), c = 1/objMax, uses the updated object
       const R cP = R(1.0 / double(s.objMax));
-      for (int r = 0; r < N; ++r)
+      parallel_rows(N, nthreads, [&](int r) {
         for (int c = 0; c < N; ++c) {
           size_t p = size_t(r) * N + c, o = size_t(r + ox) * s.Y + (c + oy);
           cx<R> oc = std::conj(s.O[o]);
@@ -393,6 +449,7 @@ R epie_iteration(State<R>& s, const R* amp, const float* pos, const R* sqsum, co
             s.Pcache[k * NN + p] = m * m;
           }
         }
+      });
       s.probeMax = probe_modal_max(s);
     }
   }
@@ -1364,7 +1421,7 @@ template <typename R> struct OrcSessionT : OrcBase {
     const int it = ++iter;
     double e = 0;
     if (algo == 0)
-      e = double(epie_iteration<R>(s, amp.data(), pos.data(), sq.data(), fl, it, rng, &status));
+      e = double(epie_iteration<R>(s, amp.data(), pos.data(), sq.data(), fl, it, rng, &status, nthreads));
     else
       dm_iteration<R>(s, d, amp.data(), pos.data(), fl, it, nthreads, reduce, reduce_user);
     if (err) *err = e;

@@ -2,7 +2,8 @@
 //
 // pty_fft2_dev needs a caller-provided work buffer and allocates its twiddle table with cudaMalloc.  This variant
 // allocates nothing: the work buffer and the twiddle tables of every supported size live in file-scope device
-// arrays below, which every GPU that loads the library holds until the process exits.
+// arrays below.  A GPU holds them from the moment the runtime loads this file's device code onto it (under the
+// default lazy module loading: the first call on that device) until the process exits.
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -103,8 +104,11 @@ extern "C" int pty_fft2_dev_noalloc(void* data_dev, int batch, int N, int invers
                                           " arrays of " + std::to_string(N) + "x" + std::to_string(N) + ")");
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+  if (e != cudaSuccess)
     return fail_with(PTY_ERR_CUDA, std::string("pty_fft2_dev_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices)
+    return fail_with(PTY_ERR_INVALID, "pty_fft2_dev_noalloc: device ordinal " + std::to_string(dev) +
+                                          " is above the " + std::to_string(kMaxDevices - 1) + " this entry supports");
   DeviceScratch* sc = nullptr;
   e = setup_device(dev, &sc);
   if (e != cudaSuccess)

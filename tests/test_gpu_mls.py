@@ -13,6 +13,10 @@ from gpu_helpers import dataset, gpu_session, mls_dataset
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-4
+# The error metric sums sqrt(sum (A - |Psi|)^2 / 4 / N^2) over the positions.  On these noise-free, model-consistent
+# data A and |Psi| agree to a few percent, so the FP32 residual A - |Psi| keeps ~5 of FP32's 7 digits: measured
+# engine-vs-FP64 differences are 4e-8 .. 4e-6 (32^2 .. 512^2).
+ERR_TOL = 1e-5
 
 
 def _pair(oracle, d, **params):
@@ -60,7 +64,8 @@ def test_mls_default_path_matches_oracle(oracle, N, nx, PPS):
         e = s.step()
         eo = o.step()
         pos = _check_default(s, o, f"iteration {it}")
-        assert abs(e - eo) <= 1e-3 * abs(eo), f"error, iteration {it}"
+        print(f"MLs default path N={N} iteration {it}: error metric rel diff {abs(e - eo) / abs(eo):.2e}")
+        assert abs(e - eo) <= ERR_TOL * abs(eo), f"error, iteration {it}"
         moved = np.abs(pos - d["raw"]).max()
         if it < PPS:
             assert moved == 0.0, "positions move only from PPS"
@@ -121,7 +126,8 @@ def test_mls_probe_modes_match_oracle(oracle, K):
         if it:
             e = s.step()
             eo = o.step()
-            assert abs(e - eo) <= 1e-3 * abs(eo), f"error, iteration {it}"
+            print(f"MLs K={K} iteration {it}: error metric rel diff {abs(e - eo) / abs(eo):.2e}")
+            assert abs(e - eo) <= ERR_TOL * abs(eo), f"error, iteration {it}"
         ob, pr, _ = o.state()
         gp = s.probe()
         assert gp.shape == (K, 64, 64)
@@ -159,9 +165,10 @@ def test_mls_matches_oracle(oracle, N, nx):
         e = s.step()
         eo = o.step()
         ob, pr, _ = o.state()
+        print(f"MLs core N={N} iteration {it}: error metric rel diff {abs(e - eo) / abs(eo):.2e}")
         assert rel_err(s.object(), ob) < TOL, f"object, iteration {it}"
         assert rel_err(s.probe(), pr) < TOL, f"probe, iteration {it}"
-        assert abs(e - eo) <= 1e-3 * abs(eo), f"error, iteration {it}"
+        assert abs(e - eo) <= ERR_TOL * abs(eo), f"error, iteration {it}"
 
 
 def test_mls_groups_of_several_and_delta_p(oracle):
