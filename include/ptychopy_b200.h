@@ -38,7 +38,8 @@ extern "C" {
 typedef struct pty_params {
   char jobID[128];
   char algorithm[8];      /* "ePIE", "DM" or "MLs" */
-  char fp[256];           /* data file pattern (file ingest is not part of this engine; must be empty) */
+  char fp[256];           /* data file pattern, '#' marking the file index conversion (e.g. "scan/d_#06d.bin");
+                             used by pty_init when no patterns were set: .bin (raw float32) or .csv files */
   int fs;
   char hdf5path[128];
   int dpf;
@@ -46,7 +47,7 @@ typedef struct pty_params {
   char probeGuess[256];   /* CSV probe guess file (reference format) or "" */
   char objectGuess[256];  /* CSV object guess file or "" */
   int size;               /* detector / probe size N */
-  int qx, qy, nx, ny;     /* file-ingest cropping (unused without file ingest) */
+  int qx, qy, nx, ny;     /* file ingest: crop centre (qx, qy) and raw pattern size nx x ny */
   int scanDimsx, scanDimsy;
   int spiralScan, flipScanAxis, mirror1stScanAxis, mirror2ndScanAxis;
   double stepx, stepy;    /* m */
@@ -288,6 +289,14 @@ int64_t pty_kernel_launches(const pty_session* s);
 const char* pty_last_error(void);
 
 /* ---- device-pointer operators (building blocks, used by the parity tests) ---------------------------- */
+
+/* The whole-mode ingest's preprocessing of `count` raw patterns (rows x cols float32, device) into size x size
+ * patterns (device): crop / zero-pad around the centre (qx, qy) unless the raw pattern is already size x size
+ * (h_symmetrizeDiffraction, src/DiffractionLoader.cpp:86-107), a quarter turn when rotate90 % 4 == 1 (d_rot90,
+ * src/DiffractionLoader.cpp:116-121), then the quadrant swap when fftShift != 0 (h_shiftFFT,
+ * src/DiffractionLoader.cpp:123-125).  Asynchronous on `stream`. */
+int pty_preprocess_patterns(const float* raw_dev, int count, int rows, int cols, int size, int qx, int qy,
+                            int rotate90, int fftShift, float* out_dev, void* stream);
 
 /* In-place batched 2-D FFT of `batch` N x N complex64 arrays in device memory (unnormalised; forward uses
  * exp(-2*pi*i*k*n/N), the CUFFT_FORWARD convention).  Replaces the cuFFT plans of FFTPlanner

@@ -338,3 +338,85 @@ class OracleMls:
 
     def __del__(self):
         self.close()
+
+
+# ---- whole-mode pattern ingest (index work: numpy) ----------------------------------------------------------------
+# DiffractionLoader::run (src/DiffractionLoader.cpp:55-131) step by step, in the reference's order.
+
+def read_pattern_file(path, rows, cols):
+    """All rows x cols sections of a .bin (raw float32, src/FileManager.cpp:145-183) or .csv file (values
+    separated by commas and line breaks, src/FileManager.cpp:185-216) as float32 (n, rows, cols)."""
+    ext = os.path.splitext(path)[1].lower()
+    if ext == ".bin":
+        v = np.fromfile(path, dtype=np.float32)
+    elif ext == ".csv":
+        with open(path) as f:
+            toks = f.read().replace(",", " ").split()
+        v = np.array([np.float32(t) for t in toks], np.float32)
+    else:
+        raise ValueError(f"unsupported pattern file {path}")
+    n = v.size // (rows * cols)
+    return v[:n * rows * cols].reshape(n, rows, cols)
+
+
+def symmetrize(raw, S, qx, qy):
+    """Crop / zero-pad a rows x cols pattern to S x S around (qx, qy) (src/DiffractionLoader.cpp:81-107); a pattern
+    that is already S x S is copied as it is.  Rows / columns the reference would write past the S x S output are
+    dropped."""
+    rows, cols = raw.shape
+    if rows == S and cols == S:
+        return raw.astype(np.float32).copy()
+    out = np.zeros((S, S), np.float32)
+    dx, dy = qx - S // 2, qy - S // 2
+    oox, dox = (-dx, 0) if dx < 0 else (0, dx)
+    ooy, doy = (-dy, 0) if dy < 0 else (0, dy)
+    numX = S if qx + S // 2 < rows else rows - dox
+    numY = S if qy + S // 2 < cols else cols - doy
+    nX, nY = max(0, min(numX, S - oox)), max(0, min(numY, S - ooy))
+    out[oox:oox + nX, ooy:ooy + nY] = raw[dox:dox + nX, doy:doy + nY]
+    return out
+
+
+def rotate90(a, times):
+    """h_realRotate90 (src/utilitiesKernels.cu:2031-2049): only times % 4 == 1 moves data, out[S-1-c][r] = in[r][c]."""
+    if times % 4 != 1:
+        return a.copy()
+    S = a.shape[0]
+    out = np.empty_like(a)
+    r, c = np.meshgrid(np.arange(S), np.arange(S), indexing="ij")
+    out[S - 1 - c, r] = a[r, c]
+    return out
+
+
+def fft_shift(a):
+    """h_shiftFFT (src/utilitiesKernels.cu:1945-1964): rows then columns shifted circularly by round(S/2)."""
+    S = a.shape[0]
+    h = int(np.floor(S / 2 + 0.5))
+    t = np.empty_like(a)
+    t[(np.arange(S) - h) % S, :] = a  # d_shiftX: out[(x - h) mod S][y] = in[x][y]
+    out = np.empty_like(a)
+    out[:, (np.arange(S) - h) % S] = t  # d_shiftY
+    return out
+
+
+def preprocess_pattern(raw, S, qx, qy, rotate90_times=0, fft_shift_data=0):
+    a = symmetrize(raw, S, qx, qy)
+    if rotate90_times > 0:
+        a = rotate90(a, rotate90_times)
+    if fft_shift_data:
+        a = fft_shift(a)
+    return a
+
+
+def ingest(fp, P, S, nx, ny, qx, qy, fs=0, dpf=1, rotate90_times=0, fft_shift_data=0):
+    """The P patterns of a whole-mode run: pattern i from section i % dpf of the file fp with '#' -> '%' formatted
+    with i // dpf + fs (src/Diffractions.cpp:188-209, src/IPhaser.cpp:203-205), then preprocessed."""
+    fmt = fp.replace("#", "%", 1)
+    out = np.zeros((P, S, S), np.float32)
+    cache = {}
+    for i in range(P):
+        name = fmt % (i // dpf + fs) if "%" in fmt else fmt
+        if name not in cache:
+            cache = {name: read_pattern_file(name, nx, ny)}
+        out[i] = preprocess_pattern(cache[name][i % dpf], S, qx, qy, rotate90_times, fft_shift_data)
+    return out

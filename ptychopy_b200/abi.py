@@ -35,7 +35,7 @@ EXPORTS = [
     "pty_warm_object", "pty_dm_psi_from_object", "pty_tc_weights_size", "pty_tc_pack_weights", "pty_tc_conv3x3",
     "pty_tc_pool2", "pty_tc_up2", "pty_tc_to_bf16", "pty_tc_first_layer", "pty_tc_last_layer", "pty_set_warm_start",
     "pty_selftest_bounded_waits", "pty_fft2_tc", "pty_autotune", "pty_get_mls_state",
-    "pty_release_cached_memory",
+    "pty_release_cached_memory", "pty_preprocess_patterns",
 ]
 
 
@@ -95,6 +95,7 @@ def lib():
             "pty_last_error": ([], ctypes.c_char_p),
             "pty_fft2_dev": ([vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
             "pty_fft2_dev_noalloc": ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
+            "pty_preprocess_patterns": ([vp] + [ctypes.c_int] * 8 + [vp, vp], ctypes.c_int),
             "pty_batch_run": ([ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "pty_simulate": ([vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int, vp], ctypes.c_int),
             "pty_set_shard": ([vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),

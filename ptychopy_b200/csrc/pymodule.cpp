@@ -9,8 +9,8 @@
 //     1 split-BF16 tensor-core FFT stages for MLs at 256 x 256), mlsCore (1: MLs without the reference's variable
 //     probe, sub-pixel shift and position search);
 //     probeNP may be (K, N, N) to supply all probe modes.
-// Whole-mode file ingest (fp, hdf5path), simulate mode and CLI strings (cmdstr) are outside this engine and raise
-// NotImplementedError.
+// Whole-mode runs from data files (epie / dm / mls with fp) read .bin and .csv files; .h5 files (hdf5path) need the
+// HDF5 library, which this build does not link, and raise NotImplementedError, as do the CLI strings (cmdstr).
 #define PY_SSIZE_T_CLEAN
 #include <Python.h>
 #define NPY_NO_DEPRECATED_API NPY_1_7_API_VERSION
@@ -79,7 +79,8 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
                                   "probeModes", "lambd", "dx_d", "z", "iter", "T", "jitterRadius", "delta_p",
                                   "threshold", "rotate90", "sqrtData", "fftShiftData", "binaryOutput", "simulate",
                                   "phaseConstraint", "updateProbe", "updateModes", "beamstopMask", "lf", "PPS",
-                                  nullptr};
+                                  "seed", "calculateRMS", "device", "wave", "returnResults", "writeResults",
+                                  "outputDir", "precision", "mlsCore", nullptr};
   int ok;
   if (np) {
     ok = PyArg_ParseTupleAndKeywords(
@@ -91,13 +92,15 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
         &PPS, &seed, &calculateRMS, &device, &wave, &out.returnResults, &out.writeResults, &out.outputDir, &out.warm,
         &out.warmWidth, &precision, &mlsCore);
   } else {
-    ok = PyArg_ParseTupleAndKeywords(args, kw, "|ssisidssiiiiiiiiiiiddidddiiidiiiiiiiiiisi",
+    ok = PyArg_ParseTupleAndKeywords(args, kw, "|ssisidssiiiiiiiiiiiddidddiiidiiiiiiiiiisiKiiiiisii",
                                      const_cast<char**>(kw_file), &jobID, &fp, &fs, &hdf5path, &dpf, &beamSize,
                                      &probeGuess, &objectGuess, &size, &qx, &qy, &nx, &ny, &scanDimsx, &scanDimsy,
                                      &spiralScan, &flipScanAxis, &mirror1, &mirror2, &stepx, &stepy, &probeModes,
                                      &lambd, &dx_d, &z, &iter, &T, &jitter, &delta_p, &threshold, &rotate90,
                                      &sqrtData, &fftShiftData, &binaryOutput, &simulate, &phaseConstraint,
-                                     &updateProbe, &updateModes, &beamstopMask, &lf, &PPS);
+                                     &updateProbe, &updateModes, &beamstopMask, &lf, &PPS, &seed, &calculateRMS,
+                                     &device, &wave, &out.returnResults, &out.writeResults, &out.outputDir,
+                                     &precision, &mlsCore);
   }
   if (!ok) return false;
   pty_params& p = out.p;
@@ -123,8 +126,24 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
 
 // Builds a session from parsed numpy inputs and runs pty_init.  Returns nullptr with a Python error set.
 pty_session* make_session(Parsed& a) {
+  const bool from_files = (!a.diff || a.diff == Py_None) && a.p.fp[0];
+  if (from_files) {  // whole-mode run: pty_init reads the patterns from the files of fp
+    pty_session* s = nullptr;
+    int rc = pty_session_create(&a.p, &s);
+    if (rc != PTY_OK) {
+      raise_status(rc);
+      return nullptr;
+    }
+    Py_BEGIN_ALLOW_THREADS rc = pty_init(s);
+    Py_END_ALLOW_THREADS if (rc != PTY_OK) {
+      raise_status(rc);
+      pty_session_destroy(s);
+      return nullptr;
+    }
+    return s;
+  }
   if (!a.diff || a.diff == Py_None) {
-    PyErr_SetString(PyExc_ValueError, "diffractionNP is required");
+    PyErr_SetString(PyExc_ValueError, "diffractionNP (or a data file pattern fp) is required");
     return nullptr;
   }
   PyArrayObject* d = nullptr;
@@ -250,10 +269,15 @@ bool write_results(pty_session* s, const Parsed& a, int r) {
   return true;
 }
 
-// Whole-mode numpy run: IPhaser::init + phase + writeResultsToDisk (src/ptychopy.c:474-487).
-PyObject* run_np(PyObject* args, PyObject* kw, const char* algorithm) {
+// Whole-mode run: IPhaser::init + phase + writeResultsToDisk (src/ptychopy.c:474-487); np selects the numpy keyword
+// list (epienp, ...) or the file one (epie, ...: patterns from the data files of fp).
+PyObject* run_np(PyObject* args, PyObject* kw, const char* algorithm, bool np = true) {
   Parsed a;
-  if (!parse_kwargs(args, kw, algorithm, true, a)) return nullptr;
+  if (!parse_kwargs(args, kw, algorithm, np, a)) return nullptr;
+  if (!np && !a.p.fp[0]) {
+    PyErr_SetString(PyExc_ValueError, "fp (the data file pattern) is required");
+    return nullptr;
+  }
   pty_session* s = make_session(a);
   if (!s) return nullptr;
   int rc;
@@ -290,8 +314,8 @@ PyObject* run_np(PyObject* args, PyObject* kw, const char* algorithm) {
 
 PyObject* not_implemented(const char* what) {
   PyErr_Format(PyExc_NotImplementedError,
-               "%s: file ingest, simulate mode and command-line strings are not part of this engine; "
-               "use the numpy entry points (epienp, dmnp, mlsnp, epienpinit)",
+               "%s: command-line strings are not part of this engine; "
+               "use the keyword entry points (epie, dm, mls, epienp, dmnp, mlsnp, epienpinit)",
                what);
   return nullptr;
 }
@@ -302,21 +326,9 @@ PyObject* m_helloworld(PyObject*, PyObject* args) {
   Py_RETURN_NONE;
 }
 
-PyObject* m_epie(PyObject*, PyObject* args, PyObject* kw) {
-  Parsed a;
-  if (!parse_kwargs(args, kw, "ePIE", false, a)) return nullptr;
-  return not_implemented("epie");
-}
-PyObject* m_dm(PyObject*, PyObject* args, PyObject* kw) {
-  Parsed a;
-  if (!parse_kwargs(args, kw, "DM", false, a)) return nullptr;
-  return not_implemented("dm");
-}
-PyObject* m_mls(PyObject*, PyObject* args, PyObject* kw) {
-  Parsed a;
-  if (!parse_kwargs(args, kw, "MLs", false, a)) return nullptr;
-  return not_implemented("mls");
-}
+PyObject* m_epie(PyObject*, PyObject* args, PyObject* kw) { return run_np(args, kw, "ePIE", false); }
+PyObject* m_dm(PyObject*, PyObject* args, PyObject* kw) { return run_np(args, kw, "DM", false); }
+PyObject* m_mls(PyObject*, PyObject* args, PyObject* kw) { return run_np(args, kw, "MLs", false); }
 PyObject* m_epienp(PyObject*, PyObject* args, PyObject* kw) { return run_np(args, kw, "ePIE"); }
 PyObject* m_dmnp(PyObject*, PyObject* args, PyObject* kw) { return run_np(args, kw, "DM"); }
 PyObject* m_mlsnp(PyObject*, PyObject* args, PyObject* kw) { return run_np(args, kw, "MLs"); }
@@ -387,9 +399,9 @@ PyObject* m_post(PyObject*, PyObject* args, PyObject* kw) {
 #define KW(f) reinterpret_cast<PyCFunction>(reinterpret_cast<void (*)(void)>(f)), METH_VARARGS | METH_KEYWORDS
 PyMethodDef methods[] = {
     {"helloworld", m_helloworld, METH_VARARGS, "Argument round-trip check."},
-    {"epie", KW(m_epie), "ePIE from data files (not part of this engine)."},
-    {"dm", KW(m_dm), "DM from data files (not part of this engine)."},
-    {"mls", KW(m_mls), "MLs from data files (not part of this engine)."},
+    {"epie", KW(m_epie), "ePIE reconstruction from data files (fp: .bin or .csv)."},
+    {"dm", KW(m_dm), "DM reconstruction from data files (fp: .bin or .csv)."},
+    {"mls", KW(m_mls), "MLs reconstruction from data files (fp: .bin or .csv)."},
     {"epienp", KW(m_epienp), "ePIE reconstruction from numpy arrays."},
     {"dmnp", KW(m_dmnp), "DM reconstruction from numpy arrays."},
     {"mlsnp", KW(m_mlsnp), "MLs reconstruction from numpy arrays."},

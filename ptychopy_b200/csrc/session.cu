@@ -2,6 +2,7 @@
 // reference's IPhaser + CXParams pair (src/IPhaser.cpp:224-365, src/Parameters.cpp:380-653), with parameters
 // held per session instead of in a process-wide singleton.
 #include <algorithm>
+#include <cctype>
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -1506,7 +1507,14 @@ int pty_session_create(const pty_params* p, pty_session** out) {
     need(p->probeModes >= 1, "probeModes must be >= 1");
     need(p->scanDimsx > 0 && p->scanDimsy > 0, "scanDimsx and scanDimsy must be positive");
     need(p->lambd > 0 && p->z > 0 && p->dx_d > 0 && p->beamSize > 0, "lambd, z, dx_d, beamSize must be positive");
-    need(p->fp[0] == 0, "file ingest (fp) is not part of this engine; pass diffractionNP", PTY_ERR_UNSUPPORTED);
+    if (p->fp[0]) {  // whole-mode ingest reads .bin and .csv; .h5 needs the HDF5 library, not linked here
+      std::string ext(p->fp);
+      const size_t dot = ext.find_last_of('.');
+      ext = dot == std::string::npos ? "" : ext.substr(dot + 1);
+      for (char& ch : ext) ch = char(std::tolower(static_cast<unsigned char>(ch)));
+      need(ext != "h5", "HDF5 pattern files need the HDF5 library, which this build does not link; convert them to "
+                        ".bin (raw float32) or .csv", PTY_ERR_UNSUPPORTED);
+    }
     need(p->simulate == 0, "simulate mode is not part of this engine", PTY_ERR_UNSUPPORTED);
     need(p->beamstopMask == 0, "beamstop masks from files are not part of this engine", PTY_ERR_UNSUPPORTED);
     s->N = p->size;
@@ -1591,9 +1599,13 @@ int pty_init(pty_session* s) {
   return guarded([&] {
     need(s != nullptr, "null session");
     need(!s->initialized, "session already initialised", PTY_ERR_STATE);
-    need(s->have_patterns, "no diffraction patterns (diffractionNP) were given", PTY_ERR_STATE);
     set_device(s);
     const pty_params& p = s->prm;
+    if (!s->have_patterns && p.fp[0]) {  // whole-mode run: patterns from the data files (ingest.cu)
+      need(s->shard_total == 0, "position shards take their patterns from pty_set_patterns", PTY_ERR_UNSUPPORTED);
+      ingest_patterns(s, s->pos_m.empty() ? p.scanDimsx * p.scanDimsy : int(s->pos_m.size() / 2));
+    }
+    need(s->have_patterns, "no diffraction patterns (diffractionNP or fp) were given", PTY_ERR_STATE);
     const int Ptot = s->pos_m.empty() ? p.scanDimsx * p.scanDimsy : int(s->pos_m.size() / 2);
     if (s->shard_total > 0) {
       need(s->algo == ALGO_DM, "position shards are supported for DM only", PTY_ERR_UNSUPPORTED);

@@ -68,6 +68,9 @@ MlsGeometry mls_geometry(const std::vector<float>& raw, int N);
 // inference + assembly that writes the session's starting object inside pty_init.
 size_t warm_param_count(int N, int w);
 void run_warm_start(pty_session* s);
+// Whole-mode ingest (ingest.cu): the P patterns of the data files named by the session's fp, preprocessed on the
+// device into the session's pattern buffer.
+void ingest_patterns(pty_session* s, int P);
 
 std::vector<float> raw_cartesian_positions(int nx, int ny, double stepx, double stepy, double dx_s, bool mirrorX,
                                            bool mirrorY);

@@ -22,7 +22,9 @@ def test_module_has_reference_methods(ptychopy):
     assert sys.modules["ptychopy"] is ptychopy
 
 
-def test_file_modes_raise_not_implemented(ptychopy):
+def test_hdf5_files_and_command_strings_raise_not_implemented(ptychopy):
+    # .bin / .csv pattern files are read (tests/test_ingest.py, tests/test_gpu_ingest.py); .h5 needs the HDF5
+    # library, which this build does not link
     with pytest.raises(NotImplementedError):
         ptychopy.epie(jobID="x", fp="/data/scan#.h5", size=256)
     with pytest.raises(NotImplementedError):
