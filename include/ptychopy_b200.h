@@ -57,7 +57,10 @@ typedef struct pty_params {
   int T;                  /* wall-time limit in s (0 = none) */
   int jitterRadius;
   double delta_p;
-  int threshold, rotate90, sqrtData, fftShiftData, binaryOutput, simulate;
+  int threshold, rotate90, sqrtData, fftShiftData, binaryOutput;
+  int simulate;           /* 1: ePIE / DM patterns from the forward model of data/lena<size>.pgm (magnitude) and
+                             data/baboon<size>.pgm (phase), read relative to the working directory, and a simulated
+                             probe with a seeded random phase (src/IPhaser.cpp:93-117) */
   int phaseConstraint, updateProbe, updateModes, beamstopMask;
   char lf[256];           /* positions list file or "" */
   int PPS;
@@ -256,6 +259,11 @@ int pty_get_dims(const pty_session* s, int* X, int* Y, int* K, int* N, int* P, i
 
 /* Copy the object (X x Y complex64) to the host.  Replaces epieresobj / mlsresobj (src/ptychopy.c:964-976). */
 int pty_get_object(pty_session* s, float* c64_out, int X, int Y);
+
+/* Copy the session's diffraction data (P x N x N float32, natural layout) to the host: the patterns as the
+ * iterations read them, after file ingest and its preprocessing or after simulation mode's forward model.  No single
+ * reference counterpart (Diffractions::getPatterns, src/Diffractions.h, is its internal accessor). */
+int pty_get_patterns(pty_session* s, float* out, int P, int N);
 
 /* Copy the probe stack (K x N x N complex64).  Replaces epieresprobe / mlsresprobe (src/ptychopy.c:978-990). */
 int pty_get_probe(pty_session* s, float* c64_out, int K, int N);

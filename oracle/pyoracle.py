@@ -420,3 +420,84 @@ def ingest(fp, P, S, nx, ny, qx, qy, fs=0, dpf=1, rotate90_times=0, fft_shift_da
             cache = {name: read_pattern_file(name, nx, ny)}
         out[i] = preprocess_pattern(cache[name][i % dpf], S, qx, qy, rotate90_times, fft_shift_data)
     return out
+
+
+# ---- simulation mode (simulate=1) ---------------------------------------------------------------------------------
+
+def read_pgm(path):
+    """8-bit PGM (P5 binary or P2 plain) as a uint8 (rows, cols) array."""
+    with open(path, "rb") as f:
+        data = f.read()
+    toks, pos = [], 0
+    while len(toks) < 4:
+        while data[pos:pos + 1].isspace():
+            pos += 1
+        if data[pos:pos + 1] == b"#":
+            pos = data.index(b"\n", pos) + 1
+            continue
+        end = pos
+        while not data[end:end + 1].isspace():
+            end += 1
+        toks.append(data[pos:end].decode())
+        pos = end
+    magic, w, h = toks[0], int(toks[1]), int(toks[2])
+    if magic == "P5":
+        return np.frombuffer(data[pos + 1:pos + 1 + w * h], np.uint8).reshape(h, w)
+    return np.array(data[pos:].split()[:w * h], dtype=np.uint8).reshape(h, w)
+
+
+def sim_object(mag_img, phase_img, X, Y):
+    """Sample::loadFromFile + h_applyHammingToSample (src/Sample.cpp:109-162, src/SampleKernels.cu:75-90,510-518):
+    magnitude (v / max) * 0.9 + 0.1, phase (v / max) * pi/3, times the 2-D Hamming window of period alignUp(w, 32) - 1,
+    centred in an X x Y zero object."""
+    h, w = mag_img.shape
+    mag = (mag_img.astype(np.float64) / mag_img.max()) * np.float64(np.float32(0.9)) + (1.0 - np.float64(np.float32(0.9)))
+    ph = (phase_img.astype(np.float64) / phase_img.max()) * 1.0471975512
+    aw = (w + 31) // 32 * 32
+    ham_c = 0.53836 - 0.46164 * np.cos(np.pi * 2.0 * np.arange(w) / (aw - 1))
+    ham_r = 0.53836 - 0.46164 * np.cos(np.pi * 2.0 * np.arange(h) / (aw - 1))
+    obj = np.zeros((X, Y), np.complex128)
+    ox, oy = X // 2 - h // 2, Y // 2 - w // 2
+    obj[ox:ox + h, oy:oy + w] = mag * np.exp(1j * ph) * ham_r[:, None] * ham_c[None, :]
+    return obj
+
+
+def _splitmix64_stream(seed, n):
+    out = np.empty(n, np.uint64)
+    s = int(seed) & 0xFFFFFFFFFFFFFFFF
+    m = 0xFFFFFFFFFFFFFFFF
+    for i in range(n):
+        s = (s + 0x9E3779B97F4A7C15) & m
+        z = s
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+        out[i] = z ^ (z >> 31)
+    return out
+
+
+def sim_probe(N, beamSize, dx_s, seed):
+    """Probe::simulate (src/Probe.cpp:184-207,332-340; d_initProbeSimulated, src/ProbeKernels.cu:192-205) with the
+    random phase field from the seed: SplitMix64 from seed ^ 0xA0761D6478BD642F, u = ((next >> 11) + 0.5) 2^-53,
+    circular convolution with a Gaussian of FWHM 10 px centred at (N/2, N/2), divided by its maximum."""
+    z = _splitmix64_stream(np.uint64(seed) ^ np.uint64(0xA0761D6478BD642F), N * N)
+    u = ((z >> np.uint64(11)).astype(np.float64) + 0.5) * 2.0 ** -53
+    u = u.reshape(N, N)
+    s = 10.0 / 2.3548
+    c = np.arange(N) - N / 2
+    g = np.exp(-(c[:, None] ** 2 + c[None, :] ** 2) / s ** 2)
+    f = np.real(np.fft.ifft2(np.fft.fft2(u) * np.fft.fft2(g)))
+    f = f / f.max()
+    window = N / (2 * 2.35)
+    factor = float(np.float32(dx_s / beamSize))
+    r = np.sqrt(c[:, None] ** 2 + c[None, :] ** 2)
+    q = r * factor
+    with np.errstate(invalid="ignore", divide="ignore"):
+        p = np.where(q != 0, np.sin(np.pi * q) / (np.pi * q), 1.0)
+    p = np.abs(p * np.exp(-r * r / window ** 2))
+    return p * np.exp(1j * np.pi * f)
+
+
+def simulate_amplitudes(obj, probe, pos):
+    """Diffractions::simulate (src/Diffractions.cpp:80-117): |FFT2(bilinear O at pos * P)| per position."""
+    N = probe.shape[0]
+    return np.stack([np.abs(fft2(extract_patch(obj, np.float32(q[0]), np.float32(q[1]), N) * probe)) for q in pos])

@@ -35,7 +35,7 @@ EXPORTS = [
     "pty_warm_object", "pty_dm_psi_from_object", "pty_tc_weights_size", "pty_tc_pack_weights", "pty_tc_conv3x3",
     "pty_tc_pool2", "pty_tc_up2", "pty_tc_to_bf16", "pty_tc_first_layer", "pty_tc_last_layer", "pty_set_warm_start",
     "pty_selftest_bounded_waits", "pty_fft2_tc", "pty_autotune", "pty_get_mls_state",
-    "pty_release_cached_memory", "pty_preprocess_patterns",
+    "pty_release_cached_memory", "pty_preprocess_patterns", "pty_get_patterns",
 ]
 
 
@@ -96,6 +96,7 @@ def lib():
             "pty_fft2_dev": ([vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
             "pty_fft2_dev_noalloc": ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
             "pty_preprocess_patterns": ([vp] + [ctypes.c_int] * 8 + [vp, vp], ctypes.c_int),
+            "pty_get_patterns": ([vp, vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "pty_batch_run": ([ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int], ctypes.c_int),
             "pty_simulate": ([vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int, vp], ctypes.c_int),
             "pty_set_shard": ([vp, ctypes.c_int, ctypes.c_int], ctypes.c_int),
@@ -247,6 +248,13 @@ class Session:
         p = np.empty((d["K"], d["N"], d["N"]), np.complex64)
         check(lib().pty_get_probe(self.h, _ptr(p), d["K"], d["N"]))
         return p
+
+    def patterns(self):
+        """The session's diffraction data (P, N, N) float32 as the iterations read them (pty_get_patterns)."""
+        d = self.dims()
+        out = np.zeros((d["P"], d["N"], d["N"]), np.float32)
+        check(lib().pty_get_patterns(self.h, _ptr(out), d["P"], d["N"]))
+        return out
 
     def positions(self):
         d = self.dims()

@@ -126,8 +126,8 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
 
 // Builds a session from parsed numpy inputs and runs pty_init.  Returns nullptr with a Python error set.
 pty_session* make_session(Parsed& a) {
-  const bool from_files = (!a.diff || a.diff == Py_None) && a.p.fp[0];
-  if (from_files) {  // whole-mode run: pty_init reads the patterns from the files of fp
+  const bool from_files = (!a.diff || a.diff == Py_None) && (a.p.fp[0] || a.p.simulate);
+  if (from_files) {  // whole-mode run: pty_init reads the patterns from the files of fp (or simulates them)
     pty_session* s = nullptr;
     int rc = pty_session_create(&a.p, &s);
     if (rc != PTY_OK) {
@@ -274,8 +274,8 @@ bool write_results(pty_session* s, const Parsed& a, int r) {
 PyObject* run_np(PyObject* args, PyObject* kw, const char* algorithm, bool np = true) {
   Parsed a;
   if (!parse_kwargs(args, kw, algorithm, np, a)) return nullptr;
-  if (!np && !a.p.fp[0]) {
-    PyErr_SetString(PyExc_ValueError, "fp (the data file pattern) is required");
+  if (!np && !a.p.fp[0] && !a.p.simulate) {
+    PyErr_SetString(PyExc_ValueError, "fp (the data file pattern) or simulate=1 is required");
     return nullptr;
   }
   pty_session* s = make_session(a);

@@ -1515,7 +1515,9 @@ int pty_session_create(const pty_params* p, pty_session** out) {
       need(ext != "h5", "HDF5 pattern files need the HDF5 library, which this build does not link; convert them to "
                         ".bin (raw float32) or .csv", PTY_ERR_UNSUPPORTED);
     }
-    need(p->simulate == 0, "simulate mode is not part of this engine", PTY_ERR_UNSUPPORTED);
+    need(p->simulate == 0 || s->algo != ALGO_MLS,
+         "simulate=1 is available for ePIE and DM (the reference's MLs simulation builds an ML mesh of its own)",
+         PTY_ERR_UNSUPPORTED);
     need(p->beamstopMask == 0, "beamstop masks from files are not part of this engine", PTY_ERR_UNSUPPORTED);
     s->N = p->size;
     s->K = p->probeModes;
@@ -1601,6 +1603,12 @@ int pty_init(pty_session* s) {
     need(!s->initialized, "session already initialised", PTY_ERR_STATE);
     set_device(s);
     const pty_params& p = s->prm;
+    if (!s->have_patterns && p.simulate) {  // simulation mode: patterns from the forward model (sim_mode.cu)
+      need(s->shard_total == 0, "position shards take their patterns from pty_set_patterns", PTY_ERR_UNSUPPORTED);
+      s->P = s->pos_m.empty() ? p.scanDimsx * p.scanDimsy : int(s->pos_m.size() / 2);
+      init_geometry(s);
+      simulate_session_patterns(s);
+    }
     if (!s->have_patterns && p.fp[0]) {  // whole-mode run: patterns from the data files (ingest.cu)
       need(s->shard_total == 0, "position shards take their patterns from pty_set_patterns", PTY_ERR_UNSUPPORTED);
       ingest_patterns(s, s->pos_m.empty() ? p.scanDimsx * p.scanDimsy : int(s->pos_m.size() / 2));
@@ -1675,6 +1683,7 @@ int pty_init(pty_session* s) {
       check_cuda(cudaStreamSynchronize(s->stream), "transpose");
       std::swap(s->amp.p, t.p);
       std::swap(s->amp.bytes, t.bytes);
+      s->amp_transposed = true;
     }
     if (s->algo == ALGO_EPIE) {
       init_epie(s);
@@ -1901,6 +1910,27 @@ int pty_get_object(pty_session* s, float* out, int X, int Y) {
     check_cuda(cudaMemcpyAsync(out, s->obj.p, sizeof(float2) * size_t(X) * Y, cudaMemcpyDeviceToHost, s->stream),
                "D2H object");
     check_cuda(cudaStreamSynchronize(s->stream), "D2H object");
+  });
+}
+
+int pty_get_patterns(pty_session* s, float* out, int P, int N) {
+  return guarded([&] {
+    need(s && out, "null argument");
+    need(s->have_patterns, "the session has no patterns", PTY_ERR_STATE);
+    need(P == s->P && N == s->N, "pattern shape differs from the session's");
+    set_device(s);
+    const size_t NN = size_t(N) * N;
+    check_cuda(cudaMemcpyAsync(out, s->amp.p, sizeof(float) * NN * P, cudaMemcpyDeviceToHost, s->stream), "D2H");
+    check_cuda(cudaStreamSynchronize(s->stream), "D2H patterns");
+    if (s->amp_transposed) {  // back to the natural [x][y] layout
+      std::vector<float> t(NN);
+      for (int i = 0; i < P; ++i) {
+        float* pl = out + NN * i;
+        for (int x = 0; x < N; ++x)
+          for (int y = 0; y < N; ++y) t[size_t(x) * N + y] = pl[size_t(y) * N + x];
+        std::copy(t.begin(), t.end(), pl);
+      }
+    }
   });
 }
 

@@ -71,6 +71,11 @@ void run_warm_start(pty_session* s);
 // Whole-mode ingest (ingest.cu): the P patterns of the data files named by the session's fp, preprocessed on the
 // device into the session's pattern buffer.
 void ingest_patterns(pty_session* s, int P);
+// Simulation mode (sim_mode.cu): the patterns from the forward model of the reference's PGM object and simulated
+// probe at the session's scan positions (geometry set); the object and probe of the simulation, for the tests.
+void simulate_session_patterns(pty_session* s);
+std::vector<float> sim_object_from_files(int N, int X, int Y);
+std::vector<float> sim_probe(int N, double beamSize, double dx_s, uint64_t seed);
 
 std::vector<float> raw_cartesian_positions(int nx, int ny, double stepx, double stepy, double dx_s, bool mirrorX,
                                            bool mirrorY);
@@ -105,6 +110,7 @@ struct pty_session {
 
   // device state
   pty::DeviceBuf amp;    // P*N*N float (natural layout; sessions of the cluster ePIE kernel transpose each plane)
+  bool amp_transposed = false;
   pty::DeviceBuf obj, probe, ocache, pcache;
   pty::DeviceBuf tw, dOffs, scal;
   // DM

@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import pyoracle as po
+from conftest import rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -100,7 +101,10 @@ def test_file_mode_equals_numpy_mode(tmp_path, algo, ext):
     run_np = {"ePIE": pt.epienp, "DM": pt.dmnp}[algo]
     o1, p1 = run_files(fp=fp, fs=fs, dpf=dpf, nx=80, ny=72, qx=40, qy=36, rotate90=1, fftShiftData=1, **kw)
     o2, p2 = run_np(diffractionNP=amp, **kw)
-    assert np.array_equal(o1, o2) and np.array_equal(p1, p2)
+    if algo == "ePIE":  # deterministic
+        assert np.array_equal(o1, o2) and np.array_equal(p1, p2)
+    else:  # DM sums its increments with float atomics, whose order varies from run to run
+        assert rel_err(o1, o2) < 1e-5 and rel_err(p1, p2) < 1e-5
 
 
 def test_file_mode_errors(tmp_path):
