@@ -78,6 +78,10 @@ typedef struct pty_params {
                              (src/Parameters.h:162-163: variable probe with one extra mode, variable intensity,
                              sub-pixel probe shift, position search from iteration PPS); 1 the fixed-probe core
                              without them */
+  int save;               /* pty_run writes the results (pty_write_results to outputDir, r = iteration / save)
+                             after every `save`-th iteration; 0 = never.  The reference's command line has this
+                             checkpoint (src/IPhaser.cpp:384-385); its Python path leaves it at 999999 */
+  char outputDir[256];    /* directory of those checkpoint files ("" = "data", the reference's) */
 } pty_params;
 
 typedef struct pty_session pty_session;

@@ -501,3 +501,35 @@ def simulate_amplitudes(obj, probe, pos):
     """Diffractions::simulate (src/Diffractions.cpp:80-117): |FFT2(bilinear O at pos * P)| per position."""
     N = probe.shape[0]
     return np.stack([np.abs(fft2(extract_patch(obj, np.float32(q[0]), np.float32(q[1]), N) * probe)) for q in pos])
+
+
+# ---- result files ---------------------------------------------------------------------------------------------------
+
+def format_complex_csv(a):
+    """Cuda2DArray::save in text mode (src/Cuda2DArray.hpp:439-464) with the complex cell of src/Cuda2DArray.cpp:46-52:
+    `re`, '+' when im >= 0, `im`, 'j', each number as an ostream prints a float (6 significant digits, %g), cells
+    joined by ", ", one line per row."""
+    a = np.asarray(a, np.complex64)
+    rows = []
+    for row in a:
+        cells = []
+        for v in row:
+            re, im = float(np.float32(v.real)), float(np.float32(v.imag))
+            cells.append("%g" % re + ("+" if im >= 0 else "") + "%g" % im + "j")
+        rows.append(", ".join(cells) + "\n")
+    return "".join(rows)
+
+
+def parse_complex_csv(text):
+    """The values of such a file as complex64 (rows, cols)."""
+    out = []
+    for line in text.splitlines():
+        if not line.strip():
+            continue
+        row = []
+        for cell in line.split(","):
+            c = cell.strip().rstrip("ji")
+            k = max(i for i in range(1, len(c)) if c[i] in "+-" and c[i - 1] not in "eE")
+            row.append(complex(np.float32(float(c[:k].rstrip("+"))), np.float32(float(c[k:]))))
+        out.append(row)
+    return np.array(out, np.complex64)

@@ -57,7 +57,7 @@ class PtyParams(ctypes.Structure):
         ("updateModes", ctypes.c_int), ("beamstopMask", ctypes.c_int), ("lf", ctypes.c_char * 256),
         ("PPS", ctypes.c_int), ("seed", ctypes.c_uint64), ("calculateRMS", ctypes.c_int),
         ("device", ctypes.c_int), ("wave", ctypes.c_int), ("precision", ctypes.c_int),
-        ("mlsCore", ctypes.c_int),
+        ("mlsCore", ctypes.c_int), ("save", ctypes.c_int), ("outputDir", ctypes.c_char * 256),
     ]
 
 

@@ -7,7 +7,8 @@
 //   * extra keywords: seed, calculateRMS, device, wave, returnResults, writeResults, outputDir, warmStart (trained
 //     warm-start network parameters, float32) and warmStartWidth (its width, default 16), precision (0 FP32 FFT,
 //     1 split-BF16 tensor-core FFT stages for MLs at 256 x 256), mlsCore (1: MLs without the reference's variable
-//     probe, sub-pixel shift and position search);
+//     probe, sub-pixel shift and position search), save (write the results every `save` iterations, like the
+//     reference's command-line option);
 //     probeNP may be (K, N, N) to supply all probe modes.
 // Whole-mode runs from data files (epie / dm / mls with fp) read .bin and .csv files; .h5 files (hdf5path) need the
 // HDF5 library, which this build does not link, and raise NotImplementedError, as do the CLI strings (cmdstr).
@@ -63,7 +64,7 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
   int phaseConstraint = 1, updateProbe = 10, updateModes = 20, beamstopMask = 0, PPS = 20;
   double beamSize = 400e-9, stepx = 40e-9, stepy = 40e-9, lambd = 2.3843e-10, dx_d = 172e-6, z = 2.2, delta_p = 0.1;
   unsigned long long seed = out.p.seed;
-  int calculateRMS = 0, device = 0, wave = 0, precision = 0, mlsCore = 0;
+  int calculateRMS = 0, device = 0, wave = 0, precision = 0, mlsCore = 0, save = 0;
   static const char* kw_np[] = {"jobID", "diffractionNP", "positionNP", "objectNP", "probeNP", "fp", "fs",
                                 "hdf5path", "dpf", "beamSize", "probeGuess", "objectGuess", "size", "qx", "qy", "nx",
                                 "ny", "scanDimsx", "scanDimsy", "spiralScan", "flipScanAxis", "mirror1stScanAxis",
@@ -72,7 +73,7 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
                                 "binaryOutput", "simulate", "phaseConstraint", "updateProbe", "updateModes",
                                 "beamstopMask", "lf", "PPS", "seed", "calculateRMS", "device", "wave",
                                 "returnResults", "writeResults", "outputDir", "warmStart", "warmStartWidth",
-                                "precision", "mlsCore", nullptr};
+                                "precision", "mlsCore", "save", nullptr};
   static const char* kw_file[] = {"jobID", "fp", "fs", "hdf5path", "dpf", "beamSize", "probeGuess", "objectGuess",
                                   "size", "qx", "qy", "nx", "ny", "scanDimsx", "scanDimsy", "spiralScan",
                                   "flipScanAxis", "mirror1stScanAxis", "mirror2ndScanAxis", "stepx", "stepy",
@@ -80,19 +81,19 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
                                   "threshold", "rotate90", "sqrtData", "fftShiftData", "binaryOutput", "simulate",
                                   "phaseConstraint", "updateProbe", "updateModes", "beamstopMask", "lf", "PPS",
                                   "seed", "calculateRMS", "device", "wave", "returnResults", "writeResults",
-                                  "outputDir", "precision", "mlsCore", nullptr};
+                                  "outputDir", "precision", "mlsCore", "save", nullptr};
   int ok;
   if (np) {
     ok = PyArg_ParseTupleAndKeywords(
-        args, kw, "|sOOOOsisidssiiiiiiiiiiiddidddiiidiiiiiiiiiisiKiiiiisOiii", const_cast<char**>(kw_np), &jobID,
+        args, kw, "|sOOOOsisidssiiiiiiiiiiiddidddiiidiiiiiiiiiisiKiiiiisOiiii", const_cast<char**>(kw_np), &jobID,
         &out.diff, &out.pos, &out.obj, &out.probe, &fp, &fs, &hdf5path, &dpf, &beamSize, &probeGuess, &objectGuess,
         &size, &qx, &qy, &nx, &ny, &scanDimsx, &scanDimsy, &spiralScan, &flipScanAxis, &mirror1, &mirror2, &stepx,
         &stepy, &probeModes, &lambd, &dx_d, &z, &iter, &T, &jitter, &delta_p, &threshold, &rotate90, &sqrtData,
         &fftShiftData, &binaryOutput, &simulate, &phaseConstraint, &updateProbe, &updateModes, &beamstopMask, &lf,
         &PPS, &seed, &calculateRMS, &device, &wave, &out.returnResults, &out.writeResults, &out.outputDir, &out.warm,
-        &out.warmWidth, &precision, &mlsCore);
+        &out.warmWidth, &precision, &mlsCore, &save);
   } else {
-    ok = PyArg_ParseTupleAndKeywords(args, kw, "|ssisidssiiiiiiiiiiiddidddiiidiiiiiiiiiisiKiiiiisii",
+    ok = PyArg_ParseTupleAndKeywords(args, kw, "|ssisidssiiiiiiiiiiiddidddiiidiiiiiiiiiisiKiiiiisiii",
                                      const_cast<char**>(kw_file), &jobID, &fp, &fs, &hdf5path, &dpf, &beamSize,
                                      &probeGuess, &objectGuess, &size, &qx, &qy, &nx, &ny, &scanDimsx, &scanDimsy,
                                      &spiralScan, &flipScanAxis, &mirror1, &mirror2, &stepx, &stepy, &probeModes,
@@ -100,7 +101,7 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
                                      &sqrtData, &fftShiftData, &binaryOutput, &simulate, &phaseConstraint,
                                      &updateProbe, &updateModes, &beamstopMask, &lf, &PPS, &seed, &calculateRMS,
                                      &device, &wave, &out.returnResults, &out.writeResults, &out.outputDir,
-                                     &precision, &mlsCore);
+                                     &precision, &mlsCore, &save);
   }
   if (!ok) return false;
   pty_params& p = out.p;
@@ -121,6 +122,8 @@ bool parse_kwargs(PyObject* args, PyObject* kw, const char* algorithm, bool np, 
   p.wave = wave;
   p.precision = precision;
   p.mlsCore = mlsCore;
+  p.save = save;
+  copy_str(p.outputDir, sizeof(p.outputDir), out.outputDir);
   return true;
 }
 

@@ -582,6 +582,21 @@ void write_complex_file(const std::string& path, const float* c64, size_t rows, 
   if (!f.good()) fail(PTY_ERR_IO, "write failed: " + path);
 }
 
+// IPhaser::writeResultsToDisk (src/IPhaser.cpp:417-428): <dir>/<jobID>_probes_<r>.<csv|bin> and _object_.
+void write_results(pty_session* s, const std::string& dir, int r, bool binary) {
+  set_device(s);
+  std::vector<float> pr(2 * size_t(s->K) * s->N * s->N), ob(2 * size_t(s->X) * s->Y);
+  check_cuda(cudaMemcpyAsync(pr.data(), s->probe.p, pr.size() * sizeof(float), cudaMemcpyDeviceToHost, s->stream),
+             "D2H");
+  check_cuda(cudaMemcpyAsync(ob.data(), s->obj.p, ob.size() * sizeof(float), cudaMemcpyDeviceToHost, s->stream),
+             "D2H");
+  check_cuda(cudaStreamSynchronize(s->stream), "D2H results");
+  const std::string ext = binary ? "bin" : "csv";
+  const std::string base = dir + "/" + s->prm.jobID;
+  write_complex_file(base + "_probes_" + std::to_string(r) + "." + ext, pr.data(), size_t(s->K) * s->N, s->N, binary);
+  write_complex_file(base + "_object_" + std::to_string(r) + "." + ext, ob.data(), s->X, s->Y, binary);
+}
+
 // Reads a complex CSV in the reference's format (probeGuess / objectGuess files).
 std::vector<float> read_complex_csv(const std::string& path, size_t& rows, size_t& cols) {
   std::ifstream f(path);
@@ -1736,6 +1751,8 @@ int pty_run(pty_session* s, int iters, double* errs) {
         step_dm(s, it);
       s->iter = it;
       if (errs) errs[i] = e;
+      if (s->prm.save > 0 && it % s->prm.save == 0)  // checkpoint (IPhaser::phaseLoop, src/IPhaser.cpp:384-385)
+        write_results(s, s->prm.outputDir[0] ? s->prm.outputDir : "data", it / s->prm.save, s->prm.binaryOutput != 0);
       if (s->prm.T > 0) {  // wall-time limit (src/IPhaser.cpp:386-387)
         check_cuda(cudaStreamSynchronize(s->stream), "iteration");
         if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >= s->prm.T) break;
@@ -1988,18 +2005,7 @@ int pty_write_results(pty_session* s, const char* dir, int r, int binary) {
   return guarded([&] {
     need(s && dir, "null argument");
     need(s->initialized, "pty_init has not run", PTY_ERR_STATE);
-    set_device(s);
-    std::vector<float> pr(2 * size_t(s->K) * s->N * s->N), ob(2 * size_t(s->X) * s->Y);
-    check_cuda(cudaMemcpyAsync(pr.data(), s->probe.p, pr.size() * sizeof(float), cudaMemcpyDeviceToHost, s->stream),
-               "D2H");
-    check_cuda(cudaMemcpyAsync(ob.data(), s->obj.p, ob.size() * sizeof(float), cudaMemcpyDeviceToHost, s->stream),
-               "D2H");
-    check_cuda(cudaStreamSynchronize(s->stream), "D2H results");
-    const std::string ext = binary ? "bin" : "csv";
-    const std::string base = std::string(dir) + "/" + s->prm.jobID;
-    write_complex_file(base + "_probes_" + std::to_string(r) + "." + ext, pr.data(), size_t(s->K) * s->N, s->N,
-                       binary != 0);
-    write_complex_file(base + "_object_" + std::to_string(r) + "." + ext, ob.data(), s->X, s->Y, binary != 0);
+    write_results(s, dir, r, binary != 0);
   });
 }
 
