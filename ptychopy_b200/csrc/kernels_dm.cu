@@ -26,6 +26,7 @@
 #include "fft_core.cuh"
 #include "kernel_util.cuh"
 #include "kernels.h"
+#include "pdl.cuh"
 
 namespace pty {
 
@@ -78,7 +79,7 @@ __device__ __forceinline__ void dm_item_rows(const DMBuffers& b, int p, int slot
 
 // Columns sub*CB .. sub*CB + CB-1 of pattern p: forward FFT along x, modulus, inverse FFT along x.
 template <int L>
-__device__ __forceinline__ void dm_item_cols(const DMBuffers& b, int p, int slot, int sub, float2* s_x,
+__device__ __forceinline__ void dm_item_cols(const DMBuffers& b, int p, int slot, int slot2, int sub, float2* s_x,
                                              const float2* s_tw) {
   using S = FftShape<L>;
   constexpr int T = S::T, E = S::E, CB = cols_per_block<L>();
@@ -101,7 +102,7 @@ __device__ __forceinline__ void dm_item_cols(const DMBuffers& b, int p, int slot
   });
   to_input_order<L>(a);
   fft_cols<L, true>(a, s, c, s_x, s_tw);
-  float2* w2 = b.W2 + size_t(slot) * L * L + col;
+  float2* w2 = b.W2 + size_t(slot2) * L * L + col;
   static_for<0, E>([&](auto ec) {
     constexpr int e = decltype(ec)::value;
     w2[size_t(s + T * e) * L] = a[out_slot<L>(e)];
@@ -166,7 +167,7 @@ __global__ void __launch_bounds__(DMShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
   float2* smem = reinterpret_cast<float2*>(smem4);
   load_twiddles<L>(smem, b.tw);  // visible after fft_cols' first barrier
   for (int item = blockIdx.x; item < NB * w.count; item += gridDim.x)
-    dm_item_cols<L>(b, w.slot_pat[item / NB], item / NB, item % NB, smem + L, smem);
+    dm_item_cols<L>(b, w.slot_pat[item / NB], item / NB, item / NB, item % NB, smem + L, smem);
 }
 
 template <int L, bool PC, bool UP>
@@ -179,6 +180,47 @@ __global__ void __launch_bounds__(DMShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS_INV)
   __syncthreads();
   for (int item = blockIdx.x; item < NB * w.count; item += gridDim.x)
     dm_item_inv<L, PC, UP>(b, w.slot_pat[item / NB], item / NB, item % NB, smem + L, smem);
+}
+
+// Skewed pipeline: launch k of an iteration runs the row items of wave k, the column items of wave k-1 and the inverse
+// items of wave k-2 (DMSkew), so an iteration is waves + 2 launches instead of 3 x waves and every launch mixes the
+// three kinds of work.  The row items depend on nothing the previous launch writes (psi of other patterns, the
+// iteration's snapshot of O and P, a W1 buffer of three that the previous launch neither reads nor writes), so they
+// run first, while the previous launch may still be finishing (programmatic dependent launch); the column and inverse
+// items wait for it (griddepcontrol.wait) and alternate item by item.  A launch lets the next one start only once all
+// its CTAs are past that wait, so at most two launches overlap (this one's second phase, the next one's row items):
+// three W1 buffers (rows k, cols k-1, the next launch's rows k+1) and two W2 buffers (cols k-1, inverse k-2) suffice.
+template <int L, bool PC, bool UP>
+__global__ void __launch_bounds__(DMShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
+    k_dm_skew(const DMBuffers b, const DMSkew k) {
+  constexpr int NB = DMShape<L>::NB;
+  extern __shared__ float4 smem4[];
+  float2* smem = reinterpret_cast<float2*>(smem4);
+  if (k.first) asm volatile("griddepcontrol.wait;" ::: "memory");
+  load_twiddles<L>(smem, b.tw);
+  __syncthreads();
+  for (int item = blockIdx.x; item < NB * k.rows_count; item += gridDim.x)
+    dm_item_rows<L>(b, k.rows_pat[item / NB], k.rows_w1 + item / NB, item % NB, smem + L, smem);
+  if (!k.first) asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const int nc = NB * k.cols_count, ni = NB * k.inv_count, n = nc + ni;
+  for (int q = blockIdx.x; q < n; q += gridDim.x) {
+    // alternate column and inverse items while both remain
+    const int m = nc < ni ? nc : ni;
+    int kind, item;
+    if (q < 2 * m) {
+      kind = q & 1;
+      item = q >> 1;
+    } else {
+      kind = nc > ni ? 0 : 1;
+      item = q - m;
+    }
+    if (kind == 0)
+      dm_item_cols<L>(b, k.cols_pat[item / NB], k.cols_w1 + item / NB, k.cols_w2 + item / NB, item % NB, smem + L,
+                      smem);
+    else
+      dm_item_inv<L, PC, UP>(b, k.inv_pat[item / NB], k.inv_w2 + item / NB, item % NB, smem + L, smem);
+  }
 }
 
 // O += dO, P += dP (mode 0), reset the accumulators, and sum |O|^2 and |P|^2 over all stacked probe modes.
@@ -231,9 +273,11 @@ __global__ void k_dm_factors(double* __restrict__ sums, double* __restrict__ fac
 template <int L>
 static cudaError_t dm_prepare_t() {
   const int sm = int(DMShape<L>::SMEM);
-  const void* fns[6] = {(const void*)k_dm_rows<L>, (const void*)k_dm_cols<L>, (const void*)k_dm_inv<L, false, false>,
-                        (const void*)k_dm_inv<L, false, true>, (const void*)k_dm_inv<L, true, false>,
-                        (const void*)k_dm_inv<L, true, true>};
+  const void* fns[10] = {(const void*)k_dm_rows<L>, (const void*)k_dm_cols<L>, (const void*)k_dm_inv<L, false, false>,
+                         (const void*)k_dm_inv<L, false, true>, (const void*)k_dm_inv<L, true, false>,
+                         (const void*)k_dm_inv<L, true, true>, (const void*)k_dm_skew<L, false, false>,
+                         (const void*)k_dm_skew<L, false, true>, (const void*)k_dm_skew<L, true, false>,
+                         (const void*)k_dm_skew<L, true, true>};
   for (const void* f : fns) {
     const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
@@ -317,6 +361,52 @@ cudaError_t dm_wave(const DMBuffers& b, const DMWave& w, bool pc, bool up, cudaS
     case 512: return dm_wave_t<512>(b, w, pc, up, st, launches);
     default: return cudaErrorInvalidValue;
   }
+}
+
+template <int L>
+static int dm_slots_skew() {
+  static const int s = resident_slots(k_dm_skew<L, true, true>, DMShape<L>::THREADS, DMShape<L>::SMEM);
+  return s;
+}
+
+template <int L>
+static cudaError_t dm_skew_t(const DMBuffers& b, const DMSkew& k, bool pc, bool up, cudaStream_t st,
+                             int64_t* launches) {
+  constexpr int NT = DMShape<L>::THREADS, NB = DMShape<L>::NB;
+  const int items = NB * (k.rows_count + k.cols_count + k.inv_count);
+  if (items == 0) return cudaSuccess;
+  const dim3 grid(std::min(dm_slots_skew<L>(), items)), block(NT);
+  const size_t sm = DMShape<L>::SMEM;
+  cudaError_t e;
+  if (pc && up)
+    e = launch_pdl(k_dm_skew<L, true, true>, grid, block, sm, st, b, k);
+  else if (pc)
+    e = launch_pdl(k_dm_skew<L, true, false>, grid, block, sm, st, b, k);
+  else if (up)
+    e = launch_pdl(k_dm_skew<L, false, true>, grid, block, sm, st, b, k);
+  else
+    e = launch_pdl(k_dm_skew<L, false, false>, grid, block, sm, st, b, k);
+  if (launches) *launches += 1;
+  return e;
+}
+
+cudaError_t dm_skew(const DMBuffers& b, const DMSkew& k, bool pc, bool up, cudaStream_t st, int64_t* launches) {
+  switch (b.N) {
+    case 32: return dm_skew_t<32>(b, k, pc, up, st, launches);
+    case 64: return dm_skew_t<64>(b, k, pc, up, st, launches);
+    case 128: return dm_skew_t<128>(b, k, pc, up, st, launches);
+    case 256: return dm_skew_t<256>(b, k, pc, up, st, launches);
+    case 512: return dm_skew_t<512>(b, k, pc, up, st, launches);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// Patterns per wave of the skewed pipeline: three W1 and two W2 buffers of a wave stay within ~48 MB of the L2.
+int dm_skew_wave_size(int N, int P) {
+  const size_t bytes_per_pattern = 5 * sizeof(float2) * size_t(N) * N;
+  const int maxwave = int(std::max<size_t>(1, (size_t(48) << 20) / bytes_per_pattern));
+  const int nwaves = (P + maxwave - 1) / maxwave;
+  return (P + nwaves - 1) / nwaves;
 }
 
 cudaError_t dm_finalize(const DMBuffers& b, bool up, cudaStream_t st, int64_t* launches) {
