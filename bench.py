@@ -79,8 +79,6 @@ def parse():
                     help="skip the ePIE 512^2 and warm-start parts of the headline after the DM line")
     ap.add_argument("--nx", type=int, default=30, help="raster size (30 = the DM configuration; smaller for profiling)")
     ap.add_argument("--wave", type=int, default=0, help="DM patterns per pipeline wave (0 = automatic)")
-    ap.add_argument("--pipeline", type=int, default=0, choices=[0, 1, 2],
-                    help="DM schedule: 0 automatic, 1 three launches per wave, 2 skewed (one launch per wave)")
     ap.add_argument("--algo", default="dm", choices=["dm", "epie", "batch", "nrmse", "mls", "warm", "infer", "fft"])
     ap.add_argument("--shard", action="store_true",
                     help="N>1: split the 900 positions over the GPUs (one NCCL all-reduce of the DM increments per "
@@ -283,7 +281,7 @@ def run_b200(args, rank, world, local):
     N, P = ds["N"], ds["P"]
     stream = torch.cuda.Stream()
     shard = args.shard
-    s = abi.Session(**dict(ds["kwargs"], algorithm="DM", device=local, wave=args.wave, pipeline=args.pipeline))
+    s = abi.Session(**dict(ds["kwargs"], algorithm="DM", device=local, wave=args.wave))
     s.set_stream(stream.cuda_stream)
     if shard:
         bounds = [P * r // world for r in range(world + 1)]

@@ -82,9 +82,6 @@ typedef struct pty_params {
                              after every `save`-th iteration; 0 = never.  The reference's command line has this
                              checkpoint (src/IPhaser.cpp:384-385); its Python path leaves it at 999999 */
   char outputDir[256];    /* directory of those checkpoint files ("" = "data", the reference's) */
-  int pipeline;           /* DM kernel schedule: 0 automatic, 1 waves of three launches (row, column, inverse
-                             passes), 2 skewed: one launch per wave mixing the row pass of a wave, the column pass of
-                             the wave before and the inverse pass of the one before that, with L2-sized waves */
 } pty_params;
 
 typedef struct pty_session pty_session;

@@ -71,22 +71,7 @@ int dm_wave_size(int N, int P);
 cudaError_t dm_wave(const DMBuffers& b, const DMWave& w, bool phaseConstraint, bool updateProbe, cudaStream_t st,
                     int64_t* launches);
 cudaError_t dm_finalize(const DMBuffers& b, bool updateProbe, cudaStream_t st, int64_t* launches);
-// One launch of the skewed DM pipeline: row items of one wave (W1 slots from rows_w1), column items of the previous
-// wave (W1 slots cols_w1 -> W2 slots cols_w2) and inverse items of the one before (W2 slots inv_w2).  first != 0: the
-// launch waits for the previous kernel before its row items too (the iteration's first launch, after finalize).
-struct DMSkew {
-  const int* rows_pat;
-  int rows_count, rows_w1;
-  const int* cols_pat;
-  int cols_count, cols_w1, cols_w2;
-  const int* inv_pat;
-  int inv_count, inv_w2;
-  int first;
-};
-cudaError_t dm_skew(const DMBuffers& b, const DMSkew& k, bool phaseConstraint, bool updateProbe, cudaStream_t st,
-                    int64_t* launches);
-// Patterns per wave of the skewed pipeline (its W1 and W2 buffers, 5 per wave, kept L2-sized).
-int dm_skew_wave_size(int N, int P);
+
 // psi_p = P * O at every pattern's rounded offset (P patterns).
 cudaError_t dm_psi_from_object(const DMBuffers& b, int P, cudaStream_t st);
 

@@ -26,7 +26,6 @@
 #include "fft_core.cuh"
 #include "kernel_util.cuh"
 #include "kernels.h"
-#include "pdl.cuh"
 
 namespace pty {
 
@@ -122,7 +121,6 @@ __device__ __forceinline__ void dm_item_inv(const DMBuffers& b, int p, int slot,
 #pragma unroll
   for (int e = 0; e < E; ++e) a[e] = row[t + T * e];
   fft_vec<L, true>(a, t, s_x + v * S::XCH, s_tw);
-  const float f0 = float(b.fac[0]), f1 = float(b.fac[1]);
   const int2 o = b.offs[p];
   const float2* prow = b.probe + size_t(x) * L;
   const float2* orow = b.obj + size_t(x + o.x) * b.Y + o.y;
@@ -134,15 +132,15 @@ __device__ __forceinline__ void dm_item_inv(const DMBuffers& b, int p, int slot,
     const int n = t + T * e;
     const float2 pn = a[out_slot<L>(e)];
     st_stream(psrow + n, pn);
+    // the increments are accumulated unscaled: finalize multiplies the sums by f1 (object) and f0 (probe), which as
+    // positive factors commute with the phase clamp
     const float2 pv = prow[n];
     float2 inc = cconjmul(pv, pn);
-    inc = make_float2(inc.x * f1, inc.y * f1);
     if constexpr (PC) inc = constrain_phase(inc);
     atomicAdd(dorow + n, inc);
     if constexpr (UP) {
       const float2 ov = orow[n];
-      const float2 pi = cconjmul(ov, pn);
-      atomicAdd(dprow + n, make_float2(pi.x * f0, pi.y * f0));
+      atomicAdd(dprow + n, cconjmul(ov, pn));
     }
   });
 }
@@ -182,56 +180,16 @@ __global__ void __launch_bounds__(DMShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS_INV)
     dm_item_inv<L, PC, UP>(b, w.slot_pat[item / NB], item / NB, item % NB, smem + L, smem);
 }
 
-// Skewed pipeline: launch k of an iteration runs the row items of wave k, the column items of wave k-1 and the inverse
-// items of wave k-2 (DMSkew), so an iteration is waves + 2 launches instead of 3 x waves and every launch mixes the
-// three kinds of work.  The row items depend on nothing the previous launch writes (psi of other patterns, the
-// iteration's snapshot of O and P, a W1 buffer of three that the previous launch neither reads nor writes), so they
-// run first, while the previous launch may still be finishing (programmatic dependent launch); the column and inverse
-// items wait for it (griddepcontrol.wait) and alternate item by item.  A launch lets the next one start only once all
-// its CTAs are past that wait, so at most two launches overlap (this one's second phase, the next one's row items):
-// three W1 buffers (rows k, cols k-1, the next launch's rows k+1) and two W2 buffers (cols k-1, inverse k-2) suffice.
-template <int L, bool PC, bool UP>
-__global__ void __launch_bounds__(DMShape<L>::THREADS, DMOcc<L>::MIN_BLOCKS)
-    k_dm_skew(const DMBuffers b, const DMSkew k) {
-  constexpr int NB = DMShape<L>::NB;
-  extern __shared__ float4 smem4[];
-  float2* smem = reinterpret_cast<float2*>(smem4);
-  if (k.first) asm volatile("griddepcontrol.wait;" ::: "memory");
-  load_twiddles<L>(smem, b.tw);
-  __syncthreads();
-  for (int item = blockIdx.x; item < NB * k.rows_count; item += gridDim.x)
-    dm_item_rows<L>(b, k.rows_pat[item / NB], k.rows_w1 + item / NB, item % NB, smem + L, smem);
-  if (!k.first) asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  const int nc = NB * k.cols_count, ni = NB * k.inv_count, n = nc + ni;
-  for (int q = blockIdx.x; q < n; q += gridDim.x) {
-    // alternate column and inverse items while both remain
-    const int m = nc < ni ? nc : ni;
-    int kind, item;
-    if (q < 2 * m) {
-      kind = q & 1;
-      item = q >> 1;
-    } else {
-      kind = nc > ni ? 0 : 1;
-      item = q - m;
-    }
-    if (kind == 0)
-      dm_item_cols<L>(b, k.cols_pat[item / NB], k.cols_w1 + item / NB, k.cols_w2 + item / NB, item % NB, smem + L,
-                      smem);
-    else
-      dm_item_inv<L, PC, UP>(b, k.inv_pat[item / NB], k.inv_w2 + item / NB, item % NB, smem + L, smem);
-  }
-}
-
 // O += dO, P += dP (mode 0), reset the accumulators, and sum |O|^2 and |P|^2 over all stacked probe modes.
 __global__ void k_dm_finalize(float2* __restrict__ obj, float2* __restrict__ dO, size_t nobj,
                               float2* __restrict__ probe, float2* __restrict__ dP, size_t nprobe0, size_t nprobe,
-                              int updateProbe, double* __restrict__ sums) {
+                              int updateProbe, double* __restrict__ sums, const double* __restrict__ fac) {
   double so = 0, sp = 0;
+  const float f0 = float(fac[0]), f1 = float(fac[1]);
   const size_t stride = size_t(gridDim.x) * blockDim.x;
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < nobj; i += stride) {
     float2 v = obj[i], d = dO[i];
-    v = cadd(v, d);
+    v = cadd(v, cscale(d, f1));
     obj[i] = v;
     dO[i] = make_float2(0.f, 0.f);
     float m = sqrtf(v.x * v.x + v.y * v.y);
@@ -240,7 +198,7 @@ __global__ void k_dm_finalize(float2* __restrict__ obj, float2* __restrict__ dO,
   for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < nprobe; i += stride) {
     float2 v = probe[i];
     if (updateProbe && i < nprobe0) {
-      v = cadd(v, dP[i]);
+      v = cadd(v, cscale(dP[i], f0));
       probe[i] = v;
       dP[i] = make_float2(0.f, 0.f);
     }
@@ -273,11 +231,9 @@ __global__ void k_dm_factors(double* __restrict__ sums, double* __restrict__ fac
 template <int L>
 static cudaError_t dm_prepare_t() {
   const int sm = int(DMShape<L>::SMEM);
-  const void* fns[10] = {(const void*)k_dm_rows<L>, (const void*)k_dm_cols<L>, (const void*)k_dm_inv<L, false, false>,
-                         (const void*)k_dm_inv<L, false, true>, (const void*)k_dm_inv<L, true, false>,
-                         (const void*)k_dm_inv<L, true, true>, (const void*)k_dm_skew<L, false, false>,
-                         (const void*)k_dm_skew<L, false, true>, (const void*)k_dm_skew<L, true, false>,
-                         (const void*)k_dm_skew<L, true, true>};
+  const void* fns[6] = {(const void*)k_dm_rows<L>, (const void*)k_dm_cols<L>, (const void*)k_dm_inv<L, false, false>,
+                        (const void*)k_dm_inv<L, false, true>, (const void*)k_dm_inv<L, true, false>,
+                        (const void*)k_dm_inv<L, true, true>};
   for (const void* f : fns) {
     const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
@@ -363,57 +319,11 @@ cudaError_t dm_wave(const DMBuffers& b, const DMWave& w, bool pc, bool up, cudaS
   }
 }
 
-template <int L>
-static int dm_slots_skew() {
-  static const int s = resident_slots(k_dm_skew<L, true, true>, DMShape<L>::THREADS, DMShape<L>::SMEM);
-  return s;
-}
-
-template <int L>
-static cudaError_t dm_skew_t(const DMBuffers& b, const DMSkew& k, bool pc, bool up, cudaStream_t st,
-                             int64_t* launches) {
-  constexpr int NT = DMShape<L>::THREADS, NB = DMShape<L>::NB;
-  const int items = NB * (k.rows_count + k.cols_count + k.inv_count);
-  if (items == 0) return cudaSuccess;
-  const dim3 grid(std::min(dm_slots_skew<L>(), items)), block(NT);
-  const size_t sm = DMShape<L>::SMEM;
-  cudaError_t e;
-  if (pc && up)
-    e = launch_pdl(k_dm_skew<L, true, true>, grid, block, sm, st, b, k);
-  else if (pc)
-    e = launch_pdl(k_dm_skew<L, true, false>, grid, block, sm, st, b, k);
-  else if (up)
-    e = launch_pdl(k_dm_skew<L, false, true>, grid, block, sm, st, b, k);
-  else
-    e = launch_pdl(k_dm_skew<L, false, false>, grid, block, sm, st, b, k);
-  if (launches) *launches += 1;
-  return e;
-}
-
-cudaError_t dm_skew(const DMBuffers& b, const DMSkew& k, bool pc, bool up, cudaStream_t st, int64_t* launches) {
-  switch (b.N) {
-    case 32: return dm_skew_t<32>(b, k, pc, up, st, launches);
-    case 64: return dm_skew_t<64>(b, k, pc, up, st, launches);
-    case 128: return dm_skew_t<128>(b, k, pc, up, st, launches);
-    case 256: return dm_skew_t<256>(b, k, pc, up, st, launches);
-    case 512: return dm_skew_t<512>(b, k, pc, up, st, launches);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-// Patterns per wave of the skewed pipeline: three W1 and two W2 buffers of a wave stay within ~48 MB of the L2.
-int dm_skew_wave_size(int N, int P) {
-  const size_t bytes_per_pattern = 5 * sizeof(float2) * size_t(N) * N;
-  const int maxwave = int(std::max<size_t>(1, (size_t(48) << 20) / bytes_per_pattern));
-  const int nwaves = (P + maxwave - 1) / maxwave;
-  return (P + nwaves - 1) / nwaves;
-}
-
 cudaError_t dm_finalize(const DMBuffers& b, bool up, cudaStream_t st, int64_t* launches) {
   const size_t nobj = size_t(b.X) * b.Y, np0 = size_t(b.N) * b.N, np = np0 * b.K;
   int grid = int((nobj + 255) / 256);
   if (grid > 1184) grid = 1184;
-  k_dm_finalize<<<grid, 256, 0, st>>>(b.obj, b.dO, nobj, b.probe, b.dP, np0, np, up ? 1 : 0, b.sums);
+  k_dm_finalize<<<grid, 256, 0, st>>>(b.obj, b.dO, nobj, b.probe, b.dP, np0, np, up ? 1 : 0, b.sums, b.fac);
   k_dm_factors<<<1, 32, 0, st>>>(b.sums, b.fac);
   if (launches) *launches += 2;
   return cudaGetLastError();

@@ -819,15 +819,13 @@ void init_dm(pty_session* s) {
   check_cuda(cudaMemsetAsync(s->dP.p, 0, s->dP.bytes, s->stream), "memset dP");
   // wave: patterns per pipeline pass (W1 + W2 = 2 * wave * 8N^2 bytes)
   check_cuda(dm_prepare(s->N), "DM kernel set-up");
-  need(s->prm.pipeline >= 0 && s->prm.pipeline <= 2, "pipeline must be 0, 1 or 2");
-  s->skew = s->prm.pipeline == 2;
   int wave = s->prm.wave;
-  if (wave <= 0) wave = s->skew ? dm_skew_wave_size(s->N, s->P) : dm_wave_size(s->N, s->P);
+  if (wave <= 0) wave = dm_wave_size(s->N, s->P);
   wave = std::min(wave, s->P);
   s->wave = wave;
   s->nwaves = (s->P + wave - 1) / wave;
-  s->W1.alloc(sizeof(float2) * NN * wave * (s->skew ? 3 : 1), "W1");
-  s->W2.alloc(sizeof(float2) * NN * wave * (s->skew ? 2 : 1), "W2");
+  s->W1.alloc(sizeof(float2) * NN * wave, "W1");
+  s->W2.alloc(sizeof(float2) * NN * wave, "W2");
   std::vector<int> slots(s->P);
   for (int i = 0; i < s->P; ++i) slots[i] = i;
   s->slots.alloc(sizeof(int) * s->P, "slots");
@@ -1219,47 +1217,19 @@ DMBuffers dm_buffers(pty_session* s) {
   return b;
 }
 
-// The passes of one DM iteration over all waves (without finalize): per wave three launches, or the skewed pipeline's
-// waves + 2 launches.
+// The passes of one DM iteration over all waves (without finalize): three launches per wave.
 cudaError_t dm_enqueue_waves(pty_session* s, const DMBuffers& b, bool pc, bool up) {
-  const int W = s->nwaves, wave = s->wave;
-  const int* slots = s->slots.as<int>();
-  auto count = [&](int w) { return std::min(wave, s->P - w * wave); };
   cudaError_t err = cudaSuccess;
-  if (!s->skew) {
-    for (int w = 0; w < W && err == cudaSuccess; ++w) {
-      DMWave wv;
-      wv.slot_pat = slots + size_t(w) * wave;
-      wv.count = count(w);
-      err = dm_wave(b, wv, pc, up, s->stream, nullptr);
-    }
-    return err;
-  }
-  for (int k = 0; k < W + 2 && err == cudaSuccess; ++k) {
-    DMSkew d = {};
-    if (k < W) {
-      d.rows_pat = slots + size_t(k) * wave;
-      d.rows_count = count(k);
-      d.rows_w1 = (k % 3) * wave;
-    }
-    if (k >= 1 && k - 1 < W) {
-      d.cols_pat = slots + size_t(k - 1) * wave;
-      d.cols_count = count(k - 1);
-      d.cols_w1 = ((k - 1) % 3) * wave;
-      d.cols_w2 = ((k - 1) % 2) * wave;
-    }
-    if (k >= 2) {
-      d.inv_pat = slots + size_t(k - 2) * wave;
-      d.inv_count = count(k - 2);
-      d.inv_w2 = ((k - 2) % 2) * wave;
-    }
-    d.first = k == 0 ? 1 : 0;
-    err = dm_skew(b, d, pc, up, s->stream, nullptr);
+  for (int w = 0; w < s->nwaves && err == cudaSuccess; ++w) {
+    DMWave wv;
+    wv.slot_pat = s->slots.as<int>() + size_t(w) * s->wave;
+    wv.count = std::min(s->wave, s->P - w * s->wave);
+    err = dm_wave(b, wv, pc, up, s->stream, nullptr);
   }
   return err;
 }
 
-int64_t dm_wave_launches(const pty_session* s) { return s->skew ? s->nwaves + 2 : 3 * int64_t(s->nwaves); }
+int64_t dm_wave_launches(const pty_session* s) { return 3 * int64_t(s->nwaves); }
 
 // One DM iteration: waves of (fwd_rows, cols, inv_rows) then finalize, replayed from a CUDA graph per flag state.
 void step_dm(pty_session* s, int it) {

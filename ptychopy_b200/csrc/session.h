@@ -116,7 +116,6 @@ struct pty_session {
   // DM
   pty::DeviceBuf psi, dO, dP, W1, W2, slots;
   int wave = 0, nwaves = 0;
-  bool skew = false;  // DM: skewed pipeline (one launch per wave, three W1 and two W2 buffers of `wave` patterns)
   cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
   // position sharding (DM over several GPUs): this session holds positions [shard_first, shard_first + P) of a scan
   // of shard_total positions; local step (waves) and finish (apply the summed increments) are separate graphs

@@ -76,20 +76,3 @@ def test_dm_config_size_first_iteration():
         exp[ox:ox + N, oy:oy + N] += inc
     assert np.isfinite(got).all()
     assert rel_err(got, exp) < TOL
-
-
-@pytest.mark.parametrize("N,nx,wave", [(64, 5, 0), (64, 5, 1), (64, 5, 3), (64, 5, 7), (32, 6, 4), (512, 3, 2)])
-def test_dm_skewed_pipeline_matches_oracle(oracle, N, nx, wave):
-    """pipeline=2: one launch per wave mixing the row pass of wave k, the column pass of wave k-1 and the inverse pass
-    of wave k-2 (programmatic dependent launch between them); ragged and single-pattern waves included."""
-    d = dataset(N=N, nx=nx, algorithm="DM", fwhm_px=39.0 if N == 512 else 10.0)
-    s = gpu_session(d, probe=d["probe"], updateProbe=2, phaseConstraint=1, pipeline=2, wave=wave)
-    o = oracle.OracleSession("DM", d["amp"], d["pos"], np.zeros((d["X"], d["Y"])), d["probe"], probe_guess_path=False,
-                             updateProbe=2, phaseConstraint=1, nthreads=8)
-    for it in range(1, 5):
-        s.step()
-        o.step()
-        ob, pr, _ = o.state()
-        assert rel_err(s.object(), ob) < TOL, f"object, iteration {it}"
-        assert rel_err(s.probe(), pr) < TOL, f"probe, iteration {it}"
-    s.close()
