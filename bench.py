@@ -242,7 +242,10 @@ def run_reference(args, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * n / value, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "N": 512, "positions": 900, "parallelism": "host threads"},
+        "config": {"workload": WORKLOAD, "N": 512, "positions": 900, "object": [ds["X"], ds["Y"]],
+                   "step": "one DM iteration over all 900 patterns",
+                   "l2": "inputs larger than L2 (exit waves 1.89 GB + amplitudes 0.94 GB per step)",
+                   "parallelism": "single GPU"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's CUDA sources do not build with CUDA 12.9; its DM is restated as a multithreaded "
@@ -391,9 +394,13 @@ def run_b200(args, rank, world, local):
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": kind,
                          "kernel": "DM iteration graph (k_dm_rows, k_dm_cols, k_dm_inv per wave + finalize)",
                          "algorithmic_bytes_per_step": bytes_step},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(amp_host.nbytes),
-                    "d2h_bytes_per_step": int(d2h),
-                    "step": f"ptychopy.dmnp(iter={args.e2e_iters}) from pinned host patterns, results to host"},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": int(amp_host.nbytes) // args.e2e_iters,
+                    "d2h_bytes_per_step": int(d2h) // args.e2e_iters,
+                    "h2d_bytes_per_call": int(amp_host.nbytes), "d2h_bytes_per_call": int(d2h),
+                    "step": f"one DM iteration; each ptychopy.dmnp(iter={args.e2e_iters}) call uploads the patterns "
+                            "from pinned host memory once and returns object and probe to the host, so the per-step "
+                            "copies are the call's divided by its iterations"},
             "gpu_launches": int(launches), "clocks": ck, "finite": finite,
         }
         if world == 1 and not args.no_cpu:
@@ -666,7 +673,8 @@ def run_nrmse(args, rank, local):
                                              "true probe given, zero object",
                                  "nrmse": "phase NRMSE after offset and linear-ramp removal over the central region "
                                           "(N/2 margin), checked every 5 iterations"},
-                      "note": "the learned warm start (the other half of the comparison) is not built"}), flush=True)
+                      "note": "the plain half of the comparison; bench.py --algo warm measures both halves"}),
+          flush=True)
 
 
 def run_warm(args, rank, local, emit=True):
