@@ -84,7 +84,8 @@ def parse():
                     help="N>1: split the 900 positions over the GPUs (one NCCL all-reduce of the DM increments per "
                          "iteration, strong scaling) instead of independent replicas")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
-                    help="--algo epie: 1 runs the transforms as split-BF16 tensor-core stages (256^2)")
+                    help="--algo epie: 1 runs the transforms as split-BF16 tensor-core stages (256^2); --algo dm: "
+                         "1 runs the column pass's 32-point DFT stages as split-FP16 tensor-core GEMMs (512^2)")
     ap.add_argument("--cfg", default="epie128", choices=["epie128", "epie256k5", "dm512"],
                     help="ePIE configuration (dm512: ePIE on the 512^2 DM configuration's scan)")
     return ap.parse_args()
@@ -284,7 +285,7 @@ def run_b200(args, rank, world, local):
     N, P = ds["N"], ds["P"]
     stream = torch.cuda.Stream()
     shard = args.shard
-    s = abi.Session(**dict(ds["kwargs"], algorithm="DM", device=local, wave=args.wave))
+    s = abi.Session(**dict(ds["kwargs"], algorithm="DM", device=local, wave=args.wave, precision=args.precision))
     s.set_stream(stream.cuda_stream)
     if shard:
         bounds = [P * r // world for r in range(world + 1)]
@@ -360,7 +361,8 @@ def run_b200(args, rank, world, local):
     amp_host = host.numpy()
     del ds["amp"]
     torch.cuda.empty_cache()
-    kw = dict(ds["kwargs"], iter=args.e2e_iters, returnResults=1, writeResults=0, device=local, wave=args.wave)
+    kw = dict(ds["kwargs"], iter=args.e2e_iters, returnResults=1, writeResults=0, device=local, wave=args.wave,
+              precision=args.precision)
     pt.dmnp(diffractionNP=amp_host, **dict(kw, iter=2))  # warm-up call
     if dist:
         dist.barrier()
@@ -384,7 +386,8 @@ def run_b200(args, rank, world, local):
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; object GRF phase, 110 nm probe, Poisson)",
+            "vs_baseline": None, "dtype": "f32 (column DFT stages split-FP16 on tensor cores)" if args.precision else "f32",
+            "data": "synthetic (seeded; object GRF phase, 110 nm probe, Poisson)",
             "config": {"workload": WORKLOAD if args.nx == 30 else f"{WORKLOAD} (raster {args.nx}x{args.nx})",
                        "N": N, "positions": P, "object": [ds["X"], ds["Y"]],
                        "step": "one DM iteration over all 900 patterns",
@@ -392,7 +395,8 @@ def run_b200(args, rank, world, local):
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": kind,
-                         "kernel": "DM iteration graph (k_dm_rows, k_dm_cols, k_dm_inv per wave + finalize)",
+                         "kernel": "DM iteration graph (k_dm_rows, %s, k_dm_inv per wave + finalize)"
+                                   % ("k_dm_cols_tc" if args.precision else "k_dm_cols"),
                          "algorithmic_bytes_per_step": bytes_step},
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": int(amp_host.nbytes) // args.e2e_iters,

@@ -62,10 +62,15 @@ struct DMBuffers {
   const float2* tw;     // twiddles for N
   double* sums;         // [0] sum|O|^2, [1] sum|P|^2 (accumulated by finalize)
   double* fac;          // [0] 1/objMax, [1] 1/probeMax (hysteresis-cached), [2] objMax, [3] probeMax
+  int* err = nullptr;   // wait-timeout flag of the tensor-core column pass
   int N, K, X, Y;
+  int tc = 0;           // column pass on the tensor cores (N = 512)
 };
 // Sets the shared-memory attributes of the DM kernels for size N (call once, outside graph capture).
 cudaError_t dm_prepare(int N);
+// The DM column pass at N = 512 with its 32-point DFT stages as FP16-split tcgen05 GEMMs (b.tc, b.err set).
+cudaError_t dm_cols_tc_prepare();
+cudaError_t dm_cols_tc(const DMBuffers& b, const DMWave& w, cudaStream_t st);
 // Patterns per pipeline wave for size N (balanced waves, W1 + W2 <= 1 GiB).
 int dm_wave_size(int N, int P);
 cudaError_t dm_wave(const DMBuffers& b, const DMWave& w, bool phaseConstraint, bool updateProbe, cudaStream_t st,

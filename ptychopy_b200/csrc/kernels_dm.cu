@@ -229,6 +229,13 @@ __global__ void k_dm_factors(double* __restrict__ sums, double* __restrict__ fac
 }
 
 template <int L>
+static int dm_slots_rows();
+template <int L>
+static int dm_slots_cols();
+template <int L>
+static int dm_slots_inv();
+
+template <int L>
 static cudaError_t dm_prepare_t() {
   const int sm = int(DMShape<L>::SMEM);
   const void* fns[6] = {(const void*)k_dm_rows<L>, (const void*)k_dm_cols<L>, (const void*)k_dm_inv<L, false, false>,
@@ -238,7 +245,11 @@ static cudaError_t dm_prepare_t() {
     const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
   }
-  return cudaSuccess;
+  // the resident-slot counts, queried here, outside any stream capture
+  dm_slots_rows<L>();
+  dm_slots_cols<L>();
+  dm_slots_inv<L>();
+  return cudaGetLastError();
 }
 
 cudaError_t dm_prepare(int N) {
@@ -247,18 +258,21 @@ cudaError_t dm_prepare(int N) {
     case 64: return dm_prepare_t<64>();
     case 128: return dm_prepare_t<128>();
     case 256: return dm_prepare_t<256>();
-    case 512: return dm_prepare_t<512>();
+    case 512: {
+      const cudaError_t e = dm_prepare_t<512>();
+      return e != cudaSuccess ? e : dm_cols_tc_prepare();
+    }
     default: return cudaErrorInvalidValue;
   }
 }
 
-// Resident CTA slots of a DM kernel (once per kernel and size).
+// Resident CTA slots of a DM kernel (once per kernel and size; first asked by dm_prepare, outside stream capture).
 template <typename K>
 static int resident_slots(K kern, int threads, size_t smem) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem) != cudaSuccess) cudaGetLastError();
   return sms * (per > 0 ? per : 1);
 }
 template <int L>
@@ -285,7 +299,16 @@ static cudaError_t dm_wave_t(const DMBuffers& b, const DMWave& w, bool pc, bool 
   const int items = NB * w.count;
   const int grid = std::min(dm_slots_inv<L>(), items);
   k_dm_rows<L><<<std::min(dm_slots_rows<L>(), items), NT, SM, st>>>(b, w);
-  k_dm_cols<L><<<std::min(dm_slots_cols<L>(), items), NT, SM, st>>>(b, w);
+  if constexpr (L == 512) {
+    if (b.tc) {
+      const cudaError_t e = dm_cols_tc(b, w, st);
+      if (e != cudaSuccess) return e;
+    } else {
+      k_dm_cols<L><<<std::min(dm_slots_cols<L>(), items), NT, SM, st>>>(b, w);
+    }
+  } else {
+    k_dm_cols<L><<<std::min(dm_slots_cols<L>(), items), NT, SM, st>>>(b, w);
+  }
   if (pc && up)
     k_dm_inv<L, true, true><<<grid, NT, SM, st>>>(b, w);
   else if (pc)

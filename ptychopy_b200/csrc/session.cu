@@ -43,27 +43,36 @@ void need_device_index(int d) {
 
 // Freed device blocks are kept per device and handed to the next request of at least their size and at most a
 // quarter more: cudaFree of a DM session's buffers (about 3 GB at 512^2 x 900 patterns) unmaps the memory and took
-// 10-160 ms, up to a third of a 100-iteration dmnp call, and the next session mapped it again.  A block enters the
-// cache after a device synchronisation (the ordering cudaFree gives).  pty_release_cached_memory returns the cache
-// to the driver; so does an allocation that fails, before its one retry.
+// 10-160 ms, up to a third of a 100-iteration dmnp call, and the next session mapped it again.
+// Ordering is per stream: inside a session's call the calling thread is bound to the session's stream (set_device;
+// guarded() restores the previous binding on return), a freed block enters the cache with an event recorded on that stream after its last use, and the next taker waits
+// for that event on its own stream; a new buffer is cleared on the bound stream and that stream alone is
+// synchronised.  Without a bound stream (the stand-alone entry points) both fall back to a device synchronisation.
+// pty_release_cached_memory returns the cache to the driver; so does an allocation that fails, before its one retry.
 namespace {
 constexpr int kMaxDevices = 64;
+struct CachedBlock {
+  void* p;
+  cudaEvent_t ready;  // recorded after the block's last use, or null (already idle)
+};
 std::mutex g_cache_mu;
-std::multimap<size_t, void*> g_cache[kMaxDevices];
+std::multimap<size_t, CachedBlock> g_cache[kMaxDevices];
+thread_local cudaStream_t t_stream = nullptr;
 
-void* cache_take(int dev, size_t n, size_t* cap) {
+void* cache_take(int dev, size_t n, size_t* cap, cudaEvent_t* ready) {
   std::lock_guard<std::mutex> lk(g_cache_mu);
   auto& c = g_cache[dev];
   auto it = c.lower_bound(n);
   if (it == c.end() || it->first > n + n / 4) return nullptr;
-  void* q = it->second;
+  void* q = it->second.p;
+  *ready = it->second.ready;
   *cap = it->first;
   c.erase(it);
   return q;
 }
 
 void cache_release(int dev) {
-  std::multimap<size_t, void*> blocks;
+  std::multimap<size_t, CachedBlock> blocks;
   {
     std::lock_guard<std::mutex> lk(g_cache_mu);
     blocks.swap(g_cache[dev]);
@@ -72,7 +81,13 @@ void cache_release(int dev) {
   int cur = 0;
   cudaGetDevice(&cur);
   if (cur != dev) cudaSetDevice(dev);
-  for (auto& kv : blocks) cudaFree(kv.second);
+  for (auto& kv : blocks) {
+    if (kv.second.ready) {
+      cudaEventSynchronize(kv.second.ready);
+      cudaEventDestroy(kv.second.ready);
+    }
+    cudaFree(kv.second.p);
+  }
   if (cur != dev) cudaSetDevice(cur);
 }
 }  // namespace
@@ -84,7 +99,16 @@ void DeviceBuf::alloc(size_t n, const char* what) {
   check_cuda(cudaGetDevice(&d), what);
   need_device_index(d);
   size_t got = 0;
-  void* q = cache_take(d, n, &got);
+  cudaEvent_t ready = nullptr;
+  void* q = cache_take(d, n, &got, &ready);
+  if (q && ready) {  // the block's last user may still be running
+    const cudaError_t e = t_stream ? cudaStreamWaitEvent(t_stream, ready, 0) : cudaEventSynchronize(ready);
+    cudaEventDestroy(ready);
+    if (e != cudaSuccess) {
+      cudaFree(q);
+      check_cuda(e, what);
+    }
+  }
   if (!q) {
     cudaError_t e = cudaMalloc(&q, n);
     if (e == cudaErrorMemoryAllocation) {  // give the cache back and try once more
@@ -97,9 +121,14 @@ void DeviceBuf::alloc(size_t n, const char* what) {
   }
   // every buffer starts at zero (accumulators, counters and padding rely on it), whether recycled or fresh (cudaMalloc
   // does not promise cleared memory: pages this process freed may come back as they were); complete before return,
-  // as the memset runs on the legacy stream, which the sessions' non-blocking streams do not order against
-  check_cuda(cudaMemset(q, 0, n), what);
-  check_cuda(cudaDeviceSynchronize(), what);
+  // since synchronous copies on the legacy stream are not ordered against the sessions' non-blocking streams
+  if (t_stream) {
+    check_cuda(cudaMemsetAsync(q, 0, n, t_stream), what);
+    check_cuda(cudaStreamSynchronize(t_stream), what);
+  } else {
+    check_cuda(cudaMemset(q, 0, n), what);
+    check_cuda(cudaDeviceSynchronize(), what);
+  }
   p = q;
   bytes = n;
   cap = got;
@@ -112,10 +141,20 @@ void DeviceBuf::free() {
     int cur = 0;
     cudaGetDevice(&cur);
     if (cur != dev) cudaSetDevice(dev);
-    cudaDeviceSynchronize();
+    cudaEvent_t ready = nullptr;
+    if (t_stream && cur == dev && cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) == cudaSuccess) {
+      if (cudaEventRecord(ready, t_stream) != cudaSuccess) {
+        cudaEventDestroy(ready);
+        ready = nullptr;
+        cudaDeviceSynchronize();
+      }
+    } else {
+      ready = nullptr;
+      cudaDeviceSynchronize();
+    }
     {
       std::lock_guard<std::mutex> lk(g_cache_mu);
-      g_cache[dev].emplace(cap, p);
+      g_cache[dev].emplace(cap, CachedBlock{p, ready});
     }
     if (cur != dev) cudaSetDevice(cur);
   }
@@ -491,6 +530,10 @@ namespace {
 
 template <typename F>
 int guarded(F&& f) {
+  struct Rebind {  // the caller's stream binding, back in place however f ends
+    cudaStream_t saved = t_stream;
+    ~Rebind() { t_stream = saved; }
+  } rebind;
   try {
     f();
     g_last_error.clear();
@@ -511,7 +554,11 @@ void need(bool cond, const std::string& msg, int code = PTY_ERR_INVALID) {
   if (!cond) fail(code, msg);
 }
 
-void set_device(pty_session* s) { check_cuda(cudaSetDevice(s->dev), "cudaSetDevice"); }
+// The session's device, and its stream as the order for the device buffers allocated and freed from here on.
+void set_device(pty_session* s) {
+  check_cuda(cudaSetDevice(s->dev), "cudaSetDevice");
+  t_stream = s->stream;
+}
 
 // A session's own stream.  MLs and ePIE are chains of small dependent kernels whose time is their latency; DM runs
 // few large kernels.  The chains get the device's highest stream priority, so that beside other sessions (a batch)
@@ -819,6 +866,7 @@ void init_dm(pty_session* s) {
   check_cuda(cudaMemsetAsync(s->dP.p, 0, s->dP.bytes, s->stream), "memset dP");
   // wave: patterns per pipeline pass (W1 + W2 = 2 * wave * 8N^2 bytes)
   check_cuda(dm_prepare(s->N), "DM kernel set-up");
+  if (s->prm.precision) s->dm_err.alloc(sizeof(int), "DM wait flag");
   int wave = s->prm.wave;
   if (wave <= 0) wave = dm_wave_size(s->N, s->P);
   wave = std::min(wave, s->P);
@@ -1210,6 +1258,8 @@ DMBuffers dm_buffers(pty_session* s) {
   b.tw = s->tw.as<float2>();
   b.sums = s->scal.as<double>();
   b.fac = s->scal.as<double>() + 2;
+  b.tc = s->prm.precision ? 1 : 0;
+  b.err = s->prm.precision ? s->dm_err.as<int>() : nullptr;
   b.N = s->N;
   b.K = s->K;
   b.X = s->X;
@@ -1230,6 +1280,16 @@ cudaError_t dm_enqueue_waves(pty_session* s, const DMBuffers& b, bool pc, bool u
 }
 
 int64_t dm_wave_launches(const pty_session* s) { return 3 * int64_t(s->nwaves); }
+
+// The tensor-core column pass (precision = 1) reports an expired wait through the session's device flag, read where
+// the host synchronises anyway (end of pty_run, results, finish of a shard step).
+void dm_check_flag(pty_session* s) {
+  if (s->algo != ALGO_DM || !s->prm.precision || !s->dm_err.p) return;
+  int flag = 0;
+  check_cuda(cudaMemcpyAsync(&flag, s->dm_err.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H flag");
+  check_cuda(cudaStreamSynchronize(s->stream), "DM iteration");
+  need(flag == 0, "DM: a tensor-core wait timed out (the iteration did not complete)", PTY_ERR_CUDA);
+}
 
 // One DM iteration: waves of (fwd_rows, cols, inv_rows) then finalize, replayed from a CUDA graph per flag state.
 void step_dm(pty_session* s, int it) {
@@ -1439,6 +1499,7 @@ double step_epie(pty_session* s, int it, bool want_err) {
 void destroy_session(pty_session* s) {
   if (!s) return;
   cudaSetDevice(s->dev);
+  t_stream = s->stream;
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (auto& g : s->graphs)
     if (g) cudaGraphExecDestroy(g);
@@ -1464,6 +1525,7 @@ void destroy_session(pty_session* s) {
   s->W1.free();
   s->W2.free();
   s->slots.free();
+  t_stream = nullptr;
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -1649,8 +1711,8 @@ int pty_init(pty_session* s) {
     s->tw.p = twp;  // allocated by make_twiddles; the cache takes it back like any block
     s->tw.bytes = s->tw.cap = sizeof(float2) * s->N;
     s->tw.dev = s->dev;
-    need(s->algo != ALGO_DM || p.precision == 0,
-         "precision=1 applies to MLs and ePIE: DM fuses its FP32 transforms into its kernels", PTY_ERR_UNSUPPORTED);
+    need(s->algo != ALGO_DM || p.precision == 0 || s->N == 512,
+         "precision=1 for DM (tensor-core column pass) needs 512 x 512 patterns", PTY_ERR_UNSUPPORTED);
     if (s->algo == ALGO_MLS) {
       need(s->warm_params.empty(), "the learned warm start is for ePIE and DM sessions", PTY_ERR_UNSUPPORTED);
       init_mls(s);
@@ -1758,6 +1820,7 @@ int pty_run(pty_session* s, int iters, double* errs) {
       }
     }
     check_cuda(cudaStreamSynchronize(s->stream), "pty_run");
+    dm_check_flag(s);
   });
 }
 
@@ -1800,6 +1863,7 @@ int pty_dm_step_finish(pty_session* s) {
     need(s->pending_iter > 0, "pty_dm_step_local has not run", PTY_ERR_STATE);
     set_device(s);
     step_dm_finish(s, s->pending_iter);
+    dm_check_flag(s);
     s->iter = s->pending_iter;
     s->pending_iter = 0;
   });
@@ -1893,6 +1957,7 @@ int pty_batch_run(pty_session* const* sessions, int n, int iters) {
     for (int it = 0; it < iters; ++it)
       for (int i = 0; i < n; ++i) {
         pty_session* s = sessions[i];
+        t_stream = s->stream;
         const int k = s->iter + 1;
         if (s->algo == ALGO_EPIE)
           step_epie(s, k, false);
@@ -1903,6 +1968,7 @@ int pty_batch_run(pty_session* const* sessions, int n, int iters) {
         s->iter = k;
       }
     for (int i = 0; i < n; ++i) check_cuda(cudaStreamSynchronize(sessions[i]->stream), "pty_batch_run");
+    for (int i = 0; i < n; ++i) dm_check_flag(sessions[i]);
   });
 }
 
@@ -1926,6 +1992,7 @@ int pty_get_object(pty_session* s, float* out, int X, int Y) {
     check_cuda(cudaMemcpyAsync(out, s->obj.p, sizeof(float2) * size_t(X) * Y, cudaMemcpyDeviceToHost, s->stream),
                "D2H object");
     check_cuda(cudaStreamSynchronize(s->stream), "D2H object");
+    dm_check_flag(s);
   });
 }
 
@@ -1960,6 +2027,7 @@ int pty_get_probe(pty_session* s, float* out, int K, int N) {
                                s->stream),
                "D2H probe");
     check_cuda(cudaStreamSynchronize(s->stream), "D2H probe");
+    dm_check_flag(s);
   });
 }
 

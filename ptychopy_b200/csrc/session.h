@@ -115,6 +115,7 @@ struct pty_session {
   pty::DeviceBuf tw, dOffs, scal;
   // DM
   pty::DeviceBuf psi, dO, dP, W1, W2, slots;
+  pty::DeviceBuf dm_err;  // wait-timeout flag of the tensor-core column pass (precision = 1)
   int wave = 0, nwaves = 0;
   cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
   // position sharding (DM over several GPUs): this session holds positions [shard_first, shard_first + P) of a scan
