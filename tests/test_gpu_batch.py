@@ -14,13 +14,19 @@ TOL = 1e-5  # float atomics accumulate in a different order when scans overlap o
 def _scans(oracle):
     d1 = dataset(N=64, nx=5, algorithm="DM")
     d2 = dataset(N=128, nx=3, algorithm="DM", seed=5)
+    d3 = dataset(N=64, nx=3, algorithm="DM", seed=7)
+    d4 = dataset(N=64, nx=4, algorithm="DM", seed=8)
     m1 = mls_dataset(oracle, N=32, nx=11)
     m2 = mls_dataset(oracle, N=64, nx=4, seed=9)
     e1 = dataset(N=32, nx=4, algorithm="ePIE", seed=6)
 
     def make():
+        # three DM scans of one size with different phase-constraint and probe schedules; d4 runs in four waves
+        # (5 + 5 + 5 + 1 patterns)
         return [gpu_session(d1, probe=d1["probe"], updateProbe=2),
                 gpu_session(d2, probe=d2["probe"]),
+                gpu_session(d3, probe=d3["probe"], updateProbe=2, phaseConstraint=2),
+                gpu_session(d4, probe=d4["probe"], updateProbe=3, wave=5),
                 gpu_session(dict(amp=m1["intens"], kw=m1["kw"]), probe=m1["probe"], obj=m1["obj"]),
                 gpu_session(dict(amp=m2["intens"], kw=m2["kw"]), probe=m2["probe"], obj=m2["obj"]),
                 gpu_session(e1, probe=e1["probe"], updateProbe=2)]
