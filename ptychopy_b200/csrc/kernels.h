@@ -71,7 +71,7 @@ cudaError_t dm_prepare(int N);
 // The DM column pass at N = 512 with its 32-point DFT stages as FP16-split tcgen05 GEMMs (b.tc, b.err set).
 cudaError_t dm_cols_tc_prepare();
 cudaError_t dm_cols_tc(const DMBuffers& b, const DMWave& w, cudaStream_t st);
-// Patterns per pipeline wave for size N (balanced waves, W1 + W2 <= 1 GiB).
+// Patterns per pipeline wave for size N (balanced waves, at least eight for large scans; two lanes of W1 + W2 <= 1 GiB).
 int dm_wave_size(int N, int P);
 cudaError_t dm_wave(const DMBuffers& b, const DMWave& w, bool phaseConstraint, bool updateProbe, cudaStream_t st,
                     int64_t* launches);

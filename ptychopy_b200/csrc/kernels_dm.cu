@@ -321,14 +321,31 @@ static cudaError_t dm_wave_t(const DMBuffers& b, const DMWave& w, bool pc, bool 
   return cudaGetLastError();
 }
 
-// Patterns per wave: the largest balanced wave with W1 + W2 within 1 GiB.  The kernels are bound by their on-chip
-// work (shared memory, L1, issue), so fewer, larger waves (less launch and tail overhead) beat L2-resident small
-// ones.
+template <int L>
+static int dm_wave_size_t(int P) {
+  const size_t bytes_per_pattern = 2 * sizeof(float2) * size_t(L) * L;
+  const int maxwave = int(std::max<size_t>(1, (size_t(1) << 29) / bytes_per_pattern));
+  int nw = (P + maxwave - 1) / maxwave;
+  const int by_items = int(size_t(P) * DMShape<L>::NB / (2 * size_t(dm_slots_inv<L>())));
+  nw = std::max(nw, std::min(8, by_items));
+  nw = std::max(1, std::min(nw, P));
+  return (P + nw - 1) / nw;
+}
+
+// Patterns per wave: balanced waves, at least eight where each still holds two persistent grids' worth of items, and
+// W1 + W2 of the two lanes of waves in flight within 1 GiB.  The kernels are bound by their on-chip work (shared
+// memory, L1, issue), not by the W1 / W2 traffic: with one lane, waves small enough for W1 + W2 to stay in L2 lost
+// more to the per-wave tails of three dependent launches than they saved (25 / 50 / 75 / 225 patterns: 3.55 / 3.35 /
+// 3.25 / 3.11 ms per 900 x 512^2 iteration); with two lanes each wave's kernels fill the other's tails.
 int dm_wave_size(int N, int P) {
-  const size_t bytes_per_pattern = 2 * sizeof(float2) * size_t(N) * N;
-  const int maxwave = int(std::max<size_t>(1, (size_t(1) << 30) / bytes_per_pattern));
-  const int nwaves = (P + maxwave - 1) / maxwave;
-  return (P + nwaves - 1) / nwaves;
+  switch (N) {
+    case 32: return dm_wave_size_t<32>(P);
+    case 64: return dm_wave_size_t<64>(P);
+    case 128: return dm_wave_size_t<128>(P);
+    case 256: return dm_wave_size_t<256>(P);
+    case 512: return dm_wave_size_t<512>(P);
+    default: return std::max(1, P);
+  }
 }
 
 cudaError_t dm_wave(const DMBuffers& b, const DMWave& w, bool pc, bool up, cudaStream_t st, int64_t* launches) {

@@ -115,6 +115,9 @@ struct pty_session {
   pty::DeviceBuf tw, dOffs, scal;
   // DM
   pty::DeviceBuf psi, dO, dP, W1, W2, slots;
+  int dm_lanes = 1;                // waves in flight side by side (W1 / W2 hold one wave per lane)
+  cudaStream_t dm_side = nullptr;  // the second lane's stream (forked from and joined to the session's stream)
+  cudaEvent_t dm_fork = nullptr, dm_join = nullptr;
   pty::DeviceBuf dm_err;  // wait-timeout flag of the tensor-core column pass (precision = 1)
   int wave = 0, nwaves = 0;
   cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
