@@ -344,6 +344,165 @@ __global__ void __launch_bounds__(TC_THREADS, 5)  // 5 CTAs per SM for the narro
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
+// ---- 3x3 convolution as nine shifted GEMMs (Cin in {16, 32, 64}; the packed weights resident in shared memory) ----
+// A CTA tile is 16 rows x 8 columns of output pixels of one image (M = 128, GEMM row m = 8 * row + column).  Its
+// input halo (18 x 10 pixels, zero outside the image; for an upsampled input each halo pixel is read from its source
+// pixel) is copied into shared memory once, as Cin / 8 planes of 18 x 10 16-byte pixel chunks (8 channels each).  For
+// tap (dy, dx) the 128 x 16 A operand of channel chunks (2j, 2j + 1) is then the canonical K-major no-swizzle matrix
+// that starts at plane 2j, halo row dy, halo column dx: its 8-row core matrices are 8 consecutive pixels of one halo
+// row (128 contiguous bytes), one halo row (160 B) apart, and its two K halves one plane apart.  So the nine taps need
+// no im2col copy, only nine descriptors, and the packed weights ([k / 8][n][8], k = tap * Cin + ci) are the B
+// operands as they stand.  The halo loads of the next two tiles (cp.async, zero-fill outside the image) overlap the
+// current tile's MMAs and epilogue.
+constexpr int TAP_ROWS = 16, TAP_COLS = 8, HALO_R = TAP_ROWS + 2, HALO_C = TAP_COLS + 2;
+constexpr int HALO_PLANE = HALO_R * HALO_C * 16;  // 2880 B
+constexpr int TAP_MAX_W_BYTES = 40 * 1024;          // packed weights resident per CTA
+constexpr int TAP_NBUF = 3;                           // halo buffers: two tiles' loads in flight behind the current
+__host__ __device__ constexpr int tap_smem(int Cin, int Npad) {
+  return Npad * 9 * Cin * 2 + TAP_NBUF * (Cin / 8) * HALO_PLANE + 64;  // weights, halo buffers, the mbarrier
+}
+
+template <int Cin>
+__global__ void __launch_bounds__(TC_THREADS, 4)
+    k_conv_tap(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wpk,
+               const float* __restrict__ bias, __nv_bfloat16* __restrict__ y, int B, int H, int W, int Cout,
+               int relu, int in_mode, int out_mode, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_skip;
+  __shared__ float s_bias[TC_MAX_N];
+  constexpr int chunks = Cin / 8;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wbytes = Cout * 9 * Cin * 2;
+  const uint32_t sbase = smem_u32(smem);
+  const uint32_t w_s = sbase, h_s = sbase + uint32_t(wbytes), hsz = uint32_t(chunks * HALO_PLANE);
+  const uint32_t bar = h_s + TAP_NBUF * hsz;
+  const int tiles_x = W / TAP_COLS, per_img = tiles_x * (H / TAP_ROWS);
+  const long long ntiles = (long long)B * per_img;
+  const uint32_t ncols = Cout <= 32 ? 32u : (Cout <= 64 ? 64u : (Cout <= 128 ? 128u : 256u));
+  const uint32_t idesc = umma_idesc_bf16(TC_M, Cout);
+  if (tid == 0) s_skip = *reinterpret_cast<volatile int*>(err);
+  __syncthreads();
+  if (s_skip || (long long)blockIdx.x >= ntiles) return;  // uniform across the CTA
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&s_tmem)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  for (int q = tid; q < Cout; q += TC_THREADS) s_bias[q] = bias[q];
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  const int Hs = in_mode == 1 ? H / 2 : H, Ws = in_mode == 1 ? W / 2 : W;  // stored input size
+
+  auto load_halo = [&](long long tile, uint32_t dst) {
+    const int b = int(tile / per_img), rem = int(tile - (long long)b * per_img);
+    const int y0 = (rem / tiles_x) * TAP_ROWS - 1, x0 = (rem % tiles_x) * TAP_COLS - 1;
+    for (int q = tid; q < HALO_R * HALO_C * chunks; q += TC_THREADS) {
+      const int j = q % chunks, pix = q / chunks, hy = pix / HALO_C, hx = pix - hy * HALO_C;
+      int sy = y0 + hy, sx = x0 + hx;
+      const bool v = sy >= 0 && sy < H && sx >= 0 && sx < W;
+      if (in_mode == 1) {
+        sy >>= 1;
+        sx >>= 1;
+      }
+      const __nv_bfloat16* src = v ? x + (((long long)b * Hs + sy) * Ws + sx) * Cin + 8 * j : x;
+      cp_async16_l1(dst + uint32_t(j * HALO_PLANE + (hy * HALO_C + hx) * 16), src, v);
+    }
+  };
+
+  const long long my_tiles = (ntiles - 1 - blockIdx.x) / gridDim.x + 1;
+  // cp.async groups: weights with tile 0's halo, then one group per tile (empty past the end), so that before tile i
+  // exactly TAP_NBUF - 2 younger groups may still be pending
+  for (int q = tid; q < wbytes / 16; q += TC_THREADS) cp_async16_cg(w_s + uint32_t(q * 16), wpk + size_t(q) * 8);
+  for (int k = 0; k < TAP_NBUF - 1; ++k) {
+    if (k < my_tiles) load_halo(blockIdx.x + k * (long long)gridDim.x, h_s + uint32_t(k) * hsz);
+    cp_async_commit();
+  }
+  bool ok = true;
+  uint32_t phase = 0;
+  for (long long i = 0; i < my_tiles; ++i) {
+    const long long tile = blockIdx.x + i * gridDim.x;
+    const uint32_t hcur = h_s + uint32_t(i % TAP_NBUF) * hsz;
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(TAP_NBUF - 2) : "memory");
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      int mm = 0;
+      for (int tap = 0; tap < 9; ++tap) {
+        const uint32_t a_tap = hcur + uint32_t(((tap / 3) * HALO_C + tap % 3) * 16);
+#pragma unroll
+        for (int jj = 0; jj < chunks / 2; ++jj, ++mm) {
+          const uint64_t da = umma_desc(a_tap + uint32_t(2 * jj * HALO_PLANE), HALO_PLANE, HALO_C * 16);
+          const uint64_t db = umma_desc(w_s + uint32_t((tap * chunks + 2 * jj) * Cout * 16), uint32_t(Cout * 16), 128u);
+          umma_bf16(tmem, da, db, idesc, mm > 0);
+        }
+      }
+      umma_commit(bar);
+    }
+    // tile i + TAP_NBUF - 1 goes into the buffer of tile i - 1, whose MMAs completed before its epilogue
+    if (i + TAP_NBUF - 1 < my_tiles)
+      load_halo(tile + (TAP_NBUF - 1) * (long long)gridDim.x, h_s + uint32_t((i + TAP_NBUF - 1) % TAP_NBUF) * hsz);
+    cp_async_commit();
+    // one thread waits for the MMAs (the others do not spin on the barrier) and the block barrier passes it on
+    if (tid == 0 && !mbar_wait(bar, phase)) {
+      atomicCAS(err, 0, 4);
+      ok = false;
+    }
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      break;
+    }
+    tc_fence_after();
+    const int b = int(tile / per_img), rem = int(tile - (long long)b * per_img);
+    const int m = warp * 32 + lane;
+    const int py = (rem / tiles_x) * TAP_ROWS + (m >> 3), px = (rem % tiles_x) * TAP_COLS + (m & 7);
+    const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
+    for (int c8 = 0; c8 < Cout / 8; ++c8) {
+      float v[8];
+      tmem_ld8(trow + uint32_t(c8 * 8), v);
+      const int co0 = c8 * 8;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        float r = v[e] + s_bias[co0 + e];
+        if (relu) r = fmaxf(r, 0.f);
+        if (out_mode == 2) {  // 2 x 2 window: lanes l, l ^ 1 (next column), l ^ 8 (next row), l ^ 9
+          r += __shfl_xor_sync(0xffffffffu, r, 1);
+          r += __shfl_xor_sync(0xffffffffu, r, 8);
+          r *= 0.25f;
+        }
+        v[e] = r;
+      }
+      __align__(16) __nv_bfloat16 o8[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) o8[e] = __float2bfloat16_rn(v[e]);
+      if (out_mode == 2) {
+        if (lane & 9) continue;
+        const long long mp = ((long long)b * (H / 2) + (py >> 1)) * (W / 2) + (px >> 1);
+        *reinterpret_cast<uint4*>(y + mp * Cout + co0) = *reinterpret_cast<uint4*>(o8);
+      } else {
+        const long long mo = ((long long)b * H + py) * W + px;
+        *reinterpret_cast<uint4*>(y + mo * Cout + co0) = *reinterpret_cast<uint4*>(o8);
+      }
+    }
+    tc_fence_before();  // TMEM reads done before the next tile's first MMA overwrites the accumulator
+  }
+  cp_async_wait_all();
+  if (!ok && tid == 0) mbar_wait(bar, phase ^ 1u);  // one more bounded wait for the MMAs in flight
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols) : "memory");
+}
+
 // wpk (stage s, chunk c, 8-row group g, row r, element e) = w[n = 8g + r][k = 64 s + 8 c + e] in BF16, the
 // k = tap * Cin + ci order of the GEMM; zero for n >= Cout or k >= 9 Cin.  Weights FP32 (Cout, Cin, 3, 3).
 __global__ void k_pack_tc_weights(const float* __restrict__ w, __nv_bfloat16* __restrict__ wpk, int Cin, int Cout,
@@ -565,8 +724,13 @@ int pty_tc_conv3x3(const void* x, const void* wpk, const float* bias, void* y, i
     return fail("pty_tc_conv3x3: bad argument", PTY_ERR_INVALID);
   if (out_mode != 1 && (Cout % 8)) return fail("pty_tc_conv3x3: NHWC output needs Cout % 8 == 0", PTY_ERR_INVALID);
   if (Cin % 8 && Cin > 8) return fail("pty_tc_conv3x3: Cin must be a multiple of 8 or at most 8", PTY_ERR_INVALID);
-  if (out_mode == 2 && ((H & 1) || (W % 16)))
-    return fail("pty_tc_conv3x3: pooled output needs an even H and W a multiple of 16", PTY_ERR_INVALID);
+  // the shifted-GEMM form: thin inputs whose packed weights fit in shared memory, tiles of 16 x 8 output pixels
+  const bool tap = (Cin == 16 || Cin == 32 || Cin == 64) && Cout % 16 == 0 && Cout * 9 * Cin * 2 <= TAP_MAX_W_BYTES &&
+                   H % TAP_ROWS == 0 && W % TAP_COLS == 0 && (in_mode == 0 || in_mode == 1) &&
+                   (out_mode == 0 || out_mode == 2);
+  if (out_mode == 2 && !tap && ((H & 1) || (W % 16)))
+    return fail("pty_tc_conv3x3: pooled output needs an even H and W a multiple of 16 (or, for Cin <= 64, H a "
+                "multiple of 16 and W of 8)", PTY_ERR_INVALID);
   if (in_mode == 1 && ((H & 1) || (W & 1))) return fail("pty_tc_conv3x3: upsampled input needs even H, W", PTY_ERR_INVALID);
   if (in_mode == 2 && (Cin != 1 || (H & 1) || (W & 1)))
     return fail("pty_tc_conv3x3: amplitude input needs Cin = 1 and even H, W", PTY_ERR_INVALID);
@@ -579,11 +743,16 @@ int pty_tc_conv3x3(const void* x, const void* wpk, const float* bias, void* y, i
   if (!attr_set[cur].load()) {
     cudaError_t e = cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          TcSmem::total(TC_MAX_N));
+    const void* taps[3] = {(const void*)k_conv_tap<16>, (const void*)k_conv_tap<32>, (const void*)k_conv_tap<64>};
+    for (const void* f : taps)
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TAP_MAX_W_BYTES + TAP_NBUF * 8 * HALO_PLANE + 64);
     if (e != cudaSuccess) return finish(e, "pty_tc_conv3x3: shared memory attribute");
     attr_set[cur].store(true);
   }
   const int Npad = pad16(Cout);
-  const int smem = TcSmem::total(Npad);
+  const int smem = tap ? tap_smem(Cin, Npad) : TcSmem::total(Npad);
   // CTAs resident per SM, from the shared-memory budget (1 KB reserved per CTA, plus the kernel's static 1 KB) and
   // the 512 TMEM columns; the runtime's occupancy query reports 1 for this kernel.  Persistent CTAs do not wait on
   // one another, so an estimate that is too high only queues CTAs.
@@ -596,11 +765,34 @@ int pty_tc_conv3x3(const void* x, const void* wpk, const float* bias, void* y, i
   int per_sm = smem_sm / (smem + 2048);
   if (per_sm > 512 / ncols) per_sm = 512 / ncols;  // TMEM columns of one SM
   if (per_sm > 2048 / TC_THREADS) per_sm = 2048 / TC_THREADS;
+  {  // registers (allocated per warp in units of 256): persistent CTAs beyond the resident ones would run as a tail
+    static int regs[4] = {0, 0, 0, 0};
+    const int ki = tap ? (Cin == 16 ? 1 : (Cin == 32 ? 2 : 3)) : 0;
+    int& r = regs[ki];
+    if (!r) {
+      const void* fns[4] = {(const void*)k_conv_tc, (const void*)k_conv_tap<16>, (const void*)k_conv_tap<32>,
+                            (const void*)k_conv_tap<64>};
+      cudaFuncAttributes fa{};
+      if (cudaFuncGetAttributes(&fa, fns[ki]) == cudaSuccess) r = fa.numRegs;
+    }
+    if (r > 0) {
+      const int per_warp = (r * 32 + 255) / 256 * 256;
+      const int by_regs = 65536 / (per_warp * (TC_THREADS / 32));
+      if (per_sm > by_regs) per_sm = by_regs;
+    }
+  }
   if (per_sm < 1) per_sm = 1;
   const long long M = (long long)B * H * W;
-  const long long tiles = (M + TC_M - 1) / TC_M;
+  const long long tiles = (M + TC_M - 1) / TC_M;  // both forms: 128 pixels per tile
   const long long resident = (long long)sms * per_sm;
   const unsigned blocks = unsigned(tiles < resident ? tiles : resident);
+  if (tap) {
+    auto kern = Cin == 16 ? k_conv_tap<16> : (Cin == 32 ? k_conv_tap<32> : k_conv_tap<64>);
+    kern<<<blocks, TC_THREADS, smem, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(wpk), bias,
+        static_cast<__nv_bfloat16*>(y), B, H, W, Cout, relu, in_mode, out_mode, err);
+    return finish(cudaGetLastError(), "pty_tc_conv3x3");
+  }
   k_conv_tc<<<blocks, TC_THREADS, smem, static_cast<cudaStream_t>(stream)>>>(
       x, static_cast<const __nv_bfloat16*>(wpk), bias, y, B, H, W, Cin, Cout, Npad, pad16(9 * Cin), relu, in_mode,
       out_mode, in_scale, err);

@@ -85,6 +85,30 @@ def test_tc_conv_matches_numpy(B, Cin, Cout, H, W, relu, out_mode):
         assert rel_err(got, ref) < 6e-3  # plus the BF16 rounding of the stored output
 
 
+@pytest.mark.parametrize("B,Cin,Cout,H,W,relu,in_mode,out_mode", [
+    (2, 16, 32, 32, 16, 1, 0, 0),   # shifted-GEMM form: Cin = 16, NHWC output, tiles across two images
+    (3, 32, 64, 16, 24, 0, 0, 2),   # Cin = 32, pooled output, three tile columns per row block
+    (2, 64, 32, 32, 32, 1, 1, 0),   # Cin = 64 read from an upsampled 16 x 16 input (the decoder layer)
+    (1, 16, 16, 48, 8, 1, 0, 2),    # one tile column, three tile rows, N = 16
+    (2, 16, 32, 64, 64, 1, 0, 2),   # the encoder's second layer at its size
+])
+def test_tc_conv_shifted_gemm_form(B, Cin, Cout, H, W, relu, in_mode, out_mode):
+    """Thin layers (Cin <= 64, weights resident in shared memory, 16 x 8 pixel tiles) run as nine shifted GEMMs over
+    an input halo in shared memory (k_conv_tap); same bounds as the im2col form."""
+    rng = np.random.default_rng(B * 131 + Cin * 7 + Cout + 3 * in_mode + out_mode)
+    hs, ws = (H // 2, W // 2) if in_mode == 1 else (H, W)
+    x = _bf16_round(rng.standard_normal((B, Cin, hs, ws)))
+    w = _bf16_round(rng.standard_normal((Cout, Cin, 3, 3)) / np.sqrt(Cin * 9))
+    b = rng.standard_normal(Cout).astype(np.float32).astype(np.float64)
+    ref = nn_ref.conv3x3(nn_ref.up2(x) if in_mode == 1 else x, w, b)
+    if relu:
+        ref = nn_ref.relu(ref)
+    if out_mode == 2:
+        ref = nn_ref.pool2(ref)
+    got = _run_conv(_nhwc_bf16(x), w, b, B, Cin, Cout, H, W, relu, in_mode, out_mode)
+    assert rel_err(got, ref) < 6e-3  # BF16 rounding of the stored output
+
+
 def test_tc_conv_upsampled_input():
     rng = np.random.default_rng(11)
     B, Cin, Cout, h, w_ = 2, 16, 24, 5, 7
