@@ -365,7 +365,7 @@ __host__ __device__ constexpr int tap_smem(int Cin, int Npad) {
 template <int Cin>
 __global__ void __launch_bounds__(TC_THREADS, 4)
     k_conv_tap(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wpk,
-               const float* __restrict__ bias, __nv_bfloat16* __restrict__ y, int B, int H, int W, int Cout,
+               const float* __restrict__ bias, void* __restrict__ y, int B, int H, int W, int Cout, int Npad,
                int relu, int in_mode, int out_mode, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ uint32_t s_tmem;
@@ -373,14 +373,14 @@ __global__ void __launch_bounds__(TC_THREADS, 4)
   __shared__ float s_bias[TC_MAX_N];
   constexpr int chunks = Cin / 8;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int wbytes = Cout * 9 * Cin * 2;
+  const int wbytes = Npad * 9 * Cin * 2;
   const uint32_t sbase = smem_u32(smem);
   const uint32_t w_s = sbase, h_s = sbase + uint32_t(wbytes), hsz = uint32_t(chunks * HALO_PLANE);
   const uint32_t bar = h_s + TAP_NBUF * hsz;
   const int tiles_x = W / TAP_COLS, per_img = tiles_x * (H / TAP_ROWS);
   const long long ntiles = (long long)B * per_img;
-  const uint32_t ncols = Cout <= 32 ? 32u : (Cout <= 64 ? 64u : (Cout <= 128 ? 128u : 256u));
-  const uint32_t idesc = umma_idesc_bf16(TC_M, Cout);
+  const uint32_t ncols = Npad <= 32 ? 32u : (Npad <= 64 ? 64u : (Npad <= 128 ? 128u : 256u));
+  const uint32_t idesc = umma_idesc_bf16(TC_M, Npad);
   if (tid == 0) s_skip = *reinterpret_cast<volatile int*>(err);
   __syncthreads();
   if (s_skip || (long long)blockIdx.x >= ntiles) return;  // uniform across the CTA
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
-  for (int q = tid; q < Cout; q += TC_THREADS) s_bias[q] = bias[q];
+  for (int q = tid; q < Npad; q += TC_THREADS) s_bias[q] = q < Cout ? bias[q] : 0.f;
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4)
 #pragma unroll
         for (int jj = 0; jj < chunks / 2; ++jj, ++mm) {
           const uint64_t da = umma_desc(a_tap + uint32_t(2 * jj * HALO_PLANE), HALO_PLANE, HALO_C * 16);
-          const uint64_t db = umma_desc(w_s + uint32_t((tap * chunks + 2 * jj) * Cout * 16), uint32_t(Cout * 16), 128u);
+          const uint64_t db = umma_desc(w_s + uint32_t((tap * chunks + 2 * jj) * Npad * 16), uint32_t(Npad * 16), 128u);
           umma_bf16(tmem, da, db, idesc, mm > 0);
         }
       }
@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4)
     const int m = warp * 32 + lane;
     const int py = (rem / tiles_x) * TAP_ROWS + (m >> 3), px = (rem % tiles_x) * TAP_COLS + (m & 7);
     const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
-    for (int c8 = 0; c8 < Cout / 8; ++c8) {
+    for (int c8 = 0; c8 < (Cout + 7) / 8; ++c8) {  // uniform across the warp (tcgen05.ld is warp-collective)
       float v[8];
       tmem_ld8(trow + uint32_t(c8 * 8), v);
       const int co0 = c8 * 8;
@@ -481,16 +481,24 @@ __global__ void __launch_bounds__(TC_THREADS, 4)
         }
         v[e] = r;
       }
+      if (out_mode == 1) {  // NCHW FP32 (the output layer)
+        float* yf = static_cast<float*>(y);
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+          if (co0 + e < Cout) yf[(((long long)b * Cout + co0 + e) * H + py) * W + px] = v[e];
+        continue;
+      }
       __align__(16) __nv_bfloat16 o8[8];
 #pragma unroll
       for (int e = 0; e < 8; ++e) o8[e] = __float2bfloat16_rn(v[e]);
+      __nv_bfloat16* yb = static_cast<__nv_bfloat16*>(y);
       if (out_mode == 2) {
         if (lane & 9) continue;
         const long long mp = ((long long)b * (H / 2) + (py >> 1)) * (W / 2) + (px >> 1);
-        *reinterpret_cast<uint4*>(y + mp * Cout + co0) = *reinterpret_cast<uint4*>(o8);
+        *reinterpret_cast<uint4*>(yb + mp * Cout + co0) = *reinterpret_cast<uint4*>(o8);
       } else {
         const long long mo = ((long long)b * H + py) * W + px;
-        *reinterpret_cast<uint4*>(y + mo * Cout + co0) = *reinterpret_cast<uint4*>(o8);
+        *reinterpret_cast<uint4*>(yb + mo * Cout + co0) = *reinterpret_cast<uint4*>(o8);
       }
     }
     tc_fence_before();  // TMEM reads done before the next tile's first MMA overwrites the accumulator
@@ -725,9 +733,8 @@ int pty_tc_conv3x3(const void* x, const void* wpk, const float* bias, void* y, i
   if (out_mode != 1 && (Cout % 8)) return fail("pty_tc_conv3x3: NHWC output needs Cout % 8 == 0", PTY_ERR_INVALID);
   if (Cin % 8 && Cin > 8) return fail("pty_tc_conv3x3: Cin must be a multiple of 8 or at most 8", PTY_ERR_INVALID);
   // the shifted-GEMM form: thin inputs whose packed weights fit in shared memory, tiles of 16 x 8 output pixels
-  const bool tap = (Cin == 16 || Cin == 32 || Cin == 64) && Cout % 16 == 0 && Cout * 9 * Cin * 2 <= TAP_MAX_W_BYTES &&
-                   H % TAP_ROWS == 0 && W % TAP_COLS == 0 && (in_mode == 0 || in_mode == 1) &&
-                   (out_mode == 0 || out_mode == 2);
+  const bool tap = (Cin == 16 || Cin == 32 || Cin == 64) && pad16(Cout) * 9 * Cin * 2 <= TAP_MAX_W_BYTES &&
+                   H % TAP_ROWS == 0 && W % TAP_COLS == 0 && (in_mode == 0 || in_mode == 1);
   if (out_mode == 2 && !tap && ((H & 1) || (W % 16)))
     return fail("pty_tc_conv3x3: pooled output needs an even H and W a multiple of 16 (or, for Cin <= 64, H a "
                 "multiple of 16 and W of 8)", PTY_ERR_INVALID);
@@ -789,8 +796,8 @@ int pty_tc_conv3x3(const void* x, const void* wpk, const float* bias, void* y, i
   if (tap) {
     auto kern = Cin == 16 ? k_conv_tap<16> : (Cin == 32 ? k_conv_tap<32> : k_conv_tap<64>);
     kern<<<blocks, TC_THREADS, smem, static_cast<cudaStream_t>(stream)>>>(
-        static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(wpk), bias,
-        static_cast<__nv_bfloat16*>(y), B, H, W, Cout, relu, in_mode, out_mode, err);
+        static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(wpk), bias, y, B, H, W, Cout, Npad,
+        relu, in_mode, out_mode, err);
     return finish(cudaGetLastError(), "pty_tc_conv3x3");
   }
   k_conv_tc<<<blocks, TC_THREADS, smem, static_cast<cudaStream_t>(stream)>>>(

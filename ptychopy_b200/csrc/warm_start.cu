@@ -71,7 +71,9 @@ void run_warm_start(pty_session* s) {
     wl[l] = prm.as<float>() + off;
     bl[l] = wl[l] + size_t(L.cout) * L.cin * 9;
     off += size_t(L.cout) * L.cin * 9 + L.cout;
-    cuda_core[l] = (l == 0 && L.cout == 16) || (int(l) == last && L.cin == 32 && L.cout <= 4);
+    // first layer (K = 9) on CUDA cores; the output layer (N = 3) on the tensor cores in the shifted-GEMM form where
+    // its size allows (H a multiple of 16), else on CUDA cores
+    cuda_core[l] = (l == 0 && L.cout == 16) || (int(l) == last && L.cin == 32 && L.cout <= 4 && L.H % 16 != 0);
     if (!cuda_core[l]) {
       const int n = pty_tc_weights_size(L.cin, L.cout);
       need(n > 0, "warm-start layer " + std::to_string(l) + " is not supported by the tensor-core path");

@@ -231,7 +231,8 @@ class TcNet:
             if l == 0 and cout == 16 and after == "pool" and relu:  # K = 9: CUDA cores
                 abi.check(L.pty_tc_first_layer(_p(cur), _p(net._w(net.params, l)), _p(net._b(net.params, l)), _p(y),
                                                B, cout, H, H, INPUT_SCALE, st))
-            elif l == last and cin == 32 and cout <= 4 and in_mode == 0 and not relu:  # N = 3: CUDA cores
+            elif l == last and cin == 32 and cout <= 4 and in_mode == 0 and not relu and H % 16:  # N = 3: CUDA cores
+                # (at H a multiple of 16 the output layer runs on the tensor cores in the shifted-GEMM form)
                 abi.check(L.pty_tc_last_layer(_p(cur), _p(net._w(net.params, l)), _p(net._b(net.params, l)), _p(y),
                                               B, cin, cout, H, H, st))
             else:
