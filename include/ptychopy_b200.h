@@ -212,9 +212,9 @@ int pty_warm_input(const float* amp, float* x, int B, int N, float scale, void* 
  * B x H/2 x W/2 x Cin, read 2x nearest-upsampled; 2: x FP32 amplitudes B x H x W (Cin = 1) read as
  * in_scale * log1p(amp) with the zero frequency moved to the centre.  Output out_mode 0: y NHWC BF16 (Cout a
  * multiple of 8); 1: y NCHW FP32; 2: y NHWC BF16 2x2-average-pooled to H/2 x W/2 (H even, W a multiple of 16; or
- * H a multiple of 16 and W of 8 for the thin layers below).  Thin layers (Cin 16, 32 or 64, packed weights
- * (Cout rounded up to 16) x 9 x Cin x 2 bytes <= 40 KB, H a multiple of 16, W of 8, in_mode 0 or 1) run as nine
- * shifted GEMMs over an input halo held in shared memory; the rest as an implicit GEMM with im2col staging.
+ * H a multiple of 16 and W of 8 for the thin layers below).  Thin layers (Cin 16, 32 or 64, packed weights plus
+ * three input halos within one CTA's shared memory, H a multiple of 16, W of 8, in_mode 0 or 1) run as nine shifted
+ * GEMMs over an input halo held in shared memory; the rest as an implicit GEMM with im2col staging.
  * *err (device int, zero on entry) receives a non-zero code if a pipeline wait timed out.
  * pty_tc_first_layer: the network's first layer on CUDA cores (K = 9 is too thin for tensor cores): y (NHWC BF16,
  * B x H/2 x W/2 x 16) = pool2(relu(bias + conv3x3(in_scale * log1p(centred amp)))) for FP32 amplitudes amp

@@ -356,8 +356,8 @@ __global__ void __launch_bounds__(TC_THREADS, 5)  // 5 CTAs per SM for the narro
 // current tile's MMAs and epilogue.
 constexpr int TAP_ROWS = 16, TAP_COLS = 8, HALO_R = TAP_ROWS + 2, HALO_C = TAP_COLS + 2;
 constexpr int HALO_PLANE = HALO_R * HALO_C * 16;  // 2880 B
-constexpr int TAP_MAX_W_BYTES = 40 * 1024;          // packed weights resident per CTA
 constexpr int TAP_NBUF = 3;                           // halo buffers: two tiles' loads in flight behind the current
+constexpr int TAP_MAX_SMEM = 225 * 1024;  // dynamic shared memory of one CTA (227 KB less the 2 KB of static data)
 __host__ __device__ constexpr int tap_smem(int Cin, int Npad) {
   return Npad * 9 * Cin * 2 + TAP_NBUF * (Cin / 8) * HALO_PLANE + 64;  // weights, halo buffers, the mbarrier
 }
@@ -509,6 +509,201 @@ __global__ void __launch_bounds__(TC_THREADS, 4)
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols) : "memory");
+}
+
+// ---- the shifted-GEMM form for wide inputs (Cin = 128 or 256, N <= 64): channel groups of 64 streamed per tile ----
+// The packed weights no longer fit beside the halos, so each tile runs over its Cin / 64 channel groups, item j =
+// (tile, group): the group's 8 halo planes (cp.async by all threads, as in k_conv_tap) and its nine 64-channel weight
+// slices (one-thread bulk copies of 8 x Npad x 16 bytes each, completing on an mbarrier) land in buffer j & 1 while
+// the MMAs of item j - 1 run; 9 x 4 MMAs per item accumulate into the tile's accumulator (two, alternating by tile,
+// so that a tile's epilogue runs after the next tile's first MMAs have been issued).
+constexpr int TAPG_HALO = 8 * HALO_PLANE;  // one group's halo: 8 planes of 8 channels
+__host__ __device__ constexpr int tapg_wbytes(int Npad) { return 9 * 8 * Npad * 16; }
+__host__ __device__ constexpr int tapg_smem(int Npad) { return 2 * (TAPG_HALO + tapg_wbytes(Npad)) + 64; }
+
+template <int Cin>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_conv_tapg(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wpk,
+                const float* __restrict__ bias, void* __restrict__ y, int B, int H, int W, int Cout, int Npad,
+                int relu, int in_mode, int out_mode, int* __restrict__ err) {
+  constexpr int G = Cin / 64;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_skip;
+  __shared__ float s_bias[TC_MAX_N];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int wbytes = tapg_wbytes(Npad);
+  const uint32_t sbase = smem_u32(smem), bufsz = uint32_t(TAPG_HALO + wbytes);
+  const uint32_t bars = sbase + 2 * bufsz;  // full0, full1 (weights landed), done0, done1 (MMAs of the buffer done)
+  const int tiles_x = W / TAP_COLS, per_img = tiles_x * (H / TAP_ROWS);
+  const long long ntiles = (long long)B * per_img;
+  const uint32_t ncols = Npad <= 32 ? 32u : 64u;
+  const uint32_t idesc = umma_idesc_bf16(TC_M, Npad);
+  if (tid == 0) s_skip = *reinterpret_cast<volatile int*>(err);
+  __syncthreads();
+  if (s_skip || (long long)blockIdx.x >= ntiles) return;  // uniform across the CTA
+  if (tid == 0) {
+    for (int q = 0; q < 4; ++q) mbar_init(bars + 8 * q, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&s_tmem)),
+                 "r"(2 * ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  for (int q = tid; q < Npad; q += TC_THREADS) s_bias[q] = q < Cout ? bias[q] : 0.f;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  const int Hs = in_mode == 1 ? H / 2 : H, Ws = in_mode == 1 ? W / 2 : W;  // stored input size
+  const long long my_tiles = (ntiles - 1 - blockIdx.x) / gridDim.x + 1, nitems = my_tiles * G;
+
+  auto load_item = [&](long long j) {
+    const long long tile = blockIdx.x + (j / G) * gridDim.x;
+    const int g = int(j % G);
+    const uint32_t hdst = sbase + uint32_t(j & 1) * bufsz, wdst = hdst + TAPG_HALO;
+    const int b = int(tile / per_img), rem = int(tile - (long long)b * per_img);
+    const int y0 = (rem / tiles_x) * TAP_ROWS - 1, x0 = (rem % tiles_x) * TAP_COLS - 1;
+    for (int q = tid; q < HALO_R * HALO_C * 8; q += TC_THREADS) {
+      const int c = q & 7, pix = q >> 3, hy = pix / HALO_C, hx = pix - hy * HALO_C;
+      int sy = y0 + hy, sx = x0 + hx;
+      const bool v = sy >= 0 && sy < H && sx >= 0 && sx < W;
+      if (in_mode == 1) {
+        sy >>= 1;
+        sx >>= 1;
+      }
+      const __nv_bfloat16* src = v ? x + (((long long)b * Hs + sy) * Ws + sx) * Cin + 64 * g + 8 * c : x;
+      cp_async16_l1(hdst + uint32_t(c * HALO_PLANE + (hy * HALO_C + hx) * 16), src, v);
+    }
+    cp_async_commit();
+    if (tid == 0) {
+      const uint32_t full = bars + 8 * uint32_t(j & 1), slice = uint32_t(8 * Npad * 16);
+      mbar_expect_tx(full, uint32_t(wbytes));
+      for (int t = 0; t < 9; ++t)
+        bulk_g2s(wdst + uint32_t(t) * slice, wpk + size_t(t * (Cin / 8) + 8 * g) * Npad * 8, slice, full);
+    }
+  };
+  auto epilogue = [&](long long i) {
+    const long long tile = blockIdx.x + i * gridDim.x;
+    const int b = int(tile / per_img), rem = int(tile - (long long)b * per_img);
+    const int m = warp * 32 + lane;
+    const int py = (rem / tiles_x) * TAP_ROWS + (m >> 3), px = (rem % tiles_x) * TAP_COLS + (m & 7);
+    const uint32_t trow = tmem + uint32_t(i & 1) * ncols + (uint32_t(warp * 32) << 16);
+    for (int c8 = 0; c8 < (Cout + 7) / 8; ++c8) {
+      float v[8];
+      tmem_ld8(trow + uint32_t(c8 * 8), v);
+      const int co0 = c8 * 8;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        float r = v[e] + s_bias[co0 + e];
+        if (relu) r = fmaxf(r, 0.f);
+        if (out_mode == 2) {
+          r += __shfl_xor_sync(0xffffffffu, r, 1);
+          r += __shfl_xor_sync(0xffffffffu, r, 8);
+          r *= 0.25f;
+        }
+        v[e] = r;
+      }
+      if (out_mode == 1) {
+        float* yf = static_cast<float*>(y);
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+          if (co0 + e < Cout) yf[(((long long)b * Cout + co0 + e) * H + py) * W + px] = v[e];
+        continue;
+      }
+      __align__(16) __nv_bfloat16 o8[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) o8[e] = __float2bfloat16_rn(v[e]);
+      __nv_bfloat16* yb = static_cast<__nv_bfloat16*>(y);
+      if (out_mode == 2) {
+        if (lane & 9) continue;
+        const long long mp = ((long long)b * (H / 2) + (py >> 1)) * (W / 2) + (px >> 1);
+        *reinterpret_cast<uint4*>(yb + mp * Cout + co0) = *reinterpret_cast<uint4*>(o8);
+      } else {
+        const long long mo = ((long long)b * H + py) * W + px;
+        *reinterpret_cast<uint4*>(yb + mo * Cout + co0) = *reinterpret_cast<uint4*>(o8);
+      }
+    }
+    tc_fence_before();  // TMEM reads done before the MMAs of tile i + 2 overwrite this accumulator
+  };
+
+  bool ok = true;
+  long long committed = 0, loaded = 1;  // items whose MMAs have been committed / whose loads have been issued
+  load_item(0);
+  for (long long j = 0; j < nitems && ok; ++j) {
+    const long long i = j / G;
+    const int g = int(j % G);
+    const uint32_t buf = sbase + uint32_t(j & 1) * bufsz, par = uint32_t((j >> 1) & 1);
+    cp_async_wait_all();
+    fence_async_smem();
+    bool fail = false;
+    if (tid == 0 && !mbar_wait(bars + 8 * uint32_t(j & 1), par)) {  // this item's weight slices
+      atomicCAS(err, 0, 5);
+      fail = true;
+    }
+    if (__syncthreads_or(fail)) {
+      ok = false;
+      break;
+    }
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t acc = tmem + uint32_t(i & 1) * ncols, wbuf = buf + TAPG_HALO;
+      for (int tap = 0; tap < 9; ++tap) {
+        const uint32_t a_tap = buf + uint32_t(((tap / 3) * HALO_C + tap % 3) * 16);
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const uint64_t da = umma_desc(a_tap + uint32_t(2 * jj * HALO_PLANE), HALO_PLANE, HALO_C * 16);
+          const uint64_t db = umma_desc(wbuf + uint32_t((tap * 8 + 2 * jj) * Npad * 16), uint32_t(Npad * 16), 128u);
+          umma_bf16(acc, da, db, idesc, g > 0 || tap > 0 || jj > 0);
+        }
+      }
+      umma_commit(bars + 16 + 8 * uint32_t(j & 1));
+    }
+    committed = j + 1;
+    // buffer (j + 1) & 1 was last read by item j - 1's MMAs
+    if (j >= 1 && tid == 0 && !mbar_wait(bars + 16 + 8 * uint32_t((j - 1) & 1), uint32_t(((j - 1) >> 1) & 1))) {
+      atomicCAS(err, 0, 6);
+      fail = true;
+    }
+    if (__syncthreads_or(fail)) {
+      ok = false;
+      break;
+    }
+    if (j + 1 < nitems) {
+      load_item(j + 1);
+      loaded = j + 2;
+    }
+    // the previous tile's MMAs (item j - 1 was its last) are done: its epilogue overlaps this tile's MMAs
+    if (g == 0 && i > 0) {
+      tc_fence_after();
+      epilogue(i - 1);
+    }
+  }
+  if (ok) {  // the last tile
+    bool fail = false;
+    if (tid == 0 && !mbar_wait(bars + 16 + 8 * uint32_t((nitems - 1) & 1), uint32_t(((nitems - 1) >> 1) & 1))) {
+      atomicCAS(err, 0, 6);
+      fail = true;
+    }
+    if (!__syncthreads_or(fail)) {
+      tc_fence_after();
+      epilogue(my_tiles - 1);
+    } else {
+      ok = false;
+    }
+  }
+  cp_async_wait_all();
+  if (!ok && tid == 0) {  // bounded waits for the MMAs and weight copies still in flight
+    for (long long j = committed > 1 ? committed - 2 : 0; j < committed; ++j)
+      mbar_wait(bars + 16 + 8 * uint32_t(j & 1), uint32_t((j >> 1) & 1));
+    for (long long j = committed; j < loaded; ++j) mbar_wait(bars + 8 * uint32_t(j & 1), uint32_t((j >> 1) & 1));
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(2 * ncols) : "memory");
 }
 
 // wpk (stage s, chunk c, 8-row group g, row r, element e) = w[n = 8g + r][k = 64 s + 8 c + e] in BF16, the
@@ -732,12 +927,15 @@ int pty_tc_conv3x3(const void* x, const void* wpk, const float* bias, void* y, i
     return fail("pty_tc_conv3x3: bad argument", PTY_ERR_INVALID);
   if (out_mode != 1 && (Cout % 8)) return fail("pty_tc_conv3x3: NHWC output needs Cout % 8 == 0", PTY_ERR_INVALID);
   if (Cin % 8 && Cin > 8) return fail("pty_tc_conv3x3: Cin must be a multiple of 8 or at most 8", PTY_ERR_INVALID);
-  // the shifted-GEMM form: thin inputs whose packed weights fit in shared memory, tiles of 16 x 8 output pixels
-  const bool tap = (Cin == 16 || Cin == 32 || Cin == 64) && pad16(Cout) * 9 * Cin * 2 <= TAP_MAX_W_BYTES &&
+  // the shifted-GEMM forms (tiles of 16 x 8 output pixels): thin inputs with the packed weights resident in shared
+  // memory, or 128 / 256 input channels streamed in groups of 64 for N <= 64
+  const bool tap = (Cin == 16 || Cin == 32 || Cin == 64) && tap_smem(Cin, pad16(Cout)) <= TAP_MAX_SMEM &&
                    H % TAP_ROWS == 0 && W % TAP_COLS == 0 && (in_mode == 0 || in_mode == 1);
-  if (out_mode == 2 && !tap && ((H & 1) || (W % 16)))
-    return fail("pty_tc_conv3x3: pooled output needs an even H and W a multiple of 16 (or, for Cin <= 64, H a "
-                "multiple of 16 and W of 8)", PTY_ERR_INVALID);
+  const bool tapg = (Cin == 128 || Cin == 256) && pad16(Cout) <= 64 && H % TAP_ROWS == 0 && W % TAP_COLS == 0 &&
+                    (in_mode == 0 || in_mode == 1);
+  if (out_mode == 2 && !tap && !tapg && ((H & 1) || (W % 16)))
+    return fail("pty_tc_conv3x3: pooled output needs an even H and W a multiple of 16 (or, in the shifted-GEMM "
+                "form, H a multiple of 16 and W of 8)", PTY_ERR_INVALID);
   if (in_mode == 1 && ((H & 1) || (W & 1))) return fail("pty_tc_conv3x3: upsampled input needs even H, W", PTY_ERR_INVALID);
   if (in_mode == 2 && (Cin != 1 || (H & 1) || (W & 1)))
     return fail("pty_tc_conv3x3: amplitude input needs Cin = 1 and even H, W", PTY_ERR_INVALID);
@@ -750,16 +948,16 @@ int pty_tc_conv3x3(const void* x, const void* wpk, const float* bias, void* y, i
   if (!attr_set[cur].load()) {
     cudaError_t e = cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          TcSmem::total(TC_MAX_N));
-    const void* taps[3] = {(const void*)k_conv_tap<16>, (const void*)k_conv_tap<32>, (const void*)k_conv_tap<64>};
+    const void* taps[5] = {(const void*)k_conv_tap<16>, (const void*)k_conv_tap<32>, (const void*)k_conv_tap<64>,
+                           (const void*)k_conv_tapg<128>, (const void*)k_conv_tapg<256>};
     for (const void* f : taps)
       if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 TAP_MAX_W_BYTES + TAP_NBUF * 8 * HALO_PLANE + 64);
+        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, TAP_MAX_SMEM);
     if (e != cudaSuccess) return finish(e, "pty_tc_conv3x3: shared memory attribute");
     attr_set[cur].store(true);
   }
   const int Npad = pad16(Cout);
-  const int smem = tap ? tap_smem(Cin, Npad) : TcSmem::total(Npad);
+  const int smem = tap ? tap_smem(Cin, Npad) : (tapg ? tapg_smem(Npad) : TcSmem::total(Npad));
   // CTAs resident per SM, from the shared-memory budget (1 KB reserved per CTA, plus the kernel's static 1 KB) and
   // the 512 TMEM columns; the runtime's occupancy query reports 1 for this kernel.  Persistent CTAs do not wait on
   // one another, so an estimate that is too high only queues CTAs.
@@ -768,17 +966,17 @@ int pty_tc_conv3x3(const void* x, const void* wpk, const float* bias, void* y, i
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   if (e != cudaSuccess) return finish(e, "pty_tc_conv3x3: device attributes");
-  const int ncols = Npad <= 32 ? 32 : (Npad <= 64 ? 64 : (Npad <= 128 ? 128 : 256));
+  const int ncols = (Npad <= 32 ? 32 : (Npad <= 64 ? 64 : (Npad <= 128 ? 128 : 256))) * (tapg ? 2 : 1);
   int per_sm = smem_sm / (smem + 2048);
   if (per_sm > 512 / ncols) per_sm = 512 / ncols;  // TMEM columns of one SM
   if (per_sm > 2048 / TC_THREADS) per_sm = 2048 / TC_THREADS;
   {  // registers (allocated per warp in units of 256): persistent CTAs beyond the resident ones would run as a tail
-    static int regs[4] = {0, 0, 0, 0};
-    const int ki = tap ? (Cin == 16 ? 1 : (Cin == 32 ? 2 : 3)) : 0;
+    static int regs[6] = {0, 0, 0, 0, 0, 0};
+    const int ki = tap ? (Cin == 16 ? 1 : (Cin == 32 ? 2 : 3)) : (tapg ? (Cin == 128 ? 4 : 5) : 0);
     int& r = regs[ki];
     if (!r) {
-      const void* fns[4] = {(const void*)k_conv_tc, (const void*)k_conv_tap<16>, (const void*)k_conv_tap<32>,
-                            (const void*)k_conv_tap<64>};
+      const void* fns[6] = {(const void*)k_conv_tc, (const void*)k_conv_tap<16>, (const void*)k_conv_tap<32>,
+                            (const void*)k_conv_tap<64>, (const void*)k_conv_tapg<128>, (const void*)k_conv_tapg<256>};
       cudaFuncAttributes fa{};
       if (cudaFuncGetAttributes(&fa, fns[ki]) == cudaSuccess) r = fa.numRegs;
     }
@@ -795,6 +993,13 @@ int pty_tc_conv3x3(const void* x, const void* wpk, const float* bias, void* y, i
   const unsigned blocks = unsigned(tiles < resident ? tiles : resident);
   if (tap) {
     auto kern = Cin == 16 ? k_conv_tap<16> : (Cin == 32 ? k_conv_tap<32> : k_conv_tap<64>);
+    kern<<<blocks, TC_THREADS, smem, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(wpk), bias, y, B, H, W, Cout, Npad,
+        relu, in_mode, out_mode, err);
+    return finish(cudaGetLastError(), "pty_tc_conv3x3");
+  }
+  if (tapg) {
+    auto kern = Cin == 128 ? k_conv_tapg<128> : k_conv_tapg<256>;
     kern<<<blocks, TC_THREADS, smem, static_cast<cudaStream_t>(stream)>>>(
         static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(wpk), bias, y, B, H, W, Cout, Npad,
         relu, in_mode, out_mode, err);

@@ -93,6 +93,9 @@ def test_tc_conv_matches_numpy(B, Cin, Cout, H, W, relu, out_mode):
     (2, 16, 32, 64, 64, 1, 0, 2),   # the encoder's second layer at its size
     (2, 32, 3, 32, 32, 0, 0, 1),    # the output layer: N padded 3 -> 16, FP32 NCHW output
     (1, 16, 24, 16, 8, 1, 0, 0),    # Cout = 24 (N padded to 32), NHWC output
+    (2, 64, 128, 16, 16, 1, 0, 2),  # 147 KB of weights: one CTA per SM (the encoder's 64 -> 128 layer)
+    (2, 256, 64, 16, 16, 1, 1, 0),  # four 64-channel groups streamed per tile, upsampled input (the decoder's first)
+    (3, 128, 48, 32, 8, 0, 0, 2),   # two groups, N padded 48, pooled, tiles across images
 ])
 def test_tc_conv_shifted_gemm_form(B, Cin, Cout, H, W, relu, in_mode, out_mode):
     """Thin layers (Cin <= 64, weights resident in shared memory, 16 x 8 pixel tiles) run as nine shifted GEMMs over
