@@ -70,10 +70,11 @@ typedef struct pty_params {
   int calculateRMS;       /* compute the per-iteration error metric (the reference's Python path never does) */
   int device;             /* CUDA device ordinal */
   int wave;               /* DM patterns per wave of its three kernels (0 = automatic) */
-  int precision;          /* FFT arithmetic: 0 FP32 (default); 1 split-BF16 tensor-core stages (pty_fft2_tc) at
-                             N = 256: MLs (its group transforms), ePIE (then run as a per-position kernel chain
-                             around the tensor-core transforms instead of the fused FP32 kernel).  DM fuses its FP32
-                             transforms into its kernels and refuses 1 (PTY_ERR_UNSUPPORTED). */
+  int precision;          /* FFT arithmetic: 0 FP32 (default); 1 tensor-core stages: at N = 256 split-BF16
+                             (pty_fft2_tc) for MLs (its group transforms) and ePIE (then run as a per-position kernel
+                             chain around the tensor-core transforms instead of the fused FP32 kernel); at N = 512
+                             for DM, whose column pass computes its 32-point DFT stages as split-FP16 GEMMs.  Other
+                             sizes refuse 1 (PTY_ERR_UNSUPPORTED). */
   int mlsCore;            /* MLs: 0 (default) the reference's path, which its Python API always runs
                              (src/Parameters.h:162-163: variable probe with one extra mode, variable intensity,
                              sub-pixel probe shift, position search from iteration PPS); 1 the fixed-probe core

@@ -6,7 +6,7 @@
 //   * objectNP/probeNP accept any complex or real dtype (the reference misreads complex64, src/ptychopy.c:383-471);
 //   * extra keywords: seed, calculateRMS, device, wave, returnResults, writeResults, outputDir, warmStart (trained
 //     warm-start network parameters, float32) and warmStartWidth (its width, default 16), precision (0 FP32 FFT,
-//     1 split-BF16 tensor-core FFT stages for MLs at 256 x 256), mlsCore (1: MLs without the reference's variable
+//     1 tensor-core FFT stages: MLs and ePIE at 256 x 256, DM at 512 x 512), mlsCore (1: MLs without the reference's variable
 //     probe, sub-pixel shift and position search), save (write the results every `save` iterations, like the
 //     reference's command-line option);
 //     probeNP may be (K, N, N) to supply all probe modes.
