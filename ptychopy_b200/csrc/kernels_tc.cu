@@ -512,29 +512,32 @@ __global__ void __launch_bounds__(TC_THREADS, 4)
 }
 
 // ---- the shifted-GEMM form for wide inputs (Cin = 128 or 256, N <= 64): channel groups of 64 streamed per tile ----
-// The packed weights no longer fit beside the halos, so each tile runs over its Cin / 64 channel groups, item j =
-// (tile, group): the group's 8 halo planes (cp.async by all threads, as in k_conv_tap) and its nine 64-channel weight
-// slices (one-thread bulk copies of 8 x Npad x 16 bytes each, completing on an mbarrier) land in buffer j & 1 while
-// the MMAs of item j - 1 run; 9 x 4 MMAs per item accumulate into the tile's accumulator (two, alternating by tile,
-// so that a tile's epilogue runs after the next tile's first MMAs have been issued).
+// The packed weights no longer fit beside the halos, so each tile runs over its Cin / 64 channel groups, and each
+// group over three items of three taps: item j = (tile, group, third).  A group's 8 halo planes (cp.async by all
+// threads, as in k_conv_tap) land in halo buffer (tile * G + group) & 1 while the previous group's items run; an
+// item's three 64-channel weight slices (one-thread bulk copies of 8 x Npad x 16 bytes each, completing on an
+// mbarrier) land in weight buffer j & 1 while item j - 1's MMAs run.  3 x 4 MMAs per item accumulate into the tile's
+// accumulator (two, alternating by tile, so that a tile's epilogue runs after the next tile's first MMAs have been
+// issued).  About 95 KB of shared memory: two CTAs per SM.
 constexpr int TAPG_HALO = 8 * HALO_PLANE;  // one group's halo: 8 planes of 8 channels
-__host__ __device__ constexpr int tapg_wbytes(int Npad) { return 9 * 8 * Npad * 16; }
-__host__ __device__ constexpr int tapg_smem(int Npad) { return 2 * (TAPG_HALO + tapg_wbytes(Npad)) + 64; }
+__host__ __device__ constexpr int tapg_wbytes(int Npad) { return 3 * 8 * Npad * 16; }  // three taps' slices
+__host__ __device__ constexpr int tapg_smem(int Npad) { return 2 * TAPG_HALO + 2 * tapg_wbytes(Npad) + 64; }
 
 template <int Cin>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(TC_THREADS, 2)
     k_conv_tapg(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wpk,
                 const float* __restrict__ bias, void* __restrict__ y, int B, int H, int W, int Cout, int Npad,
                 int relu, int in_mode, int out_mode, int* __restrict__ err) {
-  constexpr int G = Cin / 64;
+  constexpr int G = Cin / 64, IPT = 3 * G;  // items per tile
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ uint32_t s_tmem;
   __shared__ int s_skip;
   __shared__ float s_bias[TC_MAX_N];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int wbytes = tapg_wbytes(Npad);
-  const uint32_t sbase = smem_u32(smem), bufsz = uint32_t(TAPG_HALO + wbytes);
-  const uint32_t bars = sbase + 2 * bufsz;  // full0, full1 (weights landed), done0, done1 (MMAs of the buffer done)
+  const uint32_t sbase = smem_u32(smem);
+  const uint32_t h_s = sbase, w_s = sbase + 2 * TAPG_HALO;
+  const uint32_t bars = w_s + 2 * uint32_t(wbytes);  // full0, full1 (weights landed), done0, done1 (MMAs done)
   const int tiles_x = W / TAP_COLS, per_img = tiles_x * (H / TAP_ROWS);
   const long long ntiles = (long long)B * per_img;
   const uint32_t ncols = Npad <= 32 ? 32u : 64u;
@@ -558,12 +561,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   tc_fence_after();
   const uint32_t tmem = s_tmem;
   const int Hs = in_mode == 1 ? H / 2 : H, Ws = in_mode == 1 ? W / 2 : W;  // stored input size
-  const long long my_tiles = (ntiles - 1 - blockIdx.x) / gridDim.x + 1, nitems = my_tiles * G;
+  const long long my_tiles = (ntiles - 1 - blockIdx.x) / gridDim.x + 1, nitems = my_tiles * IPT;
 
-  auto load_item = [&](long long j) {
-    const long long tile = blockIdx.x + (j / G) * gridDim.x;
-    const int g = int(j % G);
-    const uint32_t hdst = sbase + uint32_t(j & 1) * bufsz, wdst = hdst + TAPG_HALO;
+  // all threads: the halo planes of group gi = tile index * G + group (halo buffer gi & 1)
+  auto load_halo = [&](long long gi) {
+    const long long tile = blockIdx.x + (gi / G) * gridDim.x;
+    const int g = int(gi % G);
+    const uint32_t hdst = h_s + uint32_t(gi & 1) * TAPG_HALO;
     const int b = int(tile / per_img), rem = int(tile - (long long)b * per_img);
     const int y0 = (rem / tiles_x) * TAP_ROWS - 1, x0 = (rem % tiles_x) * TAP_COLS - 1;
     for (int q = tid; q < HALO_R * HALO_C * 8; q += TC_THREADS) {
@@ -578,11 +582,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       cp_async16_l1(hdst + uint32_t(c * HALO_PLANE + (hy * HALO_C + hx) * 16), src, v);
     }
     cp_async_commit();
-    if (tid == 0) {
-      const uint32_t full = bars + 8 * uint32_t(j & 1), slice = uint32_t(8 * Npad * 16);
-      mbar_expect_tx(full, uint32_t(wbytes));
-      for (int t = 0; t < 9; ++t)
-        bulk_g2s(wdst + uint32_t(t) * slice, wpk + size_t(t * (Cin / 8) + 8 * g) * Npad * 8, slice, full);
+  };
+  // one thread: item j's three weight slices into weight buffer j & 1
+  auto load_weights = [&](long long j) {
+    const int g = int((j % IPT) / 3), third = int(j % 3);
+    const uint32_t full = bars + 8 * uint32_t(j & 1), slice = uint32_t(8 * Npad * 16);
+    const uint32_t wdst = w_s + uint32_t(j & 1) * uint32_t(wbytes);
+    mbar_expect_tx(full, uint32_t(wbytes));
+    for (int t = 0; t < 3; ++t) {
+      const int tap = 3 * third + t;
+      bulk_g2s(wdst + uint32_t(t) * slice, wpk + size_t(tap * (Cin / 8) + 8 * g) * Npad * 8, slice, full);
     }
   };
   auto epilogue = [&](long long i) {
@@ -630,16 +639,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   };
 
   bool ok = true;
-  long long committed = 0, loaded = 1;  // items whose MMAs have been committed / whose loads have been issued
-  load_item(0);
+  long long committed = 0, loaded = 1;  // items whose MMAs have been committed / whose weights have been requested
+  load_halo(0);
+  if (tid == 0) load_weights(0);
   for (long long j = 0; j < nitems && ok; ++j) {
-    const long long i = j / G;
-    const int g = int(j % G);
-    const uint32_t buf = sbase + uint32_t(j & 1) * bufsz, par = uint32_t((j >> 1) & 1);
-    cp_async_wait_all();
-    fence_async_smem();
+    const long long i = j / IPT, gi = j / 3;
+    const int third = int(j % 3), g = int((j % IPT) / 3);
     bool fail = false;
-    if (tid == 0 && !mbar_wait(bars + 8 * uint32_t(j & 1), par)) {  // this item's weight slices
+    if (third == 0) cp_async_wait_all();  // this group's halo (the only group in flight)
+    fence_async_smem();
+    if (tid == 0 && !mbar_wait(bars + 8 * uint32_t(j & 1), uint32_t((j >> 1) & 1))) {  // this item's weights
       atomicCAS(err, 0, 5);
       fail = true;
     }
@@ -649,20 +658,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
     if (tid == 0) {
       tc_fence_after();
-      const uint32_t acc = tmem + uint32_t(i & 1) * ncols, wbuf = buf + TAPG_HALO;
-      for (int tap = 0; tap < 9; ++tap) {
-        const uint32_t a_tap = buf + uint32_t(((tap / 3) * HALO_C + tap % 3) * 16);
+      const uint32_t acc = tmem + uint32_t(i & 1) * ncols, hbuf = h_s + uint32_t(gi & 1) * TAPG_HALO;
+      const uint32_t wbuf = w_s + uint32_t(j & 1) * uint32_t(wbytes);
+      for (int t = 0; t < 3; ++t) {
+        const int tap = 3 * third + t;
+        const uint32_t a_tap = hbuf + uint32_t(((tap / 3) * HALO_C + tap % 3) * 16);
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
           const uint64_t da = umma_desc(a_tap + uint32_t(2 * jj * HALO_PLANE), HALO_PLANE, HALO_C * 16);
-          const uint64_t db = umma_desc(wbuf + uint32_t((tap * 8 + 2 * jj) * Npad * 16), uint32_t(Npad * 16), 128u);
-          umma_bf16(acc, da, db, idesc, g > 0 || tap > 0 || jj > 0);
+          const uint64_t db = umma_desc(wbuf + uint32_t((t * 8 + 2 * jj) * Npad * 16), uint32_t(Npad * 16), 128u);
+          umma_bf16(acc, da, db, idesc, g > 0 || third > 0 || t > 0 || jj > 0);
         }
       }
       umma_commit(bars + 16 + 8 * uint32_t(j & 1));
     }
     committed = j + 1;
-    // buffer (j + 1) & 1 was last read by item j - 1's MMAs
+    // weight buffer (j + 1) & 1 was last read by item j - 1's MMAs; at a group's first item, the other halo buffer
+    // was last read by the previous group's items, whose MMAs are all done once item j - 1's are
     if (j >= 1 && tid == 0 && !mbar_wait(bars + 16 + 8 * uint32_t((j - 1) & 1), uint32_t(((j - 1) >> 1) & 1))) {
       atomicCAS(err, 0, 6);
       fail = true;
@@ -672,11 +684,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       break;
     }
     if (j + 1 < nitems) {
-      load_item(j + 1);
+      if (tid == 0) load_weights(j + 1);
       loaded = j + 2;
     }
+    if (third == 0 && (gi + 1) * 3 < nitems) load_halo(gi + 1);
     // the previous tile's MMAs (item j - 1 was its last) are done: its epilogue overlaps this tile's MMAs
-    if (g == 0 && i > 0) {
+    if (g == 0 && third == 0 && i > 0) {
       tc_fence_after();
       epilogue(i - 1);
     }
