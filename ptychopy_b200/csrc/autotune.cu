@@ -1,8 +1,9 @@
 // Autotuner: before a session's pty_init, times the launch variants of its algorithm on temporary sessions with the
 // same parameters, positions, probe, object and patterns (the patterns are shared through their device copy) and
 // keeps the fastest for the session: the DM wave size (patterns per pass of the three DM kernels, i.e. how much of the
-// W1 / W2 hand-off stays in L2 against how often the kernels drain), and the ePIE kernel (shared-memory cluster,
-// cluster of global-memory phases, or the whole-GPU cooperative kernel).  No counterpart in the reference, which has
+// W1 / W2 hand-off stays in L2 against how often the kernels drain) and the number of waves in flight (one lane, or
+// two alternating streams), and the ePIE kernel (shared-memory cluster, cluster of global-memory phases, the
+// whole-GPU cooperative kernel, or the per-position kernel chain).  No counterpart in the reference, which has
 // one fixed launch configuration per kernel.
 #include <cuda_runtime.h>
 
@@ -26,6 +27,7 @@ struct Candidate {
   int wave = 0;      // DM
   int variant = -1;  // ePIE
   std::string name;
+  int lanes = 0;     // DM: 0 automatic, 1 one lane
 };
 
 // GPU time per iteration (ms) of one candidate: a temporary session, `iters` warm-up iterations, `iters` timed
@@ -43,6 +45,7 @@ double time_candidate(const pty_session* s, const Candidate& c, int iters) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   do {
     t->epie_variant = c.variant;
+    t->dm_lanes_req = c.lanes;
     if (pty_set_patterns(t, s->amp.p, PTY_F32, s->P, s->N) != PTY_OK) break;
     if (!s->pos_m.empty() && pty_set_positions(t, s->pos_m.data(), int(s->pos_m.size() / 2)) != PTY_OK) break;
     if (!s->probe_h.empty() &&
@@ -97,12 +100,17 @@ extern "C" int pty_autotune(pty_session* s, int iters, char* report, int report_
     }
     std::sort(waves.begin() + 1, waves.end());
     waves.erase(std::unique(waves.begin() + 1, waves.end()), waves.end());
-    for (int w : waves) {
-      Candidate c;
-      c.wave = w;
-      c.name = w ? "wave " + std::to_string(w) : "wave " + std::to_string(automatic) + " (automatic)";
-      cands.push_back(c);
-    }
+    for (int lanes : {0, 1})
+      for (int w : waves) {
+        const int wv = w ? w : automatic;
+        if (lanes == 1 && (P + wv - 1) / wv < 2) continue;  // a single wave runs on one lane anyway
+        Candidate c;
+        c.wave = w;
+        c.lanes = lanes;
+        c.name = (w ? "wave " + std::to_string(w) : "wave " + std::to_string(automatic) + " (automatic)") +
+                 (lanes == 1 ? " one lane" : "");
+        cands.push_back(c);
+      }
   } else if (s->algo == ALGO_EPIE) {
     if (epie_uses_smem(N, s->K)) cands.push_back({0, 0, "shared-memory cluster"});
     cands.push_back({0, 1, "cluster"});
@@ -131,8 +139,12 @@ extern "C" int pty_autotune(pty_session* s, int iters, char* report, int report_
     set_last_error("pty_autotune: no candidate ran");
     return PTY_ERR_CUDA;
   } else {
-    if (s->algo == ALGO_DM) s->prm.wave = cands[best].wave;
-    else s->epie_variant = cands[best].variant;
+    if (s->algo == ALGO_DM) {
+      s->prm.wave = cands[best].wave;
+      s->dm_lanes_req = cands[best].lanes;
+    } else {
+      s->epie_variant = cands[best].variant;
+    }
     char buf[96];
     std::snprintf(buf, sizeof(buf), ": %s (%.3f ms/iteration);", cands[best].name.c_str(), best_ms);
     rep += buf;

@@ -875,7 +875,7 @@ void init_dm(pty_session* s) {
   // two lanes: consecutive waves alternate between the session's stream and a second one, so that one wave's
   // kernels fill the other's tails and launch gaps (900 x 512^2: 2.78-2.88 ms per iteration with 2 lanes of 113-pattern
   // waves against 2.99-3.01 ms with one lane of 225-pattern waves; 3 or 4 lanes measured the same as 2)
-  s->dm_lanes = s->nwaves >= 2 ? 2 : 1;
+  s->dm_lanes = (s->nwaves >= 2 && s->dm_lanes_req != 1) ? 2 : 1;
   if (s->dm_lanes == 2) {
     create_session_stream(s, &s->dm_side);
     check_cuda(cudaEventCreateWithFlags(&s->dm_fork, cudaEventDisableTiming), "event");

@@ -116,6 +116,7 @@ struct pty_session {
   // DM
   pty::DeviceBuf psi, dO, dP, W1, W2, slots;
   int dm_lanes = 1;                // waves in flight side by side (W1 / W2 hold one wave per lane)
+  int dm_lanes_req = 0;            // 0: automatic (two when there are two waves or more); 1: one lane (autotuner)
   cudaStream_t dm_side = nullptr;  // the second lane's stream (forked from and joined to the session's stream)
   cudaEvent_t dm_fork = nullptr, dm_join = nullptr;
   pty::DeviceBuf dm_err;  // wait-timeout flag of the tensor-core column pass (precision = 1)
