@@ -3,7 +3,8 @@
 // keeps the fastest for the session: the DM wave size (patterns per pass of the three DM kernels, i.e. how much of the
 // W1 / W2 hand-off stays in L2 against how often the kernels drain) and the number of waves in flight (one lane, or
 // two alternating streams), and the ePIE kernel (shared-memory cluster, cluster of global-memory phases, the
-// whole-GPU cooperative kernel, or the per-position kernel chain).  No counterpart in the reference, which has
+// whole-GPU cooperative kernel, or the per-position kernel chain, whose transform passes also come with 2, 4 or 8
+// rows per CTA).  No counterpart in the reference, which has
 // one fixed launch configuration per kernel.
 #include <cuda_runtime.h>
 
@@ -28,6 +29,7 @@ struct Candidate {
   int variant = -1;  // ePIE
   std::string name;
   int lanes = 0;     // DM: 0 automatic, 1 one lane
+  int rows = 0;      // ePIE kernel chain: rows per CTA of its transform passes (0 automatic)
 };
 
 // GPU time per iteration (ms) of one candidate: a temporary session, `iters` warm-up iterations, `iters` timed
@@ -46,6 +48,7 @@ double time_candidate(const pty_session* s, const Candidate& c, int iters) {
   do {
     t->epie_variant = c.variant;
     t->dm_lanes_req = c.lanes;
+    t->fft_rows = c.rows;
     if (pty_set_patterns(t, s->amp.p, PTY_F32, s->P, s->N) != PTY_OK) break;
     if (!s->pos_m.empty() && pty_set_positions(t, s->pos_m.data(), int(s->pos_m.size() / 2)) != PTY_OK) break;
     if (!s->probe_h.empty() &&
@@ -116,6 +119,13 @@ extern "C" int pty_autotune(pty_session* s, int iters, char* report, int report_
     cands.push_back({0, 1, "cluster"});
     if (N == 256 || N == 512) cands.push_back({0, 2, "whole-GPU"});
     cands.push_back({0, 3, "kernel chain"});
+    // the chain's transform passes with other row tiles (rows per CTA; 4 is the automatic tile at 512^2)
+    for (int r : {2, 4, 8}) {
+      if (N == 512 && r == 4) continue;
+      Candidate c{0, 3, "kernel chain, " + std::to_string(r) + "-row FFT tiles"};
+      c.rows = r;
+      cands.push_back(c);
+    }
   }
   std::string rep = s->algo == ALGO_DM ? "DM" : (s->algo == ALGO_EPIE ? "ePIE" : "MLs");
   int best = -1;
@@ -144,6 +154,7 @@ extern "C" int pty_autotune(pty_session* s, int iters, char* report, int report_
       s->dm_lanes_req = cands[best].lanes;
     } else {
       s->epie_variant = cands[best].variant;
+      s->fft_rows = cands[best].rows;
     }
     char buf[96];
     std::snprintf(buf, sizeof(buf), ": %s (%.3f ms/iteration);", cands[best].name.c_str(), best_ms);

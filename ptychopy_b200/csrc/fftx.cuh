@@ -30,11 +30,11 @@ struct EpiStore {
 // Rows x0 .. x0 + RC - 1 of plane b: load through pro, transform, store transposed through epi.  s_tw holds the
 // twiddles, s_x the exchange / staging buffers (rows_smem_bytes<L> with s_tw); starts with a CTA barrier so that
 // calls may follow each other.
-template <int L, bool INV, class Pro, class Epi>
+template <int L, bool INV, class Pro, class Epi, int R = FftShape<L>::RC>
 __device__ __forceinline__ void fftx_rows(float2* out, const float2* s_tw, float2* s_x, int b, int x0, const Pro& pro,
                                           Epi& epi) {
   using S = FftShape<L>;
-  constexpr int T = S::T, E = S::E, R = S::RC;
+  constexpr int T = S::T, E = S::E;
   const int v = threadIdx.x / T, t = threadIdx.x % T;
   __syncthreads();
   float2 a[E];
@@ -54,35 +54,42 @@ __device__ __forceinline__ void fftx_rows(float2* out, const float2* s_tw, float
   }
 }
 
-template <int L, bool INV, class Pro, class Epi>
-__global__ void __launch_bounds__(FftShape<L>::THREADS) k_fftx_pass(float2* __restrict__ out,
-                                                                    const float2* __restrict__ g_tw, Pro pro, Epi epi) {
+// R rows per CTA (R x T threads): the default FftShape<L>::RC fills 256 threads; fewer rows spread a plane's rows over
+// more CTAs (and SMs)
+template <int L, bool INV, class Pro, class Epi, int R = FftShape<L>::RC>
+__global__ void __launch_bounds__(R * FftShape<L>::T) k_fftx_pass(float2* __restrict__ out,
+                                                                  const float2* __restrict__ g_tw, Pro pro, Epi epi) {
+  static_assert(R * FftShape<L>::T % 32 == 0, "whole warps per CTA");
   pdl_enter();
   extern __shared__ float4 smem4[];
   float2* smem = reinterpret_cast<float2*>(smem4);
   load_twiddles<L>(smem, g_tw);
-  fftx_rows<L, INV>(out, smem, smem + L, blockIdx.y, blockIdx.x * FftShape<L>::RC, pro, epi);
+  fftx_rows<L, INV, Pro, Epi, R>(out, smem, smem + L, blockIdx.y, blockIdx.x * R, pro, epi);
   epi.finish(blockIdx.y);
 }
 
-template <int L, bool INV, class Pro, class Epi>
+template <int L, bool INV, int R = FftShape<L>::RC, class Pro, class Epi>
 inline cudaError_t launch_fftx(float2* out, const float2* tw, int batch, Pro pro, Epi epi, cudaStream_t st) {
-  constexpr int R = FftShape<L>::RC, NT = FftShape<L>::THREADS;
-  const size_t smem = rows_smem_bytes<L>();
-  cudaError_t e = cudaFuncSetAttribute(k_fftx_pass<L, INV, Pro, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(smem));
+  constexpr int NT = R * FftShape<L>::T;
+  const size_t smem = rows_smem_bytes_r<L, R>();
+  cudaError_t e = cudaFuncSetAttribute(k_fftx_pass<L, INV, Pro, Epi, R>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  return launch_pdl(k_fftx_pass<L, INV, Pro, Epi>, dim3(L / R, batch), NT, smem, st, out, tw, pro, epi);
+  return launch_pdl(k_fftx_pass<L, INV, Pro, Epi, R>, dim3(L / R, batch), NT, smem, st, out, tw, pro, epi);
 }
 
-// 2-D transform data-in (through pro) -> work (transposed) -> out (through epi)
-template <bool INV, class Pro, class Epi>
+// 2-D transform data-in (through pro) -> work (transposed) -> out (through epi); RMAX caps the rows per CTA, which
+// stay at least a whole warp's worth (32 / T rows: the row transforms use warp-wide shuffles and syncs)
+template <bool INV, class Pro, class Epi, int RMAX = 1024>
 inline cudaError_t fftx2(int N, float2* work, float2* out, const float2* tw, int batch, Pro pro, Epi epi, cudaStream_t st) {
   cudaError_t e;
-#define PTY_FFTX(L)                                                                            \
-  case L:                                                                                      \
-    if ((e = launch_fftx<L, INV>(work, tw, batch, pro, EpiStore{}, st)) != cudaSuccess) return e; \
-    return launch_fftx<L, INV>(out, tw, batch, ProLoad{work}, epi, st);
+#define PTY_FFTX(L)                                                                                          \
+  case L: {                                                                                                  \
+    constexpr int RC = FftShape<L>::RC < RMAX ? FftShape<L>::RC : RMAX, RW = 32 / FftShape<L>::T;           \
+    constexpr int R = RC > RW ? RC : RW;                                                                     \
+    if ((e = launch_fftx<L, INV, R>(work, tw, batch, pro, EpiStore{}, st)) != cudaSuccess) return e;         \
+    return launch_fftx<L, INV, R>(out, tw, batch, ProLoad{work}, epi, st);                                   \
+  }
   switch (N) {
     PTY_FFTX(32)
     PTY_FFTX(64)

@@ -20,11 +20,14 @@ __device__ __forceinline__ void pdl_enter() {
 namespace pty {
 
 // Shared memory of a row-transform CTA (FftShape<L>::RC rows): twiddles + max(exchange, transposed staging).
-template <int L>
-__host__ __device__ constexpr size_t rows_smem_bytes() {
-  constexpr int R = FftShape<L>::RC;
+template <int L, int R>
+__host__ __device__ constexpr size_t rows_smem_bytes_r() {
   constexpr int xch = R * FftShape<L>::XCH, stage = L * (R + 1);
   return sizeof(float2) * (L + (xch > stage ? xch : stage));
+}
+template <int L>
+__host__ __device__ constexpr size_t rows_smem_bytes() {
+  return rows_smem_bytes_r<L, FftShape<L>::RC>();
 }
 
 // The CTA holds rows x0..x0+R-1 (vector v = row x0+v) of a plane after fft_vec; element n = t + T*e of the row

@@ -57,6 +57,7 @@ struct EpieChainArgs {
   const float2* tw;       // twiddles of the FP32 transforms (tc = 0)
   float saturation;
   int N, K, Ka, P, X, Y, TX, TY, pc, up, rms, useAll, tc;
+  int frows;              // rows per CTA of the FP32 transform passes (0: automatic; 2, 4, 8: capped by the default)
 };
 cudaError_t epie_chain_iteration(const EpieChainArgs& g, cudaStream_t st);
 int epie_chain_launches(int P, bool up);

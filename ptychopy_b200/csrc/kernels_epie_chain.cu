@@ -20,6 +20,7 @@
 #include "kernel_util.cuh"
 #include "kernels.h"
 #include "kernels_epie.h"
+#include "fftx.cuh"
 #include "kernels_mls.h"
 #include "pdl.cuh"
 
@@ -202,9 +203,25 @@ cudaError_t epie_chain_iteration(const EpieChainArgs& g, cudaStream_t st) {
   const int gb = grid_e(NN);
   const int tiles = ((g.N + 15) / 16 + 1) * ((g.N + 15) / 16 + 1);
   cudaError_t e;
-  auto fft = [&](bool inv) {
-    return g.tc ? fft2_tc(g.psi, g.work, g.Ka, g.N, inv, g.tcerr, st)
-                : fft2_pdl(g.psi, g.work, g.tw, g.Ka, g.N, inv, st);
+  // rows per CTA of the FP32 transform passes (g.frows; 0: 4 at 512^2, where one plane's 512 rows then spread over
+  // 128 CTAs instead of 64: 35.0 against 36.6 ms per 900-position iteration; the default tile elsewhere)
+  const int rows = g.frows > 0 ? g.frows : (g.N == 512 ? 4 : 0);
+  auto fft = [&](bool inv) -> cudaError_t {
+    if (g.tc) return fft2_tc(g.psi, g.work, g.Ka, g.N, inv, g.tcerr, st);
+    const ProLoad pl{g.psi};
+    switch (rows) {
+      case 2:
+        return inv ? fftx2<true, ProLoad, EpiStore, 2>(g.N, g.work, g.psi, g.tw, g.Ka, pl, EpiStore{}, st)
+                   : fftx2<false, ProLoad, EpiStore, 2>(g.N, g.work, g.psi, g.tw, g.Ka, pl, EpiStore{}, st);
+      case 4:
+        return inv ? fftx2<true, ProLoad, EpiStore, 4>(g.N, g.work, g.psi, g.tw, g.Ka, pl, EpiStore{}, st)
+                   : fftx2<false, ProLoad, EpiStore, 4>(g.N, g.work, g.psi, g.tw, g.Ka, pl, EpiStore{}, st);
+      case 8:
+        return inv ? fftx2<true, ProLoad, EpiStore, 8>(g.N, g.work, g.psi, g.tw, g.Ka, pl, EpiStore{}, st)
+                   : fftx2<false, ProLoad, EpiStore, 8>(g.N, g.work, g.psi, g.tw, g.Ka, pl, EpiStore{}, st);
+      default:
+        return fft2_pdl(g.psi, g.work, g.tw, g.Ka, g.N, inv, st);
+    }
   };
   // the exit kernel carries the previous position's probe update, whose blocks each reduce the tile maxima of the
   // whole object first: two blocks per SM keep that reduction from dominating its one-pixel-per-thread work

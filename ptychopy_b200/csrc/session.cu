@@ -794,17 +794,26 @@ void init_object(pty_session* s) {
   s->objMax0 = 0;  // Sample::clearObjectArray (src/Sample.cpp:216-220); loadarr does not touch it
 }
 
+// The ePIE kernel of a session: the per-position chain (precision = 1, chosen, or automatic where it measured
+// fastest: with several probe modes at 256^2 3.1x the fused cluster kernel, 76.8 vs 237 ms per iteration; at 512^2
+// with one mode 1.15x the whole-GPU kernel, 39.8 vs 45.7 ms), else the shared-memory kernel where it applies and is
+// not overridden, else the cluster or whole-GPU kernel.
+bool epie_uses_chain(const pty_session* s) {
+  const int var = s->epie_variant;
+  return s->prm.precision != 0 || var == 3 || (var < 0 && ((s->K > 1 && s->N >= 256) || s->N >= 512));
+}
+bool epie_uses_sm_kernel(const pty_session* s) {
+  return !epie_uses_chain(s) && epie_uses_smem(s->N, s->K) && (s->epie_variant < 0 || s->epie_variant == 0);
+}
+
 void init_epie(pty_session* s) {
   auto* ep = new EpieState;
   s->ep = ep;
   const size_t NN = size_t(s->N) * s->N, XY = size_t(s->X) * s->Y;
   const int var = s->epie_variant;
   ep->chain_tc = s->prm.precision != 0;
-  // the chain spreads each step over the whole GPU: with several probe modes at 256^2 it measured 3.1x the fused
-  // cluster kernel (5 modes: 76.8 vs 237 ms per iteration), at 512^2 with one mode 1.15x the whole-GPU kernel
-  // (39.8 vs 45.7 ms), so it is the automatic choice there
-  ep->chain = ep->chain_tc || var == 3 || (var < 0 && ((s->K > 1 && s->N >= 256) || s->N >= 512));
-  ep->sm = !ep->chain && epie_uses_smem(s->N, s->K) && (var < 0 || var == 0);
+  ep->chain = epie_uses_chain(s);
+  ep->sm = epie_uses_sm_kernel(s);
   if (ep->chain) {
     if (ep->chain_tc) {
       need(s->N == 256, "precision=1 (tensor-core FFT stages) needs 256 x 256 patterns", PTY_ERR_UNSUPPORTED);
@@ -1480,6 +1489,7 @@ double step_epie(pty_session* s, int it, bool want_err) {
     cg.rms = g.rms;
     cg.useAll = g.useAll;
     cg.tc = ep->chain_tc ? 1 : 0;
+    cg.frows = s->fft_rows;
     const unsigned key = unsigned(Ka) | (unsigned(up) << 8) | (unsigned(pc) << 9) | (unsigned(cg.rms) << 10);
     cudaGraphExec_t& ge = ep->chain_graphs[key];
     if (!ge) {
@@ -1778,9 +1788,10 @@ int pty_init(pty_session* s) {
                                               std::to_string(want));
       run_warm_start(s);
     }
-    // the cluster ePIE kernel's column phase consumes the amplitudes column-wise: transpose each plane once (DM and
-    // the shared-memory ePIE kernel read them in their natural layout)
-    if (s->algo == ALGO_EPIE && !epie_uses_smem(s->N, s->K)) {
+    // the cluster / whole-GPU ePIE kernels and the chain consume the amplitudes column-wise: transpose each plane
+    // once (DM and the shared-memory ePIE kernel read them in their natural layout; which ePIE kernel runs also
+    // depends on the variant the autotuner chose)
+    if (s->algo == ALGO_EPIE && !epie_uses_sm_kernel(s)) {
       DeviceBuf t;
       t.alloc(s->amp.bytes, "transposed patterns");
       check_cuda(transpose_planes(s->amp.as<float>(), t.as<float>(), s->P, s->N, s->stream), "transpose");

@@ -101,6 +101,7 @@ struct pty_session {
   int probe_given_modes = 0;
   std::vector<float> warm_params;  // trained warm-start network (pty_set_warm_start) or empty
   int warm_width = 0;
+  int fft_rows = 0;       // ePIE kernel chain: rows per CTA of its transform passes (0 automatic; set by the autotuner)
   int epie_variant = -1;  // ePIE kernel: -1 automatic, 0 shared-memory cluster, 1 cluster, 2 whole-GPU, 3 a chain
                           // of whole-GPU kernels per position (autotuner; precision = 1 always runs the chain)
 
