@@ -149,9 +149,11 @@ int pty_dm_step_finish(pty_session* s);
 
 /* Autotuner (no counterpart in the reference, which has one launch configuration per kernel).  Before pty_init,
  * with the patterns (and positions, probe, object) set: times the launch variants of the session's algorithm for
- * `iters` iterations each (two interleaved rounds, the faster kept) on temporary sessions with the same inputs (DM: patterns per wave; ePIE: shared-memory
- * cluster, cluster or whole-GPU kernel), keeps the fastest for this session, and writes a one-line summary with
- * every candidate's ms per iteration into `report` (may be NULL).  MLs has no variants. */
+ * `iters` iterations each (two interleaved rounds, the faster kept) on temporary sessions with the same inputs
+ * (DM: patterns per wave, one lane or two lanes of waves in flight; ePIE: shared-memory cluster, cluster or
+ * whole-GPU kernel, or the per-position kernel chain with 2, 4 or 8 rows per CTA in its FFT passes), keeps the
+ * fastest for this session, and writes a one-line summary with every candidate's ms per iteration into `report`
+ * (may be NULL).  MLs has no variants. */
 int pty_autotune(pty_session* s, int iters, char* report, int report_len);
 
 /* Learned warm start (no counterpart in the reference, which starts from a constant object, src/Sample.cpp:216-220,
