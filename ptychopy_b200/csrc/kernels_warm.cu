@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <mutex>
 #include <string>
 
 #include "../../include/ptychopy_b200.h"
@@ -197,6 +198,29 @@ int warm_grid_size(int X, int Y) {
   return M;
 }
 
+// The twiddle table of the M x M Poisson-solve transforms, made once per device and size and kept until the process
+// exits (at most 5 x 4 KB per device): making and freeing it per call cost a device synchronisation each time.
+cudaError_t warm_twiddles(int M, const float2** out, cudaStream_t st) {
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static float2* table[kMaxDevices][10] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int lg = 0;
+  while ((1 << lg) < M) ++lg;
+  if (dev < 0 || dev >= kMaxDevices || (1 << lg) != M || lg >= 10) return cudaErrorInvalidValue;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!table[dev][lg]) {
+    float2* tw = nullptr;
+    e = make_twiddles(M, &tw, st);
+    if (e != cudaSuccess) return e;
+    table[dev][lg] = tw;
+  }
+  *out = table[dev][lg];
+  return cudaSuccess;
+}
+
 }  // namespace pty
 
 using namespace pty;
@@ -233,8 +257,8 @@ int pty_warm_object(const float* acc, int X, int Y, float wmin, float amp_fill, 
   float2* fwork = spec + MM;
   double* sums = reinterpret_cast<double*>(fwork + MM);
   float2* obj = reinterpret_cast<float2*>(obj_c64);
-  float2* tw = nullptr;
-  cudaError_t e = make_twiddles(M, &tw, st);
+  const float2* tw = nullptr;
+  cudaError_t e = warm_twiddles(M, &tw, st);
   if (e != cudaSuccess) return finish(e, "pty_warm_object: twiddles");
   k_warm_pack<<<grid1(MM), 256, 0, st>>>(acc, X, Y, M, wmin, z);
   e = fft2(z, fwork, tw, 1, M, false, st);
@@ -256,7 +280,6 @@ int pty_warm_object(const float* acc, int X, int Y, float wmin, float amp_fill, 
     }
   }
   const cudaError_t e2 = cudaStreamSynchronize(st);
-  cudaFree(tw);
   if (e == cudaSuccess) e = e2;
   return finish(e, "pty_warm_object");
 }
