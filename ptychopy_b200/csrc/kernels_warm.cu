@@ -34,33 +34,52 @@ constexpr int ST = 16;  // object tile side of one stitching CTA
 
 // acc (4 planes of X x Y): sum_p w(x - r_p) A_p, sum_p w gx_p, sum_p w gy_p, sum_p w, over the positions p whose
 // S x S output patch covers the pixel; r_p = round(pos_p) + off.  A CTA owns a 16 x 16 tile and visits the positions
-// in order, so the sums are deterministic.  Network outputs are in scaled units: A = amp_mean + o0 * amp_scale,
-// g = o * grad_scale.
+// in order, so the sums are deterministic: per chunk of 256 positions each thread tests one against the tile, an
+// order-preserving compaction (warp ballots and a scan over the warps) lists the ones whose patch meets the tile, and
+// only those are visited.  Network outputs are in scaled units: A = amp_mean + o0 * amp_scale, g = o * grad_scale.
 __global__ void __launch_bounds__(ST* ST) k_warm_stitch(const float* __restrict__ out, const float* __restrict__ pos,
                                                        int P, const float* __restrict__ wgt, int S, int off,
                                                        float amp_mean, float amp_scale, float grad_scale,
                                                        float* __restrict__ acc, int X, int Y) {
-  __shared__ int s_r[ST * ST], s_c[ST * ST];
+  constexpr int NW = ST * ST / 32;
+  __shared__ int s_r[ST * ST], s_c[ST * ST], s_p[ST * ST];
+  __shared__ int s_wcount[NW];
   const int tilesY = (Y + ST - 1) / ST;
   const int ti = blockIdx.x / tilesY, tj = blockIdx.x % tilesY;
   const int i = ti * ST + threadIdx.x / ST, j = tj * ST + threadIdx.x % ST;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const size_t SS = size_t(S) * S;
   float a = 0.f, gx = 0.f, gy = 0.f, ws = 0.f;
   for (int p0 = 0; p0 < P; p0 += ST * ST) {
     const int p = p0 + threadIdx.x;
+    int r0 = 0, c0 = 0;
+    bool hit = false;
     if (p < P) {
-      s_r[threadIdx.x] = int(rintf(pos[2 * size_t(p)])) + off;
-      s_c[threadIdx.x] = int(rintf(pos[2 * size_t(p) + 1])) + off;
+      r0 = int(rintf(pos[2 * size_t(p)])) + off;
+      c0 = int(rintf(pos[2 * size_t(p) + 1])) + off;
+      hit = !(r0 >= ti * ST + ST || r0 + S <= ti * ST || c0 >= tj * ST + ST || c0 + S <= tj * ST);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, hit);
+    if (lane == 0) s_wcount[warp] = __popc(bal);
+    __syncthreads();
+    int base = 0, cnt = 0;
+    for (int w = 0; w < NW; ++w) {
+      base += w < warp ? s_wcount[w] : 0;
+      cnt += s_wcount[w];
+    }
+    if (hit) {
+      const int k = base + __popc(bal & ((1u << lane) - 1u));
+      s_r[k] = r0;
+      s_c[k] = c0;
+      s_p[k] = p;
     }
     __syncthreads();
-    const int cnt = min(ST * ST, P - p0);
     for (int q = 0; q < cnt; ++q) {
-      const int r0 = s_r[q], c0 = s_c[q];
-      if (r0 >= ti * ST + ST || r0 + S <= ti * ST || c0 >= tj * ST + ST || c0 + S <= tj * ST) continue;
-      const int li = i - r0, lj = j - c0;
+      const int rq = s_r[q], cq = s_c[q];
+      const int li = i - rq, lj = j - cq;
       if (li >= 0 && li < S && lj >= 0 && lj < S) {
         const float wv = wgt[li * S + lj];
-        const float* o = out + size_t(p0 + q) * 3 * SS + size_t(li) * S + lj;
+        const float* o = out + size_t(s_p[q]) * 3 * SS + size_t(li) * S + lj;
         a += wv * (amp_mean + o[0] * amp_scale);
         gx += wv * (o[SS] * grad_scale);
         gy += wv * (o[2 * SS] * grad_scale);
