@@ -230,6 +230,13 @@ cudaError_t warm_twiddles(int M, const float2** out, cudaStream_t st) {
   while ((1 << lg) < M) ++lg;
   if (dev < 0 || dev >= kMaxDevices || (1 << lg) != M || lg >= 10) return cudaErrorInvalidValue;
   std::lock_guard<std::mutex> lock(mu);
+  if (table[dev][lg]) {  // a table from before a device reset is gone: make it again
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, table[dev][lg]) != cudaSuccess || at.type != cudaMemoryTypeDevice) {
+      cudaGetLastError();
+      table[dev][lg] = nullptr;
+    }
+  }
   if (!table[dev][lg]) {
     float2* tw = nullptr;
     e = make_twiddles(M, &tw, st);
