@@ -778,7 +778,7 @@ __global__ void k_to_bf16(const float* __restrict__ x, __nv_bfloat16* __restrict
 // pixels (32 x 32 convolution outputs): the 34 x 34 input halo is transformed once into shared memory, each thread
 // computes one pooled pixel's 2 x 2 outputs for all channels from a 4 x 4 window.
 template <int C1>
-__global__ void __launch_bounds__(256) k_tc_first(const float* __restrict__ amp, const float* __restrict__ w,
+__global__ void __launch_bounds__(256, 4) k_tc_first(const float* __restrict__ amp, const float* __restrict__ w,
                                                   const float* __restrict__ bias, __nv_bfloat16* __restrict__ y, int H,
                                                   int W, float in_scale) {
   __shared__ float s_in[34][35];
