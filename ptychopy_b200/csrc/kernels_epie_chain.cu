@@ -33,10 +33,8 @@ int grid_e(size_t n) {
   return int(g < 1 ? 1 : (g > 1184 ? 1184 : g));
 }
 
-// Probe update of position sp at the pixels of this thread's grid-stride loop (a7): the object max from TM (all
-// blocks compute it), P_k += (1/max |O|^2) conj(O) dpsi_k, |P_k|^2 cache, and the probe maximum into its slot.
-// The same loop as the exit wave's, so that a thread updates exactly the probe pixels it then reads.
-__device__ void ec_probe_update(const EpieChainArgs& g, int sp) {
+// The object max from TM, reduced by every block (1/max |O|^2, the probe update's step); block 0 records it.
+__device__ float ec_object_step(const EpieChainArgs& g) {
   __shared__ float s_om;
   float m = 0.f;
   for (int j = threadIdx.x; j < g.TX * g.TY; j += blockDim.x) m = fmaxf(m, g.TM[j]);
@@ -46,50 +44,82 @@ __device__ void ec_probe_update(const EpieChainArgs& g, int sp) {
     if (blockIdx.x == 0) g.sc->objMax = m;
   }
   __syncthreads();
-  const float cP = 1.0f / s_om;
+  return 1.0f / s_om;
+}
+
+// Probe update of one pixel (a7) for the position at rounded offset (ox, oy): P_k += cP conj(O) dpsi_k, |P_k|^2
+// cache, the pixel's contribution to the probe maximum.  Returns the updated mode-0 value.
+__device__ __forceinline__ float2 ec_probe_pixel(const EpieChainArgs& g, size_t idx, int x, int y, int ox, int oy,
+                                                 float cP, float& pmax) {
+  const size_t NN = size_t(g.N) * g.N;
+  const float2 oc = g.obj[size_t(x + ox) * g.Y + (y + oy)];
+  float modal = 0.f;
+  float2 p0 = make_float2(0.f, 0.f);
+  for (int k = 0; k < g.K; ++k) {
+    float cache;
+    if (k < g.Ka) {
+      const float2 u = cconjmul(oc, g.psi[k * NN + idx]);
+      float2 pv = g.probe[k * NN + idx];
+      pv = make_float2(u.x * cP + pv.x, u.y * cP + pv.y);
+      const float mg = sqrtf(pv.x * pv.x + pv.y * pv.y);
+      g.probe[k * NN + idx] = pv;
+      if (k == 0) p0 = pv;
+      cache = mg * mg;
+      g.pcache[k * NN + idx] = cache;
+    } else {
+      cache = g.pcache[k * NN + idx];
+    }
+    if (g.useAll && g.K > 1)
+      modal += cache;
+    else
+      pmax = fmaxf(pmax, cache);
+  }
+  if (g.useAll && g.K > 1) pmax = fmaxf(pmax, modal);
+  return p0;
+}
+
+__device__ __forceinline__ void ec_probe_max(const EpieChainArgs& g, int sp, float pmax) {
+  pmax = block_reduce_maxf(pmax);
+  if (threadIdx.x == 0) atomicMax(reinterpret_cast<int*>(&g.pmax2[sp & 1]), __float_as_int(pmax));
+}
+
+// Probe update of position sp over this thread's grid-stride loop (the last position's, after the loop over
+// positions).
+__device__ void ec_probe_update(const EpieChainArgs& g, int sp) {
+  const float cP = ec_object_step(g);
   const float2 q = g.pos[g.order[sp]];
   const int ox = int(roundf(q.x)), oy = int(roundf(q.y));
   const int N = g.N;
   const size_t NN = size_t(N) * N;
   float pmax = 0.f;
-  for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
-    const int x = int(idx / N), y = int(idx % N);
-    const float2 oc = g.obj[size_t(x + ox) * g.Y + (y + oy)];
-    float modal = 0.f;
-    for (int k = 0; k < g.K; ++k) {
-      float cache;
-      if (k < g.Ka) {
-        const float2 u = cconjmul(oc, g.psi[k * NN + idx]);
-        float2 pv = g.probe[k * NN + idx];
-        pv = make_float2(u.x * cP + pv.x, u.y * cP + pv.y);
-        const float mg = sqrtf(pv.x * pv.x + pv.y * pv.y);
-        g.probe[k * NN + idx] = pv;
-        cache = mg * mg;
-        g.pcache[k * NN + idx] = cache;
-      } else {
-        cache = g.pcache[k * NN + idx];
-      }
-      if (g.useAll && g.K > 1)
-        modal += cache;
-      else
-        pmax = fmaxf(pmax, cache);
-    }
-    if (g.useAll && g.K > 1) pmax = fmaxf(pmax, modal);
-  }
-  pmax = block_reduce_maxf(pmax);
-  if (threadIdx.x == 0) atomicMax(reinterpret_cast<int*>(&g.pmax2[sp & 1]), __float_as_int(pmax));
+  for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x)
+    ec_probe_pixel(g, idx, int(idx / N), int(idx % N), ox, oy, cP, pmax);
+  ec_probe_max(g, sp, pmax);
 }
 
+// Exit waves of position s, with the previous position's probe update of the same pixel first (pixel-local: the
+// thread that updates a probe pixel is the one that then multiplies it into the patch).
 __global__ void k_ec_exit(EpieChainArgs g, int s) {
   pdl_enter();
-  if (g.up && s > 0) ec_probe_update(g, s - 1);  // the previous position's probe update, pixel by pixel
+  const bool upd = g.up && s > 0;
+  float cP = 0.f;
+  int pox = 0, poy = 0;
+  if (upd) {
+    cP = ec_object_step(g);
+    const float2 pq = g.pos[g.order[s - 1]];
+    pox = int(roundf(pq.x));
+    poy = int(roundf(pq.y));
+  }
   const int i = g.order[s];
   const float2 q = g.pos[i];
   const int N = g.N;
   const size_t NN = size_t(N) * N;
   if (g.up && blockIdx.x == 0 && threadIdx.x == 0) g.pmax2[s & 1] = 0.f;  // this position's probe maximum
+  float pmax = 0.f;
   for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
     const int x = int(idx / N), y = int(idx % N);
+    float2 p0 = make_float2(0.f, 0.f);
+    if (upd) p0 = ec_probe_pixel(g, idx, x, y, pox, poy, cP, pmax);
     int r0, r1, c0, c1;
     float wb, wa;
     tex_axis(q.x, x, g.X, r0, r1, wb);
@@ -99,8 +129,9 @@ __global__ void k_ec_exit(EpieChainArgs g, int s) {
     const float w00 = (1.f - wa) * (1.f - wb), w01 = wa * (1.f - wb), w10 = (1.f - wa) * wb, w11 = wa * wb;
     const float2 patch = make_float2(v00.x * w00 + v01.x * w01 + v10.x * w10 + v11.x * w11,
                                      v00.y * w00 + v01.y * w01 + v10.y * w10 + v11.y * w11);
-    for (int k = 0; k < g.Ka; ++k) g.psi[k * NN + idx] = cmul(patch, g.probe[k * NN + idx]);
+    for (int k = 0; k < g.Ka; ++k) g.psi[k * NN + idx] = cmul(patch, (upd && k == 0) ? p0 : g.probe[k * NN + idx]);
   }
+  if (upd) ec_probe_max(g, s - 1, pmax);
 }
 
 __global__ void k_ec_modulus(EpieChainArgs g, int s) {
