@@ -40,7 +40,7 @@ struct EpieArgs {
 // ePIE as a chain of whole-GPU kernels per position (kernels_epie_chain.cu): the precision = 1 path, whose 2-D
 // transforms run as split-BF16 tensor-core stages (tc = 1, N = 256).  Same update as k_epie.
 struct EpieChainArgs {
-  const float* ampT;      // P x N x N amplitudes, transposed (A(x, y) at [y N + x])
+  const float* amp;       // P x N x N amplitudes in their natural layout (A(x, y) at [x N + y])
   float2* obj;
   float* ocache;
   float2* probe;

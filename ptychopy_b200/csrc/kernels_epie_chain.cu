@@ -140,11 +140,10 @@ __global__ void k_ec_modulus(EpieChainArgs g, int s) {
   const int N = g.N;
   const size_t NN = size_t(N) * N;
   const float nrm = 1.f / float(NN);
-  const float* Ai = g.ampT + size_t(i) * NN;  // transposed: A(x, y) at [y N + x]
+  const float* Ai = g.amp + size_t(i) * NN;  // natural layout, as psi: A(x, y) at [x N + y]
   double err = 0.0;
   for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
-    const int x = int(idx / N), y = int(idx % N);
-    const float A = Ai[size_t(y) * N + x];
+    const float A = Ai[idx];
     if (g.Ka == 1) {
       const float2 psi = g.psi[idx];
       if (g.rms) err += fabsf(A - sqrtf(psi.x * psi.x + psi.y * psi.y));

@@ -1460,7 +1460,7 @@ double step_epie(pty_session* s, int it, bool want_err) {
   g.gerr = reinterpret_cast<int*>(ep->gsync.as<unsigned>() + 2);
   if (ep->chain) {
     EpieChainArgs cg;
-    cg.ampT = g.ampT;
+    cg.amp = g.ampT;  // natural layout: the session transposes the planes only for the cluster / whole-GPU kernels
     cg.obj = g.obj;
     cg.ocache = g.ocache;
     cg.probe = g.probe;
@@ -1788,10 +1788,10 @@ int pty_init(pty_session* s) {
                                               std::to_string(want));
       run_warm_start(s);
     }
-    // the cluster / whole-GPU ePIE kernels and the chain consume the amplitudes column-wise: transpose each plane
-    // once (DM and the shared-memory ePIE kernel read them in their natural layout; which ePIE kernel runs also
-    // depends on the variant the autotuner chose)
-    if (s->algo == ALGO_EPIE && !epie_uses_sm_kernel(s)) {
+    // the cluster / whole-GPU ePIE kernels consume the amplitudes column-wise: transpose each plane once (DM, the
+    // shared-memory ePIE kernel and the chain, whose modulus step walks the plane as its transforms leave it, read
+    // them in their natural layout; which ePIE kernel runs also depends on the variant the autotuner chose)
+    if (s->algo == ALGO_EPIE && !epie_uses_sm_kernel(s) && !epie_uses_chain(s)) {
       DeviceBuf t;
       t.alloc(s->amp.bytes, "transposed patterns");
       check_cuda(transpose_planes(s->amp.as<float>(), t.as<float>(), s->P, s->N, s->stream), "transpose");
