@@ -37,7 +37,14 @@ int grid_e(size_t n) {
 __device__ float ec_object_step(const EpieChainArgs& g) {
   __shared__ float s_om;
   float m = 0.f;
-  for (int j = threadIdx.x; j < g.TX * g.TY; j += blockDim.x) m = fmaxf(m, g.TM[j]);
+  const int n = g.TX * g.TY;
+  const int n4 = (reinterpret_cast<uintptr_t>(g.TM) & 15) ? 0 : n / 4;  // 16-byte vectors, then the tail
+  const float4* tm4 = reinterpret_cast<const float4*>(g.TM);
+  for (int j = threadIdx.x; j < n4; j += blockDim.x) {
+    const float4 v = tm4[j];
+    m = fmaxf(m, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+  }
+  for (int j = 4 * n4 + threadIdx.x; j < n; j += blockDim.x) m = fmaxf(m, g.TM[j]);
   m = block_reduce_maxf(m);
   if (threadIdx.x == 0) {
     s_om = m;
