@@ -40,9 +40,20 @@ __device__ float ec_object_step(const EpieChainArgs& g) {
   const int n = g.TX * g.TY;
   const int n4 = (reinterpret_cast<uintptr_t>(g.TM) & 15) ? 0 : n / 4;  // 16-byte vectors, then the tail
   const float4* tm4 = reinterpret_cast<const float4*>(g.TM);
-  for (int j = threadIdx.x; j < n4; j += blockDim.x) {
-    const float4 v = tm4[j];
-    m = fmaxf(m, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+  // the first TMV vectors of each thread are loaded before any is used, so their L2 latencies overlap (a plain
+  // strided loop waits for each load before issuing the next)
+  constexpr int TMV = 8;
+  float4 v[TMV];
+#pragma unroll
+  for (int u = 0; u < TMV; ++u) {
+    const int j = threadIdx.x + u * blockDim.x;
+    v[u] = j < n4 ? tm4[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+#pragma unroll
+  for (int u = 0; u < TMV; ++u) m = fmaxf(m, fmaxf(fmaxf(v[u].x, v[u].y), fmaxf(v[u].z, v[u].w)));
+  for (int j = threadIdx.x + TMV * blockDim.x; j < n4; j += blockDim.x) {
+    const float4 w = tm4[j];
+    m = fmaxf(m, fmaxf(fmaxf(w.x, w.y), fmaxf(w.z, w.w)));
   }
   for (int j = 4 * n4 + threadIdx.x; j < n; j += blockDim.x) m = fmaxf(m, g.TM[j]);
   m = block_reduce_maxf(m);
@@ -125,14 +136,16 @@ __global__ void k_ec_exit(EpieChainArgs g, int s) {
   float pmax = 0.f;
   for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
     const int x = int(idx / N), y = int(idx % N);
-    float2 p0 = make_float2(0.f, 0.f);
-    if (upd) p0 = ec_probe_pixel(g, idx, x, y, pox, poy, cP, pmax);
+    // the patch gathers first: the probe update's stores would otherwise hold them back (the compiler cannot move a
+    // load of the object above a store through the probe pointers)
     int r0, r1, c0, c1;
     float wb, wa;
     tex_axis(q.x, x, g.X, r0, r1, wb);
     tex_axis(q.y, y, g.Y, c0, c1, wa);
     const float2 v00 = g.obj[size_t(r0) * g.Y + c0], v01 = g.obj[size_t(r0) * g.Y + c1];
     const float2 v10 = g.obj[size_t(r1) * g.Y + c0], v11 = g.obj[size_t(r1) * g.Y + c1];
+    float2 p0 = make_float2(0.f, 0.f);
+    if (upd) p0 = ec_probe_pixel(g, idx, x, y, pox, poy, cP, pmax);
     const float w00 = (1.f - wa) * (1.f - wb), w01 = wa * (1.f - wb), w10 = (1.f - wa) * wb, w11 = wa * wb;
     const float2 patch = make_float2(v00.x * w00 + v01.x * w01 + v10.x * w10 + v11.x * w11,
                                      v00.y * w00 + v01.y * w01 + v10.y * w10 + v11.y * w11);
