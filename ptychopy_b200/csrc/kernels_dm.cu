@@ -127,21 +127,31 @@ __device__ __forceinline__ void dm_item_inv(const DMBuffers& b, int p, int slot,
   float2* dorow = b.dO + size_t(x + o.x) * b.Y + o.y;
   float2* psrow = b.psi + (size_t(p) * L + x) * L;
   float2* dprow = b.dP + size_t(x) * L;
-  static_for<0, E>([&](auto ec) {
-    constexpr int e = decltype(ec)::value;
-    const int n = t + T * e;
-    const float2 pn = a[out_slot<L>(e)];
-    st_stream(psrow + n, pn);
-    // the increments are accumulated unscaled: finalize multiplies the sums by f1 (object) and f0 (probe), which as
-    // positive factors commute with the phase clamp
-    const float2 pv = prow[n];
-    float2 inc = cconjmul(pv, pn);
-    if constexpr (PC) inc = constrain_phase(inc);
-    atomicAdd(dorow + n, inc);
-    if constexpr (UP) {
-      const float2 ov = orow[n];
-      atomicAdd(dprow + n, cconjmul(ov, pn));
-    }
+  // probe (and object) values in batches of DB elements, loaded before the batch's stores and atomics: a load placed
+  // after a store it might alias waits for it, which would leave one L2 round trip per element
+  constexpr int DB = UP ? 2 : 4;
+  static_assert(E % DB == 0, "epilogue batches");
+  static_for<0, E / DB>([&](auto bc) {
+    constexpr int e0 = decltype(bc)::value * DB;
+    float2 pv[DB];
+    [[maybe_unused]] float2 ov[DB];
+    static_for<0, DB>([&](auto jc) {
+      constexpr int j = decltype(jc)::value;
+      pv[j] = prow[t + T * (e0 + j)];
+      if constexpr (UP) ov[j] = orow[t + T * (e0 + j)];
+    });
+    static_for<0, DB>([&](auto jc) {
+      constexpr int j = decltype(jc)::value;
+      const int n = t + T * (e0 + j);
+      const float2 pn = a[out_slot<L>(e0 + j)];
+      st_stream(psrow + n, pn);
+      // the increments are accumulated unscaled: finalize multiplies the sums by f1 (object) and f0 (probe), which
+      // as positive factors commute with the phase clamp
+      float2 inc = cconjmul(pv[j], pn);
+      if constexpr (PC) inc = constrain_phase(inc);
+      atomicAdd(dorow + n, inc);
+      if constexpr (UP) atomicAdd(dprow + n, cconjmul(ov[j], pn));
+    });
   });
 }
 
