@@ -115,6 +115,29 @@ __device__ void ec_probe_update(const EpieChainArgs& g, int sp) {
   ec_probe_max(g, sp, pmax);
 }
 
+// The global loads of one pixel of the exit kernel (one mode): the four bilinear taps of the patch and their weights,
+// and for the probe update the object at the previous position, the returned dpsi and the probe.
+struct ExitLoads {
+  float2 v00, v01, v10, v11, oc, ps, pr;
+  float wa, wb;
+};
+__device__ __forceinline__ void ec_exit_loads(const EpieChainArgs& g, float2 q, size_t idx, int pox, int poy,
+                                              bool upd, ExitLoads& l) {
+  const int x = int(idx / g.N), y = int(idx % g.N);
+  int r0, r1, c0, c1;
+  tex_axis(q.x, x, g.X, r0, r1, l.wb);
+  tex_axis(q.y, y, g.Y, c0, c1, l.wa);
+  l.v00 = g.obj[size_t(r0) * g.Y + c0];
+  l.v01 = g.obj[size_t(r0) * g.Y + c1];
+  l.v10 = g.obj[size_t(r1) * g.Y + c0];
+  l.v11 = g.obj[size_t(r1) * g.Y + c1];
+  if (upd) {
+    l.oc = g.obj[size_t(x + pox) * g.Y + (y + poy)];
+    l.ps = g.psi[idx];
+  }
+  l.pr = g.probe[idx];
+}
+
 // Exit waves of position s, with the previous position's probe update of the same pixel first (pixel-local: the
 // thread that updates a probe pixel is the one that then multiplies it into the patch).
 __global__ void k_ec_exit(EpieChainArgs g, int s) {
@@ -134,7 +157,34 @@ __global__ void k_ec_exit(EpieChainArgs g, int s) {
   const size_t NN = size_t(N) * N;
   if (g.up && blockIdx.x == 0 && threadIdx.x == 0) g.pmax2[s & 1] = 0.f;  // this position's probe maximum
   float pmax = 0.f;
-  for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
+  const size_t start = blockIdx.x * size_t(blockDim.x) + threadIdx.x, stride = size_t(gridDim.x) * blockDim.x;
+  if (g.K == 1 && g.Ka == 1) {
+    // one mode: the loop is software-pipelined, the next pixel's loads issued before this pixel's stores (which
+    // they would otherwise wait for: the compiler cannot tell that they do not alias)
+    ExitLoads cur{}, nxt{};
+    if (start < NN) ec_exit_loads(g, q, start, pox, poy, upd, cur);
+    for (size_t idx = start; idx < NN; idx += stride) {
+      if (idx + stride < NN) ec_exit_loads(g, q, idx + stride, pox, poy, upd, nxt);
+      float2 pv = cur.pr;
+      if (upd) {
+        const float2 u = cconjmul(cur.oc, cur.ps);
+        pv = make_float2(u.x * cP + pv.x, u.y * cP + pv.y);
+        const float mg = sqrtf(pv.x * pv.x + pv.y * pv.y);
+        g.probe[idx] = pv;
+        g.pcache[idx] = mg * mg;
+        pmax = fmaxf(pmax, mg * mg);
+      }
+      const float wa = cur.wa, wb = cur.wb;
+      const float w00 = (1.f - wa) * (1.f - wb), w01 = wa * (1.f - wb), w10 = (1.f - wa) * wb, w11 = wa * wb;
+      const float2 patch = make_float2(cur.v00.x * w00 + cur.v01.x * w01 + cur.v10.x * w10 + cur.v11.x * w11,
+                                       cur.v00.y * w00 + cur.v01.y * w01 + cur.v10.y * w10 + cur.v11.y * w11);
+      g.psi[idx] = cmul(patch, pv);
+      cur = nxt;
+    }
+    if (upd) ec_probe_max(g, s - 1, pmax);
+    return;
+  }
+  for (size_t idx = start; idx < NN; idx += stride) {
     const int x = int(idx / N), y = int(idx % N);
     // the patch gathers first: the probe update's stores would otherwise hold them back (the compiler cannot move a
     // load of the object above a store through the probe pointers)
