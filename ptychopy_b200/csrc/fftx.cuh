@@ -60,10 +60,10 @@ template <int L, bool INV, class Pro, class Epi, int R = FftShape<L>::RC>
 __global__ void __launch_bounds__(R * FftShape<L>::T) k_fftx_pass(float2* __restrict__ out,
                                                                   const float2* __restrict__ g_tw, Pro pro, Epi epi) {
   static_assert(R * FftShape<L>::T % 32 == 0, "whole warps per CTA");
-  pdl_enter();
   extern __shared__ float4 smem4[];
   float2* smem = reinterpret_cast<float2*>(smem4);
-  load_twiddles<L>(smem, g_tw);
+  load_twiddles<L>(smem, g_tw);  // a table written before any transform runs: loaded before the wait
+  pdl_enter();
   fftx_rows<L, INV, Pro, Epi, R>(out, smem, smem + L, blockIdx.y, blockIdx.x * R, pro, epi);
   epi.finish(blockIdx.y);
 }

@@ -141,18 +141,18 @@ __device__ __forceinline__ void ec_exit_loads(const EpieChainArgs& g, float2 q, 
 // Exit waves of position s, with the previous position's probe update of the same pixel first (pixel-local: the
 // thread that updates a probe pixel is the one that then multiplies it into the patch).
 __global__ void k_ec_exit(EpieChainArgs g, int s) {
-  pdl_enter();
+  // the visiting order and the positions stay fixed during an iteration (written before it starts): read before the
+  // wait for the previous kernel, so their latency overlaps its tail
   const bool upd = g.up && s > 0;
-  float cP = 0.f;
+  const float2 q = g.pos[g.order[s]];
   int pox = 0, poy = 0;
   if (upd) {
-    cP = ec_object_step(g);
     const float2 pq = g.pos[g.order[s - 1]];
     pox = int(roundf(pq.x));
     poy = int(roundf(pq.y));
   }
-  const int i = g.order[s];
-  const float2 q = g.pos[i];
+  pdl_enter();
+  const float cP = upd ? ec_object_step(g) : 0.f;
   const int N = g.N;
   const size_t NN = size_t(N) * N;
   if (g.up && blockIdx.x == 0 && threadIdx.x == 0) g.pmax2[s & 1] = 0.f;  // this position's probe maximum
@@ -205,15 +205,20 @@ __global__ void k_ec_exit(EpieChainArgs g, int s) {
 }
 
 __global__ void k_ec_modulus(EpieChainArgs g, int s) {
-  pdl_enter();
+  // the order and the amplitudes are fixed during an iteration: the thread's first amplitude and the pattern's sum
+  // are loaded before the wait for the previous kernel
   const int i = g.order[s];
   const int N = g.N;
   const size_t NN = size_t(N) * N;
   const float nrm = 1.f / float(NN);
   const float* Ai = g.amp + size_t(i) * NN;  // natural layout, as psi: A(x, y) at [x N + y]
+  const size_t start = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+  const float A0 = start < NN ? Ai[start] : 0.f;
+  const double sq = g.rms ? double(g.sqsum[i]) : 1.0;
+  pdl_enter();
   double err = 0.0;
-  for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
-    const float A = Ai[idx];
+  for (size_t idx = start; idx < NN; idx += size_t(gridDim.x) * blockDim.x) {
+    const float A = idx == start ? A0 : Ai[idx];
     if (g.Ka == 1) {
       const float2 psi = g.psi[idx];
       if (g.rms) err += fabsf(A - sqrtf(psi.x * psi.x + psi.y * psi.y));
@@ -241,7 +246,7 @@ __global__ void k_ec_modulus(EpieChainArgs g, int s) {
   }
   if (g.rms) {
     const double e = block_reduce_sum(err);
-    if (threadIdx.x == 0) atomicAdd(&g.sc->err, e / double(g.Ka) / double(g.sqsum[i]));
+    if (threadIdx.x == 0) atomicAdd(&g.sc->err, e / double(g.Ka) / sq);
   }
 }
 
@@ -249,11 +254,11 @@ __global__ void k_ec_modulus(EpieChainArgs g, int s) {
 // its cell when the patch covers it (as k_ec_object), then the block writes the tile's maximum of |O|^2 (cells
 // outside the patch unchanged) into TM
 __global__ void __launch_bounds__(256) k_ec_object_tiles(EpieChainArgs g, int s) {
-  pdl_enter();
-  const int i = g.order[s];
+  const int i = g.order[s];  // order and positions are fixed during an iteration: read before the wait
   const float2 q = g.pos[i];
   const int ox = int(roundf(q.x)), oy = int(roundf(q.y)), N = g.N;
   const int tr0 = ox / 16, tc0 = oy / 16, ntc = (oy + N - 1) / 16 - tc0 + 1, ntr = (ox + N - 1) / 16 - tr0 + 1;
+  pdl_enter();
   if (int(blockIdx.x) >= ntr * ntc) return;  // the grid covers the most tiles a patch can touch
   const int tr = tr0 + int(blockIdx.x) / ntc, tc = tc0 + int(blockIdx.x) % ntc;
   const int xr = tr * 16 + int(threadIdx.x) / 16, yc = tc * 16 + int(threadIdx.x) % 16;
