@@ -152,17 +152,18 @@ __global__ void k_ec_exit(EpieChainArgs g, int s) {
     poy = int(roundf(pq.y));
   }
   pdl_enter();
-  const float cP = upd ? ec_object_step(g) : 0.f;
   const int N = g.N;
   const size_t NN = size_t(N) * N;
-  if (g.up && blockIdx.x == 0 && threadIdx.x == 0) g.pmax2[s & 1] = 0.f;  // this position's probe maximum
-  float pmax = 0.f;
   const size_t start = blockIdx.x * size_t(blockDim.x) + threadIdx.x, stride = size_t(gridDim.x) * blockDim.x;
+  float pmax = 0.f;
   if (g.K == 1 && g.Ka == 1) {
     // one mode: the loop is software-pipelined, the next pixel's loads issued before this pixel's stores (which
-    // they would otherwise wait for: the compiler cannot tell that they do not alias)
+    // they would otherwise wait for: the compiler cannot tell that they do not alias); the first pixel's loads go
+    // out before the object-maximum reduction, whose latency they then share
     ExitLoads cur{}, nxt{};
     if (start < NN) ec_exit_loads(g, q, start, pox, poy, upd, cur);
+    const float cP = upd ? ec_object_step(g) : 0.f;
+    if (g.up && blockIdx.x == 0 && threadIdx.x == 0) g.pmax2[s & 1] = 0.f;  // this position's probe maximum
     for (size_t idx = start; idx < NN; idx += stride) {
       if (idx + stride < NN) ec_exit_loads(g, q, idx + stride, pox, poy, upd, nxt);
       float2 pv = cur.pr;
@@ -184,6 +185,8 @@ __global__ void k_ec_exit(EpieChainArgs g, int s) {
     if (upd) ec_probe_max(g, s - 1, pmax);
     return;
   }
+  const float cP = upd ? ec_object_step(g) : 0.f;
+  if (g.up && blockIdx.x == 0 && threadIdx.x == 0) g.pmax2[s & 1] = 0.f;  // this position's probe maximum
   for (size_t idx = start; idx < NN; idx += stride) {
     const int x = int(idx / N), y = int(idx % N);
     // the patch gathers first: the probe update's stores would otherwise hold them back (the compiler cannot move a
