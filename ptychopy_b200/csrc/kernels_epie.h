@@ -60,7 +60,7 @@ struct EpieChainArgs {
   int frows;              // rows per CTA of the FP32 transform passes (0: automatic; 2, 4, 8: capped by the default)
 };
 cudaError_t epie_chain_iteration(const EpieChainArgs& g, cudaStream_t st);
-int epie_chain_launches(int P, bool up);
+int epie_chain_launches(const EpieChainArgs& g);
 
 // Sets kernel attributes and picks the cluster size (largest resident of 16, 8, ...); returns it in C_out.
 cudaError_t epie_prepare(int N, int* C_out);

@@ -299,6 +299,72 @@ __global__ void k_ec_finish(EpieChainArgs g) {
   ec_probe_update(g, g.P - 1);
 }
 
+// One mode at L = 512: the second pass of the forward transform with the modulus step of k_ec_modulus in its
+// epilogue (the same arithmetic per element, so the same result), one launch fewer per position.  The CTA transforms
+// rows x0 .. x0 + R - 1 of the transposed work plane and stores columns x0 .. x0 + R - 1 of Psi in its natural layout;
+// the amplitudes of those elements are fixed during the iteration, so each thread loads its share before the wait for
+// the first pass (in the epilogue each load would wait for the previous element's store, which it might alias).
+template <int L, int R>
+__global__ void __launch_bounds__(R * FftShape<L>::T) k_ec_fwd2_modulus(EpieChainArgs g, int s) {
+  using S = FftShape<L>;
+  constexpr int T = S::T, E = S::E, NT = R * T, KPT = L * R / NT;
+  static_assert(NT % 32 == 0 && NT % R == 0, "whole warps, whole store rows");
+  extern __shared__ float4 smem4[];
+  float2* s_tw = reinterpret_cast<float2*>(smem4);
+  float2* s_x = s_tw + L;
+  load_twiddles<L>(s_tw, g.tw);
+  const int i = g.order[s];
+  const int x0 = int(blockIdx.x) * R;
+  const int v = threadIdx.x / T, t = threadIdx.x % T;  // transform: row x0 + v, lane t
+  const int vv = threadIdx.x % R, n0 = threadIdx.x / R;  // store: column x0 + vv, rows n0 + T k
+  const float* Ai = g.amp + size_t(i) * L * L + x0 + vv;
+  float Av[KPT];
+#pragma unroll
+  for (int k = 0; k < KPT; ++k) Av[k] = Ai[size_t(n0 + k * T) * L];
+  const double sq = g.rms ? g.sqsum[i] : 1.0;
+  pdl_enter();
+  __syncthreads();  // twiddles
+  float2 a[E];
+  const float2* wrow = g.work + size_t(x0 + v) * L;
+#pragma unroll
+  for (int e = 0; e < E; ++e) a[e] = wrow[t + T * e];
+  fft_vec<L, false>(a, t, s_x + v * S::XCH, s_tw);
+  __syncthreads();  // the staging tile aliases the exchange buffers of other warps
+  static_for<0, E>([&](auto ec) {
+    constexpr int e = decltype(ec)::value;
+    s_x[(t + T * e) * (R + 1) + v] = a[out_slot<L>(e)];
+  });
+  __syncthreads();
+  const float nrm = 1.f / float(L * L);
+  double err = 0.0;
+#pragma unroll
+  for (int k = 0; k < KPT; ++k) {
+    const int n = n0 + k * T;
+    const float2 psi = s_x[n * (R + 1) + vv];
+    const float A = Av[k];
+    if (g.rms) err += fabsf(A - sqrtf(psi.x * psi.x + psi.y * psi.y));
+    float2 rep;
+    if (A - g.saturation >= 0.f)
+      rep = make_float2(psi.x * nrm, psi.y * nrm);  // floating pixel: no modulus
+    else
+      rep = modulus_replace(psi, A * nrm);
+    g.psi[size_t(n) * L + x0 + vv] = make_float2(rep.x - psi.x * nrm, rep.y - psi.y * nrm);
+  }
+  if (g.rms) {
+    const double e = block_reduce_sum(err);
+    if (threadIdx.x == 0) atomicAdd(&g.sc->err, e / sq);
+  }
+}
+
+// The forward transform of one mode at 512^2 with the modulus step fused into its second pass (R rows per CTA).
+template <int R>
+cudaError_t ec_forward_modulus(const EpieChainArgs& g, int s, cudaStream_t st) {
+  constexpr int L = 512;
+  cudaError_t e = launch_fftx<L, false, R>(g.work, g.tw, 1, ProLoad{g.psi}, EpiStore{}, st);
+  if (e != cudaSuccess) return e;
+  return launch_pdl(k_ec_fwd2_modulus<L, R>, dim3(L / R), R * FftShape<L>::T, rows_smem_bytes_r<L, R>(), st, g, s);
+}
+
 __global__ void k_ec_scalars(EpieChainArgs g) {
   pdl_enter();
   if (threadIdx.x == 0 && blockIdx.x == 0 && g.up && g.P > 0) g.sc->probeMax = g.pmax2[(g.P - 1) & 1];
@@ -306,14 +372,24 @@ __global__ void k_ec_scalars(EpieChainArgs g) {
 
 }  // namespace
 
+namespace {
+// rows per CTA of the FP32 transform passes (g.frows; 0: 4 at 512^2, where one plane's 512 rows then spread over
+// 128 CTAs instead of 64: 35.0 against 36.6 ms per 900-position iteration; the default tile elsewhere)
+int ec_rows(const EpieChainArgs& g) { return g.frows > 0 ? g.frows : (g.N == 512 ? 4 : 0); }
+// one mode at 512^2 with FP32 transforms of 2, 4 or 8 rows per CTA: the modulus step runs in the second forward pass
+bool ec_fused_modulus(const EpieChainArgs& g) {
+  const int rows = ec_rows(g);
+  return !g.tc && g.K == 1 && g.Ka == 1 && g.N == 512 && (rows == 2 || rows == 4 || rows == 8);
+}
+}  // namespace
+
 cudaError_t epie_chain_iteration(const EpieChainArgs& g, cudaStream_t st) {
   const size_t NN = size_t(g.N) * g.N;
   const int gb = grid_e(NN);
   const int tiles = ((g.N + 15) / 16 + 1) * ((g.N + 15) / 16 + 1);
   cudaError_t e;
-  // rows per CTA of the FP32 transform passes (g.frows; 0: 4 at 512^2, where one plane's 512 rows then spread over
-  // 128 CTAs instead of 64: 35.0 against 36.6 ms per 900-position iteration; the default tile elsewhere)
-  const int rows = g.frows > 0 ? g.frows : (g.N == 512 ? 4 : 0);
+  const int rows = ec_rows(g);
+  const bool fused = ec_fused_modulus(g);
   auto fft = [&](bool inv) -> cudaError_t {
     if (g.tc) return fft2_tc(g.psi, g.work, g.Ka, g.N, inv, g.tcerr, st);
     const ProLoad pl{g.psi};
@@ -341,8 +417,14 @@ cudaError_t epie_chain_iteration(const EpieChainArgs& g, cudaStream_t st) {
   const int gx = g.up ? std::min(gb, 2 * sms) : gb;
   for (int s = 0; s < g.P; ++s) {
     if ((e = launch_pdl(k_ec_exit, gx, 256, 0, st, g, s)) != cudaSuccess) return e;
-    if ((e = fft(false)) != cudaSuccess) return e;
-    if ((e = launch_pdl(k_ec_modulus, gb, 256, 0, st, g, s)) != cudaSuccess) return e;
+    if (fused) {
+      e = rows == 2 ? ec_forward_modulus<2>(g, s, st) : rows == 4 ? ec_forward_modulus<4>(g, s, st)
+                                                              : ec_forward_modulus<8>(g, s, st);
+      if (e != cudaSuccess) return e;
+    } else {
+      if ((e = fft(false)) != cudaSuccess) return e;
+      if ((e = launch_pdl(k_ec_modulus, gb, 256, 0, st, g, s)) != cudaSuccess) return e;
+    }
     if ((e = fft(true)) != cudaSuccess) return e;
     // one block per tile the patch touches: the tile count depends on the position's offset within a tile, so the
     // grid covers the most a patch can touch and blocks past this position's tiles return
@@ -352,6 +434,6 @@ cudaError_t epie_chain_iteration(const EpieChainArgs& g, cudaStream_t st) {
   return launch_pdl(k_ec_scalars, 1, 32, 0, st, g);
 }
 
-int epie_chain_launches(int P, bool) { return P * 7 + 2; }
+int epie_chain_launches(const EpieChainArgs& g) { return g.P * (ec_fused_modulus(g) ? 6 : 7) + 2; }
 
 }  // namespace pty

@@ -1505,7 +1505,7 @@ double step_epie(pty_session* s, int it, bool want_err) {
       check_cuda(e3, "graph instantiate");
     }
     check_cuda(cudaGraphLaunch(ge, s->stream), "ePIE chain");
-    s->launches += epie_chain_launches(s->P, up);
+    s->launches += epie_chain_launches(cg);
     if (ep->chain_tc) {  // the tensor-core transforms report a wait timeout through their device flag
       int flag = 0;
       check_cuda(cudaMemcpyAsync(&flag, cg.tcerr, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H flag");
