@@ -91,6 +91,17 @@ typedef struct pty_session pty_session;
  * ptychopy_algorithmnp (src/ptychopy.c:282-323). */
 int pty_params_init(pty_params* p);
 
+/* Fill `p` from a command-line string in the format of the reference's `ptycho` program, e.g.
+ * "./ptycho -jobID=sim -scanDims=30,30 -step=50e-9,50e-9 -i=100 -size=256 -lambda=2.48e-10 -dx_d=172e-6 -z=1
+ * -simulate=1": white-space separated "-name=value" options after the program name, over the command line's own
+ * defaults (beamSize 1e-7, lambda 2.48e-10, z 1, scanDims 12 x 12, size 256, PPS 5; the rest as pty_params_init),
+ * each option with the reference's range check.  Names match exactly, ignoring case; the last occurrence wins.
+ * PTY_ERR_UNSUPPORTED for a non-zero `drift` or a `bitDepth` other than 32, PTY_ERR_INVALID for a text value longer
+ * than its field; `p` is left unchanged on an error.  Replaces the tokeniser of the command-string entry points
+ * (src/ptychopy.c:543-576) and Parameters::parseFromCommandLine (src/Parameters.cpp:66-375) with the defaults of
+ * src/Parameters.h:67-170. */
+int pty_params_from_cmdline(const char* cmdstr, pty_params* p);
+
 /* Create a reconstruction session on p->device.  Replaces `new IPhaser` + CXParams::parseFromCPython
  * (src/ptychopy.c:474-482, src/Parameters.cpp:380-653); the parameter struct is per session, not a
  * process-wide singleton. */

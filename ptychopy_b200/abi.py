@@ -35,7 +35,7 @@ EXPORTS = [
     "pty_warm_object", "pty_dm_psi_from_object", "pty_tc_weights_size", "pty_tc_pack_weights", "pty_tc_conv3x3",
     "pty_tc_pool2", "pty_tc_up2", "pty_tc_to_bf16", "pty_tc_first_layer", "pty_tc_last_layer", "pty_set_warm_start",
     "pty_selftest_bounded_waits", "pty_fft2_tc", "pty_autotune", "pty_get_mls_state",
-    "pty_release_cached_memory", "pty_preprocess_patterns", "pty_get_patterns",
+    "pty_release_cached_memory", "pty_preprocess_patterns", "pty_get_patterns", "pty_params_from_cmdline",
 ]
 
 
@@ -74,6 +74,7 @@ def lib():
         vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
         sig = {
             "pty_params_init": ([ctypes.POINTER(PtyParams)], ctypes.c_int),
+            "pty_params_from_cmdline": ([ctypes.c_char_p, ctypes.POINTER(PtyParams)], ctypes.c_int),
             "pty_session_create": ([ctypes.POINTER(PtyParams), ctypes.POINTER(vp)], ctypes.c_int),
             "pty_session_destroy": ([vp], ctypes.c_int),
             "pty_set_patterns": ([vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),

@@ -21,7 +21,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xco
 CU_SOURCES = ["kernels_common.cu", "kernels_dm.cu", "kernels_epie.cu", "kernels_mls.cu", "session.cu",
               "noalloc.cu", "kernels_nn.cu", "kernels_warm.cu", "kernels_tc.cu",
               "warm_start.cu", "kernels_fft_tc.cu", "autotune.cu", "kernels_mls_var.cu", "kernels_epie_chain.cu",
-              "ingest.cu", "sim_mode.cu", "kernels_dm_tc.cu"]
+              "ingest.cu", "sim_mode.cu", "kernels_dm_tc.cu", "cmdline.cpp"]
 HEADERS = ["fft_core.cuh", "kernel_util.cuh", "kernels.h", "kernels_epie.h", "kernels_mls.h", "session.h", "umma.cuh", "pdl.cuh", "fftx.cuh"]
 
 LIB = os.path.join(HERE, "libptychopy_b200.so")
@@ -48,7 +48,7 @@ def build(force=False, verbose=True):
     objs = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
         if force or _newer(o, [s] + hdrs):
             _run([NVCC] + NVFLAGS + ["-c", s, "-o", o], verbose)
         objs.append(o)

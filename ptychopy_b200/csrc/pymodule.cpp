@@ -11,7 +11,8 @@
 //     reference's command-line option);
 //     probeNP may be (K, N, N) to supply all probe modes.
 // Whole-mode runs from data files (epie / dm / mls with fp) read .bin and .csv files; .h5 files (hdf5path) need the
-// HDF5 library, which this build does not link, and raise NotImplementedError, as do the CLI strings (cmdstr).
+// HDF5 library, which this build does not link, and raise NotImplementedError.  Command-line strings (epiecmdstr,
+// dmcmdstr, mlscmdstr, epieinit, mlsinit) are parsed by pty_params_from_cmdline over the command line's defaults.
 #define PY_SSIZE_T_CLEAN
 #include <Python.h>
 #define NPY_NO_DEPRECATED_API NPY_1_7_API_VERSION
@@ -315,12 +316,43 @@ PyObject* run_np(PyObject* args, PyObject* kw, const char* algorithm, bool np = 
   return result;
 }
 
-PyObject* not_implemented(const char* what) {
-  PyErr_Format(PyExc_NotImplementedError,
-               "%s: command-line strings are not part of this engine; "
-               "use the keyword entry points (epie, dm, mls, epienp, dmnp, mlsnp, epienpinit)",
-               what);
-  return nullptr;
+// The single keyword `cmdstr` of the command-string entry points, parsed into `out` for `algorithm` (the entry
+// point's own: the reference's epiecmdstr runs ePIE whatever -algorithm says, src/ptychopy.c:578-612).
+bool parse_cmdstr(PyObject* args, PyObject* kw, const char* algorithm, Parsed& out) {
+  const char* cmdstr = "";
+  static const char* kwl[] = {"cmdstr", nullptr};
+  if (!PyArg_ParseTupleAndKeywords(args, kw, "|s", const_cast<char**>(kwl), &cmdstr)) return false;
+  const int rc = pty_params_from_cmdline(cmdstr, &out.p);
+  if (rc != PTY_OK) {
+    raise_status(rc);
+    return false;
+  }
+  copy_str(out.p.algorithm, sizeof(out.p.algorithm), algorithm);
+  if (!out.p.fp[0] && !out.p.simulate) {
+    PyErr_SetString(PyExc_ValueError, "the command string names no data files (-fp=...) and no -simulate=1");
+    return false;
+  }
+  return true;
+}
+
+// epiecmdstr / dmcmdstr / mlscmdstr (src/ptychopy.c:578-689): a whole run from a command string; the results are
+// written to data/ and the object is returned, complex64 (X, Y).
+PyObject* run_cmdstr(PyObject* args, PyObject* kw, const char* algorithm) {
+  Parsed a;
+  if (!parse_cmdstr(args, kw, algorithm, a)) return nullptr;
+  pty_session* s = make_session(a);
+  if (!s) return nullptr;
+  int rc;
+  const int iters = a.p.iter;
+  Py_BEGIN_ALLOW_THREADS rc = pty_run(s, iters, nullptr);
+  Py_END_ALLOW_THREADS if (rc != PTY_OK) {
+    raise_status(rc);
+    pty_session_destroy(s);
+    return nullptr;
+  }
+  PyObject* o = write_results(s, a, 0) ? object_array(s) : nullptr;
+  pty_session_destroy(s);
+  return o;
 }
 
 PyObject* m_helloworld(PyObject*, PyObject* args) {
@@ -335,7 +367,9 @@ PyObject* m_mls(PyObject*, PyObject* args, PyObject* kw) { return run_np(args, k
 PyObject* m_epienp(PyObject*, PyObject* args, PyObject* kw) { return run_np(args, kw, "ePIE"); }
 PyObject* m_dmnp(PyObject*, PyObject* args, PyObject* kw) { return run_np(args, kw, "DM"); }
 PyObject* m_mlsnp(PyObject*, PyObject* args, PyObject* kw) { return run_np(args, kw, "MLs"); }
-PyObject* m_cmdstr(PyObject*, PyObject*, PyObject*) { return not_implemented("cmdstr"); }
+PyObject* m_epiecmdstr(PyObject*, PyObject* args, PyObject* kw) { return run_cmdstr(args, kw, "ePIE"); }
+PyObject* m_dmcmdstr(PyObject*, PyObject* args, PyObject* kw) { return run_cmdstr(args, kw, "DM"); }
+PyObject* m_mlscmdstr(PyObject*, PyObject* args, PyObject* kw) { return run_cmdstr(args, kw, "MLs"); }
 
 void drop_session() {
   if (g_session) pty_session_destroy(g_session);
@@ -354,7 +388,17 @@ PyObject* npinit(PyObject* args, PyObject* kw, const char* algorithm) {
 PyObject* m_epienpinit(PyObject*, PyObject* args, PyObject* kw) { return npinit(args, kw, "ePIE"); }
 PyObject* m_dmnpinit(PyObject*, PyObject* args, PyObject* kw) { return npinit(args, kw, "DM"); }
 PyObject* m_mlsnpinit(PyObject*, PyObject* args, PyObject* kw) { return npinit(args, kw, "MLs"); }
-PyObject* m_cmdinit(PyObject*, PyObject*, PyObject*) { return not_implemented("epieinit/mlsinit"); }
+// epieinit / mlsinit (src/ptychopy.c:902-937,994-1024): step mode from a command string.
+PyObject* cmdinit(PyObject* args, PyObject* kw, const char* algorithm) {
+  Parsed a;
+  if (!parse_cmdstr(args, kw, algorithm, a)) return nullptr;
+  drop_session();
+  g_session = make_session(a);
+  if (!g_session) return nullptr;
+  Py_RETURN_TRUE;
+}
+PyObject* m_epieinit(PyObject*, PyObject* args, PyObject* kw) { return cmdinit(args, kw, "ePIE"); }
+PyObject* m_mlsinit(PyObject*, PyObject* args, PyObject* kw) { return cmdinit(args, kw, "MLs"); }
 
 PyObject* need_session() {
   PyErr_SetString(PyExc_RuntimeError, "no step-mode session: call epienpinit first");
@@ -408,16 +452,16 @@ PyMethodDef methods[] = {
     {"epienp", KW(m_epienp), "ePIE reconstruction from numpy arrays."},
     {"dmnp", KW(m_dmnp), "DM reconstruction from numpy arrays."},
     {"mlsnp", KW(m_mlsnp), "MLs reconstruction from numpy arrays."},
-    {"epiecmdstr", KW(m_cmdstr), "ePIE from a command-line string (not part of this engine)."},
-    {"dmcmdstr", KW(m_cmdstr), "DM from a command-line string (not part of this engine)."},
-    {"mlscmdstr", KW(m_cmdstr), "MLs from a command-line string (not part of this engine)."},
-    {"epieinit", KW(m_cmdinit), "Step-mode init from a command-line string (not part of this engine)."},
+    {"epiecmdstr", KW(m_epiecmdstr), "ePIE from a command-line string; returns the object."},
+    {"dmcmdstr", KW(m_dmcmdstr), "DM from a command-line string; returns the object."},
+    {"mlscmdstr", KW(m_mlscmdstr), "MLs from a command-line string; returns the object."},
+    {"epieinit", KW(m_epieinit), "Step-mode ePIE init from a command-line string."},
     {"epiepost", KW(m_post), "Write results and end the step-mode session."},
     {"epiestep", KW(m_step), "One step-mode iteration; returns the error metric."},
     {"epieresobj", KW(m_resobj), "Current object, complex64 (X, Y)."},
     {"epieresprobe", KW(m_resprobe), "Current probe modes, complex64 (K*N, N)."},
     {"epienpinit", KW(m_epienpinit), "Step-mode ePIE init from numpy arrays."},
-    {"mlsinit", KW(m_cmdinit), "Step-mode MLs init from a command-line string (not part of this engine)."},
+    {"mlsinit", KW(m_mlsinit), "Step-mode MLs init from a command-line string."},
     {"mlspost", KW(m_post), "Write results and end the step-mode session."},
     {"mlsstep", KW(m_step), "One step-mode iteration; returns the error metric."},
     {"mlsresobj", KW(m_resobj), "Current object, complex64 (X, Y)."},

@@ -22,13 +22,13 @@ def test_module_has_reference_methods(ptychopy):
     assert sys.modules["ptychopy"] is ptychopy
 
 
-def test_hdf5_files_and_command_strings_raise_not_implemented(ptychopy):
+def test_hdf5_files_raise_not_implemented(ptychopy):
     # .bin / .csv pattern files are read (tests/test_ingest.py, tests/test_gpu_ingest.py); .h5 needs the HDF5
-    # library, which this build does not link
+    # library, which this build does not link, also when a command string names them
     with pytest.raises(NotImplementedError):
         ptychopy.epie(jobID="x", fp="/data/scan#.h5", size=256)
     with pytest.raises(NotImplementedError):
-        ptychopy.dmcmdstr(cmdstr="-jobID=x")
+        ptychopy.dmcmdstr(cmdstr="./ptycho -jobID=x -fp=/data/scan#.h5")
 
 
 def test_unknown_keyword_is_a_type_error(ptychopy):
