@@ -28,6 +28,7 @@
 namespace {
 
 pty_session* g_session = nullptr;  // step-mode session (the reference's static IPhaser* phaser)
+int g_binary_output = 0;           // its result-file format (binaryOutput), for epiepost / mlspost
 
 PyObject* raise_status(int rc) {
   const char* msg = pty_last_error();
@@ -383,6 +384,7 @@ PyObject* npinit(PyObject* args, PyObject* kw, const char* algorithm) {
   drop_session();
   g_session = make_session(a);
   if (!g_session) return nullptr;
+  g_binary_output = a.p.binaryOutput;
   Py_RETURN_TRUE;
 }
 PyObject* m_epienpinit(PyObject*, PyObject* args, PyObject* kw) { return npinit(args, kw, "ePIE"); }
@@ -395,6 +397,7 @@ PyObject* cmdinit(PyObject* args, PyObject* kw, const char* algorithm) {
   drop_session();
   g_session = make_session(a);
   if (!g_session) return nullptr;
+  g_binary_output = a.p.binaryOutput;
   Py_RETURN_TRUE;
 }
 PyObject* m_epieinit(PyObject*, PyObject* args, PyObject* kw) { return cmdinit(args, kw, "ePIE"); }
@@ -422,7 +425,8 @@ PyObject* m_resprobe(PyObject*, PyObject*, PyObject*) {
   if (!g_session) return need_session();
   return probe_array(g_session);
 }
-// epiepost / mlspost: write results and release the session (src/ptychopy.c:944-953).
+// epiepost / mlspost: write results (in the session's binaryOutput format) and release the session
+// (src/ptychopy.c:944-953, IPhaser::writeResultsToDisk src/IPhaser.cpp:417-428).
 PyObject* m_post(PyObject*, PyObject* args, PyObject* kw) {
   if (!g_session) return need_session();
   int writeResults = 1;
@@ -433,7 +437,7 @@ PyObject* m_post(PyObject*, PyObject* args, PyObject* kw) {
   if (writeResults) {
     struct stat st;
     if (stat(outputDir, &st) != 0) mkdir(outputDir, 0755);
-    int rc = pty_write_results(g_session, outputDir, 0, 0);
+    int rc = pty_write_results(g_session, outputDir, 0, g_binary_output);
     if (rc != PTY_OK) {
       drop_session();
       return raise_status(rc);

@@ -43,7 +43,10 @@ def test_command_string_run_equals_keyword_run(sim_dir, algo):
         assert os.path.getsize(sim_dir / "data" / f"cmd{algo}_{part}_0.csv") > 0
     keyword_run = pt.epie if algo == "ePIE" else pt.dm
     o2, _ = keyword_run(simulate=1, returnResults=1, writeResults=0, **KW)
-    assert np.array_equal(o, o2)
+    if algo == "ePIE":
+        assert np.array_equal(o, o2)
+    else:  # DM sums the object increments of a wave with atomics: two runs agree to rounding
+        assert rel_err(o, o2) < 1e-5
 
 
 def test_step_mode_from_a_command_string(sim_dir):
@@ -51,11 +54,12 @@ def test_step_mode_from_a_command_string(sim_dir):
 
     pt = ptychopy_b200.import_ptychopy()
     whole = pt.epiecmdstr(CMD.format(algo="ePIE"))
-    assert pt.epieinit(CMD.format(algo="Step")) is True
+    assert pt.epieinit(CMD.format(algo="Step") + " -binaryOutput=1") is True
     for _ in range(3):
         pt.epiestep()
     o = pt.epieresobj()
     assert o.shape == whole.shape and rel_err(o, whole) < 1e-6
     assert pt.epieresprobe().shape == (64, 64)
     assert pt.epiepost() is True
-    assert os.path.getsize(sim_dir / "data" / "cmdStep_object_0.csv") > 0
+    # epiepost writes in the session's format: raw complex64 with -binaryOutput=1
+    assert os.path.getsize(sim_dir / "data" / "cmdStep_object_0.bin") == o.nbytes
