@@ -83,6 +83,10 @@ typedef struct pty_params {
                              after every `save`-th iteration; 0 = never.  The reference's command line has this
                              checkpoint (src/IPhaser.cpp:384-385); its Python path leaves it at 999999 */
   char outputDir[256];    /* directory of those checkpoint files ("" = "data", the reference's) */
+  double driftx, drifty;  /* linear drift of the generated scan positions, in m per row (x) and per column (y) of
+                             the mesh array (Cartesian: raster row i and column j; list and spiral: index / 1024
+                             and index % 1024), added before the pixel conversion like the reference's
+                             command-line option `drift` (d_generateMesh, src/ScanMeshKernels.cu:86-87); 0 = none */
 } pty_params;
 
 typedef struct pty_session pty_session;
@@ -96,8 +100,8 @@ int pty_params_init(pty_params* p);
  * -simulate=1": white-space separated "-name=value" options after the program name, over the command line's own
  * defaults (beamSize 1e-7, lambda 2.48e-10, z 1, scanDims 12 x 12, size 256, PPS 5; the rest as pty_params_init),
  * each option with the reference's range check.  Names match exactly, ignoring case; the last occurrence wins.
- * PTY_ERR_UNSUPPORTED for a non-zero `drift` or a `bitDepth` other than 32, PTY_ERR_INVALID for a text value longer
- * than its field; `p` is left unchanged on an error.  Replaces the tokeniser of the command-string entry points
+ * `-drift=dx,dy` sets driftx / drifty.  PTY_ERR_UNSUPPORTED for a `bitDepth` other than 32, PTY_ERR_INVALID for a
+ * text value longer than its field; `p` is left unchanged on an error.  Replaces the tokeniser of the command-string entry points
  * (src/ptychopy.c:543-576) and Parameters::parseFromCommandLine (src/Parameters.cpp:66-375) with the defaults of
  * src/Parameters.h:67-170. */
 int pty_params_from_cmdline(const char* cmdstr, pty_params* p);

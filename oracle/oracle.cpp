@@ -1220,23 +1220,64 @@ void mesh_jitter(uint64_t seed, size_t n, unsigned radius, std::vector<float>& o
 // ============================================================================================================
 // C ABI of the oracle (ctypes from tests/ and bench.py).  Complex arrays are interleaved (re, im) doubles.
 // ============================================================================================================
+// The scan drift of d_generateMesh (src/ScanMeshKernels.cu:86-87): `initialValues += index * driftCoeff` in float,
+// metres per row (x) or column (y) of the mesh array.  The reference's compiled kernel fuses the add with the
+// product that formed the value where there is one, fma(a, step, index * drift) for the Cartesian and spiral
+// meshes (checked against it on the GPU), and with index * drift for a loaded value, fma(index, drift, v) (list).
+static float drift_add(float v, int index, float drift) {
+  return drift != 0.f ? std::fma(float(index), drift, v) : v;
+}
+static float drift_mul_add(float a, float step, int index, float drift) {
+  if (drift == 0.f) return a * step;
+  volatile float d = float(index) * drift;
+  return std::fma(a, step, float(d));
+}
+
 // Raw pixel positions of an nx x ny raster before the -min shift (d_generateMesh<1>, src/ScanMeshKernels.cu:46-93,
-// launched at :153-160 with one_over_dxs = (float)(1.0/dx_s)): ((i - (nx-1)/2) * stepx) * one_over_dxs in float,
-// index i*ny + j.
-static void cartesian_raw(int nx, int ny, double stepx, double stepy, double dx_s, int mirrorX, int mirrorY, float* raw) {
+// launched at :153-160 with one_over_dxs = (float)(1.0/dx_s)): ((i - (nx-1)/2) * stepx + i * driftx) *
+// one_over_dxs in float, index i*ny + j.
+static void cartesian_raw(int nx, int ny, double stepx, double stepy, double dx_s, int mirrorX, int mirrorY,
+                          float dfx, float dfy, float* raw) {
   const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
   for (int i = 0; i < nx; ++i)
     for (int j = 0; j < ny; ++j) {
       volatile float mi = float(i), md = float(nx - 1) * 0.5f;
       volatile float dxv = mirrorX ? (md - mi) : (mi - md);
-      volatile float vx = dxv * sx;
+      volatile float vx = drift_mul_add(dxv, sx, i, dfx);
       volatile float mj = float(j), mdy = float(ny - 1) * 0.5f;
       volatile float dyv = mirrorY ? (mdy - mj) : (mj - mdy);
-      volatile float vy = dyv * sy;
+      volatile float vy = drift_mul_add(dyv, sy, j, dfy);
       volatile float px = vx * inv, py = vy * inv;
       raw[2 * (size_t(i) * ny + j)] = px;
       raw[2 * (size_t(i) * ny + j) + 1] = py;
     }
+}
+
+// The list mesh array (d_generateMesh<2>): M = ceil(P/1024)*1024 entries of 1024-wide rows, the positions in metres
+// (zero past P) plus the drift of their row index / 1024 and column index % 1024, times one_over_dxs.
+static void list_raw(const double* xy_m, int P, double dx_s, float dfx, float dfy, size_t M, float* raw) {
+  const float inv = float(1.0 / dx_s);
+  for (size_t i = 0; i < M; ++i) {
+    volatile float x = i < size_t(P) ? float(xy_m[2 * i]) : 0.f, y = i < size_t(P) ? float(xy_m[2 * i + 1]) : 0.f;
+    volatile float xd = drift_add(x, int(i / 1024), dfx), yd = drift_add(y, int(i % 1024), dfy);
+    volatile float px = xd * inv, py = yd * inv;
+    raw[2 * i] = px; raw[2 * i + 1] = py;
+  }
+}
+
+// The spiral mesh array (d_generateMesh<3>): every one of the M entries is a spiral point; drift as the list's.
+static void spiral_raw(double stepx, double stepy, double dx_s, float dfx, float dfy, size_t M, float* raw) {
+  const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
+  for (size_t i = 0; i < M; ++i) {
+    const float s = std::sqrt(float(i));
+    const float a = 4.0f * s;
+    const float c = float(std::cos(double(a))), sn = float(std::sin(double(a)));
+    volatile float vx = s * c;
+    volatile float vy = s * sn;
+    volatile float wx = drift_mul_add(vx, sx, int(i / 1024), dfx), wy = drift_mul_add(vy, sy, int(i % 1024), dfy);
+    volatile float px = wx * inv, py = wy * inv;
+    raw[2 * i] = px; raw[2 * i + 1] = py;
+  }
 }
 
 extern "C" {
@@ -1268,12 +1309,25 @@ int orc_cartesian_mesh(int nx, int ny, double stepx, double stepy, double lambda
   return orc_cartesian_mesh_j(nx, ny, stepx, stepy, lambda, z, dx_d, N, mirrorX, mirrorY, flip, 0, 0, pos, objXY);
 }
 
+int orc_cartesian_mesh_jd(int nx, int ny, double stepx, double stepy, double lambda, double z, double dx_d, int N,
+                          int mirrorX, int mirrorY, int flip, unsigned jitter, uint64_t seed, double driftx,
+                          double drifty, float* pos, int* objXY);
+
 int orc_cartesian_mesh_j(int nx, int ny, double stepx, double stepy, double lambda, double z, double dx_d, int N,
                          int mirrorX, int mirrorY, int flip, unsigned jitter, uint64_t seed, float* pos,
                          int* objXY) {
+  return orc_cartesian_mesh_jd(nx, ny, stepx, stepy, lambda, z, dx_d, N, mirrorX, mirrorY, flip, jitter, seed, 0.0,
+                               0.0, pos, objXY);
+}
+
+// ... with the scan drift (metres per raster row / column).
+int orc_cartesian_mesh_jd(int nx, int ny, double stepx, double stepy, double lambda, double z, double dx_d, int N,
+                          int mirrorX, int mirrorY, int flip, unsigned jitter, uint64_t seed, double driftx,
+                          double drifty, float* pos, int* objXY) {
   if (nx < 1 || ny < 1 || N < 1) return -1;
   std::vector<float> raw(2 * size_t(nx) * ny);
-  cartesian_raw(nx, ny, stepx, stepy, sample_pixel(lambda, z, dx_d, N), mirrorX, mirrorY, raw.data());
+  cartesian_raw(nx, ny, stepx, stepy, sample_pixel(lambda, z, dx_d, N), mirrorX, mirrorY, float(driftx),
+                float(drifty), raw.data());
   std::vector<float> jit;
   mesh_jitter(seed, size_t(nx) * ny, jitter, jit);
   for (size_t k = 0; k < raw.size(); ++k) {
@@ -1291,7 +1345,29 @@ int orc_cartesian_mesh_j(int nx, int ny, double stepx, double stepy, double lamb
 int orc_cartesian_mesh_raw(int nx, int ny, double stepx, double stepy, double lambda, double z, double dx_d, int N,
                            int mirrorX, int mirrorY, float* raw) {
   if (nx < 1 || ny < 1 || N < 1) return -1;
-  cartesian_raw(nx, ny, stepx, stepy, sample_pixel(lambda, z, dx_d, N), mirrorX, mirrorY, raw);
+  cartesian_raw(nx, ny, stepx, stepy, sample_pixel(lambda, z, dx_d, N), mirrorX, mirrorY, 0.f, 0.f, raw);
+  return 0;
+}
+
+// Raw mesh arrays with the scan drift, before jitter and the -min shift: type 1 Cartesian (2*nx*ny floats,
+// nx = a, ny = b), 2 list (xy_m in metres, P = a; 2*ceil(P/1024)*1024 floats), 3 spiral (P = a; same size).
+int orc_mesh_raw_drift(int type, int a, int b, const double* xy_m, double stepx, double stepy, double lambda,
+                       double z, double dx_d, int N, int mirrorX, int mirrorY, double driftx, double drifty,
+                       float* raw) {
+  if (a < 1 || N < 1) return -1;
+  const double dx_s = sample_pixel(lambda, z, dx_d, N);
+  const size_t M = (size_t(a) + 1023) / 1024 * 1024;
+  if (type == 1) {
+    if (b < 1) return -1;
+    cartesian_raw(a, b, stepx, stepy, dx_s, mirrorX, mirrorY, float(driftx), float(drifty), raw);
+  } else if (type == 2) {
+    if (!xy_m) return -1;
+    list_raw(xy_m, a, dx_s, float(driftx), float(drifty), M, raw);
+  } else if (type == 3) {
+    spiral_raw(stepx, stepy, dx_s, float(driftx), float(drifty), M, raw);
+  } else {
+    return -1;
+  }
   return 0;
 }
 
@@ -1303,18 +1379,22 @@ int orc_list_mesh(const double* xy_m, int P, double lambda, double z, double dx_
 
 // The mesh array holds whole 1024-wide rows: entries past P are (0, 0) plus their jitter and take part in the
 // min/max (calculateMeshDimensions reduces over the whole array).
+int orc_list_mesh_jd(const double* xy_m, int P, double lambda, double z, double dx_d, int N, int flip,
+                     unsigned jitter, uint64_t seed, double driftx, double drifty, float* pos, int* objXY);
+
 int orc_list_mesh_j(const double* xy_m, int P, double lambda, double z, double dx_d, int N, int flip, unsigned jitter,
                     uint64_t seed, float* pos, int* objXY) {
+  return orc_list_mesh_jd(xy_m, P, lambda, z, dx_d, N, flip, jitter, seed, 0.0, 0.0, pos, objXY);
+}
+
+// ... with the scan drift (metres per mesh-array row / column).
+int orc_list_mesh_jd(const double* xy_m, int P, double lambda, double z, double dx_d, int N, int flip,
+                     unsigned jitter, uint64_t seed, double driftx, double drifty, float* pos, int* objXY) {
   if (P < 1) return -1;
   const double dx_s = sample_pixel(lambda, z, dx_d, N);
-  const float inv = float(1.0 / dx_s);
   const size_t M = (size_t(P) + 1023) / 1024 * 1024;
   std::vector<float> raw(2 * M, 0.f), jit;
-  for (int i = 0; i < P; ++i) {
-    volatile float x = float(xy_m[2 * i]), y = float(xy_m[2 * i + 1]);
-    volatile float px = x * inv, py = y * inv;
-    raw[2 * i] = px; raw[2 * i + 1] = py;
-  }
+  list_raw(xy_m, P, dx_s, float(driftx), float(drifty), M, raw.data());
   mesh_jitter(seed, M, jitter, jit);
   for (size_t k = 0; k < raw.size(); ++k) {
     volatile float v = raw[k] + jit[k];
@@ -1333,25 +1413,26 @@ int orc_list_mesh_j(const double* xy_m, int P, double lambda, double z, double d
 // whole 1024-wide rows and every entry is a spiral point, so the min/max (object size, shift) cover
 // ceil(P/1024)*1024 points while only the first P are scan positions.  cos/sin of the float argument in double,
 // rounded to float.
+int orc_spiral_mesh_d(int P, double stepx, double stepy, double lambda, double z, double dx_d, int N, int flip,
+                      unsigned jitter, uint64_t seed, double driftx, double drifty, float* pos, int* objXY);
+
 int orc_spiral_mesh(int P, double stepx, double stepy, double lambda, double z, double dx_d, int N, int flip,
                     unsigned jitter, uint64_t seed, float* pos, int* objXY) {
+  return orc_spiral_mesh_d(P, stepx, stepy, lambda, z, dx_d, N, flip, jitter, seed, 0.0, 0.0, pos, objXY);
+}
+
+// ... with the scan drift (metres per mesh-array row / column).
+int orc_spiral_mesh_d(int P, double stepx, double stepy, double lambda, double z, double dx_d, int N, int flip,
+                      unsigned jitter, uint64_t seed, double driftx, double drifty, float* pos, int* objXY) {
   if (P < 1 || N < 1) return -1;
   const double dx_s = sample_pixel(lambda, z, dx_d, N);
-  const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
   const size_t M = (size_t(P) + 1023) / 1024 * 1024;
   std::vector<float> raw(2 * M), jit;
   mesh_jitter(seed, M, jitter, jit);
-  for (size_t i = 0; i < M; ++i) {
-    const float s = std::sqrt(float(i));
-    const float a = 4.0f * s;
-    const float c = float(std::cos(double(a))), sn = float(std::sin(double(a)));
-    volatile float vx = s * c;
-    volatile float vy = s * sn;
-    volatile float wx = vx * sx, wy = vy * sy;
-    volatile float px = wx * inv, py = wy * inv;
-    volatile float jx = px + jit[2 * i], jy = py + jit[2 * i + 1];
-    raw[2 * i] = jx;
-    raw[2 * i + 1] = jy;
+  spiral_raw(stepx, stepy, dx_s, float(driftx), float(drifty), M, raw.data());
+  for (size_t k = 0; k < raw.size(); ++k) {
+    volatile float v = raw[k] + jit[k];
+    raw[k] = v;
   }
   Mesh m;
   finish_mesh(raw, int(M), false, N, flip != 0, m);

@@ -44,6 +44,10 @@ def lib():
             "orc_cartesian_mesh_j": ([i, i, d, d, d, d, d, i, i, i, i, ctypes.c_uint, u64, vp, vp], i),
             "orc_list_mesh_j": ([vp, i, d, d, d, i, i, ctypes.c_uint, u64, vp, vp], i),
             "orc_spiral_mesh": ([i, d, d, d, d, d, i, i, ctypes.c_uint, u64, vp, vp], i),
+            "orc_cartesian_mesh_jd": ([i, i, d, d, d, d, d, i, i, i, i, ctypes.c_uint, u64, d, d, vp, vp], i),
+            "orc_list_mesh_jd": ([vp, i, d, d, d, i, i, ctypes.c_uint, u64, d, d, vp, vp], i),
+            "orc_spiral_mesh_d": ([i, d, d, d, d, d, i, i, ctypes.c_uint, u64, d, d, vp, vp], i),
+            "orc_mesh_raw_drift": ([i, i, i, vp, d, d, d, d, d, i, i, i, d, d, vp], i),
             "orc_mesh_jitter": ([u64, i, ctypes.c_uint, vp], i),
             "orc_set_dm_reduce": ([vp, vp, vp], i),
             "orc_probe_guess": ([vp, i, i, d, d, i, vp], i),
@@ -88,12 +92,35 @@ def sample_pixel(lambd, z, dx_d, N):
     return lib().orc_sample_pixel(lambd, z, dx_d, N)
 
 
-def cartesian_mesh(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX=0, mirrorY=0, flip=0, jitter=0, seed=0):
+def cartesian_mesh(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX=0, mirrorY=0, flip=0, jitter=0, seed=0,
+                   drift=(0.0, 0.0)):
+    """Raster positions (nx*ny, 2) in pixels after the -min shift, and the object size; drift in metres per raster
+    row / column."""
     pos = np.zeros((nx * ny, 2), np.float32)
     xy = np.zeros(2, np.int32)
-    assert lib().orc_cartesian_mesh_j(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX, mirrorY, flip, jitter, seed,
-                                      _p(pos), _p(xy)) == 0
+    assert lib().orc_cartesian_mesh_jd(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX, mirrorY, flip, jitter, seed,
+                                       drift[0], drift[1], _p(pos), _p(xy)) == 0
     return pos, int(xy[0]), int(xy[1])
+
+
+def mesh_raw_drift(kind, lambd, z, dx_d, N, drift, nx=0, ny=0, xy_m=None, P=0, stepx=0.0, stepy=0.0, mirrorX=0,
+                   mirrorY=0):
+    """The mesh array before jitter and the -min shift, in pixels, with the scan drift: kind "cartesian" (nx*ny, 2),
+    "list" (xy_m in metres) or "spiral" (P points), the last two (ceil(P/1024)*1024, 2) in 1024-wide rows."""
+    if kind == "cartesian":
+        t, a, b, n, xp = 1, nx, ny, nx * ny, None
+    else:
+        t = 2 if kind == "list" else 3
+        if t == 2:
+            xp = np.ascontiguousarray(xy_m, np.float64)
+            P = xp.shape[0]
+        else:
+            xp = None
+        a, b, n = P, 0, (P + 1023) // 1024 * 1024
+    raw = np.zeros((n, 2), np.float32)
+    assert lib().orc_mesh_raw_drift(t, a, b, None if xp is None else _p(xp), stepx, stepy, lambd, z, dx_d, N, mirrorX,
+                                    mirrorY, drift[0], drift[1], _p(raw)) == 0
+    return raw
 
 
 def cartesian_mesh_raw(nx, ny, stepx, stepy, lambd, z, dx_d, N, mirrorX=0, mirrorY=0):
@@ -122,20 +149,21 @@ def mls_lsq_terms(chi, oup, dPO, probe, lam):
     return a1, a2, a4, b1, b2
 
 
-def list_mesh(xy_m, lambd, z, dx_d, N, flip=0, jitter=0, seed=0):
+def list_mesh(xy_m, lambd, z, dx_d, N, flip=0, jitter=0, seed=0, drift=(0.0, 0.0)):
     xy_m = np.ascontiguousarray(xy_m, np.float64)
     pos = np.zeros((xy_m.shape[0], 2), np.float32)
     xy = np.zeros(2, np.int32)
-    assert lib().orc_list_mesh_j(_p(xy_m), xy_m.shape[0], lambd, z, dx_d, N, flip, jitter, seed, _p(pos),
-                                 _p(xy)) == 0
+    assert lib().orc_list_mesh_jd(_p(xy_m), xy_m.shape[0], lambd, z, dx_d, N, flip, jitter, seed, drift[0], drift[1],
+                                  _p(pos), _p(xy)) == 0
     return pos, int(xy[0]), int(xy[1])
 
 
-def spiral_mesh(P, stepx, stepy, lambd, z, dx_d, N, flip=0, jitter=0, seed=0):
+def spiral_mesh(P, stepx, stepy, lambd, z, dx_d, N, flip=0, jitter=0, seed=0, drift=(0.0, 0.0)):
     """Spiral scan positions (P, 2) in pixels after the -min shift, and the object size."""
     pos = np.zeros((P, 2), np.float32)
     xy = np.zeros(2, np.int32)
-    assert lib().orc_spiral_mesh(P, stepx, stepy, lambd, z, dx_d, N, flip, jitter, seed, _p(pos), _p(xy)) == 0
+    assert lib().orc_spiral_mesh_d(P, stepx, stepy, lambd, z, dx_d, N, flip, jitter, seed, drift[0], drift[1],
+                                   _p(pos), _p(xy)) == 0
     return pos, int(xy[0]), int(xy[1])
 
 

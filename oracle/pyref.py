@@ -40,6 +40,7 @@ def lib():
             "ref_lsq_terms": [vp, vp, vp, vp, f, i, vp, vp, vp, vp, vp],
             "ref_modulus_amplitude": [vp, vp, vp, f, i],
             "ref_cartesian_mesh": [vp, i, i, f, f, f, i, i],
+            "ref_mesh": [i, vp, i, i, f, f, f, i, i, f, f],
             "ref_symmetrize": [vp, vp, i, i, i, i, i, i, i, i],
             "ref_rotate90": [vp, vp, i, i],
             "ref_shift_fft": [vp, vp, i],

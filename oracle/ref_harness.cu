@@ -259,6 +259,26 @@ int ref_cartesian_mesh(float2* pos, int nx, int ny, float stepx, float stepy, fl
   return finish();
 }
 
+// d_generateMesh<type> (src/ScanMeshKernels.cu:46-93) with a scan drift, launched the way h_generateCartesianMesh,
+// h_generateListMesh and h_generateSpiralMesh launch it (:153-180): one block of alignedY threads per mesh-array
+// row, no jitter.  type 1 (Cartesian): rows = nx, meshY = ny, alignedY = alignUp(ny, 32); type 2 (list, the
+// positions in metres in pos on entry, stepSizeY 0) and type 3 (spiral): rows = ceil(P / 1024), meshY = alignedY =
+// 1024, no mirroring.  pos holds rows * alignedY float2.
+int ref_mesh(int type, float2* pos, int rows, int meshY, float stepx, float stepy, float one_over_dxs, int mirrorX,
+             int mirrorY, float driftx, float drifty) {
+  if (rows < 1 || meshY < 1 || meshY > 1024 || type < 1 || type > 3 || (type != 1 && meshY != 1024))
+    return int(cudaErrorInvalidValue);
+  const float2 drift = make_float2(driftx, drifty);
+  if (type == 1)
+    d_generateMesh<1><<<rows, align32(meshY)>>>(pos, meshY, stepx, stepy, one_over_dxs, 0, mirrorX != 0,
+                                                mirrorY != 0, nullptr, drift);
+  else if (type == 2)
+    d_generateMesh<2><<<rows, 1024>>>(pos, meshY, stepx, 0.f, one_over_dxs, 0, false, false, nullptr, drift);
+  else
+    d_generateMesh<3><<<rows, 1024>>>(pos, meshY, stepx, stepy, one_over_dxs, 0, false, false, nullptr, drift);
+  return finish();
+}
+
 // h_symmetrizeDiffraction (src/DiffractionsKernels.cu:171-178): copy of a numX x numY block between pitched arrays.
 int ref_symmetrize(const float* in, float* out, int dataOffX, int dataOffY, int dataAlignedY, int outOffX,
                    int outOffY, int outAlignedY, int numX, int numY) {

@@ -14,8 +14,8 @@
 //     after "-T=60" would reset T;
 //   * "-step=v" with one value reads it as a real number (the reference truncates it with atoi);
 //   * each call starts from the defaults (the reference's parameter singleton keeps what earlier calls set);
-//   * options this engine cannot honour are refused instead of ignored: a non-zero `drift` and a `bitDepth` other
-//     than 32.  Options with no effect on a reconstruction here are accepted and ignored, as the reference ignores
+//   * an option this engine cannot honour is refused instead of ignored: a `bitDepth` other than 32 (a lower
+//     saturation level).  Options with no effect on a reconstruction here are accepted and ignored, as the reference ignores
 //     names it does not know: blind (unused there), threads (file-reading threads), angles, overlap,
 //     shareFrequency (multi-GPU stitching), updateVis, wsServerUrl (rendering).
 #include <cctype>
@@ -180,9 +180,7 @@ void apply(const Options& opt, pty_params* p) {
   auto to_int = [](const char* s) { return std::atoi(s); };
   auto to_real = [](const char* s) { return std::atof(s); };
   opt.pair("scanDims", &p->scanDimsx, &p->scanDimsy, false, 1, to_int);
-  double dx = 0, dy = 0;
-  if (opt.pair("drift", &dx, &dy, false, 0.0, to_real) && (dx != 0 || dy != 0))
-    throw Refusal{PTY_ERR_UNSUPPORTED, "drift (a linear drift added to the scan positions) is not part of this engine"};
+  opt.pair("drift", &p->driftx, &p->drifty, false, 0.0, to_real);
   opt.pair("qxy", &p->qx, &p->qy, false, 0, to_int);
   opt.pair("nxy", &p->nx, &p->ny, false, 0, to_int);
   opt.pair("step", &p->stepx, &p->stepy, true, 0.0, to_real);

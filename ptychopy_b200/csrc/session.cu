@@ -208,19 +208,32 @@ static void add_jitter(std::vector<float>& raw, unsigned radius, uint64_t seed) 
   }
 }
 
+// The reference's scan drift (d_generateMesh, src/ScanMeshKernels.cu:86-87): `v += index * drift` in metres and in
+// float, index = the mesh array's row (x) or column (y).  Its compiler fuses the add with the multiply that formed
+// v where there is one (Cartesian, spiral: fma(a, step, index * drift), measured against the reference's compiled
+// kernel) and with index * drift where v is a loaded value (list: fma(index, drift, v)).
+static inline float add_drift(float v, int index, float drift) {
+  return drift != 0.f ? std::fma(float(index), drift, v) : v;
+}
+static inline float mul_add_drift(float a, float step, int index, float drift) {
+  if (drift == 0.f) return a * step;
+  volatile float d = float(index) * drift;
+  return std::fma(a, step, float(d));
+}
+
 // Cartesian raster (d_generateMesh<1>, src/ScanMeshKernels.cu:46-93): index i*ny+j,
-// ((i - (nx-1)/2) * stepx) / dx_s in float.
+// ((i - (nx-1)/2) * stepx + i * driftx) * (1 / dx_s) in float.
 Geometry cartesian_geometry(int nx, int ny, double stepx, double stepy, double dx_s, int N, bool mirrorX,
-                            bool mirrorY, bool flip, unsigned jitter, uint64_t seed) {
+                            bool mirrorY, bool flip, unsigned jitter, uint64_t seed, float dfx, float dfy) {
   const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
   std::vector<float> raw(2 * size_t(nx) * ny);
   const float mdx = float(nx - 1) * 0.5f, mdy = float(ny - 1) * 0.5f;
   for (int i = 0; i < nx; ++i)
     for (int j = 0; j < ny; ++j) {
       volatile float dx = mirrorX ? (mdx - float(i)) : (float(i) - mdx);
-      volatile float vx = float(dx) * sx;
+      volatile float vx = mul_add_drift(float(dx), sx, i, dfx);
       volatile float dy = mirrorY ? (mdy - float(j)) : (float(j) - mdy);
-      volatile float vy = float(dy) * sy;
+      volatile float vy = mul_add_drift(float(dy), sy, j, dfy);
       volatile float px = float(vx) * inv, py = float(vy) * inv;
       raw[2 * (size_t(i) * ny + j)] = px;
       raw[2 * (size_t(i) * ny + j) + 1] = py;
@@ -232,15 +245,16 @@ Geometry cartesian_geometry(int nx, int ny, double stepx, double stepy, double d
 }
 
 // Position list in metres (ListScanMesh::loadarr + d_generateMesh<2>, src/ListScanMesh.cpp:91-129).  The mesh
-// array holds whole 1024-wide rows; entries past P stay (0, 0) (plus jitter) and join the min/max.
+// array holds whole 1024-wide rows; entries past P stay (0, 0) (plus drift and jitter) and join the min/max.
 Geometry list_geometry(const std::vector<double>& xy_m, double dx_s, int N, bool flip, unsigned jitter,
-                       uint64_t seed) {
+                       uint64_t seed, float dfx, float dfy) {
   const int P = int(xy_m.size() / 2);
   const int M = (P + 1023) / 1024 * 1024;
   const float inv = float(1.0 / dx_s);
   std::vector<float> raw(2 * size_t(M), 0.f);
-  for (int i = 0; i < P; ++i) {
-    volatile float x = float(xy_m[2 * i]), y = float(xy_m[2 * i + 1]);
+  for (int i = 0; i < M; ++i) {
+    const float x0 = i < P ? float(xy_m[2 * i]) : 0.f, y0 = i < P ? float(xy_m[2 * i + 1]) : 0.f;
+    volatile float x = add_drift(x0, i / 1024, dfx), y = add_drift(y0, i % 1024, dfy);
     volatile float px = float(x) * inv, py = float(y) * inv;
     raw[2 * i] = px;
     raw[2 * i + 1] = py;
@@ -256,7 +270,7 @@ Geometry list_geometry(const std::vector<double>& xy_m, double dx_s, int N, bool
 // 1024-wide mesh array is a spiral point, so the min/max cover ceil(P/1024)*1024 points.  cos/sin of the float
 // argument are evaluated in double and rounded to float.
 Geometry spiral_geometry(int P, double stepx, double stepy, double dx_s, int N, bool flip, unsigned jitter,
-                         uint64_t seed) {
+                         uint64_t seed, float dfx, float dfy) {
   const int M = (P + 1023) / 1024 * 1024;
   const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
   std::vector<float> raw(2 * size_t(M));
@@ -265,7 +279,7 @@ Geometry spiral_geometry(int P, double stepx, double stepy, double dx_s, int N, 
     const float a = 4.0f * r;
     const float c = float(std::cos(double(a))), sn = float(std::sin(double(a)));
     volatile float vx = r * c, vy = r * sn;
-    volatile float wx = vx * sx, wy = vy * sy;
+    volatile float wx = mul_add_drift(vx, sx, i / 1024, dfx), wy = mul_add_drift(vy, sy, i % 1024, dfy);
     volatile float px = wx * inv, py = wy * inv;
     raw[2 * i] = px;
     raw[2 * i + 1] = py;
@@ -292,16 +306,16 @@ std::vector<double> read_position_file(const std::string& path, int P) {
 
 // Raw (centred, not shifted) Cartesian positions of the ML mesh: the same FP32 formula as cartesian_geometry.
 std::vector<float> raw_cartesian_positions(int nx, int ny, double stepx, double stepy, double dx_s, bool mirrorX,
-                                           bool mirrorY) {
+                                           bool mirrorY, float dfx, float dfy) {
   const float inv = float(1.0 / dx_s), sx = float(stepx), sy = float(stepy);
   std::vector<float> raw(2 * size_t(nx) * ny);
   const float mdx = float(nx - 1) * 0.5f, mdy = float(ny - 1) * 0.5f;
   for (int i = 0; i < nx; ++i)
     for (int j = 0; j < ny; ++j) {
       volatile float dx = mirrorX ? (mdx - float(i)) : (float(i) - mdx);
-      volatile float vx = float(dx) * sx;
+      volatile float vx = mul_add_drift(float(dx), sx, i, dfx);
       volatile float dy = mirrorY ? (mdy - float(j)) : (float(j) - mdy);
-      volatile float vy = float(dy) * sy;
+      volatile float vy = mul_add_drift(float(dy), sy, j, dfy);
       volatile float px = float(vx) * inv, py = float(vy) * inv;
       raw[2 * (size_t(i) * ny + j)] = px;
       raw[2 * (size_t(i) * ny + j) + 1] = py;
@@ -695,16 +709,17 @@ void init_geometry(pty_session* s) {
   // else the Cartesian raster
   need(p.jitterRadius >= 0, "jitterRadius must be >= 0");
   const unsigned jit = unsigned(p.jitterRadius);
+  const float dfx = float(p.driftx), dfy = float(p.drifty);  // the reference's float2 drift
   const int Ptot = s->shard_total > 0 ? s->shard_total : s->P;  // the whole scan's positions
   if (!s->pos_m.empty()) {
-    s->geo = list_geometry(s->pos_m, dx_s, s->N, p.flipScanAxis != 0, jit, p.seed);
+    s->geo = list_geometry(s->pos_m, dx_s, s->N, p.flipScanAxis != 0, jit, p.seed, dfx, dfy);
   } else if (p.lf[0]) {
-    s->geo = list_geometry(read_position_file(p.lf, Ptot), dx_s, s->N, p.flipScanAxis != 0, jit, p.seed);
+    s->geo = list_geometry(read_position_file(p.lf, Ptot), dx_s, s->N, p.flipScanAxis != 0, jit, p.seed, dfx, dfy);
   } else if (p.spiralScan) {
-    s->geo = spiral_geometry(Ptot, p.stepx, p.stepy, dx_s, s->N, p.flipScanAxis != 0, jit, p.seed);
+    s->geo = spiral_geometry(Ptot, p.stepx, p.stepy, dx_s, s->N, p.flipScanAxis != 0, jit, p.seed, dfx, dfy);
   } else {
     s->geo = cartesian_geometry(p.scanDimsx, p.scanDimsy, p.stepx, p.stepy, dx_s, s->N, p.mirror1stScanAxis != 0,
-                                p.mirror2ndScanAxis != 0, p.flipScanAxis != 0, jit, p.seed);
+                                p.mirror2ndScanAxis != 0, p.flipScanAxis != 0, jit, p.seed, dfx, dfy);
   }
   if (s->shard_total > 0)  // keep this shard's positions; the object size stays the whole scan's
     s->geo.pos = std::vector<float>(s->geo.pos.begin() + 2 * size_t(s->shard_first),
@@ -926,16 +941,19 @@ void init_mls(pty_session* s) {
   std::vector<float> raw;
   if (!s->pos_m.empty() || p.lf[0]) {
     const std::vector<double> xy = s->pos_m.empty() ? read_position_file(p.lf, P) : s->pos_m;
-    const float inv = float(1.0 / dx_s);
+    const float inv = float(1.0 / dx_s), dfx = float(p.driftx), dfy = float(p.drifty);
     raw.resize(2 * size_t(P));
-    for (int i = 0; i < 2 * P; ++i) raw[i] = float(xy[i]) * inv;
+    for (int i = 0; i < P; ++i) {
+      raw[2 * i] = add_drift(float(xy[2 * i]), i / 1024, dfx) * inv;
+      raw[2 * i + 1] = add_drift(float(xy[2 * i + 1]), i % 1024, dfy) * inv;
+    }
   } else {
     // the reference's spiral mesh has no ML variant (SpiralScanMesh::generateMeshML is empty); jitter is not part
     // of this engine's ML mesh
     need(p.spiralScan == 0 && p.jitterRadius == 0, "MLs supports Cartesian or listed positions without jitter",
          PTY_ERR_UNSUPPORTED);
     raw = raw_cartesian_positions(p.scanDimsx, p.scanDimsy, p.stepx, p.stepy, dx_s, p.mirror1stScanAxis != 0,
-                                  p.mirror2ndScanAxis != 0);
+                                  p.mirror2ndScanAxis != 0, float(p.driftx), float(p.drifty));
   }
   ml->geo = mls_geometry(raw, N);
   const int gX = s->X, gY = s->Y;

@@ -28,12 +28,13 @@ struct Geometry {
   int X = 0, Y = 0;
 };
 double sample_pixel_size(double lambda, double z, double dx_d, int N);
+// dfx, dfy: the scan drift in metres per mesh-array row / column (0 = none).
 Geometry cartesian_geometry(int nx, int ny, double stepx, double stepy, double dx_s, int N, bool mirrorX,
-                            bool mirrorY, bool flip, unsigned jitter, uint64_t seed);
+                            bool mirrorY, bool flip, unsigned jitter, uint64_t seed, float dfx, float dfy);
 Geometry list_geometry(const std::vector<double>& xy_m, double dx_s, int N, bool flip, unsigned jitter,
-                       uint64_t seed);
+                       uint64_t seed, float dfx, float dfy);
 Geometry spiral_geometry(int P, double stepx, double stepy, double dx_s, int N, bool flip, unsigned jitter,
-                         uint64_t seed);
+                         uint64_t seed, float dfx, float dfy);
 std::vector<double> read_position_file(const std::string& path, int P);
 
 // SplitMix64 stream and the ePIE visiting order (pick `next % remaining`, erase; src/ePIE.cpp:93-97).
@@ -78,7 +79,7 @@ std::vector<float> sim_object_from_files(int N, int X, int Y);
 std::vector<float> sim_probe(int N, double beamSize, double dx_s, uint64_t seed);
 
 std::vector<float> raw_cartesian_positions(int nx, int ny, double stepx, double stepy, double dx_s, bool mirrorX,
-                                           bool mirrorY);
+                                           bool mirrorY, float dfx, float dfy);
 
 }  // namespace pty
 

@@ -77,6 +77,12 @@ def test_flags_and_integer_options():
     assert ok("x -simulate").simulate == 0
 
 
+def test_drift():
+    p = ok("x -drift=3e-9,-1.5e-9")
+    assert (p.driftx, p.drifty) == (3e-9, -1.5e-9)
+    assert (ok("x").driftx, ok("x").drifty) == (0.0, 0.0)
+
+
 def test_range_checks_keep_the_default():
     p = ok("x -size=16 -i=-1 -dpf=0 -probeModes=0 -PPS=0 -save=0 -fs=-2")
     assert (p.size, p.iter, p.dpf, p.probeModes, p.PPS, p.save, p.fs) == (256, 100, 1, 1, 5, 0, 0)
@@ -101,12 +107,12 @@ def test_refusals_leave_the_parameters_unchanged():
     p = abi.PtyParams()
     L.pty_params_init(ctypes.byref(p))
     p.size = 77
-    for cmd, code in [("x -drift=1e-9,0", abi.PTY_ERR_UNSUPPORTED), ("x -bitDepth=16", abi.PTY_ERR_UNSUPPORTED),
-                      ("x -fp=" + "a" * 300, abi.PTY_ERR_INVALID), ("x -algorithm=TOOLONGNAME", abi.PTY_ERR_INVALID)]:
+    for cmd, code in [("x -bitDepth=16", abi.PTY_ERR_UNSUPPORTED), ("x -fp=" + "a" * 300, abi.PTY_ERR_INVALID),
+                      ("x -algorithm=TOOLONGNAME", abi.PTY_ERR_INVALID)]:
         assert L.pty_params_from_cmdline(cmd.encode(), ctypes.byref(p)) == code, cmd
         assert L.pty_last_error()
         assert p.size == 77
-    assert ok("x -drift=0,0 -bitDepth=32").size == 256
+    assert ok("x -bitDepth=32").size == 256
     assert L.pty_params_from_cmdline(None, ctypes.byref(p)) == abi.PTY_ERR_INVALID
 
 
@@ -121,6 +127,6 @@ def test_module_entry_points_check_the_string():
     with pytest.raises(NotImplementedError):  # the reference's own MLs example reads HDF5 files
         pt.mlsinit(REALSTR)
     with pytest.raises(NotImplementedError):
-        pt.epiecmdstr("./ptycho -simulate=1 -drift=1e-9,1e-9")
+        pt.epiecmdstr("./ptycho -simulate=1 -bitDepth=16")
     with pytest.raises(TypeError):
         pt.dmcmdstr(cmdstr="./ptycho", size=64)

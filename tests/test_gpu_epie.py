@@ -111,6 +111,35 @@ def test_scan_meshes_match_oracle(oracle, tmp_path):
     assert np.isfinite(s.object()).all()
 
 
+def test_scan_drift_matches_oracle(oracle, tmp_path):
+    """The scan drift (the reference's command-line `drift`): raster, spiral and position-list sessions with a drift
+    place their positions where the oracle does, bit for bit, and the object grows to hold them."""
+    from gpu_helpers import dataset, gpu_session
+
+    d = dataset(N=64, nx=5, algorithm="ePIE")
+    kw = d["kw"]
+    lam, z, dxd = kw["lambd"], kw["z"], kw["dx_d"]
+    dr = (3e-9, -2e-9)
+    s = gpu_session(d, probe=d["probe"], driftx=dr[0], drifty=dr[1])
+    pos, X, Y = oracle.cartesian_mesh(5, 5, kw["stepx"], kw["stepy"], lam, z, dxd, 64, drift=dr)
+    assert np.array_equal(s.positions(), pos) and (s.dims()["X"], s.dims()["Y"]) == (X, Y)
+    assert (X, Y) != (d["X"], d["Y"])
+    s.close()
+    s = gpu_session(d, probe=d["probe"], spiralScan=1, seed=3, driftx=dr[0], drifty=dr[1])
+    pos, X, Y = oracle.spiral_mesh(25, kw["stepx"], kw["stepy"], lam, z, dxd, 64, drift=dr)
+    assert np.array_equal(s.positions(), pos) and (s.dims()["X"], s.dims()["Y"]) == (X, Y)
+    s.close()
+    xy = (np.random.default_rng(1).random((25, 2)) * 0.4e-6).astype(np.float64)
+    f = tmp_path / "positions.csv"
+    f.write_text("".join(f"{float(a)!r},{float(b)!r}\n" for a, b in xy))
+    s = gpu_session(d, probe=d["probe"], lf=str(f), driftx=dr[0], drifty=dr[1])
+    pos, X, Y = oracle.list_mesh(xy, lam, z, dxd, 64, drift=dr)
+    assert np.array_equal(s.positions(), pos) and (s.dims()["X"], s.dims()["Y"]) == (X, Y)
+    s.step()
+    assert np.isfinite(s.object()).all()
+    s.close()
+
+
 @pytest.mark.parametrize("K", [1, 3])
 def test_epie_tensor_core_fft_chain(oracle, K):
     """precision=1: ePIE as a per-position kernel chain whose transforms run as split-BF16 tensor-core stages

@@ -69,6 +69,39 @@ def test_ref_cartesian_mesh_bit_exact(ref, oracle):
         assert np.array_equal(got, want), (nx, ny, N)
 
 
+def test_ref_mesh_drift(ref, oracle):
+    """d_generateMesh with a scan drift, Cartesian (several shapes, mirrored too), list and spiral (1100 points: two
+    1024-wide mesh rows), against the oracle's restatement.  Cartesian and list positions are bit-exact; the
+    spiral's cos/sin are CUDA's single-precision functions in the reference and double-precision ones rounded to
+    float in the oracle, so those positions agree to a few units in the last place."""
+    torch = _torch()
+    lambd, z, dx_d, N = 2.48e-10, 1.0, 172e-6, 128
+    inv = float(np.float32(1.0 / np.float64(np.float32(oracle.sample_pixel(lambd, z, dx_d, N)))))
+    for drift in [(3.1e-9, -1.7e-9), (-2.5e-10, 4.25e-9)]:
+        dr = tuple(float(np.float32(v)) for v in drift)
+        for nx, ny, step, mx, my in [(7, 13, 35e-9, 0, 0), (30, 30, 50e-9, 1, 0), (5, 40, 80e-9, 0, 1)]:
+            ay = ref.align32(ny)
+            pos = torch.zeros((nx * ay, 2), dtype=torch.float32, device="cuda")
+            s32 = float(np.float32(step))
+            ref.call("ref_mesh", 1, ref.ptr(pos), nx, ny, s32, s32, inv, mx, my, dr[0], dr[1])
+            got = pos.cpu().numpy().reshape(nx, ay, 2)[:, :ny].reshape(-1, 2)
+            want = oracle.mesh_raw_drift("cartesian", lambd, z, dx_d, N, dr, nx=nx, ny=ny, stepx=step, stepy=step,
+                                         mirrorX=mx, mirrorY=my)
+            assert np.array_equal(got, want), (nx, ny, drift)
+        xy = np.random.default_rng(5).random((1100, 2)) * 1e-6
+        buf = np.zeros((2048, 2), np.float32)
+        buf[:1100] = xy.astype(np.float32)
+        pos = _dev(buf)
+        ref.call("ref_mesh", 2, ref.ptr(pos), 2, 1024, 0.0, 0.0, inv, 0, 0, dr[0], dr[1])
+        want = oracle.mesh_raw_drift("list", lambd, z, dx_d, N, dr, xy_m=xy)
+        assert np.array_equal(pos.cpu().numpy(), want), drift
+        pos = torch.zeros((2048, 2), dtype=torch.float32, device="cuda")
+        s32 = float(np.float32(50e-9))
+        ref.call("ref_mesh", 3, ref.ptr(pos), 2, 1024, s32, s32, inv, 0, 0, dr[0], dr[1])
+        want = oracle.mesh_raw_drift("spiral", lambd, z, dx_d, N, dr, P=1100, stepx=50e-9, stepy=50e-9)
+        assert np.abs(pos.cpu().numpy() - want).max() <= 4e-6 * np.abs(want).max(), drift
+
+
 # The texture unit filters float texels with weights of 8 fractional bits (rounded to the nearest 1/256, pinned
 # bit-exactly below) but with arithmetic of about 12 significant bits: gathered values differ from an exact FP32
 # bilinear interpolation with the same weights by up to ~6e-4 of the object's magnitude (measured on B200).  The

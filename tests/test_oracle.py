@@ -284,3 +284,30 @@ def test_mls_default_path_position_steps_are_clamped(oracle):
     assert spreads[0] == 0.0, spreads  # no search before iteration PPS
     assert max(spreads) <= 0.4 + 1e-4, spreads
     assert max(spreads) > 0.2, spreads  # the search takes steps of the clamp's order
+
+
+def test_scan_drift(oracle):
+    """The scan drift adds row * driftx and column * drifty metres before the pixel conversion
+    (src/ScanMeshKernels.cu:86-87): raster rows move by i * driftx / dx_s; list and spiral points by their row
+    (index / 1024) and column (index % 1024) of the mesh array.  A zero drift changes nothing."""
+    lam, z, dxd, N = 2.48e-10, 1.0, 172e-6, 64
+    dx_s = oracle.lib().orc_sample_pixel(lam, z, dxd, N)
+    dr = (3e-9, -2e-9)
+    raw0 = oracle.mesh_raw_drift("cartesian", lam, z, dxd, N, (0.0, 0.0), nx=5, ny=7, stepx=50e-9, stepy=40e-9)
+    assert np.array_equal(raw0, oracle.cartesian_mesh_raw(5, 7, 50e-9, 40e-9, lam, z, dxd, N))
+    raw = oracle.mesh_raw_drift("cartesian", lam, z, dxd, N, dr, nx=5, ny=7, stepx=50e-9, stepy=40e-9)
+    i, j = np.divmod(np.arange(35), 7)
+    assert np.allclose(raw - raw0, np.stack([i * dr[0], j * dr[1]], 1) / dx_s, atol=1e-4)
+    p0, X0, Y0 = oracle.cartesian_mesh(5, 7, 50e-9, 40e-9, lam, z, dxd, N)
+    p1, X1, Y1 = oracle.cartesian_mesh(5, 7, 50e-9, 40e-9, lam, z, dxd, N, drift=dr)
+    assert (X1, Y1) != (X0, Y0) and p1.min() >= 0
+    xy = np.random.default_rng(2).random((1100, 2)) * 1e-6
+    l0 = oracle.mesh_raw_drift("list", lam, z, dxd, N, (0.0, 0.0), xy_m=xy)
+    l1 = oracle.mesh_raw_drift("list", lam, z, dxd, N, dr, xy_m=xy)
+    assert l1.shape == (2048, 2) and np.array_equal(l0[1100:], np.zeros((948, 2), np.float32))
+    r, c = np.divmod(np.arange(2048), 1024)
+    assert np.allclose(l1 - l0, np.stack([r * dr[0], c * dr[1]], 1) / dx_s, atol=1e-4)
+    assert np.array_equal(oracle.list_mesh(xy, lam, z, dxd, N)[0], oracle.list_mesh(xy, lam, z, dxd, N, drift=(0, 0))[0])
+    s0 = oracle.mesh_raw_drift("spiral", lam, z, dxd, N, (0.0, 0.0), P=1100, stepx=50e-9, stepy=50e-9)
+    s1 = oracle.mesh_raw_drift("spiral", lam, z, dxd, N, dr, P=1100, stepx=50e-9, stepy=50e-9)
+    assert np.allclose(s1 - s0, np.stack([r * dr[0], c * dr[1]], 1) / dx_s, atol=1e-3)
