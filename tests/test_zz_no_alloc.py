@@ -60,6 +60,10 @@ def test_no_alloc_fft_all_sizes_leave_device_memory_unchanged():
     def run(datas, side=None):
         for k, ((N, batch, inverse), d) in enumerate(zip(cases, datas)):
             stream = ctypes.c_void_p(side.cuda_stream) if side is not None and k == 2 else None
+            if stream is not None:
+                # calls share the static scratch, so they must not overlap: the side stream (non-blocking) waits
+                # for the calls already queued on the default stream
+                side.wait_stream(torch.cuda.current_stream())
             rc = lib.pty_fft2_dev_noalloc(ctypes.c_void_p(d.data_ptr()), batch, N, int(inverse), stream)
             assert rc == abi.PTY_OK, lib.pty_last_error().decode()
             if stream is not None:
