@@ -87,6 +87,12 @@ typedef struct pty_params {
                              the mesh array (Cartesian: raster row i and column j; list and spiral: index / 1024
                              and index % 1024), added before the pixel conversion like the reference's
                              command-line option `drift` (d_generateMesh, src/ScanMeshKernels.cu:86-87); 0 = none */
+  int bitDepth;           /* detector bit depth, 1..32 (0 = not given: 32), the reference's command-line `bitDepth`.
+                             ePIE lets pixels with amplitude >= the saturation level float (no modulus constraint,
+                             src/utilitiesKernels.cu:619-682); the level is 2^bitDepth - 1 - threshold, square-rooted
+                             with sqrtData, truncated to an integer at each step like the reference's
+                             pixelSaturation (src/Parameters.cpp:54-62), and set only when bitDepth, threshold or
+                             sqrtData is given (otherwise no pixel floats) */
 } pty_params;
 
 typedef struct pty_session pty_session;
@@ -100,8 +106,8 @@ int pty_params_init(pty_params* p);
  * -simulate=1": white-space separated "-name=value" options after the program name, over the command line's own
  * defaults (beamSize 1e-7, lambda 2.48e-10, z 1, scanDims 12 x 12, size 256, PPS 5; the rest as pty_params_init),
  * each option with the reference's range check.  Names match exactly, ignoring case; the last occurrence wins.
- * `-drift=dx,dy` sets driftx / drifty.  PTY_ERR_UNSUPPORTED for a `bitDepth` other than 32, PTY_ERR_INVALID for a
- * text value longer than its field; `p` is left unchanged on an error.  Replaces the tokeniser of the command-string entry points
+ * `-drift=dx,dy` sets driftx / drifty, `-bitDepth=b` bitDepth.  PTY_ERR_INVALID for a text value longer than its
+ * field or a bitDepth above 32; `p` is left unchanged on an error.  Replaces the tokeniser of the command-string entry points
  * (src/ptychopy.c:543-576) and Parameters::parseFromCommandLine (src/Parameters.cpp:66-375) with the defaults of
  * src/Parameters.h:67-170. */
 int pty_params_from_cmdline(const char* cmdstr, pty_params* p);

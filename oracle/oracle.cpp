@@ -307,6 +307,9 @@ void probe_guess(const R* amp, int P, int N, double beamSize, double dx_s, int K
 struct Flags {
   int phaseConstraint = 1, updateProbe = 10, updateModes = 20;
   int calculateRMS = 0;
+  // ePIE's saturation level (float, as the reference's saturationValue): a pixel whose amplitude A has
+  // A - saturation >= 0 floats (letFloat, src/utilitiesKernels.cu:619-624); +inf: none floats
+  float saturation = std::numeric_limits<float>::infinity();
 };
 
 template <typename R> struct State {
@@ -399,15 +402,19 @@ R epie_iteration(State<R>& s, const R* amp, const float* pos, const R* sqsum, co
     for (int k = 0; k < Ka; ++k) std::copy(&psiOld[k * NN], &psiOld[k * NN] + NN, &Psi[k * NN]);
     fft2_modes(f, Psi.data(), Ka, false, nthreads);
     const R* A = amp + size_t(i) * NN;
+    // a floating pixel (d_adjustFFT / d_adjustModalFFT, src/utilitiesKernels.cu:634-682) keeps Psi with one mode
+    // and takes the modal factor with 1 in place of A with several
+    auto floats = [&](size_t p) { return float(A[p]) - fl.saturation >= 0.f; };
     if (Ka == 1) {
-      for (size_t p = 0; p < NN; ++p) psi[p] = modulus_phase(Psi[p], A[p]) * nrm;
+      for (size_t p = 0; p < NN; ++p) psi[p] = (floats(p) ? Psi[p] : modulus_phase(Psi[p], A[p])) * nrm;
     } else {
       for (size_t p = 0; p < NN; ++p) {
         R m2 = 0;
         for (int k = 0; k < Ka; ++k) m2 += std::norm(Psi[k * NN + p]);
         // rsqrt(0) gives inf and 0*inf = NaN in the reference; a pixel with no modal power is pinned to 0 here.
         R sc = m2 > R(0) ? R(1) / std::sqrt(m2) : R(0);
-        for (int k = 0; k < Ka; ++k) psi[k * NN + p] = Psi[k * NN + p] * (A[p] * sc * nrm);
+        const R a = floats(p) ? R(1) : A[p];
+        for (int k = 0; k < Ka; ++k) psi[k * NN + p] = Psi[k * NN + p] * (a * sc * nrm);
       }
     }
     if (fl.calculateRMS) {  // error on FFT(psi_old), src/utilities.cpp:188-195, src/utilitiesKernels.cu:684-712
@@ -1481,6 +1488,7 @@ namespace {
 struct OrcBase {
   virtual ~OrcBase() {}
   virtual void set_reduce(DmReduceFn fn, void* user) = 0;
+  virtual void set_saturation(float level) = 0;
   virtual int step(double* err) = 0;
   virtual void get(double* obj, double* probe, double* scalars) = 0;
   virtual void psi(double* out) = 0;
@@ -1512,6 +1520,7 @@ template <typename R> struct OrcSessionT : OrcBase {
     reduce = fn;
     reduce_user = user;
   }
+  void set_saturation(float level) override { fl.saturation = level; }
   void get(double* obj, double* probe, double* scalars) override {
     store_state(s, obj, probe);
     if (scalars) {
@@ -1584,6 +1593,12 @@ void* orc_create(int algo, int N, int K, int P, int X, int Y, const double* amp,
                  int phaseConstraint, int updateProbe, int updateModes, int calculateRMS, int nthreads) {
   return orc_create2(0, algo, N, K, P, X, Y, amp, pos, obj, probe, probeGuessPath, modesGiven, seed,
                      phaseConstraint, updateProbe, updateModes, calculateRMS, nthreads);
+}
+
+// ePIE's saturation level (pixels with amplitude >= level float); +inf (the default) floats none.
+int orc_set_saturation(void* h, double level) {
+  static_cast<OrcBase*>(h)->set_saturation(float(level));
+  return 0;
 }
 
 // Runs the next iteration; err receives the iteration's error metric (ePIE with calculateRMS; 0 for DM).

@@ -50,6 +50,7 @@ def lib():
             "orc_mesh_raw_drift": ([i, i, i, vp, d, d, d, d, d, i, i, i, d, d, vp], i),
             "orc_mesh_jitter": ([u64, i, ctypes.c_uint, vp], i),
             "orc_set_dm_reduce": ([vp, vp, vp], i),
+            "orc_set_saturation": ([vp, d], i),
             "orc_probe_guess": ([vp, i, i, d, d, i, vp], i),
             "orc_visiting_order": ([ctypes.POINTER(u64), i, vp], None),
             "orc_extract_patch": ([vp, i, i, f, f, i, vp], i),
@@ -167,6 +168,16 @@ def spiral_mesh(P, stepx, stepy, lambd, z, dx_d, N, flip=0, jitter=0, seed=0, dr
     return pos, int(xy[0]), int(xy[1])
 
 
+def saturation_level(bitDepth=0, threshold=0, sqrtData=0):
+    """The ePIE saturation level of Parameters::updatePixelSaturation (src/Parameters.cpp:54-62): 2^bitDepth - 1 -
+    threshold (bitDepth 0: 32), square-rooted with sqrtData, each step truncated to the integer the reference holds
+    it in; inf (no pixel floats) unless one of the three is given."""
+    if bitDepth <= 0 and threshold <= 0 and not sqrtData:
+        return np.inf
+    v = max(np.floor(2.0 ** (bitDepth if bitDepth > 0 else 32) - 1 - max(threshold, 0)), 0.0)
+    return float(np.float32(np.floor(np.sqrt(v)) if sqrtData else v))
+
+
 def mesh_jitter(seed, n, radius):
     """The seeded jitter stream: (n, 2) float32 offsets in pixels."""
     out = np.zeros((n, 2), np.float32)
@@ -200,7 +211,8 @@ class OracleSession:
     """FP64 restatement of one reconstruction (algo 'ePIE' or 'DM'), stepped one iteration at a time."""
 
     def __init__(self, algo, amp, pos, obj, probe, *, probe_guess_path, modes_given=False, seed=0x5EED5EED,
-                 phaseConstraint=1, updateProbe=10, updateModes=20, calculateRMS=0, nthreads=1, fp32=False):
+                 phaseConstraint=1, updateProbe=10, updateModes=20, calculateRMS=0, nthreads=1, fp32=False,
+                 saturation=None):
         self.amp = np.ascontiguousarray(amp, np.float64)
         self.pos = np.ascontiguousarray(pos, np.float32)
         obj = np.ascontiguousarray(obj, np.complex128)
@@ -215,6 +227,8 @@ class OracleSession:
                                   seed, phaseConstraint, updateProbe, updateModes, calculateRMS, nthreads)
         if not self.h:
             raise ValueError("oracle rejected the configuration")
+        if saturation is not None:  # ePIE: pixels with amplitude >= saturation float
+            lib().orc_set_saturation(self.h, float(saturation))
 
     # DM position shards: fn(dO, dP) receives the iteration's increments as complex128 arrays (object, probe) and
     # must sum them over all shards in place.

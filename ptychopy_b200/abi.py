@@ -58,7 +58,7 @@ class PtyParams(ctypes.Structure):
         ("PPS", ctypes.c_int), ("seed", ctypes.c_uint64), ("calculateRMS", ctypes.c_int),
         ("device", ctypes.c_int), ("wave", ctypes.c_int), ("precision", ctypes.c_int),
         ("mlsCore", ctypes.c_int), ("save", ctypes.c_int), ("outputDir", ctypes.c_char * 256),
-        ("driftx", ctypes.c_double), ("drifty", ctypes.c_double),
+        ("driftx", ctypes.c_double), ("drifty", ctypes.c_double), ("bitDepth", ctypes.c_int),
     ]
 
 

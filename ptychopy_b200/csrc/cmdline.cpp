@@ -14,8 +14,8 @@
 //     after "-T=60" would reset T;
 //   * "-step=v" with one value reads it as a real number (the reference truncates it with atoi);
 //   * each call starts from the defaults (the reference's parameter singleton keeps what earlier calls set);
-//   * an option this engine cannot honour is refused instead of ignored: a `bitDepth` other than 32 (a lower
-//     saturation level).  Options with no effect on a reconstruction here are accepted and ignored, as the reference ignores
+//   * a `bitDepth` above 32 is refused (the reference's 64-bit saturation level would overflow past 63).  Options
+//     with no effect on a reconstruction here are accepted and ignored, as the reference ignores
 //     names it does not know: blind (unused there), threads (file-reading threads), angles, overlap,
 //     shareFrequency (multi-GPU stitching), updateVis, wsServerUrl (rendering).
 #include <cctype>
@@ -153,9 +153,10 @@ void apply(const Options& opt, pty_params* p) {
   if (opt.integer("beamstopMask", &v)) p->beamstopMask = v > 0;
   if (opt.integer("simulate", &v)) p->simulate = v > 0;
   if (opt.integer("spiralScan", &v)) p->spiralScan = v > 0;
-  if (opt.integer("bitDepth", &v) && v >= 1 && v != 32)
-    throw Refusal{PTY_ERR_UNSUPPORTED, "bitDepth " + std::to_string(v) +
-                                           ": this engine takes the saturation level of 32-bit detector data"};
+  if (opt.integer("bitDepth", &v) && v >= 1) {
+    if (v > 32) throw Refusal{PTY_ERR_INVALID, "bitDepth " + std::to_string(v) + " is above 32"};
+    p->bitDepth = v;
+  }
   if (opt.integer("flipScanAxis", &v)) p->flipScanAxis = v > 0;
   if (opt.integer("mirror1stScanAxis", &v)) p->mirror1stScanAxis = v > 0;
   if (opt.integer("mirror2ndScanAxis", &v)) p->mirror2ndScanAxis = v > 0;

@@ -95,18 +95,20 @@ void cache_release(int dev) {
 void DeviceBuf::alloc(size_t n, const char* what) {
   free();
   if (n == 0) n = 16;
+  const std::string w(what);
   int d = 0;
-  check_cuda(cudaGetDevice(&d), what);
+  check_cuda(cudaGetDevice(&d), (w + ": cudaGetDevice").c_str());
   need_device_index(d);
   size_t got = 0;
   cudaEvent_t ready = nullptr;
   void* q = cache_take(d, n, &got, &ready);
+  const bool recycled = q != nullptr;
   if (q && ready) {  // the block's last user may still be running
     const cudaError_t e = t_stream ? cudaStreamWaitEvent(t_stream, ready, 0) : cudaEventSynchronize(ready);
     cudaEventDestroy(ready);
     if (e != cudaSuccess) {
       cudaFree(q);
-      check_cuda(e, what);
+      check_cuda(e, (w + ": wait for the recycled block's last use").c_str());
     }
   }
   if (!q) {
@@ -116,18 +118,20 @@ void DeviceBuf::alloc(size_t n, const char* what) {
       cache_release(d);
       e = cudaMalloc(&q, n);
     }
-    check_cuda(e, what);
+    check_cuda(e, (w + ": cudaMalloc of " + std::to_string(n) + " bytes").c_str());
     got = n;
   }
   // every buffer starts at zero (accumulators, counters and padding rely on it), whether recycled or fresh (cudaMalloc
   // does not promise cleared memory: pages this process freed may come back as they were); complete before return,
   // since synchronous copies on the legacy stream are not ordered against the sessions' non-blocking streams
+  const std::string clear = w + ": clearing " + std::to_string(n) + " bytes of a " + std::to_string(got) + "-byte " +
+                            (recycled ? "recycled block" : "new block");
   if (t_stream) {
-    check_cuda(cudaMemsetAsync(q, 0, n, t_stream), what);
-    check_cuda(cudaStreamSynchronize(t_stream), what);
+    check_cuda(cudaMemsetAsync(q, 0, n, t_stream), (clear + " (cudaMemsetAsync)").c_str());
+    check_cuda(cudaStreamSynchronize(t_stream), (clear + " (stream synchronize)").c_str());
   } else {
-    check_cuda(cudaMemset(q, 0, n), what);
-    check_cuda(cudaDeviceSynchronize(), what);
+    check_cuda(cudaMemset(q, 0, n), (clear + " (cudaMemset)").c_str());
+    check_cuda(cudaDeviceSynchronize(), (clear + " (device synchronize)").c_str());
   }
   p = q;
   bytes = n;
@@ -699,6 +703,19 @@ std::vector<float> read_complex_csv(const std::string& path, size_t& rows, size_
     ++rows;
   }
   return out;
+}
+
+// The ePIE modulus step's saturation level (Parameters::updatePixelSaturation, src/Parameters.cpp:54-62):
+// 2^bitDepth - 1 - threshold, square-rooted with sqrtData, truncated to an integer at each step as the reference's
+// unsigned pixelSaturation holds it (a threshold above the range gives 0: every pixel floats).  +inf, so that no
+// pixel floats, unless bitDepth, threshold or sqrtData set it.
+float saturation_level(const pty_params& p) {
+  if (p.bitDepth <= 0 && p.threshold <= 0 && !p.sqrtData) return std::numeric_limits<float>::infinity();
+  const int bits = p.bitDepth > 0 ? p.bitDepth : 32;
+  double v = std::floor(std::ldexp(1.0, bits) - 1.0 - double(std::max(p.threshold, 0)));
+  if (v < 0) v = 0;
+  if (p.sqrtData) v = std::floor(std::sqrt(v));
+  return float(v);
 }
 
 // ---------------------------------------------------------------------------- initialisation
@@ -1456,10 +1473,7 @@ double step_epie(pty_session* s, int it, bool want_err) {
   g.sc = ep->sc.as<EpieScalars>();
   g.tw = s->tw.as<float2>();
   g.sqsum = ep->sq.as<double>();
-  g.saturation = s->prm.threshold > 0 || s->prm.sqrtData
-                     ? float(s->prm.sqrtData ? std::sqrt(4294967295.0 - s->prm.threshold)
-                                             : 4294967295.0 - s->prm.threshold)
-                     : std::numeric_limits<float>::infinity();
+  g.saturation = saturation_level(s->prm);
   g.N = s->N;
   g.K = s->K;
   g.Ka = Ka;
@@ -1637,6 +1651,7 @@ int pty_session_create(const pty_params* p, pty_session** out) {
     s->algo = parse_algo(p->algorithm);
     need(p->size > 16, "size must be larger than 16");  // src/Parameters.cpp:512-519
     need(p->probeModes >= 1, "probeModes must be >= 1");
+    need(p->bitDepth >= 0 && p->bitDepth <= 32, "bitDepth must be 1..32 (0: not given)");
     need(p->scanDimsx > 0 && p->scanDimsy > 0, "scanDimsx and scanDimsy must be positive");
     need(p->lambd > 0 && p->z > 0 && p->dx_d > 0 && p->beamSize > 0, "lambd, z, dx_d, beamSize must be positive");
     if (p->fp[0]) {  // whole-mode ingest reads .bin and .csv; .h5 needs the HDF5 library, not linked here
@@ -1814,8 +1829,7 @@ int pty_init(pty_session* s) {
       t.alloc(s->amp.bytes, "transposed patterns");
       check_cuda(transpose_planes(s->amp.as<float>(), t.as<float>(), s->P, s->N, s->stream), "transpose");
       check_cuda(cudaStreamSynchronize(s->stream), "transpose");
-      std::swap(s->amp.p, t.p);
-      std::swap(s->amp.bytes, t.bytes);
+      s->amp.swap(t);
       s->amp_transposed = true;
     }
     if (s->algo == ALGO_EPIE) {

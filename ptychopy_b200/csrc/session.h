@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/ptychopy_b200.h"
@@ -47,8 +48,18 @@ struct DeviceBuf {
   size_t bytes = 0;      // requested size
   size_t cap = 0;        // size of the underlying block
   int dev = -1;
+  DeviceBuf() = default;
+  DeviceBuf(const DeviceBuf&) = delete;  // one owner per block: a copy would return it to the cache twice
+  DeviceBuf& operator=(const DeviceBuf&) = delete;
   void alloc(size_t n, const char* what);
   void free();
+  // exchange the blocks of two buffers (every field: a block returns to the cache under its own size)
+  void swap(DeviceBuf& o) {
+    std::swap(p, o.p);
+    std::swap(bytes, o.bytes);
+    std::swap(cap, o.cap);
+    std::swap(dev, o.dev);
+  }
   template <typename T> T* as() const { return static_cast<T*>(p); }
   ~DeviceBuf() { free(); }
 };

@@ -107,12 +107,12 @@ def test_refusals_leave_the_parameters_unchanged():
     p = abi.PtyParams()
     L.pty_params_init(ctypes.byref(p))
     p.size = 77
-    for cmd, code in [("x -bitDepth=16", abi.PTY_ERR_UNSUPPORTED), ("x -fp=" + "a" * 300, abi.PTY_ERR_INVALID),
+    for cmd, code in [("x -bitDepth=40", abi.PTY_ERR_INVALID), ("x -fp=" + "a" * 300, abi.PTY_ERR_INVALID),
                       ("x -algorithm=TOOLONGNAME", abi.PTY_ERR_INVALID)]:
         assert L.pty_params_from_cmdline(cmd.encode(), ctypes.byref(p)) == code, cmd
         assert L.pty_last_error()
         assert p.size == 77
-    assert ok("x -bitDepth=32").size == 256
+    assert (ok("x -bitDepth=16").bitDepth, ok("x -bitDepth=0").bitDepth, ok("x").bitDepth) == (16, 0, 0)
     assert L.pty_params_from_cmdline(None, ctypes.byref(p)) == abi.PTY_ERR_INVALID
 
 
@@ -126,7 +126,7 @@ def test_module_entry_points_check_the_string():
         pt.epieinit(cmdstr="./ptycho -i=3")
     with pytest.raises(NotImplementedError):  # the reference's own MLs example reads HDF5 files
         pt.mlsinit(REALSTR)
-    with pytest.raises(NotImplementedError):
-        pt.epiecmdstr("./ptycho -simulate=1 -bitDepth=16")
+    with pytest.raises(ValueError):
+        pt.epiecmdstr("./ptycho -simulate=1 -bitDepth=40")
     with pytest.raises(TypeError):
         pt.dmcmdstr(cmdstr="./ptycho", size=64)

@@ -52,6 +52,31 @@ def test_epie_given_modes(oracle):
     assert rel_err(s.object(), ob) < TOL and rel_err(s.probe(), pr) < TOL
 
 
+@pytest.mark.parametrize("N,K,bits,sq", [(64, 1, 10, 1), (64, 3, 5, 0), (256, 3, 10, 1), (512, 1, 8, 1)])
+def test_epie_saturated_pixels_float(oracle, N, K, bits, sq):
+    """bitDepth (with sqrtData) sets the modulus step's saturation level; pixels at or above it float (one mode
+    keeps Psi, several take the modal factor with 1 for A: src/utilitiesKernels.cu:634-682).  Every ePIE variant
+    against the oracle with the same level: the shared-memory kernel (64^2, one mode), the cluster kernel (64^2,
+    modes from iteration 3), the kernel chain (256^2, modes from iteration 3; 512^2 with the modulus step in its
+    transform pass)."""
+    d = dataset(N=N, nx=3, K=K)
+    level = oracle.saturation_level(bits, 0, sq)
+    assert 0 < (d["amp"] >= level).mean() < 0.05  # a few pixels float
+    kw = dict(updateProbe=2, updateModes=3, calculateRMS=1, seed=9)
+    s = gpu_session(d, probe=d["probe"], bitDepth=bits, sqrtData=sq, **kw)
+    runs = [oracle.OracleSession("ePIE", d["amp"], d["pos"], np.zeros((d["X"], d["Y"])), d["probe"],
+                                 probe_guess_path=False, modes_given=K > 1, saturation=sat, **kw)
+            for sat in (level, None)]
+    for _ in range(4):
+        s.step()
+        for o in runs:
+            o.step()
+    (ob, pr, _), (ob0, _, _) = (o.state() for o in runs)
+    assert rel_err(s.object(), ob) < TOL and rel_err(s.probe(), pr) < TOL
+    assert rel_err(ob0, ob) > 10 * TOL  # the floating pixels changed the reconstruction
+    s.close()
+
+
 def test_epie_mode_initialisation(oracle):
     # modes created at updateModes from 0.05 * P0 and Gram-Schmidt: mode 0 and the object stay at parity
     # (the extra modes start at round-off level, so they are compared loosely)

@@ -311,3 +311,31 @@ def test_scan_drift(oracle):
     s0 = oracle.mesh_raw_drift("spiral", lam, z, dxd, N, (0.0, 0.0), P=1100, stepx=50e-9, stepy=50e-9)
     s1 = oracle.mesh_raw_drift("spiral", lam, z, dxd, N, dr, P=1100, stepx=50e-9, stepy=50e-9)
     assert np.allclose(s1 - s0, np.stack([r * dr[0], c * dr[1]], 1) / dx_s, atol=1e-3)
+
+
+def test_saturation_level(oracle):
+    """Parameters::updatePixelSaturation (src/Parameters.cpp:54-62): 2^bitDepth - 1 - threshold, square-rooted with
+    sqrtData, truncated at each step; no level (inf) unless one of the three is given."""
+    assert oracle.saturation_level() == np.inf
+    assert oracle.saturation_level(16, 0, 1) == 255.0  # floor(sqrt(65535)) = 255, not 255.998
+    assert oracle.saturation_level(8, 5, 0) == 250.0
+    assert oracle.saturation_level(0, 0, 1) == 65535.0
+    assert oracle.saturation_level(0, 7, 0) == float(np.float32(2.0 ** 32 - 8))
+    assert oracle.saturation_level(4, 100, 0) == 0.0  # a threshold above the range: every pixel floats
+
+
+def test_oracle_floating_pixels(oracle):
+    """An oracle ePIE iteration with a saturation level above every amplitude equals one without; a level inside
+    the data's range changes it."""
+    rng = np.random.default_rng(3)
+    N, X = 32, 48
+    amp = rng.random((4, N, N)) * 10
+    pos = np.array([[0, 0], [8, 4], [16, 16], [3, 11]], np.float32)
+    probe = (rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))) * 0.1
+    obj = np.ones((X, X), np.complex128)
+    runs = [oracle.OracleSession("ePIE", amp, pos, obj, probe, probe_guess_path=False, saturation=sat)
+            for sat in (None, 11.0, 5.0)]
+    for o in runs:
+        o.step()
+    (o0, _, _), (o1, _, _), (o2, _, _) = (o.state() for o in runs)
+    assert np.array_equal(o0, o1) and not np.allclose(o0, o2)
