@@ -95,9 +95,12 @@ void cache_release(int dev) {
 void DeviceBuf::alloc(size_t n, const char* what) {
   free();
   if (n == 0) n = 16;
-  const std::string w(what);
+  // a failure names the buffer and the CUDA call (the message is built only then)
+  auto checked = [what](cudaError_t e, const auto& step) {
+    if (e != cudaSuccess) check_cuda(e, (std::string(what) + ": " + step()).c_str());
+  };
   int d = 0;
-  check_cuda(cudaGetDevice(&d), (w + ": cudaGetDevice").c_str());
+  checked(cudaGetDevice(&d), [] { return std::string("cudaGetDevice"); });
   need_device_index(d);
   size_t got = 0;
   cudaEvent_t ready = nullptr;
@@ -108,7 +111,7 @@ void DeviceBuf::alloc(size_t n, const char* what) {
     cudaEventDestroy(ready);
     if (e != cudaSuccess) {
       cudaFree(q);
-      check_cuda(e, (w + ": wait for the recycled block's last use").c_str());
+      checked(e, [] { return std::string("wait for the recycled block's last use"); });
     }
   }
   if (!q) {
@@ -118,20 +121,24 @@ void DeviceBuf::alloc(size_t n, const char* what) {
       cache_release(d);
       e = cudaMalloc(&q, n);
     }
-    check_cuda(e, (w + ": cudaMalloc of " + std::to_string(n) + " bytes").c_str());
+    checked(e, [n] { return "cudaMalloc of " + std::to_string(n) + " bytes"; });
     got = n;
   }
   // every buffer starts at zero (accumulators, counters and padding rely on it), whether recycled or fresh (cudaMalloc
   // does not promise cleared memory: pages this process freed may come back as they were); complete before return,
   // since synchronous copies on the legacy stream are not ordered against the sessions' non-blocking streams
-  const std::string clear = w + ": clearing " + std::to_string(n) + " bytes of a " + std::to_string(got) + "-byte " +
-                            (recycled ? "recycled block" : "new block");
+  auto clear = [&](const char* call) {
+    return [=] {
+      return "clearing " + std::to_string(n) + " bytes of a " + std::to_string(got) + "-byte " +
+             (recycled ? "recycled" : "new") + " block (" + call + ")";
+    };
+  };
   if (t_stream) {
-    check_cuda(cudaMemsetAsync(q, 0, n, t_stream), (clear + " (cudaMemsetAsync)").c_str());
-    check_cuda(cudaStreamSynchronize(t_stream), (clear + " (stream synchronize)").c_str());
+    checked(cudaMemsetAsync(q, 0, n, t_stream), clear("cudaMemsetAsync"));
+    checked(cudaStreamSynchronize(t_stream), clear("stream synchronize"));
   } else {
-    check_cuda(cudaMemset(q, 0, n), (clear + " (cudaMemset)").c_str());
-    check_cuda(cudaDeviceSynchronize(), (clear + " (device synchronize)").c_str());
+    checked(cudaMemset(q, 0, n), clear("cudaMemset"));
+    checked(cudaDeviceSynchronize(), clear("device synchronize"));
   }
   p = q;
   bytes = n;
