@@ -90,7 +90,7 @@ struct Options {
     *v = std::atof(o->value.c_str());
     return true;
   }
-  // "a,b" into two values (a single value fills the first; `second_default` the second).
+  // "a,b" into two values (a single value fills the first, and the second too or `second_default`).
   template <typename T, typename Conv>
   bool pair(const char* name, T* a, T* b, bool single_fills_both, T second_default, Conv conv) const {
     const Option* o = find(name);
@@ -181,9 +181,11 @@ void apply(const Options& opt, pty_params* p) {
   auto to_int = [](const char* s) { return std::atoi(s); };
   auto to_real = [](const char* s) { return std::atof(s); };
   opt.pair("scanDims", &p->scanDimsx, &p->scanDimsy, false, 1, to_int);
-  opt.pair("drift", &p->driftx, &p->drifty, false, 0.0, to_real);
-  opt.pair("qxy", &p->qx, &p->qy, false, 0, to_int);
-  opt.pair("nxy", &p->nx, &p->ny, false, 0, to_int);
+  // one value without a comma fills both components: the reference reads the second from substr(npos + 1), i.e. from
+  // the start of the value again (src/Parameters.cpp:279-304)
+  opt.pair("drift", &p->driftx, &p->drifty, true, 0.0, to_real);
+  opt.pair("qxy", &p->qx, &p->qy, true, 0, to_int);
+  opt.pair("nxy", &p->nx, &p->ny, true, 0, to_int);
   opt.pair("step", &p->stepx, &p->stepy, true, 0.0, to_real);
   opt.real("beamSize", &p->beamSize);
   opt.real("lambda", &p->lambd);

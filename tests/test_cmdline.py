@@ -83,6 +83,14 @@ def test_drift():
     assert (ok("x").driftx, ok("x").drifty) == (0.0, 0.0)
 
 
+def test_single_values_fill_both_components():
+    """Without a comma the reference reads the second component from the start of the value again
+    (substr(npos + 1)): drift, qxy, nxy and step take one value for both; scanDims sets the second to 1."""
+    p = ok("x -drift=2e-9 -qxy=300 -nxy=640 -step=25e-9 -scanDims=9")
+    assert (p.driftx, p.drifty, p.qx, p.qy, p.nx, p.ny) == (2e-9, 2e-9, 300, 300, 640, 640)
+    assert (p.stepx, p.stepy, p.scanDimsx, p.scanDimsy) == (25e-9, 25e-9, 9, 1)
+
+
 def test_range_checks_keep_the_default():
     p = ok("x -size=16 -i=-1 -dpf=0 -probeModes=0 -PPS=0 -save=0 -fs=-2")
     assert (p.size, p.iter, p.dpf, p.probeModes, p.PPS, p.save, p.fs) == (256, 100, 1, 1, 5, 0, 0)
