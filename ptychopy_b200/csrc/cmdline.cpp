@@ -13,6 +13,7 @@
 //   * names match exactly (case-insensitive); the reference's value lookup matches by prefix, so "-threshold=5"
 //     after "-T=60" would reset T;
 //   * "-step=v" with one value reads it as a real number (the reference truncates it with atoi);
+//   * "-T=t" (the wall-time limit) keeps whole seconds, the limit pty_params holds;
 //   * each call starts from the defaults (the reference's parameter singleton keeps what earlier calls set);
 //   * a `bitDepth` above 32 is refused (the reference's 64-bit saturation level would overflow past 63).  Options
 //     with no effect on a reconstruction here are accepted and ignored, as the reference ignores
