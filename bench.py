@@ -248,7 +248,7 @@ def run_reference(args, rank):
         "config": {"workload": WORKLOAD, "N": 512, "positions": 900, "object": [ds["X"], ds["Y"]],
                    "step": "one DM iteration over all 900 patterns",
                    "l2": "inputs larger than L2 (exit waves 1.89 GB + amplitudes 0.94 GB per step)",
-                   "parallelism": "single GPU"},
+                   "parallelism": "replicas" if args.gpus > 1 else "single GPU"},  # as the GPU arm's config
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's CUDA sources do not build with CUDA 12.9; its DM is restated as a multithreaded "

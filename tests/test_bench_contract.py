@@ -1,0 +1,27 @@
+"""The benchmark's reference arm on the CPU: one JSON line with the keys the benchmark contract names, the same
+metric, unit and configuration keys as the GPU arm, and the CPU baseline it reports (no GPU needed)."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_prints_the_contract_line():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=900)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    r = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in r, k
+    assert r["impl"] == "reference" and r["value"] > 0 and r["higher_is_better"] is True
+    assert (r["n_gpus"], r["steps"], r["warmup"]) == (1, 1, 1)
+    assert set(r["config"]) == {"workload", "N", "positions", "object", "step", "l2", "parallelism"}
+    assert (r["config"]["N"], r["config"]["positions"], r["config"]["parallelism"]) == (512, 900, "single GPU")
+    cb = r["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == r["value"] and cb["sample"]
+    assert r["e2e"] == {"value": r["value"], "unit": r["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
