@@ -20,6 +20,7 @@
 //     names it does not know: blind (unused there), threads (file-reading threads), angles, overlap,
 //     shareFrequency (multi-GPU stitching), updateVis, wsServerUrl (rendering).
 #include <cctype>
+#include <climits>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -70,6 +71,15 @@ std::vector<Option> split_options(const char* s) {
   return out;
 }
 
+// atoi's reading (leading blanks, a sign, the digits up to the first other character; 0 when there are none),
+// clamped to the int range where atoi's result would be undefined.
+int to_int(const char* s) {
+  const long long v = std::strtoll(s, nullptr, 10);
+  if (v > INT_MAX) return INT_MAX;
+  if (v < INT_MIN) return INT_MIN;
+  return int(v);
+}
+
 struct Options {
   std::vector<Option> all;
   // The last occurrence of `name`, or nullptr.
@@ -82,7 +92,7 @@ struct Options {
   bool integer(const char* name, int* v) const {
     const Option* o = find(name);
     if (!o) return false;
-    *v = std::atoi(o->value.c_str());  // a bare flag reads as 0, like the reference's integer lookup
+    *v = to_int(o->value.c_str());  // a bare flag reads as 0, like the reference's integer lookup
     return true;
   }
   bool real(const char* name, double* v) const {
@@ -165,7 +175,7 @@ void apply(const Options& opt, pty_params* p) {
   if (opt.integer("binaryOutput", &v)) p->binaryOutput = v > 0;
   if (opt.integer("i", &v) && v >= 0) p->iter = v;
   if (opt.integer("save", &v) && v > 0) p->save = v;
-  if (opt.real("T", &d)) p->T = d > 0 ? int(d) : 0;
+  if (opt.real("T", &d)) p->T = d >= double(INT_MAX) ? INT_MAX : d > 0 ? int(d) : 0;
   if (opt.integer("size", &v) && v >= 32) p->size = v;
   if (opt.integer("PPS", &v) && v >= 1) p->PPS = v;
   if (opt.integer("probeModes", &v) && v >= 1) p->probeModes = v;
@@ -179,7 +189,6 @@ void apply(const Options& opt, pty_params* p) {
   if (opt.integer("phaseConstraint", &v) && v >= 0) p->phaseConstraint = v;
   text(opt, "fp", p->fp, sizeof(p->fp));
   text(opt, "hdf5path", p->hdf5path, sizeof(p->hdf5path));
-  auto to_int = [](const char* s) { return std::atoi(s); };
   auto to_real = [](const char* s) { return std::atof(s); };
   opt.pair("scanDims", &p->scanDimsx, &p->scanDimsy, false, 1, to_int);
   // one value without a comma fills both components: the reference reads the second from substr(npos + 1), i.e. from

@@ -91,6 +91,13 @@ def test_single_values_fill_both_components():
     assert (p.stepx, p.stepy, p.scanDimsx, p.scanDimsy) == (25e-9, 25e-9, 9, 1)
 
 
+def test_numbers_read_like_atoi_and_atof():
+    """Integers are read up to the first non-digit (atoi), out-of-range ones clamp; reals as atof."""
+    p = ok("x -size=128px -i=1e3 -fs= -dpf=99999999999999999999 -T=1e30 -z=2.5m -jitterRadius=-3")
+    assert (p.size, p.iter, p.fs, p.dpf, p.T, p.z) == (128, 1, 0, 2147483647, 2147483647, 2.5)
+    assert p.jitterRadius == 0  # negative: out of the option's range, the default stays
+
+
 def test_range_checks_keep_the_default():
     p = ok("x -size=16 -i=-1 -dpf=0 -probeModes=0 -PPS=0 -save=0 -fs=-2")
     assert (p.size, p.iter, p.dpf, p.probeModes, p.PPS, p.save, p.fs) == (256, 100, 1, 1, 5, 0, 0)
