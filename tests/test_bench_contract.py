@@ -2,6 +2,7 @@
 metric, unit and configuration keys as the GPU arm, and the CPU baseline it reports (no GPU needed)."""
 import json
 import os
+import socket
 import subprocess
 import sys
 
@@ -25,3 +26,20 @@ def test_reference_arm_prints_the_contract_line():
     cb = r["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == r["value"] and cb["sample"]
     assert r["e2e"] == {"value": r["value"], "unit": r["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_under_torchrun_prints_once():
+    """Launched as the multi-GPU run is (torchrun, 2 ranks): rank 0 alone runs and prints one line whose
+    configuration says replicas, like the GPU arm's at N > 1; the other rank exits 0 without work."""
+    with socket.socket() as sk:  # a free port for the rendezvous
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    out = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+                          "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
+                          "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1"],
+                         cwd=ROOT, capture_output=True, text=True, timeout=900)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    r = json.loads(lines[0])
+    assert r["impl"] == "reference" and r["n_gpus"] == 2 and r["config"]["parallelism"] == "replicas"
